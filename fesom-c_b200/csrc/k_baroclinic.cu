@@ -1,0 +1,510 @@
+// Internal-mode (baroclinic) kernels of oce_timestep case(3)
+// (src/fv_main.F90:1983-2070):
+//   pressure_col : densityJM + hydrostatic prefix sum per node column
+//   bpg_elem     : baroclinic_pressure_gradient_3D per element column
+//   velgrad3d    : vel_gradients (least squares, free slip) per (elem, level)
+//   velrhs       : compute_vel_rhs up to the AB combine, per (elem, level):
+//                  pressure force, Coriolis/AB2 history, upwind horizontal
+//                  momentum advection gathered over the element's edges,
+//                  filter viscosity, QUICK vertical advection
+//   implvisc     : implicit vertical viscosity per element column
+//                  (momentum_vert_impl_visc_tmp / momentum_vert_impl_visc)
+//   update3d     : update_3D_vel per element column
+//   wvel         : vert_vel_sigma per node column (edge gather + reverse scan)
+//   jac_swap     : jacobian bookkeeping (eta at the previous / last call)
+#include "device_common.cuh"
+
+namespace fesomc {
+
+// ---------------------------------------------------------------------------
+// pressure (fv_pressure_new.F90:91-107): one thread per node column
+// ---------------------------------------------------------------------------
+__global__ void k_pressure_col(Dev d) {
+    const double gd0 = kG / d.density_0;
+    GRID_LOOP(ii, d.N) {
+        const int n = (int)ii;
+        const int L = d.L, NS = d.NS;
+        const double a = jac_a(d, d.eta_jac, n);
+        double hp = 0.0;
+        d.hpressure[(size_t)n * NS] = 0.0;
+        for (int z = 0; z < L; ++z) {
+            const double rho = density_jm(d.TF[(size_t)n * L + z], d.SF[(size_t)n * L + z], -z_of(d, a, z), d.density_0);
+            d.rho_c[(size_t)n * L + z] = rho;
+            hp = hp + rho * jc_of(d, a, z) * gd0;
+            d.hpressure[(size_t)n * NS + z + 1] = hp;
+        }
+    }
+}
+
+// baroclinic_pressure_gradient_3D (fv_pressure_new.F90:146-221), thread per element
+__global__ void k_bpg_elem(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int L = d.L, NS = d.NS;
+        const int4 en = d.elem_nodes[e];
+        const int nd[4] = {en.x, en.y, en.z, en.w};
+        const double4 gx = d.gs_x[e], gy = d.gs_y[e], w = d.w_cv[e];
+        double dh[4], de[4];
+        for (int k = 0; k < 4; ++k) { dh[k] = d.depth[nd[k]] + d.eta_n[nd[k]]; de[k] = d.depth[nd[k]]; }
+        const double Ax = wsum(gx, dh[0], dh[1], dh[2], dh[3]);
+        const double Ay = wsum(gy, dh[0], dh[1], dh[2], dh[3]);
+        const double Bx = wsum(gx, de[0], de[1], de[2], de[3]);
+        const double By = wsum(gy, de[0], de[1], de[2], de[3]);
+        const double fac = d.elem_bpfac[e];
+        const double4 ae = elem_jac_a(d, d.eta_jac, en);
+        const double an[4] = {ae.x, ae.y, ae.z, ae.w};
+        double b1 = 0.0, b2 = 0.0;
+        for (int z = 0; z < L; ++z) {
+            const double je = je_of(d, w, ae, z);
+            const double accJe_inv = -fac / je;
+            double hu[4], hl[4], pre[4];
+            for (int k = 0; k < 4; ++k) {
+                hu[k] = d.hpressure[(size_t)nd[k] * NS + z];
+                hl[k] = d.hpressure[(size_t)nd[k] * NS + z + 1];
+                pre[k] = 0.5 * (hu[k] + hl[k]) * jc_of(d, an[k], z);
+            }
+            const double qd_up = wsum(w, hu[0], hu[1], hu[2], hu[3]);
+            const double qd_low = wsum(w, hl[0], hl[1], hl[2], hl[3]);
+            const double sx = wsum(gx, pre[0], pre[1], pre[2], pre[3]);
+            const double sy = wsum(gy, pre[0], pre[1], pre[2], pre[3]);
+            const double s0 = __ldg(d.sig + z), s1 = __ldg(d.sig + z + 1);
+            const double bu = accJe_inv * (sx + qd_low * (s1 * Ax - Bx) - qd_up * (s0 * Ax - Bx));
+            const double bv = accJe_inv * (sy + qd_low * (s1 * Ay - By) - qd_up * (s0 * Ay - By));
+            d.Bar_pru[(size_t)e * L + z] = bu;
+            d.Bar_prv[(size_t)e * L + z] = bv;
+            b1 = b1 + bu * je;
+            b2 = b2 + bv * je;
+        }
+        d.Bar_pr_2D[e] = make_double2(b1, b2);
+    }
+}
+
+// vel_gradients (fv_gradients.F90:2-93), one thread per (element, level)
+__global__ void k_velgrad3d(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        const int4 en = d.elem_nodes[e];
+        const int4 nb = d.elem_nb[e];
+        const int4 ee = d.elem_edges[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
+        const double4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const double gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const double gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const int jend = (en.x == en.w) ? 3 : 4;
+        const double u0 = d.U_n[ii], v0 = d.V_n[ii];
+        double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+        for (int j = 0; j < jend; ++j) {
+            const int e2 = nbs[j];
+            if (e2 >= 0) {
+                const double u2 = d.U_n[(size_t)e2 * L + z], v2 = d.V_n[(size_t)e2 * L + z];
+                a1 = a1 + gxa[j] * (u2 - u0);
+                a2 = a2 + gya[j] * (u2 - u0);
+                a3 = a3 + gxa[j] * (v2 - v0);
+                a4 = a4 + gya[j] * (v2 - v0);
+            } else {
+                const double2 dxy = d.edge_dxdy[eds[j]];
+                const double zc1 = dxy.x * d.elem_cos[e], zc2 = dxy.y;
+                const double un = -2.0 * (u0 * zc2 - v0 * zc1) / (zc1 * zc1 + zc2 * zc2);
+                a1 = a1 + gxa[j] * un * zc2;
+                a2 = a2 + gya[j] * un * zc2;
+                a3 = a3 - gxa[j] * un * zc1;
+                a4 = a4 - gya[j] * un * zc1;
+            }
+        }
+        d.vgux[ii] = a1;
+        d.vguy[ii] = a2;
+        d.vgvx[ii] = a3;
+        d.vgvy[ii] = a4;
+    }
+}
+
+// w-weighted element mean of a node column value: SUM(w_cv*X(k,nodes))
+__device__ __forceinline__ double wsum_col(const double4 &w, const double *X, int stride, const int4 &en, int k) {
+    return wsum(w, X[(size_t)en.x * stride + k], X[(size_t)en.y * stride + k], X[(size_t)en.z * stride + k],
+                X[(size_t)en.w * stride + k]);
+}
+__device__ __forceinline__ double wsum_zbar(const Dev &d, const double4 &w, const double4 &a, int k) {
+    return wsum(w, zbar_of(d, a.x, k), zbar_of(d, a.y, k), zbar_of(d, a.z, k), zbar_of(d, a.w, k));
+}
+__device__ __forceinline__ double wsum_z(const Dev &d, const double4 &w, const double4 &a, int k) {
+    return wsum(w, z_of(d, a.x, k), z_of(d, a.y, k), z_of(d, a.z, k), z_of(d, a.w, k));
+}
+
+// Vertical momentum flux uvertAB(:,k) of momentum_vert_adv_upwind at interface
+// k (0-based, 0..NS-1) of element e (fv_advection.F90:389-443).
+__device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const double4 &w, const double4 &a,
+                                         const int4 &en, double ar, double &fu, double &fv) {
+    const int L = d.L, NS = d.NS;
+    const double *U = d.U_n + (size_t)e * L;
+    const double *V = d.V_n + (size_t)e * L;
+    if (k == NS - 1) { fu = 0.0; fv = 0.0; return; }
+    const double wv = wsum_col(w, d.Wvel, NS, en, k) * ar;
+    if (k == 0) { fu = -wv * U[0]; fv = -wv * V[0]; return; }
+    const int nz = k + 1;  // 1-based interface index, 2..NS-1
+    double umean = 0.0, vmean = 0.0;
+    // U_n(m) 1-based  ->  U[m-1]
+    if (wv >= 0.0) {
+        if (nz == NS - 1) {
+            umean = 0.5 * (U[nz - 2] + U[nz - 1]);
+            vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
+        } else {
+            const double Z1 = wsum_zbar(d, w, a, nz - 1);
+            const double aa = Z1 - wsum_z(d, w, a, nz - 2);
+            const double bb = wsum_z(d, w, a, nz - 1) - Z1;
+            const double cc = wsum_z(d, w, a, nz) - Z1;
+            const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
+            const double dg = aa * bb * (aa + bb) / dd;
+            const double db = -aa * cc * (aa + cc) / dd;
+            const double da = 1.0 - dg - db;
+            umean = U[nz - 2] * da + U[nz - 1] * db + U[nz] * dg;
+            vmean = V[nz - 2] * da + V[nz - 1] * db + V[nz] * dg;
+        }
+    }
+    if (wv < 0.0) {
+        if (nz == 2) {
+            umean = 0.5 * (U[nz - 2] + U[nz - 1]);
+            vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
+        } else {
+            const double Z1 = wsum_zbar(d, w, a, nz - 1);
+            const double aa = wsum_z(d, w, a, nz - 1) - Z1;
+            const double bb = Z1 - wsum_z(d, w, a, nz - 2);
+            const double cc = Z1 - wsum_z(d, w, a, nz - 3);
+            const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
+            const double dg = aa * bb * (aa + bb) / dd;
+            const double db = -aa * cc * (aa + cc) / dd;
+            const double da = 1.0 - dg - db;
+            umean = U[nz - 1] * da + U[nz - 2] * db + U[nz - 3] * dg;
+            vmean = V[nz - 1] * da + V[nz - 2] * db + V[nz - 3] * dg;
+        }
+    }
+    fu = -umean * wv;
+    fv = -vmean * wv;
+}
+
+// ---------------------------------------------------------------------------
+// velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180) for one (element, level).
+// ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
+// ---------------------------------------------------------------------------
+__global__ void k_velrhs(Dev d, double ff) {
+    const long long total = (long long)d.E * d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        const int4 en = d.elem_nodes[e];
+        const int nd[4] = {en.x, en.y, en.z, en.w};
+        const double4 w = d.w_cv[e];
+        const double ar = d.elem_area[e];
+        const double4 ae = elem_jac_a(d, d.eta_jac, en);
+        const double je = je_of(d, w, ae, z);
+        // pressure force from eta_n
+        double pre[4];
+        for (int k = 0; k < 4; ++k)
+            pre[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
+        const double Fx = wsum(gx, pre[0], pre[1], pre[2], pre[3]) * ar;
+        const double Fy = wsum(gy, pre[0], pre[1], pre[2], pre[3]) * ar;
+        const double un0 = d.U_n[ii], vn0 = d.V_n[ii];
+        double ur = -(0.5 + d.epsilon) * d.U_rhsAB[ii] + Fx * je;
+        double vr = -(0.5 + d.epsilon) * d.V_rhsAB[ii] + Fy * je;
+        const double cor = d.coriolis[e];
+        double uab = vn0 * cor * ar * je;
+        double vab = -un0 * cor * ar * je;
+        // horizontal upwind momentum advection (fv_advection.F90:114-188)
+        if (d.mom_adv_3D == 1) {
+            const int4 il = d.elem_iedges[e];
+            const int codes[4] = {il.x, il.y, il.z, il.w};
+            for (int c = 0; c < 4; ++c) {
+                const int code = codes[c];
+                if (code < 0) break;
+                const int ed = code >> 1;
+                const int2 nn = d.edge_nodes[ed];
+                const int2 et = d.edge_tri[ed];
+                const double acc = 0.5 * (d.ac[nn.x] + d.ac[nn.y]);
+                const double4 X = d.edge_cross[ed];
+                const size_t i1 = (size_t)et.x * L + z, i2 = (size_t)et.y * L + z;
+                const double u1 = d.U_n[i1] - d.vgux[i1] * X.x - d.vguy[i1] * X.y;
+                const double v1 = d.V_n[i1] - d.vgvx[i1] * X.x - d.vgvy[i1] * X.y;
+                const double u2 = d.U_n[i2] - d.vgux[i2] * X.z - d.vguy[i2] * X.w;
+                const double v2 = d.V_n[i2] - d.vgvx[i2] * X.z - d.vgvy[i2] * X.w;
+                const double jd = 0.5 * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
+                const double2 dxy = d.edge_dxdy[ed];
+                const double un = 0.5 * kREarth * jd *
+                                  ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
+                double uu, vv;
+                if (un >= 0.0) { uu = u1 * un * acc; vv = v1 * un * acc; }
+                else { uu = u2 * un * acc; vv = v2 * un * acc; }
+                if (code & 1) { uab = uab + uu; vab = vab + vv; }
+                else { uab = uab - uu; vab = vab - vv; }
+            }
+        }
+        // filter viscosity (fv_viscosity.F90:842-860)
+        if (d.filt_3D) {
+            const int4 nb = d.elem_nb[e];
+            const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+            const int jend = (en.x == en.w) ? 3 : 4;
+            double u1 = 0.0, v1 = 0.0;
+            for (int j = 0; j < jend; ++j)
+                if (nbs[j] >= 0) {
+                    u1 = u1 + d.U_n[(size_t)nbs[j] * L + z] - un0;
+                    v1 = v1 + d.V_n[(size_t)nbs[j] * L + z] - vn0;
+                }
+            ur = ur + d.tau_inv_filt * u1 * ar * je;
+            vr = vr + d.tau_inv_filt * v1 * ar * je;
+        }
+        // vertical advection (fv_advection.F90:354-469)
+        const double mwd = d.mask_wd[e];
+        if (d.vert_adv == 1) {
+            if (mwd != 0.0) {
+                const double acc = d.elem_acc[e];
+                double fu0, fv0, fu1, fv1;
+                uvert_at(d, e, z, w, ae, en, ar, fu0, fv0);
+                uvert_at(d, e, z + 1, w, ae, en, ar, fu1, fv1);
+                uab = uab + (fu0 - fu1) * acc;
+                vab = vab + (fv0 - fv1) * acc;
+            } else {
+                uab = 0.0;
+                vab = 0.0;
+            }
+        }
+        d.U_rhsAB[ii] = uab;
+        d.V_rhsAB[ii] = vab;
+        const double area_inv = 1.0 / ar;
+        const double dt = d.dt;
+        d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + 0.0) / je);
+        d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + 0.0) / je);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// implvisc: momentum_vert_impl_visc_tmp (fv_viscosity.F90:1374-1486, no ice)
+// or momentum_vert_impl_visc (fv_viscosity.F90:1266-1371); thread per column.
+// ---------------------------------------------------------------------------
+template <int MAXL>
+__global__ void k_implvisc(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int L = d.L, NS = d.NS;
+        double *ur = d.U_rhs + (size_t)e * L;
+        double *vr = d.V_rhs + (size_t)e * L;
+        const double *Av = d.Av + (size_t)e * NS;
+        const double mwd = d.mask_wd[e];
+        const int4 en = d.elem_nodes[e];
+        const double4 w = d.w_cv[e];
+        const double4 ae = elem_jac_a(d, d.eta_jac, en);
+        const double dt = d.dt;
+        const double ub = d.U_n[(size_t)e * L + L - 1], vb = d.V_n[(size_t)e * L + L - 1];
+        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[e]) * d.Cd_bz + 1.0);
+        double je[MAXL];
+        for (int z = 0; z < L; ++z) je[z] = je_of(d, w, ae, z);
+        if (d.im_vert_visc) {
+            double a[MAXL], b[MAXL], c[MAXL], cp[MAXL], up[MAXL], vp[MAXL], uu[MAXL], vv[MAXL];
+            double zc[MAXL];
+            for (int z = 0; z < L; ++z) zc[z] = wsum_z(d, w, ae, z);
+            for (int z = 1; z <= L - 2; ++z) {
+                const double zinv = dt / je[z];
+                a[z] = -Av[z] / (zc[z] - zc[z - 1]) * zinv;
+                c[z] = -Av[z + 1] / (zc[z + 1] - zc[z]) * zinv;
+                b[z] = -a[z] - c[z] + 1.0;
+            }
+            double zinv = dt / je[L - 1];
+            a[L - 1] = -Av[L - 1] / (zc[L - 1] - zc[L - 2]) * zinv;
+            b[L - 1] = -a[L - 1] + 1.0;
+            c[L - 1] = 0.0;
+            zinv = dt / je[0];
+            c[0] = -Av[1] / (zc[1] - zc[0]) * zinv;
+            a[0] = 0.0;
+            b[0] = -c[0] + 1.0;
+            for (int z = 0; z < L; ++z) { uu[z] = ur[z]; vv[z] = vr[z]; }
+            uu[0] = uu[0] + zinv * d.taux[e] / d.density_0;
+            vv[0] = vv[0] + zinv * d.tauy[e] / d.density_0;
+            zinv = dt / je[L - 1];
+            const double friction = -a_Cd * sqrt(ub * ub + vb * vb);
+            uu[L - 1] = uu[L - 1] + zinv * friction * ub;
+            vv[L - 1] = vv[L - 1] + zinv * friction * vb;
+            cp[0] = c[0] / b[0];
+            up[0] = uu[0] / b[0];
+            vp[0] = vv[0] / b[0];
+            for (int z = 1; z < L; ++z) {
+                const double m = b[z] - cp[z - 1] * a[z];
+                cp[z] = c[z] / m;
+                up[z] = (uu[z] - up[z - 1] * a[z]) / m;
+                vp[z] = (vv[z] - vp[z - 1] * a[z]) / m;
+            }
+            uu[L - 1] = up[L - 1];
+            vv[L - 1] = vp[L - 1];
+            for (int z = L - 2; z >= 0; --z) {
+                uu[z] = up[z] - cp[z] * uu[z + 1];
+                vv[z] = vp[z] - cp[z] * vv[z + 1];
+            }
+            for (int z = 0; z < L; ++z) { ur[z] = uu[z] * mwd; vr[z] = vv[z] * mwd; }
+        }
+        if (d.im_vert_visc_fic) {
+            if (mwd != 0.0) {
+                double xx1[MAXL + 2], yu[MAXL + 2], yv[MAXL + 2];
+                xx1[0] = 1.0;
+                double de = je[0] / (Av[0] + Av[1]);
+                const double rw = de / d.density_0;
+                yu[0] = d.taux[e] * rw;
+                yv[0] = d.tauy[e] * rw;
+                for (int z = 0; z < L; ++z) {
+                    const double Fx = ur[z], Fy = vr[z];
+                    const double d1 = (z == 0) ? 0.5 * je[z] : 0.5 * (je[z] + je[z - 1]);
+                    const double d2 = (z == L - 1) ? 0.5 * je[z] : 0.5 * (je[z] + je[z + 1]);
+                    const double zt = dt / je[z];
+                    const double a = zt * Av[z] / d1;
+                    const double c = zt * Av[z + 1] / d2;
+                    const double b = a + c + 1.0;
+                    const double dd = b - a * xx1[z];
+                    xx1[z + 1] = c / dd;
+                    yu[z + 1] = (a * yu[z] + Fx) / dd;
+                    yv[z + 1] = (a * yv[z] + Fy) / dd;
+                }
+                de = je[L - 1] / (Av[NS - 1] + Av[L - 1]);
+                const double friction = de * a_Cd * sqrt(ub * ub + vb * vb);
+                double Ut, Vt;
+                if (d.fic_point == 0) { Ut = 0.0; Vt = 0.0; }
+                else if (d.fic_point == 1) {
+                    const double a = friction + 1.0 - xx1[L];
+                    Ut = yu[L] / a; Vt = yv[L] / a;
+                } else {
+                    const double a = 1.0 / (1.0 - friction) - xx1[L];
+                    Ut = yu[L] / a; Vt = yv[L] / a;
+                }
+                for (int z = L - 1; z >= 0; --z) {
+                    Ut = Ut * xx1[z + 1] + yu[z + 1];
+                    Vt = Vt * xx1[z + 1] + yv[z + 1];
+                    ur[z] = Ut * mwd;
+                    vr[z] = Vt * mwd;
+                }
+            } else {
+                for (int z = 0; z < L; ++z) { ur[z] = 0.0; vr[z] = 0.0; }
+            }
+        }
+    }
+}
+
+// jacobian bookkeeping after the sub-cycle (fv_main.F90:2050): Jc_old <- Jc
+__global__ void k_jac_swap(Dev d) {
+    GRID_LOOP(ii, d.N) {
+        d.eta_jac_old[ii] = d.eta_jac[ii];
+        d.eta_jac[ii] = d.eta_n[ii];
+    }
+}
+
+// update_3D_vel (fv_3D_vel.F90:201-255) with the U_filt averaging of
+// oce_barotropic_timestep (fv_main.F90:1670-1677) folded in.
+template <int MAXL>
+__global__ void k_update3d(Dev d, double Mt_inv) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int L = d.L;
+        const int4 en = d.elem_nodes[e];
+        const double4 w = d.w_cv[e];
+        const double4 ao = elem_jac_a(d, d.eta_jac_old, en);
+        const double4 an = elem_jac_a(d, d.eta_jac, en);
+        double a[MAXL];
+        for (int z = 0; z < L; ++z) a[z] = je_of(d, w, ao, z);
+        const double dmean_inv = 1.0 / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
+                                                        d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
+        const double *ur = d.U_rhs + (size_t)e * L;
+        const double *vr = d.V_rhs + (size_t)e * L;
+        double su = 0.0, sv = 0.0;
+        for (int z = 0; z < L; ++z) su = su + ur[z] * a[z];
+        for (int z = 0; z < L; ++z) sv = sv + vr[z] * a[z];
+        const double U2p = su * dmean_inv, V2p = sv * dmean_inv;
+        const double uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
+        const double vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
+        d.U_filt_2D[e] = uf;
+        d.V_filt_2D[e] = vf;
+        const double2 u2 = d.U_n_2D[e];
+        for (int z = 0; z < L; ++z) {
+            const double az = a[z] / je_of(d, w, an, z);
+            const size_t i = (size_t)e * L + z;
+            d.U_n_filt[i] = az * ur[z] + uf - U2p;
+            d.V_n_filt[i] = az * vr[z] + vf - V2p;
+            d.U_n[i] = az * ur[z] + u2.x - U2p;
+            d.V_n[i] = az * vr[z] + u2.y - V2p;
+        }
+    }
+}
+
+// vert_vel_sigma (fv_3D_vel.F90:309-456): per node, gather the layer
+// transport divergence over the node's edges in edge order, then the
+// reverse prefix sum over levels and the division by the area.
+template <int MAXL>
+__global__ void k_wvel(Dev d) {
+    GRID_LOOP(ii, d.N) {
+        const int n = (int)ii;
+        const int L = d.L, NS = d.NS;
+        double W[MAXL + 1];
+        for (int z = 0; z < L; ++z) W[z] = 0.0;
+        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
+            const int code = d.node_eidx[p];
+            const int ed = code >> 1;
+            const int2 et = d.edge_tri[ed];
+            const double4 X = d.edge_cross[ed];
+            const double4 a1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
+            const double4 w1 = d.w_cv[et.x];
+            const double uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
+            const bool internal = ed < d.Ed_in;
+            double4 a2 = a1, w2 = w1;
+            double uf2 = 0.0, vf2 = 0.0;
+            if (internal) {
+                a2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
+                w2 = d.w_cv[et.y];
+                uf2 = d.U_filt_2D[et.y];
+                vf2 = d.V_filt_2D[et.y];
+            }
+            for (int z = 0; z < L; ++z) {
+                const size_t i1 = (size_t)et.x * L + z;
+                double c1 = je_of(d, w1, a1, z) * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
+                if (internal) {
+                    const size_t i2 = (size_t)et.y * L + z;
+                    c1 = c1 + je_of(d, w2, a2, z) * (-(d.V_n_filt[i2] - vf2) * X.z + (d.U_n_filt[i2] - uf2) * X.w);
+                }
+                if (code & 1) W[z] = W[z] - c1;
+                else W[z] = W[z] + c1;
+            }
+        }
+        const double area_inv = 1.0 / d.area[n];
+        double *Wn = d.Wvel + (size_t)n * NS;
+        double below = Wn[NS - 1];
+        for (int z = L - 1; z >= 0; --z) {
+            below = W[z] + below;
+            W[z] = below;
+        }
+        for (int z = 0; z < L; ++z) Wn[z] = W[z] * area_inv;
+    }
+}
+
+// ---- launch wrappers --------------------------------------------------------
+#define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
+    do {                                                                                   \
+        if (d.L <= 24) KERNEL<24><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                \
+        else if (d.L <= 48) KERNEL<48><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);           \
+        else KERNEL<128><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                         \
+    } while (0)
+
+void launch_pressure(const Dev &d, cudaStream_t s) {
+    k_pressure_col<<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d);
+}
+void launch_velgrad3d(const Dev &d, cudaStream_t s) {
+    k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
+    k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
+}
+void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d); }
+void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
+void launch_update3d(const Dev &d, double Mt_inv, cudaStream_t s) {
+    MAXL_DISPATCH(k_update3d, grid_for(d.E, 128), 128, s, d, Mt_inv);
+}
+void launch_wvel(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_wvel, grid_for(d.N, 128), 128, s, d); }
+
+}  // namespace fesomc

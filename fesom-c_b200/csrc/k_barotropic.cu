@@ -1,0 +1,382 @@
+// External-mode (barotropic) sub-cycle kernels: one sub-step of
+// timestep_AB_2D (src/fv_main.F90:1372-1634) is
+//   ab3_elem  : AB3 extrapolation of U, element mean total depth (aux_elem)
+//               and the least-squares velocity gradients of UAB
+//   ssh_node  : edge-flux divergence gathered per node in edge order
+//               (compute_ssh_rhs_elem), rivers, OB tide, eta update, AM4
+//   [sub-step 1 only: puls_elem, el2nodes, p1_elem]
+//   u2d_elem  : update_2D_vel (pressure gradient, Coriolis, wind, upwind
+//               momentum advection gathered per element, filter viscosity,
+//               3D->2D forcing, implicit friction, wet/dry mask) fused with
+//               the time-level rotation of U and the U_filt accumulation
+//   rot_nodes : eta time-level rotation
+// All kernels are HBM-bandwidth bound.
+#include "device_common.cuh"
+
+namespace fesomc {
+
+// AB3 coefficients, timestep_AB_2D fv_main.F90:1403,1408
+__device__ __forceinline__ double ab3(double b, double x0, double x1, double x2) {
+    return (1.5 + b) * x0 - (0.5 + 2.0 * b) * x1 + b * x2;
+}
+__device__ __forceinline__ double2 ab3v(double b, double2 x0, double2 x1, double2 x2) {
+    return make_double2(ab3(b, x0.x, x1.x, x2.x), ab3(b, x0.y, x1.y, x2.y));
+}
+
+// ---------------------------------------------------------------------------
+// ab3_elem: UAB (fv_main.F90:1407-1410), aux_elem (fv_average_dynamic.F90:66-86)
+// and vel_gradients_2D(UAB) (fv_gradients.F90:97-176, free slip).
+// ---------------------------------------------------------------------------
+__global__ void k_ab3_elem(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const double b = d.beta;
+        const double2 uab = ab3v(b, d.U_n_2D[e], d.U_n_1[e], d.U_n_2[e]);
+        d.UAB[e] = uab;
+        const int4 en = d.elem_nodes[e];
+        const int nd[4] = {en.x, en.y, en.z, en.w};
+        double ad[4];
+        for (int i = 0; i < 4; ++i) {
+            const int n = nd[i];
+            double etaab = ab3(b, d.eta_n[n], d.eta_n_1[n], d.eta_n_2[n]);
+            ad[i] = d.Dmin;
+            double ttl = etaab + d.depth[n];
+            if (ttl > d.Dmin) ad[i] = ttl;
+        }
+        const double4 w = d.w_cv[e];
+        d.aux_elem[e] = wexp(w, ad[0], ad[1], ad[2], ad[3]);
+        // velocity gradients of UAB
+        const int4 nb = d.elem_nb[e];
+        const int4 ee = d.elem_edges[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
+        const double4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const double gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const double gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const int jend = (en.x == en.w) ? 3 : 4;
+        double g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0;
+        for (int j = 0; j < jend; ++j) {
+            const int e2 = nbs[j];
+            if (e2 >= 0) {
+                const double2 u2 = ab3v(b, d.U_n_2D[e2], d.U_n_1[e2], d.U_n_2[e2]);
+                g1 = g1 + gxa[j] * (u2.x - uab.x);
+                g2 = g2 + gya[j] * (u2.x - uab.x);
+                g3 = g3 + gxa[j] * (u2.y - uab.y);
+                g4 = g4 + gya[j] * (u2.y - uab.y);
+            } else {
+                const double2 dxy = d.edge_dxdy[eds[j]];
+                const double zc1 = dxy.x * d.elem_cos[e];
+                const double zc2 = dxy.y;
+                const double un = -2.0 * (uab.x * zc2 - uab.y * zc1) / (zc1 * zc1 + zc2 * zc2);
+                g1 = g1 + gxa[j] * un * zc2;
+                g2 = g2 + gya[j] * un * zc2;
+                g3 = g3 - gxa[j] * un * zc1;
+                g4 = g4 - gya[j] * un * zc1;
+            }
+        }
+        d.vel_grad[e] = make_double4(g1, g2, g3, g4);
+    }
+}
+
+// edge flux c1 of compute_ssh_rhs_elem (fv_average_dynamic.F90:119-120, 152-153)
+__device__ __forceinline__ double ssh_edge_flux(const Dev &d, int ed) {
+    const int2 et = d.edge_tri[ed];
+    const double4 X = d.edge_cross[ed];
+    const double2 u1 = d.UAB[et.x];
+    double c1 = (u1.y * X.x - u1.x * X.y) * d.aux_elem[et.x];
+    if (ed < d.Ed_in) {
+        const double2 u2 = d.UAB[et.y];
+        c1 = c1 + (-u2.y * X.z + u2.x * X.w) * d.aux_elem[et.y];
+    }
+    return c1;
+}
+
+// ---------------------------------------------------------------------------
+// ssh_node: ssh_rhs gather (serial scatter order), rivers, open boundary,
+// eta_new = eta_n + dt_2D*rhs/area (fv_main.F90:1432-1435), then the AM4
+// elevation of update_2D_vel (fv_average_dynamic.F90:290-295) into etaAB and
+// the node wet/dry mask (wad_mask, fv_main.F90:1302-1304).
+// ob_val holds the open-boundary elevation of this sub-step, computed on the
+// host with the reference formula (fv_average_dynamic.F90:190-216).
+// ---------------------------------------------------------------------------
+__global__ void k_ssh_node(Dev d, int sub) {
+    const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
+    GRID_LOOP(ii, d.N) {
+        const int n = (int)ii;
+        double acc = 0.0;
+        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
+        for (int p = p0; p < p1; ++p) {
+            const int code = d.node_eidx[p];
+            const double c1 = ssh_edge_flux(d, code >> 1);
+            if (code & 1) acc = acc - c1;
+            else acc = acc + c1;
+        }
+        if (d.key_rivers) {
+            for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) acc = acc + d.runoff[d.node_ridx[p]];
+        }
+        const int q = d.obn_of_node[n];
+        if (d.TF_presence && q >= 0) acc = d.ob_val[(size_t)sub * d.nobn + q];
+        const double en = d.eta_n[n];
+        double enew = acc;
+        if (d.index_nod2D[n] < 2) enew = en + d.dt_2D * acc / d.area[n];
+        d.eta_new[n] = enew;
+        const double eab = de * enew + fe * en + ga * d.eta_n_1[n] + ep * d.eta_n_2[n];
+        d.etaAB[n] = eab;
+        if (d.wet_dry_on) d.mask_wd_node[n] = (d.depth[n] + eab > d.Dmin) ? 1.0 : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sub-step 1 (fv_main.F90:1451-1520): dmean_n, compute_puls_vel
+// (fv_3D_vel.F90:257-307), one thread per (element, level).
+// ---------------------------------------------------------------------------
+__global__ void k_puls_elem(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int4 en = d.elem_nodes[e];
+        const double4 w = d.w_cv[e];
+        const double dmn = dmax(d.Dmin, wexp(w, d.eta_n[en.x] + d.depth[en.x], d.eta_n[en.y] + d.depth[en.y],
+                                              d.eta_n[en.z] + d.depth[en.z], d.eta_n[en.w] + d.depth[en.w]));
+        const double a = dmn / dmax(d.Dmin, wsum(w, d.eta_new[en.x] + d.depth[en.x], d.eta_new[en.y] + d.depth[en.y],
+                                                 d.eta_new[en.z] + d.depth[en.z], d.eta_new[en.w] + d.depth[en.w]));
+        const double2 u2 = d.U_n_2D[e];
+        d.U_puls[ii] = d.U_n[ii] - a * u2.x;
+        d.V_puls[ii] = d.V_n[ii] - a * u2.y;
+        if (ii % d.L == 0) d.dmean_n[e] = dmn;
+    }
+}
+
+// compute_el2nodes_3D (fv_utilit.F90:644-700), one thread per (node, level)
+__global__ void k_el2nodes(Dev d, const double *Ue, const double *Ve, double *Un, double *Vn) {
+    const long long total = (long long)d.N * d.L;
+    GRID_LOOP(ii, total) {
+        const int n = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const double tvol_inv = 1.0 / d.node_tvol[n];
+        double su = 0.0, sv = 0.0;
+        for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
+            const int el = d.node_nidx[p];
+            const double ar = d.elem_area[el];
+            su = su + Ue[(size_t)el * d.L + z] * ar;
+            sv = sv + Ve[(size_t)el * d.L + z] * ar;
+        }
+        Un[ii] = su * tvol_inv;
+        Vn[ii] = sv * tvol_inv;
+    }
+}
+
+// momentum_adv_P1_3D_to_2D (fv_advection.F90:676-793) gathered per element,
+// optional viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939), divided by
+// dmean_n (fv_main.F90:1504-1513).
+__global__ void k_p1_elem(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int L = d.L;
+        double rx = 0.0, ry = 0.0;
+        const int4 il = d.elem_iedges[e];
+        const int codes[4] = {il.x, il.y, il.z, il.w};
+        const double4 ae = elem_jac_a(d, d.eta_jac, d.elem_nodes[e]);
+        const double4 we = d.w_cv[e];
+        for (int c = 0; c < 4; ++c) {
+            const int code = codes[c];
+            if (code < 0) break;
+            const int ed = code >> 1;
+            const int2 nn = d.edge_nodes[ed];
+            const int2 et = d.edge_tri[ed];
+            const double acc = (d.ac[nn.x] + d.ac[nn.y]) * .5;
+            const double2 dxy = d.edge_dxdy[ed];
+            const double xe = dxy.x * kREarth * 0.5 * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+            const double ye = dxy.y * kREarth;
+            const double a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
+            double s_u = 0.0, s_v = 0.0;
+            for (int z = 0; z < L; ++z) {
+                const double uu = 0.5 * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
+                const double vv = 0.5 * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
+                const double jd = 0.5 * (jc_of(d, a1, z) + jc_of(d, a2, z));
+                const double un = (uu * ye - vv * xe) * jd;
+                const double je = je_of(d, we, ae, z);
+                s_u = s_u + uu * un * je;
+                s_v = s_v + vv * un * je;
+            }
+            if (code & 1) { rx = rx + acc * s_u; ry = ry + acc * s_v; }
+            else { rx = rx - acc * s_u; ry = ry - acc * s_v; }
+        }
+        if (d.filt_3D) {
+            const int4 en = d.elem_nodes[e];
+            const int4 nb = d.elem_nb[e];
+            const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+            const int jend = (en.x == en.w) ? 3 : 4;
+            double anb[4][4];
+            for (int j = 0; j < jend; ++j)
+                if (nbs[j] >= 0) {
+                    const double4 t = elem_jac_a(d, d.eta_jac, d.elem_nodes[nbs[j]]);
+                    anb[j][0] = t.x; anb[j][1] = t.y; anb[j][2] = t.z; anb[j][3] = t.w;
+                }
+            const double tau = d.tau_inv_filt, ar = d.elem_area[e];
+            for (int z = 0; z < L; ++z) {
+                const double je = je_of(d, we, ae, z);
+                const double up = d.U_puls[(size_t)e * L + z], vp = d.V_puls[(size_t)e * L + z];
+                double u1 = 0.0, v1 = 0.0;
+                for (int j = 0; j < jend; ++j) {
+                    const int ne = nbs[j];
+                    if (ne < 0) continue;
+                    const double4 wn = d.w_cv[ne];
+                    const double4 an = make_double4(anb[j][0], anb[j][1], anb[j][2], anb[j][3]);
+                    const double jn = je_of(d, wn, an, z);
+                    u1 = u1 + d.U_puls[(size_t)ne * L + z] * jn - up * je;
+                    v1 = v1 + d.V_puls[(size_t)ne * L + z] * jn - vp * je;
+                }
+                const double fu = tau * u1 * ar, fv = tau * v1 * ar;
+                rx = rx + fu * je;
+                ry = ry + fv * je;
+            }
+        }
+        const double dm = d.dmean_n[e];
+        d.U_rhs_2D_3D[e] = make_double2(rx / dm, ry / dm);
+    }
+}
+
+// One upwind edge flux of momentum_adv_upwind_2D (fv_advection.F90:589-643)
+__device__ __forceinline__ void adv2d_edge(const Dev &d, int ed, double &uu, double &vv) {
+    const int2 nn = d.edge_nodes[ed];
+    const int2 et = d.edge_tri[ed];
+    const double dmean = dmax(d.Dmin, 0.5 * ((d.etaAB[nn.x] + d.depth[nn.x]) + (d.etaAB[nn.y] + d.depth[nn.y])));
+    const double acc = (d.ac[nn.x] + d.ac[nn.y]) * 0.5;
+    const double4 X = d.edge_cross[ed];
+    const double2 U1 = d.UAB[et.x], U2 = d.UAB[et.y];
+    const double4 g1 = d.vel_grad[et.x], g2 = d.vel_grad[et.y];
+    const double u1 = U1.x - g1.x * X.x - g1.y * X.y;
+    const double v1 = U1.y - g1.z * X.x - g1.w * X.y;
+    const double u2 = U2.x - g2.x * X.z - g2.y * X.w;
+    const double v2 = U2.y - g2.z * X.z - g2.w * X.w;
+    const double2 dxy = d.edge_dxdy[ed];
+    const double un = 0.5 * kREarth * dmean *
+                      ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
+    if (un >= 0.0) { uu = un * U1.x * acc; vv = un * U1.y * acc; }
+    else { uu = un * U2.x * acc; vv = un * U2.y * acc; }
+}
+
+// ---------------------------------------------------------------------------
+// u2d_elem: update_2D_vel (fv_average_dynamic.F90:228-443, type_task 3,
+// key_atm off) + rotation of U time levels + U_filt accumulation
+// (fv_main.F90:1568-1606).
+// ---------------------------------------------------------------------------
+__global__ void k_u2d_elem(Dev d) {
+    const double d0inv = 1.0 / d.density_0;
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int4 en = d.elem_nodes[e];
+        const int nd[4] = {en.x, en.y, en.z, en.w};
+        double eab[4], dep[4], etag[4];
+        for (int k = 0; k < 4; ++k) {
+            eab[k] = d.etaAB[nd[k]];
+            dep[k] = d.depth[nd[k]];
+            etag[k] = kG * (d.atp1[nd[k]] * eab[k] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+        }
+        double mwd = d.mask_wd[e];
+        if (d.wet_dry_on) {
+            const double dmin4 = dmin(dmin(dep[0], dep[1]), dmin(dep[2], dep[3]));
+            const double emax4 = dmax(dmax(eab[0], eab[1]), dmax(eab[2], eab[3]));
+            mwd = (dmin4 + emax4 > d.Dmin) ? 1.0 : 0.0;
+            d.mask_wd[e] = mwd;
+        }
+        const double4 w = d.w_cv[e];
+        const double ar = d.elem_area[e];
+        const double dmean = dmax(d.Dmin, wexp(w, eab[0] + dep[0], eab[1] + dep[1], eab[2] + dep[2], eab[3] + dep[3]));
+        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
+        const double2 uab = d.UAB[e];
+        const double cor = d.coriolis[e];
+        double rx = ar * (-dmean * (gx.x * etag[0] + gx.y * etag[1] + gx.z * etag[2] + gx.w * etag[3])
+                          + uab.y * dmean * cor + d.taux[e] * d0inv);
+        double ry = ar * (-dmean * (gy.x * etag[0] + gy.y * etag[1] + gy.z * etag[2] + gy.w * etag[3])
+                          - uab.x * dmean * cor + d.tauy[e] * d0inv);
+        if (d.mom_adv_2D == 2) {
+            const int4 il = d.elem_iedges[e];
+            const int codes[4] = {il.x, il.y, il.z, il.w};
+            for (int c = 0; c < 4; ++c) {
+                const int code = codes[c];
+                if (code < 0) break;
+                double uu, vv;
+                adv2d_edge(d, code >> 1, uu, vv);
+                if (code & 1) { rx = rx + uu; ry = ry + vv; }
+                else { rx = rx - uu; ry = ry - vv; }
+            }
+        }
+        if (d.filt_2D) {
+            const int4 nb = d.elem_nb[e];
+            const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+            const int jend = (en.x == en.w) ? 3 : 4;
+            double u1 = 0.0, u2 = 0.0;
+            for (int j = 0; j < jend; ++j)
+                if (nbs[j] >= 0) {
+                    const double2 un = d.UAB[nbs[j]];
+                    u1 = u1 + un.x - uab.x;
+                    u2 = u2 + un.y - uab.y;
+                }
+            const double sd = wsum(w, dep[0], dep[1], dep[2], dep[3]);
+            rx = rx + d.tau_inv_filt * u1 * ar * sd;
+            ry = ry + d.tau_inv_filt * u2 * ar * sd;
+        }
+        const double2 r3 = d.U_rhs_2D_3D[e];
+        rx = rx + r3.x;
+        ry = ry + r3.y;
+        // final update with implicit bottom drag
+        double eo[4], enw[4];
+        for (int k = 0; k < 4; ++k) { eo[k] = d.eta_n[nd[k]]; enw[k] = d.eta_new[nd[k]]; }
+        const double dmo = dmax(d.Dmin, wsum(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
+        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[e]) * d.Cd_bz + 1.0);
+        const double ub = d.U_n[(size_t)e * d.L + d.L - 1], vb = d.V_n[(size_t)e * d.L + d.L - 1];
+        const double friction = a_Cd * sqrt(ub * ub + vb * vb);
+        const double ff = 1.0 / (dmax(d.Dmin, wsum(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
+                                 + friction * d.dt_2D);
+        const double dt2 = d.dt_2D;
+        const double2 u0 = d.U_n_2D[e];
+        const double2 bp = d.Bar_pr_2D[e];
+        const double nx = mwd * ((dmo * u0.x - dt2 * friction * (ub - u0.x) + dt2 * bp.x + dt2 * rx / ar) * ff + 0.0);
+        const double ny = mwd * ((dmo * u0.y - dt2 * friction * (vb - u0.y) + dt2 * bp.y + dt2 * ry / ar) * ff + 0.0);
+        // rotate U_n_2 <- U_n_1 <- U_n_2D <- new (fv_main.F90:1569-1578)
+        d.U_n_2[e] = d.U_n_1[e];
+        d.U_n_1[e] = u0;
+        d.U_n_2D[e] = make_double2(nx, ny);
+        // U_filt accumulation with the new elevation (fv_main.F90:1596-1605)
+        const double dmn = dmax(d.Dmin, wexp(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]));
+        d.U_filt_2D[e] = d.U_filt_2D[e] + nx * dmn;
+        d.V_filt_2D[e] = d.V_filt_2D[e] + ny * dmn;
+    }
+}
+
+// eta time-level rotation (fv_main.F90:1547-1551)
+__global__ void k_rot_nodes(Dev d) {
+    GRID_LOOP(ii, d.N) {
+        const int n = (int)ii;
+        const double e0 = d.eta_n[n], e1 = d.eta_n_1[n];
+        d.eta_n_2[n] = e1;
+        d.eta_n_1[n] = e0;
+        d.eta_n[n] = d.eta_new[n];
+    }
+}
+
+// U_filt_2D = V_filt_2D = 0 at the start of the sub-cycle
+__global__ void k_zero_filt(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        d.U_filt_2D[ii] = 0.0;
+        d.V_filt_2D[ii] = 0.0;
+    }
+}
+
+// ---- launch wrappers --------------------------------------------------------
+void launch_ab3_elem(const Dev &d, cudaStream_t s) { k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) { k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub); }
+void launch_puls_elem(const Dev &d, cudaStream_t s) {
+    k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_el2nodes(const Dev &d, const double *Ue, const double *Ve, double *Un, double *Vn, cudaStream_t s) {
+    k_el2nodes<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d, Ue, Ve, Un, Vn);
+}
+void launch_p1_elem(const Dev &d, cudaStream_t s) { k_p1_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
+void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
+void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+
+}  // namespace fesomc

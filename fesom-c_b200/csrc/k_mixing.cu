@@ -1,0 +1,150 @@
+// Vertical turbulence closure d3_end (src/fv_mixing.F90:73-347): one thread
+// per node column.  Each column iterates its implicit turbulence-energy
+// sweep up to 200 times (relative tolerance 1e-6); columns that reach the cap
+// are counted in the device status (the reference silently continues).
+// Compute / latency bound (FP64 divisions, log, sqrt).
+#include "device_common.cuh"
+
+namespace fesomc {
+
+template <int MAXNS>
+__global__ void k_d3end(Dev d) {
+    const double t_inv = 1.0 / d.dt;
+    const double cka = d.cka;
+    const double B1cka2 = 16.6 * (cka * cka);
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        const int NS = d.NS, L = d.L;
+        const double *bt = d.bt + (size_t)node * NS;
+        const double *snu = d.snu + (size_t)node * NS;
+        const double *Kv = d.Kv + (size_t)node * NS;
+        const double *Un = d.Unode + (size_t)node * L;
+        const double *Vn = d.Vnode + (size_t)node * L;
+        const double *T = d.TF + (size_t)node * L;
+        const double *S = d.SF + (size_t)node * L;
+        double *Ri = d.Ri + (size_t)node * NS;
+        double *tke = d.tke_dissip + (size_t)node * NS;
+        // arrays indexed 1..NS like the Fortran ones
+        double xx1[MAXNS + 2], yy1[MAXNS + 2], btr[MAXNS + 2], btr1[MAXNS + 2];
+        double b1[MAXNS + 2], b2[MAXNS + 2], c2[MAXNS + 2], sn[MAXNS + 2], bo[MAXNS + 2];
+        const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const double dmean2 = dmean * dmean;
+        const double ajac = jac_a(d, d.eta_jac, node);
+        for (int nz = 1; nz <= NS; ++nz) {
+            btr[nz] = bt[nz - 1];
+            bo[nz] = bt[nz - 1];
+            sn[nz] = snu[nz - 1];
+        }
+        Ri[0] = 0.0;
+        Ri[NS - 1] = 0.0;
+        for (int nz = 2; nz <= NS - 1; ++nz) {
+            const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+            const double d1 = s_m - s_0;
+            const double d2 = s_0 - s_p;
+            const double dd = 0.5 * (d1 + d2);
+            double ap1 = Un[nz - 2] - Un[nz - 1];
+            const double ap2 = Vn[nz - 2] - Vn[nz - 1];
+            b1[nz] = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            b1[nz] = b1[nz] / dmean2;
+            const double zb = zbar_of(d, ajac, nz - 1);
+            const double rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
+            const double rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
+            ap1 = (rho_up - rho_dn) / dd;
+            b2[nz] = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
+            const double snu_m = 0.5 * (sn[nz] + sn[nz + 1]);
+            c2[nz] = 0.5 * 0.73 * (snu_p * (bo[nz - 1] - bo[nz]) / d1 - snu_m * (bo[nz] - bo[nz + 1]) / d2) / dd;
+            c2[nz] = c2[nz] / dmean2;
+            if (b1[nz] > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1[nz] * sn[nz];
+            else Ri[nz - 1] = 10000.0;
+        }
+        xx1[2] = 1.0;
+        yy1[2] = 0.0;
+        {
+            const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const double wx = d.windx[node], wy = d.windy[node];
+            const double u_din_sur = 0.05 * (wx * wx + wy * wy);
+            const double snu_m = 0.5 * (sn[NS] + sn[NS - 1]);
+            yy1[2] = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
+        }
+        // bottom boundary value (independent of the iteration)
+        const double delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const double lg = log(delta_b / d.z0b_min);
+        const double bott_R = B1cka2 / (lg * lg);
+        const double ubt = Un[L - 1], vbt = Vn[L - 1];
+        const double bot = bott_R * (ubt * ubt + vbt * vbt);
+        bool converged = false;
+        for (int it = 1; it <= 200; ++it) {
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const double dd1 = s_m - s_0;
+                const double dd2 = s_0 - s_p;
+                const double dd = 0.5 * (dd1 + dd2);
+                const double c1 = 0.046 * (btr[nz] * btr[nz]) / sn[nz];
+                tke[nz - 1] = c1;
+                const double fr = -b1[nz] - b2[nz] - c1 - t_inv * bo[nz] - c2[nz];
+                const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
+                const double snu_mm = 0.5 * (sn[nz] + sn[nz + 1]);
+                const double am = 0.5 * (snu_p * 0.73) / (dmean2 * dd1 * dd);
+                const double cm = 0.5 * (snu_mm * 0.73) / (dmean2 * dd2 * dd);
+                const double bm = am + cm + (2.0 * 0.046 * btr[nz]) / sn[nz] + t_inv;
+                const double a = bm - am * xx1[nz];
+                xx1[nz + 1] = cm / a;
+                yy1[nz + 1] = (am * yy1[nz] - fr) / a;
+            }
+            btr1[NS] = bot;
+            for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
+            double bbb_max = 0.0;
+            for (int nz = 1; nz <= NS; ++nz) {
+                const double a = btr[nz] - btr1[nz];
+                const double b = dmax(btr1[nz], btr[nz]) + 1.0e-8;
+                const double c = fabs(a / b);
+                if (c > bbb_max) bbb_max = c;
+            }
+            if (bbb_max < 1.0e-6) { converged = true; break; }
+            for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
+        }
+        if (!converged) {
+            atomicAdd(d.notconv, 1);
+        }
+        double *btw = d.bt + (size_t)node * NS;
+        double *snw = d.snu + (size_t)node * NS;
+        double *Kvw = d.Kv + (size_t)node * NS;
+        for (int nz = 1; nz <= NS; ++nz) {
+            const double btn = dmax(btr[nz], 1.0e-8);
+            btw[nz - 1] = btn;
+            const double zt = __ldg(d.sig + nz - 1) * dmean;
+            const double Zh = zt + d.z0b_min;
+            const double Zd = fabs(dmean - zt) + d.z0s_min;
+            const double Z0 = 1.0 - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const double scale_t = cka * Zh * Zd * Z0 / dmean;
+            double s = scale_t * sqrt(btn) + d.snul;
+            if (s >= 0.2) s = 0.2;
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+}
+
+// Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
+__global__ void k_av(Dev d) {
+    const long long total = (long long)d.E * d.NS;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.NS);
+        const int z = (int)(ii % d.NS);
+        const int4 en = d.elem_nodes[e];
+        const double4 w = d.w_cv[e];
+        const int NS = d.NS;
+        d.Av[ii] = wsum(w, d.snu[(size_t)en.x * NS + z], d.snu[(size_t)en.y * NS + z], d.snu[(size_t)en.z * NS + z],
+                        d.snu[(size_t)en.w * NS + z]);
+    }
+}
+
+void launch_d3end(const Dev &d, cudaStream_t s) {
+    if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    else if (d.NS <= 48) k_d3end<48><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d);
+}
+
+}  // namespace fesomc

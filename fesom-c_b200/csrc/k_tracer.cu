@@ -1,0 +1,585 @@
+// Tracer kernels of solve_tracers (src/fv_main.F90:1707-1836):
+//   minmax      : global T/S min/max -> T_aver, S_aver (two-pass reduction)
+//   upwind_h    : solve_tracer_upwind (fv_tracer.F90:390-923) per (node, level):
+//                 edge fluxes gathered in edge order, QUICK vertical fluxes,
+//                 open-boundary relaxation, AB2 update (T and S together)
+//   muscl_*     : solve_tracer_muscl (fv_tracer.F90:8-379) for T and S:
+//                 element gradients, node-averaged gradients
+//                 (fill_up_dn_grad fallback), edge gather + vertical + update
+//   vdiff_col   : river salinity source + tracer_impl_vert_diff
+//                 (fv_tracer.F90:1319-1494) per node column, with the
+//                 negative-salinity / low-temperature checks as status bits
+//   energy      : energy diagnostic (fv_average_dynamic.F90:476-554),
+//                 compensated deterministic two-pass reduction
+#include "device_common.cuh"
+
+namespace fesomc {
+
+constexpr int kRedBlock = 256;
+constexpr int kRedGrid = 592;  // 4 x 148 SMs
+
+// ---------------------------------------------------------------------------
+// global min / max of TF and SF
+// ---------------------------------------------------------------------------
+__global__ void k_minmax_part(Dev d) {
+    __shared__ double s[4][kRedBlock];
+    const long long total = (long long)d.N * d.L;
+    double tmin = d.TF[0], tmax = d.TF[0], smin = d.SF[0], smax = d.SF[0];
+    GRID_LOOP(i, total) {
+        const double t = d.TF[i], x = d.SF[i];
+        tmin = dmin(tmin, t); tmax = dmax(tmax, t);
+        smin = dmin(smin, x); smax = dmax(smax, x);
+    }
+    s[0][threadIdx.x] = tmin; s[1][threadIdx.x] = tmax; s[2][threadIdx.x] = smin; s[3][threadIdx.x] = smax;
+    __syncthreads();
+    for (int o = kRedBlock / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s[0][threadIdx.x] = dmin(s[0][threadIdx.x], s[0][threadIdx.x + o]);
+            s[1][threadIdx.x] = dmax(s[1][threadIdx.x], s[1][threadIdx.x + o]);
+            s[2][threadIdx.x] = dmin(s[2][threadIdx.x], s[2][threadIdx.x + o]);
+            s[3][threadIdx.x] = dmax(s[3][threadIdx.x], s[3][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) d.mm_part[(size_t)blockIdx.x * 4 + k] = s[k][0];
+}
+
+__global__ void k_minmax_final(Dev d, int nparts) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double tmin = d.mm_part[0], tmax = d.mm_part[1], smin = d.mm_part[2], smax = d.mm_part[3];
+    for (int b = 1; b < nparts; ++b) {
+        tmin = dmin(tmin, d.mm_part[4 * b + 0]);
+        tmax = dmax(tmax, d.mm_part[4 * b + 1]);
+        smin = dmin(smin, d.mm_part[4 * b + 2]);
+        smax = dmax(smax, d.mm_part[4 * b + 3]);
+    }
+    d.aver[0] = 0.5 * (tmin + tmax);
+    d.aver[1] = 0.5 * (smin + smax);
+}
+
+// AB2 value of a tracer at (node, level) minus its mean (fv_tracer.F90:433)
+__device__ __forceinline__ double ab2(const Dev &d, const double *Tn, const double *To, size_t i, double aver) {
+    return -(0.5 + d.epsilon) * To[i] + (1.5 + d.epsilon) * Tn[i] - aver;
+}
+
+// Vel_nor at node n from its boundary edges (fv_tracer.F90:862-873)
+__device__ __forceinline__ double vel_nor(const Dev &d, int n) {
+    double v = 0.0;
+    for (int p = d.node_bptr[n]; p < d.node_bptr[n + 1]; ++p) {
+        const int code = d.node_bidx[p];
+        const int ed = code >> 1;
+        const int2 nn = d.edge_nodes[ed];
+        const int e1 = d.edge_tri[ed].x;
+        const double dmean = dmax(d.Dmin, 0.5 * (d.eta_n[nn.x] + d.depth[nn.x] + d.eta_n[nn.y] + d.depth[nn.y]));
+        const double4 X = d.edge_cross[ed];
+        const double un1 = (d.V_filt_2D[e1] * X.x - d.U_filt_2D[e1] * X.y) * dmean;
+        if (code & 1) v = v - un1 / d.area[n];
+        else v = v + un1 / d.area[n];
+    }
+    return v;
+}
+
+// QUICK vertical flux tvert(k) of solve_tracer_upwind at interface k
+// (0-based, 0..NS-1) of node n; TO(m) returns the AB2 tracer of layer m.
+template <typename F>
+__device__ __forceinline__ double tvert_upwind(const Dev &d, int k, double a, const double *W, F TO) {
+    const int NS = d.NS;
+    if (k == NS - 1) return 0.0;
+    if (k == 0) return -W[0] * TO(0);
+    const int nz = k + 1;  // 1-based
+    // Z(m), zbar(m) 1-based
+    auto Z = [&](int m) { return z_of(d, a, m - 1); };
+    auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
+    auto T = [&](int m) { return TO(m - 1); };
+    const double w = W[nz - 1];
+    if (nz == 2) {
+        if (w > 0.0) {
+            const double dg = (ZB(2) - Z(1)) * (Z(2) - ZB(2)) / ((Z(3) - Z(1)) * (Z(2) - Z(3)));
+            const double db = -(ZB(2) - Z(1)) * (Z(3) - ZB(2)) / ((Z(2) - Z(1)) * (Z(2) - Z(3)));
+            return -(T(1) * (1.0 - dg - db) + T(2) * db + T(3) * dg) * w;
+        }
+        return -T(1) * w;
+    }
+    if (nz <= NS - 2) {
+        if (w >= 0.0) {
+            const double dg = (ZB(nz) - Z(nz - 1)) * (Z(nz) - ZB(nz)) / ((Z(nz + 1) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+            const double db = -(ZB(nz) - Z(nz - 1)) * (Z(nz + 1) - ZB(nz)) / ((Z(nz) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+            return -(T(nz - 1) * (1.0 - dg - db) + T(nz) * db + T(nz + 1) * dg) * w;
+        }
+        const double dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
+        const double db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
+        return -(T(nz) * (1.0 - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
+    }
+    // nz == NS-1
+    if (w >= 0.0) return -T(nz) * w;
+    const double dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
+    const double db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
+    return -(T(nz) * (1.0 - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
+}
+
+// ---------------------------------------------------------------------------
+// solve_tracer_upwind, one thread per (node, level)
+// ---------------------------------------------------------------------------
+__global__ void k_upwind_h(Dev d) {
+    const long long total = (long long)d.N * d.L;
+    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    GRID_LOOP(ii, total) {
+        const int n = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L, NS = d.NS;
+        double acc_t = 0.0, acc_s = 0.0, acc_c = 0.0;
+        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
+            const int code = d.node_eidx[p];
+            const int ed = code >> 1;
+            const int2 nn = d.edge_nodes[ed];
+            const int2 et = d.edge_tri[ed];
+            const double4 X = d.edge_cross[ed];
+            const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
+            const double t1 = ab2(d, d.TF, d.T_old, i1, T_aver), t2 = ab2(d, d.TF, d.T_old, i2, T_aver);
+            const double s1 = ab2(d, d.SF, d.S_old, i1, S_aver), s2 = ab2(d, d.SF, d.S_old, i2, S_aver);
+            const double4 w1 = d.w_cv[et.x];
+            const double4 a1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
+            const double J1 = je_of(d, w1, a1, z);
+            const size_t e1 = (size_t)et.x * L + z;
+            const double c1 = d.V_n_filt[e1] * X.x - d.U_n_filt[e1] * X.y;
+            double aux_c, t_aux, s_aux;
+            if (ed < d.Ed_in) {
+                const double4 w2 = d.w_cv[et.y];
+                const double4 a2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
+                const double J2 = je_of(d, w2, a2, z);
+                const size_t e2 = (size_t)et.y * L + z;
+                const double c2 = -d.V_n_filt[e2] * X.z + d.U_n_filt[e2] * X.w;
+                aux_c = J1 * c1 + J2 * c2;
+                if (c1 > 0.0 && c2 > 0.0) {
+                    t_aux = J1 * c1 * t2 + J2 * c2 * t2;
+                    s_aux = J1 * c1 * s2 + J2 * c2 * s2;
+                } else if (c1 > 0.0) {
+                    t_aux = J1 * c1 * t2 + J2 * c2 * t1;
+                    s_aux = J1 * c1 * s2 + J2 * c2 * s1;
+                } else if (c2 > 0.0) {
+                    t_aux = J1 * c1 * t1 + J2 * c2 * t2;
+                    s_aux = J1 * c1 * s1 + J2 * c2 * s2;
+                } else {
+                    t_aux = J1 * c1 * t1 + J2 * c2 * t1;
+                    s_aux = J1 * c1 * s1 + J2 * c2 * s1;
+                }
+            } else {
+                aux_c = J1 * c1;
+                if (c1 > 0.0) { t_aux = aux_c * t2; s_aux = aux_c * s2; }
+                else { t_aux = aux_c * t1; s_aux = aux_c * s1; }
+            }
+            if (code & 1) { acc_c = acc_c - aux_c; acc_t = acc_t - t_aux; acc_s = acc_s - s_aux; }
+            else { acc_c = acc_c + aux_c; acc_t = acc_t + t_aux; acc_s = acc_s + s_aux; }
+        }
+        // vertical part
+        const double a = jac_a(d, d.eta_jac, n);
+        const double *W = d.Wvel + (size_t)n * NS;
+        const size_t base = (size_t)n * L;
+        auto TO = [&](int m) { return ab2(d, d.TF, d.T_old, base + m, T_aver); };
+        auto SO = [&](int m) { return ab2(d, d.SF, d.S_old, base + m, S_aver); };
+        const double tv0 = tvert_upwind(d, z, a, W, TO), tv1 = tvert_upwind(d, z + 1, a, W, TO);
+        const double sv0 = tvert_upwind(d, z, a, W, SO), sv1 = tvert_upwind(d, z + 1, a, W, SO);
+        const double area_inv = 1.0 / d.area[n];
+        const double to = TO(z), so = SO(z);
+        const double jc = jc_of(d, a, z);
+        double tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
+        double sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
+        if (d.cl_relax && d.index_nod2D[n] == 2) {
+            const double vn = vel_nor(d, n);
+            if (vn > 0.0) {
+                tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (to + T_aver));
+                sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (so + S_aver));
+            } else {
+                tr = d.clim_relax * (d.Tclim[ii] - (to + T_aver));
+                sr = d.clim_relax * (d.Sclim[ii] - (so + S_aver));
+            }
+        }
+        const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+        d.Told_new[ii] = ttf + T_aver;
+        d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+        d.Sold_new[ii] = stf + S_aver;
+        d.SF_adv[ii] = stf + sr * d.dt + S_aver;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MUSCL (fv_tracer.F90:8-379) for T and S
+// ---------------------------------------------------------------------------
+// tracer_gradient_elements of the AB2 tracer, thread per (element, level)
+__global__ void k_muscl_egrad(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        const int4 en = d.elem_nodes[e];
+        const size_t i1 = (size_t)en.x * L + z, i2 = (size_t)en.y * L + z, i3 = (size_t)en.z * L + z,
+                     i4 = (size_t)en.w * L + z;
+        const double t1 = ab2(d, d.TF, d.T_old, i1, T_aver), t2 = ab2(d, d.TF, d.T_old, i2, T_aver),
+                     t3 = ab2(d, d.TF, d.T_old, i3, T_aver), t4 = ab2(d, d.TF, d.T_old, i4, T_aver);
+        const double s1 = ab2(d, d.SF, d.S_old, i1, S_aver), s2 = ab2(d, d.SF, d.S_old, i2, S_aver),
+                     s3 = ab2(d, d.SF, d.S_old, i3, S_aver), s4 = ab2(d, d.SF, d.S_old, i4, S_aver);
+        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
+        d.ttx[ii] = wsum(gx, t1, t2, t3, t4);
+        d.tty[ii] = wsum(gy, t1, t2, t3, t4);
+        d.stx[ii] = wsum(gx, s1, s2, s3, s4);
+        d.sty[ii] = wsum(gy, s1, s2, s3, s4);
+    }
+}
+
+// area-weighted node mean of the element gradients (fill_up_dn_grad fallback,
+// fv_gradients.F90:292-318: tx/tvol with running sums)
+__global__ void k_muscl_ngrad(Dev d) {
+    const long long total = (long long)d.N * d.L;
+    GRID_LOOP(ii, total) {
+        const int n = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        double tvol = 0.0, a = 0.0, b = 0.0, c = 0.0, e4 = 0.0;
+        for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
+            const int el = d.node_nidx[p];
+            const double ar = d.elem_area[el];
+            const size_t i = (size_t)el * L + z;
+            tvol = tvol + ar;
+            a = a + d.ttx[i] * ar;
+            b = b + d.tty[i] * ar;
+            c = c + d.stx[i] * ar;
+            e4 = e4 + d.sty[i] * ar;
+        }
+        d.tnx[ii] = a / tvol;
+        d.tny[ii] = b / tvol;
+        d.snx[ii] = c / tvol;
+        d.sny[ii] = e4 / tvol;
+    }
+}
+
+// MUSCL vertical flux (fv_tracer.F90:225-271) at interface k (0-based) of a
+// column with AB2 tracer TO(m); Tmean carries over when W == 0 as in the
+// reference.
+template <typename F>
+__device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, const double *W, F TO) {
+    const int NS = d.NS;
+    if (k == NS - 1) return 0.0;
+    if (k == 0) return -W[0] * TO(0);
+    double Tmean = 0.0;
+    // replay interfaces 2..k+1 only for the carried Tmean when W == 0
+    int start = k + 1;
+    while (start > 2 && W[start - 1] == 0.0) --start;
+    for (int nz = start; nz <= k + 1; ++nz) {
+        const double w = W[nz - 1];
+        auto Z = [&](int m) { return z_of(d, a, m - 1); };
+        auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
+        if (w > 0.0) {
+            if (nz == NS - 1) Tmean = TO(nz - 1);
+            else {
+                const double aa = ZB(nz) - Z(nz - 1), bb = Z(nz) - ZB(nz), cc = Z(nz + 1) - ZB(nz);
+                const double dg = aa * bb / (cc + aa) / (bb - cc);
+                const double db = -aa * cc / (bb + aa) / (bb - cc);
+                const double da = 1.0 - dg - db;
+                Tmean = TO(nz - 2) * da + TO(nz - 1) * db + TO(nz) * dg;
+            }
+        }
+        if (w < 0.0) {
+            if (nz == 2) Tmean = TO(nz - 2);
+            else {
+                const double aa = Z(nz) - ZB(nz), bb = ZB(nz) - Z(nz - 1), cc = ZB(nz) - Z(nz - 2);
+                const double dg = aa * bb / (cc + aa) / (bb - cc);
+                const double db = -aa * cc / (bb + aa) / (bb - cc);
+                const double da = 1.0 - dg - db;
+                Tmean = TO(nz - 1) * da + TO(nz - 2) * db + TO(nz - 3) * dg;
+            }
+        }
+    }
+    return -Tmean * W[k];
+}
+
+__global__ void k_muscl_h(Dev d) {
+    const long long total = (long long)d.N * d.L;
+    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    GRID_LOOP(ii, total) {
+        const int n = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L, NS = d.NS;
+        double rt = 0.0, rs = 0.0, rc = 0.0;
+        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
+            const int code = d.node_eidx[p];
+            const int ed = code >> 1;
+            const int2 nn = d.edge_nodes[ed];
+            const int2 et = d.edge_tri[ed];
+            const int2 ud = d.edge_updn[ed];
+            const double4 X = d.edge_cross[ed];
+            const double2 exy = d.edge_dxdy[ed];
+            const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
+            const double T1 = ab2(d, d.TF, d.T_old, i1, T_aver), T2 = ab2(d, d.TF, d.T_old, i2, T_aver);
+            const double S1 = ab2(d, d.SF, d.S_old, i1, S_aver), S2 = ab2(d, d.SF, d.S_old, i2, S_aver);
+            double g1, g2, g3, g4, h1, h2, h3, h4;
+            if (ud.x >= 0 && ud.y >= 0) {
+                const size_t u = (size_t)ud.x * L + z, w = (size_t)ud.y * L + z;
+                g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
+                h1 = d.stx[u]; h2 = d.stx[w]; h3 = d.sty[u]; h4 = d.sty[w];
+            } else {
+                g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
+                h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
+            }
+            const double a = kREarth * d.elem_cos[et.x];
+            const size_t e1 = (size_t)et.x * L + z;
+            const double4 w1 = d.w_cv[et.x];
+            const double4 ja1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
+            const double J1 = je_of(d, w1, ja1, z);
+            const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+            const bool up1 = V1 * X.x - U1 * X.y > 0;
+            {
+                const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
+                const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
+                const double Tm = up1 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+                const double c1 = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
+                const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
+                const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
+                const double Sm = up1 ? 0.15 * Sm2 + 0.85 * (Sm1 + Sm2) / 2.0 : 0.15 * Sm1 + 0.85 * (Sm1 + Sm2) / 2.0;
+                const double s1c = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
+                if (code & 1) { rt = rt - c1; rs = rs - s1c; }
+                else { rt = rt + c1; rs = rs + s1c; }
+            }
+            double cc1 = J1 * V1 * X.x - J1 * U1 * X.y;
+            if (code & 1) rc = rc - cc1;
+            else rc = rc + cc1;
+            if (et.y >= 0) {
+                const double b = kREarth * d.elem_cos[et.y];
+                const size_t e2 = (size_t)et.y * L + z;
+                const double4 w2 = d.w_cv[et.y];
+                const double4 ja2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
+                const double J2 = je_of(d, w2, ja2, z);
+                const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
+                const bool up2 = V2f * X.z - U2f * X.w < 0;
+                const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
+                const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
+                const double Tm = up2 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+                const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
+                const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
+                const double Sm = up2 ? 0.15 * Sm2 + 0.85 * (Sm1 + Sm2) / 2.0 : 0.15 * Sm1 + 0.85 * (Sm1 + Sm2) / 2.0;
+                // second segment uses U_n / V_n (fv_tracer.F90:158-159)
+                const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
+                const double c2 = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
+                const double s2c = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
+                if (code & 1) { rt = rt - c2; rs = rs - s2c; }
+                else { rt = rt + c2; rs = rs + s2c; }
+            }
+        }
+        // ttrhs_c: separate accumulator filled in a second edge loop in the
+        // reference; same per-node order, so it is the rc sum above except
+        // that the second segment contribution must follow the first of the
+        // same edge -- recompute it in edge order here.
+        rc = 0.0;
+        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
+            const int code = d.node_eidx[p];
+            const int ed = code >> 1;
+            const int2 et = d.edge_tri[ed];
+            const double4 X = d.edge_cross[ed];
+            const size_t e1 = (size_t)et.x * L + z;
+            const double J1 = je_of(d, d.w_cv[et.x], elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]), z);
+            const double c1 = J1 * d.V_n_filt[e1] * X.x - J1 * d.U_n_filt[e1] * X.y;
+            if (code & 1) rc = rc - c1;
+            else rc = rc + c1;
+            if (et.y >= 0) {
+                const size_t e2 = (size_t)et.y * L + z;
+                const double J2 = je_of(d, d.w_cv[et.y], elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]), z);
+                const double c2 = -J2 * d.V_n_filt[e2] * X.z + J2 * d.U_n_filt[e2] * X.w;
+                if (code & 1) rc = rc - c2;
+                else rc = rc + c2;
+            }
+        }
+        const double a = jac_a(d, d.eta_jac, n);
+        const double *W = d.Wvel + (size_t)n * NS;
+        const size_t base = (size_t)n * L;
+        auto TO = [&](int m) { return ab2(d, d.TF, d.T_old, base + m, T_aver); };
+        auto SO = [&](int m) { return ab2(d, d.SF, d.S_old, base + m, S_aver); };
+        const double tv0 = tvert_muscl(d, z, a, W, TO), tv1 = tvert_muscl(d, z + 1, a, W, TO);
+        const double sv0 = tvert_muscl(d, z, a, W, SO), sv1 = tvert_muscl(d, z + 1, a, W, SO);
+        const double jc = jc_of(d, a, z);
+        const double aj = d.area[n] * jc;
+        const double to = TO(z), so = SO(z);
+        double tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
+        double sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
+        const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+        if (d.cl_relax && d.index_nod2D[n] == 2) {
+            const double vn = vel_nor(d, n);
+            if (vn > 0.0) {
+                tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
+            } else {
+                tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
+                sr = d.clim_relax * (d.Sclim[ii] - (stf + S_aver));
+            }
+        }
+        d.Told_new[ii] = ttf + T_aver;
+        d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+        d.Sold_new[ii] = stf + S_aver;
+        d.SF_adv[ii] = stf + sr * d.dt + S_aver;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// rivers + tracer_impl_vert_diff, one thread per node column
+// ---------------------------------------------------------------------------
+template <int MAXL>
+__global__ void k_vdiff_col(Dev d) {
+    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    GRID_LOOP(ii, d.N) {
+        const int n = (int)ii;
+        const int L = d.L, NS = d.NS;
+        const size_t base = (size_t)n * L;
+        const double aj = jac_a(d, d.eta_jac, n);
+        double T[MAXL], S[MAXL], So[MAXL];
+        for (int z = 0; z < L; ++z) {
+            T[z] = d.TF_adv[base + z];
+            S[z] = d.SF_adv[base + z];
+            So[z] = d.Sold_new[base + z];
+        }
+        if (d.key_rivers) {
+            for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) {
+                const double r = d.runoff[d.node_ridx[p]];
+                for (int z = 0; z < L; ++z) {
+                    const double coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
+                    const double delta = (d.river_salinity - So[z]);
+                    S[z] = S[z] + delta * coeff;
+                }
+            }
+        }
+        for (int z = 0; z < L; ++z) { T[z] = T[z] - T_aver; S[z] = S[z] - S_aver; }
+        const double *Kv = d.Kv + (size_t)n * NS;
+        const double dt = d.dt;
+        double a[MAXL], b[MAXL], c[MAXL], tr[MAXL], sr[MAXL];
+        double Zc[MAXL], ZBc[MAXL + 1];
+        for (int z = 0; z < L; ++z) Zc[z] = z_of(d, aj, z);
+        for (int z = 0; z < NS; ++z) ZBc[z] = zbar_of(d, aj, z);
+        // 1-based nz -> 0-based index nz-1
+        for (int nz = 2; nz <= NS - 2; ++nz) {
+            const int k = nz - 1;
+            a[k] = -dt * Kv[nz - 1] / ((Zc[k - 1] - Zc[k]) * (ZBc[k] - ZBc[k + 1]));
+            c[k] = -dt * Kv[nz - 1] / ((Zc[k] - Zc[k + 1]) * (ZBc[k] - ZBc[k + 1]));
+            b[k] = -a[k] - c[k] + 1.0;
+        }
+        c[0] = -dt * Kv[1] / ((Zc[0] - Zc[1]) * (ZBc[0] - ZBc[1]));
+        a[0] = 0.0;
+        b[0] = -c[0] + 1.0;
+        a[L - 1] = -dt * Kv[L - 1] / ((Zc[L - 2] - Zc[L - 1]) * (ZBc[L - 1] - ZBc[NS - 1]));
+        b[L - 1] = -a[L - 1] + 1.0;
+        c[L - 1] = 0.0;
+        tr[0] = c[0] * (-T[1] + T[0]);
+        sr[0] = c[0] * (-S[1] + S[0]);
+        for (int k = 1; k <= L - 2; ++k) {
+            tr[k] = -a[k] * T[k - 1] - c[k] * T[k + 1] + (a[k] + c[k]) * T[k];
+            sr[k] = -a[k] * S[k - 1] - c[k] * S[k + 1] + (a[k] + c[k]) * S[k];
+        }
+        tr[L - 1] = a[L - 1] * (T[L - 1] - T[L - 2]);
+        sr[L - 1] = a[L - 1] * (S[L - 1] - S[L - 2]);
+        double cp[MAXL], tp[MAXL], sp[MAXL];
+        cp[0] = c[0] / b[0];
+        tp[0] = tr[0] / b[0];
+        sp[0] = sr[0] / b[0];
+        for (int k = 1; k < L; ++k) {
+            const double m = 1.0 / (b[k] - cp[k - 1] * a[k]);
+            cp[k] = c[k] * m;
+            tp[k] = (tr[k] - tp[k - 1] * a[k]) * m;
+            sp[k] = (sr[k] - sp[k - 1] * a[k]) * m;
+        }
+        tr[L - 1] = tp[L - 1];
+        sr[L - 1] = sp[L - 1];
+        for (int k = L - 2; k >= 0; --k) {
+            tr[k] = tp[k] - cp[k] * tr[k + 1];
+            sr[k] = sp[k] - cp[k] * sr[k + 1];
+        }
+        unsigned int st = 0;
+        for (int z = 0; z < L; ++z) {
+            double t = T[z] + tr[z] + T_aver;
+            double s = S[z] + sr[z] + S_aver;
+            if (fabs(s) < 1.0e-12) s = fabs(s);
+            if (s < 0.0) st |= 0x1u;
+            if (t < -3.0) st |= 0x2u;
+            if (!isfinite(t) || !isfinite(s)) st |= 0x4u;
+            d.TF[base + z] = t;
+            d.SF[base + z] = s;
+            d.T_old[base + z] = d.Told_new[base + z];
+            d.S_old[base + z] = So[z];
+        }
+        if (!isfinite(d.eta_n[n])) st |= 0x4u;
+        if (st) atomicOr(d.status, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// energy: compensated (Neumaier) partial sums per block, then one block
+// ---------------------------------------------------------------------------
+struct KSum {
+    double s, c;
+    __device__ void add(double x) {
+        double t = s + x;
+        if (fabs(s) >= fabs(x)) c += (s - t) + x;
+        else c += (x - t) + s;
+        s = t;
+    }
+    __device__ double value() const { return s + c; }
+};
+
+__global__ void k_energy_part(Dev d, double *part) {
+    __shared__ double sh[3][kRedBlock];
+    KSum pe{0.0, 0.0}, ke{0.0, 0.0}, ar{0.0, 0.0};
+    GRID_LOOP(i, d.N) {
+        const double e = d.eta_n[i];
+        pe.add(0.5 * kG * d.area[i] * (e * e));
+        ar.add(d.area[i]);
+    }
+    GRID_LOOP(i, d.E) {
+        const int4 en = d.elem_nodes[i];
+        const double4 w = d.w_cv[i];
+        const double s = wsum(w, dmax(d.Dmin, d.depth[en.x] + d.eta_n[en.x]), dmax(d.Dmin, d.depth[en.y] + d.eta_n[en.y]),
+                              dmax(d.Dmin, d.depth[en.z] + d.eta_n[en.z]), dmax(d.Dmin, d.depth[en.w] + d.eta_n[en.w]));
+        const double2 u = d.U_n_2D[i];
+        ke.add(0.5 * s * d.elem_area[i] * (u.x * u.x + u.y * u.y));
+    }
+    sh[0][threadIdx.x] = pe.value();
+    sh[1][threadIdx.x] = ke.value();
+    sh[2][threadIdx.x] = ar.value();
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        KSum t{0.0, 0.0};
+        for (int k = 0; k < kRedBlock; ++k) t.add(sh[threadIdx.x][k]);
+        part[(size_t)blockIdx.x * 3 + threadIdx.x] = t.value();
+    }
+}
+
+__global__ void k_energy_final(const double *part, int nparts, double *out) {
+    if (threadIdx.x < 3 && blockIdx.x == 0) {
+        KSum t{0.0, 0.0};
+        for (int b = 0; b < nparts; ++b) t.add(part[(size_t)b * 3 + threadIdx.x]);
+        out[threadIdx.x] = t.value();
+    }
+}
+
+// ---- launch wrappers --------------------------------------------------------
+void launch_minmax(const Dev &d, cudaStream_t s) {
+    k_minmax_part<<<kRedGrid, kRedBlock, 0, s>>>(d);
+    k_minmax_final<<<1, 32, 0, s>>>(d, kRedGrid);
+}
+void launch_upwind(const Dev &d, cudaStream_t s) {
+    k_upwind_h<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_muscl(const Dev &d, cudaStream_t s) {
+    k_muscl_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+    k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
+}
+void launch_vdiff(const Dev &d, cudaStream_t s) {
+    if (d.L <= 24) k_vdiff_col<24><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    else if (d.L <= 48) k_vdiff_col<48><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    else k_vdiff_col<128><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+}
+int energy_parts() { return kRedGrid; }
+void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {
+    k_energy_part<<<kRedGrid, kRedBlock, 0, s>>>(d, part);
+    k_energy_final<<<1, 32, 0, s>>>(part, kRedGrid, out);
+}
+
+}  // namespace fesomc

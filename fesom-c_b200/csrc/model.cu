@@ -1,0 +1,688 @@
+// C-ABI of the B200 FESOM-C time step: set-up of the device mesh (CSR
+// gather lists in reference edge order), device state, the per-step launch
+// sequence of oce_timestep case(3) (src/fv_main.F90:1983-2095) and its
+// capture into one CUDA graph, forcing upload, state sync and diagnostics.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "fesomc_gpu.h"
+
+namespace fesomc {
+// kernels (k_*.cu)
+void launch_ab3_elem(const Dev &, cudaStream_t);
+void launch_ssh_node(const Dev &, int, cudaStream_t);
+void launch_puls_elem(const Dev &, cudaStream_t);
+void launch_el2nodes(const Dev &, const double *, const double *, double *, double *, cudaStream_t);
+void launch_p1_elem(const Dev &, cudaStream_t);
+void launch_u2d_elem(const Dev &, cudaStream_t);
+void launch_rot_nodes(const Dev &, cudaStream_t);
+void launch_zero_filt(const Dev &, cudaStream_t);
+void launch_pressure(const Dev &, cudaStream_t);
+void launch_velgrad3d(const Dev &, cudaStream_t);
+void launch_velrhs(const Dev &, double, cudaStream_t);
+void launch_implvisc(const Dev &, cudaStream_t);
+void launch_jac_swap(const Dev &, cudaStream_t);
+void launch_update3d(const Dev &, double, cudaStream_t);
+void launch_wvel(const Dev &, cudaStream_t);
+void launch_d3end(const Dev &, cudaStream_t);
+void launch_minmax(const Dev &, cudaStream_t);
+void launch_upwind(const Dev &, cudaStream_t);
+void launch_muscl(const Dev &, cudaStream_t);
+void launch_vdiff(const Dev &, cudaStream_t);
+int energy_parts();
+void launch_energy(const Dev &, double *, double *, cudaStream_t);
+
+int grid_for(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    const long long cap = 148LL * 32;
+    return (int)(g < cap ? g : cap);
+}
+
+// Harmonics_tf_period (fv_var.F90:171-172), hours
+static const double kHarmPeriod[12] = {12.4200, 12.00, 12.6584, 11.9673, 23.9344, 25.8194,
+                                       24.0659, 26.8684, 327.85, 661.31, 4383.05, 6.2103};
+static const double kPi = 3.14159265358979;
+}  // namespace fesomc
+
+using namespace fesomc;
+
+struct fesomc_model {
+    Dev d{};
+    fesomc_params p{};
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocs;
+    // host copies needed per step
+    std::vector<double> ampt, fazt;
+    double amp_factor[12], phy_factor[12];
+    // pinned staging for per-step uploads (double buffered)
+    double *h_stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    int stage_i = 0;
+    size_t stage_len = 0;
+    double *h_runoff = nullptr;  // host copy of current runoff
+    bool runoff_dirty = false;
+    // diagnostics
+    double *d_epart = nullptr, *d_eout = nullptr;
+    unsigned int *h_status = nullptr;
+    int *h_notconv = nullptr;
+    unsigned int status_acc = 0;
+    int notconv_acc = 0;
+    // time
+    double time_jd = 0.0;
+    int lfirst = 1;
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    bool use_graph = true;
+    long long launches = 0;
+    int launches_per_step = 0;
+};
+
+namespace {
+
+#define CK(x)                                                                           \
+    do {                                                                                \
+        cudaError_t e_ = (x);                                                           \
+        if (e_ != cudaSuccess) {                                                        \
+            std::fprintf(stderr, "fesomc: CUDA error %s at %s:%d\n", cudaGetErrorString(e_), \
+                         __FILE__, __LINE__);                                           \
+            return FESOMC_ECUDA;                                                        \
+        }                                                                               \
+    } while (0)
+
+template <typename T>
+int dalloc(fesomc_model *m, T **p, size_t n) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) return FESOMC_ENOMEM;
+    cudaMemset(q, 0, (n ? n : 1) * sizeof(T));
+    m->allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return FESOMC_OK;
+}
+
+template <typename T>
+int upload(fesomc_model *m, const T **dst, const std::vector<T> &src) {
+    T *q = nullptr;
+    int rc = dalloc(m, &q, src.size());
+    if (rc) return rc;
+    if (!src.empty()) CK(cudaMemcpy(q, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = q;
+    return FESOMC_OK;
+}
+
+// field table for state sync: name of the fesomc_state member, device pointer, count, group
+struct FieldRef {
+    double *fesomc_state::*host;
+    double *dev;
+    size_t count;
+    uint32_t group;
+};
+
+std::vector<FieldRef> field_table(fesomc_model *m) {
+    Dev &d = m->d;
+    const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
+    return {
+        {&fesomc_state::eta_n, d.eta_n, N, FESOMC_F_ETA},
+        {&fesomc_state::eta_n_1, d.eta_n_1, N, FESOMC_F_ETA},
+        {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA},
+        {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA},
+        {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA},
+        {&fesomc_state::U_n_2D, reinterpret_cast<double *>(d.U_n_2D), 2 * E, FESOMC_F_UV2D},
+        {&fesomc_state::U_n_1, reinterpret_cast<double *>(d.U_n_1), 2 * E, FESOMC_F_UV2D},
+        {&fesomc_state::U_n_2, reinterpret_cast<double *>(d.U_n_2), 2 * E, FESOMC_F_UV2D},
+        {&fesomc_state::U_filt_2D, d.U_filt_2D, E, FESOMC_F_UV2D},
+        {&fesomc_state::V_filt_2D, d.V_filt_2D, E, FESOMC_F_UV2D},
+        {&fesomc_state::U_n, d.U_n, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::V_n, d.V_n, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::U_rhsAB, d.U_rhsAB, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::V_rhsAB, d.V_rhsAB, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::U_n_filt, d.U_n_filt, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::V_n_filt, d.V_n_filt, L * E, FESOMC_F_UV3D},
+        {&fesomc_state::TF, d.TF, L * N, FESOMC_F_TS},
+        {&fesomc_state::SF, d.SF, L * N, FESOMC_F_TS},
+        {&fesomc_state::T_old, d.T_old, L * N, FESOMC_F_TS},
+        {&fesomc_state::S_old, d.S_old, L * N, FESOMC_F_TS},
+        {&fesomc_state::Tclim, d.Tclim, L * N, FESOMC_F_CLIM},
+        {&fesomc_state::Sclim, d.Sclim, L * N, FESOMC_F_CLIM},
+        {&fesomc_state::bt, d.bt, NS * N, FESOMC_F_MIX},
+        {&fesomc_state::snu, d.snu, NS * N, FESOMC_F_MIX},
+        {&fesomc_state::Kv, d.Kv, NS * N, FESOMC_F_MIX},
+        {&fesomc_state::Ri, d.Ri, NS * N, FESOMC_F_MIX},
+        {&fesomc_state::tke_dissip, d.tke_dissip, NS * N, FESOMC_F_MIX},
+        {&fesomc_state::Av, d.Av, NS * E, FESOMC_F_MIX},
+        {&fesomc_state::Wvel, d.Wvel, NS * N, FESOMC_F_WVEL},
+        {&fesomc_state::mask_wd, d.mask_wd, E, FESOMC_F_MASK},
+        {&fesomc_state::mask_wd_node, d.mask_wd_node, N, FESOMC_F_MASK},
+        {&fesomc_state::rho_c, d.rho_c, L * N, FESOMC_F_DIAG},
+        {&fesomc_state::hpressure, d.hpressure, NS * N, FESOMC_F_DIAG},
+        {&fesomc_state::Bar_pr_2D, reinterpret_cast<double *>(d.Bar_pr_2D), 2 * E, FESOMC_F_DIAG},
+    };
+}
+
+int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
+    Dev &d = m->d;
+    const int N = msh->nod2D, E = msh->elem2D, Ed = msh->edge2D, Ed_in = msh->edge2D_in, NS = msh->nsigma;
+    const int L = NS - 1;
+    d.N = N; d.E = E; d.Ed = Ed; d.Ed_in = Ed_in; d.L = L; d.NS = NS;
+    d.nobn = msh->nobn; d.n_rivers = msh->n_rivers;
+    std::vector<double> sig(msh->sigma, msh->sigma + NS), dsig(L);
+    for (int k = 0; k < L; ++k) dsig[k] = sig[k] - sig[k + 1];
+    int rc;
+    if ((rc = upload(m, &d.sig, sig)) || (rc = upload(m, &d.dsig, dsig))) return rc;
+    std::vector<int4> en(E), nb(E), ee(E), iel(E);
+    std::vector<double4> wcv(E), gsx(E), gsy(E), gvx(E), gvy(E);
+    std::vector<double> eacc(E), bpf(E);
+    for (int e = 0; e < E; ++e) {
+        const int32_t *q = msh->elem2D_nodes + 4 * e;
+        for (int k = 0; k < 4; ++k)
+            if (q[k] < 1 || q[k] > N) return FESOMC_EINVAL;
+        en[e] = make_int4(q[0] - 1, q[1] - 1, q[2] - 1, q[3] - 1);
+        const int32_t *b = msh->elem_neighbors + 4 * e;
+        nb[e] = make_int4(b[0] > 0 ? b[0] - 1 : -1, b[1] > 0 ? b[1] - 1 : -1, b[2] > 0 ? b[2] - 1 : -1,
+                          b[3] > 0 ? b[3] - 1 : -1);
+        const int32_t *g = msh->elem_edges + 4 * e;
+        ee[e] = make_int4(g[0] - 1, g[1] - 1, g[2] - 1, g[3] - 1);
+        const double *w = msh->w_cv + 4 * e;
+        wcv[e] = make_double4(w[0], w[1], w[2], w[3]);
+        const double *s = msh->gradient_sca + 8 * e;
+        gsx[e] = make_double4(s[0], s[1], s[2], s[3]);
+        gsy[e] = make_double4(s[4], s[5], s[6], s[7]);
+        const double *v = msh->gradient_vec + 8 * e;
+        gvx[e] = make_double4(v[0], v[1], v[2], v[3]);
+        gvy[e] = make_double4(v[4], v[5], v[6], v[7]);
+        double acc = 0.0;
+        for (int k = 0; k < 4; ++k) acc = acc + w[k] * msh->ac[q[k] - 1];
+        eacc[e] = acc;
+        bpf[e] = std::pow(acc, m->p.Bp_bz) * 1.0;
+        // internal edges of this element, in edge order, with the side
+        const int q1 = (q[0] == q[3]) ? 3 : 4;
+        int list[4], nl = 0;
+        for (int j = 0; j < q1; ++j) {
+            const int edg = g[j];
+            if (edg < 1 || edg > Ed) return FESOMC_EINVAL;
+            if (edg > Ed_in) continue;
+            bool dup = false;
+            for (int t = 0; t < nl; ++t) dup |= ((list[t] >> 1) == edg - 1);
+            if (dup) continue;
+            const int side = (msh->edge_tri[2 * (edg - 1)] == e + 1) ? 0 : 1;
+            list[nl++] = ((edg - 1) << 1) | side;
+        }
+        for (int a = 1; a < nl; ++a)
+            for (int b2 = a; b2 > 0 && list[b2 - 1] > list[b2]; --b2) std::swap(list[b2 - 1], list[b2]);
+        int tmp[4] = {-1, -1, -1, -1};
+        for (int t = 0; t < nl; ++t) tmp[t] = list[t];
+        iel[e] = make_int4(tmp[0], tmp[1], tmp[2], tmp[3]);
+    }
+    std::vector<int2> edn(Ed), edt(Ed), eud(Ed);
+    std::vector<double2> exy(Ed);
+    std::vector<double4> ecr(Ed);
+    std::vector<int> ecount(N + 1, 0), bcount(N + 1, 0);
+    for (int ed = 0; ed < Ed; ++ed) {
+        const int n1 = msh->edge_nodes[2 * ed], n2 = msh->edge_nodes[2 * ed + 1];
+        if (n1 < 1 || n1 > N || n2 < 1 || n2 > N) return FESOMC_EINVAL;
+        edn[ed] = make_int2(n1 - 1, n2 - 1);
+        const int t1 = msh->edge_tri[2 * ed], t2 = msh->edge_tri[2 * ed + 1];
+        if (t1 < 1 || t1 > E) return FESOMC_EINVAL;
+        if ((ed < Ed_in) != (t2 > 0)) return FESOMC_EINVAL;
+        edt[ed] = make_int2(t1 - 1, t2 > 0 ? t2 - 1 : -1);
+        if (msh->edge_up_dn_tri) {
+            const int u = msh->edge_up_dn_tri[2 * ed], w = msh->edge_up_dn_tri[2 * ed + 1];
+            eud[ed] = make_int2(u > 0 ? u - 1 : -1, w > 0 ? w - 1 : -1);
+        } else {
+            eud[ed] = make_int2(-1, -1);
+        }
+        exy[ed] = make_double2(msh->edge_dxdy[2 * ed], msh->edge_dxdy[2 * ed + 1]);
+        const double *c = msh->edge_cross_dxdy + 4 * ed;
+        ecr[ed] = make_double4(c[0], c[1], c[2], c[3]);
+        ecount[n1]++; ecount[n2]++;
+        if (ed >= Ed_in) { bcount[n1]++; bcount[n2]++; }
+    }
+    // CSR node -> edges (appending in edge order keeps each list sorted)
+    std::vector<int> eptr(N + 1, 0), bptr(N + 1, 0);
+    for (int n = 0; n < N; ++n) { eptr[n + 1] = eptr[n] + ecount[n + 1]; bptr[n + 1] = bptr[n] + bcount[n + 1]; }
+    std::vector<int> eidx(eptr[N]), bidx(bptr[N]), efill(eptr.begin(), eptr.end() - 1), bfill(bptr.begin(), bptr.end() - 1);
+    for (int ed = 0; ed < Ed; ++ed) {
+        eidx[efill[edn[ed].x]++] = (ed << 1) | 0;
+        eidx[efill[edn[ed].y]++] = (ed << 1) | 1;
+        if (ed >= Ed_in) {
+            bidx[bfill[edn[ed].x]++] = (ed << 1) | 0;
+            bidx[bfill[edn[ed].y]++] = (ed << 1) | 1;
+        }
+    }
+    // CSR node -> elements (nod_in_elem2D order) and the summed area
+    std::vector<int> nptr(N + 1, 0), nidx;
+    std::vector<double> tvol(N);
+    for (int n = 0; n < N; ++n) {
+        const int num = msh->nod_in_elem2D_num[n];
+        double s = 0.0;
+        for (int k = 0; k < num; ++k) {
+            const int el = msh->nod_in_elem2D[(size_t)msh->nod_in_elem2D_max * n + k];
+            if (el < 1 || el > E) return FESOMC_EINVAL;
+            nidx.push_back(el - 1);
+            s = s + msh->elem_area[el - 1];
+        }
+        nptr[n + 1] = (int)nidx.size();
+        tvol[n] = s;
+    }
+    // rivers and open boundary
+    std::vector<int> rcount(N + 1, 0);
+    for (int i = 0; i < msh->n_rivers; ++i) {
+        const int nd = msh->nod_rivers[i];
+        if (nd < 1 || nd > N) return FESOMC_EINVAL;
+        rcount[nd]++;
+    }
+    std::vector<int> rptr(N + 1, 0);
+    for (int n = 0; n < N; ++n) rptr[n + 1] = rptr[n] + rcount[n + 1];
+    std::vector<int> ridx(rptr[N]), rfill(rptr.begin(), rptr.end() - 1);
+    for (int i = 0; i < msh->n_rivers; ++i) ridx[rfill[msh->nod_rivers[i] - 1]++] = i;
+    std::vector<int> obn(N, -1);
+    for (int i = 0; i < msh->nobn; ++i) {
+        const int nd = msh->in_obn[i];
+        if (nd < 1 || nd > N) return FESOMC_EINVAL;
+        obn[nd - 1] = i;
+    }
+    std::vector<int> idx(msh->index_nod2D, msh->index_nod2D + N);
+    std::vector<double> dep(msh->depth, msh->depth + N), area(msh->area, msh->area + N), ac(msh->ac, msh->ac + N);
+    std::vector<double> atp1(msh->a_tp, msh->a_tp + N), atp2(msh->a_tp + N, msh->a_tp + 2 * (size_t)N);
+    std::vector<double> ea(msh->elem_area, msh->elem_area + E), ec(msh->elem_cos, msh->elem_cos + E),
+        cor(msh->coriolis, msh->coriolis + E);
+    if ((rc = upload(m, &d.elem_nodes, en)) || (rc = upload(m, &d.elem_nb, nb)) || (rc = upload(m, &d.elem_edges, ee)) ||
+        (rc = upload(m, &d.elem_iedges, iel)) || (rc = upload(m, &d.edge_nodes, edn)) ||
+        (rc = upload(m, &d.edge_tri, edt)) || (rc = upload(m, &d.edge_updn, eud)) ||
+        (rc = upload(m, &d.node_eptr, eptr)) || (rc = upload(m, &d.node_eidx, eidx)) ||
+        (rc = upload(m, &d.node_nptr, nptr)) || (rc = upload(m, &d.node_nidx, nidx)) ||
+        (rc = upload(m, &d.node_bptr, bptr)) || (rc = upload(m, &d.node_bidx, bidx)) ||
+        (rc = upload(m, &d.node_rptr, rptr)) || (rc = upload(m, &d.node_ridx, ridx)) ||
+        (rc = upload(m, &d.obn_of_node, obn)) || (rc = upload(m, &d.index_nod2D, idx)) ||
+        (rc = upload(m, &d.w_cv, wcv)) || (rc = upload(m, &d.gs_x, gsx)) || (rc = upload(m, &d.gs_y, gsy)) ||
+        (rc = upload(m, &d.gv_x, gvx)) || (rc = upload(m, &d.gv_y, gvy)) || (rc = upload(m, &d.elem_area, ea)) ||
+        (rc = upload(m, &d.elem_cos, ec)) || (rc = upload(m, &d.coriolis, cor)) || (rc = upload(m, &d.area, area)) ||
+        (rc = upload(m, &d.depth, dep)) || (rc = upload(m, &d.ac, ac)) || (rc = upload(m, &d.atp1, atp1)) ||
+        (rc = upload(m, &d.atp2, atp2)) || (rc = upload(m, &d.elem_acc, eacc)) ||
+        (rc = upload(m, &d.elem_bpfac, bpf)) || (rc = upload(m, &d.edge_dxdy, exy)) ||
+        (rc = upload(m, &d.edge_cross, ecr)) || (rc = upload(m, &d.node_tvol, tvol)))
+        return rc;
+    return FESOMC_OK;
+}
+
+int alloc_state(fesomc_model *m) {
+    Dev &d = m->d;
+    const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
+    int rc = 0;
+    double **nodes[] = {&d.eta_n, &d.eta_n_1, &d.eta_n_2, &d.eta_new, &d.etaAB, &d.ssh_gp, &d.eta_jac,
+                        &d.eta_jac_old, &d.mask_wd_node, &d.windx, &d.windy};
+    for (auto p : nodes) if ((rc = dalloc(m, p, N))) return rc;
+    double **elems[] = {&d.aux_elem, &d.dmean_n, &d.U_filt_2D, &d.V_filt_2D, &d.mask_wd, &d.taux, &d.tauy};
+    for (auto p : elems) if ((rc = dalloc(m, p, E))) return rc;
+    double2 **e2[] = {&d.U_n_2D, &d.U_n_1, &d.U_n_2, &d.UAB, &d.U_rhs_2D_3D, &d.Bar_pr_2D};
+    for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
+    if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
+    double **le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
+                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv};
+    for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
+    double **ln[] = {&d.Unode, &d.Vnode, &d.Unode_p, &d.Vnode_p, &d.TF, &d.SF, &d.T_old, &d.S_old, &d.Tclim,
+                     &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new};
+    for (auto p : ln) if ((rc = dalloc(m, p, L * N))) return rc;
+    if (m->p.tracer_adv == FESOMC_TRACER_MUSCL || m->p.tracer_adv == FESOMC_TRACER_MIURA) {
+        double **lg[] = {&d.ttx, &d.tty, &d.stx, &d.sty};
+        for (auto p : lg) if ((rc = dalloc(m, p, L * E))) return rc;
+        double **lgn[] = {&d.tnx, &d.tny, &d.snx, &d.sny};
+        for (auto p : lgn) if ((rc = dalloc(m, p, L * N))) return rc;
+    }
+    double **nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
+    for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
+    if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
+    if ((rc = dalloc(m, &d.runoff, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1)))) return rc;
+    if ((rc = dalloc(m, &d.ob_val, (size_t)(d.nobn > 0 ? d.nobn : 1) * (m->p.Mt > 0 ? m->p.Mt : 1)))) return rc;
+    if ((rc = dalloc(m, &d.mm_part, (size_t)4 * 1024))) return rc;
+    if ((rc = dalloc(m, &d.aver, 2))) return rc;
+    if ((rc = dalloc(m, &d.status, 1))) return rc;
+    if ((rc = dalloc(m, &d.notconv, 1))) return rc;
+    if ((rc = dalloc(m, &m->d_epart, (size_t)3 * energy_parts()))) return rc;
+    if ((rc = dalloc(m, &m->d_eout, 4))) return rc;
+    return FESOMC_OK;
+}
+
+void set_params(Dev &d, const fesomc_params &p) {
+    d.dt = p.dt; d.dt_2D = p.dt_2D; d.Dmin = p.Dmin; d.C_d = p.C_d; d.beta = p.beta; d.epsilon = p.epsilon;
+    d.density_0 = p.density_0; d.scale_area = p.scale_area; d.snul = p.snul; d.z0b_min = p.z0b_min;
+    d.z0s_min = p.z0s_min; d.Pr_num = p.Pr_num; d.beta_scale = p.beta_scale; d.cka = p.cka;
+    d.tau_inv_filt = p.tau_inv_filt; d.K_hor = p.K_hor; d.Cd_bz = p.Cd_bz; d.clim_relax = p.clim_relax;
+    d.relax2clim_ac = p.relax2clim_ac; d.river_salinity = p.river_salinity; d.Mt = p.Mt;
+    d.mom_adv_2D = p.mom_adv_2D; d.mom_adv_3D = p.mom_adv_3D; d.vert_adv = p.vert_adv;
+    d.im_vert_visc = p.im_vert_visc; d.im_vert_visc_fic = p.im_vert_visc_fic; d.fic_point = p.fic_point;
+    d.tracer_adv = p.tracer_adv; d.ver_mix = p.ver_mix; d.filt_2D = p.filt_2D; d.filt_3D = p.filt_3D;
+    d.wet_dry_on = p.wet_dry_on; d.key_rivers = p.key_rivers; d.TF_presence = p.TF_presence; d.cl_relax = p.cl_relax;
+}
+
+// The kernel sequence of one internal step (oce_timestep case(3)).
+int enqueue_step(fesomc_model *m, double ff) {
+    const Dev &d = m->d;
+    cudaStream_t s = m->stream;
+    int n = 0;
+    launch_pressure(d, s); n += 2;
+    launch_el2nodes(d, d.U_n, d.V_n, d.Unode, d.Vnode, s); n += 1;
+    if (d.ver_mix == 3) { launch_d3end(d, s); n += 2; }
+    launch_velgrad3d(d, s); n += 1;
+    launch_velrhs(d, ff, s); n += 1;
+    if (d.im_vert_visc || d.im_vert_visc_fic) { launch_implvisc(d, s); n += 1; }
+    launch_zero_filt(d, s); n += 1;
+    for (int sub = 0; sub < d.Mt; ++sub) {
+        launch_ab3_elem(d, s);
+        launch_ssh_node(d, sub, s);
+        n += 2;
+        if (sub == 0) {
+            launch_puls_elem(d, s);
+            launch_el2nodes(d, d.U_puls, d.V_puls, d.Unode_p, d.Vnode_p, s);
+            launch_p1_elem(d, s);
+            n += 3;
+        }
+        launch_u2d_elem(d, s);
+        launch_rot_nodes(d, s);
+        n += 2;
+    }
+    launch_jac_swap(d, s); n += 1;
+    launch_update3d(d, 1.0 / (double)d.Mt, s); n += 1;
+    launch_wvel(d, s); n += 1;
+    launch_minmax(d, s); n += 2;
+    if (d.tracer_adv == FESOMC_TRACER_MUSCL) { launch_muscl(d, s); n += 3; }
+    else { launch_upwind(d, s); n += 1; }
+    launch_vdiff(d, s); n += 1;
+    m->launches_per_step = n;
+    CK(cudaGetLastError());
+    return FESOMC_OK;
+}
+
+// Open-boundary elevation for the Mt sub-steps of the coming internal step
+// (compute_ssh_rhs_elem, fv_average_dynamic.F90:190-216), on the host with
+// the reference formula; 'time' is the internal-step time in seconds.
+void ob_values(const fesomc_model *m, double time, double time_jd, double *out) {
+    const fesomc_params &p = m->p;
+    const int nobn = m->d.nobn;
+    for (int sub = 0; sub < p.Mt; ++sub) {
+        const double time_2D = time + p.dt_2D * (sub + 1);
+        for (int q = 0; q < nobn; ++q) {
+            double v = 0.0;
+            for (int j = 0; j < 12; ++j)
+                v = v + m->amp_factor[j] * m->ampt[(size_t)nobn * j + q] *
+                            std::cos((time_2D - p.time_jd0 * 86400.0) * 2.0 * kPi / (kHarmPeriod[j] * 3600.0) -
+                                     (m->fazt[(size_t)nobn * j + q] + m->phy_factor[j]));
+            if (!p.restart)
+                if (time_jd - p.time_jd0 < 10.0) v = v * (time_jd - p.time_jd0) / 10.0;
+            out[(size_t)sub * nobn + q] = v;
+        }
+    }
+}
+
+int upload_step_inputs(fesomc_model *m, double time, double time_jd) {
+    const int nobn = m->d.nobn, nr = m->d.n_rivers;
+    const bool need_ob = m->p.TF_presence && nobn > 0;
+    const bool need_r = m->p.key_rivers && nr > 0 && m->runoff_dirty;
+    if (!need_ob && !need_r) return FESOMC_OK;
+    const int i = m->stage_i;
+    m->stage_i ^= 1;
+    CK(cudaEventSynchronize(m->stage_ev[i]));
+    double *h = m->h_stage[i];
+    size_t off = 0;
+    if (need_ob) {
+        ob_values(m, time, time_jd, h);
+        CK(cudaMemcpyAsync(m->d.ob_val, h, sizeof(double) * nobn * m->p.Mt, cudaMemcpyHostToDevice, m->stream));
+        off += (size_t)nobn * m->p.Mt;
+    }
+    if (need_r) {
+        std::memcpy(h + off, m->h_runoff, sizeof(double) * nr);
+        CK(cudaMemcpyAsync(m->d.runoff, h + off, sizeof(double) * nr, cudaMemcpyHostToDevice, m->stream));
+        m->runoff_dirty = false;
+    }
+    CK(cudaEventRecord(m->stage_ev[i], m->stream));
+    return FESOMC_OK;
+}
+
+int collect_status(fesomc_model *m) {
+    Dev &d = m->d;
+    CK(cudaMemcpyAsync(m->h_status, d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaMemcpyAsync(m->h_notconv, d.notconv, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaMemsetAsync(d.status, 0, sizeof(unsigned), m->stream));
+    CK(cudaMemsetAsync(d.notconv, 0, sizeof(int), m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    m->status_acc |= *m->h_status;
+    m->notconv_acc += *m->h_notconv;
+    return FESOMC_OK;
+}
+
+int status_code(unsigned st) {
+    if (st & FESOMC_ST_NONFINITE) return FESOMC_ENONFINITE;
+    if (st & FESOMC_ST_NEGSALT) return FESOMC_ENEGSALT;
+    if (st & FESOMC_ST_LOWTEMP) return FESOMC_ELOWTEMP;
+    return FESOMC_OK;
+}
+
+int run_steps(fesomc_model *m, int nsteps) {
+    for (int k = 0; k < nsteps; ++k) {
+        // time update of the main loop (fv_main.F90:400-401)
+        m->time_jd = m->time_jd + m->p.dt / 86400.0;
+        const double time = m->time_jd * 86400.0;
+        int rc = upload_step_inputs(m, time, m->time_jd);
+        if (rc) return rc;
+        if (m->lfirst) {
+            // first call of compute_vel_rhs: AB2 factor 1 (fv_3D_vel.F90:124-128)
+            rc = enqueue_step(m, 1.0);
+            if (rc) return rc;
+            m->lfirst = 0;
+        } else if (m->use_graph) {
+            if (!m->graph) {
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+                rc = enqueue_step(m, 1.5 + m->p.epsilon);
+                cudaError_t ce = cudaStreamEndCapture(m->stream, &g);
+                if (rc) return rc;
+                CK(ce);
+                CK(cudaGraphInstantiate(&m->graph, g, 0));
+                CK(cudaGraphDestroy(g));
+            }
+            CK(cudaGraphLaunch(m->graph, m->stream));
+        } else {
+            rc = enqueue_step(m, 1.5 + m->p.epsilon);
+            if (rc) return rc;
+        }
+        m->launches += m->launches_per_step;
+    }
+    return FESOMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fesomc_state *st, fesomc_model **out) {
+    if (!mesh || !par || !st || !out) return FESOMC_EINVAL;
+    *out = nullptr;
+    if (mesh->nsigma < 5 || mesh->nsigma > 129 || mesh->nod2D < 3 || mesh->elem2D < 1) return FESOMC_EINVAL;
+    if (par->Mt < 1 || par->dt <= 0.0 || par->dt_2D <= 0.0) return FESOMC_EINVAL;
+    if (par->ver_mix != 3 && par->ver_mix != 0) return FESOMC_EINVAL;
+    if (par->tracer_adv != FESOMC_TRACER_UPWIND && par->tracer_adv != FESOMC_TRACER_MUSCL) return FESOMC_EINVAL;
+    if (par->tracer_adv == FESOMC_TRACER_MUSCL && !mesh->edge_up_dn_tri) return FESOMC_EINVAL;
+    if (par->cl_solid_boder_relax) return FESOMC_EINVAL;
+    if (par->mom_adv_2D != 2 && par->mom_adv_2D != 0) return FESOMC_EINVAL;
+    if (par->mom_adv_3D != 1 && par->mom_adv_3D != 0) return FESOMC_EINVAL;
+    if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
+    fesomc_model *m = new (std::nothrow) fesomc_model();
+    if (!m) return FESOMC_ENOMEM;
+    m->p = *par;
+    set_params(m->d, *par);
+    int rc = FESOMC_OK;
+    auto fail = [&](int code) {
+        fesomc_gpu_finalize(m);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(FESOMC_ECUDA);
+    if ((rc = build_mesh(m, mesh))) return fail(rc);
+    if ((rc = alloc_state(m))) return fail(rc);
+    const size_t nobn = (size_t)(mesh->nobn > 0 ? mesh->nobn : 0);
+    m->ampt.assign(nobn * 12, 0.0);
+    m->fazt.assign(nobn * 12, 0.0);
+    for (int j = 0; j < 12; ++j) { m->amp_factor[j] = 1.0; m->phy_factor[j] = 0.0; }
+    m->stage_len = nobn * (size_t)par->Mt + (size_t)(mesh->n_rivers > 0 ? mesh->n_rivers : 0) + 8;
+    for (int i = 0; i < 2; ++i) {
+        if (cudaMallocHost(&m->h_stage[i], m->stage_len * sizeof(double)) != cudaSuccess) return fail(FESOMC_ENOMEM);
+        if (cudaEventCreateWithFlags(&m->stage_ev[i], cudaEventDisableTiming) != cudaSuccess) return fail(FESOMC_ECUDA);
+    }
+    if (cudaMallocHost(&m->h_runoff, sizeof(double) * (mesh->n_rivers + 1)) != cudaSuccess) return fail(FESOMC_ENOMEM);
+    std::memset(m->h_runoff, 0, sizeof(double) * (mesh->n_rivers + 1));
+    if (cudaMallocHost(&m->h_status, sizeof(unsigned) * 2) != cudaSuccess) return fail(FESOMC_ENOMEM);
+    if (cudaMallocHost(&m->h_notconv, sizeof(int) * 2) != cudaSuccess) return fail(FESOMC_ENOMEM);
+    // state upload (all groups that are provided)
+    if ((rc = fesomc_gpu_sync_from_host(m, FESOMC_F_ALL, st))) return fail(rc);
+    if (!st->mask_wd) {
+        std::vector<double> ones(mesh->elem2D, 1.0);
+        if (cudaMemcpy(m->d.mask_wd, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice)) return fail(FESOMC_ECUDA);
+    }
+    if (!st->mask_wd_node) {
+        std::vector<double> ones(mesh->nod2D, 1.0);
+        if (cudaMemcpy(m->d.mask_wd_node, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice)) return fail(FESOMC_ECUDA);
+    }
+    // jacobian state before the main loop: both calls see the initial eta
+    if (cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice) ||
+        cudaMemcpy(m->d.eta_jac_old, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice))
+        return fail(FESOMC_ECUDA);
+    m->lfirst = st->lfirst;
+    m->time_jd = st->time_jd;
+    if (cudaDeviceSynchronize() != cudaSuccess) return fail(FESOMC_ECUDA);
+    *out = m;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
+    if (!m || !f) return FESOMC_EINVAL;
+    Dev &d = m->d;
+    const size_t N = d.N, E = d.E, L = d.L;
+    cudaStream_t s = m->stream;
+    // large fields are copied synchronously with respect to the stream so the
+    // caller may reuse its buffers on return
+    if (f->taux) CK(cudaMemcpyAsync(d.taux, f->taux, E * 8, cudaMemcpyHostToDevice, s));
+    if (f->tauy) CK(cudaMemcpyAsync(d.tauy, f->tauy, E * 8, cudaMemcpyHostToDevice, s));
+    if (f->windx) CK(cudaMemcpyAsync(d.windx, f->windx, N * 8, cudaMemcpyHostToDevice, s));
+    if (f->windy) CK(cudaMemcpyAsync(d.windy, f->windy, N * 8, cudaMemcpyHostToDevice, s));
+    if (f->Tclim) CK(cudaMemcpyAsync(d.Tclim, f->Tclim, L * N * 8, cudaMemcpyHostToDevice, s));
+    if (f->Sclim) CK(cudaMemcpyAsync(d.Sclim, f->Sclim, L * N * 8, cudaMemcpyHostToDevice, s));
+    if (f->taux || f->tauy || f->windx || f->windy || f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
+    if (f->runoff_rivers && d.n_rivers > 0) {
+        std::memcpy(m->h_runoff, f->runoff_rivers, sizeof(double) * d.n_rivers);
+        m->runoff_dirty = true;
+    }
+    const size_t nobn = (size_t)d.nobn;
+    if (f->ampt && nobn) std::memcpy(m->ampt.data(), f->ampt, nobn * 12 * 8);
+    if (f->fazt && nobn) std::memcpy(m->fazt.data(), f->fazt, nobn * 12 * 8);
+    if (f->amp_factor) std::memcpy(m->amp_factor, f->amp_factor, 12 * 8);
+    if (f->phy_factor) std::memcpy(m->phy_factor, f->phy_factor, 12 * 8);
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_step(fesomc_model *m, int32_t n_dt) {
+    (void)n_dt;
+    if (!m) return FESOMC_ESTATE;
+    int rc = run_steps(m, 1);
+    if (rc) return rc;
+    if ((rc = collect_status(m))) return rc;
+    return status_code(m->status_acc);
+}
+
+int fesomc_gpu_run(fesomc_model *m, int32_t n_dt0, int32_t nsteps) {
+    (void)n_dt0;
+    if (!m || nsteps < 0) return FESOMC_EINVAL;
+    int rc = run_steps(m, nsteps);
+    if (rc) return rc;
+    if ((rc = collect_status(m))) return rc;
+    return status_code(m->status_acc);
+}
+
+int fesomc_gpu_sync_to_host(fesomc_model *m, uint32_t mask, fesomc_state *st) {
+    if (!m || !st) return FESOMC_EINVAL;
+    CK(cudaStreamSynchronize(m->stream));
+    for (const FieldRef &f : field_table(m)) {
+        double *h = st->*(f.host);
+        if ((f.group & mask) && h) CK(cudaMemcpy(h, f.dev, f.count * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    st->lfirst = m->lfirst;
+    st->time_jd = m->time_jd;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state *st) {
+    if (!m || !st) return FESOMC_EINVAL;
+    CK(cudaStreamSynchronize(m->stream));
+    for (const FieldRef &f : field_table(m)) {
+        const double *h = st->*(f.host);
+        if ((f.group & mask) && h) CK(cudaMemcpy(f.dev, h, f.count * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (mask == FESOMC_F_ALL) {
+        m->lfirst = st->lfirst;
+        m->time_jd = st->time_jd;
+    }
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_energy(fesomc_model *m, double *eout) {
+    if (!m || !eout) return FESOMC_EINVAL;
+    launch_energy(m->d, m->d_epart, m->d_eout, m->stream);
+    m->launches += 2;
+    double h[3];
+    CK(cudaMemcpyAsync(h, m->d_eout, 3 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    *eout = (h[0] + h[1]) / h[2];
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv) {
+    if (!m) return FESOMC_EINVAL;
+    if (status) *status = m->status_acc | (m->notconv_acc ? FESOMC_ST_NOTCONV : 0u);
+    if (notconv) *notconv = m->notconv_acc;
+    m->status_acc = 0;
+    m->notconv_acc = 0;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_finalize(fesomc_model *m) {
+    if (!m) return FESOMC_OK;
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (void *p : m->allocs) cudaFree(p);
+    for (int i = 0; i < 2; ++i) {
+        if (m->h_stage[i]) cudaFreeHost(m->h_stage[i]);
+        if (m->stage_ev[i]) cudaEventDestroy(m->stage_ev[i]);
+    }
+    if (m->h_runoff) cudaFreeHost(m->h_runoff);
+    if (m->h_status) cudaFreeHost(m->h_status);
+    if (m->h_notconv) cudaFreeHost(m->h_notconv);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return FESOMC_OK;
+}
+
+const char *fesomc_gpu_error_string(int code) {
+    switch (code) {
+        case FESOMC_OK: return "ok";
+        case FESOMC_EINVAL: return "invalid argument or unsupported option";
+        case FESOMC_ENOMEM: return "out of memory";
+        case FESOMC_ECUDA: return "CUDA runtime error";
+        case FESOMC_ESTATE: return "call out of order";
+        case FESOMC_ENEGSALT: return "negative salinity, time resolution is insufficient";
+        case FESOMC_ELOWTEMP: return "temperature below -3 C, time resolution is insufficient";
+        case FESOMC_ENONFINITE: return "non-finite value in the prognostic state";
+        case FESOMC_ENOTCONV: return "d3_end did not converge in 200 iterations";
+        case FESOMC_EMESH: return "inconsistent element node list";
+        default: return "unknown error";
+    }
+}
+
+const char *fesomc_gpu_version(void) { return "fesomc-b200 0.1 (sm_100a, FP64 plain path)"; }
+
+int64_t fesomc_gpu_kernel_launches(fesomc_model *m) { return m ? m->launches : 0; }
+
+}  // extern "C"

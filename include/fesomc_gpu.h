@@ -1,0 +1,262 @@
+/*
+ * fesomc_gpu.h -- C-ABI of the B200 (sm_100a) FESOM-C ocean time step.
+ *
+ * The reference hot path (FESOM-C, Fortran 90) consists of argument-less
+ * subroutines that read and write module globals (o_PARAM / o_MESH /
+ * o_ARRAYS, src/fv_var.F90:1-438).  The Fortran driver calls them from
+ * oce_timestep (src/fv_main.F90:1877-2106).  This library replaces the body
+ * of oce_timestep for type_task 3 (src/fv_main.F90:1983-2095): the driver
+ * keeps reading namelists, the mesh and forcing, and keeps writing output;
+ * it hands the already-built module arrays to fesomc_gpu_init once, pushes
+ * forcing each internal step with fesomc_gpu_set_forcing, advances with
+ * fesomc_gpu_step and pulls state back with fesomc_gpu_sync_to_host before
+ * output, energy diagnostics and restarts.
+ *
+ * Conventions
+ *  - All arrays are in the reference's Fortran layout: a field dimensioned
+ *    (K, M) in Fortran is passed as a C pointer to K*M values with the first
+ *    index fastest (levels contiguous per node / element).
+ *  - Connectivity arrays carry 1-based indices exactly as the Fortran module
+ *    arrays hold them; boundary markers (edge_tri(2,:) = -999,
+ *    elem_neighbors <= 0) are kept.  The library converts on the host.
+ *  - Every entry point returns 0 on success or one of FESOMC_E* (> 0).
+ *  - The whole mesh lives on one GPU: there is no halo exchange (the MPI
+ *    g_comm / exchange_* calls of the reference drop out).  A caller with
+ *    npes > 1 must not call fesomc_gpu_init (it would return FESOMC_EINVAL).
+ *  - Call from one host thread, outside any OpenMP parallel region.
+ */
+#ifndef FESOMC_GPU_H
+#define FESOMC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- error codes -------------------------------------------------------- */
+#define FESOMC_OK            0
+#define FESOMC_EINVAL        1  /* bad argument / unsupported option          */
+#define FESOMC_ENOMEM        2  /* device or host allocation failed          */
+#define FESOMC_ECUDA         3  /* a CUDA runtime call failed                */
+#define FESOMC_ESTATE        4  /* call out of order (e.g. step before init) */
+#define FESOMC_ENEGSALT      5  /* negative salinity  (fv_tracer.F90:1469-1473) */
+#define FESOMC_ELOWTEMP      6  /* temperature < -3 C (fv_tracer.F90:1478-1482) */
+#define FESOMC_ENONFINITE    7  /* NaN / Inf found in the prognostic state    */
+#define FESOMC_ENOTCONV      8  /* d3_end hit its 200-iteration cap (reported,
+                                   not fatal; see fesomc_gpu_last_status)   */
+#define FESOMC_EMESH         9  /* mesh builder: inconsistent node list
+                                   (test_elem "Node list problem", fv_mesh_array.F90:62-66) */
+
+/* ---- status word bits (device side, read back once per step) ------------ */
+#define FESOMC_ST_NEGSALT    0x1u
+#define FESOMC_ST_LOWTEMP    0x2u
+#define FESOMC_ST_NONFINITE  0x4u
+#define FESOMC_ST_NOTCONV    0x8u
+
+/* ---- field masks for sync ----------------------------------------------- */
+#define FESOMC_F_ETA      0x0001u /* eta_n, eta_n_1, eta_n_2, etaAB           */
+#define FESOMC_F_UV2D     0x0002u /* U_n_2D, U_n_1, U_n_2, U_filt_2D, V_filt_2D */
+#define FESOMC_F_UV3D     0x0004u /* U_n, V_n, U_rhsAB, V_rhsAB, U_n_filt, V_n_filt */
+#define FESOMC_F_TS       0x0008u /* TF, SF, T_old, S_old                     */
+#define FESOMC_F_MIX      0x0010u /* bt, snu, Kv, Av, Ri, tke_dissip           */
+#define FESOMC_F_WVEL     0x0020u /* Wvel                                     */
+#define FESOMC_F_MASK     0x0040u /* mask_wd, mask_wd_node                     */
+#define FESOMC_F_CLIM     0x0080u /* Tclim, Sclim                              */
+#define FESOMC_F_DIAG     0x0100u /* rho_c, hpressure, Bar_pr_2D               */
+#define FESOMC_F_ALL      0xFFFFu
+
+/* ---- option values (fv_run.dat keys, src/fv_read_run.F90) --------------- */
+#define FESOMC_TRACER_UPWIND 1    /* tracer_adv = 1 : solve_tracer_upwind     */
+#define FESOMC_TRACER_MUSCL  2    /* tracer_adv = 2 : solve_tracer_muscl      */
+#define FESOMC_TRACER_MIURA  4    /* tracer_adv = 4 : solve_tracer_miura      */
+
+/*
+ * Mesh, as left in o_MESH by read_mesh_ser / find_edges / find_elem_neighbors
+ * / mesh_arrays1 / mesh_arrays2 / SET_SIGMA (src/fv_main.F90:787-945,
+ * src/fv_mesh_array.F90:1-1386, src/fv_vert_coord.F90:135-280).
+ */
+typedef struct fesomc_mesh {
+    int32_t nod2D, elem2D, edge2D, edge2D_in, nsigma;
+    int32_t nod_in_elem2D_max;        /* leading dimension of nod_in_elem2D   */
+    const int32_t *index_nod2D;       /* (nod2D) 0 interior, 1 solid, 2 open   */
+    const int32_t *elem2D_nodes;      /* (4,elem2D); triangles: node4 = node1 */
+    const int32_t *edge_nodes;        /* (2,edge2D)                           */
+    const int32_t *edge_tri;          /* (2,edge2D); el2 = -999 on boundary   */
+    const int32_t *elem_edges;        /* (4,elem2D)                           */
+    const int32_t *elem_neighbors;    /* (4,elem2D); <= 0 on the boundary     */
+    const int32_t *nod_in_elem2D_num; /* (nod2D)                              */
+    const int32_t *nod_in_elem2D;     /* (nod_in_elem2D_max,nod2D)            */
+    const int32_t *edge_up_dn_tri;    /* (2,edge2D) or NULL (MUSCL only)      */
+    const double  *coord_nod2D;       /* (2,nod2D) radians                    */
+    const double  *depth;             /* (nod2D)                              */
+    const double  *area;              /* (nod2D)                              */
+    const double  *elem_area;         /* (elem2D)                             */
+    const double  *elem_cos;          /* (elem2D)                             */
+    const double  *coriolis;          /* (elem2D)                             */
+    const double  *w_cv;              /* (4,elem2D)                           */
+    const double  *gradient_sca;      /* (8,elem2D)                           */
+    const double  *gradient_vec;      /* (8,elem2D)                           */
+    const double  *edge_dxdy;         /* (2,edge2D)                           */
+    const double  *edge_cross_dxdy;   /* (4,edge2D)                           */
+    const double  *sigma;             /* (nsigma)                             */
+    const double  *a_tp;              /* (nod2D,2)  (fv_ini.F90:94-107)       */
+    const double  *ac;                /* (nod2D) sponge factor, 1 = none      */
+    /* open-boundary nodes (my_in_obn, read_mesh_ser fv_main.F90:841-851)    */
+    int32_t nobn;
+    const int32_t *in_obn;            /* (nobn) 1-based node ids              */
+    /* river nodes (my_nod_rivers, fv_rivers.F90)                            */
+    int32_t n_rivers;
+    const int32_t *nod_rivers;        /* (n_rivers) 1-based node ids          */
+} fesomc_mesh;
+
+/*
+ * Resolved run parameters (o_PARAM after READ_DATA_RUN and initial_state).
+ * Booleans are 0/1.  Times in seconds unless noted.
+ */
+typedef struct fesomc_params {
+    double dt, dt_2D;             /* Mt = int(dt/dt_2D) (fv_read_run.F90:1060) */
+    int32_t Mt;
+    double Dmin;
+    double C_d;                   /* C_d_el = C_d (fv_average_dynamic.F90:262) */
+    double beta, epsilon;         /* AB3 / AB2 coefficients (fv_var.F90:108,110) */
+    double density_0;             /* set by initial_state (fv_ini.F90:187-199)  */
+    double scale_area;            /* sum(elem_area)/elem2D (fv_ini.F90:81)      */
+    double snul, z0b_min, z0s_min, Pr_num, beta_scale, cka;
+    double tau_inv_filt, K_hor, Cd_bz, Bp_bz;
+    double clim_relax, relax2clim_ac;   /* already in 1/s (fv_read_run.F90:884,894) */
+    double river_salinity;        /* 0.2 psu in the reference (fv_main.F90:1818) */
+    double time_jd0;              /* JD0 (days)                                 */
+    int32_t mom_adv_2D;           /* 2 = upwind (only value on the path)       */
+    int32_t mom_adv_3D;           /* 1 = upwind                                */
+    int32_t vert_adv;             /* 1 = upwind QUICK                          */
+    int32_t im_vert_visc;         /* momentum_vert_impl_visc                   */
+    int32_t im_vert_visc_fic;     /* momentum_vert_impl_visc_tmp (fictitious point) */
+    int32_t fic_point;            /* 0, 1, 2                                   */
+    int32_t tracer_adv;           /* FESOMC_TRACER_*                           */
+    int32_t ver_mix;              /* 3 = d3_end (only closure that runs)       */
+    int32_t filt_2D, filt_3D;     /* viscosity_filt_2D / _3D / _3D_to_2D        */
+    int32_t wet_dry_on;
+    int32_t key_rivers;
+    int32_t TF_presence;          /* open-boundary tides                       */
+    int32_t restart;              /* hot start: no 10-day OB ramp              */
+    int32_t cl_relax;
+    int32_t cl_solid_boder_relax; /* not supported: must be 0                  */
+    int32_t temp_on, salinity_on; /* type_task 3 when either is set            */
+    int32_t n_harm;               /* number of tidal harmonics in use (<=12)    */
+    int32_t harm_index[12];       /* 0-based index into the 12 reference waves  */
+} fesomc_params;
+
+/*
+ * Prognostic state (o_ARRAYS) exchanged with the host.  Every pointer may be
+ * NULL on sync_to_host when its field group is not requested.
+ */
+typedef struct fesomc_state {
+    double *eta_n, *eta_n_1, *eta_n_2, *etaAB;        /* (nod2D)              */
+    double *U_n_2D, *U_n_1, *U_n_2;                   /* (2,elem2D)           */
+    double *U_filt_2D, *V_filt_2D;                    /* (elem2D)             */
+    double *U_n, *V_n, *U_rhsAB, *V_rhsAB;            /* (nsigma-1,elem2D)    */
+    double *U_n_filt, *V_n_filt;                      /* (nsigma-1,elem2D)    */
+    double *TF, *SF, *T_old, *S_old;                  /* (nsigma-1,nod2D)     */
+    double *Tclim, *Sclim;                            /* (nsigma-1,nod2D)     */
+    double *bt, *snu, *Kv, *Ri, *tke_dissip;          /* (nsigma,nod2D)       */
+    double *Av;                                       /* (nsigma,elem2D)      */
+    double *Wvel;                                     /* (nsigma,nod2D)       */
+    double *mask_wd;                                  /* (elem2D)             */
+    double *mask_wd_node;                             /* (nod2D)              */
+    double *ssh_gp;                                   /* (nod2D) tidal geopotential */
+    double *rho_c;                                    /* (nsigma-1,nod2D)     */
+    double *hpressure;                                /* (nsigma,nod2D)       */
+    double *Bar_pr_2D;                                /* (2,elem2D)           */
+    int32_t lfirst;                                   /* AB start flag (fv_var.F90:244) */
+    double time_jd;                                   /* model time (days)    */
+} fesomc_state;
+
+/*
+ * Per-internal-step forcing (what rivers_do / sbc_do / obc_do leave in
+ * o_ARRAYS, src/fv_main.F90:412-431).  NULL = keep previous values.
+ */
+typedef struct fesomc_forcing {
+    const double *taux, *tauy;      /* (elem2D) surface stress, N/m^2          */
+    const double *windx, *windy;    /* (nod2D) 10 m wind, m/s                  */
+    const double *runoff_rivers;    /* (n_rivers) m^3/s, ramp already applied  */
+    const double *Tclim, *Sclim;    /* (nsigma-1,nod2D)                        */
+    const double *ampt, *fazt;      /* (nobn,12) OB tidal amplitude / phase    */
+    const double *amp_factor, *phy_factor; /* (12)                             */
+} fesomc_forcing;
+
+/* Opaque model instance. */
+typedef struct fesomc_model fesomc_model;
+
+/* ---- drop-in entry points -------------------------------------------------
+ * fesomc_gpu_init replaces: array_setup .. initial_state state as left at
+ *   src/fv_main.F90:157-362 (jacobian is recomputed on the device).
+ * fesomc_gpu_set_forcing replaces: the module-array writes of rivers_do,
+ *   sbc_do and obc_do (src/fv_main.F90:412-431).
+ * fesomc_gpu_step replaces: oce_timestep, case(3) (src/fv_main.F90:1983-2095)
+ *   together with the time update at src/fv_main.F90:400-401.
+ * fesomc_gpu_sync_to_host / _from_host: before ncoutput(mpi)_do, energy and
+ *   write_restart_separate / after read_restart_separate.
+ * fesomc_gpu_energy replaces: energy(eout) (src/fv_average_dynamic.F90:476-554).
+ */
+int  fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par,
+                     const fesomc_state *state, fesomc_model **out);
+int  fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f);
+int  fesomc_gpu_step(fesomc_model *m, int32_t n_dt);
+int  fesomc_gpu_run(fesomc_model *m, int32_t n_dt0, int32_t nsteps);
+int  fesomc_gpu_sync_to_host(fesomc_model *m, uint32_t field_mask, fesomc_state *state);
+int  fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t field_mask, const fesomc_state *state);
+int  fesomc_gpu_energy(fesomc_model *m, double *eout);
+int  fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv_columns);
+int  fesomc_gpu_finalize(fesomc_model *m);
+const char *fesomc_gpu_error_string(int code);
+
+/* ---- host mesh builder ----------------------------------------------------
+ * Restates read_mesh_ser (triangles first, coordinate scaling,
+ * fv_main.F90:787-945), test_elem (fv_mesh_array.F90:1-82), find_edges
+ * (:395-718), find_elem_neighbors (:791-946), mesh_arrays1 (:948-1139),
+ * mesh_arrays2 (:1155-1386), find_up_downwind_triangles (:1390-1618) and
+ * SET_SIGMA cases 1 and 2 (fv_vert_coord.F90:135-280).  Produces the arrays
+ * a fesomc_mesh points to.  Inputs: node coordinates as in nod2d.out
+ * (metres if cartesian, degrees otherwise), node flags, and elements as in
+ * elem2d.out (4 nodes per row, node4 = node1 for triangles; 1-based).
+ */
+typedef struct fesomc_mesh_builder fesomc_mesh_builder;
+
+typedef struct fesomc_mesh_opts {
+    int32_t cartesian;
+    int32_t coriolis_on;          /* Coriolis_TF                              */
+    double  lat_cartesian_deg;    /* latitude for cartesian Coriolis          */
+    double  cyclic_length_deg;    /* 360 in the reference test case           */
+    int32_t nsigma;
+    int32_t ind_sigma;            /* 1 or 2                                   */
+    double  pow_sig, lev_bot, lev_sur;
+    int32_t T_potential;          /* a_tp = (0.918, 0.69) instead of (1, 0)    */
+    int32_t with_up_dn_tri;       /* compute edge_up_dn_tri (MUSCL)           */
+} fesomc_mesh_opts;
+
+int  fesomc_mesh_build(int32_t nod2D, const double *xy, const int32_t *index_nod2D,
+                       int32_t elem2D, const int32_t *elem_nodes4,
+                       const double *depth, const fesomc_mesh_opts *opts,
+                       fesomc_mesh_builder **out);
+/* Fills *mesh with pointers owned by the builder (valid until free). */
+int  fesomc_mesh_view(const fesomc_mesh_builder *b, fesomc_mesh *mesh);
+/* scale_area = sum(elem_area)/elem2D, sequential sum (fv_ini.F90:81). */
+double fesomc_mesh_scale_area(const fesomc_mesh_builder *b);
+int  fesomc_mesh_set_rivers(fesomc_mesh_builder *b, int32_t n, const int32_t *nodes);
+void fesomc_mesh_free(fesomc_mesh_builder *b);
+
+/* Jackett-McDougall density anomaly rho(t,s,pz) - density_0 on the host, as
+ * initial_state needs it to set density_0 = 1000 + densityJM(T_const, S_const, 0)
+ * (src/fv_ini.F90:187-199; densityJM src/fv_pressure_new.F90:340-414). */
+double fesomc_host_density_jm(double t, double s, double pz, double density_0);
+
+/* ---- version / introspection --------------------------------------------- */
+const char *fesomc_gpu_version(void);
+/* Number of kernels launched by this instance since init. */
+int64_t fesomc_gpu_kernel_launches(fesomc_model *m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FESOMC_GPU_H */

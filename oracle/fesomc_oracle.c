@@ -1,0 +1,1845 @@
+/*
+ * fesomc_oracle.c -- CPU oracle for the FESOM-C ocean time step.
+ *
+ * TEST INFRASTRUCTURE, NOT PRODUCT CODE.  Only the test suite, the smoke
+ * check and the CPU-baseline leg of the benchmark load this library; the
+ * GPU library never links or calls it.
+ *
+ * This is a line-by-line C restatement of the reference Fortran hot path
+ * (rakowsk/fesom-c, src/).  Every routine cites the lines it follows.  It
+ * keeps the reference's serial loop order (edge scatters in edge order),
+ * its operand order inside each expression, its single-precision literals
+ * (Fortran literals without _WP are REAL(4) constants promoted to REAL(8))
+ * and its quirks.  Compile with -ffp-contract=off so no FMA is introduced.
+ *
+ * Parity pins: the mesh arrays it consumes are pinned against the
+ * reference's edges.out / edge_tri.out (LE_medium test case); the whole time
+ * step is pinned against the reference's energy_tocheck.dat series for the
+ * LE_medium lock-exchange case (see tests/).
+ *
+ * Loops that the reference runs with !$OMP DO (or that are independent per
+ * node / element / column) carry "#pragma omp parallel for"; scatter loops
+ * stay serial as in the reference, so results do not depend on the thread
+ * count.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../include/fesomc_gpu.h"
+
+/* ---------------------------------------------------------------- consts */
+static const double WP_PI = 3.14159265358979;   /* fv_var.F90:8 */
+static const double WP_G = 9.8;                 /* fv_var.F90:13 */
+static const double WP_R_EARTH = 6400000.0;     /* fv_var.F90:14 */
+static const double WP_P_REF = 101325.0;        /* fv_var.F90:17 */
+/* Harmonics_tf_period, fv_var.F90:171-172 (hours) */
+static const double HARM_PERIOD[12] = {12.4200, 12.00, 12.6584, 11.9673, 23.9344, 25.8194,
+                                       24.0659, 26.8684, 327.85, 661.31, 4383.05, 6.2103};
+/* REAL(4) literal promoted to REAL(8) */
+#define R4(x) ((double)(float)(x))
+
+#define MAXD(a, b) ((a) > (b) ? (a) : (b))
+#define MIND(a, b) ((a) < (b) ? (a) : (b))
+
+typedef struct oracle_model {
+    int N, E, Ed, Ed_in, NS, L, NIE;
+    fesomc_params p;
+    /* mesh (0-based storage, 1-based content for connectivity) */
+    int32_t *index_nod2D, *elem2D_nodes, *edge_nodes, *edge_tri, *elem_edges, *elem_neighbors,
+        *nod_in_elem2D_num, *nod_in_elem2D, *edge_up_dn_tri, *in_obn, *nod_rivers;
+    int nobn, n_rivers;
+    double *depth, *area, *elem_area, *elem_cos, *coriolis, *w_cv, *gradient_sca, *gradient_vec,
+        *edge_dxdy, *edge_cross_dxdy, *sigma, *a_tp, *ac;
+    /* 2D state */
+    double *eta_n, *eta_n_1, *eta_n_2, *etaAB, *ssh_rhs, *ssh_gp, *eta_p, *eta_tmp;
+    double *U_n_2D, *U_n_1, *U_n_2, *UAB, *U_rhs_2D, *U_rhs_2D_3D, *vel_grad, *dmean_n;
+    double *U_filt_2D, *V_filt_2D, *taux, *tauy, *windx, *windy, *C_d_el;
+    double *mask_wd, *mask_wd_node, *mask_ad, *mask_bpr;
+    double *aux_elem, *c1e;
+    /* 3D state */
+    double *Jc, *Jc_old, *Je, *Jd, *Z, *zbar;
+    double *U_n, *V_n, *U_rhs, *V_rhs, *U_rhsAB, *V_rhsAB, *U_n_filt, *V_n_filt;
+    double *vgux, *vguy, *vgvx, *vgvy, *U_puls, *V_puls, *Unode, *Vnode, *Unode_p, *Vnode_p;
+    double *TF, *SF, *T_old, *S_old, *Tclim, *Sclim, *rho_c, *hpressure;
+    double *Bar_pru_3D, *Bar_prv_3D, *Bar_pr_2D;
+    double *bt, *snu, *Kv, *Av, *Ri, *tke_dissip, *Wvel;
+    /* forcing */
+    double *runoff, *ampt, *fazt, amp_factor[12], phy_factor[12];
+    /* scratch */
+    double *s_e1, *s_e2, *s_e3, *s_e4, *s_n1, *s_n2, *s_n3, *s_n4, *s_ed1, *s_ed2, *s_ed3, *s_ed4;
+    double *s_gr;
+    double T_aver, S_aver;
+    double time_jd, time, time_2D;
+    int lfirst;
+    int status, notconv;
+} oracle_model;
+
+/* 1-based accessors ------------------------------------------------------ */
+#define ELN(q, e) (m->elem2D_nodes[4 * ((e)-1) + (q)-1])
+#define EDN(k, ed) (m->edge_nodes[2 * ((ed)-1) + (k)-1])
+#define EDT(k, ed) (m->edge_tri[2 * ((ed)-1) + (k)-1])
+#define ELE(k, e) (m->elem_edges[4 * ((e)-1) + (k)-1])
+#define ELNB(k, e) (m->elem_neighbors[4 * ((e)-1) + (k)-1])
+#define NIE(k, n) (m->nod_in_elem2D[(size_t)m->NIE * ((n)-1) + (k)-1])
+#define NIEN(n) (m->nod_in_elem2D_num[(n)-1])
+#define WCV(k, e) (m->w_cv[4 * ((e)-1) + (k)-1])
+#define GS(k, e) (m->gradient_sca[8 * ((e)-1) + (k)-1])
+#define GV(k, e) (m->gradient_vec[8 * ((e)-1) + (k)-1])
+#define EDXY(k, ed) (m->edge_dxdy[2 * ((ed)-1) + (k)-1])
+#define ECR(k, ed) (m->edge_cross_dxdy[4 * ((ed)-1) + (k)-1])
+#define SIG(k) (m->sigma[(k)-1])
+#define N1(a, n) ((a)[(n)-1])
+#define V2(a, k, e) ((a)[2 * ((e)-1) + (k)-1])
+#define F3(a, nz, i) ((a)[(size_t)m->L * ((i)-1) + (nz)-1])   /* (L, *)  */
+#define W3(a, nz, i) ((a)[(size_t)m->NS * ((i)-1) + (nz)-1])  /* (NS, *) */
+#define ATP(n, k) (m->a_tp[(size_t)m->N * ((k)-1) + (n)-1])
+#define AMPT(q, j) (m->ampt[(size_t)m->nobn * ((j)-1) + (q)-1])
+#define FAZT(q, j) (m->fazt[(size_t)m->nobn * ((j)-1) + (q)-1])
+
+static double *dalloc(size_t n) {
+    double *p = (double *)calloc(n ? n : 1, sizeof(double));
+    return p;
+}
+static int32_t *icopy(const int32_t *src, size_t n) {
+    int32_t *p = (int32_t *)calloc(n ? n : 1, sizeof(int32_t));
+    if (p && src) memcpy(p, src, n * sizeof(int32_t));
+    return p;
+}
+static double *dcopy(const double *src, size_t n) {
+    double *p = dalloc(n);
+    if (p && src) memcpy(p, src, n * sizeof(double));
+    return p;
+}
+
+/* ====================================================================== */
+/* densityJM, fv_pressure_new.F90:340-414                                  */
+/* ====================================================================== */
+static double densityJM(double t, double s, double pz, double density_0) {
+    double ss3 = sqrt(s * s * s);
+    double bulk = 19092.56 + t * (209.8925 - t * (3.041638 - t * (-R4(1.852732e-3) - t * (R4(1.361629e-5)))))
+                + s * (104.4077 - t * (6.500517 - t * (.1553190 - t * (-R4(2.326469e-4)))))
+                + ss3 * (-5.587545 + t * (0.7390729 - t * (R4(1.909078e-2))))
+                - pz * (R4(4.721788e-1) + t * (R4(1.028859e-2) + t * (-R4(2.512549e-4) - t * (R4(5.939910e-7)))))
+                - pz * s * (-R4(1.571896e-2) - t * (R4(2.598241e-4) + t * (-R4(7.267926e-6))))
+                - pz * ss3 * R4(2.042967e-3)
+                + pz * pz * (R4(1.045941e-5) - t * (R4(5.782165e-10) - t * (R4(1.296821e-7))))
+                + pz * pz * s * (-R4(2.595994e-7) + t * (-R4(1.248266e-9) + t * (-R4(3.508914e-9))));
+    double rhopot = 999.842594
+                  + t * (R4(6.793952e-2) + t * (-R4(9.095290e-3) + t * (R4(1.001685e-4)
+                  + t * (-R4(1.120083e-6) + t * R4(6.536332e-9)))))
+                  + s * (0.824493 + t * (-R4(4.08990e-3) + t * (R4(7.64380e-5)
+                  + t * (-R4(8.24670e-7) + t * R4(5.38750e-9)))))
+                  + ss3 * (-R4(5.72466e-3) + t * (R4(1.02270e-4) + t * (-R4(1.65460e-6))))
+                  + R4(4.8314e-4) * s * s;
+    return rhopot * bulk / (bulk + 0.1 * pz) - density_0;
+}
+
+double oracle_densityJM(double t, double s, double pz, double density_0) {
+    return densityJM(t, s, pz, density_0);
+}
+
+/* ====================================================================== */
+/* jacobian, fv_main.F90:1208-1267                                          */
+/* ====================================================================== */
+static void jacobian(oracle_model *m) {
+    const int NS = m->NS, L = m->L;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        for (int k = 1; k <= L; ++k) F3(m->Jc_old, k, n) = F3(m->Jc, k, n);
+        double a = MAXD(N1(m->depth, n) + N1(m->eta_n, n), m->p.Dmin);
+        for (int k = 1; k <= NS; ++k) W3(m->zbar, k, n) = (1.0 - SIG(k)) * a;
+        for (int k = 1; k <= L; ++k) F3(m->Jc, k, n) = a * (SIG(k) - SIG(k + 1));
+        for (int k = 1; k <= L; ++k) F3(m->Z, k, n) = 0.5 * (W3(m->zbar, k, n) + W3(m->zbar, k + 1, n));
+    }
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el)
+        for (int k = 1; k <= L; ++k)
+            F3(m->Je, k, el) = WCV(1, el) * F3(m->Jc, k, ELN(1, el)) + WCV(2, el) * F3(m->Jc, k, ELN(2, el))
+                             + WCV(3, el) * F3(m->Jc, k, ELN(3, el)) + WCV(4, el) * F3(m->Jc, k, ELN(4, el));
+#pragma omp parallel for
+    for (int ed = 1; ed <= m->Ed; ++ed)
+        for (int k = 1; k <= L; ++k)
+            F3(m->Jd, k, ed) = 0.5 * (F3(m->Jc, k, EDN(1, ed)) + F3(m->Jc, k, EDN(2, ed)));
+}
+
+/* wad_mask, fv_main.F90:1269-1307 */
+static void wad_mask(oracle_model *m) {
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double dmin4 = MIND(MIND(N1(m->depth, ELN(1, el)), N1(m->depth, ELN(2, el))),
+                            MIND(N1(m->depth, ELN(3, el)), N1(m->depth, ELN(4, el))));
+        double emax4 = MAXD(MAXD(N1(m->etaAB, ELN(1, el)), N1(m->etaAB, ELN(2, el))),
+                            MAXD(N1(m->etaAB, ELN(3, el)), N1(m->etaAB, ELN(4, el))));
+        N1(m->mask_wd, el) = (dmin4 + emax4 > m->p.Dmin) ? 1.0 : 0.0;
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        N1(m->mask_wd_node, n) = (N1(m->depth, n) + N1(m->etaAB, n) > m->p.Dmin) ? 1.0 : 0.0;
+}
+
+/* adv_tracer_mask, fv_main.F90:1309-1335 (H_advtr_crit=0.1, H_advtr_min=0, fv_var.F90:49,51) */
+static void adv_tracer_mask(oracle_model *m) {
+    const double crit = 0.1, hmin = 0.0;
+    for (int n = 1; n <= m->N; ++n) {
+        double dmean = MAXD(m->p.Dmin, N1(m->depth, n) + N1(m->eta_n, n));
+        if (dmean > crit) N1(m->mask_ad, n) = 1.0;
+        else if (dmean < hmin) N1(m->mask_ad, n) = 0.0;
+        else N1(m->mask_ad, n) = (dmean - hmin) / (crit - hmin);
+    }
+}
+
+/* ====================================================================== */
+/* vel_gradients_2D, fv_gradients.F90:97-176 (free_slip = .true.)          */
+/* ====================================================================== */
+static void vel_gradients_2D(oracle_model *m, const double *Uin) {
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        double g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0;
+        for (int j = 1; j <= jend; ++j) {
+            int el2 = ELNB(j, el);
+            if (el2 > 0) {
+                g1 = g1 + GV(j, el) * (V2(Uin, 1, el2) - V2(Uin, 1, el));
+                g2 = g2 + GV(j + 4, el) * (V2(Uin, 1, el2) - V2(Uin, 1, el));
+                g3 = g3 + GV(j, el) * (V2(Uin, 2, el2) - V2(Uin, 2, el));
+                g4 = g4 + GV(j + 4, el) * (V2(Uin, 2, el2) - V2(Uin, 2, el));
+            } else {
+                double zc1 = EDXY(1, ELE(j, el)) * N1(m->elem_cos, el);
+                double zc2 = EDXY(2, ELE(j, el));
+                double un = -2.0 * (V2(Uin, 1, el) * zc2 - V2(Uin, 2, el) * zc1) / (zc1 * zc1 + zc2 * zc2);
+                g1 = g1 + GV(j, el) * un * zc2;
+                g2 = g2 + GV(j + 4, el) * un * zc2;
+                g3 = g3 - GV(j, el) * un * zc1;
+                g4 = g4 - GV(j + 4, el) * un * zc1;
+            }
+        }
+        m->vel_grad[4 * (el - 1) + 0] = g1;  /* vel_grad is (4,E) */
+        m->vel_grad[4 * (el - 1) + 1] = g2;
+        m->vel_grad[4 * (el - 1) + 2] = g3;
+        m->vel_grad[4 * (el - 1) + 3] = g4;
+    }
+}
+#define VG(k, e) (m->vel_grad[4 * ((e)-1) + (k)-1])
+
+/* ====================================================================== */
+/* compute_ssh_rhs_elem, fv_average_dynamic.F90:1-226 (no ice)              */
+/* ====================================================================== */
+static void compute_ssh_rhs_elem(oracle_model *m) {
+    double *c1 = m->c1e, *aux_elem = m->aux_elem;
+    for (int i = 1; i <= m->Ed; ++i) N1(c1, i) = 0.0;
+    for (int n = 1; n <= m->N; ++n) N1(m->ssh_rhs, n) = 0.0;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double ad[4];
+        for (int i = 1; i <= 4; ++i) {
+            ad[i - 1] = m->p.Dmin;
+            double ttldep = N1(m->etaAB, ELN(i, el)) + N1(m->depth, ELN(i, el));
+            if (ttldep > m->p.Dmin) ad[i - 1] = ttldep;
+        }
+        N1(aux_elem, el) = WCV(1, el) * ad[0] + WCV(2, el) * ad[1] + WCV(3, el) * ad[2] + WCV(4, el) * ad[3];
+    }
+#pragma omp parallel for
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        N1(c1, ed) = (V2(m->UAB, 2, e1) * ECR(1, ed) - V2(m->UAB, 1, e1) * ECR(2, ed)) * N1(aux_elem, e1)
+                   + (-V2(m->UAB, 2, e2) * ECR(3, ed) + V2(m->UAB, 1, e2) * ECR(4, ed)) * N1(aux_elem, e2);
+    }
+#pragma omp parallel for
+    for (int ed = 1 + m->Ed_in; ed <= m->Ed; ++ed) {
+        int e1 = EDT(1, ed);
+        N1(c1, ed) = (V2(m->UAB, 2, e1) * ECR(1, ed) - V2(m->UAB, 1, e1) * ECR(2, ed)) * N1(aux_elem, e1);
+    }
+    for (int ed = 1; ed <= m->Ed; ++ed) {
+        N1(m->ssh_rhs, EDN(1, ed)) = N1(m->ssh_rhs, EDN(1, ed)) + N1(c1, ed);
+        N1(m->ssh_rhs, EDN(2, ed)) = N1(m->ssh_rhs, EDN(2, ed)) - N1(c1, ed);
+    }
+    if (m->p.key_rivers)
+        for (int n = 1; n <= m->n_rivers; ++n)
+            N1(m->ssh_rhs, m->nod_rivers[n - 1]) = N1(m->ssh_rhs, m->nod_rivers[n - 1]) + N1(m->runoff, n);
+    if (m->p.TF_presence && m->nobn > 0) {
+        for (int i = 1; i <= m->nobn; ++i) N1(m->ssh_rhs, m->in_obn[i - 1]) = 0.0;
+        for (int i = 1; i <= m->nobn; ++i) {
+            int n = m->in_obn[i - 1], q = i;
+            for (int j = 1; j <= 12; ++j)
+                N1(m->ssh_rhs, n) = N1(m->ssh_rhs, n) + m->amp_factor[j - 1] * AMPT(q, j)
+                    * cos((m->time_2D - m->p.time_jd0 * 86400.0) * 2.0 * WP_PI / (HARM_PERIOD[j - 1] * 3600.0)
+                          - (FAZT(q, j) + m->phy_factor[j - 1]));
+            if (!m->p.restart)
+                if (m->time_jd - m->p.time_jd0 < 10.0)
+                    N1(m->ssh_rhs, n) = N1(m->ssh_rhs, n) * (m->time_jd - m->p.time_jd0) / 10.0;
+        }
+    }
+}
+
+/* momentum_adv_upwind_2D, fv_advection.F90:546-669 */
+static void momentum_adv_upwind_2D(oracle_model *m) {
+    double *uu = m->s_ed1, *vv = m->s_ed2;
+    for (int ed = 1; ed <= m->Ed; ++ed) { N1(uu, ed) = 0.0; N1(vv, ed) = 0.0; }
+#pragma omp parallel for
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int n1 = EDN(1, ed), n2 = EDN(2, ed);
+        double dmean = MAXD(m->p.Dmin, 0.5 * ((N1(m->etaAB, n1) + N1(m->depth, n1)) + (N1(m->etaAB, n2) + N1(m->depth, n2))));
+        double acc = (N1(m->ac, n1) + N1(m->ac, n2)) * 0.5;
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double u1 = V2(m->UAB, 1, e1) - VG(1, e1) * ECR(1, ed) - VG(2, e1) * ECR(2, ed);
+        double v1 = V2(m->UAB, 2, e1) - VG(3, e1) * ECR(1, ed) - VG(4, e1) * ECR(2, ed);
+        double u2 = V2(m->UAB, 1, e2) - VG(1, e2) * ECR(3, ed) - VG(2, e2) * ECR(4, ed);
+        double v2 = V2(m->UAB, 2, e2) - VG(3, e2) * ECR(3, ed) - VG(4, e2) * ECR(4, ed);
+        double un = 0.5 * WP_R_EARTH * dmean *
+                    ((u1 + u2) * EDXY(2, ed) - (v1 * N1(m->elem_cos, e1) + v2 * N1(m->elem_cos, e2)) * EDXY(1, ed));
+        u1 = V2(m->UAB, 1, e1); v1 = V2(m->UAB, 2, e1);
+        u2 = V2(m->UAB, 1, e2); v2 = V2(m->UAB, 2, e2);
+        if (un >= 0.0) { N1(uu, ed) = un * u1 * acc; N1(vv, ed) = un * v1 * acc; }
+        else { N1(uu, ed) = un * u2 * acc; N1(vv, ed) = un * v2 * acc; }
+    }
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        V2(m->U_rhs_2D, 1, e1) = V2(m->U_rhs_2D, 1, e1) - N1(uu, ed);
+        V2(m->U_rhs_2D, 2, e1) = V2(m->U_rhs_2D, 2, e1) - N1(vv, ed);
+        V2(m->U_rhs_2D, 1, e2) = V2(m->U_rhs_2D, 1, e2) + N1(uu, ed);
+        V2(m->U_rhs_2D, 2, e2) = V2(m->U_rhs_2D, 2, e2) + N1(vv, ed);
+    }
+}
+
+/* viscosity_filt_2D, fv_viscosity.F90:769-813 */
+static void viscosity_filt_2D(oracle_model *m) {
+    double tau_inv = m->p.tau_inv_filt;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        double u1 = 0.0, u2 = 0.0;
+        for (int j = 1; j <= jend; ++j) {
+            int ne = ELNB(j, el);
+            if (ne > 0) {
+                u1 = u1 + V2(m->UAB, 1, ne) - V2(m->UAB, 1, el);
+                u2 = u2 + V2(m->UAB, 2, ne) - V2(m->UAB, 2, el);
+            }
+        }
+        double sd = 0.0;
+        for (int k = 1; k <= 4; ++k) sd = sd + WCV(k, el) * N1(m->depth, ELN(k, el));
+        V2(m->U_rhs_2D, 1, el) = V2(m->U_rhs_2D, 1, el) + tau_inv * u1 * N1(m->elem_area, el) * sd;
+        V2(m->U_rhs_2D, 2, el) = V2(m->U_rhs_2D, 2, el) + tau_inv * u2 * N1(m->elem_area, el) * sd;
+    }
+}
+
+/* sum(w_cv(1:4,el)*(x(nodes)+y(nodes))) with the Fortran SUM order */
+static inline double wsum2(const oracle_model *m, int el, const double *x, const double *y) {
+    double s = 0.0;
+    for (int k = 1; k <= 4; ++k) s = s + WCV(k, el) * (N1(x, ELN(k, el)) + N1(y, ELN(k, el)));
+    return s;
+}
+/* explicit 4-term form  w1*(x1+y1) + w2*(x2+y2) + ... */
+static inline double wsum2e(const oracle_model *m, int el, const double *x, const double *y) {
+    return WCV(1, el) * (N1(x, ELN(1, el)) + N1(y, ELN(1, el))) + WCV(2, el) * (N1(x, ELN(2, el)) + N1(y, ELN(2, el)))
+         + WCV(3, el) * (N1(x, ELN(3, el)) + N1(y, ELN(3, el))) + WCV(4, el) * (N1(x, ELN(4, el)) + N1(y, ELN(4, el)));
+}
+
+/* update_2D_vel, fv_average_dynamic.F90:228-443 (type_task 3, key_atm off) */
+static void update_2D_vel(oracle_model *m, int step) {
+    (void)step;
+    const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
+    double *eta = m->eta_tmp;
+    vel_gradients_2D(m, m->UAB);
+    for (int el = 1; el <= m->E; ++el) N1(m->C_d_el, el) = m->p.C_d;
+    double density0_inv = 1.0 / m->p.density_0;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        N1(m->eta_n_2, n) = de * N1(m->ssh_rhs, n) + fe * N1(m->eta_n, n) + ga * N1(m->eta_n_1, n) + ep * N1(m->eta_n_2, n);
+        N1(m->etaAB, n) = N1(m->eta_n_2, n);
+        N1(eta, n) = WP_G * (ATP(n, 1) * N1(m->eta_n_2, n) - ATP(n, 2) * N1(m->ssh_gp, n));
+    }
+    if (m->p.wet_dry_on) wad_mask(m);
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double dmean = MAXD(m->p.Dmin, wsum2e(m, el, m->etaAB, m->depth));
+        int n1 = ELN(1, el), n2 = ELN(2, el), n3 = ELN(3, el), n4 = ELN(4, el);
+        V2(m->U_rhs_2D, 1, el) = N1(m->elem_area, el) *
+            (-dmean * (GS(1, el) * N1(eta, n1) + GS(2, el) * N1(eta, n2) + GS(3, el) * N1(eta, n3) + GS(4, el) * N1(eta, n4))
+             + V2(m->UAB, 2, el) * dmean * N1(m->coriolis, el) + N1(m->taux, el) * density0_inv);
+        V2(m->U_rhs_2D, 2, el) = N1(m->elem_area, el) *
+            (-dmean * (GS(5, el) * N1(eta, n1) + GS(6, el) * N1(eta, n2) + GS(7, el) * N1(eta, n3) + GS(8, el) * N1(eta, n4))
+             - V2(m->UAB, 1, el) * dmean * N1(m->coriolis, el) + N1(m->tauy, el) * density0_inv);
+    }
+    if (m->p.mom_adv_2D == 2) momentum_adv_upwind_2D(m);
+    if (m->p.filt_2D) viscosity_filt_2D(m);
+    for (int el = 1; el <= m->E; ++el) {
+        V2(m->U_rhs_2D, 1, el) = V2(m->U_rhs_2D, 1, el) + V2(m->U_rhs_2D_3D, 1, el);
+        V2(m->U_rhs_2D, 2, el) = V2(m->U_rhs_2D, 2, el) + V2(m->U_rhs_2D_3D, 2, el);
+    }
+    const int L = m->L;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double dmean = MAXD(m->p.Dmin, wsum2(m, el, m->eta_n, m->depth));
+        double sac = 0.0;
+        for (int k = 1; k <= 4; ++k) sac = sac + WCV(k, el) * N1(m->ac, ELN(k, el));
+        double a_Cd = N1(m->C_d_el, el) * ((1.0 - sac) * m->p.Cd_bz + 1.0);
+        double ub = F3(m->U_n, L, el), vb = F3(m->V_n, L, el);
+        double friction = a_Cd * sqrt(ub * ub + vb * vb);
+        double ff = 1.0 / (MAXD(m->p.Dmin, wsum2(m, el, m->ssh_rhs, m->depth)) + friction * m->p.dt_2D);
+        double dt2 = m->p.dt_2D;
+        V2(m->U_rhs_2D, 1, el) = N1(m->mask_wd, el) * ((dmean * V2(m->U_n_2D, 1, el) -
+            dt2 * friction * (ub - V2(m->U_n_2D, 1, el)) + dt2 * V2(m->Bar_pr_2D, 1, el) +
+            dt2 * V2(m->U_rhs_2D, 1, el) / N1(m->elem_area, el)) * ff + 0.0);
+        V2(m->U_rhs_2D, 2, el) = N1(m->mask_wd, el) * ((dmean * V2(m->U_n_2D, 2, el) -
+            dt2 * friction * (vb - V2(m->U_n_2D, 2, el)) + dt2 * V2(m->Bar_pr_2D, 2, el) +
+            dt2 * V2(m->U_rhs_2D, 2, el) / N1(m->elem_area, el)) * ff + 0.0);
+    }
+}
+
+/* compute_puls_vel, fv_3D_vel.F90:257-307 */
+static void compute_puls_vel(oracle_model *m) {
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double a = N1(m->dmean_n, el) / MAXD(m->p.Dmin, wsum2(m, el, m->ssh_rhs, m->depth));
+        for (int k = 1; k <= m->L; ++k) {
+            F3(m->U_puls, k, el) = F3(m->U_n, k, el) - a * V2(m->U_n_2D, 1, el);
+            F3(m->V_puls, k, el) = F3(m->V_n, k, el) - a * V2(m->U_n_2D, 2, el);
+        }
+    }
+}
+
+/* compute_el2nodes_3D, fv_utilit.F90:644-700 */
+static void compute_el2nodes_3D(oracle_model *m, const double *Ue, const double *Ve, double *Un, double *Vn) {
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        int num = NIEN(n);
+        double s = 0.0;
+        for (int k = 1; k <= num; ++k) s = s + N1(m->elem_area, NIE(k, n));
+        double tvol_inv = 1.0 / s;
+        for (int z = 1; z <= m->L; ++z) { F3(Un, z, n) = 0.0; F3(Vn, z, n) = 0.0; }
+        for (int k = 1; k <= num; ++k) {
+            int el = NIE(k, n);
+            for (int z = 1; z <= m->L; ++z) {
+                F3(Un, z, n) = F3(Un, z, n) + F3(Ue, z, el) * N1(m->elem_area, el);
+                F3(Vn, z, n) = F3(Vn, z, n) + F3(Ve, z, el) * N1(m->elem_area, el);
+            }
+        }
+        for (int z = 1; z <= m->L; ++z) {
+            F3(Un, z, n) = F3(Un, z, n) * tvol_inv;
+            F3(Vn, z, n) = F3(Vn, z, n) * tvol_inv;
+        }
+    }
+}
+
+/* momentum_adv_P1_3D_to_2D, fv_advection.F90:676-793 */
+static void momentum_adv_P1_3D_to_2D(oracle_model *m) {
+    double *ue1 = m->s_ed1, *ue2 = m->s_ed2, *ve1 = m->s_ed3, *ve2 = m->s_ed4;
+    for (int ed = 1; ed <= m->Ed; ++ed) { N1(ue1, ed) = 0; N1(ue2, ed) = 0; N1(ve1, ed) = 0; N1(ve2, ed) = 0; }
+#pragma omp parallel for
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int n1 = EDN(1, ed), n2 = EDN(2, ed), e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double acc = (N1(m->ac, n1) + N1(m->ac, n2)) * .5;
+        double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+        for (int z = 1; z <= m->L; ++z) {
+            double uu = 0.5 * (F3(m->Unode_p, z, n1) + F3(m->Unode_p, z, n2));
+            double vv = 0.5 * (F3(m->Vnode_p, z, n1) + F3(m->Vnode_p, z, n2));
+            double un = (uu * ye - vv * xe) * F3(m->Jd, z, ed);
+            s1 = s1 + uu * un * F3(m->Je, z, e1);
+            s2 = s2 + vv * un * F3(m->Je, z, e1);
+            s3 = s3 + uu * un * F3(m->Je, z, e2);
+            s4 = s4 + vv * un * F3(m->Je, z, e2);
+        }
+        N1(ue1, ed) = acc * s1; N1(ve1, ed) = acc * s2;
+        N1(ue2, ed) = acc * s3; N1(ve2, ed) = acc * s4;
+    }
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        V2(m->U_rhs_2D_3D, 1, e1) = V2(m->U_rhs_2D_3D, 1, e1) - N1(ue1, ed);
+        V2(m->U_rhs_2D_3D, 2, e1) = V2(m->U_rhs_2D_3D, 2, e1) - N1(ve1, ed);
+        V2(m->U_rhs_2D_3D, 1, e2) = V2(m->U_rhs_2D_3D, 1, e2) + N1(ue2, ed);
+        V2(m->U_rhs_2D_3D, 2, e2) = V2(m->U_rhs_2D_3D, 2, e2) + N1(ve2, ed);
+    }
+}
+
+/* viscosity_filt_3D_to_2D, fv_viscosity.F90:870-939 */
+static void viscosity_filt_3D_to_2D(oracle_model *m) {
+    double tau_inv = m->p.tau_inv_filt;
+    double *Uf = m->U_rhs, *Vf = m->V_rhs; /* scratch (L,E); overwritten later by compute_vel_rhs anyway? no: use dedicated */
+    Uf = m->s_gr; Vf = m->s_gr + (size_t)m->L * m->E;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        for (int z = 1; z <= m->L; ++z) {
+            double u1 = 0.0, v1 = 0.0;
+            for (int j = 1; j <= jend; ++j) {
+                int ne = ELNB(j, el);
+                if (ne > 0) {
+                    u1 = u1 + F3(m->U_puls, z, ne) * F3(m->Je, z, ne) - F3(m->U_puls, z, el) * F3(m->Je, z, el);
+                    v1 = v1 + F3(m->V_puls, z, ne) * F3(m->Je, z, ne) - F3(m->V_puls, z, el) * F3(m->Je, z, el);
+                }
+            }
+            F3(Uf, z, el) = tau_inv * u1 * N1(m->elem_area, el);
+            F3(Vf, z, el) = tau_inv * v1 * N1(m->elem_area, el);
+        }
+    }
+    for (int el = 1; el <= m->E; ++el)
+        for (int z = 1; z <= m->L; ++z) {
+            V2(m->U_rhs_2D_3D, 1, el) = V2(m->U_rhs_2D_3D, 1, el) + F3(Uf, z, el) * F3(m->Je, z, el);
+            V2(m->U_rhs_2D_3D, 2, el) = V2(m->U_rhs_2D_3D, 2, el) + F3(Vf, z, el) * F3(m->Je, z, el);
+        }
+}
+
+/* timestep_AB_2D, fv_main.F90:1372-1634 */
+static void timestep_AB_2D(oracle_model *m, int step) {
+    const double beta = m->p.beta;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        N1(m->etaAB, n) = (1.5 + beta) * N1(m->eta_n, n) - (0.5 + 2.0 * beta) * N1(m->eta_n_1, n) + beta * N1(m->eta_n_2, n);
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        V2(m->UAB, 1, el) = (1.5 + beta) * V2(m->U_n_2D, 1, el) - (0.5 + 2.0 * beta) * V2(m->U_n_1, 1, el) + beta * V2(m->U_n_2, 1, el);
+        V2(m->UAB, 2, el) = (1.5 + beta) * V2(m->U_n_2D, 2, el) - (0.5 + 2.0 * beta) * V2(m->U_n_1, 2, el) + beta * V2(m->U_n_2, 2, el);
+    }
+    compute_ssh_rhs_elem(m);
+#pragma omp parallel for
+    for (int i = 1; i <= m->N; ++i)
+        if (N1(m->index_nod2D, i) < 2)
+            N1(m->ssh_rhs, i) = N1(m->eta_n, i) + m->p.dt_2D * N1(m->ssh_rhs, i) / N1(m->area, i);
+    if (step == 1) {
+        for (int el = 1; el <= m->E; ++el) { V2(m->U_rhs_2D_3D, 1, el) = 0.0; V2(m->U_rhs_2D_3D, 2, el) = 0.0; }
+#pragma omp parallel for
+        for (int el = 1; el <= m->E; ++el)
+            N1(m->dmean_n, el) = MAXD(m->p.Dmin, wsum2e(m, el, m->eta_n, m->depth));
+        for (int i = 1; i <= m->N; ++i) N1(m->eta_p, i) = N1(m->eta_n, i);
+        compute_puls_vel(m);
+        compute_el2nodes_3D(m, m->U_puls, m->V_puls, m->Unode_p, m->Vnode_p);
+        momentum_adv_P1_3D_to_2D(m);
+        if (m->p.filt_3D) viscosity_filt_3D_to_2D(m);
+        for (int el = 1; el <= m->E; ++el) {
+            V2(m->U_rhs_2D_3D, 1, el) = V2(m->U_rhs_2D_3D, 1, el) / N1(m->dmean_n, el);
+            V2(m->U_rhs_2D_3D, 2, el) = V2(m->U_rhs_2D_3D, 2, el) / N1(m->dmean_n, el);
+        }
+    }
+    update_2D_vel(m, step);
+    for (int n = 1; n <= m->N; ++n) {
+        N1(m->eta_n_2, n) = N1(m->eta_n_1, n);
+        N1(m->eta_n_1, n) = N1(m->eta_n, n);
+        N1(m->eta_n, n) = N1(m->ssh_rhs, n);
+    }
+    for (int el = 1; el <= m->E; ++el)
+        for (int k = 1; k <= 2; ++k) {
+            V2(m->U_n_2, k, el) = V2(m->U_n_1, k, el);
+            V2(m->U_n_1, k, el) = V2(m->U_n_2D, k, el);
+            V2(m->U_n_2D, k, el) = V2(m->U_rhs_2D, k, el);
+        }
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double dmean = MAXD(m->p.Dmin, wsum2e(m, el, m->eta_n, m->depth));
+        N1(m->U_filt_2D, el) = N1(m->U_filt_2D, el) + V2(m->U_rhs_2D, 1, el) * dmean;
+        N1(m->V_filt_2D, el) = N1(m->V_filt_2D, el) + V2(m->U_rhs_2D, 2, el) * dmean;
+    }
+}
+
+/* oce_barotropic_timestep, fv_main.F90:1636-1703 */
+static void oce_barotropic_timestep(oracle_model *m) {
+    for (int el = 1; el <= m->E; ++el) { N1(m->U_filt_2D, el) = 0.0; N1(m->V_filt_2D, el) = 0.0; }
+    for (int n = 1; n <= m->p.Mt; ++n) {
+        m->time_2D = m->time + m->p.dt_2D * n;
+        timestep_AB_2D(m, n);
+    }
+    double Mt_inv = 1.0 / (double)m->p.Mt;
+    for (int el = 1; el <= m->E; ++el) {
+        N1(m->U_filt_2D, el) = N1(m->U_filt_2D, el) * Mt_inv;
+        N1(m->V_filt_2D, el) = N1(m->V_filt_2D, el) * Mt_inv;
+    }
+}
+
+/* ====================================================================== */
+/* pressure + baroclinic_pressure_gradient_3D, fv_pressure_new.F90:7-221    */
+/* (mixed_BP_grad_OB = .false., comp_sediment = .false.)                    */
+/* ====================================================================== */
+static void pressure(oracle_model *m) {
+    const int L = m->L;
+    double g_density0_inv = WP_G / m->p.density_0;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        W3(m->hpressure, 1, n) = 0.0;
+        for (int z = 1; z <= L; ++z) {
+            F3(m->rho_c, z, n) = densityJM(F3(m->TF, z, n), F3(m->SF, z, n), -F3(m->Z, z, n), m->p.density_0);
+            W3(m->hpressure, z + 1, n) = W3(m->hpressure, z, n) + F3(m->rho_c, z, n) * F3(m->Jc, z, n) * g_density0_inv;
+        }
+    }
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double Ax = 0, Ay = 0, Bx = 0, By = 0, acc = 0;
+        for (int k = 1; k <= 4; ++k) Ax = Ax + GS(k, el) * (N1(m->depth, ELN(k, el)) + N1(m->eta_n, ELN(k, el)));
+        for (int k = 1; k <= 4; ++k) Ay = Ay + GS(k + 4, el) * (N1(m->depth, ELN(k, el)) + N1(m->eta_n, ELN(k, el)));
+        for (int k = 1; k <= 4; ++k) Bx = Bx + GS(k, el) * N1(m->depth, ELN(k, el));
+        for (int k = 1; k <= 4; ++k) By = By + GS(k + 4, el) * N1(m->depth, ELN(k, el));
+        for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+        double acc_to_Bp_bz = pow(acc, m->p.Bp_bz) * N1(m->mask_bpr, el);
+        for (int z = 1; z <= L; ++z) {
+            double accJe_inv = -acc_to_Bp_bz / F3(m->Je, z, el);
+            double qd_up = 0, qd_low = 0, pre[4];
+            for (int k = 1; k <= 4; ++k) qd_up = qd_up + WCV(k, el) * W3(m->hpressure, z, ELN(k, el));
+            for (int k = 1; k <= 4; ++k) qd_low = qd_low + WCV(k, el) * W3(m->hpressure, z + 1, ELN(k, el));
+            for (int k = 1; k <= 4; ++k) {
+                int nk = ELN(k, el);
+                pre[k - 1] = 0.5 * (W3(m->hpressure, z, nk) + W3(m->hpressure, z + 1, nk)) * F3(m->Jc, z, nk);
+            }
+            double sx = 0, sy = 0;
+            for (int k = 1; k <= 4; ++k) sx = sx + GS(k, el) * pre[k - 1];
+            for (int k = 1; k <= 4; ++k) sy = sy + GS(k + 4, el) * pre[k - 1];
+            F3(m->Bar_pru_3D, z, el) = accJe_inv * (sx + qd_low * (SIG(z + 1) * Ax - Bx) - qd_up * (SIG(z) * Ax - Bx));
+            F3(m->Bar_prv_3D, z, el) = accJe_inv * (sy + qd_low * (SIG(z + 1) * Ay - By) - qd_up * (SIG(z) * Ay - By));
+        }
+        double b1 = 0, b2 = 0;
+        for (int z = 1; z <= L; ++z) b1 = b1 + F3(m->Bar_pru_3D, z, el) * F3(m->Je, z, el);
+        for (int z = 1; z <= L; ++z) b2 = b2 + F3(m->Bar_prv_3D, z, el) * F3(m->Je, z, el);
+        V2(m->Bar_pr_2D, 1, el) = b1;
+        V2(m->Bar_pr_2D, 2, el) = b2;
+    }
+}
+
+/* ====================================================================== */
+/* d3_end, fv_mixing.F90:73-347                                             */
+/* ====================================================================== */
+static void d3_end(oracle_model *m) {
+    const int NS = m->NS;
+    const double t_inv = 1.0 / m->p.dt;
+    const double cka = m->p.cka;
+    const double B1cka2 = 16.6 * (cka * cka);
+    int notconv = 0;
+    for (size_t i = 0; i < (size_t)NS * m->N; ++i) m->Ri[i] = 0.0;
+#pragma omp parallel for reduction(+ : notconv)
+    for (int node = 1; node <= m->N; ++node) {
+        double xx1[NS + 2], yy1[NS + 2], btr[NS + 2], btr1[NS + 2], b1[NS + 2], b2[NS + 2], c2[NS + 2];
+        for (int i = 0; i < NS + 2; ++i) { xx1[i] = yy1[i] = btr[i] = btr1[i] = b1[i] = b2[i] = c2[i] = 0.0; }
+        double dmean = MAXD(m->p.Dmin, N1(m->depth, node) + N1(m->eta_n, node));
+        double dmean2 = dmean * dmean;
+        for (int nz = 1; nz <= NS; ++nz) btr[nz] = W3(m->bt, nz, node);
+        for (int nz = 2; nz <= NS - 1; ++nz) {
+            double d1 = SIG(nz - 1) - SIG(nz);
+            double d2 = SIG(nz) - SIG(nz + 1);
+            double d = 0.5 * (d1 + d2);
+            double ap1 = F3(m->Unode, nz - 1, node) - F3(m->Unode, nz, node);
+            double ap2 = F3(m->Vnode, nz - 1, node) - F3(m->Vnode, nz, node);
+            b1[nz] = W3(m->snu, nz, node) * (ap1 * ap1 + ap2 * ap2) / (d * d);
+            b1[nz] = b1[nz] / dmean2;
+            double rho_up = densityJM(F3(m->TF, nz - 1, node), F3(m->SF, nz - 1, node), -W3(m->zbar, nz, node), m->p.density_0);
+            double rho_dn = densityJM(F3(m->TF, nz, node), F3(m->SF, nz, node), -W3(m->zbar, nz, node), m->p.density_0);
+            ap1 = (rho_up - rho_dn) / d;
+            b2[nz] = -0.5 * WP_G * W3(m->Kv, nz, node) * ap1 / (m->p.density_0 * dmean);
+            double snu_p = 0.5 * (W3(m->snu, nz - 1, node) + W3(m->snu, nz, node));
+            double snu_m = 0.5 * (W3(m->snu, nz, node) + W3(m->snu, nz + 1, node));
+            c2[nz] = 0.5 * 0.73 * (snu_p * (W3(m->bt, nz - 1, node) - W3(m->bt, nz, node)) / d1 -
+                                   snu_m * (W3(m->bt, nz, node) - W3(m->bt, nz + 1, node)) / d2) / d;
+            c2[nz] = c2[nz] / dmean2;
+            if (b1[nz] > 0.0) W3(m->Ri, nz, node) = -WP_G * ap1 / (m->p.density_0 * dmean) / b1[nz] * W3(m->snu, nz, node);
+            else W3(m->Ri, nz, node) = 10000.0;
+        }
+        xx1[2] = 1.0;
+        yy1[2] = 0.0;
+        double d1 = 0.5 * (SIG(NS - 1) - SIG(NS));
+        double wx = N1(m->windx, node), wy = N1(m->windy, node);
+        double u_din_sur = 0.05 * (wx * wx + wy * wy);
+        double snu_m = 0.5 * (W3(m->snu, NS, node) + W3(m->snu, NS - 1, node));
+        yy1[2] = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
+        int converged = 0;
+        for (int it = 1; it <= 200; ++it) {
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                double dd1 = SIG(nz - 1) - SIG(nz);
+                double dd2 = SIG(nz) - SIG(nz + 1);
+                double d = 0.5 * (dd1 + dd2);
+                double c1 = 0.046 * (btr[nz] * btr[nz]) / W3(m->snu, nz, node);
+                W3(m->tke_dissip, nz, node) = c1;
+                double fr = -b1[nz] - b2[nz] - c1 - t_inv * W3(m->bt, nz, node) - c2[nz];
+                double snu_p = 0.5 * (W3(m->snu, nz - 1, node) + W3(m->snu, nz, node));
+                double snu_mm = 0.5 * (W3(m->snu, nz, node) + W3(m->snu, nz + 1, node));
+                double am = 0.5 * (snu_p * 0.73) / (dmean2 * dd1 * d);
+                double cm = 0.5 * (snu_mm * 0.73) / (dmean2 * dd2 * d);
+                double bm = am + cm + (2.0 * 0.046 * btr[nz]) / W3(m->snu, nz, node) + t_inv;
+                double a = bm - am * xx1[nz];
+                xx1[nz + 1] = cm / a;
+                yy1[nz + 1] = (am * yy1[nz] - fr) / a;
+            }
+            double delta_b = F3(m->Jc, NS - 1, node) + m->p.z0b_min;
+            double lg = log(delta_b / m->p.z0b_min);
+            double bott_R = B1cka2 / (lg * lg);
+            double ub = F3(m->Unode, NS - 1, node), vb = F3(m->Vnode, NS - 1, node);
+            btr1[NS] = bott_R * (ub * ub + vb * vb);
+            for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
+            double bbb_max = 0.0;
+            for (int nz = 1; nz <= NS; ++nz) {
+                double a = btr[nz] - btr1[nz];
+                double b = MAXD(btr1[nz], btr[nz]) + 1.0e-8;
+                double c = fabs(a / b);
+                if (c > bbb_max) bbb_max = c;
+            }
+            if (bbb_max < 1.0e-6) { converged = 1; break; }
+            for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
+        }
+        if (!converged) notconv += 1;
+        for (int nz = 1; nz <= NS; ++nz) {
+            W3(m->bt, nz, node) = MAXD(btr[nz], 1.0e-8);
+            double zt = SIG(nz) * dmean;
+            double Zh = zt + m->p.z0b_min;
+            double Zd = fabs(dmean - zt) + m->p.z0s_min;
+            double Z0 = 1.0 - m->p.beta_scale * Zh * Zd / (dmean * dmean);
+            double scale_t = cka * Zh * Zd * Z0 / dmean;
+            W3(m->snu, nz, node) = scale_t * sqrt(W3(m->bt, nz, node)) + m->p.snul;
+            if (W3(m->snu, nz, node) >= 0.2) W3(m->snu, nz, node) = 0.2;
+            W3(m->Kv, nz, node) = m->p.Pr_num * W3(m->snu, nz, node);
+        }
+    }
+    m->notconv = notconv;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el)
+        for (int nz = 1; nz <= NS; ++nz) {
+            double s = 0.0;
+            for (int k = 1; k <= 4; ++k) s = s + WCV(k, el) * W3(m->snu, nz, ELN(k, el));
+            W3(m->Av, nz, el) = s;
+        }
+}
+
+/* ====================================================================== */
+/* compute_vel_rhs and its callees, fv_3D_vel.F90:1-197                    */
+/* ====================================================================== */
+/* vel_gradients, fv_gradients.F90:2-93 */
+static void vel_gradients(oracle_model *m) {
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        for (int z = 1; z <= m->L; ++z) {
+            F3(m->vgux, z, el) = 0.0; F3(m->vguy, z, el) = 0.0;
+            F3(m->vgvx, z, el) = 0.0; F3(m->vgvy, z, el) = 0.0;
+        }
+        for (int j = 1; j <= jend; ++j) {
+            int el2 = ELNB(j, el);
+            if (el2 > 0) {
+                for (int z = 1; z <= m->L; ++z) {
+                    F3(m->vgux, z, el) = F3(m->vgux, z, el) + GV(j, el) * (F3(m->U_n, z, el2) - F3(m->U_n, z, el));
+                    F3(m->vguy, z, el) = F3(m->vguy, z, el) + GV(j + 4, el) * (F3(m->U_n, z, el2) - F3(m->U_n, z, el));
+                    F3(m->vgvx, z, el) = F3(m->vgvx, z, el) + GV(j, el) * (F3(m->V_n, z, el2) - F3(m->V_n, z, el));
+                    F3(m->vgvy, z, el) = F3(m->vgvy, z, el) + GV(j + 4, el) * (F3(m->V_n, z, el2) - F3(m->V_n, z, el));
+                }
+            } else {
+                double zc1 = EDXY(1, ELE(j, el)), zc2 = EDXY(2, ELE(j, el));
+                zc1 = zc1 * N1(m->elem_cos, el);
+                for (int z = 1; z <= m->L; ++z) {
+                    double un = -2.0 * (F3(m->U_n, z, el) * zc2 - F3(m->V_n, z, el) * zc1) / (zc1 * zc1 + zc2 * zc2);
+                    F3(m->vgux, z, el) = F3(m->vgux, z, el) + GV(j, el) * un * zc2;
+                    F3(m->vguy, z, el) = F3(m->vguy, z, el) + GV(j + 4, el) * un * zc2;
+                    F3(m->vgvx, z, el) = F3(m->vgvx, z, el) - GV(j, el) * un * zc1;
+                    F3(m->vgvy, z, el) = F3(m->vgvy, z, el) - GV(j + 4, el) * un * zc1;
+                }
+            }
+        }
+    }
+}
+
+/* momentum_adv_upwind, fv_advection.F90:64-197 */
+static void momentum_adv_upwind(oracle_model *m) {
+    const int L = m->L;
+    double *uu = m->s_gr, *vv = m->s_gr + (size_t)L * m->Ed;
+#pragma omp parallel for
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double acc = 0.5 * (N1(m->ac, EDN(1, ed)) + N1(m->ac, EDN(2, ed)));
+        for (int z = 1; z <= L; ++z) {
+            double u1 = F3(m->U_n, z, e1) - F3(m->vgux, z, e1) * ECR(1, ed) - F3(m->vguy, z, e1) * ECR(2, ed);
+            double v1 = F3(m->V_n, z, e1) - F3(m->vgvx, z, e1) * ECR(1, ed) - F3(m->vgvy, z, e1) * ECR(2, ed);
+            double u2 = F3(m->U_n, z, e2) - F3(m->vgux, z, e2) * ECR(3, ed) - F3(m->vguy, z, e2) * ECR(4, ed);
+            double v2 = F3(m->V_n, z, e2) - F3(m->vgvx, z, e2) * ECR(3, ed) - F3(m->vgvy, z, e2) * ECR(4, ed);
+            double un = 0.5 * WP_R_EARTH * F3(m->Jd, z, ed) *
+                        ((u1 + u2) * EDXY(2, ed) - (v1 * N1(m->elem_cos, e1) + v2 * N1(m->elem_cos, e2)) * EDXY(1, ed));
+            if (un >= 0.0) { F3(uu, z, ed) = u1 * un * acc; F3(vv, z, ed) = v1 * un * acc; }
+            else { F3(uu, z, ed) = u2 * un * acc; F3(vv, z, ed) = v2 * un * acc; }
+        }
+    }
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_rhsAB, z, e1) = F3(m->U_rhsAB, z, e1) - F3(uu, z, ed);
+            F3(m->V_rhsAB, z, e1) = F3(m->V_rhsAB, z, e1) - F3(vv, z, ed);
+        }
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_rhsAB, z, e2) = F3(m->U_rhsAB, z, e2) + F3(uu, z, ed);
+            F3(m->V_rhsAB, z, e2) = F3(m->V_rhsAB, z, e2) + F3(vv, z, ed);
+        }
+    }
+}
+
+/* viscosity_filt_3D, fv_viscosity.F90:815-868 */
+static void viscosity_filt_3D(oracle_model *m) {
+    double tau_inv = m->p.tau_inv_filt;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        for (int z = 1; z <= m->L; ++z) {
+            double u1 = 0.0, v1 = 0.0;
+            for (int j = 1; j <= jend; ++j) {
+                int ne = ELNB(j, el);
+                if (ne > 0) {
+                    u1 = u1 + F3(m->U_n, z, ne) - F3(m->U_n, z, el);
+                    v1 = v1 + F3(m->V_n, z, ne) - F3(m->V_n, z, el);
+                }
+            }
+            F3(m->U_rhs, z, el) = F3(m->U_rhs, z, el) + tau_inv * u1 * N1(m->elem_area, el) * F3(m->Je, z, el);
+            F3(m->V_rhs, z, el) = F3(m->V_rhs, z, el) + tau_inv * v1 * N1(m->elem_area, el) * F3(m->Je, z, el);
+        }
+    }
+}
+
+static inline double wsumN(const oracle_model *m, int el, const double *a, int z, int stride) {
+    double s = 0.0;
+    for (int k = 1; k <= 4; ++k) s = s + WCV(k, el) * a[(size_t)stride * (ELN(k, el) - 1) + z - 1];
+    return s;
+}
+
+/* momentum_vert_adv_upwind, fv_advection.F90:354-469 */
+static void momentum_vert_adv_upwind(oracle_model *m) {
+    const int NS = m->NS, L = m->L;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double uv1[NS + 2], uv2[NS + 2];
+        if (N1(m->mask_wd, el) != 0.0) {
+            double acc = 0.0;
+            for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+            double umean = 0.0, vmean = 0.0;
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                double w = wsumN(m, el, m->Wvel, nz, NS) * N1(m->elem_area, el);
+                if (w >= 0.0) {
+                    if (nz == NS - 1) {
+                        umean = 0.5 * (F3(m->U_n, nz - 1, el) + F3(m->U_n, nz, el));
+                        vmean = 0.5 * (F3(m->V_n, nz - 1, el) + F3(m->V_n, nz, el));
+                    } else {
+                        double Z1 = wsumN(m, el, m->zbar, nz, NS);
+                        double a = Z1 - wsumN(m, el, m->Z, nz - 1, L);
+                        double b = wsumN(m, el, m->Z, nz, L) - Z1;
+                        double c = wsumN(m, el, m->Z, nz + 1, L) - Z1;
+                        double d = (c + a) * (b * b - a * a) - (c * c - a * a) * (b + a);
+                        double dg = a * b * (a + b) / d;
+                        double db = -a * c * (a + c) / d;
+                        double da = 1.0 - dg - db;
+                        umean = F3(m->U_n, nz - 1, el) * da + F3(m->U_n, nz, el) * db + F3(m->U_n, nz + 1, el) * dg;
+                        vmean = F3(m->V_n, nz - 1, el) * da + F3(m->V_n, nz, el) * db + F3(m->V_n, nz + 1, el) * dg;
+                    }
+                }
+                if (w < 0.0) {
+                    if (nz == 2) {
+                        umean = 0.5 * (F3(m->U_n, nz - 1, el) + F3(m->U_n, nz, el));
+                        vmean = 0.5 * (F3(m->V_n, nz - 1, el) + F3(m->V_n, nz, el));
+                    } else {
+                        double Z1 = wsumN(m, el, m->zbar, nz, NS);
+                        double a = wsumN(m, el, m->Z, nz, L) - Z1;
+                        double b = Z1 - wsumN(m, el, m->Z, nz - 1, L);
+                        double c = Z1 - wsumN(m, el, m->Z, nz - 2, L);
+                        double d = (c + a) * (b * b - a * a) - (c * c - a * a) * (b + a);
+                        double dg = a * b * (a + b) / d;
+                        double db = -a * c * (a + c) / d;
+                        double da = 1.0 - dg - db;
+                        umean = F3(m->U_n, nz, el) * da + F3(m->U_n, nz - 1, el) * db + F3(m->U_n, nz - 2, el) * dg;
+                        vmean = F3(m->V_n, nz, el) * da + F3(m->V_n, nz - 1, el) * db + F3(m->V_n, nz - 2, el) * dg;
+                    }
+                }
+                uv1[nz] = -umean * w;
+                uv2[nz] = -vmean * w;
+            }
+            double w = wsumN(m, el, m->Wvel, 1, NS) * N1(m->elem_area, el);
+            uv1[1] = -w * F3(m->U_n, 1, el);
+            uv2[1] = -w * F3(m->V_n, 1, el);
+            uv1[NS] = 0.0;
+            uv2[NS] = 0.0;
+            for (int nz = 1; nz <= L; ++nz) {
+                F3(m->U_rhsAB, nz, el) = F3(m->U_rhsAB, nz, el) + (uv1[nz] - uv1[nz + 1]) * acc;
+                F3(m->V_rhsAB, nz, el) = F3(m->V_rhsAB, nz, el) + (uv2[nz] - uv2[nz + 1]) * acc;
+            }
+        } else {
+            for (int nz = 1; nz <= L; ++nz) { F3(m->U_rhsAB, nz, el) = 0.0; F3(m->V_rhsAB, nz, el) = 0.0; }
+        }
+    }
+}
+
+/* momentum_vert_impl_visc, fv_viscosity.F90:1266-1371 */
+static void momentum_vert_impl_visc(oracle_model *m) {
+    const int NS = m->NS, L = m->L;
+    const double dt = m->p.dt;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double a[NS + 1], b[NS + 1], c[NS + 1], ur[NS + 1], vr[NS + 1], cp[NS + 1], up[NS + 1], vp[NS + 1];
+        double acc = 0.0;
+        for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+        double a_Cd = N1(m->C_d_el, el) * ((1.0 - acc) * m->p.Cd_bz + 1.0);
+        for (int nz = 2; nz <= NS - 2; ++nz) {
+            double zinv = dt / F3(m->Je, nz, el);
+            double Z_c = wsumN(m, el, m->Z, nz, L), Z_u = wsumN(m, el, m->Z, nz - 1, L), Z_b = wsumN(m, el, m->Z, nz + 1, L);
+            a[nz] = -W3(m->Av, nz, el) / (Z_c - Z_u) * zinv;
+            c[nz] = -W3(m->Av, nz + 1, el) / (Z_b - Z_c) * zinv;
+            b[nz] = -a[nz] - c[nz] + 1.0;
+        }
+        double zinv = dt / F3(m->Je, L, el);
+        double Z_c = wsumN(m, el, m->Z, L, L), Z_u = wsumN(m, el, m->Z, L - 1, L);
+        a[L] = -W3(m->Av, L, el) / (Z_c - Z_u) * zinv;
+        b[L] = -a[L] + 1.0;
+        c[L] = 0.0;
+        zinv = dt / F3(m->Je, 1, el);
+        Z_c = wsumN(m, el, m->Z, 1, L);
+        double Z_b = wsumN(m, el, m->Z, 2, L);
+        c[1] = -W3(m->Av, 2, el) / (Z_b - Z_c) * zinv;
+        a[1] = 0.0;
+        b[1] = -c[1] + 1.0;
+        for (int nz = 1; nz <= L; ++nz) { ur[nz] = F3(m->U_rhs, nz, el); vr[nz] = F3(m->V_rhs, nz, el); }
+        ur[1] = ur[1] + zinv * N1(m->taux, el) / m->p.density_0;
+        vr[1] = vr[1] + zinv * N1(m->tauy, el) / m->p.density_0;
+        zinv = dt / F3(m->Je, L, el);
+        double ub = F3(m->U_n, L, el), vb = F3(m->V_n, L, el);
+        double friction = -a_Cd * sqrt(ub * ub + vb * vb);
+        ur[L] = ur[L] + zinv * friction * ub;
+        vr[L] = vr[L] + zinv * friction * vb;
+        cp[1] = c[1] / b[1];
+        up[1] = ur[1] / b[1];
+        vp[1] = vr[1] / b[1];
+        for (int nz = 2; nz <= L; ++nz) {
+            double mm = b[nz] - cp[nz - 1] * a[nz];
+            cp[nz] = c[nz] / mm;
+            up[nz] = (ur[nz] - up[nz - 1] * a[nz]) / mm;
+            vp[nz] = (vr[nz] - vp[nz - 1] * a[nz]) / mm;
+        }
+        ur[L] = up[L];
+        vr[L] = vp[L];
+        for (int nz = L - 1; nz >= 1; --nz) {
+            ur[nz] = up[nz] - cp[nz] * ur[nz + 1];
+            vr[nz] = vp[nz] - cp[nz] * vr[nz + 1];
+        }
+        for (int nz = 1; nz <= L; ++nz) {
+            F3(m->U_rhs, nz, el) = ur[nz] * N1(m->mask_wd, el);
+            F3(m->V_rhs, nz, el) = vr[nz] * N1(m->mask_wd, el);
+        }
+    }
+}
+
+/* momentum_vert_impl_visc_tmp, fv_viscosity.F90:1374-1486 (no ice) */
+static void momentum_vert_impl_visc_tmp(oracle_model *m) {
+    const int NS = m->NS, L = m->L;
+    const double dt = m->p.dt;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double xx1[NS + 2], yyu[NS + 2], yyv[NS + 2], Ut[NS + 2], Vt[NS + 2];
+        if (N1(m->mask_wd, el) != 0.0) {
+            xx1[1] = 1.0;
+            double de = F3(m->Je, 1, el) / (W3(m->Av, 1, el) + W3(m->Av, 2, el));
+            double rw = de / m->p.density_0;
+            yyu[1] = N1(m->taux, el) * rw;
+            yyv[1] = N1(m->tauy, el) * rw;
+            for (int nz = 1; nz <= L; ++nz) {
+                double Fx = F3(m->U_rhs, nz, el), Fy = F3(m->V_rhs, nz, el);
+                double delta_1 = (nz == 1) ? 0.5 * F3(m->Je, nz, el) : 0.5 * (F3(m->Je, nz, el) + F3(m->Je, nz - 1, el));
+                double delta_2 = (nz == L) ? 0.5 * F3(m->Je, nz, el) : 0.5 * (F3(m->Je, nz, el) + F3(m->Je, nz + 1, el));
+                double zt = dt / F3(m->Je, nz, el);
+                double a = zt * W3(m->Av, nz, el) / delta_1;
+                double c = zt * W3(m->Av, nz + 1, el) / delta_2;
+                double b = a + c + 1.0;
+                double d = b - a * xx1[nz];
+                xx1[nz + 1] = c / d;
+                yyu[nz + 1] = (a * yyu[nz] + Fx) / d;
+                yyv[nz + 1] = (a * yyv[nz] + Fy) / d;
+            }
+            double acc = 0.0;
+            for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+            double a_Cd = N1(m->C_d_el, el) * ((1.0 - acc) * m->p.Cd_bz + 1.0);
+            de = F3(m->Je, L, el) / (W3(m->Av, NS, el) + W3(m->Av, L, el));
+            double ub = F3(m->U_n, L, el), vb = F3(m->V_n, L, el);
+            double friction = de * a_Cd * sqrt(ub * ub + vb * vb);
+            if (m->p.fic_point == 0) { Ut[NS] = 0.0; Vt[NS] = 0.0; }
+            else if (m->p.fic_point == 1) {
+                double a = friction + 1.0 - xx1[NS];
+                Ut[NS] = yyu[NS] / a; Vt[NS] = yyv[NS] / a;
+            } else {
+                double a = 1.0 / (1.0 - friction) - xx1[NS];
+                Ut[NS] = yyu[NS] / a; Vt[NS] = yyv[NS] / a;
+            }
+            for (int nz = L; nz >= 1; --nz) {
+                Ut[nz] = Ut[nz + 1] * xx1[nz + 1] + yyu[nz + 1];
+                Vt[nz] = Vt[nz + 1] * xx1[nz + 1] + yyv[nz + 1];
+            }
+            for (int nz = 1; nz <= L; ++nz) {
+                F3(m->U_rhs, nz, el) = Ut[nz] * N1(m->mask_wd, el);
+                F3(m->V_rhs, nz, el) = Vt[nz] * N1(m->mask_wd, el);
+            }
+        } else {
+            for (int nz = 1; nz <= L; ++nz) { F3(m->U_rhs, nz, el) = 0.0; F3(m->V_rhs, nz, el) = 0.0; }
+        }
+    }
+}
+
+/* compute_vel_rhs, fv_3D_vel.F90:1-197 (key_atm off) */
+static void compute_vel_rhs(oracle_model *m) {
+    const int L = m->L;
+    const double eps = m->p.epsilon;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double pre[4];
+        for (int k = 1; k <= 4; ++k) {
+            int nk = ELN(k, el);
+            pre[k - 1] = -WP_G * (ATP(nk, 1) * N1(m->eta_n, nk) - ATP(nk, 2) * N1(m->ssh_gp, nk));
+        }
+        double sx = 0, sy = 0;
+        for (int k = 1; k <= 4; ++k) sx = sx + GS(k, el) * pre[k - 1];
+        for (int k = 1; k <= 4; ++k) sy = sy + GS(k + 4, el) * pre[k - 1];
+        double Fx = sx * N1(m->elem_area, el), Fy = sy * N1(m->elem_area, el);
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_rhs, z, el) = -(0.5 + eps) * F3(m->U_rhsAB, z, el) + Fx * F3(m->Je, z, el);
+            F3(m->V_rhs, z, el) = -(0.5 + eps) * F3(m->V_rhsAB, z, el) + Fy * F3(m->Je, z, el);
+        }
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_rhsAB, z, el) = F3(m->V_n, z, el) * N1(m->coriolis, el) * N1(m->elem_area, el) * F3(m->Je, z, el);
+            F3(m->V_rhsAB, z, el) = -F3(m->U_n, z, el) * N1(m->coriolis, el) * N1(m->elem_area, el) * F3(m->Je, z, el);
+        }
+    }
+    vel_gradients(m);
+    if (m->p.mom_adv_3D == 1) momentum_adv_upwind(m);
+    if (m->p.filt_3D) viscosity_filt_3D(m);
+    if (m->p.vert_adv == 1) momentum_vert_adv_upwind(m);
+    double ff = 1.5 + eps;
+    if (m->lfirst) { ff = 1.0; m->lfirst = 0; }
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double area_inv = 1.0 / N1(m->elem_area, el);
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_rhs, z, el) = N1(m->mask_wd, el) * (F3(m->U_n, z, el) + F3(m->Bar_pru_3D, z, el) * m->p.dt +
+                (m->p.dt * (F3(m->U_rhs, z, el) + F3(m->U_rhsAB, z, el) * ff) * area_inv + 0.0) / F3(m->Je, z, el));
+            F3(m->V_rhs, z, el) = N1(m->mask_wd, el) * (F3(m->V_n, z, el) + F3(m->Bar_prv_3D, z, el) * m->p.dt +
+                (m->p.dt * (F3(m->V_rhs, z, el) + F3(m->V_rhsAB, z, el) * ff) * area_inv + 0.0) / F3(m->Je, z, el));
+        }
+    }
+    if (m->p.im_vert_visc) momentum_vert_impl_visc(m);
+    if (m->p.im_vert_visc_fic) momentum_vert_impl_visc_tmp(m);
+}
+
+/* update_3D_vel, fv_3D_vel.F90:201-255 */
+static void update_3D_vel(oracle_model *m) {
+    const int L = m->L;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        double a[L + 1];
+        for (int z = 1; z <= L; ++z)
+            a[z] = WCV(1, el) * F3(m->Jc_old, z, ELN(1, el)) + WCV(2, el) * F3(m->Jc_old, z, ELN(2, el))
+                 + WCV(3, el) * F3(m->Jc_old, z, ELN(3, el)) + WCV(4, el) * F3(m->Jc_old, z, ELN(4, el));
+        double dmean_inv = 1.0 / MAXD(m->p.Dmin, wsum2(m, el, m->depth, m->eta_n));
+        double su = 0.0, sv = 0.0;
+        for (int z = 1; z <= L; ++z) su = su + F3(m->U_rhs, z, el) * a[z];
+        for (int z = 1; z <= L; ++z) sv = sv + F3(m->V_rhs, z, el) * a[z];
+        double U_2D_p = su * dmean_inv, V_2D_p = sv * dmean_inv;
+        N1(m->U_filt_2D, el) = N1(m->U_filt_2D, el) * dmean_inv;
+        N1(m->V_filt_2D, el) = N1(m->V_filt_2D, el) * dmean_inv;
+        for (int z = 1; z <= L; ++z) a[z] = a[z] / F3(m->Je, z, el);
+        for (int z = 1; z <= L; ++z) {
+            F3(m->U_n_filt, z, el) = a[z] * F3(m->U_rhs, z, el) + N1(m->U_filt_2D, el) - U_2D_p;
+            F3(m->V_n_filt, z, el) = a[z] * F3(m->V_rhs, z, el) + N1(m->V_filt_2D, el) - V_2D_p;
+            F3(m->U_n, z, el) = a[z] * F3(m->U_rhs, z, el) + V2(m->U_n_2D, 1, el) - U_2D_p;
+            F3(m->V_n, z, el) = a[z] * F3(m->V_rhs, z, el) + V2(m->U_n_2D, 2, el) - V_2D_p;
+        }
+    }
+}
+
+/* vert_vel_sigma, fv_3D_vel.F90:309-456 (serial build path) */
+static void vert_vel_sigma(oracle_model *m) {
+    const int L = m->L, NS = m->NS;
+    double c1[L + 1];
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, n) = 0.0;
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        for (int z = 1; z <= L; ++z)
+            c1[z] = F3(m->Je, z, e1) * ((F3(m->V_n_filt, z, e1) - N1(m->V_filt_2D, e1)) * ECR(1, ed)
+                                       - (F3(m->U_n_filt, z, e1) - N1(m->U_filt_2D, e1)) * ECR(2, ed))
+                  + F3(m->Je, z, e2) * (-(F3(m->V_n_filt, z, e2) - N1(m->V_filt_2D, e2)) * ECR(3, ed)
+                                       + (F3(m->U_n_filt, z, e2) - N1(m->U_filt_2D, e2)) * ECR(4, ed));
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, EDN(1, ed)) = W3(m->Wvel, z, EDN(1, ed)) + c1[z];
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, EDN(2, ed)) = W3(m->Wvel, z, EDN(2, ed)) - c1[z];
+    }
+    for (int ed = 1 + m->Ed_in; ed <= m->Ed; ++ed) {
+        int e1 = EDT(1, ed);
+        for (int z = 1; z <= L; ++z)
+            c1[z] = F3(m->Je, z, e1) * ((F3(m->V_n_filt, z, e1) - N1(m->V_filt_2D, e1)) * ECR(1, ed)
+                                       - (F3(m->U_n_filt, z, e1) - N1(m->U_filt_2D, e1)) * ECR(2, ed));
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, EDN(1, ed)) = W3(m->Wvel, z, EDN(1, ed)) + c1[z];
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, EDN(2, ed)) = W3(m->Wvel, z, EDN(2, ed)) - c1[z];
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        double area_inv = 1.0 / N1(m->area, n);
+        for (int z = NS - 1; z >= 1; --z) W3(m->Wvel, z, n) = W3(m->Wvel, z, n) + W3(m->Wvel, z + 1, n);
+        for (int z = 1; z <= L; ++z) W3(m->Wvel, z, n) = W3(m->Wvel, z, n) * area_inv;
+    }
+}
+
+/* ====================================================================== */
+/* tracers                                                                 */
+/* ====================================================================== */
+/* Vel_nor from boundary edges (shared by the three advection schemes) */
+static void vel_nor(oracle_model *m, double *Vel_nor) {
+    for (int n = 1; n <= m->N; ++n) N1(Vel_nor, n) = 0.0;
+    for (int ed = 1 + m->Ed_in; ed <= m->Ed; ++ed) {
+        int n1 = EDN(1, ed), n2 = EDN(2, ed), e1 = EDT(1, ed);
+        double dmean = MAXD(m->p.Dmin, 0.5 * (N1(m->eta_n, n1) + N1(m->depth, n1) + N1(m->eta_n, n2) + N1(m->depth, n2)));
+        double un1 = (N1(m->V_filt_2D, e1) * ECR(1, ed) - N1(m->U_filt_2D, e1) * ECR(2, ed)) * dmean;
+        N1(Vel_nor, n1) = N1(Vel_nor, n1) + un1 / N1(m->area, n1);
+        N1(Vel_nor, n2) = N1(Vel_nor, n2) - un1 / N1(m->area, n2);
+    }
+}
+
+/* solve_tracer_upwind, fv_tracer.F90:390-923 (serial build path) */
+static void solve_tracer_upwind(oracle_model *m) {
+    const int L = m->L, NS = m->NS;
+    const double eps = m->p.epsilon, T_aver = m->T_aver, S_aver = m->S_aver;
+    double *ttf = m->TF, *ttfold = m->T_old, *stf = m->SF, *stfold = m->S_old;
+    double *ttrhs = m->s_n1, *strhs = m->s_n2, *trhs_c = m->s_n3, *Vel = m->s_n4;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            F3(ttfold, z, n) = -(0.5 + eps) * F3(ttfold, z, n) + (1.5 + eps) * F3(ttf, z, n) - T_aver;
+            F3(ttf, z, n) = F3(ttf, z, n) - T_aver;
+            F3(stfold, z, n) = -(0.5 + eps) * F3(stfold, z, n) + (1.5 + eps) * F3(stf, z, n) - S_aver;
+            F3(stf, z, n) = F3(stf, z, n) - S_aver;
+            F3(ttrhs, z, n) = 0.0; F3(strhs, z, n) = 0.0; F3(trhs_c, z, n) = 0.0;
+        }
+    double aux_c[L + 1], t_aux[L + 1], s_aux[L + 1];
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int nod1 = EDN(1, ed), nod2 = EDN(2, ed), el1 = EDT(1, ed), el2 = EDT(2, ed);
+        for (int z = 1; z <= L; ++z) {
+            double c1 = F3(m->V_n_filt, z, el1) * ECR(1, ed) - F3(m->U_n_filt, z, el1) * ECR(2, ed);
+            double c2 = -F3(m->V_n_filt, z, el2) * ECR(3, ed) + F3(m->U_n_filt, z, el2) * ECR(4, ed);
+            double J1 = F3(m->Je, z, el1), J2 = F3(m->Je, z, el2);
+            aux_c[z] = J1 * c1 + J2 * c2;
+            if (c1 > 0.0 && c2 > 0.0) {
+                t_aux[z] = J1 * c1 * F3(ttfold, z, nod2) + J2 * c2 * F3(ttfold, z, nod2);
+                s_aux[z] = J1 * c1 * F3(stfold, z, nod2) + J2 * c2 * F3(stfold, z, nod2);
+            } else if (c1 > 0.0) {
+                t_aux[z] = J1 * c1 * F3(ttfold, z, nod2) + J2 * c2 * F3(ttfold, z, nod1);
+                s_aux[z] = J1 * c1 * F3(stfold, z, nod2) + J2 * c2 * F3(stfold, z, nod1);
+            } else if (c2 > 0.0) {
+                t_aux[z] = J1 * c1 * F3(ttfold, z, nod1) + J2 * c2 * F3(ttfold, z, nod2);
+                s_aux[z] = J1 * c1 * F3(stfold, z, nod1) + J2 * c2 * F3(stfold, z, nod2);
+            } else {
+                t_aux[z] = J1 * c1 * F3(ttfold, z, nod1) + J2 * c2 * F3(ttfold, z, nod1);
+                s_aux[z] = J1 * c1 * F3(stfold, z, nod1) + J2 * c2 * F3(stfold, z, nod1);
+            }
+        }
+        for (int z = 1; z <= L; ++z) {
+            F3(trhs_c, z, nod1) = F3(trhs_c, z, nod1) + aux_c[z];
+            F3(ttrhs, z, nod1) = F3(ttrhs, z, nod1) + t_aux[z];
+            F3(strhs, z, nod1) = F3(strhs, z, nod1) + s_aux[z];
+            F3(trhs_c, z, nod2) = F3(trhs_c, z, nod2) - aux_c[z];
+            F3(ttrhs, z, nod2) = F3(ttrhs, z, nod2) - t_aux[z];
+            F3(strhs, z, nod2) = F3(strhs, z, nod2) - s_aux[z];
+        }
+    }
+    for (int ed = m->Ed_in + 1; ed <= m->Ed; ++ed) {
+        int nod1 = EDN(1, ed), nod2 = EDN(2, ed), el1 = EDT(1, ed);
+        for (int z = 1; z <= L; ++z) {
+            double c1 = F3(m->V_n_filt, z, el1) * ECR(1, ed) - F3(m->U_n_filt, z, el1) * ECR(2, ed);
+            aux_c[z] = F3(m->Je, z, el1) * c1;
+            if (c1 > 0.0) {
+                t_aux[z] = aux_c[z] * F3(ttfold, z, nod2);
+                s_aux[z] = aux_c[z] * F3(stfold, z, nod2);
+            } else {
+                t_aux[z] = aux_c[z] * F3(ttfold, z, nod1);
+                s_aux[z] = aux_c[z] * F3(stfold, z, nod1);
+            }
+        }
+        for (int z = 1; z <= L; ++z) {
+            F3(trhs_c, z, nod1) = F3(trhs_c, z, nod1) + aux_c[z];
+            F3(ttrhs, z, nod1) = F3(ttrhs, z, nod1) + t_aux[z];
+            F3(strhs, z, nod1) = F3(strhs, z, nod1) + s_aux[z];
+            F3(trhs_c, z, nod2) = F3(trhs_c, z, nod2) - aux_c[z];
+            F3(ttrhs, z, nod2) = F3(ttrhs, z, nod2) - t_aux[z];
+            F3(strhs, z, nod2) = F3(strhs, z, nod2) - s_aux[z];
+        }
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        double tvert[NS + 1], svert[NS + 1];
+        double dg, db;
+#define ZZ(k) F3(m->Z, k, n)
+#define ZB(k) W3(m->zbar, k, n)
+#define TO(k) F3(ttfold, k, n)
+#define SO(k) F3(stfold, k, n)
+#define WV(k) W3(m->Wvel, k, n)
+        for (int k = 0; k <= NS; ++k) { tvert[k] = 0.0; svert[k] = 0.0; }
+        tvert[1] = -WV(1) * TO(1);
+        svert[1] = -WV(1) * SO(1);
+        tvert[NS] = 0.0;
+        if (WV(2) > 0.0) {
+            dg = (ZB(2) - ZZ(1)) * (ZZ(2) - ZB(2)) / ((ZZ(3) - ZZ(1)) * (ZZ(2) - ZZ(3)));
+            db = -(ZB(2) - ZZ(1)) * (ZZ(3) - ZB(2)) / ((ZZ(2) - ZZ(1)) * (ZZ(2) - ZZ(3)));
+            tvert[2] = -(TO(1) * (1.0 - dg - db) + TO(2) * db + TO(3) * dg) * WV(2);
+            svert[2] = -(SO(1) * (1.0 - dg - db) + SO(2) * db + SO(3) * dg) * WV(2);
+        } else {
+            tvert[2] = -TO(1) * WV(2);
+            svert[2] = -SO(1) * WV(2);
+        }
+        for (int nz = 3; nz <= NS - 2; ++nz) {
+            if (WV(nz) >= 0.0) {
+                dg = (ZB(nz) - ZZ(nz - 1)) * (ZZ(nz) - ZB(nz)) / ((ZZ(nz + 1) - ZZ(nz - 1)) * (ZZ(nz) - ZZ(nz + 1)));
+                db = -(ZB(nz) - ZZ(nz - 1)) * (ZZ(nz + 1) - ZB(nz)) / ((ZZ(nz) - ZZ(nz - 1)) * (ZZ(nz) - ZZ(nz + 1)));
+                tvert[nz] = -(TO(nz - 1) * (1.0 - dg - db) + TO(nz) * db + TO(nz + 1) * dg) * WV(nz);
+                svert[nz] = -(SO(nz - 1) * (1.0 - dg - db) + SO(nz) * db + SO(nz + 1) * dg) * WV(nz);
+            } else {
+                dg = (ZZ(nz) - ZB(nz)) * (ZB(nz) - ZZ(nz - 1)) / ((ZZ(nz) - ZZ(nz - 2)) * (ZZ(nz - 2) - ZZ(nz - 1)));
+                db = -(ZZ(nz) - ZB(nz)) * (ZB(nz) - ZZ(nz - 2)) / ((ZZ(nz) - ZZ(nz - 1)) * (ZZ(nz - 2) - ZZ(nz - 1)));
+                tvert[nz] = -(TO(nz) * (1.0 - dg - db) + TO(nz - 1) * db + TO(nz - 2) * dg) * WV(nz);
+                svert[nz] = -(SO(nz) * (1.0 - dg - db) + SO(nz - 1) * db + SO(nz - 2) * dg) * WV(nz);
+            }
+        }
+        {
+            int nz = NS - 1;
+            if (WV(nz) >= 0.0) {
+                tvert[nz] = -TO(nz) * WV(nz);
+                svert[nz] = -SO(nz) * WV(nz);
+            } else {
+                dg = (ZZ(nz) - ZB(nz)) * (ZB(nz) - ZZ(nz - 1)) / ((ZZ(nz) - ZZ(nz - 2)) * (ZZ(nz - 2) - ZZ(nz - 1)));
+                db = -(ZZ(nz) - ZB(nz)) * (ZB(nz) - ZZ(nz - 2)) / ((ZZ(nz) - ZZ(nz - 1)) * (ZZ(nz - 2) - ZZ(nz - 1)));
+                tvert[nz] = -(TO(nz) * (1.0 - dg - db) + TO(nz - 1) * db + TO(nz - 2) * dg) * WV(nz);
+                svert[nz] = -(SO(nz) * (1.0 - dg - db) + SO(nz - 1) * db + SO(nz - 2) * dg) * WV(nz);
+            }
+        }
+        double area_inv = 1.0 / N1(m->area, n);
+        for (int nz = 1; nz <= L; ++nz) {
+            F3(ttrhs, nz, n) = ((F3(ttrhs, nz, n) - TO(nz) * F3(trhs_c, nz, n)) * area_inv
+                                + TO(nz) * (WV(nz) - WV(nz + 1)) + (tvert[nz] - tvert[nz + 1])) / F3(m->Jc, nz, n);
+            F3(strhs, nz, n) = ((F3(strhs, nz, n) - SO(nz) * F3(trhs_c, nz, n)) * area_inv
+                                + SO(nz) * (WV(nz) - WV(nz + 1)) + (svert[nz] - svert[nz + 1])) / F3(m->Jc, nz, n);
+        }
+#undef ZZ
+#undef ZB
+#undef TO
+#undef SO
+#undef WV
+    }
+    if (m->p.cl_relax) {
+        vel_nor(m, Vel);
+        for (int n = 1; n <= m->N; ++n) {
+            if (N1(m->index_nod2D, n) != 2) continue;
+            if (N1(Vel, n) > 0.0) {
+                for (int z = 1; z <= L; ++z) {
+                    F3(ttrhs, z, n) = F3(ttrhs, z, n) + m->p.relax2clim_ac * (F3(m->Tclim, z, n) - (F3(ttfold, z, n) + T_aver));
+                    F3(strhs, z, n) = F3(strhs, z, n) + m->p.relax2clim_ac * (F3(m->Sclim, z, n) - (F3(stfold, z, n) + S_aver));
+                }
+            } else {
+                for (int z = 1; z <= L; ++z) {
+                    F3(ttrhs, z, n) = m->p.clim_relax * (F3(m->Tclim, z, n) - (F3(ttfold, z, n) + T_aver));
+                    F3(strhs, z, n) = m->p.clim_relax * (F3(m->Sclim, z, n) - (F3(stfold, z, n) + S_aver));
+                }
+            }
+        }
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            F3(ttfold, z, n) = F3(ttf, z, n) + T_aver;
+            F3(ttf, z, n) = F3(ttf, z, n) + F3(ttrhs, z, n) * m->p.dt + T_aver;
+            F3(stfold, z, n) = F3(stf, z, n) + S_aver;
+            F3(stf, z, n) = F3(stf, z, n) + F3(strhs, z, n) * m->p.dt + S_aver;
+        }
+}
+
+/* tracer_gradient_elements, fv_gradients.F90:180-214 */
+static void tracer_gradient_elements(oracle_model *m, const double *ttf, double *ttx, double *tty) {
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el)
+        for (int z = 1; z <= m->L; ++z) {
+            double sx = 0.0, sy = 0.0;
+            for (int k = 1; k <= 4; ++k) sx = sx + GS(k, el) * F3(ttf, z, ELN(k, el));
+            for (int k = 1; k <= 4; ++k) sy = sy + GS(k + 4, el) * F3(ttf, z, ELN(k, el));
+            F3(ttx, z, el) = sx;
+            F3(tty, z, el) = sy;
+        }
+}
+
+/* tracer_gradient_nodes, fv_gradients.F90:217-260 */
+static void tracer_gradient_nodes(oracle_model *m, const double *ttx, const double *tty, double *txn, double *tyn) {
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        int num = NIEN(n);
+        double s = 0.0;
+        for (int k = 1; k <= num; ++k) s = s + N1(m->elem_area, NIE(k, n));
+        double tvol = 1.0 / s;
+        for (int z = 1; z <= m->L; ++z) {
+            double tx = 0.0, ty = 0.0;
+            for (int k = 1; k <= num; ++k) {
+                int el = NIE(k, n);
+                tx = tx + F3(ttx, z, el) * N1(m->elem_area, el);
+                ty = ty + F3(tty, z, el) * N1(m->elem_area, el);
+            }
+            F3(txn, z, n) = tx * tvol;
+            F3(tyn, z, n) = ty * tvol;
+        }
+    }
+}
+
+/* common vertical QUICK flux of solve_tracer_miura / solve_tracer_muscl
+ * (fv_tracer.F90:1171-1207 and :235-271).  'muscl' selects the a*b/(c+a)/(b-c)
+ * grouping of the MUSCL routine instead of a*b/((c+a)*(b-c)). */
+static void tvert_quick(oracle_model *m, int n, const double *T, double *tvert, int muscl) {
+    const int NS = m->NS;
+    double Tmean = 0.0;
+    tvert[1] = -W3(m->Wvel, 1, n) * F3(T, 1, n);
+    tvert[NS] = 0.0;
+    for (int nz = 2; nz <= NS - 1; ++nz) {
+        double W = W3(m->Wvel, nz, n);
+        if (W > 0.0) {
+            if (nz == NS - 1) Tmean = F3(T, nz, n);
+            else {
+                double a = W3(m->zbar, nz, n) - F3(m->Z, nz - 1, n);
+                double b = F3(m->Z, nz, n) - W3(m->zbar, nz, n);
+                double c = F3(m->Z, nz + 1, n) - W3(m->zbar, nz, n);
+                double dg = muscl ? a * b / (c + a) / (b - c) : a * b / ((c + a) * (b - c));
+                double db = muscl ? -a * c / (b + a) / (b - c) : -a * c / ((b + a) * (b - c));
+                double da = 1.0 - dg - db;
+                Tmean = F3(T, nz - 1, n) * da + F3(T, nz, n) * db + F3(T, nz + 1, n) * dg;
+            }
+        }
+        if (W < 0.0) {
+            if (nz == 2) Tmean = F3(T, nz - 1, n);
+            else {
+                double a = F3(m->Z, nz, n) - W3(m->zbar, nz, n);
+                double b = W3(m->zbar, nz, n) - F3(m->Z, nz - 1, n);
+                double c = W3(m->zbar, nz, n) - F3(m->Z, nz - 2, n);
+                double dg = muscl ? a * b / (c + a) / (b - c) : a * b / ((c + a) * (b - c));
+                double db = muscl ? -a * c / (b + a) / (b - c) : -a * c / ((b + a) * (b - c));
+                double da = 1.0 - dg - db;
+                Tmean = F3(T, nz, n) * da + F3(T, nz - 1, n) * db + F3(T, nz - 2, n) * dg;
+            }
+        }
+        tvert[nz] = -Tmean * W;
+    }
+}
+
+/* relaxation at open-boundary nodes (fv_tracer.F90:1221-1278 / :282-334) */
+static void relax_ob(oracle_model *m, double *ttrhs, const double *ttf, const double *clim, double aver) {
+    double *Vel = m->s_n4;
+    vel_nor(m, Vel);
+    for (int n = 1; n <= m->N; ++n) {
+        if (N1(m->index_nod2D, n) != 2) continue;
+        if (N1(Vel, n) > 0.0) {
+            for (int z = 1; z <= m->L; ++z)
+                F3(ttrhs, z, n) = F3(ttrhs, z, n) + m->p.relax2clim_ac * (F3(clim, z, n) - (F3(ttf, z, n) + aver));
+        } else {
+            for (int z = 1; z <= m->L; ++z)
+                F3(ttrhs, z, n) = m->p.clim_relax * (F3(clim, z, n) - (F3(ttf, z, n) + aver));
+        }
+    }
+}
+
+/* solve_tracer_miura, fv_tracer.F90:930-1316 */
+static void solve_tracer_miura(oracle_model *m, double *ttf, double *ttfold, int is_salt) {
+    const int L = m->L, NS = m->NS;
+    const double eps = m->p.epsilon, dt = m->p.dt;
+    double TS_aver = is_salt ? m->S_aver : m->T_aver;
+    double *ttrhs = m->s_n1, *ttrhs_c = m->s_n2, *txn = m->s_n3, *tyn = m->s_n4 + 0;
+    double *ttx = m->s_gr, *tty = m->s_gr + (size_t)L * m->E;
+    double *tynb = m->s_e4; /* (L,N) buffer distinct from s_n4 (vel_nor uses s_n4) */
+    tyn = tynb;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        for (int z = 1; z <= L; ++z) {
+            F3(ttfold, z, n) = -(0.5 + eps) * F3(ttfold, z, n) + (1.5 + eps) * F3(ttf, z, n) - TS_aver;
+            F3(ttf, z, n) = F3(ttf, z, n) - TS_aver;
+        }
+        for (int z = 1; z <= L; ++z) { F3(ttrhs, z, n) = 0.0; F3(ttrhs_c, z, n) = 0.0; }
+    }
+    tracer_gradient_elements(m, ttf, ttx, tty);
+    tracer_gradient_nodes(m, ttx, tty, txn, tyn);
+    for (int edge = 1; edge <= m->Ed; ++edge) {
+        int n1 = EDN(1, edge), n2 = EDN(2, edge);
+        double crt1 = 0.5 * (N1(m->mask_ad, n1) + N1(m->mask_ad, n2));
+        int el1 = EDT(1, edge), el2 = EDT(2, edge);
+        double dX1 = ECR(1, edge), dY1 = ECR(2, edge), dX2 = 0.0, dY2 = 0.0;
+        double Kh = N1(m->elem_area, el1), a = 1.0, b = 1.0;
+        if (el2 > 0) {
+            dX2 = ECR(3, edge); dY2 = ECR(4, edge);
+            b = 1.0;
+            Kh = 0.5 * (Kh + N1(m->elem_area, el2));
+        }
+        Kh = m->p.K_hor * Kh / m->p.scale_area;
+        for (int z = 1; z <= L; ++z) {
+            double Tx, Ty, Tmean;
+            if (el2 > 0) {
+                Tx = 0.5 * Kh * (F3(ttx, z, el1) + F3(ttx, z, el2));
+                Ty = 0.5 * Kh * (F3(tty, z, el1) + F3(tty, z, el2));
+            } else {
+                Tx = Kh * F3(ttx, z, el1);
+                Ty = Kh * F3(tty, z, el1);
+            }
+            double U1 = F3(m->U_n_filt, z, el1), V1 = F3(m->V_n_filt, z, el1);
+            if (V1 * dX1 - U1 * dY1 > 0) {
+                /* no *dt on the V term in this branch (fv_tracer.F90:1057) */
+                Tmean = F3(ttf, z, n2) + (0.5 * (-EDXY(1, edge) * a + dX1 - U1 * dt) * F3(txn, z, n2) +
+                                          0.5 * (-EDXY(2, edge) * WP_R_EARTH + dY1 - V1) * F3(tyn, z, n2)) * crt1;
+            } else {
+                Tmean = F3(ttf, z, n1) + (0.5 * (EDXY(1, edge) * a + dX1 - U1 * dt) * F3(txn, z, n1) +
+                                          0.5 * (EDXY(2, edge) * WP_R_EARTH + dY1 - V1 * dt) * F3(tyn, z, n1)) * crt1;
+            }
+            double c1 = (F3(m->Je, z, el1) * V1 * Tmean - Ty) * dX1 - (F3(m->Je, z, el1) * U1 * Tmean - Tx) * dY1;
+            F3(ttrhs, z, n1) = F3(ttrhs, z, n1) + c1;
+            F3(ttrhs, z, n2) = F3(ttrhs, z, n2) - c1;
+        }
+        if (el2 > 0) {
+            for (int z = 1; z <= L; ++z) {
+                double Tx = 0.5 * Kh * (F3(ttx, z, el1) + F3(ttx, z, el2));
+                double Ty = 0.5 * Kh * (F3(tty, z, el1) + F3(tty, z, el2));
+                double U2 = F3(m->U_n_filt, z, el2), V2v = F3(m->V_n_filt, z, el2), Tmean;
+                if (V2v * dX2 - U2 * dY2 < 0) {
+                    Tmean = F3(ttf, z, n2) + (0.5 * (-EDXY(1, edge) * b + dX2 - U2 * dt) * F3(txn, z, n2) +
+                                              0.5 * (-EDXY(2, edge) * WP_R_EARTH + dY2 - V2v * dt) * F3(tyn, z, n2)) * crt1;
+                } else {
+                    Tmean = F3(ttf, z, n1) + (0.5 * (EDXY(1, edge) * b + dX2 - U2 * dt) * F3(txn, z, n1) +
+                                              0.5 * (EDXY(2, edge) * WP_R_EARTH + dY2 - V2v * dt) * F3(tyn, z, n1)) * crt1;
+                }
+                double c2 = -(F3(m->Je, z, el2) * V2v * Tmean - Ty) * dX2 + (F3(m->Je, z, el2) * U2 * Tmean - Tx) * dY2;
+                F3(ttrhs, z, n1) = F3(ttrhs, z, n1) + c2;
+                F3(ttrhs, z, n2) = F3(ttrhs, z, n2) - c2;
+            }
+        }
+        for (int z = 1; z <= L; ++z) {
+            double c1 = F3(m->Je, z, el1) * F3(m->V_n_filt, z, el1) * dX1 - F3(m->Je, z, el1) * F3(m->U_n_filt, z, el1) * dY1;
+            F3(ttrhs_c, z, n1) = F3(ttrhs_c, z, n1) + c1;
+            F3(ttrhs_c, z, n2) = F3(ttrhs_c, z, n2) - c1;
+        }
+        if (el2 > 0)
+            for (int z = 1; z <= L; ++z) {
+                double c2 = -F3(m->Je, z, el2) * F3(m->V_n_filt, z, el2) * dX2 + F3(m->Je, z, el2) * F3(m->U_n_filt, z, el2) * dY2;
+                F3(ttrhs_c, z, n1) = F3(ttrhs_c, z, n1) + c2;
+                F3(ttrhs_c, z, n2) = F3(ttrhs_c, z, n2) - c2;
+            }
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        double tvert[NS + 1];
+        tvert_quick(m, n, ttf, tvert, 0);
+        for (int z = 1; z <= L; ++z)
+            F3(ttrhs, z, n) = ((F3(ttrhs, z, n) - F3(ttfold, z, n) * F3(ttrhs_c, z, n)) / N1(m->area, n)
+                               + F3(ttfold, z, n) * (W3(m->Wvel, z, n) - W3(m->Wvel, z + 1, n))
+                               + tvert[z] - tvert[z + 1]) / F3(m->Jc, z, n);
+    }
+    if (m->p.cl_relax) relax_ob(m, ttrhs, ttf, is_salt ? m->Sclim : m->Tclim, is_salt ? m->S_aver : m->T_aver);
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            F3(ttfold, z, n) = F3(ttf, z, n) + TS_aver;
+            F3(ttf, z, n) = F3(ttf, z, n) + F3(ttrhs, z, n) * dt + TS_aver;
+        }
+}
+
+/* fill_up_dn_grad, fv_gradients.F90:263-323 : edge_up_dn_grad is (4,L,Ed) */
+static void fill_up_dn_grad(oracle_model *m, const double *ttx, const double *tty, double *g) {
+    const int L = m->L;
+#define UDG(k, z, ed) g[((size_t)((ed)-1) * L + ((z)-1)) * 4 + (k)-1]
+#pragma omp parallel for
+    for (int edge = 1; edge <= m->Ed; ++edge) {
+        int u = m->edge_up_dn_tri[2 * (edge - 1)], d = m->edge_up_dn_tri[2 * (edge - 1) + 1];
+        if (u != 0 && d != 0) {
+            for (int z = 1; z <= L; ++z) {
+                UDG(1, z, edge) = F3(ttx, z, u); UDG(2, z, edge) = F3(ttx, z, d);
+                UDG(3, z, edge) = F3(tty, z, u); UDG(4, z, edge) = F3(tty, z, d);
+            }
+        } else {
+            for (int side = 1; side <= 2; ++side) {
+                int nd = EDN(side, edge);
+                for (int z = 1; z <= L; ++z) {
+                    double tvol = 0.0, tx = 0.0, ty = 0.0;
+                    for (int k = 1; k <= NIEN(nd); ++k) {
+                        int el = NIE(k, nd);
+                        tvol = tvol + N1(m->elem_area, el);
+                        tx = tx + F3(ttx, z, el) * N1(m->elem_area, el);
+                        ty = ty + F3(tty, z, el) * N1(m->elem_area, el);
+                    }
+                    UDG(side, z, edge) = tx / tvol;
+                    UDG(side + 2, z, edge) = ty / tvol;
+                }
+            }
+        }
+    }
+}
+
+/* solve_tracer_muscl, fv_tracer.F90:8-379 */
+static void solve_tracer_muscl(oracle_model *m, double *ttf, double *ttfold, int is_salt, double *g) {
+    const int L = m->L, NS = m->NS;
+    const double eps = m->p.epsilon, dt = m->p.dt;
+    double aver = is_salt ? m->S_aver : m->T_aver;
+    double *ttrhs = m->s_n1, *ttrhs_c = m->s_n2;
+    double *ttx = m->s_gr, *tty = m->s_gr + (size_t)L * m->E;
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            F3(ttfold, z, n) = -(0.5 + eps) * F3(ttfold, z, n) + (1.5 + eps) * F3(ttf, z, n);
+            F3(ttfold, z, n) = F3(ttfold, z, n) - aver;
+            F3(ttf, z, n) = F3(ttf, z, n) - aver;
+            F3(ttrhs, z, n) = 0.0;
+            F3(ttrhs_c, z, n) = 0.0;
+        }
+    tracer_gradient_elements(m, ttfold, ttx, tty);
+    fill_up_dn_grad(m, ttx, tty, g);
+    for (int edge = 1; edge <= m->Ed; ++edge) {
+        int n1 = EDN(1, edge), n2 = EDN(2, edge), e1 = EDT(1, edge), e2 = EDT(2, edge);
+        double dX1 = ECR(1, edge), dY1 = ECR(2, edge), dX2 = 0, dY2 = 0;
+        double a = WP_R_EARTH * N1(m->elem_cos, e1), b = 0.0;
+        if (e2 > 0) { dX2 = ECR(3, edge); dY2 = ECR(4, edge); b = WP_R_EARTH * N1(m->elem_cos, e2); }
+        double ex = EDXY(1, edge), ey = EDXY(2, edge);
+        for (int z = 1; z <= L; ++z) {
+            double T1 = F3(ttfold, z, n1), T2 = F3(ttfold, z, n2);
+            double Tm2 = T2 - (2.0 * (T2 - T1) + ex * a * UDG(2, z, edge) + ey * WP_R_EARTH * UDG(4, z, edge)) / 6.0;
+            double Tm1 = T1 + (2.0 * (T2 - T1) + ex * a * UDG(1, z, edge) + ey * WP_R_EARTH * UDG(3, z, edge)) / 6.0;
+            double Tmean;
+            if (F3(m->V_n_filt, z, e1) * dX1 - F3(m->U_n_filt, z, e1) * dY1 > 0)
+                Tmean = 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0;
+            else
+                Tmean = 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+            double c1 = (F3(m->Je, z, e1) * F3(m->V_n_filt, z, e1) * Tmean) * dX1
+                      - (F3(m->Je, z, e1) * F3(m->U_n_filt, z, e1) * Tmean) * dY1;
+            F3(ttrhs, z, n1) = F3(ttrhs, z, n1) + c1;
+            F3(ttrhs, z, n2) = F3(ttrhs, z, n2) - c1;
+        }
+        if (e2 > 0)
+            for (int z = 1; z <= L; ++z) {
+                double T1 = F3(ttfold, z, n1), T2 = F3(ttfold, z, n2);
+                double Tm2 = T2 - (2.0 * (T2 - T1) + ex * b * UDG(2, z, edge) + ey * WP_R_EARTH * UDG(4, z, edge)) / 6.0;
+                double Tm1 = T1 + (2.0 * (T2 - T1) + ex * b * UDG(1, z, edge) + ey * WP_R_EARTH * UDG(3, z, edge)) / 6.0;
+                double Tmean;
+                if (F3(m->V_n_filt, z, e2) * dX2 - F3(m->U_n_filt, z, e2) * dY2 < 0)
+                    Tmean = 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0;
+                else
+                    Tmean = 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+                /* second segment uses U_n / V_n, not the filtered velocity (fv_tracer.F90:158-159) */
+                double c2 = -(F3(m->Je, z, e2) * F3(m->V_n, z, e2) * Tmean) * dX2
+                          + (F3(m->Je, z, e2) * F3(m->U_n, z, e2) * Tmean) * dY2;
+                F3(ttrhs, z, n1) = F3(ttrhs, z, n1) + c2;
+                F3(ttrhs, z, n2) = F3(ttrhs, z, n2) - c2;
+            }
+    }
+    for (int edge = 1; edge <= m->Ed; ++edge) {
+        int n1 = EDN(1, edge), n2 = EDN(2, edge), e1 = EDT(1, edge), e2 = EDT(2, edge);
+        double dX1 = ECR(1, edge), dY1 = ECR(2, edge);
+        for (int z = 1; z <= L; ++z) {
+            double c1 = F3(m->Je, z, e1) * F3(m->V_n_filt, z, e1) * dX1 - F3(m->Je, z, e1) * F3(m->U_n_filt, z, e1) * dY1;
+            F3(ttrhs_c, z, n1) = F3(ttrhs_c, z, n1) + c1;
+            F3(ttrhs_c, z, n2) = F3(ttrhs_c, z, n2) - c1;
+        }
+        if (e2 > 0) {
+            double dX2 = ECR(3, edge), dY2 = ECR(4, edge);
+            for (int z = 1; z <= L; ++z) {
+                double c2 = -F3(m->Je, z, e2) * F3(m->V_n_filt, z, e2) * dX2 + F3(m->Je, z, e2) * F3(m->U_n_filt, z, e2) * dY2;
+                F3(ttrhs_c, z, n1) = F3(ttrhs_c, z, n1) + c2;
+                F3(ttrhs_c, z, n2) = F3(ttrhs_c, z, n2) - c2;
+            }
+        }
+    }
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n) {
+        double tvert[NS + 1];
+        tvert_quick(m, n, ttfold, tvert, 1);
+        for (int z = 1; z <= L; ++z) {
+            double a = F3(ttfold, z, n);
+            double aj = N1(m->area, n) * F3(m->Jc, z, n);
+            F3(ttrhs, z, n) = F3(ttrhs, z, n) / aj - a * F3(ttrhs_c, z, n) / aj
+                            + a * (W3(m->Wvel, z, n) - W3(m->Wvel, z + 1, n)) / F3(m->Jc, z, n)
+                            + (tvert[z] - tvert[z + 1]) / F3(m->Jc, z, n);
+        }
+    }
+    if (m->p.cl_relax) relax_ob(m, ttrhs, ttf, is_salt ? m->Sclim : m->Tclim, aver);
+#pragma omp parallel for
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            double t = F3(ttf, z, n);
+            F3(ttfold, z, n) = t + aver;
+            F3(ttf, z, n) = t + F3(ttrhs, z, n) * dt + aver;
+        }
+#undef UDG
+}
+
+/* tracer_impl_vert_diff, fv_tracer.F90:1319-1494 (key_atm off) */
+static void tracer_impl_vert_diff(oracle_model *m) {
+    const int L = m->L, NS = m->NS;
+    const double dt = m->p.dt, T_aver = m->T_aver, S_aver = m->S_aver;
+    int bad_s = 0, bad_t = 0;
+#pragma omp parallel for reduction(| : bad_s, bad_t)
+    for (int n = 1; n <= m->N; ++n) {
+        double a[NS + 1], b[NS + 1], c[NS + 1], tr[NS + 1], sr[NS + 1], cp[NS + 1], tp[NS + 1], sp[NS + 1];
+#define ZZ(k) F3(m->Z, k, n)
+#define ZB(k) W3(m->zbar, k, n)
+#define TT(k) F3(m->TF, k, n)
+#define SS(k) F3(m->SF, k, n)
+        for (int z = 1; z <= L; ++z) { TT(z) = TT(z) - T_aver; SS(z) = SS(z) - S_aver; }
+        for (int nz = 2; nz <= NS - 2; ++nz) {
+            a[nz] = -dt * W3(m->Kv, nz, n) / ((ZZ(nz - 1) - ZZ(nz)) * (ZB(nz) - ZB(nz + 1)));
+            c[nz] = -dt * W3(m->Kv, nz, n) / ((ZZ(nz) - ZZ(nz + 1)) * (ZB(nz) - ZB(nz + 1)));
+            b[nz] = -a[nz] - c[nz] + 1.0;
+        }
+        c[1] = -dt * W3(m->Kv, 2, n) / ((ZZ(1) - ZZ(2)) * (ZB(1) - ZB(2)));
+        a[1] = 0.0;
+        b[1] = -c[1] + 1.0;
+        a[L] = -dt * W3(m->Kv, L, n) / ((ZZ(L - 1) - ZZ(L)) * (ZB(L) - ZB(NS)));
+        b[L] = -a[L] + 1.0;
+        c[L] = 0.0;
+        tr[1] = c[1] * (-TT(2) + TT(1));
+        sr[1] = c[1] * (-SS(2) + SS(1));
+        for (int nz = 2; nz <= NS - 2; ++nz) {
+            tr[nz] = -a[nz] * TT(nz - 1) - c[nz] * TT(nz + 1) + (a[nz] + c[nz]) * TT(nz);
+            sr[nz] = -a[nz] * SS(nz - 1) - c[nz] * SS(nz + 1) + (a[nz] + c[nz]) * SS(nz);
+        }
+        tr[L] = a[L] * (TT(L) - TT(L - 1));
+        sr[L] = a[L] * (SS(L) - SS(L - 1));
+        cp[1] = c[1] / b[1];
+        tp[1] = tr[1] / b[1];
+        sp[1] = sr[1] / b[1];
+        for (int nz = 2; nz <= L; ++nz) {
+            double mm = 1.0 / (b[nz] - cp[nz - 1] * a[nz]);
+            cp[nz] = c[nz] * mm;
+            tp[nz] = (tr[nz] - tp[nz - 1] * a[nz]) * mm;
+            sp[nz] = (sr[nz] - sp[nz - 1] * a[nz]) * mm;
+        }
+        tr[L] = tp[L];
+        sr[L] = sp[L];
+        for (int nz = L - 1; nz >= 1; --nz) {
+            tr[nz] = tp[nz] - cp[nz] * tr[nz + 1];
+            sr[nz] = sp[nz] - cp[nz] * sr[nz + 1];
+        }
+        for (int nz = 1; nz <= L; ++nz) {
+            TT(nz) = TT(nz) + tr[nz] + T_aver;
+            SS(nz) = SS(nz) + sr[nz] + S_aver;
+        }
+        for (int nz = 1; nz <= L; ++nz) {
+            if (fabs(SS(nz)) < 1.0e-12) SS(nz) = fabs(SS(nz));
+            if (SS(nz) < 0.0) bad_s = 1;
+            if (TT(nz) < -3.0) bad_t = 1;
+        }
+#undef ZZ
+#undef ZB
+#undef TT
+#undef SS
+    }
+    if (bad_s) m->status |= FESOMC_ST_NEGSALT;
+    if (bad_t) m->status |= FESOMC_ST_LOWTEMP;
+}
+
+/* solve_tracers, fv_main.F90:1707-1836 */
+static void solve_tracers(oracle_model *m) {
+    const int L = m->L;
+    double tmin = F3(m->TF, 1, 1), tmax = tmin, smin = F3(m->SF, 1, 1), smax = smin;
+    for (int n = 1; n <= m->N; ++n)
+        for (int z = 1; z <= L; ++z) {
+            double t = F3(m->TF, z, n), s = F3(m->SF, z, n);
+            if (t < tmin) tmin = t;
+            if (t > tmax) tmax = t;
+            if (s < smin) smin = s;
+            if (s > smax) smax = s;
+        }
+    m->T_aver = 0.5 * (tmin + tmax);
+    m->S_aver = 0.5 * (smin + smax);
+    adv_tracer_mask(m);
+    if (m->p.tracer_adv == FESOMC_TRACER_MUSCL) {
+        double *udg = dalloc((size_t)4 * L * m->Ed);
+        solve_tracer_muscl(m, m->TF, m->T_old, 0, udg);
+        solve_tracer_muscl(m, m->SF, m->S_old, 1, udg);
+        free(udg);
+    } else if (m->p.tracer_adv == FESOMC_TRACER_UPWIND) {
+        solve_tracer_upwind(m);
+    } else if (m->p.tracer_adv == FESOMC_TRACER_MIURA) {
+        solve_tracer_miura(m, m->TF, m->T_old, 0);
+    }
+    if (m->p.key_rivers) {
+        for (int n = 1; n <= m->n_rivers; ++n)
+            for (int nz = 1; nz <= L; ++nz) {
+                int node = m->nod_rivers[n - 1];
+                double river_coeff = N1(m->runoff, n) * (SIG(nz) - SIG(nz + 1)) * m->p.dt / (N1(m->area, node) * F3(m->Jc, nz, node));
+                double river_delta = (m->p.river_salinity - F3(m->S_old, nz, node));
+                F3(m->SF, nz, node) = F3(m->SF, nz, node) + river_delta * river_coeff;
+            }
+    }
+    tracer_impl_vert_diff(m);
+}
+
+/* oce_timestep case(3), fv_main.F90:1983-2095, preceded by the time update
+ * of the main loop (fv_main.F90:400-401). */
+static void oce_timestep(oracle_model *m) {
+    m->time_jd = m->time_jd + m->p.dt / 86400.0;
+    m->time = m->time_jd * 86400.0;
+    pressure(m);
+    compute_el2nodes_3D(m, m->U_n, m->V_n, m->Unode, m->Vnode);
+    if (m->p.ver_mix == 3) d3_end(m);
+    compute_vel_rhs(m);
+    oce_barotropic_timestep(m);
+    jacobian(m);
+    update_3D_vel(m);
+    vert_vel_sigma(m);
+    solve_tracers(m);
+    for (size_t i = 0; i < (size_t)m->N; ++i)
+        if (!isfinite(m->eta_n[i])) { m->status |= FESOMC_ST_NONFINITE; break; }
+}
+
+/* energy, fv_average_dynamic.F90:476-554 (serial path) */
+double oracle_energy(oracle_model *m) {
+    double eout = 0.0, my_area = 0.0;
+    for (int n = 1; n <= m->N; ++n) {
+        eout = eout + 0.5 * WP_G * N1(m->area, n) * (N1(m->eta_n, n) * N1(m->eta_n, n));
+        my_area = my_area + N1(m->area, n);
+    }
+    double sum_ekin = 0.0;
+    for (int el = 1; el <= m->E; ++el) {
+        double s = 0.0;
+        for (int k = 1; k <= 4; ++k) s = s + WCV(k, el) * MAXD(m->p.Dmin, N1(m->depth, ELN(k, el)) + N1(m->eta_n, ELN(k, el)));
+        double u = V2(m->U_n_2D, 1, el), v = V2(m->U_n_2D, 2, el);
+        double ekin = 0.5 * s * N1(m->elem_area, el) * (u * u + v * v);
+        sum_ekin = sum_ekin + ekin;
+    }
+    return (eout + sum_ekin) / my_area;
+}
+
+/* ====================================================================== */
+/* public API                                                              */
+/* ====================================================================== */
+oracle_model *oracle_create(const fesomc_mesh *msh, const fesomc_params *par, const fesomc_state *st) {
+    oracle_model *m = (oracle_model *)calloc(1, sizeof(oracle_model));
+    if (!m) return NULL;
+    m->N = msh->nod2D; m->E = msh->elem2D; m->Ed = msh->edge2D; m->Ed_in = msh->edge2D_in;
+    m->NS = msh->nsigma; m->L = msh->nsigma - 1; m->NIE = msh->nod_in_elem2D_max;
+    m->p = *par;
+    const size_t N = m->N, E = m->E, Ed = m->Ed, L = m->L, NS = m->NS;
+    m->index_nod2D = icopy(msh->index_nod2D, N);
+    m->elem2D_nodes = icopy(msh->elem2D_nodes, 4 * E);
+    m->edge_nodes = icopy(msh->edge_nodes, 2 * Ed);
+    m->edge_tri = icopy(msh->edge_tri, 2 * Ed);
+    m->elem_edges = icopy(msh->elem_edges, 4 * E);
+    m->elem_neighbors = icopy(msh->elem_neighbors, 4 * E);
+    m->nod_in_elem2D_num = icopy(msh->nod_in_elem2D_num, N);
+    m->nod_in_elem2D = icopy(msh->nod_in_elem2D, (size_t)m->NIE * N);
+    m->edge_up_dn_tri = icopy(msh->edge_up_dn_tri, 2 * Ed);
+    m->nobn = msh->nobn;
+    m->in_obn = icopy(msh->in_obn, msh->nobn);
+    m->n_rivers = msh->n_rivers;
+    m->nod_rivers = icopy(msh->nod_rivers, msh->n_rivers);
+    m->depth = dcopy(msh->depth, N); m->area = dcopy(msh->area, N);
+    m->elem_area = dcopy(msh->elem_area, E); m->elem_cos = dcopy(msh->elem_cos, E);
+    m->coriolis = dcopy(msh->coriolis, E); m->w_cv = dcopy(msh->w_cv, 4 * E);
+    m->gradient_sca = dcopy(msh->gradient_sca, 8 * E); m->gradient_vec = dcopy(msh->gradient_vec, 8 * E);
+    m->edge_dxdy = dcopy(msh->edge_dxdy, 2 * Ed); m->edge_cross_dxdy = dcopy(msh->edge_cross_dxdy, 4 * Ed);
+    m->sigma = dcopy(msh->sigma, NS); m->a_tp = dcopy(msh->a_tp, 2 * N); m->ac = dcopy(msh->ac, N);
+#define ST(field, n) m->field = dcopy(st->field, n)
+    ST(eta_n, N); ST(eta_n_1, N); ST(eta_n_2, N); ST(etaAB, N); ST(ssh_gp, N);
+    ST(U_n_2D, 2 * E); ST(U_n_1, 2 * E); ST(U_n_2, 2 * E); ST(U_filt_2D, E); ST(V_filt_2D, E);
+    ST(U_n, L * E); ST(V_n, L * E); ST(U_rhsAB, L * E); ST(V_rhsAB, L * E); ST(U_n_filt, L * E); ST(V_n_filt, L * E);
+    ST(TF, L * N); ST(SF, L * N); ST(T_old, L * N); ST(S_old, L * N); ST(Tclim, L * N); ST(Sclim, L * N);
+    ST(bt, NS * N); ST(snu, NS * N); ST(Kv, NS * N); ST(Ri, NS * N); ST(tke_dissip, NS * N);
+    ST(Av, NS * E); ST(Wvel, NS * N); ST(mask_wd, E); ST(mask_wd_node, N);
+    ST(rho_c, L * N); ST(hpressure, NS * N); ST(Bar_pr_2D, 2 * E);
+#undef ST
+    if (!st->mask_wd) for (size_t i = 0; i < E; ++i) m->mask_wd[i] = 1.0;
+    if (!st->mask_wd_node) for (size_t i = 0; i < N; ++i) m->mask_wd_node[i] = 1.0;
+    m->ssh_rhs = dalloc(N); m->eta_p = dalloc(N); m->eta_tmp = dalloc(N);
+    m->UAB = dalloc(2 * E); m->U_rhs_2D = dalloc(2 * E); m->U_rhs_2D_3D = dalloc(2 * E);
+    m->vel_grad = dalloc(4 * E); m->dmean_n = dalloc(E);
+    m->taux = dalloc(E); m->tauy = dalloc(E); m->windx = dalloc(N); m->windy = dalloc(N);
+    m->C_d_el = dalloc(E); m->mask_ad = dalloc(N); m->mask_bpr = dalloc(E);
+    for (size_t i = 0; i < E; ++i) { m->mask_bpr[i] = 1.0; m->C_d_el[i] = par->C_d; }
+    for (size_t i = 0; i < N; ++i) m->mask_ad[i] = 1.0;
+    m->aux_elem = dalloc(E); m->c1e = dalloc(Ed);
+    m->Jc = dalloc(L * N); m->Jc_old = dalloc(L * N); m->Je = dalloc(L * E); m->Jd = dalloc(L * Ed);
+    m->Z = dalloc(L * N); m->zbar = dalloc(NS * N);
+    m->U_rhs = dalloc(L * E); m->V_rhs = dalloc(L * E);
+    m->vgux = dalloc(L * E); m->vguy = dalloc(L * E); m->vgvx = dalloc(L * E); m->vgvy = dalloc(L * E);
+    m->U_puls = dalloc(L * E); m->V_puls = dalloc(L * E);
+    m->Unode = dalloc(L * N); m->Vnode = dalloc(L * N); m->Unode_p = dalloc(L * N); m->Vnode_p = dalloc(L * N);
+    m->Bar_pru_3D = dalloc(L * E); m->Bar_prv_3D = dalloc(L * E);
+    m->runoff = dalloc(msh->n_rivers);
+    m->ampt = dalloc((size_t)msh->nobn * 12); m->fazt = dalloc((size_t)msh->nobn * 12);
+    for (int j = 0; j < 12; ++j) { m->amp_factor[j] = 1.0; m->phy_factor[j] = 0.0; }
+    size_t big = L * (E > N ? E : N);
+    if (L * Ed > big) big = L * Ed;
+    m->s_e1 = dalloc(big); m->s_e2 = dalloc(big); m->s_e3 = dalloc(big); m->s_e4 = dalloc(big);
+    m->s_n1 = dalloc(big); m->s_n2 = dalloc(big); m->s_n3 = dalloc(big); m->s_n4 = dalloc(big);
+    m->s_ed1 = dalloc(Ed); m->s_ed2 = dalloc(Ed); m->s_ed3 = dalloc(Ed); m->s_ed4 = dalloc(Ed);
+    m->s_gr = dalloc(2 * big);
+    m->lfirst = st->lfirst;
+    m->time_jd = st->time_jd;
+    /* Jc as left by the two jacobian calls before the main loop (fv_main.F90:162,362) */
+    jacobian(m);
+    jacobian(m);
+    return m;
+}
+
+int oracle_set_forcing(oracle_model *m, const fesomc_forcing *f) {
+    const size_t N = m->N, E = m->E, L = m->L;
+    if (f->taux) memcpy(m->taux, f->taux, E * 8);
+    if (f->tauy) memcpy(m->tauy, f->tauy, E * 8);
+    if (f->windx) memcpy(m->windx, f->windx, N * 8);
+    if (f->windy) memcpy(m->windy, f->windy, N * 8);
+    if (f->runoff_rivers && m->n_rivers) memcpy(m->runoff, f->runoff_rivers, (size_t)m->n_rivers * 8);
+    if (f->Tclim) memcpy(m->Tclim, f->Tclim, L * N * 8);
+    if (f->Sclim) memcpy(m->Sclim, f->Sclim, L * N * 8);
+    if (f->ampt && m->nobn) memcpy(m->ampt, f->ampt, (size_t)m->nobn * 12 * 8);
+    if (f->fazt && m->nobn) memcpy(m->fazt, f->fazt, (size_t)m->nobn * 12 * 8);
+    if (f->amp_factor) memcpy(m->amp_factor, f->amp_factor, 12 * 8);
+    if (f->phy_factor) memcpy(m->phy_factor, f->phy_factor, 12 * 8);
+    return 0;
+}
+
+int oracle_step(oracle_model *m) {
+    m->status = 0;
+    oce_timestep(m);
+    return m->status;
+}
+
+int oracle_notconv(oracle_model *m) { return m->notconv; }
+
+/* Copy state out (reference layout).  NULL destinations are skipped. */
+void oracle_get_state(oracle_model *m, fesomc_state *st) {
+    const size_t N = m->N, E = m->E, L = m->L, NS = m->NS;
+#define GT(field, n) if (st->field) memcpy(st->field, m->field, (n) * sizeof(double))
+    GT(eta_n, N); GT(eta_n_1, N); GT(eta_n_2, N); GT(etaAB, N); GT(ssh_gp, N);
+    GT(U_n_2D, 2 * E); GT(U_n_1, 2 * E); GT(U_n_2, 2 * E); GT(U_filt_2D, E); GT(V_filt_2D, E);
+    GT(U_n, L * E); GT(V_n, L * E); GT(U_rhsAB, L * E); GT(V_rhsAB, L * E); GT(U_n_filt, L * E); GT(V_n_filt, L * E);
+    GT(TF, L * N); GT(SF, L * N); GT(T_old, L * N); GT(S_old, L * N); GT(Tclim, L * N); GT(Sclim, L * N);
+    GT(bt, NS * N); GT(snu, NS * N); GT(Kv, NS * N); GT(Ri, NS * N); GT(tke_dissip, NS * N);
+    GT(Av, NS * E); GT(Wvel, NS * N); GT(mask_wd, E); GT(mask_wd_node, N);
+    GT(rho_c, L * N); GT(hpressure, NS * N); GT(Bar_pr_2D, 2 * E);
+#undef GT
+    st->lfirst = m->lfirst;
+    st->time_jd = m->time_jd;
+}
+
+/* Internal arrays for white-box tests (name -> pointer, count). */
+const double *oracle_array(oracle_model *m, const char *name, int64_t *count) {
+    const int64_t N = m->N, E = m->E, L = m->L, NS = m->NS, Ed = m->Ed;
+    struct { const char *n; const double *p; int64_t c; } t[] = {
+        {"Jc", m->Jc, L * N}, {"Jc_old", m->Jc_old, L * N}, {"Je", m->Je, L * E}, {"Jd", m->Jd, L * Ed},
+        {"Z", m->Z, L * N}, {"zbar", m->zbar, NS * N}, {"U_rhs", m->U_rhs, L * E}, {"V_rhs", m->V_rhs, L * E},
+        {"Unode", m->Unode, L * N}, {"Vnode", m->Vnode, L * N}, {"Bar_pru_3D", m->Bar_pru_3D, L * E},
+        {"Bar_prv_3D", m->Bar_prv_3D, L * E}, {"vel_grad", m->vel_grad, 4 * E}, {"UAB", m->UAB, 2 * E},
+        {"ssh_rhs", m->ssh_rhs, N}, {"U_rhs_2D_3D", m->U_rhs_2D_3D, 2 * E}, {"mask_ad", m->mask_ad, N},
+        {"vgux", m->vgux, L * E}, {"vguy", m->vguy, L * E}, {"vgvx", m->vgvx, L * E}, {"vgvy", m->vgvy, L * E},
+    };
+    for (size_t i = 0; i < sizeof(t) / sizeof(t[0]); ++i)
+        if (strcmp(t[i].n, name) == 0) { if (count) *count = t[i].c; return t[i].p; }
+    if (count) *count = 0;
+    return NULL;
+}
+
+double oracle_T_aver(oracle_model *m) { return m->T_aver; }
+double oracle_S_aver(oracle_model *m) { return m->S_aver; }
+
+void oracle_free(oracle_model *m) {
+    if (!m) return;
+    void *ptrs[] = {m->index_nod2D, m->elem2D_nodes, m->edge_nodes, m->edge_tri, m->elem_edges, m->elem_neighbors,
+                    m->nod_in_elem2D_num, m->nod_in_elem2D, m->edge_up_dn_tri, m->in_obn, m->nod_rivers,
+                    m->depth, m->area, m->elem_area, m->elem_cos, m->coriolis, m->w_cv, m->gradient_sca,
+                    m->gradient_vec, m->edge_dxdy, m->edge_cross_dxdy, m->sigma, m->a_tp, m->ac,
+                    m->eta_n, m->eta_n_1, m->eta_n_2, m->etaAB, m->ssh_rhs, m->ssh_gp, m->eta_p, m->eta_tmp,
+                    m->U_n_2D, m->U_n_1, m->U_n_2, m->UAB, m->U_rhs_2D, m->U_rhs_2D_3D, m->vel_grad, m->dmean_n,
+                    m->U_filt_2D, m->V_filt_2D, m->taux, m->tauy, m->windx, m->windy, m->C_d_el,
+                    m->mask_wd, m->mask_wd_node, m->mask_ad, m->mask_bpr, m->aux_elem, m->c1e,
+                    m->Jc, m->Jc_old, m->Je, m->Jd, m->Z, m->zbar, m->U_n, m->V_n, m->U_rhs, m->V_rhs,
+                    m->U_rhsAB, m->V_rhsAB, m->U_n_filt, m->V_n_filt, m->vgux, m->vguy, m->vgvx, m->vgvy,
+                    m->U_puls, m->V_puls, m->Unode, m->Vnode, m->Unode_p, m->Vnode_p, m->TF, m->SF,
+                    m->T_old, m->S_old, m->Tclim, m->Sclim, m->rho_c, m->hpressure, m->Bar_pru_3D,
+                    m->Bar_prv_3D, m->Bar_pr_2D, m->bt, m->snu, m->Kv, m->Av, m->Ri, m->tke_dissip, m->Wvel,
+                    m->runoff, m->ampt, m->fazt, m->s_e1, m->s_e2, m->s_e3, m->s_e4, m->s_n1, m->s_n2,
+                    m->s_n3, m->s_n4, m->s_ed1, m->s_ed2, m->s_ed3, m->s_ed4, m->s_gr};
+    for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
+    free(m);
+}

@@ -1,0 +1,108 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Used by tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py
+as the checker; never by the GPU product path.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+
+def build():
+    r = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB
+
+
+_lib = None
+
+
+def load(abi):
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        lib = C.CDLL(LIB)
+        lib.oracle_create.restype = C.c_void_p
+        lib.oracle_create.argtypes = [C.POINTER(abi.Mesh), C.POINTER(abi.Params), C.POINTER(abi.State)]
+        lib.oracle_set_forcing.restype = C.c_int
+        lib.oracle_set_forcing.argtypes = [C.c_void_p, C.POINTER(abi.Forcing)]
+        lib.oracle_step.restype = C.c_int
+        lib.oracle_step.argtypes = [C.c_void_p]
+        lib.oracle_energy.restype = C.c_double
+        lib.oracle_energy.argtypes = [C.c_void_p]
+        lib.oracle_get_state.restype = None
+        lib.oracle_get_state.argtypes = [C.c_void_p, C.POINTER(abi.State)]
+        lib.oracle_array.restype = C.POINTER(C.c_double)
+        lib.oracle_array.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]
+        lib.oracle_free.restype = None
+        lib.oracle_free.argtypes = [C.c_void_p]
+        lib.oracle_notconv.restype = C.c_int
+        lib.oracle_notconv.argtypes = [C.c_void_p]
+        lib.oracle_T_aver.restype = C.c_double
+        lib.oracle_T_aver.argtypes = [C.c_void_p]
+        lib.oracle_densityJM.restype = C.c_double
+        lib.oracle_densityJM.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
+        _lib = lib
+    return _lib
+
+
+class Oracle:
+    """One oracle model instance driven like the reference main loop."""
+
+    def __init__(self, case, abi, cases_mod):
+        self.lib = load(abi)
+        self.case, self.abi, self.cm = case, abi, cases_mod
+        self.arrays = case.new_state_arrays()
+        st = case.state_struct(self.arrays, case.params.time_jd0, lfirst=1)
+        self.h = self.lib.oracle_create(C.byref(case.mesh.c), C.byref(case.params), C.byref(st))
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+        self.time_jd = case.params.time_jd0
+        self.nstep = 0
+
+    def step(self, nsteps=1):
+        rc = 0
+        for _ in range(nsteps):
+            self.nstep += 1
+            t_next = self.cm.advance_time(self.time_jd, self.case.params.dt)
+            f = self.case.forcing_fn(self.nstep, t_next)
+            fs = self.cm.forcing_struct(f)
+            self.lib.oracle_set_forcing(self.h, C.byref(fs))
+            rc |= self.lib.oracle_step(self.h)
+            self.time_jd = t_next
+        return rc
+
+    def energy(self):
+        return self.lib.oracle_energy(self.h)
+
+    def state(self):
+        out = {k: np.empty_like(v) for k, v in self.case.state0.items()}
+        st = self.case.state_struct(out, 0.0)
+        self.lib.oracle_get_state(self.h, C.byref(st))
+        out["_time_jd"] = st.time_jd
+        return out
+
+    def array(self, name):
+        n = C.c_int64()
+        p = self.lib.oracle_array(self.h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
