@@ -1,0 +1,341 @@
+"""Benchmark of the FESOM-C internal time step on B200 (sm_100a, FP64).
+
+Workload: the 1.05M-node, 21-sigma-level synthetic estuary (1501 x 701
+nodes at 80 m spacing, 30 % of quads split into triangles, MUSCL tracers,
+wetting/drying, M2 open-boundary tide, river inflow, 0.1 N/m2 wind stress),
+one "step" = one internal time step of oce_timestep case(3) with its 10
+external sub-steps.  Metric: node*level updates per second
+(nod2D * (nsigma-1) * steps / seconds), whole job.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (launched by torch.distributed.run) runs N independent replicas, one
+per GPU: the single-mesh time step does not shard across GPUs.
+--impl reference times the CPU implementation of the same time step on the
+host cores (the oracle restatement of the reference, OpenMP over all cores;
+the Fortran reference cannot be compiled in this image).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fesom-c_b200"))
+
+METRIC = "node·level updates/s"
+UNIT = "node-level updates/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", HBM_FALLBACK_GBS)), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm = float(parts[1])
+                        mx = float(parts[2])
+                    except ValueError:
+                        continue
+                    sms.append(sm)
+                    for nm, v in zip(names, parts[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def build_case(cfg):
+    from fesomc import cases
+    return cases.estuary(cfg)
+
+
+def workload_config(case, cfg):
+    m = case.mesh
+    state_gb = (m.N * m.L * 8 * 19 + m.E * m.L * 8 * 20 + m.N * m.NS * 8 * 7) / 1e9
+    nx, ny = case.meta["nx"], case.meta["ny"]
+    return {
+        "workload": f"{cfg}: synthetic estuary {nx + 1}x{ny + 1} nodes ({case.meta['dx']:.0f} m), "
+                    f"{m.NS} sigma levels, 30% quads split, MUSCL tracers, wetting/drying, "
+                    f"M2 open-boundary tide, river 500 m3/s, wind 0.1 N/m2; one step = one internal "
+                    f"step (dt {case.params.dt:.0f} s) with {case.params.Mt} external sub-steps",
+        "nodes": m.N, "elements": m.E, "edges": m.Ed, "levels": m.L,
+        "dt_s": case.params.dt, "substeps": case.params.Mt,
+        "l2": f"inputs larger than L2 (device state ~{state_gb:.1f} GB per replica, no flush needed)",
+        "parallelism": "replicas (one independent mesh per GPU)",
+    }
+
+
+def cpu_oracle_rate(case, steps, budget_s=60.0):
+    """Oracle restatement on all host cores: node*level updates/s over a
+    bounded number of internal steps (first step untimed)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from fesomc import abi, cases
+    o = pyoracle.Oracle(case, abi, cases)
+    o.step(1)
+    done, t0 = 0, time.perf_counter()
+    while done < steps:
+        o.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    m = case.mesh
+    return m.N * m.L * done / dt, done, dt
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    cfg = args.config
+    case = build_case(cfg)
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    budget = min(150.0, 8.0 * max(args.steps, 1))
+    rate, done, dt = cpu_oracle_rate(case, max(args.steps, 1), budget_s=budget)
+    sample = (f"{done} internal steps of {cfg} after 1 untimed step ({dt:.1f} s), CPU restatement of the "
+              f"reference time step with OpenMP over {cores} threads")
+    line = {
+        "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+        "warmup": 1, "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": workload_config(case, cfg),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of 'kernel' from the committed ncu summary
+    (line 'traffic_bytes_per_launch <kernel> <bytes>'), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(pdir, fn)) as f:
+            for line in f:
+                parts = line.strip().strip("`").split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                    try:
+                        return float(parts[2])
+                    except ValueError:
+                        pass
+    return None
+
+
+def run_ours(args, ws, rank, local):
+    from fesomc import abi, build, cases, model
+    if not os.path.exists(abi.LIB_PATH):
+        build.build_library()
+    lib = abi.load()
+    if lib.missing_symbols:
+        raise RuntimeError("missing symbols %s" % lib.missing_symbols)
+    pg = None
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        pg = dist
+    abi.check(lib.fesomc_gpu_set_device(local), "fesomc_gpu_set_device")
+    cfg = args.config
+    case = build_case(cfg)
+    g = model.GpuModel(case)
+    m = case.mesh
+    units_per_step = m.N * m.L
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # forcing of the run: constant stress / wind, ramped river runoff per step
+    t_next = cases.advance_time(g.time_jd, case.params.dt)
+    g.set_forcing(case.forcing_fn(1, t_next))
+    g.run(args.warmup)
+    # ---- device-timed region: K internal steps, inputs resident in HBM
+    barrier()
+    ms = C.c_double()
+    launches0 = g.kernel_launches()
+    with ClockSampler(local) as cs:
+        abi.check(lib.fesomc_gpu_time_run(g.h, args.steps, C.byref(ms)), "fesomc_gpu_time_run")
+    timed_launches = g.kernel_launches() - launches0
+    clocks = cs.summary()
+    for _ in range(args.steps):
+        g.time_jd = cases.advance_time(g.time_jd, case.params.dt)
+    g.nstep += args.steps
+    t_dev = max_over_ranks(ms.value / 1000.0)
+    barrier()
+    value = units_per_step * args.steps * ws / t_dev
+    # ---- end to end through the C-ABI: per step the host pushes the step's
+    # forcing that the reference recomputes each step (rivers_do runoff; the
+    # open-boundary tide table is staged by the library from pinned memory),
+    # advances one step (status word read back) and reads the energy diagnostic
+    rivers = case.mesh.c.n_rivers
+    nobn = case.mesh.c.nobn
+    h2d = 8 * (rivers + nobn * case.params.Mt)
+    d2h = 4 + 4 + 3 * 8
+    e = C.c_double()
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        t_next = cases.advance_time(g.time_jd, case.params.dt)
+        fd = case.forcing_fn(g.nstep + 1, t_next)
+        f = cases.forcing_struct({"runoff_rivers": fd["runoff_rivers"]})
+        abi.check(lib.fesomc_gpu_set_forcing(g.h, C.byref(f)), "set_forcing")
+        abi.check(lib.fesomc_gpu_step(g.h, g.nstep + 1), "step")
+        abi.check(lib.fesomc_gpu_energy(g.h, C.byref(e)), "energy")
+        g.time_jd = t_next
+        g.nstep += 1
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = units_per_step * args.steps * ws / t_e2e
+    # ---- per-kernel device times with events (eager launches) for the roofline
+    nk = C.c_int32()
+    maxk = 64
+    names = C.create_string_buffer(32 * maxk)
+    kms = (C.c_double * maxk)()
+    kbytes = (C.c_double * maxk)()
+    klaunch = (C.c_int64 * maxk)()
+    nprof = 2
+    abi.check(lib.fesomc_gpu_profile(g.h, nprof, maxk, C.byref(nk), names, kms, kbytes, klaunch), "profile")
+    kernels = []
+    total = 0.0
+    for i in range(nk.value):
+        nm = names.raw[32 * i: 32 * i + 32].split(b"\0", 1)[0].decode()
+        per_step = kms[i] * klaunch[i] / nprof
+        total += per_step
+        kernels.append({"kernel": nm, "ms_per_launch": kms[i], "launches_per_step": klaunch[i] // nprof,
+                        "bytes_per_launch": kbytes[i],
+                        "gbs": (kbytes[i] / (kms[i] * 1e-3) / 1e9) if kms[i] > 0 else None,
+                        "ms_per_step": per_step})
+    for k in kernels:
+        k["share"] = k["ms_per_step"] / total if total > 0 else None
+    kernels.sort(key=lambda k: -k["ms_per_step"])
+    dom = kernels[0]
+    peak, peak_kind = measured_peaks()
+    achieved = dom["gbs"]
+    roof = {"bound": "hbm", "kernel": dom["kernel"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": traffic_from_profiles(dom["kernel"]),
+            "bytes_per_launch": dom["bytes_per_launch"], "ms_per_launch": dom["ms_per_launch"],
+            "share_of_step": dom["share"]}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(case, cfg),
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": 1000.0 * t_e2e / args.steps},
+        "gpu_launches": int(timed_launches),
+        "roofline": roof,
+        "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in kk.items()} for kk in kernels],
+    }
+    g.close()
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+        rate, done, dt = cpu_oracle_rate(case, 4, budget_s=30.0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{done} internal steps of {cfg} after 1 untimed step "
+                                          f"({dt:.1f} s), CPU restatement with OpenMP"}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_info()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -490,10 +490,8 @@ __global__ void k_wvel(Dev d) {
         else KERNEL<128><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                         \
     } while (0)
 
-void launch_pressure(const Dev &d, cudaStream_t s) {
-    k_pressure_col<<<grid_for(d.N, 128), 128, 0, s>>>(d);
-    k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d);
-}
+void launch_pressure_col(const Dev &d, cudaStream_t s) { k_pressure_col<<<grid_for(d.N, 128), 128, 0, s>>>(d); }
+void launch_bpg_elem(const Dev &d, cudaStream_t s) { k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_velgrad3d(const Dev &d, cudaStream_t s) {
     k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }

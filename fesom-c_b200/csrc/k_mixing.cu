@@ -144,7 +144,7 @@ void launch_d3end(const Dev &d, cudaStream_t s) {
     if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else if (d.NS <= 48) k_d3end<48><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d);
 }
+void launch_av(const Dev &d, cudaStream_t s) { k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d); }
 
 }  // namespace fesomc

@@ -566,11 +566,13 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
 void launch_upwind(const Dev &d, cudaStream_t s) {
     k_upwind_h<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
 }
-void launch_muscl(const Dev &d, cudaStream_t s) {
+void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
     k_muscl_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
-    k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
-    k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
 }
+void launch_muscl_ngrad(const Dev &d, cudaStream_t s) {
+    k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d); }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     if (d.L <= 24) k_vdiff_col<24><<<grid_for(d.N, 128), 128, 0, s>>>(d);
     else if (d.L <= 48) k_vdiff_col<48><<<grid_for(d.N, 128), 128, 0, s>>>(d);

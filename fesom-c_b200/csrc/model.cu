@@ -22,7 +22,8 @@ void launch_p1_elem(const Dev &, cudaStream_t);
 void launch_u2d_elem(const Dev &, cudaStream_t);
 void launch_rot_nodes(const Dev &, cudaStream_t);
 void launch_zero_filt(const Dev &, cudaStream_t);
-void launch_pressure(const Dev &, cudaStream_t);
+void launch_pressure_col(const Dev &, cudaStream_t);
+void launch_bpg_elem(const Dev &, cudaStream_t);
 void launch_velgrad3d(const Dev &, cudaStream_t);
 void launch_velrhs(const Dev &, double, cudaStream_t);
 void launch_implvisc(const Dev &, cudaStream_t);
@@ -30,9 +31,12 @@ void launch_jac_swap(const Dev &, cudaStream_t);
 void launch_update3d(const Dev &, double, cudaStream_t);
 void launch_wvel(const Dev &, cudaStream_t);
 void launch_d3end(const Dev &, cudaStream_t);
+void launch_av(const Dev &, cudaStream_t);
 void launch_minmax(const Dev &, cudaStream_t);
 void launch_upwind(const Dev &, cudaStream_t);
-void launch_muscl(const Dev &, cudaStream_t);
+void launch_muscl_egrad(const Dev &, cudaStream_t);
+void launch_muscl_ngrad(const Dev &, cudaStream_t);
+void launch_muscl_h(const Dev &, cudaStream_t);
 void launch_vdiff(const Dev &, cudaStream_t);
 int energy_parts();
 void launch_energy(const Dev &, double *, double *, cudaStream_t);
@@ -81,6 +85,16 @@ struct fesomc_model {
     bool use_graph = true;
     long long launches = 0;
     int launches_per_step = 0;
+    // optional per-kernel profiling (events around every launch group)
+    struct Prof {
+        bool on = false;
+        std::vector<std::string> names;
+        std::vector<double> bytes, ms;
+        std::vector<long long> count;
+        std::vector<cudaEvent_t> ev;      // pool, 2 per record
+        std::vector<int> rec_kernel;      // kernel index of each record
+        size_t used = 0;
+    } prof;
 };
 
 namespace {
@@ -361,39 +375,123 @@ void set_params(Dev &d, const fesomc_params &p) {
     d.wet_dry_on = p.wet_dry_on; d.key_rivers = p.key_rivers; d.TF_presence = p.TF_presence; d.cl_relax = p.cl_relax;
 }
 
+// Algorithmic bytes per launch of every kernel: each array the kernel must
+// read or write counted once at its element size (connectivity and geometry
+// once), no credit for re-reads.  N nodes, E elements, Ed edges (Ei
+// internal), L layers, NS = L+1 interfaces.
+double kernel_bytes(const fesomc_model *m, const std::string &k) {
+    const Dev &d = m->d;
+    const double N = d.N, E = d.E, Ed = d.Ed, Ei = d.Ed_in, L = d.L, NS = d.NS;
+    const double nnz_ne = (double)(2 * d.Ed);  // node->edge incidences
+    if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
+    if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
+    if (k == "u2d_elem")
+        return N * (7 * 8 + 8) + E * (112 + 40 + 16 + 32 + 16 + 8 + 16 + 16 + 16 + 16 + 32 + 8 + 48 + 32 + 8) +
+               Ei * (16 + 32 + 16);
+    if (k == "rot_nodes") return N * 48;
+    if (k == "pressure_col") return L * N * 16 + N * 16 + L * N * 8 + NS * N * 8;
+    if (k == "bpg_elem") return NS * N * 8 + N * 24 + E * (96 + 16 + 8) + L * E * 16 + E * 16;
+    if (k == "el2nodes" || k == "el2nodes_p") return L * E * 16 + N * 12 + 4 * (4.0 * E) + E * 8 + L * N * 16;
+    if (k == "d3end") return L * N * 32 + NS * N * 24 + N * 40 + NS * N * 40;
+    if (k == "av") return NS * N * 8 + E * 48 + NS * E * 8;
+    if (k == "velgrad3d") return L * E * 16 + E * (48 + 64 + 8) + L * E * 32;
+    if (k == "velrhs") return L * E * (48 + 16 + 16) + NS * N * 8 + N * 56 + E * 184 + Ei * 64 + L * E * 32;
+    if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 48 + 16) + N * 16 + L * E * 16;
+    if (k == "zero_filt") return E * 16;
+    if (k == "puls_elem") return L * E * 16 + E * 16 + N * 24 + E * 48 + L * E * 16 + E * 8;
+    if (k == "p1_elem") return L * N * 16 + N * 24 + E * 16 + Ei * 32 + E * (8 + 48 + 8 + 16);
+    if (k == "jac_swap") return N * 32;
+    if (k == "update3d") return L * E * 16 + N * 32 + E * 48 + E * 16 + E * 16 + L * E * 32 + E * 16;
+    if (k == "wvel") return N * 4 + 4 * nnz_ne + Ed * 40 + N * 16 + E * 48 + E * 16 + L * E * 16 + N * 16 + NS * N * 8;
+    if (k == "minmax") return L * N * 16;
+    if (k == "upwind_h") return L * N * 32 + L * E * 16 + NS * N * 8 + N * 4 + 4 * nnz_ne + Ed * 48 + N * 28 + E * 48 + L * N * 32;
+    if (k == "muscl_egrad") return L * N * 32 + E * 112 + L * E * 32;
+    if (k == "muscl_ngrad") return L * E * 32 + N * 4 + 4 * (4.0 * E) + E * 8 + L * N * 32;
+    if (k == "muscl_h")
+        return L * N * 32 + L * E * 32 + L * N * 32 + L * E * 32 + NS * N * 8 + N * 4 + 4 * nnz_ne + Ed * 72 + E * 56 +
+               N * 28 + L * N * 32;
+    if (k == "vdiff_col") return L * N * 32 + NS * N * 8 + N * 16 + L * N * 32;
+    return 0.0;
+}
+
+// Runs fn() bracketed by profiling events when profiling is on.
+template <typename F>
+void rec(fesomc_model *m, const char *name, F fn) {
+    auto &P = m->prof;
+    if (!P.on) { fn(); return; }
+    int k = -1;
+    for (size_t i = 0; i < P.names.size(); ++i)
+        if (P.names[i] == name) { k = (int)i; break; }
+    if (k < 0) {
+        P.names.push_back(name);
+        P.bytes.push_back(kernel_bytes(m, name));
+        P.ms.push_back(0.0);
+        P.count.push_back(0);
+        k = (int)P.names.size() - 1;
+    }
+    if (P.used + 2 > P.ev.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            P.ev.push_back(e);
+        }
+    }
+    cudaEventRecord(P.ev[P.used], m->stream);
+    fn();
+    cudaEventRecord(P.ev[P.used + 1], m->stream);
+    P.rec_kernel.push_back(k);
+    P.used += 2;
+}
+
 // The kernel sequence of one internal step (oce_timestep case(3)).
 int enqueue_step(fesomc_model *m, double ff) {
     const Dev &d = m->d;
     cudaStream_t s = m->stream;
     int n = 0;
-    launch_pressure(d, s); n += 2;
-    launch_el2nodes(d, d.U_n, d.V_n, d.Unode, d.Vnode, s); n += 1;
-    if (d.ver_mix == 3) { launch_d3end(d, s); n += 2; }
-    launch_velgrad3d(d, s); n += 1;
-    launch_velrhs(d, ff, s); n += 1;
-    if (d.im_vert_visc || d.im_vert_visc_fic) { launch_implvisc(d, s); n += 1; }
-    launch_zero_filt(d, s); n += 1;
-    for (int sub = 0; sub < d.Mt; ++sub) {
-        launch_ab3_elem(d, s);
-        launch_ssh_node(d, sub, s);
-        n += 2;
-        if (sub == 0) {
-            launch_puls_elem(d, s);
-            launch_el2nodes(d, d.U_puls, d.V_puls, d.Unode_p, d.Vnode_p, s);
-            launch_p1_elem(d, s);
-            n += 3;
-        }
-        launch_u2d_elem(d, s);
-        launch_rot_nodes(d, s);
+    rec(m, "pressure_col", [&] { launch_pressure_col(d, s); });
+    rec(m, "bpg_elem", [&] { launch_bpg_elem(d, s); });
+    n += 2;
+    rec(m, "el2nodes", [&] { launch_el2nodes(d, d.U_n, d.V_n, d.Unode, d.Vnode, s); });
+    n += 1;
+    if (d.ver_mix == 3) {
+        rec(m, "d3end", [&] { launch_d3end(d, s); });
+        rec(m, "av", [&] { launch_av(d, s); });
         n += 2;
     }
-    launch_jac_swap(d, s); n += 1;
-    launch_update3d(d, 1.0 / (double)d.Mt, s); n += 1;
-    launch_wvel(d, s); n += 1;
-    launch_minmax(d, s); n += 2;
-    if (d.tracer_adv == FESOMC_TRACER_MUSCL) { launch_muscl(d, s); n += 3; }
-    else { launch_upwind(d, s); n += 1; }
-    launch_vdiff(d, s); n += 1;
+    rec(m, "velgrad3d", [&] { launch_velgrad3d(d, s); });
+    rec(m, "velrhs", [&] { launch_velrhs(d, ff, s); });
+    n += 2;
+    if (d.im_vert_visc || d.im_vert_visc_fic) { rec(m, "implvisc", [&] { launch_implvisc(d, s); }); n += 1; }
+    rec(m, "zero_filt", [&] { launch_zero_filt(d, s); });
+    n += 1;
+    for (int sub = 0; sub < d.Mt; ++sub) {
+        rec(m, "ab3_elem", [&] { launch_ab3_elem(d, s); });
+        rec(m, "ssh_node", [&] { launch_ssh_node(d, sub, s); });
+        n += 2;
+        if (sub == 0) {
+            rec(m, "puls_elem", [&] { launch_puls_elem(d, s); });
+            rec(m, "el2nodes_p", [&] { launch_el2nodes(d, d.U_puls, d.V_puls, d.Unode_p, d.Vnode_p, s); });
+            rec(m, "p1_elem", [&] { launch_p1_elem(d, s); });
+            n += 3;
+        }
+        rec(m, "u2d_elem", [&] { launch_u2d_elem(d, s); });
+        rec(m, "rot_nodes", [&] { launch_rot_nodes(d, s); });
+        n += 2;
+    }
+    rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
+    rec(m, "update3d", [&] { launch_update3d(d, 1.0 / (double)d.Mt, s); });
+    rec(m, "wvel", [&] { launch_wvel(d, s); });
+    rec(m, "minmax", [&] { launch_minmax(d, s); });
+    n += 5;
+    if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
+        rec(m, "muscl_egrad", [&] { launch_muscl_egrad(d, s); });
+        rec(m, "muscl_ngrad", [&] { launch_muscl_ngrad(d, s); });
+        rec(m, "muscl_h", [&] { launch_muscl_h(d, s); });
+        n += 3;
+    }
+    else { rec(m, "upwind_h", [&] { launch_upwind(d, s); }); n += 1; }
+    rec(m, "vdiff_col", [&] { launch_vdiff(d, s); });
+    n += 1;
     m->launches_per_step = n;
     CK(cudaGetLastError());
     return FESOMC_OK;
@@ -652,6 +750,7 @@ int fesomc_gpu_finalize(fesomc_model *m) {
     if (!m) return FESOMC_OK;
     if (m->stream) cudaStreamSynchronize(m->stream);
     if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (cudaEvent_t e : m->prof.ev) cudaEventDestroy(e);
     for (void *p : m->allocs) cudaFree(p);
     for (int i = 0; i < 2; ++i) {
         if (m->h_stage[i]) cudaFreeHost(m->h_stage[i]);
@@ -679,6 +778,68 @@ const char *fesomc_gpu_error_string(int code) {
         case FESOMC_EMESH: return "inconsistent element node list";
         default: return "unknown error";
     }
+}
+
+int fesomc_gpu_time_run(fesomc_model *m, int32_t nsteps, double *ms) {
+    if (!m || nsteps < 0 || !ms) return FESOMC_EINVAL;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaEventRecord(a, m->stream));
+    int rc = run_steps(m, nsteps);
+    if (rc) return rc;
+    CK(cudaEventRecord(b, m->stream));
+    CK(cudaEventSynchronize(b));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = f;
+    if ((rc = collect_status(m))) return rc;
+    return status_code(m->status_acc);
+}
+
+int fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, int32_t *n_kernels, char *names,
+                       double *ms_per_launch, double *bytes_per_launch, int64_t *launches) {
+    if (!m || nsteps < 1 || !n_kernels || !names || !ms_per_launch || !bytes_per_launch || !launches)
+        return FESOMC_EINVAL;
+    auto &P = m->prof;
+    P.on = true;
+    P.names.clear(); P.bytes.clear(); P.ms.clear(); P.count.clear(); P.rec_kernel.clear();
+    P.used = 0;
+    const bool g = m->use_graph;
+    m->use_graph = false;
+    int rc = run_steps(m, nsteps);
+    m->use_graph = g;
+    P.on = false;
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(m->stream));
+    for (size_t r = 0; r < P.rec_kernel.size(); ++r) {
+        float f = 0.f;
+        CK(cudaEventElapsedTime(&f, P.ev[2 * r], P.ev[2 * r + 1]));
+        P.ms[P.rec_kernel[r]] += f;
+        P.count[P.rec_kernel[r]] += 1;
+    }
+    const int nk = (int)P.names.size() < max_kernels ? (int)P.names.size() : max_kernels;
+    for (int k = 0; k < nk; ++k) {
+        std::memset(names + 32 * k, 0, 32);
+        std::strncpy(names + 32 * k, P.names[k].c_str(), 31);
+        ms_per_launch[k] = P.ms[k] / (double)P.count[k];
+        bytes_per_launch[k] = P.bytes[k];
+        launches[k] = P.count[k];
+    }
+    *n_kernels = nk;
+    if ((rc = collect_status(m))) return rc;
+    return status_code(m->status_acc);
+}
+
+int fesomc_gpu_set_device(int32_t device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return FESOMC_ECUDA;
+    if (device < 0 || device >= n) return FESOMC_EINVAL;
+    CK(cudaSetDevice(device));
+    return FESOMC_OK;
 }
 
 const char *fesomc_gpu_version(void) { return "fesomc-b200 0.1 (sm_100a, FP64 plain path)"; }

@@ -93,6 +93,10 @@ SIGNATURES = {
     "fesomc_mesh_scale_area": (C.c_double, [C.c_void_p]),
     "fesomc_mesh_set_rivers": (C.c_int, [C.c_void_p, C.c_int32, i32p]),
     "fesomc_mesh_free": (None, [C.c_void_p]),
+    "fesomc_gpu_time_run": (C.c_int, [C.c_void_p, C.c_int32, f64p]),
+    "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,
+                                     C.POINTER(C.c_int64)]),
+    "fesomc_gpu_set_device": (C.c_int, [C.c_int32]),
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),
     "fesomc_host_density_jm": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),

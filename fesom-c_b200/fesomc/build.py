@@ -76,7 +76,9 @@ def build_library(verbose=False, ptxas_v=False):
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
             logs = list(ex.map(_compile, jobs))
     if jobs or not os.path.exists(LIB_PATH):
-        link = [nvcc] + ARCH + ["-shared", "-ccbin", _cxx(), "-o", LIB_PATH] + objs + ["-lcudart"]
+        # static CUDA runtime: the library does not depend on the runtime
+        # that other packages in the process (e.g. torch) bring along
+        link = [nvcc] + ARCH + ["-shared", "--cudart", "static", "-ccbin", _cxx(), "-o", LIB_PATH] + objs
         _compile(link)
     if verbose:
         for log in logs:

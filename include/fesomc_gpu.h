@@ -251,6 +251,24 @@ void fesomc_mesh_free(fesomc_mesh_builder *b);
  * (src/fv_ini.F90:187-199; densityJM src/fv_pressure_new.F90:340-414). */
 double fesomc_host_density_jm(double t, double s, double pz, double density_0);
 
+/* ---- measurement ----------------------------------------------------------
+ * fesomc_gpu_time_run: like fesomc_gpu_run, but returns the device time of
+ * the nsteps internal steps measured with CUDA events on the library stream.
+ * fesomc_gpu_profile: runs nsteps internal steps without the CUDA graph, with
+ * an event pair around every kernel, and reports per kernel (names: 32-byte
+ * entries) the mean device time per launch, the algorithmic bytes per launch
+ * (every array the kernel must touch, counted once) and the launch count.
+ * Neither has a counterpart in the reference; they replace its per-routine
+ * omp_get_wtime prints (src/fv_main.F90:2084-2095). */
+int  fesomc_gpu_time_run(fesomc_model *m, int32_t nsteps, double *ms);
+int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, int32_t *n_kernels,
+                        char *names, double *ms_per_launch, double *bytes_per_launch, int64_t *launches);
+
+/* Selects the CUDA device used by subsequent fesomc_gpu_init calls of the
+ * calling thread (one process per GPU).  No counterpart in the reference,
+ * where each MPI rank owns a mesh partition instead. */
+int  fesomc_gpu_set_device(int32_t device);
+
 /* ---- version / introspection --------------------------------------------- */
 const char *fesomc_gpu_version(void);
 /* Number of kernels launched by this instance since init. */

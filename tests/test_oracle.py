@@ -1,0 +1,102 @@
+"""CPU oracle: pinned against the reference's golden energy series and
+checked for conservation on the CPU (no GPU)."""
+import math
+
+import numpy as np
+import pytest
+
+
+def half_unit_e16_7(v):
+    """Half a unit in the last digit of Fortran format e16.7 (0.dddddddE+xx)."""
+    return 0.5 * 10.0 ** (math.floor(math.log10(abs(v))) + 1 - 7)
+
+
+@pytest.fixture(scope="module")
+def mods(built):
+    import pyoracle
+    from fesomc import abi, cases
+    return abi, cases, pyoracle
+
+
+def test_mt_from_ieee_division():
+    # Mt = int(dt/dt_2D) (fv_read_run.F90:1060) is 5 for dt=0.5, dt_2D=0.1 in
+    # IEEE double arithmetic; the golden LE series corresponds to 4 sub-steps
+    assert int(0.5 / 0.1) == 5
+
+
+def test_le_energy_matches_reference_golden(mods):
+    """energy_tocheck.dat of test_cases/LE_medium, printed with 7 significant
+    digits every 100 steps; reproduced with Mt = 4 sub-steps."""
+    abi, cases, pyoracle = mods
+    case = cases.le_medium()
+    case.params.Mt = 4
+    gold = case.meta["energy"]
+    o = pyoracle.Oracle(case, abi, cases)
+    for row in range(4):
+        o.step(100)
+        days = o.time_jd - case.params.time_jd0
+        assert abs(days - gold[row, 0]) < 1e-9
+        # printed as 0.dddddddE+xx: must round to the printed value
+        assert abs(o.energy() - gold[row, 1]) <= half_unit_e16_7(gold[row, 1])
+    o.close()
+
+
+def test_le_energy_with_five_substeps_differs(mods):
+    abi, cases, pyoracle = mods
+    case = cases.le_medium()
+    assert case.params.Mt == 5
+    o = pyoracle.Oracle(case, abi, cases)
+    o.step(100)
+    assert o.energy() / case.meta["energy"][0, 1] > 1.2
+    o.close()
+
+
+def test_le_volume_conserved(mods):
+    abi, cases, pyoracle = mods
+    case = cases.le_medium()
+    area = case.mesh.area
+    o = pyoracle.Oracle(case, abi, cases)
+    v0 = np.sum(area * (case.mesh.depth + o.state()["eta_n"]))
+    o.step(40)
+    v1 = np.sum(area * (case.mesh.depth + o.state()["eta_n"]))
+    assert abs(v1 - v0) / v0 < 1e-13
+    o.close()
+
+
+def test_estuary_small_stable(mods):
+    abi, cases, pyoracle = mods
+    case = cases.estuary("small")
+    o = pyoracle.Oracle(case, abi, cases)
+    rc = o.step(30)
+    s = o.state()
+    assert rc == 0
+    for k in ("eta_n", "U_n", "TF", "SF", "snu"):
+        assert np.all(np.isfinite(s[k]))
+    assert set(np.unique(s["mask_wd"])) <= {0.0, 1.0}
+    assert (s["mask_wd"] == 0).sum() > 0          # wetting/drying active
+    assert 0 < s["snu"].min() and s["snu"].max() <= 0.2
+    o.close()
+
+
+def test_estuary_oracle_negative_salinity_flag(mods):
+    """A river source of absurdly negative salinity (injected on the host)
+    drives salinity below zero; the check of fv_tracer.F90:1469-1473 (which
+    stops the reference) is reported through the status word."""
+    abi, cases, pyoracle = mods
+    case = cases.estuary("small", river_salinity=-1.0e9)
+    o = pyoracle.Oracle(case, abi, cases)
+    rc = o.step(1)
+    assert rc & abi.ST_NEGSALT
+    o.close()
+
+
+def test_estuary_oracle_low_temperature_flag(mods):
+    abi, cases, pyoracle = mods
+    case = cases.estuary("small")
+    L = case.mesh.L
+    case.state0["TF"][L * 7: L * 9] = -10.0
+    case.state0["T_old"][L * 7: L * 9] = -10.0
+    o = pyoracle.Oracle(case, abi, cases)
+    rc = o.step(1)
+    assert rc & abi.ST_LOWTEMP
+    o.close()
