@@ -71,6 +71,9 @@ struct Dev {
     double *TF, *SF, *T_old, *S_old, *Tclim, *Sclim, *rho_c;
     double *hpressure, *bt, *snu, *Kv, *Ri, *tke_dissip, *Wvel;   // NS per node
     double *Av;                                                   // NS per element
+    double *Je;                           // L per element, from eta_jac (refreshed after each jacobian)
+    double *ttfold, *stfold;              // L per node, AB2 tracer minus its mean (this step)
+    double2 *adv2d;                       // per internal edge: upwind 2D momentum flux of the sub-step
     // tracer scratch
     double *TF_adv, *SF_adv, *Told_new, *Sold_new;
     double *ttx, *tty, *stx, *sty;       // L per element (MUSCL / Miura element gradients)
@@ -142,6 +145,19 @@ __device__ __forceinline__ double density_jm(double t, double s, double pz, doub
                   + ss3 * (-R4(5.72466e-3) + t * (R4(1.02270e-4) + t * (-R4(1.65460e-6))))
                   + R4(4.8314e-4) * s * s;
     return rhopot * bulk / (bulk + 0.1 * pz) - density_0;
+}
+
+// ---- one warp per entity, lane = level ----------------------------------------
+constexpr unsigned kFull = 0xffffffffu;
+#define WARP_LOOP(ent, count)                                                                           \
+    for (long long ent = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ent < (long long)(count); \
+         ent += ((long long)gridDim.x * blockDim.x) >> 5)
+
+// acc = (((acc + v_0) + v_1) + ... + v_{n-1}) with v_j held by lane j:
+// the sequential Fortran sum, evaluated identically in every lane.
+__device__ __forceinline__ double warp_seq_sum(double acc, double v, int n) {
+    for (int j = 0; j < n; ++j) acc = acc + __shfl_sync(kFull, v, j);
+    return acc;
 }
 
 // grid-stride helper

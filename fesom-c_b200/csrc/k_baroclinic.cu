@@ -396,6 +396,18 @@ __global__ void k_jac_swap(Dev d) {
     }
 }
 
+// Je of every (element, level) from eta_jac, stored after each jacobian
+// call (fv_main.F90:1208-1267) for the kernels that gather it
+__global__ void k_je_elem(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int4 en = d.elem_nodes[e];
+        d.Je[ii] = je_of(d, d.w_cv[e], elem_jac_a(d, d.eta_jac, en), z);
+    }
+}
+
 // update_3D_vel (fv_3D_vel.F90:201-255) with the U_filt averaging of
 // oce_barotropic_timestep (fv_main.F90:1670-1677) folded in.
 template <int MAXL>
@@ -500,6 +512,7 @@ void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
 }
 void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d); }
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
+void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
 void launch_update3d(const Dev &d, double Mt_inv, cudaStream_t s) {
     MAXL_DISPATCH(k_update3d, grid_for(d.E, 128), 128, s, d, Mt_inv);
 }

@@ -118,88 +118,107 @@ __device__ __forceinline__ double tvert_upwind(const Dev &d, int k, double a, co
     return -(T(nz) * (1.0 - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
 }
 
-// ---------------------------------------------------------------------------
-// solve_tracer_upwind, one thread per (node, level)
-// ---------------------------------------------------------------------------
-__global__ void k_upwind_h(Dev d) {
+// AB2 tracers of this step minus their means, stored once per (node, level)
+// for the gathers below (fv_tracer.F90:433,435 and :39-47)
+__global__ void k_ab2_node(Dev d) {
     const long long total = (long long)d.N * d.L;
     const double T_aver = d.aver[0], S_aver = d.aver[1];
-    GRID_LOOP(ii, total) {
-        const int n = (int)(ii / d.L);
-        const int z = (int)(ii % d.L);
-        const int L = d.L, NS = d.NS;
-        double acc_t = 0.0, acc_s = 0.0, acc_c = 0.0;
-        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
-            const int code = d.node_eidx[p];
-            const int ed = code >> 1;
-            const int2 nn = d.edge_nodes[ed];
-            const int2 et = d.edge_tri[ed];
-            const double4 X = d.edge_cross[ed];
-            const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
-            const double t1 = ab2(d, d.TF, d.T_old, i1, T_aver), t2 = ab2(d, d.TF, d.T_old, i2, T_aver);
-            const double s1 = ab2(d, d.SF, d.S_old, i1, S_aver), s2 = ab2(d, d.SF, d.S_old, i2, S_aver);
-            const double4 w1 = d.w_cv[et.x];
-            const double4 a1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
-            const double J1 = je_of(d, w1, a1, z);
-            const size_t e1 = (size_t)et.x * L + z;
-            const double c1 = d.V_n_filt[e1] * X.x - d.U_n_filt[e1] * X.y;
-            double aux_c, t_aux, s_aux;
-            if (ed < d.Ed_in) {
-                const double4 w2 = d.w_cv[et.y];
-                const double4 a2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
-                const double J2 = je_of(d, w2, a2, z);
-                const size_t e2 = (size_t)et.y * L + z;
-                const double c2 = -d.V_n_filt[e2] * X.z + d.U_n_filt[e2] * X.w;
-                aux_c = J1 * c1 + J2 * c2;
-                if (c1 > 0.0 && c2 > 0.0) {
-                    t_aux = J1 * c1 * t2 + J2 * c2 * t2;
-                    s_aux = J1 * c1 * s2 + J2 * c2 * s2;
-                } else if (c1 > 0.0) {
-                    t_aux = J1 * c1 * t2 + J2 * c2 * t1;
-                    s_aux = J1 * c1 * s2 + J2 * c2 * s1;
-                } else if (c2 > 0.0) {
-                    t_aux = J1 * c1 * t1 + J2 * c2 * t2;
-                    s_aux = J1 * c1 * s1 + J2 * c2 * s2;
-                } else {
-                    t_aux = J1 * c1 * t1 + J2 * c2 * t1;
-                    s_aux = J1 * c1 * s1 + J2 * c2 * s1;
-                }
-            } else {
-                aux_c = J1 * c1;
-                if (c1 > 0.0) { t_aux = aux_c * t2; s_aux = aux_c * s2; }
-                else { t_aux = aux_c * t1; s_aux = aux_c * s1; }
-            }
-            if (code & 1) { acc_c = acc_c - aux_c; acc_t = acc_t - t_aux; acc_s = acc_s - s_aux; }
-            else { acc_c = acc_c + aux_c; acc_t = acc_t + t_aux; acc_s = acc_s + s_aux; }
-        }
-        // vertical part
+    GRID_LOOP(i, total) {
+        d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
+        d.stfold[i] = ab2(d, d.SF, d.S_old, i, S_aver);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// solve_tracer_upwind: one warp per node, lane = level.  Edge data are
+// warp-uniform (broadcast loads), level data coalesced.
+// ---------------------------------------------------------------------------
+__global__ void k_upwind_h(Dev d) {
+    const int lane = threadIdx.x & 31;
+    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    const int L = d.L, NS = d.NS;
+    WARP_LOOP(nn_, d.N) {
+        const int n = (int)nn_;
         const double a = jac_a(d, d.eta_jac, n);
         const double *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
-        auto TO = [&](int m) { return ab2(d, d.TF, d.T_old, base + m, T_aver); };
-        auto SO = [&](int m) { return ab2(d, d.SF, d.S_old, base + m, S_aver); };
-        const double tv0 = tvert_upwind(d, z, a, W, TO), tv1 = tvert_upwind(d, z + 1, a, W, TO);
-        const double sv0 = tvert_upwind(d, z, a, W, SO), sv1 = tvert_upwind(d, z + 1, a, W, SO);
         const double area_inv = 1.0 / d.area[n];
-        const double to = TO(z), so = SO(z);
-        const double jc = jc_of(d, a, z);
-        double tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
-        double sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
-        if (d.cl_relax && d.index_nod2D[n] == 2) {
-            const double vn = vel_nor(d, n);
-            if (vn > 0.0) {
-                tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (to + T_aver));
-                sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (so + S_aver));
-            } else {
-                tr = d.clim_relax * (d.Tclim[ii] - (to + T_aver));
-                sr = d.clim_relax * (d.Sclim[ii] - (so + S_aver));
+        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
+        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
+        const double vn = relax ? vel_nor(d, n) : 0.0;
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            const int zc = z < L ? z : L - 1;
+            double acc_t = 0.0, acc_s = 0.0, acc_c = 0.0;
+            for (int p = p0; p < p1; ++p) {
+                const int code = d.node_eidx[p];
+                const int ed = code >> 1;
+                const int2 nn = d.edge_nodes[ed];
+                const int2 et = d.edge_tri[ed];
+                const double4 X = d.edge_cross[ed];
+                const size_t i1 = (size_t)nn.x * L + zc, i2 = (size_t)nn.y * L + zc;
+                const double t1 = d.ttfold[i1], t2 = d.ttfold[i2];
+                const double s1 = d.stfold[i1], s2 = d.stfold[i2];
+                const size_t e1 = (size_t)et.x * L + zc;
+                const double J1 = d.Je[e1];
+                const double c1 = d.V_n_filt[e1] * X.x - d.U_n_filt[e1] * X.y;
+                double aux_c, t_aux, s_aux;
+                if (ed < d.Ed_in) {
+                    const size_t e2 = (size_t)et.y * L + zc;
+                    const double J2 = d.Je[e2];
+                    const double c2 = -d.V_n_filt[e2] * X.z + d.U_n_filt[e2] * X.w;
+                    aux_c = J1 * c1 + J2 * c2;
+                    if (c1 > 0.0 && c2 > 0.0) {
+                        t_aux = J1 * c1 * t2 + J2 * c2 * t2;
+                        s_aux = J1 * c1 * s2 + J2 * c2 * s2;
+                    } else if (c1 > 0.0) {
+                        t_aux = J1 * c1 * t2 + J2 * c2 * t1;
+                        s_aux = J1 * c1 * s2 + J2 * c2 * s1;
+                    } else if (c2 > 0.0) {
+                        t_aux = J1 * c1 * t1 + J2 * c2 * t2;
+                        s_aux = J1 * c1 * s1 + J2 * c2 * s2;
+                    } else {
+                        t_aux = J1 * c1 * t1 + J2 * c2 * t1;
+                        s_aux = J1 * c1 * s1 + J2 * c2 * s1;
+                    }
+                } else {
+                    aux_c = J1 * c1;
+                    if (c1 > 0.0) { t_aux = aux_c * t2; s_aux = aux_c * s2; }
+                    else { t_aux = aux_c * t1; s_aux = aux_c * s1; }
+                }
+                if (code & 1) { acc_c = acc_c - aux_c; acc_t = acc_t - t_aux; acc_s = acc_s - s_aux; }
+                else { acc_c = acc_c + aux_c; acc_t = acc_t + t_aux; acc_s = acc_s + s_aux; }
+            }
+            auto TO = [&](int m) { return d.ttfold[base + m]; };
+            auto SO = [&](int m) { return d.stfold[base + m]; };
+            const double tv0 = tvert_upwind(d, zc, a, W, TO), sv0 = tvert_upwind(d, zc, a, W, SO);
+            double tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
+            if (lane == 31 || zc == L - 1) {
+                tv1 = tvert_upwind(d, zc + 1, a, W, TO);
+                sv1 = tvert_upwind(d, zc + 1, a, W, SO);
+            }
+            if (z < L) {
+                const size_t ii = base + z;
+                const double to = d.ttfold[ii], so = d.stfold[ii];
+                const double jc = jc_of(d, a, z);
+                double tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
+                double sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
+                if (relax) {
+                    if (vn > 0.0) {
+                        tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (to + T_aver));
+                        sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (so + S_aver));
+                    } else {
+                        tr = d.clim_relax * (d.Tclim[ii] - (to + T_aver));
+                        sr = d.clim_relax * (d.Sclim[ii] - (so + S_aver));
+                    }
+                }
+                const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+                d.Told_new[ii] = ttf + T_aver;
+                d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+                d.Sold_new[ii] = stf + S_aver;
+                d.SF_adv[ii] = stf + sr * d.dt + S_aver;
             }
         }
-        const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
-        d.Told_new[ii] = ttf + T_aver;
-        d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
-        d.Sold_new[ii] = stf + S_aver;
-        d.SF_adv[ii] = stf + sr * d.dt + S_aver;
     }
 }
 
@@ -209,7 +228,6 @@ __global__ void k_upwind_h(Dev d) {
 // tracer_gradient_elements of the AB2 tracer, thread per (element, level)
 __global__ void k_muscl_egrad(Dev d) {
     const long long total = (long long)d.E * d.L;
-    const double T_aver = d.aver[0], S_aver = d.aver[1];
     GRID_LOOP(ii, total) {
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
@@ -217,10 +235,8 @@ __global__ void k_muscl_egrad(Dev d) {
         const int4 en = d.elem_nodes[e];
         const size_t i1 = (size_t)en.x * L + z, i2 = (size_t)en.y * L + z, i3 = (size_t)en.z * L + z,
                      i4 = (size_t)en.w * L + z;
-        const double t1 = ab2(d, d.TF, d.T_old, i1, T_aver), t2 = ab2(d, d.TF, d.T_old, i2, T_aver),
-                     t3 = ab2(d, d.TF, d.T_old, i3, T_aver), t4 = ab2(d, d.TF, d.T_old, i4, T_aver);
-        const double s1 = ab2(d, d.SF, d.S_old, i1, S_aver), s2 = ab2(d, d.SF, d.S_old, i2, S_aver),
-                     s3 = ab2(d, d.SF, d.S_old, i3, S_aver), s4 = ab2(d, d.SF, d.S_old, i4, S_aver);
+        const double t1 = d.ttfold[i1], t2 = d.ttfold[i2], t3 = d.ttfold[i3], t4 = d.ttfold[i4];
+        const double s1 = d.stfold[i1], s2 = d.stfold[i2], s3 = d.stfold[i3], s4 = d.stfold[i4];
         const double4 gx = d.gs_x[e], gy = d.gs_y[e];
         d.ttx[ii] = wsum(gx, t1, t2, t3, t4);
         d.tty[ii] = wsum(gy, t1, t2, t3, t4);
@@ -264,7 +280,7 @@ __device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, con
     if (k == NS - 1) return 0.0;
     if (k == 0) return -W[0] * TO(0);
     double Tmean = 0.0;
-    // replay interfaces 2..k+1 only for the carried Tmean when W == 0
+    // replay interfaces back to the last one with W /= 0 (carried Tmean)
     int start = k + 1;
     while (start > 2 && W[start - 1] == 0.0) --start;
     for (int nz = start; nz <= k + 1; ++nz) {
@@ -295,128 +311,118 @@ __device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, con
     return -Tmean * W[k];
 }
 
+__device__ __forceinline__ double muscl_mean(bool upw2, double Tm1, double Tm2) {
+    return upw2 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+}
+
+// edge gather + vertical + update, one warp per node, lane = level
 __global__ void k_muscl_h(Dev d) {
-    const long long total = (long long)d.N * d.L;
+    const int lane = threadIdx.x & 31;
     const double T_aver = d.aver[0], S_aver = d.aver[1];
-    GRID_LOOP(ii, total) {
-        const int n = (int)(ii / d.L);
-        const int z = (int)(ii % d.L);
-        const int L = d.L, NS = d.NS;
-        double rt = 0.0, rs = 0.0, rc = 0.0;
-        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
-            const int code = d.node_eidx[p];
-            const int ed = code >> 1;
-            const int2 nn = d.edge_nodes[ed];
-            const int2 et = d.edge_tri[ed];
-            const int2 ud = d.edge_updn[ed];
-            const double4 X = d.edge_cross[ed];
-            const double2 exy = d.edge_dxdy[ed];
-            const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
-            const double T1 = ab2(d, d.TF, d.T_old, i1, T_aver), T2 = ab2(d, d.TF, d.T_old, i2, T_aver);
-            const double S1 = ab2(d, d.SF, d.S_old, i1, S_aver), S2 = ab2(d, d.SF, d.S_old, i2, S_aver);
-            double g1, g2, g3, g4, h1, h2, h3, h4;
-            if (ud.x >= 0 && ud.y >= 0) {
-                const size_t u = (size_t)ud.x * L + z, w = (size_t)ud.y * L + z;
-                g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
-                h1 = d.stx[u]; h2 = d.stx[w]; h3 = d.sty[u]; h4 = d.sty[w];
-            } else {
-                g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
-                h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
-            }
-            const double a = kREarth * d.elem_cos[et.x];
-            const size_t e1 = (size_t)et.x * L + z;
-            const double4 w1 = d.w_cv[et.x];
-            const double4 ja1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
-            const double J1 = je_of(d, w1, ja1, z);
-            const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
-            const bool up1 = V1 * X.x - U1 * X.y > 0;
-            {
-                const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
-                const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
-                const double Tm = up1 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
-                const double c1 = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
-                const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
-                const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
-                const double Sm = up1 ? 0.15 * Sm2 + 0.85 * (Sm1 + Sm2) / 2.0 : 0.15 * Sm1 + 0.85 * (Sm1 + Sm2) / 2.0;
-                const double s1c = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
-                if (code & 1) { rt = rt - c1; rs = rs - s1c; }
-                else { rt = rt + c1; rs = rs + s1c; }
-            }
-            double cc1 = J1 * V1 * X.x - J1 * U1 * X.y;
-            if (code & 1) rc = rc - cc1;
-            else rc = rc + cc1;
-            if (et.y >= 0) {
-                const double b = kREarth * d.elem_cos[et.y];
-                const size_t e2 = (size_t)et.y * L + z;
-                const double4 w2 = d.w_cv[et.y];
-                const double4 ja2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
-                const double J2 = je_of(d, w2, ja2, z);
-                const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
-                const bool up2 = V2f * X.z - U2f * X.w < 0;
-                const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
-                const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
-                const double Tm = up2 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
-                const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
-                const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
-                const double Sm = up2 ? 0.15 * Sm2 + 0.85 * (Sm1 + Sm2) / 2.0 : 0.15 * Sm1 + 0.85 * (Sm1 + Sm2) / 2.0;
-                // second segment uses U_n / V_n (fv_tracer.F90:158-159)
-                const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
-                const double c2 = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
-                const double s2c = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
-                if (code & 1) { rt = rt - c2; rs = rs - s2c; }
-                else { rt = rt + c2; rs = rs + s2c; }
-            }
-        }
-        // ttrhs_c: separate accumulator filled in a second edge loop in the
-        // reference; same per-node order, so it is the rc sum above except
-        // that the second segment contribution must follow the first of the
-        // same edge -- recompute it in edge order here.
-        rc = 0.0;
-        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
-            const int code = d.node_eidx[p];
-            const int ed = code >> 1;
-            const int2 et = d.edge_tri[ed];
-            const double4 X = d.edge_cross[ed];
-            const size_t e1 = (size_t)et.x * L + z;
-            const double J1 = je_of(d, d.w_cv[et.x], elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]), z);
-            const double c1 = J1 * d.V_n_filt[e1] * X.x - J1 * d.U_n_filt[e1] * X.y;
-            if (code & 1) rc = rc - c1;
-            else rc = rc + c1;
-            if (et.y >= 0) {
-                const size_t e2 = (size_t)et.y * L + z;
-                const double J2 = je_of(d, d.w_cv[et.y], elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]), z);
-                const double c2 = -J2 * d.V_n_filt[e2] * X.z + J2 * d.U_n_filt[e2] * X.w;
-                if (code & 1) rc = rc - c2;
-                else rc = rc + c2;
-            }
-        }
-        const double a = jac_a(d, d.eta_jac, n);
+    const int L = d.L, NS = d.NS;
+    WARP_LOOP(nn_, d.N) {
+        const int n = (int)nn_;
+        const double an = jac_a(d, d.eta_jac, n);
         const double *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
-        auto TO = [&](int m) { return ab2(d, d.TF, d.T_old, base + m, T_aver); };
-        auto SO = [&](int m) { return ab2(d, d.SF, d.S_old, base + m, S_aver); };
-        const double tv0 = tvert_muscl(d, z, a, W, TO), tv1 = tvert_muscl(d, z + 1, a, W, TO);
-        const double sv0 = tvert_muscl(d, z, a, W, SO), sv1 = tvert_muscl(d, z + 1, a, W, SO);
-        const double jc = jc_of(d, a, z);
-        const double aj = d.area[n] * jc;
-        const double to = TO(z), so = SO(z);
-        double tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
-        double sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
-        const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
-        if (d.cl_relax && d.index_nod2D[n] == 2) {
-            const double vn = vel_nor(d, n);
-            if (vn > 0.0) {
-                tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
-                sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
-            } else {
-                tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
-                sr = d.clim_relax * (d.Sclim[ii] - (stf + S_aver));
+        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
+        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
+        const double vn = relax ? vel_nor(d, n) : 0.0;
+        const double area = d.area[n];
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            const int zc = z < L ? z : L - 1;
+            double rt = 0.0, rs = 0.0, rc = 0.0;
+            for (int p = p0; p < p1; ++p) {
+                const int code = d.node_eidx[p];
+                const int ed = code >> 1;
+                const int2 nn = d.edge_nodes[ed];
+                const int2 et = d.edge_tri[ed];
+                const int2 ud = d.edge_updn[ed];
+                const double4 X = d.edge_cross[ed];
+                const double2 exy = d.edge_dxdy[ed];
+                const size_t i1 = (size_t)nn.x * L + zc, i2 = (size_t)nn.y * L + zc;
+                const double T1 = d.ttfold[i1], T2 = d.ttfold[i2];
+                const double S1 = d.stfold[i1], S2 = d.stfold[i2];
+                double g1, g2, g3, g4, h1, h2, h3, h4;
+                if (ud.x >= 0 && ud.y >= 0) {
+                    const size_t u = (size_t)ud.x * L + zc, w = (size_t)ud.y * L + zc;
+                    g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
+                    h1 = d.stx[u]; h2 = d.stx[w]; h3 = d.sty[u]; h4 = d.sty[w];
+                } else {
+                    g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
+                    h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
+                }
+                const double a = kREarth * d.elem_cos[et.x];
+                const size_t e1 = (size_t)et.x * L + zc;
+                const double J1 = d.Je[e1];
+                const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+                const bool up1 = V1 * X.x - U1 * X.y > 0;
+                {
+                    const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
+                    const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
+                    const double Tm = muscl_mean(up1, Tm1, Tm2);
+                    const double c1 = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
+                    const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
+                    const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
+                    const double Sm = muscl_mean(up1, Sm1, Sm2);
+                    const double s1c = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
+                    const double cc1 = J1 * V1 * X.x - J1 * U1 * X.y;
+                    if (code & 1) { rt = rt - c1; rs = rs - s1c; rc = rc - cc1; }
+                    else { rt = rt + c1; rs = rs + s1c; rc = rc + cc1; }
+                }
+                if (et.y >= 0) {
+                    const double b = kREarth * d.elem_cos[et.y];
+                    const size_t e2 = (size_t)et.y * L + zc;
+                    const double J2 = d.Je[e2];
+                    const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
+                    const bool up2 = V2f * X.z - U2f * X.w < 0;
+                    const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
+                    const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
+                    const double Tm = muscl_mean(up2, Tm1, Tm2);
+                    const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
+                    const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
+                    const double Sm = muscl_mean(up2, Sm1, Sm2);
+                    // second segment uses U_n / V_n (fv_tracer.F90:158-159)
+                    const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
+                    const double c2 = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
+                    const double s2c = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
+                    const double cc2 = -J2 * V2f * X.z + J2 * U2f * X.w;
+                    if (code & 1) { rt = rt - c2; rs = rs - s2c; rc = rc - cc2; }
+                    else { rt = rt + c2; rs = rs + s2c; rc = rc + cc2; }
+                }
+            }
+            auto TO = [&](int m) { return d.ttfold[base + m]; };
+            auto SO = [&](int m) { return d.stfold[base + m]; };
+            const double tv0 = tvert_muscl(d, zc, an, W, TO), sv0 = tvert_muscl(d, zc, an, W, SO);
+            double tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
+            if (lane == 31 || zc == L - 1) {
+                tv1 = tvert_muscl(d, zc + 1, an, W, TO);
+                sv1 = tvert_muscl(d, zc + 1, an, W, SO);
+            }
+            if (z < L) {
+                const size_t ii = base + z;
+                const double jc = jc_of(d, an, z);
+                const double aj = area * jc;
+                const double to = d.ttfold[ii], so = d.stfold[ii];
+                double tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
+                double sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
+                const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+                if (relax) {
+                    if (vn > 0.0) {
+                        tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                        sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
+                    } else {
+                        tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
+                        sr = d.clim_relax * (d.Sclim[ii] - (stf + S_aver));
+                    }
+                }
+                d.Told_new[ii] = ttf + T_aver;
+                d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+                d.Sold_new[ii] = stf + S_aver;
+                d.SF_adv[ii] = stf + sr * d.dt + S_aver;
             }
         }
-        d.Told_new[ii] = ttf + T_aver;
-        d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
-        d.Sold_new[ii] = stf + S_aver;
-        d.SF_adv[ii] = stf + sr * d.dt + S_aver;
     }
 }
 
@@ -563,16 +569,16 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
     k_minmax_part<<<kRedGrid, kRedBlock, 0, s>>>(d);
     k_minmax_final<<<1, 32, 0, s>>>(d, kRedGrid);
 }
-void launch_upwind(const Dev &d, cudaStream_t s) {
-    k_upwind_h<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
-}
+static int warp_grid(long long entities, int block) { return grid_for(entities * 32, block); }
+void launch_ab2(const Dev &d, cudaStream_t s) { k_ab2_node<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d); }
+void launch_upwind(const Dev &d, cudaStream_t s) { k_upwind_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
 void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
     k_muscl_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_muscl_ngrad(const Dev &d, cudaStream_t s) {
     k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
 }
-void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d); }
+void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     if (d.L <= 24) k_vdiff_col<24><<<grid_for(d.N, 128), 128, 0, s>>>(d);
     else if (d.L <= 48) k_vdiff_col<48><<<grid_for(d.N, 128), 128, 0, s>>>(d);

@@ -28,6 +28,8 @@ void launch_velgrad3d(const Dev &, cudaStream_t);
 void launch_velrhs(const Dev &, double, cudaStream_t);
 void launch_implvisc(const Dev &, cudaStream_t);
 void launch_jac_swap(const Dev &, cudaStream_t);
+void launch_je(const Dev &, cudaStream_t);
+void launch_ab2(const Dev &, cudaStream_t);
 void launch_update3d(const Dev &, double, cudaStream_t);
 void launch_wvel(const Dev &, cudaStream_t);
 void launch_d3end(const Dev &, cudaStream_t);
@@ -338,10 +340,10 @@ int alloc_state(fesomc_model *m) {
     for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
     if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
     double **le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
-                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv};
+                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv, &d.Je};
     for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
     double **ln[] = {&d.Unode, &d.Vnode, &d.Unode_p, &d.Vnode_p, &d.TF, &d.SF, &d.T_old, &d.S_old, &d.Tclim,
-                     &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new};
+                     &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new, &d.ttfold, &d.stfold};
     for (auto p : ln) if ((rc = dalloc(m, p, L * N))) return rc;
     if (m->p.tracer_adv == FESOMC_TRACER_MUSCL || m->p.tracer_adv == FESOMC_TRACER_MIURA) {
         double **lg[] = {&d.ttx, &d.tty, &d.stx, &d.sty};
@@ -404,12 +406,18 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     if (k == "update3d") return L * E * 16 + N * 32 + E * 48 + E * 16 + E * 16 + L * E * 32 + E * 16;
     if (k == "wvel") return N * 4 + 4 * nnz_ne + Ed * 40 + N * 16 + E * 48 + E * 16 + L * E * 16 + N * 16 + NS * N * 8;
     if (k == "minmax") return L * N * 16;
-    if (k == "upwind_h") return L * N * 32 + L * E * 16 + NS * N * 8 + N * 4 + 4 * nnz_ne + Ed * 48 + N * 28 + E * 48 + L * N * 32;
-    if (k == "muscl_egrad") return L * N * 32 + E * 112 + L * E * 32;
+    if (k == "je_elem") return N * 16 + E * 48 + L * E * 8;
+    if (k == "ab2_node") return L * N * 32 + L * N * 16;
+    // tracer gathers: AB2 tracers (2 per node level), Je and transports per
+    // element level, W per node interface, T/S of the node, edge geometry,
+    // and the four outputs per node level
+    if (k == "upwind_h")
+        return L * N * 16 + L * E * 24 + NS * N * 8 + L * N * 16 + N * 28 + 4 * nnz_ne + Ed * 48 + L * N * 32;
+    if (k == "muscl_egrad") return L * N * 16 + E * 80 + L * E * 32;
     if (k == "muscl_ngrad") return L * E * 32 + N * 4 + 4 * (4.0 * E) + E * 8 + L * N * 32;
     if (k == "muscl_h")
-        return L * N * 32 + L * E * 32 + L * N * 32 + L * E * 32 + NS * N * 8 + N * 4 + 4 * nnz_ne + Ed * 72 + E * 56 +
-               N * 28 + L * N * 32;
+        return L * N * 16 + L * E * 32 + L * N * 32 + L * E * 40 + NS * N * 8 + L * N * 16 + N * 28 + 4 * nnz_ne +
+               Ed * 72 + E * 8 + L * N * 32;
     if (k == "vdiff_col") return L * N * 32 + NS * N * 8 + N * 16 + L * N * 32;
     return 0.0;
 }
@@ -479,10 +487,12 @@ int enqueue_step(fesomc_model *m, double ff) {
         n += 2;
     }
     rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
+    rec(m, "je_elem", [&] { launch_je(d, s); });
     rec(m, "update3d", [&] { launch_update3d(d, 1.0 / (double)d.Mt, s); });
     rec(m, "wvel", [&] { launch_wvel(d, s); });
     rec(m, "minmax", [&] { launch_minmax(d, s); });
-    n += 5;
+    rec(m, "ab2_node", [&] { launch_ab2(d, s); });
+    n += 7;
     if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
         rec(m, "muscl_egrad", [&] { launch_muscl_egrad(d, s); });
         rec(m, "muscl_ngrad", [&] { launch_muscl_ngrad(d, s); });
@@ -649,6 +659,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice) ||
         cudaMemcpy(m->d.eta_jac_old, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice))
         return fail(FESOMC_ECUDA);
+    launch_je(m->d, m->stream);
+    if (cudaGetLastError() != cudaSuccess) return fail(FESOMC_ECUDA);
     m->lfirst = st->lfirst;
     m->time_jd = st->time_jd;
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(FESOMC_ECUDA);
