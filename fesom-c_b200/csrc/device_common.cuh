@@ -13,9 +13,11 @@
 //     sorted by the reference edge number, so every node / element receives
 //     its contributions in the same order as the serial Fortran loop and the
 //     FP64 sums are bit-identical (compiled with --fmad=false).
-//   * Jc, Je, Jd, Z, zbar (subroutine jacobian, fv_main.F90:1208-1267) are
-//     not stored: they are recomputed with the same expressions from the
-//     elevation at the last jacobian call (eta_jac) and sigma.
+//   * Jc, Jd, Z, zbar (subroutine jacobian, fv_main.F90:1208-1267) are not
+//     stored: they are recomputed with the same expressions from the
+//     elevation at the last jacobian call (eta_jac) and sigma.  The element
+//     quantities Je and the w_cv-weighted Z / zbar, which every element
+//     kernel needs at every level, are stored once per jacobian call.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -71,8 +73,15 @@ struct Dev {
     double *TF, *SF, *T_old, *S_old, *Tclim, *Sclim, *rho_c;
     double *hpressure, *bt, *snu, *Kv, *Ri, *tke_dissip, *Wvel;   // NS per node
     double *Av;                                                   // NS per element
-    double *Je;                           // L per element, from eta_jac (refreshed after each jacobian)
+    // element-level Jacobian quantities from eta_jac, refreshed by update3d
+    // right after each jacobian call (and once at init):
+    double *Je;                           // Je(k,e)                    L per element
+    double *Ze;                           // SUM(w_cv*Z(k,nodes))       L per element
+    double *ZBe;                          // SUM(w_cv*zbar(k,nodes))    L per element (interfaces 1..L)
     double *ttfold, *stfold;              // L per node, AB2 tracer minus its mean (this step)
+    // MUSCL segment fluxes per (edge, level): (first, second segment) of
+    // the T flux, the S flux and the continuity term
+    double2 *mflT, *mflS, *mflC;
     double2 *adv2d;                       // per internal edge: upwind 2D momentum flux of the sub-step
     // tracer scratch
     double *TF_adv, *SF_adv, *Told_new, *Sold_new;
@@ -153,11 +162,26 @@ constexpr unsigned kFull = 0xffffffffu;
     for (long long ent = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ent < (long long)(count); \
          ent += ((long long)gridDim.x * blockDim.x) >> 5)
 
+// levels handled by the chunk of 32 starting at z0
+__device__ __forceinline__ int chunk_len(int L, int z0) { return L - z0 < 32 ? L - z0 : 32; }
+
 // acc = (((acc + v_0) + v_1) + ... + v_{n-1}) with v_j held by lane j:
 // the sequential Fortran sum, evaluated identically in every lane.
 __device__ __forceinline__ double warp_seq_sum(double acc, double v, int n) {
     for (int j = 0; j < n; ++j) acc = acc + __shfl_sync(kFull, v, j);
     return acc;
+}
+
+// inclusive sequential prefix: lane j receives acc + v_0 + ... + v_j (left
+// to right); acc is advanced past all n values in every lane.
+__device__ __forceinline__ double warp_seq_scan(double &acc, double v, int n) {
+    const int lane = threadIdx.x & 31;
+    double mine = 0.0;
+    for (int j = 0; j < n; ++j) {
+        acc = acc + __shfl_sync(kFull, v, j);
+        if (lane == j) mine = acc;
+    }
+    return mine;
 }
 
 // grid-stride helper

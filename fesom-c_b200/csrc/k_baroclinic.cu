@@ -9,29 +9,39 @@
 //                  filter viscosity, QUICK vertical advection
 //   implvisc     : implicit vertical viscosity per element column
 //                  (momentum_vert_impl_visc_tmp / momentum_vert_impl_visc)
-//   update3d     : update_3D_vel per element column
+//   update3d     : update_3D_vel per element column; stores the new Je, Ze, ZBe
 //   wvel         : vert_vel_sigma per node column (edge gather + reverse scan)
 //   jac_swap     : jacobian bookkeeping (eta at the previous / last call)
+//   je_elem      : Je, Ze, ZBe at init
 #include "device_common.cuh"
 
 namespace fesomc {
 
 // ---------------------------------------------------------------------------
-// pressure (fv_pressure_new.F90:91-107): one thread per node column
+// pressure (fv_pressure_new.F90:91-107): one warp per node column, lane =
+// level; density in parallel, the hydrostatic sum as an ordered warp scan
 // ---------------------------------------------------------------------------
 __global__ void k_pressure_col(Dev d) {
     const double gd0 = kG / d.density_0;
-    GRID_LOOP(ii, d.N) {
-        const int n = (int)ii;
-        const int L = d.L, NS = d.NS;
+    const int lane = threadIdx.x & 31;
+    const int L = d.L, NS = d.NS;
+    WARP_LOOP(ent, d.N) {
+        const int n = (int)ent;
         const double a = jac_a(d, d.eta_jac, n);
+        const size_t bl = (size_t)n * L, bs = (size_t)n * NS;
         double hp = 0.0;
-        d.hpressure[(size_t)n * NS] = 0.0;
-        for (int z = 0; z < L; ++z) {
-            const double rho = density_jm(d.TF[(size_t)n * L + z], d.SF[(size_t)n * L + z], -z_of(d, a, z), d.density_0);
-            d.rho_c[(size_t)n * L + z] = rho;
-            hp = hp + rho * jc_of(d, a, z) * gd0;
-            d.hpressure[(size_t)n * NS + z + 1] = hp;
+        if (lane == 0) d.hpressure[bs] = 0.0;
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            const bool ok = z < L;
+            const int zc = ok ? z : L - 1;
+            const double rho = density_jm(d.TF[bl + zc], d.SF[bl + zc], -z_of(d, a, zc), d.density_0);
+            const double t = rho * jc_of(d, a, zc) * gd0;
+            const double mine = warp_seq_scan(hp, t, chunk_len(L, z0));
+            if (ok) {
+                d.rho_c[bl + z] = rho;
+                d.hpressure[bs + z + 1] = mine;
+            }
         }
     }
 }
@@ -53,9 +63,10 @@ __global__ void k_bpg_elem(Dev d) {
         const double fac = d.elem_bpfac[e];
         const double4 ae = elem_jac_a(d, d.eta_jac, en);
         const double an[4] = {ae.x, ae.y, ae.z, ae.w};
+        const double *je_e = d.Je + (size_t)e * L;
         double b1 = 0.0, b2 = 0.0;
         for (int z = 0; z < L; ++z) {
-            const double je = je_of(d, w, ae, z);
+            const double je = je_e[z];
             const double accJe_inv = -fac / je;
             double hu[4], hl[4], pre[4];
             for (int k = 0; k < 4; ++k) {
@@ -135,9 +146,10 @@ __device__ __forceinline__ double wsum_z(const Dev &d, const double4 &w, const d
 }
 
 // Vertical momentum flux uvertAB(:,k) of momentum_vert_adv_upwind at interface
-// k (0-based, 0..NS-1) of element e (fv_advection.F90:389-443).
-__device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const double4 &w, const double4 &a,
-                                         const int4 &en, double ar, double &fu, double &fv) {
+// k (0-based, 0..NS-1) of element e (fv_advection.F90:389-443); the element
+// means of Z and zbar come from the stored Ze / ZBe.
+__device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const double4 &w, const int4 &en, double ar,
+                                         double &fu, double &fv) {
     const int L = d.L, NS = d.NS;
     const double *U = d.U_n + (size_t)e * L;
     const double *V = d.V_n + (size_t)e * L;
@@ -145,6 +157,8 @@ __device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const doubl
     const double wv = wsum_col(w, d.Wvel, NS, en, k) * ar;
     if (k == 0) { fu = -wv * U[0]; fv = -wv * V[0]; return; }
     const int nz = k + 1;  // 1-based interface index, 2..NS-1
+    const double *ZE = d.Ze + (size_t)e * L;   // ZE[m-1] = SUM(w*Z(m))
+    const double *ZB = d.ZBe + (size_t)e * L;  // ZB[m-1] = SUM(w*zbar(m))
     double umean = 0.0, vmean = 0.0;
     // U_n(m) 1-based  ->  U[m-1]
     if (wv >= 0.0) {
@@ -152,10 +166,10 @@ __device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const doubl
             umean = 0.5 * (U[nz - 2] + U[nz - 1]);
             vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
         } else {
-            const double Z1 = wsum_zbar(d, w, a, nz - 1);
-            const double aa = Z1 - wsum_z(d, w, a, nz - 2);
-            const double bb = wsum_z(d, w, a, nz - 1) - Z1;
-            const double cc = wsum_z(d, w, a, nz) - Z1;
+            const double Z1 = ZB[nz - 1];
+            const double aa = Z1 - ZE[nz - 2];
+            const double bb = ZE[nz - 1] - Z1;
+            const double cc = ZE[nz] - Z1;
             const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
             const double dg = aa * bb * (aa + bb) / dd;
             const double db = -aa * cc * (aa + cc) / dd;
@@ -169,10 +183,10 @@ __device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const doubl
             umean = 0.5 * (U[nz - 2] + U[nz - 1]);
             vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
         } else {
-            const double Z1 = wsum_zbar(d, w, a, nz - 1);
-            const double aa = wsum_z(d, w, a, nz - 1) - Z1;
-            const double bb = Z1 - wsum_z(d, w, a, nz - 2);
-            const double cc = Z1 - wsum_z(d, w, a, nz - 3);
+            const double Z1 = ZB[nz - 1];
+            const double aa = ZE[nz - 1] - Z1;
+            const double bb = Z1 - ZE[nz - 2];
+            const double cc = Z1 - ZE[nz - 3];
             const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
             const double dg = aa * bb * (aa + bb) / dd;
             const double db = -aa * cc * (aa + cc) / dd;
@@ -186,12 +200,18 @@ __device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const doubl
 }
 
 // ---------------------------------------------------------------------------
-// velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180) for one (element, level).
+// velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
+// level) with levels on consecutive lanes.  The loop runs over whole warps so
+// that the vertical flux at interface z+1 comes from the next lane.
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
 // ---------------------------------------------------------------------------
 __global__ void k_velrhs(Dev d, double ff) {
     const long long total = (long long)d.E * d.L;
-    GRID_LOOP(ii, total) {
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
+        const bool valid = wbase + lane < total;
+        const long long ii = valid ? wbase + lane : total - 1;
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
@@ -199,8 +219,7 @@ __global__ void k_velrhs(Dev d, double ff) {
         const int nd[4] = {en.x, en.y, en.z, en.w};
         const double4 w = d.w_cv[e];
         const double ar = d.elem_area[e];
-        const double4 ae = elem_jac_a(d, d.eta_jac, en);
-        const double je = je_of(d, w, ae, z);
+        const double je = d.Je[ii];
         // pressure force from eta_n
         double pre[4];
         for (int k = 0; k < 4; ++k)
@@ -256,14 +275,17 @@ __global__ void k_velrhs(Dev d, double ff) {
             ur = ur + d.tau_inv_filt * u1 * ar * je;
             vr = vr + d.tau_inv_filt * v1 * ar * je;
         }
-        // vertical advection (fv_advection.F90:354-469)
+        // vertical advection (fv_advection.F90:354-469): flux at interface z
+        // here, at z+1 from the next lane (same element) or computed
         const double mwd = d.mask_wd[e];
         if (d.vert_adv == 1) {
+            double fu0, fv0;
+            uvert_at(d, e, z, w, en, ar, fu0, fv0);
+            double fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
+            if (z == L - 1) { fu1 = 0.0; fv1 = 0.0; }
+            else if (lane == 31) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
             if (mwd != 0.0) {
                 const double acc = d.elem_acc[e];
-                double fu0, fv0, fu1, fv1;
-                uvert_at(d, e, z, w, ae, en, ar, fu0, fv0);
-                uvert_at(d, e, z + 1, w, ae, en, ar, fu1, fv1);
                 uab = uab + (fu0 - fu1) * acc;
                 vab = vab + (fv0 - fv1) * acc;
             } else {
@@ -271,12 +293,14 @@ __global__ void k_velrhs(Dev d, double ff) {
                 vab = 0.0;
             }
         }
-        d.U_rhsAB[ii] = uab;
-        d.V_rhsAB[ii] = vab;
-        const double area_inv = 1.0 / ar;
-        const double dt = d.dt;
-        d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + 0.0) / je);
-        d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + 0.0) / je);
+        if (valid) {
+            d.U_rhsAB[ii] = uab;
+            d.V_rhsAB[ii] = vab;
+            const double area_inv = 1.0 / ar;
+            const double dt = d.dt;
+            d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + 0.0) / je);
+            d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + 0.0) / je);
+        }
     }
 }
 
@@ -293,18 +317,13 @@ __global__ void k_implvisc(Dev d) {
         double *vr = d.V_rhs + (size_t)e * L;
         const double *Av = d.Av + (size_t)e * NS;
         const double mwd = d.mask_wd[e];
-        const int4 en = d.elem_nodes[e];
-        const double4 w = d.w_cv[e];
-        const double4 ae = elem_jac_a(d, d.eta_jac, en);
         const double dt = d.dt;
         const double ub = d.U_n[(size_t)e * L + L - 1], vb = d.V_n[(size_t)e * L + L - 1];
         const double a_Cd = d.C_d * ((1.0 - d.elem_acc[e]) * d.Cd_bz + 1.0);
-        double je[MAXL];
-        for (int z = 0; z < L; ++z) je[z] = je_of(d, w, ae, z);
+        const double *je = d.Je + (size_t)e * L;
         if (d.im_vert_visc) {
             double a[MAXL], b[MAXL], c[MAXL], cp[MAXL], up[MAXL], vp[MAXL], uu[MAXL], vv[MAXL];
-            double zc[MAXL];
-            for (int z = 0; z < L; ++z) zc[z] = wsum_z(d, w, ae, z);
+            const double *zc = d.Ze + (size_t)e * L;
             for (int z = 1; z <= L - 2; ++z) {
                 const double zinv = dt / je[z];
                 a[z] = -Av[z] / (zc[z] - zc[z - 1]) * zinv;
@@ -396,113 +415,120 @@ __global__ void k_jac_swap(Dev d) {
     }
 }
 
-// Je of every (element, level) from eta_jac, stored after each jacobian
-// call (fv_main.F90:1208-1267) for the kernels that gather it
+// Je, Ze, ZBe of every (element, level) from eta_jac (jacobian,
+// fv_main.F90:1208-1267); at init, afterwards refreshed by update3d
 __global__ void k_je_elem(Dev d) {
     const long long total = (long long)d.E * d.L;
     GRID_LOOP(ii, total) {
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
-        const int4 en = d.elem_nodes[e];
-        d.Je[ii] = je_of(d, d.w_cv[e], elem_jac_a(d, d.eta_jac, en), z);
+        const double4 w = d.w_cv[e];
+        const double4 a = elem_jac_a(d, d.eta_jac, d.elem_nodes[e]);
+        d.Je[ii] = je_of(d, w, a, z);
+        d.Ze[ii] = wsum_z(d, w, a, z);
+        d.ZBe[ii] = wsum_zbar(d, w, a, z);
     }
 }
 
 // update_3D_vel (fv_3D_vel.F90:201-255) with the U_filt averaging of
-// oce_barotropic_timestep (fv_main.F90:1670-1677) folded in.
-template <int MAXL>
+// oce_barotropic_timestep (fv_main.F90:1670-1677) folded in; one warp per
+// element, lane = level.  Runs right after the jacobian call: the stored Je
+// still holds the previous jacobian (Jc_old), and is replaced here by the
+// new Je / Ze / ZBe.
 __global__ void k_update3d(Dev d, double Mt_inv) {
-    GRID_LOOP(ii, d.E) {
-        const int e = (int)ii;
-        const int L = d.L;
+    const int lane = threadIdx.x & 31;
+    const int L = d.L;
+    WARP_LOOP(ent, d.E) {
+        const int e = (int)ent;
         const int4 en = d.elem_nodes[e];
         const double4 w = d.w_cv[e];
-        const double4 ao = elem_jac_a(d, d.eta_jac_old, en);
         const double4 an = elem_jac_a(d, d.eta_jac, en);
-        double a[MAXL];
-        for (int z = 0; z < L; ++z) a[z] = je_of(d, w, ao, z);
+        const size_t base = (size_t)e * L;
         const double dmean_inv = 1.0 / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
                                                         d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
-        const double *ur = d.U_rhs + (size_t)e * L;
-        const double *vr = d.V_rhs + (size_t)e * L;
         double su = 0.0, sv = 0.0;
-        for (int z = 0; z < L; ++z) su = su + ur[z] * a[z];
-        for (int z = 0; z < L; ++z) sv = sv + vr[z] * a[z];
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            const int zc = z < L ? z : L - 1;
+            const double a = d.Je[base + zc];
+            const int n = chunk_len(L, z0);
+            su = warp_seq_sum(su, d.U_rhs[base + zc] * a, n);
+            sv = warp_seq_sum(sv, d.V_rhs[base + zc] * a, n);
+        }
         const double U2p = su * dmean_inv, V2p = sv * dmean_inv;
         const double uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
         const double vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
-        d.U_filt_2D[e] = uf;
-        d.V_filt_2D[e] = vf;
         const double2 u2 = d.U_n_2D[e];
-        for (int z = 0; z < L; ++z) {
-            const double az = a[z] / je_of(d, w, an, z);
-            const size_t i = (size_t)e * L + z;
-            d.U_n_filt[i] = az * ur[z] + uf - U2p;
-            d.V_n_filt[i] = az * vr[z] + vf - V2p;
-            d.U_n[i] = az * ur[z] + u2.x - U2p;
-            d.V_n[i] = az * vr[z] + u2.y - V2p;
+        __syncwarp();
+        if (lane == 0) {
+            d.U_filt_2D[e] = uf;
+            d.V_filt_2D[e] = vf;
+        }
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            if (z >= L) continue;
+            const size_t i = base + z;
+            const double jn = je_of(d, w, an, z);
+            const double az = d.Je[i] / jn;
+            const double ur = d.U_rhs[i], vr = d.V_rhs[i];
+            d.U_n_filt[i] = az * ur + uf - U2p;
+            d.V_n_filt[i] = az * vr + vf - V2p;
+            d.U_n[i] = az * ur + u2.x - U2p;
+            d.V_n[i] = az * vr + u2.y - V2p;
+            d.Je[i] = jn;
+            d.Ze[i] = wsum_z(d, w, an, z);
+            d.ZBe[i] = wsum_zbar(d, w, an, z);
         }
     }
 }
 
-// vert_vel_sigma (fv_3D_vel.F90:309-456): per node, gather the layer
-// transport divergence over the node's edges in edge order, then the
-// reverse prefix sum over levels and the division by the area.
-template <int MAXL>
+// vert_vel_sigma (fv_3D_vel.F90:309-456): one warp per node, lane = level;
+// the layer transport divergence is gathered over the node's edges in edge
+// order, then summed upward from the bottom as an ordered warp scan.
 __global__ void k_wvel(Dev d) {
-    GRID_LOOP(ii, d.N) {
-        const int n = (int)ii;
-        const int L = d.L, NS = d.NS;
-        double W[MAXL + 1];
-        for (int z = 0; z < L; ++z) W[z] = 0.0;
-        for (int p = d.node_eptr[n]; p < d.node_eptr[n + 1]; ++p) {
-            const int code = d.node_eidx[p];
-            const int ed = code >> 1;
-            const int2 et = d.edge_tri[ed];
-            const double4 X = d.edge_cross[ed];
-            const double4 a1 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.x]);
-            const double4 w1 = d.w_cv[et.x];
-            const double uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
-            const bool internal = ed < d.Ed_in;
-            double4 a2 = a1, w2 = w1;
-            double uf2 = 0.0, vf2 = 0.0;
-            if (internal) {
-                a2 = elem_jac_a(d, d.eta_jac, d.elem_nodes[et.y]);
-                w2 = d.w_cv[et.y];
-                uf2 = d.U_filt_2D[et.y];
-                vf2 = d.V_filt_2D[et.y];
-            }
-            for (int z = 0; z < L; ++z) {
-                const size_t i1 = (size_t)et.x * L + z;
-                double c1 = je_of(d, w1, a1, z) * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
-                if (internal) {
-                    const size_t i2 = (size_t)et.y * L + z;
-                    c1 = c1 + je_of(d, w2, a2, z) * (-(d.V_n_filt[i2] - vf2) * X.z + (d.U_n_filt[i2] - uf2) * X.w);
-                }
-                if (code & 1) W[z] = W[z] - c1;
-                else W[z] = W[z] + c1;
-            }
-        }
+    const int lane = threadIdx.x & 31;
+    const int L = d.L, NS = d.NS;
+    WARP_LOOP(ent, d.N) {
+        const int n = (int)ent;
+        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
         const double area_inv = 1.0 / d.area[n];
         double *Wn = d.Wvel + (size_t)n * NS;
         double below = Wn[NS - 1];
-        for (int z = L - 1; z >= 0; --z) {
-            below = W[z] + below;
-            W[z] = below;
+        for (int z0 = ((L - 1) / 32) * 32; z0 >= 0; z0 -= 32) {
+            const int z = z0 + lane;
+            const bool ok = z < L;
+            const int zc = ok ? z : L - 1;
+            double W = 0.0;
+            for (int p = p0; p < p1; ++p) {
+                const int code = d.node_eidx[p];
+                const int ed = code >> 1;
+                const int2 et = d.edge_tri[ed];
+                const double4 X = d.edge_cross[ed];
+                const double uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
+                const size_t i1 = (size_t)et.x * L + zc;
+                double c1 = d.Je[i1] * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
+                if (ed < d.Ed_in) {
+                    const double uf2 = d.U_filt_2D[et.y], vf2 = d.V_filt_2D[et.y];
+                    const size_t i2 = (size_t)et.y * L + zc;
+                    c1 = c1 + d.Je[i2] * (-(d.V_n_filt[i2] - vf2) * X.z + (d.U_n_filt[i2] - uf2) * X.w);
+                }
+                if (code & 1) W = W - c1;
+                else W = W + c1;
+            }
+            // below = W(z) + below, from the bottom level upward
+            double mine = 0.0;
+            for (int j = chunk_len(L, z0) - 1; j >= 0; --j) {
+                below = __shfl_sync(kFull, W, j) + below;
+                if (lane == j) mine = below;
+            }
+            if (ok) Wn[z] = mine * area_inv;
         }
-        for (int z = 0; z < L; ++z) Wn[z] = W[z] * area_inv;
     }
 }
 
 // ---- launch wrappers --------------------------------------------------------
-#define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
-    do {                                                                                   \
-        if (d.L <= 24) KERNEL<24><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                \
-        else if (d.L <= 48) KERNEL<48><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);           \
-        else KERNEL<128><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                         \
-    } while (0)
-
-void launch_pressure_col(const Dev &d, cudaStream_t s) { k_pressure_col<<<grid_for(d.N, 128), 128, 0, s>>>(d); }
+static int warp_grid(long long entities, int block) { return grid_for(entities * 32, block); }
+void launch_pressure_col(const Dev &d, cudaStream_t s) { k_pressure_col<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
 void launch_bpg_elem(const Dev &d, cudaStream_t s) { k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_velgrad3d(const Dev &d, cudaStream_t s) {
     k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
@@ -510,12 +536,18 @@ void launch_velgrad3d(const Dev &d, cudaStream_t s) {
 void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
     k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
 }
+#define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
+    do {                                                                                   \
+        if (d.L <= 24) KERNEL<24><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                \
+        else if (d.L <= 48) KERNEL<48><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);           \
+        else KERNEL<128><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                         \
+    } while (0)
 void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d); }
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
 void launch_update3d(const Dev &d, double Mt_inv, cudaStream_t s) {
-    MAXL_DISPATCH(k_update3d, grid_for(d.E, 128), 128, s, d, Mt_inv);
+    k_update3d<<<warp_grid(d.E, 128), 128, 0, s>>>(d, Mt_inv);
 }
-void launch_wvel(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_wvel, grid_for(d.N, 128), 128, s, d); }
+void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
 
 }  // namespace fesomc

@@ -168,7 +168,8 @@ __global__ void k_el2nodes(Dev d, const double *Ue, const double *Ve, double *Un
 
 // momentum_adv_P1_3D_to_2D (fv_advection.F90:676-793) gathered per element,
 // optional viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939), divided by
-// dmean_n (fv_main.F90:1504-1513).
+// dmean_n (fv_main.F90:1504-1513).  One thread per element; the level sums
+// run in level order.
 __global__ void k_p1_elem(Dev d) {
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
@@ -176,8 +177,7 @@ __global__ void k_p1_elem(Dev d) {
         double rx = 0.0, ry = 0.0;
         const int4 il = d.elem_iedges[e];
         const int codes[4] = {il.x, il.y, il.z, il.w};
-        const double4 ae = elem_jac_a(d, d.eta_jac, d.elem_nodes[e]);
-        const double4 we = d.w_cv[e];
+        const double *je_e = d.Je + (size_t)e * L;
         for (int c = 0; c < 4; ++c) {
             const int code = codes[c];
             if (code < 0) break;
@@ -195,7 +195,7 @@ __global__ void k_p1_elem(Dev d) {
                 const double vv = 0.5 * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
                 const double jd = 0.5 * (jc_of(d, a1, z) + jc_of(d, a2, z));
                 const double un = (uu * ye - vv * xe) * jd;
-                const double je = je_of(d, we, ae, z);
+                const double je = je_e[z];
                 s_u = s_u + uu * un * je;
                 s_v = s_v + vv * un * je;
             }
@@ -207,23 +207,15 @@ __global__ void k_p1_elem(Dev d) {
             const int4 nb = d.elem_nb[e];
             const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
             const int jend = (en.x == en.w) ? 3 : 4;
-            double anb[4][4];
-            for (int j = 0; j < jend; ++j)
-                if (nbs[j] >= 0) {
-                    const double4 t = elem_jac_a(d, d.eta_jac, d.elem_nodes[nbs[j]]);
-                    anb[j][0] = t.x; anb[j][1] = t.y; anb[j][2] = t.z; anb[j][3] = t.w;
-                }
             const double tau = d.tau_inv_filt, ar = d.elem_area[e];
             for (int z = 0; z < L; ++z) {
-                const double je = je_of(d, we, ae, z);
+                const double je = je_e[z];
                 const double up = d.U_puls[(size_t)e * L + z], vp = d.V_puls[(size_t)e * L + z];
                 double u1 = 0.0, v1 = 0.0;
                 for (int j = 0; j < jend; ++j) {
                     const int ne = nbs[j];
                     if (ne < 0) continue;
-                    const double4 wn = d.w_cv[ne];
-                    const double4 an = make_double4(anb[j][0], anb[j][1], anb[j][2], anb[j][3]);
-                    const double jn = je_of(d, wn, an, z);
+                    const double jn = d.Je[(size_t)ne * L + z];
                     u1 = u1 + d.U_puls[(size_t)ne * L + z] * jn - up * je;
                     v1 = v1 + d.V_puls[(size_t)ne * L + z] * jn - vp * je;
                 }

@@ -7,6 +7,139 @@
 
 namespace fesomc {
 
+// d3_end, fully unrolled for a compile-time level count: the iterated state
+// (btr, xx1, yy1) stays in registers, the iteration-independent terms of
+// each level in shared memory ([term][level][thread]).  One thread per node
+// column.
+template <int NS, int BD>
+__global__ void __launch_bounds__(BD) k_d3end_r(Dev d) {
+    extern __shared__ double sm[];
+    double *col = sm + threadIdx.x;
+#define PRM(a, k) col[((a) * NS + (k)) * BD]
+    enum { SN = 0, PB, QB, C2, AM, CM };
+    constexpr int L = NS - 1;
+    const double t_inv = 1.0 / d.dt;
+    const double cka = d.cka;
+    const double B1cka2 = 16.6 * (cka * cka);
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        const double *bt = d.bt + (size_t)node * NS;
+        const double *snu = d.snu + (size_t)node * NS;
+        const double *Kv = d.Kv + (size_t)node * NS;
+        const double *Un = d.Unode + (size_t)node * L;
+        const double *Vn = d.Vnode + (size_t)node * L;
+        const double *T = d.TF + (size_t)node * L;
+        const double *S = d.SF + (size_t)node * L;
+        double *Ri = d.Ri + (size_t)node * NS;
+        double *tke = d.tke_dissip + (size_t)node * NS;
+        const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const double dmean2 = dmean * dmean;
+        const double ajac = jac_a(d, d.eta_jac, node);
+        // arrays indexed 1..NS like the Fortran ones
+        double btr[NS + 1], xx1[NS + 1], yy1[NS + 1];
+#pragma unroll
+        for (int nz = 1; nz <= NS; ++nz) btr[nz] = bt[nz - 1];
+        Ri[0] = 0.0;
+        Ri[NS - 1] = 0.0;
+#pragma unroll
+        for (int nz = 2; nz <= NS - 1; ++nz) {
+            const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+            const double d1 = s_m - s_0;
+            const double d2 = s_0 - s_p;
+            const double dd = 0.5 * (d1 + d2);
+            const double sn_m = snu[nz - 2], sn_0 = snu[nz - 1], sn_p = snu[nz];
+            double ap1 = Un[nz - 2] - Un[nz - 1];
+            const double ap2 = Vn[nz - 2] - Vn[nz - 1];
+            double b1 = sn_0 * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            b1 = b1 / dmean2;
+            const double zb = zbar_of(d, ajac, nz - 1);
+            const double rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
+            const double rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
+            ap1 = (rho_up - rho_dn) / dd;
+            const double b2 = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const double snu_p = 0.5 * (sn_m + sn_0);
+            const double snu_m = 0.5 * (sn_0 + sn_p);
+            double c2 = 0.5 * 0.73 * (snu_p * (btr[nz - 1] - btr[nz]) / d1 - snu_m * (btr[nz] - btr[nz + 1]) / d2) / dd;
+            c2 = c2 / dmean2;
+            if (b1 > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn_0;
+            else Ri[nz - 1] = 10000.0;
+            PRM(SN, nz) = sn_0;
+            PRM(PB, nz) = -b1 - b2;
+            PRM(QB, nz) = t_inv * btr[nz];
+            PRM(C2, nz) = c2;
+            PRM(AM, nz) = 0.5 * (snu_p * 0.73) / (dmean2 * d1 * dd);
+            PRM(CM, nz) = 0.5 * (snu_m * 0.73) / (dmean2 * d2 * dd);
+        }
+        xx1[2] = 1.0;
+        {
+            const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const double wx = d.windx[node], wy = d.windy[node];
+            const double u_din_sur = 0.05 * (wx * wx + wy * wy);
+            const double snu_m = 0.5 * (snu[NS - 1] + snu[NS - 2]);
+            yy1[2] = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
+        }
+        const double delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const double lg = log(delta_b / d.z0b_min);
+        const double bott_R = B1cka2 / (lg * lg);
+        const double ubt = Un[L - 1], vbt = Vn[L - 1];
+        const double bot = bott_R * (ubt * ubt + vbt * vbt);
+        bool converged = false;
+        for (int it = 1; it <= 200; ++it) {
+#pragma unroll
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const double b = btr[nz], sn = PRM(SN, nz);
+                const double c1 = 0.046 * (b * b) / sn;
+                if (it == 200) tke[nz - 1] = c1;
+                const double fr = PRM(PB, nz) - c1 - PRM(QB, nz) - PRM(C2, nz);
+                const double am = PRM(AM, nz), cm = PRM(CM, nz);
+                const double bm = am + cm + (2.0 * 0.046 * b) / sn + t_inv;
+                const double a = bm - am * xx1[nz];
+                xx1[nz + 1] = cm / a;
+                yy1[nz + 1] = (am * yy1[nz] - fr) / a;
+            }
+            double btr1[NS + 1];
+            btr1[NS] = bot;
+#pragma unroll
+            for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
+            double bbb_max = 0.0;
+#pragma unroll
+            for (int nz = 1; nz <= NS; ++nz) {
+                const double c = fabs((btr[nz] - btr1[nz]) / (dmax(btr1[nz], btr[nz]) + 1.0e-8));
+                if (c > bbb_max) bbb_max = c;
+            }
+            if (bbb_max < 1.0e-6) { converged = true; break; }
+#pragma unroll
+            for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
+        }
+        if (converged) {
+#pragma unroll
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / PRM(SN, nz);
+        } else {
+            atomicAdd(d.notconv, 1);
+        }
+        double *btw = d.bt + (size_t)node * NS;
+        double *snw = d.snu + (size_t)node * NS;
+        double *Kvw = d.Kv + (size_t)node * NS;
+#pragma unroll
+        for (int nz = 1; nz <= NS; ++nz) {
+            const double btn = dmax(btr[nz], 1.0e-8);
+            btw[nz - 1] = btn;
+            const double zt = __ldg(d.sig + nz - 1) * dmean;
+            const double Zh = zt + d.z0b_min;
+            const double Zd = fabs(dmean - zt) + d.z0s_min;
+            const double Z0 = 1.0 - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const double scale_t = cka * Zh * Zd * Z0 / dmean;
+            double s = scale_t * sqrt(btn) + d.snul;
+            if (s >= 0.2) s = 0.2;
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+#undef PRM
+}
+constexpr int kD3Terms = 6;
+
+// Generic level count: per-column arrays in local memory.
 template <int MAXNS>
 __global__ void k_d3end(Dev d) {
     const double t_inv = 1.0 / d.dt;
@@ -140,8 +273,18 @@ __global__ void k_av(Dev d) {
     }
 }
 
+template <int NS>
+static size_t d3end_r_smem() { return (size_t)kD3Terms * NS * 64 * sizeof(double); }
+int config_d3end(const Dev &d) {
+    cudaError_t e = cudaSuccess;
+    if (d.NS == 11) e = cudaFuncSetAttribute(k_d3end_r<11, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d3end_r_smem<11>());
+    if (d.NS == 21) e = cudaFuncSetAttribute(k_d3end_r<21, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d3end_r_smem<21>());
+    return e == cudaSuccess ? 0 : 1;
+}
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    if (d.NS == 11) k_d3end_r<11, 64><<<grid_for(d.N, 64), 64, d3end_r_smem<11>(), s>>>(d);
+    else if (d.NS == 21) k_d3end_r<21, 64><<<grid_for(d.N, 64), 64, d3end_r_smem<21>(), s>>>(d);
+    else if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else if (d.NS <= 48) k_d3end<48><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
 }

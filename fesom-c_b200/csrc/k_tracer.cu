@@ -5,7 +5,8 @@
 //                 open-boundary relaxation, AB2 update (T and S together)
 //   muscl_*     : solve_tracer_muscl (fv_tracer.F90:8-379) for T and S:
 //                 element gradients, node-averaged gradients
-//                 (fill_up_dn_grad fallback), edge gather + vertical + update
+//                 (fill_up_dn_grad fallback), segment fluxes per (edge,
+//                 level), node gather in edge order + vertical + update
 //   vdiff_col   : river salinity source + tracer_impl_vert_diff
 //                 (fv_tracer.F90:1319-1494) per node column, with the
 //                 negative-salinity / low-temperature checks as status bits
@@ -315,7 +316,78 @@ __device__ __forceinline__ double muscl_mean(bool upw2, double Tm1, double Tm2) 
     return upw2 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
 }
 
-// edge gather + vertical + update, one warp per node, lane = level
+// MUSCL segment fluxes of one (edge, level) (fv_tracer.F90:59-170 for T and
+// S, :172-209 for the continuity term); thread per (edge, level), levels on
+// consecutive threads.  Each flux is computed once here and gathered by both
+// end nodes below.
+__global__ void k_muscl_edge(Dev d) {
+    const long long total = (long long)d.Ed * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const int2 ud = d.edge_updn[ed];
+        const double4 X = d.edge_cross[ed];
+        const double2 exy = d.edge_dxdy[ed];
+        const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
+        const double T1 = d.ttfold[i1], T2 = d.ttfold[i2];
+        const double S1 = d.stfold[i1], S2 = d.stfold[i2];
+        double g1, g2, g3, g4, h1, h2, h3, h4;
+        if (ud.x >= 0 && ud.y >= 0) {
+            const size_t u = (size_t)ud.x * L + z, w = (size_t)ud.y * L + z;
+            g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
+            h1 = d.stx[u]; h2 = d.stx[w]; h3 = d.sty[u]; h4 = d.sty[w];
+        } else {
+            g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
+            h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
+        }
+        double2 fT, fS, fC;
+        {
+            const double a = kREarth * d.elem_cos[et.x];
+            const size_t e1 = (size_t)et.x * L + z;
+            const double J1 = d.Je[e1];
+            const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+            const bool up1 = V1 * X.x - U1 * X.y > 0;
+            const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
+            const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
+            const double Tm = muscl_mean(up1, Tm1, Tm2);
+            fT.x = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
+            const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
+            const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
+            const double Sm = muscl_mean(up1, Sm1, Sm2);
+            fS.x = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
+            fC.x = J1 * V1 * X.x - J1 * U1 * X.y;
+        }
+        if (et.y >= 0) {
+            const double b = kREarth * d.elem_cos[et.y];
+            const size_t e2 = (size_t)et.y * L + z;
+            const double J2 = d.Je[e2];
+            const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
+            const bool up2 = V2f * X.z - U2f * X.w < 0;
+            const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
+            const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
+            const double Tm = muscl_mean(up2, Tm1, Tm2);
+            const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
+            const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
+            const double Sm = muscl_mean(up2, Sm1, Sm2);
+            // second segment uses U_n / V_n (fv_tracer.F90:158-159)
+            const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
+            fT.y = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
+            fS.y = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
+            fC.y = -J2 * V2f * X.z + J2 * U2f * X.w;
+        } else {
+            fT.y = 0.0; fS.y = 0.0; fC.y = 0.0;
+        }
+        d.mflT[ii] = fT;
+        d.mflS[ii] = fS;
+        d.mflC[ii] = fC;
+    }
+}
+
+// node gather of the edge fluxes in edge order + vertical + update, one
+// warp per node, lane = level
 __global__ void k_muscl_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const double T_aver = d.aver[0], S_aver = d.aver[1];
@@ -336,60 +408,15 @@ __global__ void k_muscl_h(Dev d) {
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
-                const int2 nn = d.edge_nodes[ed];
-                const int2 et = d.edge_tri[ed];
-                const int2 ud = d.edge_updn[ed];
-                const double4 X = d.edge_cross[ed];
-                const double2 exy = d.edge_dxdy[ed];
-                const size_t i1 = (size_t)nn.x * L + zc, i2 = (size_t)nn.y * L + zc;
-                const double T1 = d.ttfold[i1], T2 = d.ttfold[i2];
-                const double S1 = d.stfold[i1], S2 = d.stfold[i2];
-                double g1, g2, g3, g4, h1, h2, h3, h4;
-                if (ud.x >= 0 && ud.y >= 0) {
-                    const size_t u = (size_t)ud.x * L + zc, w = (size_t)ud.y * L + zc;
-                    g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
-                    h1 = d.stx[u]; h2 = d.stx[w]; h3 = d.sty[u]; h4 = d.sty[w];
+                const size_t i = (size_t)ed * L + zc;
+                const double2 fT = d.mflT[i], fS = d.mflS[i], fC = d.mflC[i];
+                const bool internal = ed < d.Ed_in;
+                if (code & 1) {
+                    rt = rt - fT.x; rs = rs - fS.x; rc = rc - fC.x;
+                    if (internal) { rt = rt - fT.y; rs = rs - fS.y; rc = rc - fC.y; }
                 } else {
-                    g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
-                    h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
-                }
-                const double a = kREarth * d.elem_cos[et.x];
-                const size_t e1 = (size_t)et.x * L + zc;
-                const double J1 = d.Je[e1];
-                const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
-                const bool up1 = V1 * X.x - U1 * X.y > 0;
-                {
-                    const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
-                    const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
-                    const double Tm = muscl_mean(up1, Tm1, Tm2);
-                    const double c1 = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
-                    const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
-                    const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
-                    const double Sm = muscl_mean(up1, Sm1, Sm2);
-                    const double s1c = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
-                    const double cc1 = J1 * V1 * X.x - J1 * U1 * X.y;
-                    if (code & 1) { rt = rt - c1; rs = rs - s1c; rc = rc - cc1; }
-                    else { rt = rt + c1; rs = rs + s1c; rc = rc + cc1; }
-                }
-                if (et.y >= 0) {
-                    const double b = kREarth * d.elem_cos[et.y];
-                    const size_t e2 = (size_t)et.y * L + zc;
-                    const double J2 = d.Je[e2];
-                    const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
-                    const bool up2 = V2f * X.z - U2f * X.w < 0;
-                    const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
-                    const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
-                    const double Tm = muscl_mean(up2, Tm1, Tm2);
-                    const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
-                    const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
-                    const double Sm = muscl_mean(up2, Sm1, Sm2);
-                    // second segment uses U_n / V_n (fv_tracer.F90:158-159)
-                    const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
-                    const double c2 = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
-                    const double s2c = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
-                    const double cc2 = -J2 * V2f * X.z + J2 * U2f * X.w;
-                    if (code & 1) { rt = rt - c2; rs = rs - s2c; rc = rc - cc2; }
-                    else { rt = rt + c2; rs = rs + s2c; rc = rc + cc2; }
+                    rt = rt + fT.x; rs = rs + fS.x; rc = rc + fC.x;
+                    if (internal) { rt = rt + fT.y; rs = rs + fS.y; rc = rc + fC.y; }
                 }
             }
             auto TO = [&](int m) { return d.ttfold[base + m]; };
@@ -426,89 +453,112 @@ __global__ void k_muscl_h(Dev d) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// rivers + tracer_impl_vert_diff, one thread per node column
-// ---------------------------------------------------------------------------
-template <int MAXL>
-__global__ void k_vdiff_col(Dev d) {
+// Tracer after advection and the river source, minus its mean: T(k) / S(k)
+// of tracer_impl_vert_diff.  The river source (fv_main.F90:1804-1823) adds
+// its terms to S in river-list order.
+__device__ __forceinline__ double vd_salt(const Dev &d, int n, size_t base, int z, double aj, double S_aver) {
+    double S = d.SF_adv[base + z];
+    if (d.key_rivers) {
+        for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) {
+            const double r = d.runoff[d.node_ridx[p]];
+            const double coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
+            const double delta = (d.river_salinity - d.Sold_new[base + z]);
+            S = S + delta * coeff;
+        }
+    }
+    return S - S_aver;
+}
+
+// Tridiagonal coefficients a(k), b(k), c(k) of layer k (0-based) of node
+// column n (fv_tracer.F90:1380-1420).
+__device__ __forceinline__ void vd_coef(const Dev &d, const double *Kv, double aj, int k, double &a, double &b,
+                                        double &c) {
+    const int L = d.L, NS = d.NS;
+    const double dt = d.dt;
+    auto Zc = [&](int m) { return z_of(d, aj, m); };
+    auto ZBc = [&](int m) { return zbar_of(d, aj, m); };
+    if (k == 0) {
+        c = -dt * Kv[1] / ((Zc(0) - Zc(1)) * (ZBc(0) - ZBc(1)));
+        a = 0.0;
+        b = -c + 1.0;
+    } else if (k == L - 1) {
+        a = -dt * Kv[L - 1] / ((Zc(L - 2) - Zc(L - 1)) * (ZBc(L - 1) - ZBc(NS - 1)));
+        b = -a + 1.0;
+        c = 0.0;
+    } else {
+        a = -dt * Kv[k] / ((Zc(k - 1) - Zc(k)) * (ZBc(k) - ZBc(k + 1)));
+        c = -dt * Kv[k] / ((Zc(k) - Zc(k + 1)) * (ZBc(k) - ZBc(k + 1)));
+        b = -a - c + 1.0;
+    }
+}
+
+// rivers + tracer_impl_vert_diff (fv_tracer.F90:1319-1494), one thread per
+// node column.  The sweep coefficients live in shared memory
+// ([array][level][thread]); T and S are re-read instead of stored.
+constexpr int kVdBlock = 128;
+__global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
+    extern __shared__ double sm[];
     const double T_aver = d.aver[0], S_aver = d.aver[1];
+    const int L = d.L, NS = d.NS;
+    double *col = sm + threadIdx.x;
+    const int bd = blockDim.x;
+    auto CP = [&](int k) -> double & { return col[((size_t)0 * L + k) * bd]; };
+    auto TP = [&](int k) -> double & { return col[((size_t)1 * L + k) * bd]; };
+    auto SP = [&](int k) -> double & { return col[((size_t)2 * L + k) * bd]; };
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
-        const int L = d.L, NS = d.NS;
         const size_t base = (size_t)n * L;
         const double aj = jac_a(d, d.eta_jac, n);
-        double T[MAXL], S[MAXL], So[MAXL];
-        for (int z = 0; z < L; ++z) {
-            T[z] = d.TF_adv[base + z];
-            S[z] = d.SF_adv[base + z];
-            So[z] = d.Sold_new[base + z];
-        }
-        if (d.key_rivers) {
-            for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) {
-                const double r = d.runoff[d.node_ridx[p]];
-                for (int z = 0; z < L; ++z) {
-                    const double coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
-                    const double delta = (d.river_salinity - So[z]);
-                    S[z] = S[z] + delta * coeff;
-                }
-            }
-        }
-        for (int z = 0; z < L; ++z) { T[z] = T[z] - T_aver; S[z] = S[z] - S_aver; }
         const double *Kv = d.Kv + (size_t)n * NS;
-        const double dt = d.dt;
-        double a[MAXL], b[MAXL], c[MAXL], tr[MAXL], sr[MAXL];
-        double Zc[MAXL], ZBc[MAXL + 1];
-        for (int z = 0; z < L; ++z) Zc[z] = z_of(d, aj, z);
-        for (int z = 0; z < NS; ++z) ZBc[z] = zbar_of(d, aj, z);
-        // 1-based nz -> 0-based index nz-1
-        for (int nz = 2; nz <= NS - 2; ++nz) {
-            const int k = nz - 1;
-            a[k] = -dt * Kv[nz - 1] / ((Zc[k - 1] - Zc[k]) * (ZBc[k] - ZBc[k + 1]));
-            c[k] = -dt * Kv[nz - 1] / ((Zc[k] - Zc[k + 1]) * (ZBc[k] - ZBc[k + 1]));
-            b[k] = -a[k] - c[k] + 1.0;
+        auto Tz = [&](int z) { return d.TF_adv[base + z] - T_aver; };
+        auto Sz = [&](int z) { return vd_salt(d, n, base, z, aj, S_aver); };
+        // forward elimination; the right-hand side of layer k uses T(k-1..k+1)
+        double Tm = 0.0, T0 = Tz(0), Tp = Tz(1);
+        double Sm = 0.0, S0 = Sz(0), Sp = Sz(1);
+        for (int k = 0; k < L; ++k) {
+            double a, b, c, tr, sr;
+            vd_coef(d, Kv, aj, k, a, b, c);
+            if (k == 0) {
+                tr = c * (-Tp + T0);
+                sr = c * (-Sp + S0);
+            } else if (k == L - 1) {
+                tr = a * (T0 - Tm);
+                sr = a * (S0 - Sm);
+            } else {
+                tr = -a * Tm - c * Tp + (a + c) * T0;
+                sr = -a * Sm - c * Sp + (a + c) * S0;
+            }
+            if (k == 0) {
+                CP(0) = c / b;
+                TP(0) = tr / b;
+                SP(0) = sr / b;
+            } else {
+                const double m = 1.0 / (b - CP(k - 1) * a);
+                CP(k) = c * m;
+                TP(k) = (tr - TP(k - 1) * a) * m;
+                SP(k) = (sr - SP(k - 1) * a) * m;
+            }
+            Tm = T0; T0 = Tp;
+            Sm = S0; S0 = Sp;
+            if (k + 2 < L) { Tp = Tz(k + 2); Sp = Sz(k + 2); }
         }
-        c[0] = -dt * Kv[1] / ((Zc[0] - Zc[1]) * (ZBc[0] - ZBc[1]));
-        a[0] = 0.0;
-        b[0] = -c[0] + 1.0;
-        a[L - 1] = -dt * Kv[L - 1] / ((Zc[L - 2] - Zc[L - 1]) * (ZBc[L - 1] - ZBc[NS - 1]));
-        b[L - 1] = -a[L - 1] + 1.0;
-        c[L - 1] = 0.0;
-        tr[0] = c[0] * (-T[1] + T[0]);
-        sr[0] = c[0] * (-S[1] + S[0]);
-        for (int k = 1; k <= L - 2; ++k) {
-            tr[k] = -a[k] * T[k - 1] - c[k] * T[k + 1] + (a[k] + c[k]) * T[k];
-            sr[k] = -a[k] * S[k - 1] - c[k] * S[k + 1] + (a[k] + c[k]) * S[k];
-        }
-        tr[L - 1] = a[L - 1] * (T[L - 1] - T[L - 2]);
-        sr[L - 1] = a[L - 1] * (S[L - 1] - S[L - 2]);
-        double cp[MAXL], tp[MAXL], sp[MAXL];
-        cp[0] = c[0] / b[0];
-        tp[0] = tr[0] / b[0];
-        sp[0] = sr[0] / b[0];
-        for (int k = 1; k < L; ++k) {
-            const double m = 1.0 / (b[k] - cp[k - 1] * a[k]);
-            cp[k] = c[k] * m;
-            tp[k] = (tr[k] - tp[k - 1] * a[k]) * m;
-            sp[k] = (sr[k] - sp[k - 1] * a[k]) * m;
-        }
-        tr[L - 1] = tp[L - 1];
-        sr[L - 1] = sp[L - 1];
-        for (int k = L - 2; k >= 0; --k) {
-            tr[k] = tp[k] - cp[k] * tr[k + 1];
-            sr[k] = sp[k] - cp[k] * sr[k + 1];
-        }
+        // back substitution and update, bottom to top
         unsigned int st = 0;
-        for (int z = 0; z < L; ++z) {
-            double t = T[z] + tr[z] + T_aver;
-            double s = S[z] + sr[z] + S_aver;
+        double tr = 0.0, sr = 0.0;
+        for (int z = L - 1; z >= 0; --z) {
+            if (z == L - 1) { tr = TP(z); sr = SP(z); }
+            else { tr = TP(z) - CP(z) * tr; sr = SP(z) - CP(z) * sr; }
+            const size_t i = base + z;
+            double t = Tz(z) + tr + T_aver;
+            double s = Sz(z) + sr + S_aver;
             if (fabs(s) < 1.0e-12) s = fabs(s);
             if (s < 0.0) st |= 0x1u;
             if (t < -3.0) st |= 0x2u;
             if (!isfinite(t) || !isfinite(s)) st |= 0x4u;
-            d.TF[base + z] = t;
-            d.SF[base + z] = s;
-            d.T_old[base + z] = d.Told_new[base + z];
-            d.S_old[base + z] = So[z];
+            d.TF[i] = t;
+            d.SF[i] = s;
+            d.T_old[i] = d.Told_new[i];
+            d.S_old[i] = d.Sold_new[i];
         }
         if (!isfinite(d.eta_n[n])) st |= 0x4u;
         if (st) atomicOr(d.status, st);
@@ -578,11 +628,18 @@ void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
 void launch_muscl_ngrad(const Dev &d, cudaStream_t s) {
     k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
 }
+void launch_muscl_edge(const Dev &d, cudaStream_t s) {
+    k_muscl_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
+}
 void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
+static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
+static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(double); }
+int config_vdiff(const Dev &d) {
+    return cudaFuncSetAttribute(k_vdiff_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vdiff_smem(d)) ==
+                   cudaSuccess ? 0 : 1;
+}
 void launch_vdiff(const Dev &d, cudaStream_t s) {
-    if (d.L <= 24) k_vdiff_col<24><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-    else if (d.L <= 48) k_vdiff_col<48><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-    else k_vdiff_col<128><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    k_vdiff_col<<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
 }
 int energy_parts() { return kRedGrid; }
 void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {

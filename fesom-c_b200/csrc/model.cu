@@ -29,6 +29,8 @@ void launch_velrhs(const Dev &, double, cudaStream_t);
 void launch_implvisc(const Dev &, cudaStream_t);
 void launch_jac_swap(const Dev &, cudaStream_t);
 void launch_je(const Dev &, cudaStream_t);
+int config_d3end(const Dev &);
+int config_vdiff(const Dev &);
 void launch_ab2(const Dev &, cudaStream_t);
 void launch_update3d(const Dev &, double, cudaStream_t);
 void launch_wvel(const Dev &, cudaStream_t);
@@ -38,6 +40,7 @@ void launch_minmax(const Dev &, cudaStream_t);
 void launch_upwind(const Dev &, cudaStream_t);
 void launch_muscl_egrad(const Dev &, cudaStream_t);
 void launch_muscl_ngrad(const Dev &, cudaStream_t);
+void launch_muscl_edge(const Dev &, cudaStream_t);
 void launch_muscl_h(const Dev &, cudaStream_t);
 void launch_vdiff(const Dev &, cudaStream_t);
 int energy_parts();
@@ -340,7 +343,7 @@ int alloc_state(fesomc_model *m) {
     for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
     if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
     double **le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
-                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv, &d.Je};
+                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv, &d.Je, &d.Ze, &d.ZBe};
     for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
     double **ln[] = {&d.Unode, &d.Vnode, &d.Unode_p, &d.Vnode_p, &d.TF, &d.SF, &d.T_old, &d.S_old, &d.Tclim,
                      &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new, &d.ttfold, &d.stfold};
@@ -350,6 +353,8 @@ int alloc_state(fesomc_model *m) {
         for (auto p : lg) if ((rc = dalloc(m, p, L * E))) return rc;
         double **lgn[] = {&d.tnx, &d.tny, &d.snx, &d.sny};
         for (auto p : lgn) if ((rc = dalloc(m, p, L * N))) return rc;
+        double2 **fl[] = {&d.mflT, &d.mflS, &d.mflC};
+        for (auto p : fl) if ((rc = dalloc(m, p, L * (size_t)d.Ed))) return rc;
     }
     double **nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
     for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
@@ -392,21 +397,22 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
                Ei * (16 + 32 + 16);
     if (k == "rot_nodes") return N * 48;
     if (k == "pressure_col") return L * N * 16 + N * 16 + L * N * 8 + NS * N * 8;
-    if (k == "bpg_elem") return NS * N * 8 + N * 24 + E * (96 + 16 + 8) + L * E * 16 + E * 16;
+    if (k == "bpg_elem") return NS * N * 8 + N * 24 + E * (96 + 16 + 8) + L * E * 8 + L * E * 16 + E * 16;
     if (k == "el2nodes" || k == "el2nodes_p") return L * E * 16 + N * 12 + 4 * (4.0 * E) + E * 8 + L * N * 16;
     if (k == "d3end") return L * N * 32 + NS * N * 24 + N * 40 + NS * N * 40;
     if (k == "av") return NS * N * 8 + E * 48 + NS * E * 8;
     if (k == "velgrad3d") return L * E * 16 + E * (48 + 64 + 8) + L * E * 32;
-    if (k == "velrhs") return L * E * (48 + 16 + 16) + NS * N * 8 + N * 56 + E * 184 + Ei * 64 + L * E * 32;
-    if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 48 + 16) + N * 16 + L * E * 16;
+    if (k == "velrhs") return L * E * (80 + 24) + NS * N * 8 + N * 56 + E * 184 + Ei * 64 + L * E * 32;
+    if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 16) + L * E * 16 + L * E * 16;
     if (k == "zero_filt") return E * 16;
     if (k == "puls_elem") return L * E * 16 + E * 16 + N * 24 + E * 48 + L * E * 16 + E * 8;
-    if (k == "p1_elem") return L * N * 16 + N * 24 + E * 16 + Ei * 32 + E * (8 + 48 + 8 + 16);
+    if (k == "p1_elem")
+        return L * N * 16 + N * 24 + E * 16 + Ei * 32 + E * (8 + 48 + 8 + 16) + L * E * 8 + (d.filt_3D ? L * E * 16 : 0.0);
     if (k == "jac_swap") return N * 32;
-    if (k == "update3d") return L * E * 16 + N * 32 + E * 48 + E * 16 + E * 16 + L * E * 32 + E * 16;
-    if (k == "wvel") return N * 4 + 4 * nnz_ne + Ed * 40 + N * 16 + E * 48 + E * 16 + L * E * 16 + N * 16 + NS * N * 8;
+    if (k == "update3d") return L * E * (16 + 8 + 32 + 24) + N * 24 + E * 48 + E * 32 + E * 16;
+    if (k == "wvel") return N * 4 + 4 * nnz_ne + Ed * 40 + E * 16 + L * E * 24 + N * 8 + NS * N * 8;
     if (k == "minmax") return L * N * 16;
-    if (k == "je_elem") return N * 16 + E * 48 + L * E * 8;
+    if (k == "je_elem") return N * 16 + E * 48 + L * E * 24;
     if (k == "ab2_node") return L * N * 32 + L * N * 16;
     // tracer gathers: AB2 tracers (2 per node level), Je and transports per
     // element level, W per node interface, T/S of the node, edge geometry,
@@ -415,9 +421,14 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
         return L * N * 16 + L * E * 24 + NS * N * 8 + L * N * 16 + N * 28 + 4 * nnz_ne + Ed * 48 + L * N * 32;
     if (k == "muscl_egrad") return L * N * 16 + E * 80 + L * E * 32;
     if (k == "muscl_ngrad") return L * E * 32 + N * 4 + 4 * (4.0 * E) + E * 8 + L * N * 32;
+    // edge pass: AB2 tracers of the 2 end nodes and gradients (up/down
+    // elements or the node fallback), Je / transports of the 2 elements,
+    // edge geometry; 3 flux pairs per (edge, level) written
+    if (k == "muscl_edge") return L * N * 16 + L * E * 32 + L * N * 32 + L * E * 40 + Ed * 64 + E * 8 + L * Ed * 48;
+    // node pass: flux pairs of the node's edges (each edge by its 2 nodes),
+    // AB2 tracers, W, T/S, outputs
     if (k == "muscl_h")
-        return L * N * 16 + L * E * 32 + L * N * 32 + L * E * 40 + NS * N * 8 + L * N * 16 + N * 28 + 4 * nnz_ne +
-               Ed * 72 + E * 8 + L * N * 32;
+        return 2 * L * Ed * 48 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 16 + N * 28 + L * N * 32;
     if (k == "vdiff_col") return L * N * 32 + NS * N * 8 + N * 16 + L * N * 32;
     return 0.0;
 }
@@ -487,17 +498,17 @@ int enqueue_step(fesomc_model *m, double ff) {
         n += 2;
     }
     rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
-    rec(m, "je_elem", [&] { launch_je(d, s); });
     rec(m, "update3d", [&] { launch_update3d(d, 1.0 / (double)d.Mt, s); });
     rec(m, "wvel", [&] { launch_wvel(d, s); });
     rec(m, "minmax", [&] { launch_minmax(d, s); });
     rec(m, "ab2_node", [&] { launch_ab2(d, s); });
-    n += 7;
+    n += 6;
     if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
         rec(m, "muscl_egrad", [&] { launch_muscl_egrad(d, s); });
         rec(m, "muscl_ngrad", [&] { launch_muscl_ngrad(d, s); });
+        rec(m, "muscl_edge", [&] { launch_muscl_edge(d, s); });
         rec(m, "muscl_h", [&] { launch_muscl_h(d, s); });
-        n += 3;
+        n += 4;
     }
     else { rec(m, "upwind_h", [&] { launch_upwind(d, s); }); n += 1; }
     rec(m, "vdiff_col", [&] { launch_vdiff(d, s); });
@@ -611,7 +622,7 @@ extern "C" {
 int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fesomc_state *st, fesomc_model **out) {
     if (!mesh || !par || !st || !out) return FESOMC_EINVAL;
     *out = nullptr;
-    if (mesh->nsigma < 5 || mesh->nsigma > 129 || mesh->nod2D < 3 || mesh->elem2D < 1) return FESOMC_EINVAL;
+    if (mesh->nsigma < 5 || mesh->nsigma > 127 || mesh->nod2D < 3 || mesh->elem2D < 1) return FESOMC_EINVAL;
     if (par->Mt < 1 || par->dt <= 0.0 || par->dt_2D <= 0.0) return FESOMC_EINVAL;
     if (par->ver_mix != 3 && par->ver_mix != 0) return FESOMC_EINVAL;
     if (par->tracer_adv != FESOMC_TRACER_UPWIND && par->tracer_adv != FESOMC_TRACER_MUSCL) return FESOMC_EINVAL;
@@ -632,6 +643,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(FESOMC_ECUDA);
     if ((rc = build_mesh(m, mesh))) return fail(rc);
     if ((rc = alloc_state(m))) return fail(rc);
+    // kernels whose shared-memory scratch scales with the level count
+    if (config_d3end(m->d) || config_vdiff(m->d)) return fail(FESOMC_EINVAL);
     const size_t nobn = (size_t)(mesh->nobn > 0 ? mesh->nobn : 0);
     m->ampt.assign(nobn * 12, 0.0);
     m->fazt.assign(nobn * 12, 0.0);

@@ -218,6 +218,8 @@ ESTUARY_CFGS = {
     "cfg1": (1500, 700, 80.0, 21, 2.0, 40.0, 0.1),
     "small": (40, 16, 300.0, 11, 2.0, 25.0, 0.05),
     "medium": (300, 140, 150.0, 21, 2.0, 40.0, 0.1),
+    # cfg1 generator at a quarter of the nodes: profiling captures
+    "quarter": (700, 330, 170.0, 21, 2.0, 40.0, 0.1),
 }
 
 

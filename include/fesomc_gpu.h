@@ -198,6 +198,9 @@ typedef struct fesomc_model fesomc_model;
  * fesomc_gpu_sync_to_host / _from_host: before ncoutput(mpi)_do, energy and
  *   write_restart_separate / after read_restart_separate.
  * fesomc_gpu_energy replaces: energy(eout) (src/fv_average_dynamic.F90:476-554).
+ * fesomc_gpu_init accepts 5 <= nsigma <= 127 (per-column scratch of the
+ * vertical solvers is held in shared memory) and returns FESOMC_EINVAL
+ * otherwise.
  */
 int  fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par,
                      const fesomc_state *state, fesomc_model **out);
