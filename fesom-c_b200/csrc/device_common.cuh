@@ -63,6 +63,8 @@ struct Dev {
     // 2D state
     double *eta_n, *eta_n_1, *eta_n_2, *eta_new, *etaAB, *ssh_gp, *eta_jac, *eta_jac_old;
     double2 *U_n_2D, *U_n_1, *U_n_2, *UAB, *U_rhs_2D_3D, *Bar_pr_2D;
+    double4 *bfric;                       // per element for the sub-cycle: bottom U, V, a_Cd*|U|
+    double2 *Fp;                          // per element: surface pressure force * elem_area (compute_vel_rhs)
     double *aux_elem, *dmean_n, *U_filt_2D, *V_filt_2D, *mask_wd, *mask_wd_node;
     double4 *vel_grad;
     double *taux, *tauy, *windx, *windy, *runoff, *ob_val;
@@ -83,6 +85,7 @@ struct Dev {
     // the T flux, the S flux and the continuity term
     double2 *mflT, *mflS, *mflC;
     double2 *adv2d;                       // per internal edge: upwind 2D momentum flux of the sub-step
+    double2 *adv3;                        // per (internal edge, level): upwind 3D momentum flux (uu, vv)
     // tracer scratch
     double *TF_adv, *SF_adv, *Told_new, *Sold_new;
     double *ttx, *tty, *stx, *sty;       // L per element (MUSCL / Miura element gradients)

@@ -3,10 +3,11 @@
 //   pressure_col : densityJM + hydrostatic prefix sum per node column
 //   bpg_elem     : baroclinic_pressure_gradient_3D per element column
 //   velgrad3d    : vel_gradients (least squares, free slip) per (elem, level)
+//   adv3_edge    : upwind horizontal momentum flux per (internal edge, level)
 //   velrhs       : compute_vel_rhs up to the AB combine, per (elem, level):
-//                  pressure force, Coriolis/AB2 history, upwind horizontal
-//                  momentum advection gathered over the element's edges,
-//                  filter viscosity, QUICK vertical advection
+//                  pressure force, Coriolis/AB2 history, the edge momentum
+//                  fluxes gathered in edge order, filter viscosity, QUICK
+//                  vertical advection
 //   implvisc     : implicit vertical viscosity per element column
 //                  (momentum_vert_impl_visc_tmp / momentum_vert_impl_visc)
 //   update3d     : update_3D_vel per element column; stores the new Je, Ze, ZBe
@@ -87,6 +88,13 @@ __global__ void k_bpg_elem(Dev d) {
             b2 = b2 + bv * je;
         }
         d.Bar_pr_2D[e] = make_double2(b1, b2);
+        // surface pressure force of compute_vel_rhs (fv_3D_vel.F90:60-75),
+        // the same for every level of the element
+        double pr[4];
+        for (int k = 0; k < 4; ++k)
+            pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+        const double ar = d.elem_area[e];
+        d.Fp[e] = make_double2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
     }
 }
 
@@ -199,6 +207,36 @@ __device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const doubl
     fv = -vmean * wv;
 }
 
+// Upwind horizontal momentum flux of one (internal edge, level)
+// (momentum_adv_upwind, fv_advection.F90:114-188), computed once and gathered
+// by the edge's two elements in velrhs.  Thread per (edge, level), levels on
+// consecutive threads.
+__global__ void k_adv3_edge(Dev d) {
+    const long long total = (long long)d.Ed_in * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const double acc = 0.5 * (d.ac[nn.x] + d.ac[nn.y]);
+        const double4 X = d.edge_cross[ed];
+        const size_t i1 = (size_t)et.x * L + z, i2 = (size_t)et.y * L + z;
+        const double u1 = d.U_n[i1] - d.vgux[i1] * X.x - d.vguy[i1] * X.y;
+        const double v1 = d.V_n[i1] - d.vgvx[i1] * X.x - d.vgvy[i1] * X.y;
+        const double u2 = d.U_n[i2] - d.vgux[i2] * X.z - d.vguy[i2] * X.w;
+        const double v2 = d.V_n[i2] - d.vgvx[i2] * X.z - d.vgvy[i2] * X.w;
+        const double jd = 0.5 * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
+        const double2 dxy = d.edge_dxdy[ed];
+        const double un = 0.5 * kREarth * jd *
+                          ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
+        double uu, vv;
+        if (un >= 0.0) { uu = u1 * un * acc; vv = v1 * un * acc; }
+        else { uu = u2 * un * acc; vv = v2 * un * acc; }
+        d.adv3[ii] = make_double2(uu, vv);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
 // level) with levels on consecutive lanes.  The loop runs over whole warps so
@@ -220,45 +258,26 @@ __global__ void k_velrhs(Dev d, double ff) {
         const double4 w = d.w_cv[e];
         const double ar = d.elem_area[e];
         const double je = d.Je[ii];
-        // pressure force from eta_n
-        double pre[4];
-        for (int k = 0; k < 4; ++k)
-            pre[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
-        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
-        const double Fx = wsum(gx, pre[0], pre[1], pre[2], pre[3]) * ar;
-        const double Fy = wsum(gy, pre[0], pre[1], pre[2], pre[3]) * ar;
+        // pressure force from eta_n (per element, from bpg_elem)
+        const double2 F = d.Fp[e];
+        const double Fx = F.x, Fy = F.y;
         const double un0 = d.U_n[ii], vn0 = d.V_n[ii];
         double ur = -(0.5 + d.epsilon) * d.U_rhsAB[ii] + Fx * je;
         double vr = -(0.5 + d.epsilon) * d.V_rhsAB[ii] + Fy * je;
         const double cor = d.coriolis[e];
         double uab = vn0 * cor * ar * je;
         double vab = -un0 * cor * ar * je;
-        // horizontal upwind momentum advection (fv_advection.F90:114-188)
+        // horizontal upwind momentum advection (fv_advection.F90:114-188):
+        // edge fluxes in edge order
         if (d.mom_adv_3D == 1) {
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
             for (int c = 0; c < 4; ++c) {
                 const int code = codes[c];
                 if (code < 0) break;
-                const int ed = code >> 1;
-                const int2 nn = d.edge_nodes[ed];
-                const int2 et = d.edge_tri[ed];
-                const double acc = 0.5 * (d.ac[nn.x] + d.ac[nn.y]);
-                const double4 X = d.edge_cross[ed];
-                const size_t i1 = (size_t)et.x * L + z, i2 = (size_t)et.y * L + z;
-                const double u1 = d.U_n[i1] - d.vgux[i1] * X.x - d.vguy[i1] * X.y;
-                const double v1 = d.V_n[i1] - d.vgvx[i1] * X.x - d.vgvy[i1] * X.y;
-                const double u2 = d.U_n[i2] - d.vgux[i2] * X.z - d.vguy[i2] * X.w;
-                const double v2 = d.V_n[i2] - d.vgvx[i2] * X.z - d.vgvy[i2] * X.w;
-                const double jd = 0.5 * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
-                const double2 dxy = d.edge_dxdy[ed];
-                const double un = 0.5 * kREarth * jd *
-                                  ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
-                double uu, vv;
-                if (un >= 0.0) { uu = u1 * un * acc; vv = v1 * un * acc; }
-                else { uu = u2 * un * acc; vv = v2 * un * acc; }
-                if (code & 1) { uab = uab + uu; vab = vab + vv; }
-                else { uab = uab - uu; vab = vab - vv; }
+                const double2 f = d.adv3[(size_t)(code >> 1) * L + z];
+                if (code & 1) { uab = uab + f.x; vab = vab + f.y; }
+                else { uab = uab - f.x; vab = vab - f.y; }
             }
         }
         // filter viscosity (fv_viscosity.F90:842-860)
@@ -532,6 +551,9 @@ void launch_pressure_col(const Dev &d, cudaStream_t s) { k_pressure_col<<<warp_g
 void launch_bpg_elem(const Dev &d, cudaStream_t s) { k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_velgrad3d(const Dev &d, cudaStream_t s) {
     k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_adv3_edge(const Dev &d, cudaStream_t s) {
+    k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
     k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);

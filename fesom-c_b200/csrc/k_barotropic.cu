@@ -105,6 +105,7 @@ __global__ void k_ssh_node(Dev d, int sub) {
         const int n = (int)ii;
         double acc = 0.0;
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
+#pragma unroll 4
         for (int p = p0; p < p1; ++p) {
             const int code = d.node_eidx[p];
             const double c1 = ssh_edge_flux(d, code >> 1);
@@ -166,66 +167,116 @@ __global__ void k_el2nodes(Dev d, const double *Ue, const double *Ve, double *Un
     }
 }
 
-// momentum_adv_P1_3D_to_2D (fv_advection.F90:676-793) gathered per element,
-// optional viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939), divided by
-// dmean_n (fv_main.F90:1504-1513).  One thread per element; the level sums
-// run in level order.
+// momentum_adv_P1_3D_to_2D (fv_advection.F90:676-793): the edge part
+// uu*un, vv*un of every (internal edge, level), thread per (edge, level).
+// Stored in the adv3 buffer, which velrhs has finished with.
+__global__ void k_p1_edge(Dev d) {
+    const long long total = (long long)d.Ed_in * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const double2 dxy = d.edge_dxdy[ed];
+        const double xe = dxy.x * kREarth * 0.5 * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+        const double ye = dxy.y * kREarth;
+        const double a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
+        const double uu = 0.5 * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
+        const double vv = 0.5 * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
+        const double jd = 0.5 * (jc_of(d, a1, z) + jc_of(d, a2, z));
+        const double un = (uu * ye - vv * xe) * jd;
+        d.adv3[ii] = make_double2(uu * un, vv * un);
+    }
+}
+
+// Element part of momentum_adv_P1_3D_to_2D, optional
+// viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939), divided by dmean_n
+// (fv_main.F90:1504-1513).
+// A block takes B consecutive elements with one thread per (element, level)
+// (coalesced column loads).  Every thread writes its level's terms for the
+// element's edge slots and the filter into shared memory; then one thread
+// per element sums them in the reference's order: each slot's level sum
+// in level order (the slot sums are independent chains, interleaved), then
+// the slot contributions in slot order, then the filter terms.
+constexpr int kP1Slots = 5;  // 4 internal-edge slots + the filter
 __global__ void k_p1_elem(Dev d) {
-    GRID_LOOP(ii, d.E) {
-        const int e = (int)ii;
-        const int L = d.L;
-        double rx = 0.0, ry = 0.0;
-        const int4 il = d.elem_iedges[e];
-        const int codes[4] = {il.x, il.y, il.z, il.w};
-        const double *je_e = d.Je + (size_t)e * L;
-        for (int c = 0; c < 4; ++c) {
-            const int code = codes[c];
-            if (code < 0) break;
-            const int ed = code >> 1;
-            const int2 nn = d.edge_nodes[ed];
-            const int2 et = d.edge_tri[ed];
-            const double acc = (d.ac[nn.x] + d.ac[nn.y]) * .5;
-            const double2 dxy = d.edge_dxdy[ed];
-            const double xe = dxy.x * kREarth * 0.5 * (d.elem_cos[et.x] + d.elem_cos[et.y]);
-            const double ye = dxy.y * kREarth;
-            const double a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
-            double s_u = 0.0, s_v = 0.0;
-            for (int z = 0; z < L; ++z) {
-                const double uu = 0.5 * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
-                const double vv = 0.5 * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
-                const double jd = 0.5 * (jc_of(d, a1, z) + jc_of(d, a2, z));
-                const double un = (uu * ye - vv * xe) * jd;
-                const double je = je_e[z];
-                s_u = s_u + uu * un * je;
-                s_v = s_v + vv * un * je;
+    extern __shared__ double sm[];
+    const int L = d.L;
+    const int B = (int)blockDim.x / L;
+    const int S = 2 * kP1Slots * L + 1;  // per-element stride, odd: conflict-free
+    const int jl = (int)threadIdx.x / L, z = (int)threadIdx.x % L;
+    for (long long eb = (long long)blockIdx.x * B; eb < d.E; eb += (long long)gridDim.x * B) {
+        const long long e_ = eb + jl;
+        if (jl < B && e_ < d.E) {
+            const int e = (int)e_;
+            double *T = sm + (size_t)jl * S;  // T[(slot*2 + uv)*L + z]
+            const double je = d.Je[(size_t)e * L + z];
+            const int4 il = d.elem_iedges[e];
+            const int codes[4] = {il.x, il.y, il.z, il.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (codes[c] >= 0) {
+                    const double2 pq = d.adv3[(size_t)(codes[c] >> 1) * L + z];
+                    T[(c * 2 + 0) * L + z] = pq.x * je;
+                    T[(c * 2 + 1) * L + z] = pq.y * je;
+                }
             }
-            if (code & 1) { rx = rx + acc * s_u; ry = ry + acc * s_v; }
-            else { rx = rx - acc * s_u; ry = ry - acc * s_v; }
-        }
-        if (d.filt_3D) {
-            const int4 en = d.elem_nodes[e];
-            const int4 nb = d.elem_nb[e];
-            const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
-            const int jend = (en.x == en.w) ? 3 : 4;
-            const double tau = d.tau_inv_filt, ar = d.elem_area[e];
-            for (int z = 0; z < L; ++z) {
-                const double je = je_e[z];
+            if (d.filt_3D) {
+                const int4 en = d.elem_nodes[e];
+                const int4 nb4 = d.elem_nb[e];
+                const int nbs[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
+                const int jend = (en.x == en.w) ? 3 : 4;
+                const double tau = d.tau_inv_filt, ar = d.elem_area[e];
                 const double up = d.U_puls[(size_t)e * L + z], vp = d.V_puls[(size_t)e * L + z];
                 double u1 = 0.0, v1 = 0.0;
-                for (int j = 0; j < jend; ++j) {
-                    const int ne = nbs[j];
+                for (int k = 0; k < jend; ++k) {
+                    const int ne = nbs[k];
                     if (ne < 0) continue;
-                    const double jn = d.Je[(size_t)ne * L + z];
-                    u1 = u1 + d.U_puls[(size_t)ne * L + z] * jn - up * je;
-                    v1 = v1 + d.V_puls[(size_t)ne * L + z] * jn - vp * je;
+                    const size_t i = (size_t)ne * L + z;
+                    const double jn = d.Je[i];
+                    u1 = u1 + d.U_puls[i] * jn - up * je;
+                    v1 = v1 + d.V_puls[i] * jn - vp * je;
                 }
                 const double fu = tau * u1 * ar, fv = tau * v1 * ar;
-                rx = rx + fu * je;
-                ry = ry + fv * je;
+                T[(4 * 2 + 0) * L + z] = fu * je;
+                T[(4 * 2 + 1) * L + z] = fv * je;
             }
         }
-        const double dm = d.dmean_n[e];
-        d.U_rhs_2D_3D[e] = make_double2(rx / dm, ry / dm);
+        __syncthreads();
+        const long long es = eb + threadIdx.x;
+        if ((int)threadIdx.x < B && es < d.E) {
+            const int e = (int)es;
+            const double *T = sm + (size_t)threadIdx.x * S;
+            const int4 il = d.elem_iedges[e];
+            const int codes[4] = {il.x, il.y, il.z, il.w};
+            double su[4] = {0.0, 0.0, 0.0, 0.0}, sv[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = 0; k < L; ++k) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    su[c] = su[c] + T[(c * 2 + 0) * L + k];
+                    sv[c] = sv[c] + T[(c * 2 + 1) * L + k];
+                }
+            }
+            double rx = 0.0, ry = 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int code = codes[c];
+                if (code < 0) break;
+                const int2 nn = d.edge_nodes[code >> 1];
+                const double acc = (d.ac[nn.x] + d.ac[nn.y]) * .5;
+                if (code & 1) { rx = rx + acc * su[c]; ry = ry + acc * sv[c]; }
+                else { rx = rx - acc * su[c]; ry = ry - acc * sv[c]; }
+            }
+            if (d.filt_3D)
+                for (int k = 0; k < L; ++k) {
+                    rx = rx + T[(4 * 2 + 0) * L + k];
+                    ry = ry + T[(4 * 2 + 1) * L + k];
+                }
+            const double dm = d.dmean_n[e];
+            d.U_rhs_2D_3D[e] = make_double2(rx / dm, ry / dm);
+        }
+        __syncthreads();
     }
 }
 
@@ -249,12 +300,21 @@ __device__ __forceinline__ void adv2d_edge(const Dev &d, int ed, double &uu, dou
     else { uu = un * U2.x * acc; vv = un * U2.y * acc; }
 }
 
+// momentum_adv_upwind_2D edge fluxes of the sub-step, once per internal edge
+__global__ void k_adv2d_edge(Dev d) {
+    GRID_LOOP(ed, d.Ed_in) {
+        double uu, vv;
+        adv2d_edge(d, (int)ed, uu, vv);
+        d.adv2d[ed] = make_double2(uu, vv);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // u2d_elem: update_2D_vel (fv_average_dynamic.F90:228-443, type_task 3,
 // key_atm off) + rotation of U time levels + U_filt accumulation
 // (fv_main.F90:1568-1606).
 // ---------------------------------------------------------------------------
-__global__ void k_u2d_elem(Dev d) {
+__global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
     const double d0inv = 1.0 / d.density_0;
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
@@ -286,13 +346,13 @@ __global__ void k_u2d_elem(Dev d) {
         if (d.mom_adv_2D == 2) {
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
+#pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int code = codes[c];
                 if (code < 0) break;
-                double uu, vv;
-                adv2d_edge(d, code >> 1, uu, vv);
-                if (code & 1) { rx = rx + uu; ry = ry + vv; }
-                else { rx = rx - uu; ry = ry - vv; }
+                const double2 f = d.adv2d[code >> 1];
+                if (code & 1) { rx = rx + f.x; ry = ry + f.y; }
+                else { rx = rx - f.x; ry = ry - f.y; }
             }
         }
         if (d.filt_2D) {
@@ -317,9 +377,8 @@ __global__ void k_u2d_elem(Dev d) {
         double eo[4], enw[4];
         for (int k = 0; k < 4; ++k) { eo[k] = d.eta_n[nd[k]]; enw[k] = d.eta_new[nd[k]]; }
         const double dmo = dmax(d.Dmin, wsum(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
-        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[e]) * d.Cd_bz + 1.0);
-        const double ub = d.U_n[(size_t)e * d.L + d.L - 1], vb = d.V_n[(size_t)e * d.L + d.L - 1];
-        const double friction = a_Cd * sqrt(ub * ub + vb * vb);
+        const double4 bf = d.bfric[e];
+        const double ub = bf.x, vb = bf.y, friction = bf.z;
         const double ff = 1.0 / (dmax(d.Dmin, wsum(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
                                  + friction * d.dt_2D);
         const double dt2 = d.dt_2D;
@@ -349,11 +408,17 @@ __global__ void k_rot_nodes(Dev d) {
     }
 }
 
-// U_filt_2D = V_filt_2D = 0 at the start of the sub-cycle
+// U_filt_2D = V_filt_2D = 0 at the start of the sub-cycle, and the bottom
+// velocity and quadratic drag a_Cd*|U_b| that update_2D_vel uses in every
+// sub-step (fv_average_dynamic.F90:262, 400-420; U_n is fixed during the
+// sub-cycle)
 __global__ void k_zero_filt(Dev d) {
     GRID_LOOP(ii, d.E) {
         d.U_filt_2D[ii] = 0.0;
         d.V_filt_2D[ii] = 0.0;
+        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[ii]) * d.Cd_bz + 1.0);
+        const double ub = d.U_n[(size_t)ii * d.L + d.L - 1], vb = d.V_n[(size_t)ii * d.L + d.L - 1];
+        d.bfric[ii] = make_double4(ub, vb, a_Cd * sqrt(ub * ub + vb * vb), 0.0);
     }
 }
 
@@ -366,8 +431,23 @@ void launch_puls_elem(const Dev &d, cudaStream_t s) {
 void launch_el2nodes(const Dev &d, const double *Ue, const double *Ve, double *Un, double *Vn, cudaStream_t s) {
     k_el2nodes<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d, Ue, Ve, Un, Vn);
 }
-void launch_p1_elem(const Dev &d, cudaStream_t s) { k_p1_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
-void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+// B elements per block: B*L threads, at most 1024 and at most 32 elements
+static int p1_elems(const Dev &d) { int b = 1024 / d.L; return b > 32 ? 32 : b; }
+static size_t p1_smem(const Dev &d) { return (size_t)p1_elems(d) * (2 * kP1Slots * d.L + 1) * sizeof(double); }
+int config_p1(const Dev &d) {
+    return cudaFuncSetAttribute(k_p1_elem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(d)) == cudaSuccess
+               ? 0 : 1;
+}
+void launch_p1_edge(const Dev &d, cudaStream_t s) {
+    k_p1_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_p1_elem(const Dev &d, cudaStream_t s) {
+    const int B = p1_elems(d);
+    const long long blocks = ((long long)d.E + B - 1) / B;
+    k_p1_elem<<<(int)(blocks < 148LL * 16 ? blocks : 148LL * 16), B * d.L, p1_smem(d), s>>>(d);
+}
+void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
+void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 

@@ -282,9 +282,7 @@ int config_d3end(const Dev &d) {
     return e == cudaSuccess ? 0 : 1;
 }
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.NS == 11) k_d3end_r<11, 64><<<grid_for(d.N, 64), 64, d3end_r_smem<11>(), s>>>(d);
-    else if (d.NS == 21) k_d3end_r<21, 64><<<grid_for(d.N, 64), 64, d3end_r_smem<21>(), s>>>(d);
-    else if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else if (d.NS <= 48) k_d3end<48><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
 }

@@ -387,8 +387,9 @@ __global__ void k_muscl_edge(Dev d) {
 }
 
 // node gather of the edge fluxes in edge order + vertical + update, one
-// warp per node, lane = level
-__global__ void k_muscl_h(Dev d) {
+// warp per node, lane = level.  The edge loop is unrolled so the flux loads
+// of several edges are in flight together; the sums stay in edge order.
+__global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const double T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
@@ -405,6 +406,7 @@ __global__ void k_muscl_h(Dev d) {
             const int z = z0 + lane;
             const int zc = z < L ? z : L - 1;
             double rt = 0.0, rs = 0.0, rc = 0.0;
+#pragma unroll 4
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;

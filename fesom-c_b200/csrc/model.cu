@@ -18,19 +18,23 @@ void launch_ab3_elem(const Dev &, cudaStream_t);
 void launch_ssh_node(const Dev &, int, cudaStream_t);
 void launch_puls_elem(const Dev &, cudaStream_t);
 void launch_el2nodes(const Dev &, const double *, const double *, double *, double *, cudaStream_t);
+void launch_p1_edge(const Dev &, cudaStream_t);
 void launch_p1_elem(const Dev &, cudaStream_t);
+void launch_adv2d_edge(const Dev &, cudaStream_t);
 void launch_u2d_elem(const Dev &, cudaStream_t);
 void launch_rot_nodes(const Dev &, cudaStream_t);
 void launch_zero_filt(const Dev &, cudaStream_t);
 void launch_pressure_col(const Dev &, cudaStream_t);
 void launch_bpg_elem(const Dev &, cudaStream_t);
 void launch_velgrad3d(const Dev &, cudaStream_t);
+void launch_adv3_edge(const Dev &, cudaStream_t);
 void launch_velrhs(const Dev &, double, cudaStream_t);
 void launch_implvisc(const Dev &, cudaStream_t);
 void launch_jac_swap(const Dev &, cudaStream_t);
 void launch_je(const Dev &, cudaStream_t);
 int config_d3end(const Dev &);
 int config_vdiff(const Dev &);
+int config_p1(const Dev &);
 void launch_ab2(const Dev &, cudaStream_t);
 void launch_update3d(const Dev &, double, cudaStream_t);
 void launch_wvel(const Dev &, cudaStream_t);
@@ -342,6 +346,10 @@ int alloc_state(fesomc_model *m) {
     double2 **e2[] = {&d.U_n_2D, &d.U_n_1, &d.U_n_2, &d.UAB, &d.U_rhs_2D_3D, &d.Bar_pr_2D};
     for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
     if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
+    if ((rc = dalloc(m, &d.bfric, E))) return rc;
+    if ((rc = dalloc(m, &d.Fp, E))) return rc;
+    if ((rc = dalloc(m, &d.adv3, L * (size_t)d.Ed_in))) return rc;
+    if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
     double **le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
                      &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv, &d.Je, &d.Ze, &d.ZBe};
     for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
@@ -392,22 +400,31 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     const double nnz_ne = (double)(2 * d.Ed);  // node->edge incidences
     if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
+    // per internal edge: nodes (etaAB, depth, ac), elements (UAB, vel_grad,
+    // cos), geometry; one flux pair written
+    if (k == "adv2d_edge") return N * 24 + E * (16 + 32 + 8) + Ei * (8 + 8 + 32 + 16 + 16);
+    // per element: 4 nodes' etaAB, depth, atp1/2, ssh_gp, eta_n, eta_new;
+    // element fields read / written once; edge fluxes of its internal edges
     if (k == "u2d_elem")
-        return N * (7 * 8 + 8) + E * (112 + 40 + 16 + 32 + 16 + 8 + 16 + 16 + 16 + 16 + 32 + 8 + 48 + 32 + 8) +
-               Ei * (16 + 32 + 16);
+        return N * 56 + E * (16 + 8 + 32 + 8 + 64 + 16 + 8 + 16 + 16 + 16 + 16 + 32 + 16 + 16 + 16 + 16) +
+               2 * Ei * 16 + E * (8 + 16 + 16 + 16 + 16);
     if (k == "rot_nodes") return N * 48;
     if (k == "pressure_col") return L * N * 16 + N * 16 + L * N * 8 + NS * N * 8;
-    if (k == "bpg_elem") return NS * N * 8 + N * 24 + E * (96 + 16 + 8) + L * E * 8 + L * E * 16 + E * 16;
+    if (k == "bpg_elem") return NS * N * 8 + N * 48 + E * (96 + 16 + 8 + 8) + L * E * 8 + L * E * 16 + E * 32;
     if (k == "el2nodes" || k == "el2nodes_p") return L * E * 16 + N * 12 + 4 * (4.0 * E) + E * 8 + L * N * 16;
     if (k == "d3end") return L * N * 32 + NS * N * 24 + N * 40 + NS * N * 40;
     if (k == "av") return NS * N * 8 + E * 48 + NS * E * 8;
     if (k == "velgrad3d") return L * E * 16 + E * (48 + 64 + 8) + L * E * 32;
-    if (k == "velrhs") return L * E * (80 + 24) + NS * N * 8 + N * 56 + E * 184 + Ei * 64 + L * E * 32;
+    if (k == "adv3_edge") return L * E * 48 + N * 24 + Ei * 64 + E * 8 + L * Ei * 16;
+    if (k == "velrhs")
+        return L * E * (48 + 24) + L * Ei * 16 * 2 + NS * N * 8 + N * 16 + E * 168 + L * E * 32;
     if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 16) + L * E * 16 + L * E * 16;
-    if (k == "zero_filt") return E * 16;
+    if (k == "zero_filt") return E * 16 + E * 8 + E * 16 + E * 32;
     if (k == "puls_elem") return L * E * 16 + E * 16 + N * 24 + E * 48 + L * E * 16 + E * 8;
+    if (k == "p1_edge") return L * N * 16 + N * 16 + Ei * 32 + E * 8 + L * Ei * 16;
     if (k == "p1_elem")
-        return L * N * 16 + N * 24 + E * 16 + Ei * 32 + E * (8 + 48 + 8 + 16) + L * E * 8 + (d.filt_3D ? L * E * 16 : 0.0);
+        return 2 * L * Ei * 16 + E * (16 + 16 + 16) + Ei * 8 + N * 8 + L * E * 8 +
+               (d.filt_3D ? L * E * 16 + E * 24 : 0.0);
     if (k == "jac_swap") return N * 32;
     if (k == "update3d") return L * E * (16 + 8 + 32 + 24) + N * 24 + E * 48 + E * 32 + E * 16;
     if (k == "wvel") return N * 4 + 4 * nnz_ne + Ed * 40 + E * 16 + L * E * 24 + N * 8 + NS * N * 8;
@@ -478,8 +495,10 @@ int enqueue_step(fesomc_model *m, double ff) {
         n += 2;
     }
     rec(m, "velgrad3d", [&] { launch_velgrad3d(d, s); });
+    n += 1;
+    if (d.mom_adv_3D == 1) { rec(m, "adv3_edge", [&] { launch_adv3_edge(d, s); }); n += 1; }
     rec(m, "velrhs", [&] { launch_velrhs(d, ff, s); });
-    n += 2;
+    n += 1;
     if (d.im_vert_visc || d.im_vert_visc_fic) { rec(m, "implvisc", [&] { launch_implvisc(d, s); }); n += 1; }
     rec(m, "zero_filt", [&] { launch_zero_filt(d, s); });
     n += 1;
@@ -490,9 +509,11 @@ int enqueue_step(fesomc_model *m, double ff) {
         if (sub == 0) {
             rec(m, "puls_elem", [&] { launch_puls_elem(d, s); });
             rec(m, "el2nodes_p", [&] { launch_el2nodes(d, d.U_puls, d.V_puls, d.Unode_p, d.Vnode_p, s); });
+            rec(m, "p1_edge", [&] { launch_p1_edge(d, s); });
             rec(m, "p1_elem", [&] { launch_p1_elem(d, s); });
-            n += 3;
+            n += 4;
         }
+        if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { launch_adv2d_edge(d, s); }); n += 1; }
         rec(m, "u2d_elem", [&] { launch_u2d_elem(d, s); });
         rec(m, "rot_nodes", [&] { launch_rot_nodes(d, s); });
         n += 2;
@@ -644,7 +665,7 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if ((rc = build_mesh(m, mesh))) return fail(rc);
     if ((rc = alloc_state(m))) return fail(rc);
     // kernels whose shared-memory scratch scales with the level count
-    if (config_d3end(m->d) || config_vdiff(m->d)) return fail(FESOMC_EINVAL);
+    if (config_d3end(m->d) || config_vdiff(m->d) || config_p1(m->d)) return fail(FESOMC_EINVAL);
     const size_t nobn = (size_t)(mesh->nobn > 0 ? mesh->nobn : 0);
     m->ampt.assign(nobn * 12, 0.0);
     m->fazt.assign(nobn * 12, 0.0);
