@@ -100,6 +100,8 @@ SIGNATURES = {
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),
     "fesomc_host_density_jm": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
+    "fesomc_energy_device": (C.c_int, [C.c_int32, C.c_int32, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, f64p]),
 }
 
 _lib = None

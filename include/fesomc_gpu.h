@@ -272,6 +272,24 @@ int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, in
  * where each MPI rank owns a mesh partition instead. */
 int  fesomc_gpu_set_device(int32_t device);
 
+/* Domain energy (as fesomc_gpu_energy, src/fv_average_dynamic.F90:476-554)
+ * of a state held in caller-owned DEVICE arrays, without creating a model
+ * and without allocating device memory.  No counterpart in the reference.
+ * It serves callers that own the state in their own device buffers or that
+ * have reserved all device memory and may not allocate more.  Arrays use the
+ * reference shapes: eta_n, depth, area (nod2D); elem2D_nodes (4,elem2D),
+ * 1-based; w_cv (4,elem2D); U_n_2D (2,elem2D); elem_area (elem2D).  stream
+ * is a cudaStream_t (NULL = default stream); the call returns after the
+ * result is on the host.  The reduction scratch is a fixed 14,256-byte
+ * device array shared by all calls on a device: it needs no initial zeroing,
+ * and calls that overlap in time race on it.  The first call on a device
+ * (with that device current) looks up the array once; make it before any
+ * stream capture begins.  Returns FESOMC_EINVAL for bad arguments. */
+int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const double *eta_n,
+                          const double *depth, const double *area, const int32_t *elem2D_nodes,
+                          const double *w_cv, const double *U_n_2D, const double *elem_area,
+                          void *stream, double *eout);
+
 /* ---- version / introspection --------------------------------------------- */
 const char *fesomc_gpu_version(void);
 /* Number of kernels launched by this instance since init. */
