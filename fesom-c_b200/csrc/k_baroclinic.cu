@@ -18,56 +18,82 @@
 
 namespace fesomc {
 
+// Column blocks: B consecutive entities per block, one thread per (entity,
+// level), levels on consecutive threads (coalesced column access).  Level
+// sums / scans that the reference does sequentially go through shared memory
+// (one row of L per entity, odd row stride) and are done by one thread per
+// entity, in level order.
+struct ColBlock {
+    int L, B, jl, z;
+    __device__ ColBlock(int L_) : L(L_), B((int)blockDim.x / L_), jl((int)threadIdx.x / L_), z((int)threadIdx.x % L_) {}
+};
+
 // ---------------------------------------------------------------------------
-// pressure (fv_pressure_new.F90:91-107): one warp per node column, lane =
-// level; density in parallel, the hydrostatic sum as an ordered warp scan
+// pressure (fv_pressure_new.F90:91-107): density per (node, level), the
+// hydrostatic sum per node in level order
 // ---------------------------------------------------------------------------
 __global__ void k_pressure_col(Dev d) {
+    extern __shared__ double sm[];
     const double gd0 = kG / d.density_0;
-    const int lane = threadIdx.x & 31;
     const int L = d.L, NS = d.NS;
-    WARP_LOOP(ent, d.N) {
-        const int n = (int)ent;
-        const double a = jac_a(d, d.eta_jac, n);
-        const size_t bl = (size_t)n * L, bs = (size_t)n * NS;
-        double hp = 0.0;
-        if (lane == 0) d.hpressure[bs] = 0.0;
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            const bool ok = z < L;
-            const int zc = ok ? z : L - 1;
-            const double rho = density_jm(d.TF[bl + zc], d.SF[bl + zc], -z_of(d, a, zc), d.density_0);
-            const double t = rho * jc_of(d, a, zc) * gd0;
-            const double mine = warp_seq_scan(hp, t, chunk_len(L, z0));
-            if (ok) {
-                d.rho_c[bl + z] = rho;
-                d.hpressure[bs + z + 1] = mine;
+    const ColBlock cb(L);
+    const int S = L | 1;
+    for (long long nb = (long long)blockIdx.x * cb.B; nb < d.N; nb += (long long)gridDim.x * cb.B) {
+        const long long n_ = nb + cb.jl;
+        const bool act = cb.jl < cb.B && n_ < d.N;
+        if (act) {
+            const int n = (int)n_;
+            const double a = jac_a(d, d.eta_jac, n);
+            const size_t i = (size_t)n * L + cb.z;
+            const double rho = density_jm(d.TF[i], d.SF[i], -z_of(d, a, cb.z), d.density_0);
+            d.rho_c[i] = rho;
+            sm[cb.jl * S + cb.z] = rho * jc_of(d, a, cb.z) * gd0;
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < cb.B && nb + threadIdx.x < d.N) {
+            double *row = sm + threadIdx.x * S;
+            double hp = 0.0;
+            for (int k = 0; k < L; ++k) {
+                hp = hp + row[k];
+                row[k] = hp;
             }
         }
+        __syncthreads();
+        if (act) {
+            const size_t bs = (size_t)n_ * NS;
+            d.hpressure[bs + cb.z + 1] = sm[cb.jl * S + cb.z];
+            if (cb.z == 0) d.hpressure[bs] = 0.0;
+        }
+        __syncthreads();
     }
 }
 
-// baroclinic_pressure_gradient_3D (fv_pressure_new.F90:146-221), thread per element
+// baroclinic_pressure_gradient_3D (fv_pressure_new.F90:146-221) per
+// (element, level); Bar_pr_2D as a level-ordered sum per element.  Also the
+// element's surface pressure force of compute_vel_rhs (fv_3D_vel.F90:60-75),
+// the same for every level.
 __global__ void k_bpg_elem(Dev d) {
-    GRID_LOOP(ii, d.E) {
-        const int e = (int)ii;
-        const int L = d.L, NS = d.NS;
-        const int4 en = d.elem_nodes[e];
-        const int nd[4] = {en.x, en.y, en.z, en.w};
-        const double4 gx = d.gs_x[e], gy = d.gs_y[e], w = d.w_cv[e];
-        double dh[4], de[4];
-        for (int k = 0; k < 4; ++k) { dh[k] = d.depth[nd[k]] + d.eta_n[nd[k]]; de[k] = d.depth[nd[k]]; }
-        const double Ax = wsum(gx, dh[0], dh[1], dh[2], dh[3]);
-        const double Ay = wsum(gy, dh[0], dh[1], dh[2], dh[3]);
-        const double Bx = wsum(gx, de[0], de[1], de[2], de[3]);
-        const double By = wsum(gy, de[0], de[1], de[2], de[3]);
-        const double fac = d.elem_bpfac[e];
-        const double4 ae = elem_jac_a(d, d.eta_jac, en);
-        const double an[4] = {ae.x, ae.y, ae.z, ae.w};
-        const double *je_e = d.Je + (size_t)e * L;
-        double b1 = 0.0, b2 = 0.0;
-        for (int z = 0; z < L; ++z) {
-            const double je = je_e[z];
+    extern __shared__ double sm[];
+    const int L = d.L, NS = d.NS;
+    const ColBlock cb(L);
+    const int S = 2 * L + 1;
+    for (long long eb = (long long)blockIdx.x * cb.B; eb < d.E; eb += (long long)gridDim.x * cb.B) {
+        const long long e_ = eb + cb.jl;
+        if (cb.jl < cb.B && e_ < d.E) {
+            const int e = (int)e_, z = cb.z;
+            const int4 en = d.elem_nodes[e];
+            const int nd[4] = {en.x, en.y, en.z, en.w};
+            const double4 gx = d.gs_x[e], gy = d.gs_y[e], w = d.w_cv[e];
+            double dh[4], de[4];
+            for (int k = 0; k < 4; ++k) { dh[k] = d.depth[nd[k]] + d.eta_n[nd[k]]; de[k] = d.depth[nd[k]]; }
+            const double Ax = wsum(gx, dh[0], dh[1], dh[2], dh[3]);
+            const double Ay = wsum(gy, dh[0], dh[1], dh[2], dh[3]);
+            const double Bx = wsum(gx, de[0], de[1], de[2], de[3]);
+            const double By = wsum(gy, de[0], de[1], de[2], de[3]);
+            const double fac = d.elem_bpfac[e];
+            const double4 ae = elem_jac_a(d, d.eta_jac, en);
+            const double an[4] = {ae.x, ae.y, ae.z, ae.w};
+            const double je = d.Je[(size_t)e * L + z];
             const double accJe_inv = -fac / je;
             double hu[4], hl[4], pre[4];
             for (int k = 0; k < 4; ++k) {
@@ -84,17 +110,30 @@ __global__ void k_bpg_elem(Dev d) {
             const double bv = accJe_inv * (sy + qd_low * (s1 * Ay - By) - qd_up * (s0 * Ay - By));
             d.Bar_pru[(size_t)e * L + z] = bu;
             d.Bar_prv[(size_t)e * L + z] = bv;
-            b1 = b1 + bu * je;
-            b2 = b2 + bv * je;
+            sm[cb.jl * S + z] = bu * je;
+            sm[cb.jl * S + L + z] = bv * je;
         }
-        d.Bar_pr_2D[e] = make_double2(b1, b2);
-        // surface pressure force of compute_vel_rhs (fv_3D_vel.F90:60-75),
-        // the same for every level of the element
-        double pr[4];
-        for (int k = 0; k < 4; ++k)
-            pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
-        const double ar = d.elem_area[e];
-        d.Fp[e] = make_double2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
+        __syncthreads();
+        const long long es = eb + threadIdx.x;
+        if ((int)threadIdx.x < cb.B && es < d.E) {
+            const int e = (int)es;
+            const double *row = sm + threadIdx.x * S;
+            double b1 = 0.0, b2 = 0.0;
+            for (int k = 0; k < L; ++k) {
+                b1 = b1 + row[k];
+                b2 = b2 + row[L + k];
+            }
+            d.Bar_pr_2D[e] = make_double2(b1, b2);
+            const int4 en = d.elem_nodes[e];
+            const int nd[4] = {en.x, en.y, en.z, en.w};
+            const double4 gx = d.gs_x[e], gy = d.gs_y[e];
+            double pr[4];
+            for (int k = 0; k < 4; ++k)
+                pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+            const double ar = d.elem_area[e];
+            d.Fp[e] = make_double2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
+        }
+        __syncthreads();
     }
 }
 
@@ -243,7 +282,7 @@ __global__ void k_adv3_edge(Dev d) {
 // that the vertical flux at interface z+1 comes from the next lane.
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
 // ---------------------------------------------------------------------------
-__global__ void k_velrhs(Dev d, double ff) {
+__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
     const long long total = (long long)d.E * d.L;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -254,7 +293,6 @@ __global__ void k_velrhs(Dev d, double ff) {
         const int z = (int)(ii % d.L);
         const int L = d.L;
         const int4 en = d.elem_nodes[e];
-        const int nd[4] = {en.x, en.y, en.z, en.w};
         const double4 w = d.w_cv[e];
         const double ar = d.elem_area[e];
         const double je = d.Je[ii];
@@ -450,46 +488,63 @@ __global__ void k_je_elem(Dev d) {
 }
 
 // update_3D_vel (fv_3D_vel.F90:201-255) with the U_filt averaging of
-// oce_barotropic_timestep (fv_main.F90:1670-1677) folded in; one warp per
-// element, lane = level.  Runs right after the jacobian call: the stored Je
-// still holds the previous jacobian (Jc_old), and is replaced here by the
-// new Je / Ze / ZBe.
+// oce_barotropic_timestep (fv_main.F90:1670-1677) folded in; column block
+// per element.  Runs right after the jacobian call: the stored Je still holds
+// the previous jacobian (Jc_old), and is replaced here by the new Je / Ze /
+// ZBe.
 __global__ void k_update3d(Dev d, double Mt_inv) {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ double sm[];
     const int L = d.L;
-    WARP_LOOP(ent, d.E) {
-        const int e = (int)ent;
-        const int4 en = d.elem_nodes[e];
-        const double4 w = d.w_cv[e];
-        const double4 an = elem_jac_a(d, d.eta_jac, en);
-        const size_t base = (size_t)e * L;
-        const double dmean_inv = 1.0 / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
-                                                        d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
-        double su = 0.0, sv = 0.0;
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            const int zc = z < L ? z : L - 1;
-            const double a = d.Je[base + zc];
-            const int n = chunk_len(L, z0);
-            su = warp_seq_sum(su, d.U_rhs[base + zc] * a, n);
-            sv = warp_seq_sum(sv, d.V_rhs[base + zc] * a, n);
+    const ColBlock cb(L);
+    const int S = 2 * L + 1;
+    double *sc = sm + (size_t)cb.B * S;  // 4 scalars per element
+    for (long long eb = (long long)blockIdx.x * cb.B; eb < d.E; eb += (long long)gridDim.x * cb.B) {
+        const long long e_ = eb + cb.jl;
+        const bool act = cb.jl < cb.B && e_ < d.E;
+        const size_t i = (size_t)e_ * L + cb.z;
+        double a_old = 0.0, ur = 0.0, vr = 0.0;
+        if (act) {
+            a_old = d.Je[i];
+            ur = d.U_rhs[i];
+            vr = d.V_rhs[i];
+            sm[cb.jl * S + cb.z] = ur * a_old;
+            sm[cb.jl * S + L + cb.z] = vr * a_old;
         }
-        const double U2p = su * dmean_inv, V2p = sv * dmean_inv;
-        const double uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
-        const double vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
-        const double2 u2 = d.U_n_2D[e];
-        __syncwarp();
-        if (lane == 0) {
+        __syncthreads();
+        const long long es = eb + threadIdx.x;
+        if ((int)threadIdx.x < cb.B && es < d.E) {
+            const int e = (int)es;
+            const double *row = sm + threadIdx.x * S;
+            double su = 0.0, sv = 0.0;
+            for (int k = 0; k < L; ++k) {
+                su = su + row[k];
+                sv = sv + row[L + k];
+            }
+            const int4 en = d.elem_nodes[e];
+            const double4 w = d.w_cv[e];
+            const double dmean_inv = 1.0 / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
+                                                            d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
+            const double uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
+            const double vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
             d.U_filt_2D[e] = uf;
             d.V_filt_2D[e] = vf;
+            double *o = sc + 4 * threadIdx.x;
+            o[0] = su * dmean_inv;
+            o[1] = sv * dmean_inv;
+            o[2] = uf;
+            o[3] = vf;
         }
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            if (z >= L) continue;
-            const size_t i = base + z;
+        __syncthreads();
+        if (act) {
+            const int e = (int)e_, z = cb.z;
+            const double *o = sc + 4 * cb.jl;
+            const double U2p = o[0], V2p = o[1], uf = o[2], vf = o[3];
+            const int4 en = d.elem_nodes[e];
+            const double4 w = d.w_cv[e];
+            const double4 an = elem_jac_a(d, d.eta_jac, en);
+            const double2 u2 = d.U_n_2D[e];
             const double jn = je_of(d, w, an, z);
-            const double az = d.Je[i] / jn;
-            const double ur = d.U_rhs[i], vr = d.V_rhs[i];
+            const double az = a_old / jn;
             d.U_n_filt[i] = az * ur + uf - U2p;
             d.V_n_filt[i] = az * vr + vf - V2p;
             d.U_n[i] = az * ur + u2.x - U2p;
@@ -498,57 +553,85 @@ __global__ void k_update3d(Dev d, double Mt_inv) {
             d.Ze[i] = wsum_z(d, w, an, z);
             d.ZBe[i] = wsum_zbar(d, w, an, z);
         }
+        __syncthreads();
     }
 }
 
-// vert_vel_sigma (fv_3D_vel.F90:309-456): one warp per node, lane = level;
-// the layer transport divergence is gathered over the node's edges in edge
-// order, then summed upward from the bottom as an ordered warp scan.
+// vert_vel_sigma (fv_3D_vel.F90:309-456): column block per node; the layer
+// transport divergence of (node, level) gathered over the node's edges in
+// edge order, then summed upward from the bottom per node.
 __global__ void k_wvel(Dev d) {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ double sm[];
     const int L = d.L, NS = d.NS;
-    WARP_LOOP(ent, d.N) {
-        const int n = (int)ent;
-        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
-        const double area_inv = 1.0 / d.area[n];
-        double *Wn = d.Wvel + (size_t)n * NS;
-        double below = Wn[NS - 1];
-        for (int z0 = ((L - 1) / 32) * 32; z0 >= 0; z0 -= 32) {
-            const int z = z0 + lane;
-            const bool ok = z < L;
-            const int zc = ok ? z : L - 1;
+    const ColBlock cb(L);
+    const int S = L | 1;
+    for (long long nb = (long long)blockIdx.x * cb.B; nb < d.N; nb += (long long)gridDim.x * cb.B) {
+        const long long n_ = nb + cb.jl;
+        const bool act = cb.jl < cb.B && n_ < d.N;
+        if (act) {
+            const int n = (int)n_, z = cb.z;
+            const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
             double W = 0.0;
+#pragma unroll 4
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
                 const int2 et = d.edge_tri[ed];
                 const double4 X = d.edge_cross[ed];
                 const double uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
-                const size_t i1 = (size_t)et.x * L + zc;
+                const size_t i1 = (size_t)et.x * L + z;
                 double c1 = d.Je[i1] * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
                 if (ed < d.Ed_in) {
                     const double uf2 = d.U_filt_2D[et.y], vf2 = d.V_filt_2D[et.y];
-                    const size_t i2 = (size_t)et.y * L + zc;
+                    const size_t i2 = (size_t)et.y * L + z;
                     c1 = c1 + d.Je[i2] * (-(d.V_n_filt[i2] - vf2) * X.z + (d.U_n_filt[i2] - uf2) * X.w);
                 }
                 if (code & 1) W = W - c1;
                 else W = W + c1;
             }
-            // below = W(z) + below, from the bottom level upward
-            double mine = 0.0;
-            for (int j = chunk_len(L, z0) - 1; j >= 0; --j) {
-                below = __shfl_sync(kFull, W, j) + below;
-                if (lane == j) mine = below;
-            }
-            if (ok) Wn[z] = mine * area_inv;
+            sm[cb.jl * S + z] = W;
         }
+        __syncthreads();
+        const long long ns = nb + threadIdx.x;
+        if ((int)threadIdx.x < cb.B && ns < d.N) {
+            double *row = sm + threadIdx.x * S;
+            double below = d.Wvel[(size_t)ns * NS + NS - 1];
+            for (int k = L - 1; k >= 0; --k) {
+                below = row[k] + below;
+                row[k] = below;
+            }
+        }
+        __syncthreads();
+        if (act) d.Wvel[(size_t)n_ * NS + cb.z] = sm[cb.jl * S + cb.z] * (1.0 / d.area[n_]);
+        __syncthreads();
     }
 }
 
 // ---- launch wrappers --------------------------------------------------------
-static int warp_grid(long long entities, int block) { return grid_for(entities * 32, block); }
-void launch_pressure_col(const Dev &d, cudaStream_t s) { k_pressure_col<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
-void launch_bpg_elem(const Dev &d, cudaStream_t s) { k_bpg_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
+// column blocks: B = min(16, 1024 / L) entities, B * L threads
+static int col_b(const Dev &d) { int b = 1024 / d.L; return b > 16 ? 16 : b; }
+static int col_grid(const Dev &d, long long count) {
+    const long long blocks = (count + col_b(d) - 1) / col_b(d);
+    return (int)(blocks < 148LL * 8 ? blocks : 148LL * 8);
+}
+static size_t col_smem(const Dev &d, int rows, int scalars) {
+    const int S = rows == 1 ? (d.L | 1) : rows * d.L + 1;
+    return ((size_t)col_b(d) * S + (size_t)col_b(d) * scalars) * sizeof(double);
+}
+int config_columns(const Dev &d) {
+    const size_t big = col_smem(d, 2, 4);
+    cudaError_t e = cudaFuncSetAttribute(k_bpg_elem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update3d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pressure_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_wvel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+    return e == cudaSuccess ? 0 : 1;
+}
+void launch_pressure_col(const Dev &d, cudaStream_t s) {
+    k_pressure_col<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 0), s>>>(d);
+}
+void launch_bpg_elem(const Dev &d, cudaStream_t s) {
+    k_bpg_elem<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, 0), s>>>(d);
+}
 void launch_velgrad3d(const Dev &d, cudaStream_t s) {
     k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
@@ -568,8 +651,8 @@ void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, g
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
 void launch_update3d(const Dev &d, double Mt_inv, cudaStream_t s) {
-    k_update3d<<<warp_grid(d.E, 128), 128, 0, s>>>(d, Mt_inv);
+    k_update3d<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, 4), s>>>(d, Mt_inv);
 }
-void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
+void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 0), s>>>(d); }
 
 }  // namespace fesomc

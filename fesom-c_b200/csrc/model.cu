@@ -35,6 +35,7 @@ void launch_je(const Dev &, cudaStream_t);
 int config_d3end(const Dev &);
 int config_vdiff(const Dev &);
 int config_p1(const Dev &);
+int config_columns(const Dev &);
 void launch_ab2(const Dev &, cudaStream_t);
 void launch_update3d(const Dev &, double, cudaStream_t);
 void launch_wvel(const Dev &, cudaStream_t);
@@ -665,7 +666,7 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if ((rc = build_mesh(m, mesh))) return fail(rc);
     if ((rc = alloc_state(m))) return fail(rc);
     // kernels whose shared-memory scratch scales with the level count
-    if (config_d3end(m->d) || config_vdiff(m->d) || config_p1(m->d)) return fail(FESOMC_EINVAL);
+    if (config_d3end(m->d) || config_vdiff(m->d) || config_p1(m->d) || config_columns(m->d)) return fail(FESOMC_EINVAL);
     const size_t nobn = (size_t)(mesh->nobn > 0 ? mesh->nobn : 0);
     m->ampt.assign(nobn * 12, 0.0);
     m->fazt.assign(nobn * 12, 0.0);
