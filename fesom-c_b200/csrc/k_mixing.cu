@@ -7,6 +7,59 @@
 
 namespace fesomc {
 
+// Convergence test of d3_end's sweep (fv_mixing.F90:250-259) for one level:
+// the reference forms c = |a/b| and stops when the largest c is below 1e-6
+// (a NaN c never raises the maximum).  Returns true when this level forbids
+// convergence, i.e. when RN(|a|/|b|) >= 1e-6.  The quotient is only formed
+// when |a| lies within a relative 2^-30 of 1e-6*|b|; outside that band the
+// comparison of |a| with the product decides it with certainty (the band is
+// far wider than the rounding of the product and of the quotient).
+__device__ __forceinline__ bool d3_above_tol(double a, double b) {
+    const double aa = fabs(a), bb = fabs(b);
+    if (bb > 1.0e-290 && bb < 1.0e290 && aa < 1.0e300) {
+        const double t = 1.0e-6 * bb;
+        if (aa <= t * (1.0 - 0x1p-30)) return false;
+        if (aa >= t * (1.0 + 0x1p-30)) return true;
+    }
+    return fabs(a / b) >= 1.0e-6;
+}
+
+// One iteration of the implicit turbulence-energy sweep of d3_end
+// (fv_mixing.F90:204-266) on register arrays indexed 1..NS; STORE writes
+// tke_dissip (the reference writes it in every iteration; only the last
+// one survives).  Returns true when converged (btr left unchanged),
+// otherwise replaces btr by the new solution.
+template <int NS, int BD, bool STORE>
+__device__ __forceinline__ bool d3_iterate(double (&btr)[NS + 1], double (&xx1)[NS + 1], double (&yy1)[NS + 1],
+                                           const double *col, double t_inv, double bot, double *tke) {
+#define PRM(a, k) col[((a) * NS + (k)) * BD]
+    enum { SN = 0, PB, QB, C2, AM, CM };
+#pragma unroll
+    for (int nz = 2; nz <= NS - 1; ++nz) {
+        const double b = btr[nz], sn = PRM(SN, nz);
+        const double c1 = 0.046 * (b * b) / sn;
+        if (STORE) tke[nz - 1] = c1;
+        const double fr = PRM(PB, nz) - c1 - PRM(QB, nz) - PRM(C2, nz);
+        const double am = PRM(AM, nz), cm = PRM(CM, nz);
+        const double bm = am + cm + (2.0 * 0.046 * b) / sn + t_inv;
+        const double a = bm - am * xx1[nz];
+        xx1[nz + 1] = cm / a;
+        yy1[nz + 1] = (am * yy1[nz] - fr) / a;
+    }
+#undef PRM
+    double btr1[NS + 1];
+    btr1[NS] = bot;
+#pragma unroll
+    for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
+    bool above = false;
+#pragma unroll
+    for (int nz = 1; nz <= NS; ++nz) above |= d3_above_tol(btr[nz] - btr1[nz], dmax(btr1[nz], btr[nz]) + 1.0e-8);
+    if (!above) return true;
+#pragma unroll
+    for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
+    return false;
+}
+
 // d3_end, fully unrolled for a compile-time level count: the iterated state
 // (btr, xx1, yy1) stays in registers, the iteration-independent terms of
 // each level in shared memory ([term][level][thread]).  One thread per node
@@ -83,39 +136,16 @@ __global__ void __launch_bounds__(BD) k_d3end_r(Dev d) {
         const double bott_R = B1cka2 / (lg * lg);
         const double ubt = Un[L - 1], vbt = Vn[L - 1];
         const double bot = bott_R * (ubt * ubt + vbt * vbt);
+        // iterations 1..199 without the tke_dissip stores, the 200th with them
         bool converged = false;
-        for (int it = 1; it <= 200; ++it) {
-#pragma unroll
-            for (int nz = 2; nz <= NS - 1; ++nz) {
-                const double b = btr[nz], sn = PRM(SN, nz);
-                const double c1 = 0.046 * (b * b) / sn;
-                if (it == 200) tke[nz - 1] = c1;
-                const double fr = PRM(PB, nz) - c1 - PRM(QB, nz) - PRM(C2, nz);
-                const double am = PRM(AM, nz), cm = PRM(CM, nz);
-                const double bm = am + cm + (2.0 * 0.046 * b) / sn + t_inv;
-                const double a = bm - am * xx1[nz];
-                xx1[nz + 1] = cm / a;
-                yy1[nz + 1] = (am * yy1[nz] - fr) / a;
-            }
-            double btr1[NS + 1];
-            btr1[NS] = bot;
-#pragma unroll
-            for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
-            double bbb_max = 0.0;
-#pragma unroll
-            for (int nz = 1; nz <= NS; ++nz) {
-                const double c = fabs((btr[nz] - btr1[nz]) / (dmax(btr1[nz], btr[nz]) + 1.0e-8));
-                if (c > bbb_max) bbb_max = c;
-            }
-            if (bbb_max < 1.0e-6) { converged = true; break; }
-#pragma unroll
-            for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
-        }
+        for (int it = 1; it < 200 && !converged; ++it)
+            converged = d3_iterate<NS, BD, false>(btr, xx1, yy1, col, t_inv, bot, tke);
         if (converged) {
 #pragma unroll
             for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / PRM(SN, nz);
         } else {
-            atomicAdd(d.notconv, 1);
+            converged = d3_iterate<NS, BD, true>(btr, xx1, yy1, col, t_inv, bot, tke);
+            if (!converged) atomicAdd(d.notconv, 1);
         }
         double *btw = d.bt + (size_t)node * NS;
         double *snw = d.snu + (size_t)node * NS;
@@ -139,7 +169,13 @@ __global__ void __launch_bounds__(BD) k_d3end_r(Dev d) {
 }
 constexpr int kD3Terms = 6;
 
-// Generic level count: per-column arrays in local memory.
+// d3_end per node column, arrays indexed 1..NS like the Fortran ones (local
+// memory).  The terms that do not change over the iterations are formed
+// once per level: -b1-b2, t_inv*bo, c2, am, cm (the reference recomputes
+// am, cm in every iteration with the same expressions).  btr1(k) is kept in
+// xx1(k+1), which the back substitution no longer needs.  tke_dissip, which
+// the reference overwrites in every iteration, is written once from the
+// btr of the last iteration.
 template <int MAXNS>
 __global__ void k_d3end(Dev d) {
     const double t_inv = 1.0 / d.dt;
@@ -157,15 +193,13 @@ __global__ void k_d3end(Dev d) {
         const double *S = d.SF + (size_t)node * L;
         double *Ri = d.Ri + (size_t)node * NS;
         double *tke = d.tke_dissip + (size_t)node * NS;
-        // arrays indexed 1..NS like the Fortran ones
-        double xx1[MAXNS + 2], yy1[MAXNS + 2], btr[MAXNS + 2], btr1[MAXNS + 2];
-        double b1[MAXNS + 2], b2[MAXNS + 2], c2[MAXNS + 2], sn[MAXNS + 2], bo[MAXNS + 2];
+        double xx1[MAXNS + 2], yy1[MAXNS + 2], btr[MAXNS + 2];
+        double pb[MAXNS + 2], qb[MAXNS + 2], c2[MAXNS + 2], am[MAXNS + 2], cm[MAXNS + 2], sn[MAXNS + 2];
         const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
         const double dmean2 = dmean * dmean;
         const double ajac = jac_a(d, d.eta_jac, node);
         for (int nz = 1; nz <= NS; ++nz) {
             btr[nz] = bt[nz - 1];
-            bo[nz] = bt[nz - 1];
             sn[nz] = snu[nz - 1];
         }
         Ri[0] = 0.0;
@@ -177,22 +211,24 @@ __global__ void k_d3end(Dev d) {
             const double dd = 0.5 * (d1 + d2);
             double ap1 = Un[nz - 2] - Un[nz - 1];
             const double ap2 = Vn[nz - 2] - Vn[nz - 1];
-            b1[nz] = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
-            b1[nz] = b1[nz] / dmean2;
+            double b1 = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            b1 = b1 / dmean2;
             const double zb = zbar_of(d, ajac, nz - 1);
             const double rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
             const double rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
             ap1 = (rho_up - rho_dn) / dd;
-            b2[nz] = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const double b2 = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
             const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
             const double snu_m = 0.5 * (sn[nz] + sn[nz + 1]);
-            c2[nz] = 0.5 * 0.73 * (snu_p * (bo[nz - 1] - bo[nz]) / d1 - snu_m * (bo[nz] - bo[nz + 1]) / d2) / dd;
-            c2[nz] = c2[nz] / dmean2;
-            if (b1[nz] > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1[nz] * sn[nz];
+            double cc = 0.5 * 0.73 * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
+            c2[nz] = cc / dmean2;
+            if (b1 > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn[nz];
             else Ri[nz - 1] = 10000.0;
+            pb[nz] = -b1 - b2;
+            qb[nz] = t_inv * bt[nz - 1];
+            am[nz] = 0.5 * (snu_p * 0.73) / (dmean2 * d1 * dd);
+            cm[nz] = 0.5 * (snu_m * 0.73) / (dmean2 * d2 * dd);
         }
-        xx1[2] = 1.0;
-        yy1[2] = 0.0;
         {
             const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
             const double wx = d.windx[node], wy = d.windy[node];
@@ -208,36 +244,31 @@ __global__ void k_d3end(Dev d) {
         const double bot = bott_R * (ubt * ubt + vbt * vbt);
         bool converged = false;
         for (int it = 1; it <= 200; ++it) {
+            xx1[2] = 1.0;
             for (int nz = 2; nz <= NS - 1; ++nz) {
-                const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
-                const double dd1 = s_m - s_0;
-                const double dd2 = s_0 - s_p;
-                const double dd = 0.5 * (dd1 + dd2);
-                const double c1 = 0.046 * (btr[nz] * btr[nz]) / sn[nz];
-                tke[nz - 1] = c1;
-                const double fr = -b1[nz] - b2[nz] - c1 - t_inv * bo[nz] - c2[nz];
-                const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
-                const double snu_mm = 0.5 * (sn[nz] + sn[nz + 1]);
-                const double am = 0.5 * (snu_p * 0.73) / (dmean2 * dd1 * dd);
-                const double cm = 0.5 * (snu_mm * 0.73) / (dmean2 * dd2 * dd);
-                const double bm = am + cm + (2.0 * 0.046 * btr[nz]) / sn[nz] + t_inv;
-                const double a = bm - am * xx1[nz];
-                xx1[nz + 1] = cm / a;
-                yy1[nz + 1] = (am * yy1[nz] - fr) / a;
+                const double b = btr[nz];
+                const double c1 = 0.046 * (b * b) / sn[nz];
+                if (it == 200) tke[nz - 1] = c1;
+                const double fr = pb[nz] - c1 - qb[nz] - c2[nz];
+                const double bm = am[nz] + cm[nz] + (2.0 * 0.046 * b) / sn[nz] + t_inv;
+                const double a = bm - am[nz] * xx1[nz];
+                xx1[nz + 1] = cm[nz] / a;
+                yy1[nz + 1] = (am[nz] * yy1[nz] - fr) / a;
             }
-            btr1[NS] = bot;
-            for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
-            double bbb_max = 0.0;
-            for (int nz = 1; nz <= NS; ++nz) {
-                const double a = btr[nz] - btr1[nz];
-                const double b = dmax(btr1[nz], btr[nz]) + 1.0e-8;
-                const double c = fabs(a / b);
-                if (c > bbb_max) bbb_max = c;
+            double b1v = bot;  // btr1(NS)
+            bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + 1.0e-8);
+            for (int nz = NS; nz >= 2; --nz) {
+                b1v = b1v * xx1[nz] + yy1[nz];  // btr1(nz-1)
+                xx1[nz] = b1v;
+                above |= d3_above_tol(btr[nz - 1] - b1v, dmax(b1v, btr[nz - 1]) + 1.0e-8);
             }
-            if (bbb_max < 1.0e-6) { converged = true; break; }
-            for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
+            if (!above) { converged = true; break; }
+            for (int nz = 1; nz <= NS - 1; ++nz) btr[nz] = xx1[nz + 1];
+            btr[NS] = bot;
         }
-        if (!converged) {
+        if (converged) {
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / sn[nz];
+        } else {
             atomicAdd(d.notconv, 1);
         }
         double *btw = d.bt + (size_t)node * NS;
