@@ -191,38 +191,23 @@ def traffic_from_profiles(kernel):
 
 
 def run_ours(args, ws, rank, local):
-    from fesomc import abi, build, cases, model
+    from fesomc import abi, build, cases, model, replicas
     if not os.path.exists(abi.LIB_PATH):
         build.build_library()
     lib = abi.load()
     if lib.missing_symbols:
         raise RuntimeError("missing symbols %s" % lib.missing_symbols)
-    pg = None
     if ws > 1:
         import torch
-        import torch.distributed as dist
-        from datetime import timedelta
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        pg = dist
+    reps = replicas.Replicas(ws, "nccl")
     abi.check(lib.fesomc_gpu_set_device(local), "fesomc_gpu_set_device")
     cfg = args.config
     case = build_case(cfg)
     g = model.GpuModel(case)
     m = case.mesh
     units_per_step = m.N * m.L
-
-    def barrier():
-        if pg:
-            pg.barrier()
-
-    def max_over_ranks(x):
-        if not pg:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     # forcing of the run: constant stress / wind, ramped river runoff per step
     t_next = cases.advance_time(g.time_jd, case.params.dt)
@@ -241,7 +226,7 @@ def run_ours(args, ws, rank, local):
     g.nstep += args.steps
     t_dev = max_over_ranks(ms.value / 1000.0)
     barrier()
-    value = units_per_step * args.steps * ws / t_dev
+    value = replicas.whole_job_rate(units_per_step, args.steps, ws, t_dev)
     # ---- end to end through the C-ABI: per step the host pushes the step's
     # forcing that the reference recomputes each step (rivers_do runoff; the
     # open-boundary tide table is staged by the library from pinned memory),
@@ -263,7 +248,7 @@ def run_ours(args, ws, rank, local):
         g.time_jd = t_next
         g.nstep += 1
     t_e2e = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = units_per_step * args.steps * ws / t_e2e
+    e2e_value = replicas.whole_job_rate(units_per_step, args.steps, ws, t_e2e)
     # ---- per-kernel device times with events (eager launches) for the roofline
     nk = C.c_int32()
     maxk = 64
@@ -314,9 +299,7 @@ def run_ours(args, ws, rank, local):
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{done} internal steps of {cfg} after 1 untimed step "
                                           f"({dt:.1f} s), CPU restatement with OpenMP"}
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    reps.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -90,6 +90,8 @@ struct Dev {
     double *TF_adv, *SF_adv, *Told_new, *Sold_new;
     double *ttx, *tty, *stx, *sty;       // L per element (MUSCL / Miura element gradients)
     double *tnx, *tny, *snx, *sny;       // L per node   (node-averaged gradients)
+    double *tnow;                         // L per node: T minus its mean (Miura)
+    double *mask_ad;                      // per node: advection-order mask (adv_tracer_mask)
     double *trhs_a, *trhs_b, *trhs_c;    // L per node scratch
     double *mm_part;                      // reduction partials
     double *aver;                         // [0]=T_aver [1]=S_aver

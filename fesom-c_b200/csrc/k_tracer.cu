@@ -1,5 +1,6 @@
 // Tracer kernels of solve_tracers (src/fv_main.F90:1707-1836):
 //   minmax      : global T/S min/max -> T_aver, S_aver (two-pass reduction)
+//   miura_*     : solve_tracer_miura (fv_tracer.F90:930-1316), T only
 //   upwind_h    : solve_tracer_upwind (fv_tracer.F90:390-923) per (node, level):
 //                 edge fluxes gathered in edge order, QUICK vertical fluxes,
 //                 open-boundary relaxation, AB2 update (T and S together)
@@ -272,11 +273,13 @@ __global__ void k_muscl_ngrad(Dev d) {
     }
 }
 
-// MUSCL vertical flux (fv_tracer.F90:225-271) at interface k (0-based) of a
-// column with AB2 tracer TO(m); Tmean carries over when W == 0 as in the
-// reference.
-template <typename F>
-__device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, const double *W, F TO) {
+// Vertical QUICK flux shared by solve_tracer_muscl (fv_tracer.F90:225-271)
+// and solve_tracer_miura (fv_tracer.F90:1171-1207) at interface k (0-based)
+// of a column with tracer TO(m); Tmean carries over interfaces with W == 0
+// as in the reference.  MUSCL groups the weights as a*b/(c+a)/(b-c), Miura
+// as a*b/((c+a)*(b-c)).
+template <bool MUSCL, typename F>
+__device__ __forceinline__ double tvert_quick(const Dev &d, int k, double a, const double *W, F TO) {
     const int NS = d.NS;
     if (k == NS - 1) return 0.0;
     if (k == 0) return -W[0] * TO(0);
@@ -292,8 +295,8 @@ __device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, con
             if (nz == NS - 1) Tmean = TO(nz - 1);
             else {
                 const double aa = ZB(nz) - Z(nz - 1), bb = Z(nz) - ZB(nz), cc = Z(nz + 1) - ZB(nz);
-                const double dg = aa * bb / (cc + aa) / (bb - cc);
-                const double db = -aa * cc / (bb + aa) / (bb - cc);
+                const double dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const double db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
                 const double da = 1.0 - dg - db;
                 Tmean = TO(nz - 2) * da + TO(nz - 1) * db + TO(nz) * dg;
             }
@@ -302,14 +305,18 @@ __device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, con
             if (nz == 2) Tmean = TO(nz - 2);
             else {
                 const double aa = Z(nz) - ZB(nz), bb = ZB(nz) - Z(nz - 1), cc = ZB(nz) - Z(nz - 2);
-                const double dg = aa * bb / (cc + aa) / (bb - cc);
-                const double db = -aa * cc / (bb + aa) / (bb - cc);
+                const double dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const double db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
                 const double da = 1.0 - dg - db;
                 Tmean = TO(nz - 1) * da + TO(nz - 2) * db + TO(nz - 3) * dg;
             }
         }
     }
     return -Tmean * W[k];
+}
+template <typename F>
+__device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, const double *W, F TO) {
+    return tvert_quick<true>(d, k, a, W, TO);
 }
 
 __device__ __forceinline__ double muscl_mean(bool upw2, double Tm1, double Tm2) {
@@ -450,6 +457,192 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
                 d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
                 d.Sold_new[ii] = stf + S_aver;
                 d.SF_adv[ii] = stf + sr * d.dt + S_aver;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// solve_tracer_miura (fv_tracer.F90:930-1316): temperature only, as in the
+// reference driver (fv_main.F90:1790-1799); salinity passes through.
+// ---------------------------------------------------------------------------
+// AB2 of T minus its mean (ttfold), T minus its mean (tnow) and the
+// advection-order mask of adv_tracer_mask (fv_main.F90:1309-1335,
+// H_advtr_crit = 0.1, H_advtr_min = 0)
+__global__ void k_miura_prep(Dev d) {
+    const long long total = (long long)d.N * d.L;
+    const double T_aver = d.aver[0];
+    GRID_LOOP(i, total) {
+        d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
+        d.tnow[i] = d.TF[i] - T_aver;
+        if (i % d.L == 0) {
+            const int n = (int)(i / d.L);
+            const double crit = 0.1, hmin = 0.0;
+            const double dmean = dmax(d.Dmin, d.depth[n] + d.eta_n[n]);
+            double m;
+            if (dmean > crit) m = 1.0;
+            else if (dmean < hmin) m = 0.0;
+            else m = (dmean - hmin) / (crit - hmin);
+            d.mask_ad[n] = m;
+        }
+    }
+}
+
+// tracer_gradient_elements of T - T_aver (fv_gradients.F90:180-214)
+__global__ void k_miura_egrad(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        const int4 en = d.elem_nodes[e];
+        const double t1 = d.tnow[(size_t)en.x * L + z], t2 = d.tnow[(size_t)en.y * L + z];
+        const double t3 = d.tnow[(size_t)en.z * L + z], t4 = d.tnow[(size_t)en.w * L + z];
+        d.ttx[ii] = wsum(d.gs_x[e], t1, t2, t3, t4);
+        d.tty[ii] = wsum(d.gs_y[e], t1, t2, t3, t4);
+    }
+}
+
+// tracer_gradient_nodes (fv_gradients.F90:217-260): area-weighted sums
+// times the reciprocal of the summed area
+__global__ void k_miura_ngrad(Dev d) {
+    const long long total = (long long)d.N * d.L;
+    GRID_LOOP(ii, total) {
+        const int n = (int)(ii / d.L);
+        const int z = (int)(ii % d.L);
+        const int L = d.L;
+        double s = 0.0;
+        for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) s = s + d.elem_area[d.node_nidx[p]];
+        const double tvol = 1.0 / s;
+        double tx = 0.0, ty = 0.0;
+        for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
+            const int el = d.node_nidx[p];
+            const double ar = d.elem_area[el];
+            tx = tx + d.ttx[(size_t)el * L + z] * ar;
+            ty = ty + d.tty[(size_t)el * L + z] * ar;
+        }
+        d.tnx[ii] = tx * tvol;
+        d.tny[ii] = ty * tvol;
+    }
+}
+
+// Miura segment fluxes of one (edge, level) (fv_tracer.F90:1010-1140) and the
+// continuity terms (:1141-1168); thread per (edge, level)
+__global__ void k_miura_edge(Dev d) {
+    const long long total = (long long)d.Ed * d.L;
+    const int L = d.L;
+    const double dt = d.dt;
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const double4 X = d.edge_cross[ed];
+        const double2 exy = d.edge_dxdy[ed];
+        const double crt1 = 0.5 * (d.mask_ad[nn.x] + d.mask_ad[nn.y]);
+        const bool two = et.y >= 0;
+        const double a = 1.0, b = 1.0;
+        double Kh = d.elem_area[et.x];
+        if (two) Kh = 0.5 * (Kh + d.elem_area[et.y]);
+        Kh = d.K_hor * Kh / d.scale_area;
+        const size_t e1 = (size_t)et.x * L + z;
+        const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
+        double Tx, Ty;
+        if (two) {
+            const size_t e2 = (size_t)et.y * L + z;
+            Tx = 0.5 * Kh * (d.ttx[e1] + d.ttx[e2]);
+            Ty = 0.5 * Kh * (d.tty[e1] + d.tty[e2]);
+        } else {
+            Tx = Kh * d.ttx[e1];
+            Ty = Kh * d.tty[e1];
+        }
+        const double J1 = d.Je[e1];
+        const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+        double Tmean;
+        if (V1 * X.x - U1 * X.y > 0) {
+            // no dt on the V term in this branch (fv_tracer.F90:1057)
+            Tmean = d.tnow[i2] + (0.5 * (-exy.x * a + X.x - U1 * dt) * d.tnx[i2] +
+                                  0.5 * (-exy.y * kREarth + X.y - V1) * d.tny[i2]) * crt1;
+        } else {
+            Tmean = d.tnow[i1] + (0.5 * (exy.x * a + X.x - U1 * dt) * d.tnx[i1] +
+                                  0.5 * (exy.y * kREarth + X.y - V1 * dt) * d.tny[i1]) * crt1;
+        }
+        double2 fT, fC;
+        fT.x = (J1 * V1 * Tmean - Ty) * X.x - (J1 * U1 * Tmean - Tx) * X.y;
+        fC.x = J1 * V1 * X.x - J1 * U1 * X.y;
+        if (two) {
+            const size_t e2 = (size_t)et.y * L + z;
+            const double J2 = d.Je[e2];
+            const double U2 = d.U_n_filt[e2], V2 = d.V_n_filt[e2];
+            if (V2 * X.z - U2 * X.w < 0) {
+                Tmean = d.tnow[i2] + (0.5 * (-exy.x * b + X.z - U2 * dt) * d.tnx[i2] +
+                                      0.5 * (-exy.y * kREarth + X.w - V2 * dt) * d.tny[i2]) * crt1;
+            } else {
+                Tmean = d.tnow[i1] + (0.5 * (exy.x * b + X.z - U2 * dt) * d.tnx[i1] +
+                                      0.5 * (exy.y * kREarth + X.w - V2 * dt) * d.tny[i1]) * crt1;
+            }
+            fT.y = -(J2 * V2 * Tmean - Ty) * X.z + (J2 * U2 * Tmean - Tx) * X.w;
+            fC.y = -J2 * V2 * X.z + J2 * U2 * X.w;
+        } else {
+            fT.y = 0.0; fC.y = 0.0;
+        }
+        d.mflT[ii] = fT;
+        d.mflC[ii] = fC;
+    }
+}
+
+// node gather of the Miura fluxes in edge order + vertical + update (T),
+// salinity passed through; one warp per node, lane = level
+__global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
+    const int lane = threadIdx.x & 31;
+    const double T_aver = d.aver[0];
+    const int L = d.L, NS = d.NS;
+    WARP_LOOP(nn_, d.N) {
+        const int n = (int)nn_;
+        const double an = jac_a(d, d.eta_jac, n);
+        const double *W = d.Wvel + (size_t)n * NS;
+        const size_t base = (size_t)n * L;
+        const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
+        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
+        const double vn = relax ? vel_nor(d, n) : 0.0;
+        const double area = d.area[n];
+        for (int z0 = 0; z0 < L; z0 += 32) {
+            const int z = z0 + lane;
+            const int zc = z < L ? z : L - 1;
+            double rt = 0.0, rc = 0.0;
+#pragma unroll 4
+            for (int p = p0; p < p1; ++p) {
+                const int code = d.node_eidx[p];
+                const int ed = code >> 1;
+                const size_t i = (size_t)ed * L + zc;
+                const double2 fT = d.mflT[i], fC = d.mflC[i];
+                const bool internal = ed < d.Ed_in;
+                if (code & 1) {
+                    rt = rt - fT.x; rc = rc - fC.x;
+                    if (internal) { rt = rt - fT.y; rc = rc - fC.y; }
+                } else {
+                    rt = rt + fT.x; rc = rc + fC.x;
+                    if (internal) { rt = rt + fT.y; rc = rc + fC.y; }
+                }
+            }
+            auto TN = [&](int m) { return d.tnow[base + m]; };
+            const double tv0 = tvert_quick<false>(d, zc, an, W, TN);
+            double tv1 = __shfl_down_sync(kFull, tv0, 1);
+            if (lane == 31 || zc == L - 1) tv1 = tvert_quick<false>(d, zc + 1, an, W, TN);
+            if (z < L) {
+                const size_t ii = base + z;
+                const double jc = jc_of(d, an, z);
+                const double to = d.ttfold[ii];
+                const double ttf = d.tnow[ii];
+                double tr = ((rt - to * rc) / area + to * (W[z] - W[z + 1]) + tv0 - tv1) / jc;
+                if (relax) {
+                    if (vn > 0.0) tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                    else tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
+                }
+                d.Told_new[ii] = ttf + T_aver;
+                d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+                d.Sold_new[ii] = d.S_old[ii];
+                d.SF_adv[ii] = d.SF[ii];
             }
         }
     }
@@ -629,6 +822,13 @@ void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
 }
 void launch_muscl_ngrad(const Dev &d, cudaStream_t s) {
     k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_miura(const Dev &d, cudaStream_t s) {
+    k_miura_prep<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+    k_miura_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    k_miura_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+    k_miura_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
+    k_miura_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d);
 }
 void launch_muscl_edge(const Dev &d, cudaStream_t s) {
     k_muscl_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);

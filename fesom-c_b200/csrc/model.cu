@@ -46,6 +46,7 @@ void launch_upwind(const Dev &, cudaStream_t);
 void launch_muscl_egrad(const Dev &, cudaStream_t);
 void launch_muscl_ngrad(const Dev &, cudaStream_t);
 void launch_muscl_edge(const Dev &, cudaStream_t);
+void launch_miura(const Dev &, cudaStream_t);
 void launch_muscl_h(const Dev &, cudaStream_t);
 void launch_vdiff(const Dev &, cudaStream_t);
 int energy_parts();
@@ -365,6 +366,10 @@ int alloc_state(fesomc_model *m) {
         double2 **fl[] = {&d.mflT, &d.mflS, &d.mflC};
         for (auto p : fl) if ((rc = dalloc(m, p, L * (size_t)d.Ed))) return rc;
     }
+    if (m->p.tracer_adv == FESOMC_TRACER_MIURA) {
+        if ((rc = dalloc(m, &d.tnow, L * N))) return rc;
+        if ((rc = dalloc(m, &d.mask_ad, N))) return rc;
+    }
     double **nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
     for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
@@ -432,6 +437,11 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     if (k == "minmax") return L * N * 16;
     if (k == "je_elem") return N * 16 + E * 48 + L * E * 24;
     if (k == "ab2_node") return L * N * 32 + L * N * 16;
+    if (k == "miura")
+        return (L * N * 24 + N * 24 + L * N * 16) + (L * N * 8 + E * 80 + L * E * 16) +
+               (L * E * 16 + N * 4 + 4 * (4.0 * E) + E * 8 + L * N * 16) +
+               (L * N * 40 + N * 8 + L * E * 48 + Ed * 64 + E * 8 + L * Ed * 32) +
+               (2 * L * Ed * 32 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 32 + L * N * 32);
     // tracer gathers: AB2 tracers (2 per node level), Je and transports per
     // element level, W per node interface, T/S of the node, edge geometry,
     // and the four outputs per node level
@@ -523,9 +533,10 @@ int enqueue_step(fesomc_model *m, double ff) {
     rec(m, "update3d", [&] { launch_update3d(d, 1.0 / (double)d.Mt, s); });
     rec(m, "wvel", [&] { launch_wvel(d, s); });
     rec(m, "minmax", [&] { launch_minmax(d, s); });
-    rec(m, "ab2_node", [&] { launch_ab2(d, s); });
-    n += 6;
-    if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
+    n += 5;
+    if (d.tracer_adv != FESOMC_TRACER_MIURA) { rec(m, "ab2_node", [&] { launch_ab2(d, s); }); n += 1; }
+    if (d.tracer_adv == FESOMC_TRACER_MIURA) { rec(m, "miura", [&] { launch_miura(d, s); }); n += 5; }
+    else if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
         rec(m, "muscl_egrad", [&] { launch_muscl_egrad(d, s); });
         rec(m, "muscl_ngrad", [&] { launch_muscl_ngrad(d, s); });
         rec(m, "muscl_edge", [&] { launch_muscl_edge(d, s); });
@@ -647,7 +658,9 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (mesh->nsigma < 5 || mesh->nsigma > 127 || mesh->nod2D < 3 || mesh->elem2D < 1) return FESOMC_EINVAL;
     if (par->Mt < 1 || par->dt <= 0.0 || par->dt_2D <= 0.0) return FESOMC_EINVAL;
     if (par->ver_mix != 3 && par->ver_mix != 0) return FESOMC_EINVAL;
-    if (par->tracer_adv != FESOMC_TRACER_UPWIND && par->tracer_adv != FESOMC_TRACER_MUSCL) return FESOMC_EINVAL;
+    if (par->tracer_adv != FESOMC_TRACER_UPWIND && par->tracer_adv != FESOMC_TRACER_MUSCL &&
+        par->tracer_adv != FESOMC_TRACER_MIURA)
+        return FESOMC_EINVAL;
     if (par->tracer_adv == FESOMC_TRACER_MUSCL && !mesh->edge_up_dn_tri) return FESOMC_EINVAL;
     if (par->cl_solid_boder_relax) return FESOMC_EINVAL;
     if (par->mom_adv_2D != 2 && par->mom_adv_2D != 0) return FESOMC_EINVAL;

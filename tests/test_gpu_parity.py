@@ -83,6 +83,25 @@ def test_estuary_upwind_implicit_visc_bit_exact(mods):
     assert bad == []
 
 
+def test_estuary_miura_bit_exact(mods):
+    """solve_tracer_miura (temperature only, salinity passes through
+    advection) with wetting/drying, tides and rivers."""
+    abi, cases, model, pyoracle = mods
+    case = cases.estuary("small", tracer_adv=abi.TRACER_MIURA)
+    bad, eg, eo = run_pair(mods, case, 20)
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+
+
+def test_le_medium_miura_bit_exact(mods):
+    abi, cases, model, pyoracle = mods
+    case = cases.le_medium()
+    case.params.Mt = 4
+    case.params.tracer_adv = abi.TRACER_MIURA
+    bad, _, _ = run_pair(mods, case, 20)
+    assert bad == []
+
+
 def test_estuary_both_vertical_viscosities_and_fic_points(mods):
     abi, cases, model, pyoracle = mods
     for fic in (0, 2):

@@ -78,6 +78,26 @@ def test_estuary_small_stable(mods):
     o.close()
 
 
+def test_estuary_miura_oracle_advects_temperature_only(mods):
+    """tracer_adv = 4 advances T with the Miura scheme and leaves S to the
+    river source and vertical diffusion (fv_main.F90:1790-1799)."""
+    abi, cases, pyoracle = mods
+    case = cases.estuary("small", tracer_adv=abi.TRACER_MIURA, key_rivers=0)
+    o = pyoracle.Oracle(case, abi, cases)
+    s0 = o.state()
+    rc = o.step(10)
+    s = o.state()
+    assert rc == 0
+    assert np.all(np.isfinite(s["TF"]))
+    assert not np.array_equal(s["TF"], s0["TF"])
+    # without rivers, S only diffuses vertically: column means are kept
+    L = case.mesh.L
+    m0 = s0["SF"].reshape(-1, L).mean(axis=1)
+    m1 = s["SF"].reshape(-1, L).mean(axis=1)
+    assert np.max(np.abs(m1 - m0)) < 0.05
+    o.close()
+
+
 def test_estuary_oracle_negative_salinity_flag(mods):
     """A river source of absurdly negative salinity (injected on the host)
     drives salinity below zero; the check of fv_tracer.F90:1469-1473 (which
