@@ -47,17 +47,28 @@ __global__ void k_minmax_part(Dev d) {
         for (int k = 0; k < 4; ++k) d.mm_part[(size_t)blockIdx.x * 4 + k] = s[k][0];
 }
 
+// min / max are exact, so the order in which the partials are combined does
+// not change the result
 __global__ void k_minmax_final(Dev d, int nparts) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0) return;
+    const int lane = threadIdx.x & 31;
     double tmin = d.mm_part[0], tmax = d.mm_part[1], smin = d.mm_part[2], smax = d.mm_part[3];
-    for (int b = 1; b < nparts; ++b) {
+    for (int b = lane; b < nparts; b += 32) {
         tmin = dmin(tmin, d.mm_part[4 * b + 0]);
         tmax = dmax(tmax, d.mm_part[4 * b + 1]);
         smin = dmin(smin, d.mm_part[4 * b + 2]);
         smax = dmax(smax, d.mm_part[4 * b + 3]);
     }
-    d.aver[0] = 0.5 * (tmin + tmax);
-    d.aver[1] = 0.5 * (smin + smax);
+    for (int o = 16; o > 0; o >>= 1) {
+        tmin = dmin(tmin, __shfl_xor_sync(kFull, tmin, o));
+        tmax = dmax(tmax, __shfl_xor_sync(kFull, tmax, o));
+        smin = dmin(smin, __shfl_xor_sync(kFull, smin, o));
+        smax = dmax(smax, __shfl_xor_sync(kFull, smax, o));
+    }
+    if (lane == 0) {
+        d.aver[0] = 0.5 * (tmin + tmax);
+        d.aver[1] = 0.5 * (smin + smax);
+    }
 }
 
 // AB2 value of a tracer at (node, level) minus its mean (fv_tracer.F90:433)

@@ -413,7 +413,7 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     // element fields read / written once; edge fluxes of its internal edges
     if (k == "u2d_elem")
         return N * 56 + E * (16 + 8 + 32 + 8 + 64 + 16 + 8 + 16 + 16 + 16 + 16 + 32 + 16 + 16 + 16 + 16) +
-               2 * Ei * 16 + E * (8 + 16 + 16 + 16 + 16);
+               Ei * 16 + E * (8 + 16 + 16 + 16 + 16);
     if (k == "rot_nodes") return N * 48;
     if (k == "pressure_col") return L * N * 16 + N * 16 + L * N * 8 + NS * N * 8;
     if (k == "bpg_elem") return NS * N * 8 + N * 48 + E * (96 + 16 + 8 + 8) + L * E * 8 + L * E * 16 + E * 32;
@@ -423,13 +423,13 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     if (k == "velgrad3d") return L * E * 16 + E * (48 + 64 + 8) + L * E * 32;
     if (k == "adv3_edge") return L * E * 48 + N * 24 + Ei * 64 + E * 8 + L * Ei * 16;
     if (k == "velrhs")
-        return L * E * (48 + 24) + L * Ei * 16 * 2 + NS * N * 8 + N * 16 + E * 168 + L * E * 32;
+        return L * E * (48 + 24) + L * Ei * 16 + NS * N * 8 + N * 16 + E * 168 + L * E * 32;
     if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 16) + L * E * 16 + L * E * 16;
     if (k == "zero_filt") return E * 16 + E * 8 + E * 16 + E * 32;
     if (k == "puls_elem") return L * E * 16 + E * 16 + N * 24 + E * 48 + L * E * 16 + E * 8;
     if (k == "p1_edge") return L * N * 16 + N * 16 + Ei * 32 + E * 8 + L * Ei * 16;
     if (k == "p1_elem")
-        return 2 * L * Ei * 16 + E * (16 + 16 + 16) + Ei * 8 + N * 8 + L * E * 8 +
+        return L * Ei * 16 + E * (16 + 16 + 16) + Ei * 8 + N * 8 + L * E * 8 +
                (d.filt_3D ? L * E * 16 + E * 24 : 0.0);
     if (k == "jac_swap") return N * 32;
     if (k == "update3d") return L * E * (16 + 8 + 32 + 24) + N * 24 + E * 48 + E * 32 + E * 16;
@@ -441,7 +441,7 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
         return (L * N * 24 + N * 24 + L * N * 16) + (L * N * 8 + E * 80 + L * E * 16) +
                (L * E * 16 + N * 4 + 4 * (4.0 * E) + E * 8 + L * N * 16) +
                (L * N * 40 + N * 8 + L * E * 48 + Ed * 64 + E * 8 + L * Ed * 32) +
-               (2 * L * Ed * 32 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 32 + L * N * 32);
+               (L * Ed * 32 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 32 + L * N * 32);
     // tracer gathers: AB2 tracers (2 per node level), Je and transports per
     // element level, W per node interface, T/S of the node, edge geometry,
     // and the four outputs per node level
@@ -453,10 +453,10 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     // elements or the node fallback), Je / transports of the 2 elements,
     // edge geometry; 3 flux pairs per (edge, level) written
     if (k == "muscl_edge") return L * N * 16 + L * E * 32 + L * N * 32 + L * E * 40 + Ed * 64 + E * 8 + L * Ed * 48;
-    // node pass: flux pairs of the node's edges (each edge by its 2 nodes),
+    // node pass: flux pairs of the node's edges (each array counted once),
     // AB2 tracers, W, T/S, outputs
     if (k == "muscl_h")
-        return 2 * L * Ed * 48 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 16 + N * 28 + L * N * 32;
+        return L * Ed * 48 + 4 * nnz_ne + N * 4 + L * N * 16 + NS * N * 8 + L * N * 16 + N * 28 + L * N * 32;
     if (k == "vdiff_col") return L * N * 32 + NS * N * 8 + N * 16 + L * N * 32;
     return 0.0;
 }
