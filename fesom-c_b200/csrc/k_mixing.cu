@@ -24,159 +24,21 @@ __device__ __forceinline__ bool d3_above_tol(double a, double b) {
     return fabs(a / b) >= 1.0e-6;
 }
 
-// One iteration of the implicit turbulence-energy sweep of d3_end
-// (fv_mixing.F90:204-266) on register arrays indexed 1..NS; STORE writes
-// tke_dissip (the reference writes it in every iteration; only the last
-// one survives).  Returns true when converged (btr left unchanged),
-// otherwise replaces btr by the new solution.
-template <int NS, int BD, bool STORE>
-__device__ __forceinline__ bool d3_iterate(double (&btr)[NS + 1], double (&xx1)[NS + 1], double (&yy1)[NS + 1],
-                                           const double *col, double t_inv, double bot, double *tke) {
-#define PRM(a, k) col[((a) * NS + (k)) * BD]
-    enum { SN = 0, PB, QB, C2, AM, CM };
-#pragma unroll
-    for (int nz = 2; nz <= NS - 1; ++nz) {
-        const double b = btr[nz], sn = PRM(SN, nz);
-        const double c1 = 0.046 * (b * b) / sn;
-        if (STORE) tke[nz - 1] = c1;
-        const double fr = PRM(PB, nz) - c1 - PRM(QB, nz) - PRM(C2, nz);
-        const double am = PRM(AM, nz), cm = PRM(CM, nz);
-        const double bm = am + cm + (2.0 * 0.046 * b) / sn + t_inv;
-        const double a = bm - am * xx1[nz];
-        xx1[nz + 1] = cm / a;
-        yy1[nz + 1] = (am * yy1[nz] - fr) / a;
-    }
-#undef PRM
-    double btr1[NS + 1];
-    btr1[NS] = bot;
-#pragma unroll
-    for (int nz = NS; nz >= 2; --nz) btr1[nz - 1] = btr1[nz] * xx1[nz] + yy1[nz];
-    bool above = false;
-#pragma unroll
-    for (int nz = 1; nz <= NS; ++nz) above |= d3_above_tol(btr[nz] - btr1[nz], dmax(btr1[nz], btr[nz]) + 1.0e-8);
-    if (!above) return true;
-#pragma unroll
-    for (int nz = 1; nz <= NS; ++nz) btr[nz] = btr1[nz];
-    return false;
-}
-
-// d3_end, fully unrolled for a compile-time level count: the iterated state
-// (btr, xx1, yy1) stays in registers, the iteration-independent terms of
-// each level in shared memory ([term][level][thread]).  One thread per node
-// column.
-template <int NS, int BD>
-__global__ void __launch_bounds__(BD) k_d3end_r(Dev d) {
-    extern __shared__ double sm[];
-    double *col = sm + threadIdx.x;
-#define PRM(a, k) col[((a) * NS + (k)) * BD]
-    enum { SN = 0, PB, QB, C2, AM, CM };
-    constexpr int L = NS - 1;
-    const double t_inv = 1.0 / d.dt;
-    const double cka = d.cka;
-    const double B1cka2 = 16.6 * (cka * cka);
-    GRID_LOOP(ii, d.N) {
-        const int node = (int)ii;
-        const double *bt = d.bt + (size_t)node * NS;
-        const double *snu = d.snu + (size_t)node * NS;
-        const double *Kv = d.Kv + (size_t)node * NS;
-        const double *Un = d.Unode + (size_t)node * L;
-        const double *Vn = d.Vnode + (size_t)node * L;
-        const double *T = d.TF + (size_t)node * L;
-        const double *S = d.SF + (size_t)node * L;
-        double *Ri = d.Ri + (size_t)node * NS;
-        double *tke = d.tke_dissip + (size_t)node * NS;
-        const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
-        const double dmean2 = dmean * dmean;
-        const double ajac = jac_a(d, d.eta_jac, node);
-        // arrays indexed 1..NS like the Fortran ones
-        double btr[NS + 1], xx1[NS + 1], yy1[NS + 1];
-#pragma unroll
-        for (int nz = 1; nz <= NS; ++nz) btr[nz] = bt[nz - 1];
-        Ri[0] = 0.0;
-        Ri[NS - 1] = 0.0;
-#pragma unroll
-        for (int nz = 2; nz <= NS - 1; ++nz) {
-            const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
-            const double d1 = s_m - s_0;
-            const double d2 = s_0 - s_p;
-            const double dd = 0.5 * (d1 + d2);
-            const double sn_m = snu[nz - 2], sn_0 = snu[nz - 1], sn_p = snu[nz];
-            double ap1 = Un[nz - 2] - Un[nz - 1];
-            const double ap2 = Vn[nz - 2] - Vn[nz - 1];
-            double b1 = sn_0 * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
-            b1 = b1 / dmean2;
-            const double zb = zbar_of(d, ajac, nz - 1);
-            const double rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
-            const double rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
-            ap1 = (rho_up - rho_dn) / dd;
-            const double b2 = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
-            const double snu_p = 0.5 * (sn_m + sn_0);
-            const double snu_m = 0.5 * (sn_0 + sn_p);
-            double c2 = 0.5 * 0.73 * (snu_p * (btr[nz - 1] - btr[nz]) / d1 - snu_m * (btr[nz] - btr[nz + 1]) / d2) / dd;
-            c2 = c2 / dmean2;
-            if (b1 > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn_0;
-            else Ri[nz - 1] = 10000.0;
-            PRM(SN, nz) = sn_0;
-            PRM(PB, nz) = -b1 - b2;
-            PRM(QB, nz) = t_inv * btr[nz];
-            PRM(C2, nz) = c2;
-            PRM(AM, nz) = 0.5 * (snu_p * 0.73) / (dmean2 * d1 * dd);
-            PRM(CM, nz) = 0.5 * (snu_m * 0.73) / (dmean2 * d2 * dd);
-        }
-        xx1[2] = 1.0;
-        {
-            const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
-            const double wx = d.windx[node], wy = d.windy[node];
-            const double u_din_sur = 0.05 * (wx * wx + wy * wy);
-            const double snu_m = 0.5 * (snu[NS - 1] + snu[NS - 2]);
-            yy1[2] = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
-        }
-        const double delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
-        const double lg = log(delta_b / d.z0b_min);
-        const double bott_R = B1cka2 / (lg * lg);
-        const double ubt = Un[L - 1], vbt = Vn[L - 1];
-        const double bot = bott_R * (ubt * ubt + vbt * vbt);
-        // iterations 1..199 without the tke_dissip stores, the 200th with them
-        bool converged = false;
-        for (int it = 1; it < 200 && !converged; ++it)
-            converged = d3_iterate<NS, BD, false>(btr, xx1, yy1, col, t_inv, bot, tke);
-        if (converged) {
-#pragma unroll
-            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / PRM(SN, nz);
-        } else {
-            converged = d3_iterate<NS, BD, true>(btr, xx1, yy1, col, t_inv, bot, tke);
-            if (!converged) atomicAdd(d.notconv, 1);
-        }
-        double *btw = d.bt + (size_t)node * NS;
-        double *snw = d.snu + (size_t)node * NS;
-        double *Kvw = d.Kv + (size_t)node * NS;
-#pragma unroll
-        for (int nz = 1; nz <= NS; ++nz) {
-            const double btn = dmax(btr[nz], 1.0e-8);
-            btw[nz - 1] = btn;
-            const double zt = __ldg(d.sig + nz - 1) * dmean;
-            const double Zh = zt + d.z0b_min;
-            const double Zd = fabs(dmean - zt) + d.z0s_min;
-            const double Z0 = 1.0 - d.beta_scale * Zh * Zd / (dmean * dmean);
-            const double scale_t = cka * Zh * Zd * Z0 / dmean;
-            double s = scale_t * sqrt(btn) + d.snul;
-            if (s >= 0.2) s = 0.2;
-            snw[nz - 1] = s;
-            Kvw[nz - 1] = d.Pr_num * s;
-        }
-    }
-#undef PRM
-}
-constexpr int kD3Terms = 6;
-
-// d3_end per node column, arrays indexed 1..NS like the Fortran ones (local
-// memory).  The terms that do not change over the iterations are formed
-// once per level: -b1-b2, t_inv*bo, c2, am, cm (the reference recomputes
-// am, cm in every iteration with the same expressions).  btr1(k) is kept in
-// xx1(k+1), which the back substitution no longer needs.  tke_dissip, which
-// the reference overwrites in every iteration, is written once from the
-// btr of the last iteration.
-template <int MAXNS>
+// d3_end per node column (local-memory arrays indexed 1..NS like the Fortran
+// ones, ARR >= NS + 1 entries each).  The kernel is bound by the traffic of
+// those arrays: the working set of the resident columns does not fit in L2,
+// so each iteration streams them through DRAM.  It therefore keeps the
+// array count and the accesses per level low:
+//   * -b1-b2, t_inv*bo and c2 are formed once per level; am and cm are
+//     recomputed in each iteration from snu(k-1..k+1) held in registers (the
+//     reference recomputes them the same way);
+//   * xx1(k), yy1(k) feed the next level from registers, the arrays only
+//     carry them to the back substitution;
+//   * btr and btr1 alternate between two arrays instead of being copied;
+//   * tke_dissip, which the reference overwrites in every iteration, is
+//     written once from the btr of the last iteration;
+//   * the convergence test forms the quotient only near the threshold.
+template <int ARR>
 __global__ void k_d3end(Dev d) {
     const double t_inv = 1.0 / d.dt;
     const double cka = d.cka;
@@ -193,13 +55,12 @@ __global__ void k_d3end(Dev d) {
         const double *S = d.SF + (size_t)node * L;
         double *Ri = d.Ri + (size_t)node * NS;
         double *tke = d.tke_dissip + (size_t)node * NS;
-        double xx1[MAXNS + 2], yy1[MAXNS + 2], btr[MAXNS + 2];
-        double pb[MAXNS + 2], qb[MAXNS + 2], c2[MAXNS + 2], am[MAXNS + 2], cm[MAXNS + 2], sn[MAXNS + 2];
+        double xx1[ARR], yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
         const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
         const double dmean2 = dmean * dmean;
         const double ajac = jac_a(d, d.eta_jac, node);
         for (int nz = 1; nz <= NS; ++nz) {
-            btr[nz] = bt[nz - 1];
+            bA[nz] = bt[nz - 1];
             sn[nz] = snu[nz - 1];
         }
         Ri[0] = 0.0;
@@ -220,51 +81,71 @@ __global__ void k_d3end(Dev d) {
             const double b2 = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
             const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
             const double snu_m = 0.5 * (sn[nz] + sn[nz + 1]);
-            double cc = 0.5 * 0.73 * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
+            const double cc = 0.5 * 0.73 * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
             c2[nz] = cc / dmean2;
             if (b1 > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn[nz];
             else Ri[nz - 1] = 10000.0;
             pb[nz] = -b1 - b2;
             qb[nz] = t_inv * bt[nz - 1];
-            am[nz] = 0.5 * (snu_p * 0.73) / (dmean2 * d1 * dd);
-            cm[nz] = 0.5 * (snu_m * 0.73) / (dmean2 * d2 * dd);
         }
+        double y2;
         {
             const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
             const double wx = d.windx[node], wy = d.windy[node];
             const double u_din_sur = 0.05 * (wx * wx + wy * wy);
             const double snu_m = 0.5 * (sn[NS] + sn[NS - 1]);
-            yy1[2] = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
+            y2 = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
         }
+        xx1[2] = 1.0;
+        yy1[2] = y2;
         // bottom boundary value (independent of the iteration)
         const double delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
         const double lg = log(delta_b / d.z0b_min);
         const double bott_R = B1cka2 / (lg * lg);
         const double ubt = Un[L - 1], vbt = Vn[L - 1];
         const double bot = bott_R * (ubt * ubt + vbt * vbt);
+        double *btr = bA, *btr1 = bB;
         bool converged = false;
         for (int it = 1; it <= 200; ++it) {
-            xx1[2] = 1.0;
+            double x = 1.0, y = y2;
+            double s_lo = sn[1], s_mid = sn[2];
             for (int nz = 2; nz <= NS - 1; ++nz) {
+                const double s_hi = sn[nz + 1];
+                const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const double dd1 = s_m - s_0;
+                const double dd2 = s_0 - s_p;
+                const double dd = 0.5 * (dd1 + dd2);
                 const double b = btr[nz];
-                const double c1 = 0.046 * (b * b) / sn[nz];
+                const double c1 = 0.046 * (b * b) / s_mid;
                 if (it == 200) tke[nz - 1] = c1;
                 const double fr = pb[nz] - c1 - qb[nz] - c2[nz];
-                const double bm = am[nz] + cm[nz] + (2.0 * 0.046 * b) / sn[nz] + t_inv;
-                const double a = bm - am[nz] * xx1[nz];
-                xx1[nz + 1] = cm[nz] / a;
-                yy1[nz + 1] = (am[nz] * yy1[nz] - fr) / a;
+                const double snu_p = 0.5 * (s_lo + s_mid);
+                const double snu_mm = 0.5 * (s_mid + s_hi);
+                const double am = 0.5 * (snu_p * 0.73) / (dmean2 * dd1 * dd);
+                const double cm = 0.5 * (snu_mm * 0.73) / (dmean2 * dd2 * dd);
+                const double bm = am + cm + (2.0 * 0.046 * b) / s_mid + t_inv;
+                const double a = bm - am * x;
+                const double xn = cm / a;
+                const double yn = (am * y - fr) / a;
+                xx1[nz + 1] = xn;
+                yy1[nz + 1] = yn;
+                x = xn;
+                y = yn;
+                s_lo = s_mid;
+                s_mid = s_hi;
             }
             double b1v = bot;  // btr1(NS)
+            btr1[NS] = b1v;
             bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + 1.0e-8);
             for (int nz = NS; nz >= 2; --nz) {
                 b1v = b1v * xx1[nz] + yy1[nz];  // btr1(nz-1)
-                xx1[nz] = b1v;
+                btr1[nz - 1] = b1v;
                 above |= d3_above_tol(btr[nz - 1] - b1v, dmax(b1v, btr[nz - 1]) + 1.0e-8);
             }
             if (!above) { converged = true; break; }
-            for (int nz = 1; nz <= NS - 1; ++nz) btr[nz] = xx1[nz + 1];
-            btr[NS] = bot;
+            double *t = btr;
+            btr = btr1;
+            btr1 = t;
         }
         if (converged) {
             for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / sn[nz];
@@ -304,17 +185,11 @@ __global__ void k_av(Dev d) {
     }
 }
 
-template <int NS>
-static size_t d3end_r_smem() { return (size_t)kD3Terms * NS * 64 * sizeof(double); }
-int config_d3end(const Dev &d) {
-    cudaError_t e = cudaSuccess;
-    if (d.NS == 11) e = cudaFuncSetAttribute(k_d3end_r<11, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d3end_r_smem<11>());
-    if (d.NS == 21) e = cudaFuncSetAttribute(k_d3end_r<21, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d3end_r_smem<21>());
-    return e == cudaSuccess ? 0 : 1;
-}
+int config_d3end(const Dev &d) { return d.NS <= 127 ? 0 : 1; }
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.NS <= 24) k_d3end<24><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    else if (d.NS <= 48) k_d3end<48><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    if (d.NS <= 11) k_d3end<12><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    else if (d.NS <= 21) k_d3end<22><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    else if (d.NS <= 40) k_d3end<41><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
 }
 void launch_av(const Dev &d, cudaStream_t s) { k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d); }
