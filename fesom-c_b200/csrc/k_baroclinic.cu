@@ -16,7 +16,7 @@
 //   je_elem      : Je, Ze, ZBe at init
 #include "device_common.cuh"
 
-namespace fesomc {
+FESOMC_PREC_BEGIN
 
 // Column blocks: B consecutive entities per block, one thread per (entity,
 // level), levels on consecutive threads (coalesced column access).  Level
@@ -33,8 +33,9 @@ struct ColBlock {
 // hydrostatic sum per node in level order
 // ---------------------------------------------------------------------------
 __global__ void k_pressure_col(Dev d) {
-    extern __shared__ double sm[];
-    const double gd0 = kG / d.density_0;
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
+    const real gd0 = kG / d.density_0;
     const int L = d.L, NS = d.NS;
     const ColBlock cb(L);
     const int S = L | 1;
@@ -43,16 +44,16 @@ __global__ void k_pressure_col(Dev d) {
         const bool act = cb.jl < cb.B && n_ < d.N;
         if (act) {
             const int n = (int)n_;
-            const double a = jac_a(d, d.eta_jac, n);
+            const real a = jac_a(d, d.eta_jac, n);
             const size_t i = (size_t)n * L + cb.z;
-            const double rho = density_jm(d.TF[i], d.SF[i], -z_of(d, a, cb.z), d.density_0);
+            const real rho = density_jm(d.TF[i], d.SF[i], -z_of(d, a, cb.z), d.density_0);
             d.rho_c[i] = rho;
             sm[cb.jl * S + cb.z] = rho * jc_of(d, a, cb.z) * gd0;
         }
         __syncthreads();
         if ((int)threadIdx.x < cb.B && nb + threadIdx.x < d.N) {
-            double *row = sm + threadIdx.x * S;
-            double hp = 0.0;
+            real *row = sm + threadIdx.x * S;
+            real hp = real(0.0);
             for (int k = 0; k < L; ++k) {
                 hp = hp + row[k];
                 row[k] = hp;
@@ -62,7 +63,7 @@ __global__ void k_pressure_col(Dev d) {
         if (act) {
             const size_t bs = (size_t)n_ * NS;
             d.hpressure[bs + cb.z + 1] = sm[cb.jl * S + cb.z];
-            if (cb.z == 0) d.hpressure[bs] = 0.0;
+            if (cb.z == 0) d.hpressure[bs] = real(0.0);
         }
         __syncthreads();
     }
@@ -73,7 +74,8 @@ __global__ void k_pressure_col(Dev d) {
 // element's surface pressure force of compute_vel_rhs (fv_3D_vel.F90:60-75),
 // the same for every level.
 __global__ void k_bpg_elem(Dev d) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L, NS = d.NS;
     const ColBlock cb(L);
     const int S = 2 * L + 1;
@@ -83,31 +85,31 @@ __global__ void k_bpg_elem(Dev d) {
             const int e = (int)e_, z = cb.z;
             const int4 en = d.elem_nodes[e];
             const int nd[4] = {en.x, en.y, en.z, en.w};
-            const double4 gx = d.gs_x[e], gy = d.gs_y[e], w = d.w_cv[e];
-            double dh[4], de[4];
+            const real4 gx = d.gs_x[e], gy = d.gs_y[e], w = d.w_cv[e];
+            real dh[4], de[4];
             for (int k = 0; k < 4; ++k) { dh[k] = d.depth[nd[k]] + d.eta_n[nd[k]]; de[k] = d.depth[nd[k]]; }
-            const double Ax = wsum(gx, dh[0], dh[1], dh[2], dh[3]);
-            const double Ay = wsum(gy, dh[0], dh[1], dh[2], dh[3]);
-            const double Bx = wsum(gx, de[0], de[1], de[2], de[3]);
-            const double By = wsum(gy, de[0], de[1], de[2], de[3]);
-            const double fac = d.elem_bpfac[e];
-            const double4 ae = elem_jac_a(d, d.eta_jac, en);
-            const double an[4] = {ae.x, ae.y, ae.z, ae.w};
-            const double je = d.Je[(size_t)e * L + z];
-            const double accJe_inv = -fac / je;
-            double hu[4], hl[4], pre[4];
+            const real Ax = wsum(gx, dh[0], dh[1], dh[2], dh[3]);
+            const real Ay = wsum(gy, dh[0], dh[1], dh[2], dh[3]);
+            const real Bx = wsum(gx, de[0], de[1], de[2], de[3]);
+            const real By = wsum(gy, de[0], de[1], de[2], de[3]);
+            const real fac = d.elem_bpfac[e];
+            const real4 ae = elem_jac_a(d, d.eta_jac, en);
+            const real an[4] = {ae.x, ae.y, ae.z, ae.w};
+            const real je = d.Je[(size_t)e * L + z];
+            const real accJe_inv = -fac / je;
+            real hu[4], hl[4], pre[4];
             for (int k = 0; k < 4; ++k) {
                 hu[k] = d.hpressure[(size_t)nd[k] * NS + z];
                 hl[k] = d.hpressure[(size_t)nd[k] * NS + z + 1];
-                pre[k] = 0.5 * (hu[k] + hl[k]) * jc_of(d, an[k], z);
+                pre[k] = real(0.5) * (hu[k] + hl[k]) * jc_of(d, an[k], z);
             }
-            const double qd_up = wsum(w, hu[0], hu[1], hu[2], hu[3]);
-            const double qd_low = wsum(w, hl[0], hl[1], hl[2], hl[3]);
-            const double sx = wsum(gx, pre[0], pre[1], pre[2], pre[3]);
-            const double sy = wsum(gy, pre[0], pre[1], pre[2], pre[3]);
-            const double s0 = __ldg(d.sig + z), s1 = __ldg(d.sig + z + 1);
-            const double bu = accJe_inv * (sx + qd_low * (s1 * Ax - Bx) - qd_up * (s0 * Ax - Bx));
-            const double bv = accJe_inv * (sy + qd_low * (s1 * Ay - By) - qd_up * (s0 * Ay - By));
+            const real qd_up = wsum(w, hu[0], hu[1], hu[2], hu[3]);
+            const real qd_low = wsum(w, hl[0], hl[1], hl[2], hl[3]);
+            const real sx = wsum(gx, pre[0], pre[1], pre[2], pre[3]);
+            const real sy = wsum(gy, pre[0], pre[1], pre[2], pre[3]);
+            const real s0 = __ldg(d.sig + z), s1 = __ldg(d.sig + z + 1);
+            const real bu = accJe_inv * (sx + qd_low * (s1 * Ax - Bx) - qd_up * (s0 * Ax - Bx));
+            const real bv = accJe_inv * (sy + qd_low * (s1 * Ay - By) - qd_up * (s0 * Ay - By));
             d.Bar_pru[(size_t)e * L + z] = bu;
             d.Bar_prv[(size_t)e * L + z] = bv;
             sm[cb.jl * S + z] = bu * je;
@@ -117,8 +119,8 @@ __global__ void k_bpg_elem(Dev d) {
         const long long es = eb + threadIdx.x;
         if ((int)threadIdx.x < cb.B && es < d.E) {
             const int e = (int)es;
-            const double *row = sm + threadIdx.x * S;
-            double b1 = 0.0, b2 = 0.0;
+            const real *row = sm + threadIdx.x * S;
+            real b1 = real(0.0), b2 = real(0.0);
             for (int k = 0; k < L; ++k) {
                 b1 = b1 + row[k];
                 b2 = b2 + row[L + k];
@@ -126,12 +128,12 @@ __global__ void k_bpg_elem(Dev d) {
             d.Bar_pr_2D[e] = make_double2(b1, b2);
             const int4 en = d.elem_nodes[e];
             const int nd[4] = {en.x, en.y, en.z, en.w};
-            const double4 gx = d.gs_x[e], gy = d.gs_y[e];
-            double pr[4];
+            const real4 gx = d.gs_x[e], gy = d.gs_y[e];
+            real pr[4];
             for (int k = 0; k < 4; ++k)
                 pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
-            const double ar = d.elem_area[e];
-            d.Fp[e] = make_double2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
+            const real ar = d.elem_area[e];
+            d.Fp[e] = make_real2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
         }
         __syncthreads();
     }
@@ -149,24 +151,24 @@ __global__ void k_velgrad3d(Dev d) {
         const int4 ee = d.elem_edges[e];
         const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
         const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
-        const double4 gx = d.gv_x[e], gy = d.gv_y[e];
-        const double gxa[4] = {gx.x, gx.y, gx.z, gx.w};
-        const double gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const real4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
         const int jend = (en.x == en.w) ? 3 : 4;
-        const double u0 = d.U_n[ii], v0 = d.V_n[ii];
-        double a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+        const real u0 = d.U_n[ii], v0 = d.V_n[ii];
+        real a1 = real(0.0), a2 = real(0.0), a3 = real(0.0), a4 = real(0.0);
         for (int j = 0; j < jend; ++j) {
             const int e2 = nbs[j];
             if (e2 >= 0) {
-                const double u2 = d.U_n[(size_t)e2 * L + z], v2 = d.V_n[(size_t)e2 * L + z];
+                const real u2 = d.U_n[(size_t)e2 * L + z], v2 = d.V_n[(size_t)e2 * L + z];
                 a1 = a1 + gxa[j] * (u2 - u0);
                 a2 = a2 + gya[j] * (u2 - u0);
                 a3 = a3 + gxa[j] * (v2 - v0);
                 a4 = a4 + gya[j] * (v2 - v0);
             } else {
-                const double2 dxy = d.edge_dxdy[eds[j]];
-                const double zc1 = dxy.x * d.elem_cos[e], zc2 = dxy.y;
-                const double un = -2.0 * (u0 * zc2 - v0 * zc1) / (zc1 * zc1 + zc2 * zc2);
+                const real2 dxy = d.edge_dxdy[eds[j]];
+                const real zc1 = dxy.x * d.elem_cos[e], zc2 = dxy.y;
+                const real un = -real(2.0) * (u0 * zc2 - v0 * zc1) / (zc1 * zc1 + zc2 * zc2);
                 a1 = a1 + gxa[j] * un * zc2;
                 a2 = a2 + gya[j] * un * zc2;
                 a3 = a3 - gxa[j] * un * zc1;
@@ -181,63 +183,63 @@ __global__ void k_velgrad3d(Dev d) {
 }
 
 // w-weighted element mean of a node column value: SUM(w_cv*X(k,nodes))
-__device__ __forceinline__ double wsum_col(const double4 &w, const double *X, int stride, const int4 &en, int k) {
+__device__ __forceinline__ real wsum_col(const real4 &w, const real *X, int stride, const int4 &en, int k) {
     return wsum(w, X[(size_t)en.x * stride + k], X[(size_t)en.y * stride + k], X[(size_t)en.z * stride + k],
                 X[(size_t)en.w * stride + k]);
 }
-__device__ __forceinline__ double wsum_zbar(const Dev &d, const double4 &w, const double4 &a, int k) {
+__device__ __forceinline__ real wsum_zbar(const Dev &d, const real4 &w, const real4 &a, int k) {
     return wsum(w, zbar_of(d, a.x, k), zbar_of(d, a.y, k), zbar_of(d, a.z, k), zbar_of(d, a.w, k));
 }
-__device__ __forceinline__ double wsum_z(const Dev &d, const double4 &w, const double4 &a, int k) {
+__device__ __forceinline__ real wsum_z(const Dev &d, const real4 &w, const real4 &a, int k) {
     return wsum(w, z_of(d, a.x, k), z_of(d, a.y, k), z_of(d, a.z, k), z_of(d, a.w, k));
 }
 
 // Vertical momentum flux uvertAB(:,k) of momentum_vert_adv_upwind at interface
 // k (0-based, 0..NS-1) of element e (fv_advection.F90:389-443); the element
 // means of Z and zbar come from the stored Ze / ZBe.
-__device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const double4 &w, const int4 &en, double ar,
-                                         double &fu, double &fv) {
+__device__ __forceinline__ void uvert_at(const Dev &d, int e, int k, const real4 &w, const int4 &en, real ar,
+                                         real &fu, real &fv) {
     const int L = d.L, NS = d.NS;
-    const double *U = d.U_n + (size_t)e * L;
-    const double *V = d.V_n + (size_t)e * L;
-    if (k == NS - 1) { fu = 0.0; fv = 0.0; return; }
-    const double wv = wsum_col(w, d.Wvel, NS, en, k) * ar;
+    const real *U = d.U_n + (size_t)e * L;
+    const real *V = d.V_n + (size_t)e * L;
+    if (k == NS - 1) { fu = real(0.0); fv = real(0.0); return; }
+    const real wv = wsum_col(w, d.Wvel, NS, en, k) * ar;
     if (k == 0) { fu = -wv * U[0]; fv = -wv * V[0]; return; }
     const int nz = k + 1;  // 1-based interface index, 2..NS-1
-    const double *ZE = d.Ze + (size_t)e * L;   // ZE[m-1] = SUM(w*Z(m))
-    const double *ZB = d.ZBe + (size_t)e * L;  // ZB[m-1] = SUM(w*zbar(m))
-    double umean = 0.0, vmean = 0.0;
+    const real *ZE = d.Ze + (size_t)e * L;   // ZE[m-1] = SUM(w*Z(m))
+    const real *ZB = d.ZBe + (size_t)e * L;  // ZB[m-1] = SUM(w*zbar(m))
+    real umean = real(0.0), vmean = real(0.0);
     // U_n(m) 1-based  ->  U[m-1]
-    if (wv >= 0.0) {
+    if (wv >= real(0.0)) {
         if (nz == NS - 1) {
-            umean = 0.5 * (U[nz - 2] + U[nz - 1]);
-            vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
+            umean = real(0.5) * (U[nz - 2] + U[nz - 1]);
+            vmean = real(0.5) * (V[nz - 2] + V[nz - 1]);
         } else {
-            const double Z1 = ZB[nz - 1];
-            const double aa = Z1 - ZE[nz - 2];
-            const double bb = ZE[nz - 1] - Z1;
-            const double cc = ZE[nz] - Z1;
-            const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
-            const double dg = aa * bb * (aa + bb) / dd;
-            const double db = -aa * cc * (aa + cc) / dd;
-            const double da = 1.0 - dg - db;
+            const real Z1 = ZB[nz - 1];
+            const real aa = Z1 - ZE[nz - 2];
+            const real bb = ZE[nz - 1] - Z1;
+            const real cc = ZE[nz] - Z1;
+            const real dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
+            const real dg = aa * bb * (aa + bb) / dd;
+            const real db = -aa * cc * (aa + cc) / dd;
+            const real da = real(1.0) - dg - db;
             umean = U[nz - 2] * da + U[nz - 1] * db + U[nz] * dg;
             vmean = V[nz - 2] * da + V[nz - 1] * db + V[nz] * dg;
         }
     }
-    if (wv < 0.0) {
+    if (wv < real(0.0)) {
         if (nz == 2) {
-            umean = 0.5 * (U[nz - 2] + U[nz - 1]);
-            vmean = 0.5 * (V[nz - 2] + V[nz - 1]);
+            umean = real(0.5) * (U[nz - 2] + U[nz - 1]);
+            vmean = real(0.5) * (V[nz - 2] + V[nz - 1]);
         } else {
-            const double Z1 = ZB[nz - 1];
-            const double aa = ZE[nz - 1] - Z1;
-            const double bb = Z1 - ZE[nz - 2];
-            const double cc = Z1 - ZE[nz - 3];
-            const double dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
-            const double dg = aa * bb * (aa + bb) / dd;
-            const double db = -aa * cc * (aa + cc) / dd;
-            const double da = 1.0 - dg - db;
+            const real Z1 = ZB[nz - 1];
+            const real aa = ZE[nz - 1] - Z1;
+            const real bb = Z1 - ZE[nz - 2];
+            const real cc = Z1 - ZE[nz - 3];
+            const real dd = (cc + aa) * (bb * bb - aa * aa) - (cc * cc - aa * aa) * (bb + aa);
+            const real dg = aa * bb * (aa + bb) / dd;
+            const real db = -aa * cc * (aa + cc) / dd;
+            const real da = real(1.0) - dg - db;
             umean = U[nz - 1] * da + U[nz - 2] * db + U[nz - 3] * dg;
             vmean = V[nz - 1] * da + V[nz - 2] * db + V[nz - 3] * dg;
         }
@@ -258,21 +260,21 @@ __global__ void k_adv3_edge(Dev d) {
         const int z = (int)(ii % L);
         const int2 nn = d.edge_nodes[ed];
         const int2 et = d.edge_tri[ed];
-        const double acc = 0.5 * (d.ac[nn.x] + d.ac[nn.y]);
-        const double4 X = d.edge_cross[ed];
+        const real acc = real(0.5) * (d.ac[nn.x] + d.ac[nn.y]);
+        const real4 X = d.edge_cross[ed];
         const size_t i1 = (size_t)et.x * L + z, i2 = (size_t)et.y * L + z;
-        const double u1 = d.U_n[i1] - d.vgux[i1] * X.x - d.vguy[i1] * X.y;
-        const double v1 = d.V_n[i1] - d.vgvx[i1] * X.x - d.vgvy[i1] * X.y;
-        const double u2 = d.U_n[i2] - d.vgux[i2] * X.z - d.vguy[i2] * X.w;
-        const double v2 = d.V_n[i2] - d.vgvx[i2] * X.z - d.vgvy[i2] * X.w;
-        const double jd = 0.5 * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
-        const double2 dxy = d.edge_dxdy[ed];
-        const double un = 0.5 * kREarth * jd *
+        const real u1 = d.U_n[i1] - d.vgux[i1] * X.x - d.vguy[i1] * X.y;
+        const real v1 = d.V_n[i1] - d.vgvx[i1] * X.x - d.vgvy[i1] * X.y;
+        const real u2 = d.U_n[i2] - d.vgux[i2] * X.z - d.vguy[i2] * X.w;
+        const real v2 = d.V_n[i2] - d.vgvx[i2] * X.z - d.vgvy[i2] * X.w;
+        const real jd = real(0.5) * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
+        const real2 dxy = d.edge_dxdy[ed];
+        const real un = real(0.5) * kREarth * jd *
                           ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
-        double uu, vv;
-        if (un >= 0.0) { uu = u1 * un * acc; vv = v1 * un * acc; }
+        real uu, vv;
+        if (un >= real(0.0)) { uu = u1 * un * acc; vv = v1 * un * acc; }
         else { uu = u2 * un * acc; vv = v2 * un * acc; }
-        d.adv3[ii] = make_double2(uu, vv);
+        d.adv3[ii] = make_real2(uu, vv);
     }
 }
 
@@ -282,7 +284,7 @@ __global__ void k_adv3_edge(Dev d) {
 // that the vertical flux at interface z+1 comes from the next lane.
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
+__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, real ff) {
     const long long total = (long long)d.E * d.L;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -293,18 +295,18 @@ __global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
         const int z = (int)(ii % d.L);
         const int L = d.L;
         const int4 en = d.elem_nodes[e];
-        const double4 w = d.w_cv[e];
-        const double ar = d.elem_area[e];
-        const double je = d.Je[ii];
+        const real4 w = d.w_cv[e];
+        const real ar = d.elem_area[e];
+        const real je = d.Je[ii];
         // pressure force from eta_n (per element, from bpg_elem)
-        const double2 F = d.Fp[e];
-        const double Fx = F.x, Fy = F.y;
-        const double un0 = d.U_n[ii], vn0 = d.V_n[ii];
-        double ur = -(0.5 + d.epsilon) * d.U_rhsAB[ii] + Fx * je;
-        double vr = -(0.5 + d.epsilon) * d.V_rhsAB[ii] + Fy * je;
-        const double cor = d.coriolis[e];
-        double uab = vn0 * cor * ar * je;
-        double vab = -un0 * cor * ar * je;
+        const real2 F = d.Fp[e];
+        const real Fx = F.x, Fy = F.y;
+        const real un0 = d.U_n[ii], vn0 = d.V_n[ii];
+        real ur = -(real(0.5) + d.epsilon) * d.U_rhsAB[ii] + Fx * je;
+        real vr = -(real(0.5) + d.epsilon) * d.V_rhsAB[ii] + Fy * je;
+        const real cor = d.coriolis[e];
+        real uab = vn0 * cor * ar * je;
+        real vab = -un0 * cor * ar * je;
         // horizontal upwind momentum advection (fv_advection.F90:114-188):
         // edge fluxes in edge order
         if (d.mom_adv_3D == 1) {
@@ -313,7 +315,7 @@ __global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
             for (int c = 0; c < 4; ++c) {
                 const int code = codes[c];
                 if (code < 0) break;
-                const double2 f = d.adv3[(size_t)(code >> 1) * L + z];
+                const real2 f = d.adv3[(size_t)(code >> 1) * L + z];
                 if (code & 1) { uab = uab + f.x; vab = vab + f.y; }
                 else { uab = uab - f.x; vab = vab - f.y; }
             }
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
             const int4 nb = d.elem_nb[e];
             const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
             const int jend = (en.x == en.w) ? 3 : 4;
-            double u1 = 0.0, v1 = 0.0;
+            real u1 = real(0.0), v1 = real(0.0);
             for (int j = 0; j < jend; ++j)
                 if (nbs[j] >= 0) {
                     u1 = u1 + d.U_n[(size_t)nbs[j] * L + z] - un0;
@@ -334,29 +336,29 @@ __global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, double ff) {
         }
         // vertical advection (fv_advection.F90:354-469): flux at interface z
         // here, at z+1 from the next lane (same element) or computed
-        const double mwd = d.mask_wd[e];
+        const real mwd = d.mask_wd[e];
         if (d.vert_adv == 1) {
-            double fu0, fv0;
+            real fu0, fv0;
             uvert_at(d, e, z, w, en, ar, fu0, fv0);
-            double fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
-            if (z == L - 1) { fu1 = 0.0; fv1 = 0.0; }
+            real fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
+            if (z == L - 1) { fu1 = real(0.0); fv1 = real(0.0); }
             else if (lane == 31) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
-            if (mwd != 0.0) {
-                const double acc = d.elem_acc[e];
+            if (mwd != real(0.0)) {
+                const real acc = d.elem_acc[e];
                 uab = uab + (fu0 - fu1) * acc;
                 vab = vab + (fv0 - fv1) * acc;
             } else {
-                uab = 0.0;
-                vab = 0.0;
+                uab = real(0.0);
+                vab = real(0.0);
             }
         }
         if (valid) {
             d.U_rhsAB[ii] = uab;
             d.V_rhsAB[ii] = vab;
-            const double area_inv = 1.0 / ar;
-            const double dt = d.dt;
-            d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + 0.0) / je);
-            d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + 0.0) / je);
+            const real area_inv = real(1.0) / ar;
+            const real dt = d.dt;
+            d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + real(0.0)) / je);
+            d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + real(0.0)) / je);
         }
     }
 }
@@ -370,43 +372,43 @@ __global__ void k_implvisc(Dev d) {
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
         const int L = d.L, NS = d.NS;
-        double *ur = d.U_rhs + (size_t)e * L;
-        double *vr = d.V_rhs + (size_t)e * L;
-        const double *Av = d.Av + (size_t)e * NS;
-        const double mwd = d.mask_wd[e];
-        const double dt = d.dt;
-        const double ub = d.U_n[(size_t)e * L + L - 1], vb = d.V_n[(size_t)e * L + L - 1];
-        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[e]) * d.Cd_bz + 1.0);
-        const double *je = d.Je + (size_t)e * L;
+        real *ur = d.U_rhs + (size_t)e * L;
+        real *vr = d.V_rhs + (size_t)e * L;
+        const real *Av = d.Av + (size_t)e * NS;
+        const real mwd = d.mask_wd[e];
+        const real dt = d.dt;
+        const real ub = d.U_n[(size_t)e * L + L - 1], vb = d.V_n[(size_t)e * L + L - 1];
+        const real a_Cd = d.C_d * ((real(1.0) - d.elem_acc[e]) * d.Cd_bz + real(1.0));
+        const real *je = d.Je + (size_t)e * L;
         if (d.im_vert_visc) {
-            double a[MAXL], b[MAXL], c[MAXL], cp[MAXL], up[MAXL], vp[MAXL], uu[MAXL], vv[MAXL];
-            const double *zc = d.Ze + (size_t)e * L;
+            real a[MAXL], b[MAXL], c[MAXL], cp[MAXL], up[MAXL], vp[MAXL], uu[MAXL], vv[MAXL];
+            const real *zc = d.Ze + (size_t)e * L;
             for (int z = 1; z <= L - 2; ++z) {
-                const double zinv = dt / je[z];
+                const real zinv = dt / je[z];
                 a[z] = -Av[z] / (zc[z] - zc[z - 1]) * zinv;
                 c[z] = -Av[z + 1] / (zc[z + 1] - zc[z]) * zinv;
-                b[z] = -a[z] - c[z] + 1.0;
+                b[z] = -a[z] - c[z] + real(1.0);
             }
-            double zinv = dt / je[L - 1];
+            real zinv = dt / je[L - 1];
             a[L - 1] = -Av[L - 1] / (zc[L - 1] - zc[L - 2]) * zinv;
-            b[L - 1] = -a[L - 1] + 1.0;
-            c[L - 1] = 0.0;
+            b[L - 1] = -a[L - 1] + real(1.0);
+            c[L - 1] = real(0.0);
             zinv = dt / je[0];
             c[0] = -Av[1] / (zc[1] - zc[0]) * zinv;
-            a[0] = 0.0;
-            b[0] = -c[0] + 1.0;
+            a[0] = real(0.0);
+            b[0] = -c[0] + real(1.0);
             for (int z = 0; z < L; ++z) { uu[z] = ur[z]; vv[z] = vr[z]; }
             uu[0] = uu[0] + zinv * d.taux[e] / d.density_0;
             vv[0] = vv[0] + zinv * d.tauy[e] / d.density_0;
             zinv = dt / je[L - 1];
-            const double friction = -a_Cd * sqrt(ub * ub + vb * vb);
+            const real friction = -a_Cd * sqrt(ub * ub + vb * vb);
             uu[L - 1] = uu[L - 1] + zinv * friction * ub;
             vv[L - 1] = vv[L - 1] + zinv * friction * vb;
             cp[0] = c[0] / b[0];
             up[0] = uu[0] / b[0];
             vp[0] = vv[0] / b[0];
             for (int z = 1; z < L; ++z) {
-                const double m = b[z] - cp[z - 1] * a[z];
+                const real m = b[z] - cp[z - 1] * a[z];
                 cp[z] = c[z] / m;
                 up[z] = (uu[z] - up[z - 1] * a[z]) / m;
                 vp[z] = (vv[z] - vp[z - 1] * a[z]) / m;
@@ -420,35 +422,35 @@ __global__ void k_implvisc(Dev d) {
             for (int z = 0; z < L; ++z) { ur[z] = uu[z] * mwd; vr[z] = vv[z] * mwd; }
         }
         if (d.im_vert_visc_fic) {
-            if (mwd != 0.0) {
-                double xx1[MAXL + 2], yu[MAXL + 2], yv[MAXL + 2];
-                xx1[0] = 1.0;
-                double de = je[0] / (Av[0] + Av[1]);
-                const double rw = de / d.density_0;
+            if (mwd != real(0.0)) {
+                real xx1[MAXL + 2], yu[MAXL + 2], yv[MAXL + 2];
+                xx1[0] = real(1.0);
+                real de = je[0] / (Av[0] + Av[1]);
+                const real rw = de / d.density_0;
                 yu[0] = d.taux[e] * rw;
                 yv[0] = d.tauy[e] * rw;
                 for (int z = 0; z < L; ++z) {
-                    const double Fx = ur[z], Fy = vr[z];
-                    const double d1 = (z == 0) ? 0.5 * je[z] : 0.5 * (je[z] + je[z - 1]);
-                    const double d2 = (z == L - 1) ? 0.5 * je[z] : 0.5 * (je[z] + je[z + 1]);
-                    const double zt = dt / je[z];
-                    const double a = zt * Av[z] / d1;
-                    const double c = zt * Av[z + 1] / d2;
-                    const double b = a + c + 1.0;
-                    const double dd = b - a * xx1[z];
+                    const real Fx = ur[z], Fy = vr[z];
+                    const real d1 = (z == 0) ? real(0.5) * je[z] : real(0.5) * (je[z] + je[z - 1]);
+                    const real d2 = (z == L - 1) ? real(0.5) * je[z] : real(0.5) * (je[z] + je[z + 1]);
+                    const real zt = dt / je[z];
+                    const real a = zt * Av[z] / d1;
+                    const real c = zt * Av[z + 1] / d2;
+                    const real b = a + c + real(1.0);
+                    const real dd = b - a * xx1[z];
                     xx1[z + 1] = c / dd;
                     yu[z + 1] = (a * yu[z] + Fx) / dd;
                     yv[z + 1] = (a * yv[z] + Fy) / dd;
                 }
                 de = je[L - 1] / (Av[NS - 1] + Av[L - 1]);
-                const double friction = de * a_Cd * sqrt(ub * ub + vb * vb);
-                double Ut, Vt;
-                if (d.fic_point == 0) { Ut = 0.0; Vt = 0.0; }
+                const real friction = de * a_Cd * sqrt(ub * ub + vb * vb);
+                real Ut, Vt;
+                if (d.fic_point == 0) { Ut = real(0.0); Vt = real(0.0); }
                 else if (d.fic_point == 1) {
-                    const double a = friction + 1.0 - xx1[L];
+                    const real a = friction + real(1.0) - xx1[L];
                     Ut = yu[L] / a; Vt = yv[L] / a;
                 } else {
-                    const double a = 1.0 / (1.0 - friction) - xx1[L];
+                    const real a = real(1.0) / (real(1.0) - friction) - xx1[L];
                     Ut = yu[L] / a; Vt = yv[L] / a;
                 }
                 for (int z = L - 1; z >= 0; --z) {
@@ -458,7 +460,7 @@ __global__ void k_implvisc(Dev d) {
                     vr[z] = Vt * mwd;
                 }
             } else {
-                for (int z = 0; z < L; ++z) { ur[z] = 0.0; vr[z] = 0.0; }
+                for (int z = 0; z < L; ++z) { ur[z] = real(0.0); vr[z] = real(0.0); }
             }
         }
     }
@@ -479,8 +481,8 @@ __global__ void k_je_elem(Dev d) {
     GRID_LOOP(ii, total) {
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
-        const double4 w = d.w_cv[e];
-        const double4 a = elem_jac_a(d, d.eta_jac, d.elem_nodes[e]);
+        const real4 w = d.w_cv[e];
+        const real4 a = elem_jac_a(d, d.eta_jac, d.elem_nodes[e]);
         d.Je[ii] = je_of(d, w, a, z);
         d.Ze[ii] = wsum_z(d, w, a, z);
         d.ZBe[ii] = wsum_zbar(d, w, a, z);
@@ -492,17 +494,18 @@ __global__ void k_je_elem(Dev d) {
 // per element.  Runs right after the jacobian call: the stored Je still holds
 // the previous jacobian (Jc_old), and is replaced here by the new Je / Ze /
 // ZBe.
-__global__ void k_update3d(Dev d, double Mt_inv) {
-    extern __shared__ double sm[];
+__global__ void k_update3d(Dev d, real Mt_inv) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L;
     const ColBlock cb(L);
     const int S = 2 * L + 1;
-    double *sc = sm + (size_t)cb.B * S;  // 4 scalars per element
+    real *sc = sm + (size_t)cb.B * S;  // 4 scalars per element
     for (long long eb = (long long)blockIdx.x * cb.B; eb < d.E; eb += (long long)gridDim.x * cb.B) {
         const long long e_ = eb + cb.jl;
         const bool act = cb.jl < cb.B && e_ < d.E;
         const size_t i = (size_t)e_ * L + cb.z;
-        double a_old = 0.0, ur = 0.0, vr = 0.0;
+        real a_old = real(0.0), ur = real(0.0), vr = real(0.0);
         if (act) {
             a_old = d.Je[i];
             ur = d.U_rhs[i];
@@ -514,21 +517,21 @@ __global__ void k_update3d(Dev d, double Mt_inv) {
         const long long es = eb + threadIdx.x;
         if ((int)threadIdx.x < cb.B && es < d.E) {
             const int e = (int)es;
-            const double *row = sm + threadIdx.x * S;
-            double su = 0.0, sv = 0.0;
+            const real *row = sm + threadIdx.x * S;
+            real su = real(0.0), sv = real(0.0);
             for (int k = 0; k < L; ++k) {
                 su = su + row[k];
                 sv = sv + row[L + k];
             }
             const int4 en = d.elem_nodes[e];
-            const double4 w = d.w_cv[e];
-            const double dmean_inv = 1.0 / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
+            const real4 w = d.w_cv[e];
+            const real dmean_inv = real(1.0) / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
                                                             d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
-            const double uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
-            const double vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
+            const real uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
+            const real vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
             d.U_filt_2D[e] = uf;
             d.V_filt_2D[e] = vf;
-            double *o = sc + 4 * threadIdx.x;
+            real *o = sc + 4 * threadIdx.x;
             o[0] = su * dmean_inv;
             o[1] = sv * dmean_inv;
             o[2] = uf;
@@ -537,14 +540,15 @@ __global__ void k_update3d(Dev d, double Mt_inv) {
         __syncthreads();
         if (act) {
             const int e = (int)e_, z = cb.z;
-            const double *o = sc + 4 * cb.jl;
-            const double U2p = o[0], V2p = o[1], uf = o[2], vf = o[3];
+            const real *o = sc + 4 * cb.jl;
+            const real U2p = o[0], V2p = o[1], uf = o[2], vf = o[3];
             const int4 en = d.elem_nodes[e];
-            const double4 w = d.w_cv[e];
-            const double4 an = elem_jac_a(d, d.eta_jac, en);
-            const double2 u2 = d.U_n_2D[e];
-            const double jn = je_of(d, w, an, z);
-            const double az = a_old / jn;
+            const real4 w = d.w_cv[e];
+            const real4 an = elem_jac_a(d, d.eta_jac, en);
+            const double2 u2d = d.U_n_2D[e];
+            const real2 u2 = make_real2((real)u2d.x, (real)u2d.y);
+            const real jn = je_of(d, w, an, z);
+            const real az = a_old / jn;
             d.U_n_filt[i] = az * ur + uf - U2p;
             d.V_n_filt[i] = az * vr + vf - V2p;
             d.U_n[i] = az * ur + u2.x - U2p;
@@ -561,7 +565,8 @@ __global__ void k_update3d(Dev d, double Mt_inv) {
 // transport divergence of (node, level) gathered over the node's edges in
 // edge order, then summed upward from the bottom per node.
 __global__ void k_wvel(Dev d) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L, NS = d.NS;
     const ColBlock cb(L);
     const int S = L | 1;
@@ -571,18 +576,18 @@ __global__ void k_wvel(Dev d) {
         if (act) {
             const int n = (int)n_, z = cb.z;
             const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
-            double W = 0.0;
+            real W = real(0.0);
 #pragma unroll 4
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
                 const int2 et = d.edge_tri[ed];
-                const double4 X = d.edge_cross[ed];
-                const double uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
+                const real4 X = d.edge_cross[ed];
+                const real uf1 = d.U_filt_2D[et.x], vf1 = d.V_filt_2D[et.x];
                 const size_t i1 = (size_t)et.x * L + z;
-                double c1 = d.Je[i1] * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
+                real c1 = d.Je[i1] * ((d.V_n_filt[i1] - vf1) * X.x - (d.U_n_filt[i1] - uf1) * X.y);
                 if (ed < d.Ed_in) {
-                    const double uf2 = d.U_filt_2D[et.y], vf2 = d.V_filt_2D[et.y];
+                    const real uf2 = d.U_filt_2D[et.y], vf2 = d.V_filt_2D[et.y];
                     const size_t i2 = (size_t)et.y * L + z;
                     c1 = c1 + d.Je[i2] * (-(d.V_n_filt[i2] - vf2) * X.z + (d.U_n_filt[i2] - uf2) * X.w);
                 }
@@ -594,15 +599,15 @@ __global__ void k_wvel(Dev d) {
         __syncthreads();
         const long long ns = nb + threadIdx.x;
         if ((int)threadIdx.x < cb.B && ns < d.N) {
-            double *row = sm + threadIdx.x * S;
-            double below = d.Wvel[(size_t)ns * NS + NS - 1];
+            real *row = sm + threadIdx.x * S;
+            real below = d.Wvel[(size_t)ns * NS + NS - 1];
             for (int k = L - 1; k >= 0; --k) {
                 below = row[k] + below;
                 row[k] = below;
             }
         }
         __syncthreads();
-        if (act) d.Wvel[(size_t)n_ * NS + cb.z] = sm[cb.jl * S + cb.z] * (1.0 / d.area[n_]);
+        if (act) d.Wvel[(size_t)n_ * NS + cb.z] = sm[cb.jl * S + cb.z] * (real(1.0) / d.area[n_]);
         __syncthreads();
     }
 }
@@ -616,7 +621,7 @@ static int col_grid(const Dev &d, long long count) {
 }
 static size_t col_smem(const Dev &d, int rows, int scalars) {
     const int S = rows == 1 ? (d.L | 1) : rows * d.L + 1;
-    return ((size_t)col_b(d) * S + (size_t)col_b(d) * scalars) * sizeof(double);
+    return ((size_t)col_b(d) * S + (size_t)col_b(d) * scalars) * sizeof(real);
 }
 int config_columns(const Dev &d) {
     const size_t big = col_smem(d, 2, 4);
@@ -638,7 +643,7 @@ void launch_velgrad3d(const Dev &d, cudaStream_t s) {
 void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
 }
-void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
+void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
     k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
 }
 #define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
@@ -650,9 +655,9 @@ void launch_velrhs(const Dev &d, double ff, cudaStream_t s) {
 void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d); }
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
-void launch_update3d(const Dev &d, double Mt_inv, cudaStream_t s) {
+void launch_update3d(const Dev &d, real Mt_inv, cudaStream_t s) {
     k_update3d<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, 4), s>>>(d, Mt_inv);
 }
 void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 0), s>>>(d); }
 
-}  // namespace fesomc
+FESOMC_PREC_END

@@ -13,14 +13,15 @@
 // All kernels are HBM-bandwidth bound.
 #include "device_common.cuh"
 
-namespace fesomc {
+FESOMC_PREC_BEGIN
 
+#if !FESOMC_FP32  // the 2D sub-cycle kernels exist in FP64 only
 // AB3 coefficients, timestep_AB_2D fv_main.F90:1403,1408
-__device__ __forceinline__ double ab3(double b, double x0, double x1, double x2) {
-    return (1.5 + b) * x0 - (0.5 + 2.0 * b) * x1 + b * x2;
+__device__ __forceinline__ real ab3(real b, real x0, real x1, real x2) {
+    return (real(1.5) + b) * x0 - (real(0.5) + real(2.0) * b) * x1 + b * x2;
 }
-__device__ __forceinline__ double2 ab3v(double b, double2 x0, double2 x1, double2 x2) {
-    return make_double2(ab3(b, x0.x, x1.x, x2.x), ab3(b, x0.y, x1.y, x2.y));
+__device__ __forceinline__ real2 ab3v(real b, real2 x0, real2 x1, real2 x2) {
+    return make_real2(ab3(b, x0.x, x1.x, x2.x), ab3(b, x0.y, x1.y, x2.y));
 }
 
 // ---------------------------------------------------------------------------
@@ -30,62 +31,62 @@ __device__ __forceinline__ double2 ab3v(double b, double2 x0, double2 x1, double
 __global__ void k_ab3_elem(Dev d) {
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
-        const double b = d.beta;
-        const double2 uab = ab3v(b, d.U_n_2D[e], d.U_n_1[e], d.U_n_2[e]);
+        const real b = d.beta;
+        const real2 uab = ab3v(b, d.U_n_2D[e], d.U_n_1[e], d.U_n_2[e]);
         d.UAB[e] = uab;
         const int4 en = d.elem_nodes[e];
         const int nd[4] = {en.x, en.y, en.z, en.w};
-        double ad[4];
+        real ad[4];
         for (int i = 0; i < 4; ++i) {
             const int n = nd[i];
-            double etaab = ab3(b, d.eta_n[n], d.eta_n_1[n], d.eta_n_2[n]);
+            real etaab = ab3(b, d.eta_n[n], d.eta_n_1[n], d.eta_n_2[n]);
             ad[i] = d.Dmin;
-            double ttl = etaab + d.depth[n];
+            real ttl = etaab + d.depth[n];
             if (ttl > d.Dmin) ad[i] = ttl;
         }
-        const double4 w = d.w_cv[e];
+        const real4 w = d.w_cv[e];
         d.aux_elem[e] = wexp(w, ad[0], ad[1], ad[2], ad[3]);
         // velocity gradients of UAB
         const int4 nb = d.elem_nb[e];
         const int4 ee = d.elem_edges[e];
         const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
         const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
-        const double4 gx = d.gv_x[e], gy = d.gv_y[e];
-        const double gxa[4] = {gx.x, gx.y, gx.z, gx.w};
-        const double gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const real4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
         const int jend = (en.x == en.w) ? 3 : 4;
-        double g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0;
+        real g1 = real(0.0), g2 = real(0.0), g3 = real(0.0), g4 = real(0.0);
         for (int j = 0; j < jend; ++j) {
             const int e2 = nbs[j];
             if (e2 >= 0) {
-                const double2 u2 = ab3v(b, d.U_n_2D[e2], d.U_n_1[e2], d.U_n_2[e2]);
+                const real2 u2 = ab3v(b, d.U_n_2D[e2], d.U_n_1[e2], d.U_n_2[e2]);
                 g1 = g1 + gxa[j] * (u2.x - uab.x);
                 g2 = g2 + gya[j] * (u2.x - uab.x);
                 g3 = g3 + gxa[j] * (u2.y - uab.y);
                 g4 = g4 + gya[j] * (u2.y - uab.y);
             } else {
-                const double2 dxy = d.edge_dxdy[eds[j]];
-                const double zc1 = dxy.x * d.elem_cos[e];
-                const double zc2 = dxy.y;
-                const double un = -2.0 * (uab.x * zc2 - uab.y * zc1) / (zc1 * zc1 + zc2 * zc2);
+                const real2 dxy = d.edge_dxdy[eds[j]];
+                const real zc1 = dxy.x * d.elem_cos[e];
+                const real zc2 = dxy.y;
+                const real un = -real(2.0) * (uab.x * zc2 - uab.y * zc1) / (zc1 * zc1 + zc2 * zc2);
                 g1 = g1 + gxa[j] * un * zc2;
                 g2 = g2 + gya[j] * un * zc2;
                 g3 = g3 - gxa[j] * un * zc1;
                 g4 = g4 - gya[j] * un * zc1;
             }
         }
-        d.vel_grad[e] = make_double4(g1, g2, g3, g4);
+        d.vel_grad[e] = make_real4(g1, g2, g3, g4);
     }
 }
 
 // edge flux c1 of compute_ssh_rhs_elem (fv_average_dynamic.F90:119-120, 152-153)
-__device__ __forceinline__ double ssh_edge_flux(const Dev &d, int ed) {
+__device__ __forceinline__ real ssh_edge_flux(const Dev &d, int ed) {
     const int2 et = d.edge_tri[ed];
-    const double4 X = d.edge_cross[ed];
-    const double2 u1 = d.UAB[et.x];
-    double c1 = (u1.y * X.x - u1.x * X.y) * d.aux_elem[et.x];
+    const real4 X = d.edge_cross[ed];
+    const real2 u1 = d.UAB[et.x];
+    real c1 = (u1.y * X.x - u1.x * X.y) * d.aux_elem[et.x];
     if (ed < d.Ed_in) {
-        const double2 u2 = d.UAB[et.y];
+        const real2 u2 = d.UAB[et.y];
         c1 = c1 + (-u2.y * X.z + u2.x * X.w) * d.aux_elem[et.y];
     }
     return c1;
@@ -100,15 +101,15 @@ __device__ __forceinline__ double ssh_edge_flux(const Dev &d, int ed) {
 // host with the reference formula (fv_average_dynamic.F90:190-216).
 // ---------------------------------------------------------------------------
 __global__ void k_ssh_node(Dev d, int sub) {
-    const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
+    const real de = real(0.614), ga = real(0.088), ep = real(0.013), fe = real(1.0) - de - ga - ep;
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
-        double acc = 0.0;
+        real acc = real(0.0);
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
 #pragma unroll 4
         for (int p = p0; p < p1; ++p) {
             const int code = d.node_eidx[p];
-            const double c1 = ssh_edge_flux(d, code >> 1);
+            const real c1 = ssh_edge_flux(d, code >> 1);
             if (code & 1) acc = acc - c1;
             else acc = acc + c1;
         }
@@ -117,16 +118,17 @@ __global__ void k_ssh_node(Dev d, int sub) {
         }
         const int q = d.obn_of_node[n];
         if (d.TF_presence && q >= 0) acc = d.ob_val[(size_t)sub * d.nobn + q];
-        const double en = d.eta_n[n];
-        double enew = acc;
+        const real en = d.eta_n[n];
+        real enew = acc;
         if (d.index_nod2D[n] < 2) enew = en + d.dt_2D * acc / d.area[n];
         d.eta_new[n] = enew;
-        const double eab = de * enew + fe * en + ga * d.eta_n_1[n] + ep * d.eta_n_2[n];
+        const real eab = de * enew + fe * en + ga * d.eta_n_1[n] + ep * d.eta_n_2[n];
         d.etaAB[n] = eab;
-        if (d.wet_dry_on) d.mask_wd_node[n] = (d.depth[n] + eab > d.Dmin) ? 1.0 : 0.0;
+        if (d.wet_dry_on) d.mask_wd_node[n] = (d.depth[n] + eab > d.Dmin) ? real(1.0) : real(0.0);
     }
 }
 
+#endif
 // ---------------------------------------------------------------------------
 // sub-step 1 (fv_main.F90:1451-1520): dmean_n, compute_puls_vel
 // (fv_3D_vel.F90:257-307), one thread per (element, level).
@@ -136,12 +138,13 @@ __global__ void k_puls_elem(Dev d) {
     GRID_LOOP(ii, total) {
         const int e = (int)(ii / d.L);
         const int4 en = d.elem_nodes[e];
-        const double4 w = d.w_cv[e];
-        const double dmn = dmax(d.Dmin, wexp(w, d.eta_n[en.x] + d.depth[en.x], d.eta_n[en.y] + d.depth[en.y],
+        const real4 w = d.w_cv[e];
+        const real dmn = dmax(d.Dmin, wexp(w, d.eta_n[en.x] + d.depth[en.x], d.eta_n[en.y] + d.depth[en.y],
                                               d.eta_n[en.z] + d.depth[en.z], d.eta_n[en.w] + d.depth[en.w]));
-        const double a = dmn / dmax(d.Dmin, wsum(w, d.eta_new[en.x] + d.depth[en.x], d.eta_new[en.y] + d.depth[en.y],
+        const real a = dmn / dmax(d.Dmin, wsum(w, d.eta_new[en.x] + d.depth[en.x], d.eta_new[en.y] + d.depth[en.y],
                                                  d.eta_new[en.z] + d.depth[en.z], d.eta_new[en.w] + d.depth[en.w]));
-        const double2 u2 = d.U_n_2D[e];
+        const double2 u2d = d.U_n_2D[e];
+        const real2 u2 = make_real2((real)u2d.x, (real)u2d.y);
         d.U_puls[ii] = d.U_n[ii] - a * u2.x;
         d.V_puls[ii] = d.V_n[ii] - a * u2.y;
         if (ii % d.L == 0) d.dmean_n[e] = dmn;
@@ -149,16 +152,16 @@ __global__ void k_puls_elem(Dev d) {
 }
 
 // compute_el2nodes_3D (fv_utilit.F90:644-700), one thread per (node, level)
-__global__ void k_el2nodes(Dev d, const double *Ue, const double *Ve, double *Un, double *Vn) {
+__global__ void k_el2nodes(Dev d, const real *Ue, const real *Ve, real *Un, real *Vn) {
     const long long total = (long long)d.N * d.L;
     GRID_LOOP(ii, total) {
         const int n = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
-        const double tvol_inv = 1.0 / d.node_tvol[n];
-        double su = 0.0, sv = 0.0;
+        const real tvol_inv = real(1.0) / d.node_tvol[n];
+        real su = real(0.0), sv = real(0.0);
         for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
             const int el = d.node_nidx[p];
-            const double ar = d.elem_area[el];
+            const real ar = d.elem_area[el];
             su = su + Ue[(size_t)el * d.L + z] * ar;
             sv = sv + Ve[(size_t)el * d.L + z] * ar;
         }
@@ -178,15 +181,15 @@ __global__ void k_p1_edge(Dev d) {
         const int z = (int)(ii % L);
         const int2 nn = d.edge_nodes[ed];
         const int2 et = d.edge_tri[ed];
-        const double2 dxy = d.edge_dxdy[ed];
-        const double xe = dxy.x * kREarth * 0.5 * (d.elem_cos[et.x] + d.elem_cos[et.y]);
-        const double ye = dxy.y * kREarth;
-        const double a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
-        const double uu = 0.5 * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
-        const double vv = 0.5 * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
-        const double jd = 0.5 * (jc_of(d, a1, z) + jc_of(d, a2, z));
-        const double un = (uu * ye - vv * xe) * jd;
-        d.adv3[ii] = make_double2(uu * un, vv * un);
+        const real2 dxy = d.edge_dxdy[ed];
+        const real xe = dxy.x * kREarth * real(0.5) * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+        const real ye = dxy.y * kREarth;
+        const real a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
+        const real uu = real(0.5) * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
+        const real vv = real(0.5) * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
+        const real jd = real(0.5) * (jc_of(d, a1, z) + jc_of(d, a2, z));
+        const real un = (uu * ye - vv * xe) * jd;
+        d.adv3[ii] = make_real2(uu * un, vv * un);
     }
 }
 
@@ -201,7 +204,8 @@ __global__ void k_p1_edge(Dev d) {
 // the slot contributions in slot order, then the filter terms.
 constexpr int kP1Slots = 5;  // 4 internal-edge slots + the filter
 __global__ void k_p1_elem(Dev d) {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L;
     const int B = (int)blockDim.x / L;
     const int S = 2 * kP1Slots * L + 1;  // per-element stride, odd: conflict-free
@@ -210,14 +214,14 @@ __global__ void k_p1_elem(Dev d) {
         const long long e_ = eb + jl;
         if (jl < B && e_ < d.E) {
             const int e = (int)e_;
-            double *T = sm + (size_t)jl * S;  // T[(slot*2 + uv)*L + z]
-            const double je = d.Je[(size_t)e * L + z];
+            real *T = sm + (size_t)jl * S;  // T[(slot*2 + uv)*L + z]
+            const real je = d.Je[(size_t)e * L + z];
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 if (codes[c] >= 0) {
-                    const double2 pq = d.adv3[(size_t)(codes[c] >> 1) * L + z];
+                    const real2 pq = d.adv3[(size_t)(codes[c] >> 1) * L + z];
                     T[(c * 2 + 0) * L + z] = pq.x * je;
                     T[(c * 2 + 1) * L + z] = pq.y * je;
                 }
@@ -227,18 +231,18 @@ __global__ void k_p1_elem(Dev d) {
                 const int4 nb4 = d.elem_nb[e];
                 const int nbs[4] = {nb4.x, nb4.y, nb4.z, nb4.w};
                 const int jend = (en.x == en.w) ? 3 : 4;
-                const double tau = d.tau_inv_filt, ar = d.elem_area[e];
-                const double up = d.U_puls[(size_t)e * L + z], vp = d.V_puls[(size_t)e * L + z];
-                double u1 = 0.0, v1 = 0.0;
+                const real tau = d.tau_inv_filt, ar = d.elem_area[e];
+                const real up = d.U_puls[(size_t)e * L + z], vp = d.V_puls[(size_t)e * L + z];
+                real u1 = real(0.0), v1 = real(0.0);
                 for (int k = 0; k < jend; ++k) {
                     const int ne = nbs[k];
                     if (ne < 0) continue;
                     const size_t i = (size_t)ne * L + z;
-                    const double jn = d.Je[i];
+                    const real jn = d.Je[i];
                     u1 = u1 + d.U_puls[i] * jn - up * je;
                     v1 = v1 + d.V_puls[i] * jn - vp * je;
                 }
-                const double fu = tau * u1 * ar, fv = tau * v1 * ar;
+                const real fu = tau * u1 * ar, fv = tau * v1 * ar;
                 T[(4 * 2 + 0) * L + z] = fu * je;
                 T[(4 * 2 + 1) * L + z] = fv * je;
             }
@@ -247,10 +251,10 @@ __global__ void k_p1_elem(Dev d) {
         const long long es = eb + threadIdx.x;
         if ((int)threadIdx.x < B && es < d.E) {
             const int e = (int)es;
-            const double *T = sm + (size_t)threadIdx.x * S;
+            const real *T = sm + (size_t)threadIdx.x * S;
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
-            double su[4] = {0.0, 0.0, 0.0, 0.0}, sv[4] = {0.0, 0.0, 0.0, 0.0};
+            real su[4] = {real(0.0), real(0.0), real(0.0), real(0.0)}, sv[4] = {real(0.0), real(0.0), real(0.0), real(0.0)};
             for (int k = 0; k < L; ++k) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
@@ -258,13 +262,13 @@ __global__ void k_p1_elem(Dev d) {
                     sv[c] = sv[c] + T[(c * 2 + 1) * L + k];
                 }
             }
-            double rx = 0.0, ry = 0.0;
+            real rx = real(0.0), ry = real(0.0);
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 const int code = codes[c];
                 if (code < 0) break;
                 const int2 nn = d.edge_nodes[code >> 1];
-                const double acc = (d.ac[nn.x] + d.ac[nn.y]) * .5;
+                const real acc = (d.ac[nn.x] + d.ac[nn.y]) * real(.5);
                 if (code & 1) { rx = rx + acc * su[c]; ry = ry + acc * sv[c]; }
                 else { rx = rx - acc * su[c]; ry = ry - acc * sv[c]; }
             }
@@ -273,39 +277,40 @@ __global__ void k_p1_elem(Dev d) {
                     rx = rx + T[(4 * 2 + 0) * L + k];
                     ry = ry + T[(4 * 2 + 1) * L + k];
                 }
-            const double dm = d.dmean_n[e];
+            const real dm = d.dmean_n[e];
             d.U_rhs_2D_3D[e] = make_double2(rx / dm, ry / dm);
         }
         __syncthreads();
     }
 }
 
+#if !FESOMC_FP32
 // One upwind edge flux of momentum_adv_upwind_2D (fv_advection.F90:589-643)
-__device__ __forceinline__ void adv2d_edge(const Dev &d, int ed, double &uu, double &vv) {
+__device__ __forceinline__ void adv2d_edge(const Dev &d, int ed, real &uu, real &vv) {
     const int2 nn = d.edge_nodes[ed];
     const int2 et = d.edge_tri[ed];
-    const double dmean = dmax(d.Dmin, 0.5 * ((d.etaAB[nn.x] + d.depth[nn.x]) + (d.etaAB[nn.y] + d.depth[nn.y])));
-    const double acc = (d.ac[nn.x] + d.ac[nn.y]) * 0.5;
-    const double4 X = d.edge_cross[ed];
-    const double2 U1 = d.UAB[et.x], U2 = d.UAB[et.y];
-    const double4 g1 = d.vel_grad[et.x], g2 = d.vel_grad[et.y];
-    const double u1 = U1.x - g1.x * X.x - g1.y * X.y;
-    const double v1 = U1.y - g1.z * X.x - g1.w * X.y;
-    const double u2 = U2.x - g2.x * X.z - g2.y * X.w;
-    const double v2 = U2.y - g2.z * X.z - g2.w * X.w;
-    const double2 dxy = d.edge_dxdy[ed];
-    const double un = 0.5 * kREarth * dmean *
+    const real dmean = dmax(d.Dmin, real(0.5) * ((d.etaAB[nn.x] + d.depth[nn.x]) + (d.etaAB[nn.y] + d.depth[nn.y])));
+    const real acc = (d.ac[nn.x] + d.ac[nn.y]) * real(0.5);
+    const real4 X = d.edge_cross[ed];
+    const real2 U1 = d.UAB[et.x], U2 = d.UAB[et.y];
+    const real4 g1 = d.vel_grad[et.x], g2 = d.vel_grad[et.y];
+    const real u1 = U1.x - g1.x * X.x - g1.y * X.y;
+    const real v1 = U1.y - g1.z * X.x - g1.w * X.y;
+    const real u2 = U2.x - g2.x * X.z - g2.y * X.w;
+    const real v2 = U2.y - g2.z * X.z - g2.w * X.w;
+    const real2 dxy = d.edge_dxdy[ed];
+    const real un = real(0.5) * kREarth * dmean *
                       ((u1 + u2) * dxy.y - (v1 * d.elem_cos[et.x] + v2 * d.elem_cos[et.y]) * dxy.x);
-    if (un >= 0.0) { uu = un * U1.x * acc; vv = un * U1.y * acc; }
+    if (un >= real(0.0)) { uu = un * U1.x * acc; vv = un * U1.y * acc; }
     else { uu = un * U2.x * acc; vv = un * U2.y * acc; }
 }
 
 // momentum_adv_upwind_2D edge fluxes of the sub-step, once per internal edge
 __global__ void k_adv2d_edge(Dev d) {
     GRID_LOOP(ed, d.Ed_in) {
-        double uu, vv;
+        real uu, vv;
         adv2d_edge(d, (int)ed, uu, vv);
-        d.adv2d[ed] = make_double2(uu, vv);
+        d.adv2d[ed] = make_real2(uu, vv);
     }
 }
 
@@ -315,33 +320,33 @@ __global__ void k_adv2d_edge(Dev d) {
 // (fv_main.F90:1568-1606).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
-    const double d0inv = 1.0 / d.density_0;
+    const real d0inv = real(1.0) / d.density_0;
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
         const int4 en = d.elem_nodes[e];
         const int nd[4] = {en.x, en.y, en.z, en.w};
-        double eab[4], dep[4], etag[4];
+        real eab[4], dep[4], etag[4];
         for (int k = 0; k < 4; ++k) {
             eab[k] = d.etaAB[nd[k]];
             dep[k] = d.depth[nd[k]];
             etag[k] = kG * (d.atp1[nd[k]] * eab[k] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
         }
-        double mwd = d.mask_wd[e];
+        real mwd = d.mask_wd[e];
         if (d.wet_dry_on) {
-            const double dmin4 = dmin(dmin(dep[0], dep[1]), dmin(dep[2], dep[3]));
-            const double emax4 = dmax(dmax(eab[0], eab[1]), dmax(eab[2], eab[3]));
-            mwd = (dmin4 + emax4 > d.Dmin) ? 1.0 : 0.0;
+            const real dmin4 = dmin(dmin(dep[0], dep[1]), dmin(dep[2], dep[3]));
+            const real emax4 = dmax(dmax(eab[0], eab[1]), dmax(eab[2], eab[3]));
+            mwd = (dmin4 + emax4 > d.Dmin) ? real(1.0) : real(0.0);
             d.mask_wd[e] = mwd;
         }
-        const double4 w = d.w_cv[e];
-        const double ar = d.elem_area[e];
-        const double dmean = dmax(d.Dmin, wexp(w, eab[0] + dep[0], eab[1] + dep[1], eab[2] + dep[2], eab[3] + dep[3]));
-        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
-        const double2 uab = d.UAB[e];
-        const double cor = d.coriolis[e];
-        double rx = ar * (-dmean * (gx.x * etag[0] + gx.y * etag[1] + gx.z * etag[2] + gx.w * etag[3])
+        const real4 w = d.w_cv[e];
+        const real ar = d.elem_area[e];
+        const real dmean = dmax(d.Dmin, wexp(w, eab[0] + dep[0], eab[1] + dep[1], eab[2] + dep[2], eab[3] + dep[3]));
+        const real4 gx = d.gs_x[e], gy = d.gs_y[e];
+        const real2 uab = d.UAB[e];
+        const real cor = d.coriolis[e];
+        real rx = ar * (-dmean * (gx.x * etag[0] + gx.y * etag[1] + gx.z * etag[2] + gx.w * etag[3])
                           + uab.y * dmean * cor + d.taux[e] * d0inv);
-        double ry = ar * (-dmean * (gy.x * etag[0] + gy.y * etag[1] + gy.z * etag[2] + gy.w * etag[3])
+        real ry = ar * (-dmean * (gy.x * etag[0] + gy.y * etag[1] + gy.z * etag[2] + gy.w * etag[3])
                           - uab.x * dmean * cor + d.tauy[e] * d0inv);
         if (d.mom_adv_2D == 2) {
             const int4 il = d.elem_iedges[e];
@@ -350,7 +355,7 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
             for (int c = 0; c < 4; ++c) {
                 const int code = codes[c];
                 if (code < 0) break;
-                const double2 f = d.adv2d[code >> 1];
+                const real2 f = d.adv2d[code >> 1];
                 if (code & 1) { rx = rx + f.x; ry = ry + f.y; }
                 else { rx = rx - f.x; ry = ry - f.y; }
             }
@@ -359,39 +364,39 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
             const int4 nb = d.elem_nb[e];
             const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
             const int jend = (en.x == en.w) ? 3 : 4;
-            double u1 = 0.0, u2 = 0.0;
+            real u1 = real(0.0), u2 = real(0.0);
             for (int j = 0; j < jend; ++j)
                 if (nbs[j] >= 0) {
-                    const double2 un = d.UAB[nbs[j]];
+                    const real2 un = d.UAB[nbs[j]];
                     u1 = u1 + un.x - uab.x;
                     u2 = u2 + un.y - uab.y;
                 }
-            const double sd = wsum(w, dep[0], dep[1], dep[2], dep[3]);
+            const real sd = wsum(w, dep[0], dep[1], dep[2], dep[3]);
             rx = rx + d.tau_inv_filt * u1 * ar * sd;
             ry = ry + d.tau_inv_filt * u2 * ar * sd;
         }
-        const double2 r3 = d.U_rhs_2D_3D[e];
+        const real2 r3 = d.U_rhs_2D_3D[e];
         rx = rx + r3.x;
         ry = ry + r3.y;
         // final update with implicit bottom drag
-        double eo[4], enw[4];
+        real eo[4], enw[4];
         for (int k = 0; k < 4; ++k) { eo[k] = d.eta_n[nd[k]]; enw[k] = d.eta_new[nd[k]]; }
-        const double dmo = dmax(d.Dmin, wsum(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
-        const double4 bf = d.bfric[e];
-        const double ub = bf.x, vb = bf.y, friction = bf.z;
-        const double ff = 1.0 / (dmax(d.Dmin, wsum(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
+        const real dmo = dmax(d.Dmin, wsum(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
+        const real4 bf = d.bfric[e];
+        const real ub = bf.x, vb = bf.y, friction = bf.z;
+        const real ff = real(1.0) / (dmax(d.Dmin, wsum(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
                                  + friction * d.dt_2D);
-        const double dt2 = d.dt_2D;
-        const double2 u0 = d.U_n_2D[e];
-        const double2 bp = d.Bar_pr_2D[e];
-        const double nx = mwd * ((dmo * u0.x - dt2 * friction * (ub - u0.x) + dt2 * bp.x + dt2 * rx / ar) * ff + 0.0);
-        const double ny = mwd * ((dmo * u0.y - dt2 * friction * (vb - u0.y) + dt2 * bp.y + dt2 * ry / ar) * ff + 0.0);
+        const real dt2 = d.dt_2D;
+        const real2 u0 = d.U_n_2D[e];
+        const real2 bp = d.Bar_pr_2D[e];
+        const real nx = mwd * ((dmo * u0.x - dt2 * friction * (ub - u0.x) + dt2 * bp.x + dt2 * rx / ar) * ff + real(0.0));
+        const real ny = mwd * ((dmo * u0.y - dt2 * friction * (vb - u0.y) + dt2 * bp.y + dt2 * ry / ar) * ff + real(0.0));
         // rotate U_n_2 <- U_n_1 <- U_n_2D <- new (fv_main.F90:1569-1578)
         d.U_n_2[e] = d.U_n_1[e];
         d.U_n_1[e] = u0;
-        d.U_n_2D[e] = make_double2(nx, ny);
+        d.U_n_2D[e] = make_real2(nx, ny);
         // U_filt accumulation with the new elevation (fv_main.F90:1596-1605)
-        const double dmn = dmax(d.Dmin, wexp(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]));
+        const real dmn = dmax(d.Dmin, wexp(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]));
         d.U_filt_2D[e] = d.U_filt_2D[e] + nx * dmn;
         d.V_filt_2D[e] = d.V_filt_2D[e] + ny * dmn;
     }
@@ -401,39 +406,42 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
 __global__ void k_rot_nodes(Dev d) {
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
-        const double e0 = d.eta_n[n], e1 = d.eta_n_1[n];
+        const real e0 = d.eta_n[n], e1 = d.eta_n_1[n];
         d.eta_n_2[n] = e1;
         d.eta_n_1[n] = e0;
         d.eta_n[n] = d.eta_new[n];
     }
 }
 
+#endif
 // U_filt_2D = V_filt_2D = 0 at the start of the sub-cycle, and the bottom
 // velocity and quadratic drag a_Cd*|U_b| that update_2D_vel uses in every
 // sub-step (fv_average_dynamic.F90:262, 400-420; U_n is fixed during the
 // sub-cycle)
 __global__ void k_zero_filt(Dev d) {
     GRID_LOOP(ii, d.E) {
-        d.U_filt_2D[ii] = 0.0;
-        d.V_filt_2D[ii] = 0.0;
-        const double a_Cd = d.C_d * ((1.0 - d.elem_acc[ii]) * d.Cd_bz + 1.0);
-        const double ub = d.U_n[(size_t)ii * d.L + d.L - 1], vb = d.V_n[(size_t)ii * d.L + d.L - 1];
+        d.U_filt_2D[ii] = real(0.0);
+        d.V_filt_2D[ii] = real(0.0);
+        const real a_Cd = d.C_d * ((real(1.0) - d.elem_acc[ii]) * d.Cd_bz + real(1.0));
+        const real ub = d.U_n[(size_t)ii * d.L + d.L - 1], vb = d.V_n[(size_t)ii * d.L + d.L - 1];
         d.bfric[ii] = make_double4(ub, vb, a_Cd * sqrt(ub * ub + vb * vb), 0.0);
     }
 }
 
 // ---- launch wrappers --------------------------------------------------------
+#if !FESOMC_FP32
 void launch_ab3_elem(const Dev &d, cudaStream_t s) { k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) { k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub); }
+#endif
 void launch_puls_elem(const Dev &d, cudaStream_t s) {
     k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
-void launch_el2nodes(const Dev &d, const double *Ue, const double *Ve, double *Un, double *Vn, cudaStream_t s) {
+void launch_el2nodes(const Dev &d, const real *Ue, const real *Ve, real *Un, real *Vn, cudaStream_t s) {
     k_el2nodes<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d, Ue, Ve, Un, Vn);
 }
 // B elements per block: B*L threads, at most 1024 and at most 32 elements
 static int p1_elems(const Dev &d) { int b = 1024 / d.L; return b > 32 ? 32 : b; }
-static size_t p1_smem(const Dev &d) { return (size_t)p1_elems(d) * (2 * kP1Slots * d.L + 1) * sizeof(double); }
+static size_t p1_smem(const Dev &d) { return (size_t)p1_elems(d) * (2 * kP1Slots * d.L + 1) * sizeof(real); }
 int config_p1(const Dev &d) {
     return cudaFuncSetAttribute(k_p1_elem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(d)) == cudaSuccess
                ? 0 : 1;
@@ -446,9 +454,11 @@ void launch_p1_elem(const Dev &d, cudaStream_t s) {
     const long long blocks = ((long long)d.E + B - 1) / B;
     k_p1_elem<<<(int)(blocks < 148LL * 16 ? blocks : 148LL * 16), B * d.L, p1_smem(d), s>>>(d);
 }
+#if !FESOMC_FP32
 void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
 void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
+#endif
 void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 
-}  // namespace fesomc
+FESOMC_PREC_END

@@ -28,6 +28,7 @@
 
 namespace fesomc {
 namespace {
+using namespace fesomc::f64;
 
 constexpr int kEsBlock = 256;
 constexpr int kEsParts = 592;                    // 4 blocks per SM on 148 SMs

@@ -5,7 +5,7 @@
 // Compute / latency bound (FP64 divisions, log, sqrt).
 #include "device_common.cuh"
 
-namespace fesomc {
+FESOMC_PREC_BEGIN
 
 // Convergence test of d3_end's sweep (fv_mixing.F90:250-259) for one level:
 // the reference forms c = |a/b| and stops when the largest c is below 1e-6
@@ -14,14 +14,14 @@ namespace fesomc {
 // when |a| lies within a relative 2^-30 of 1e-6*|b|; outside that band the
 // comparison of |a| with the product decides it with certainty (the band is
 // far wider than the rounding of the product and of the quotient).
-__device__ __forceinline__ bool d3_above_tol(double a, double b) {
-    const double aa = fabs(a), bb = fabs(b);
-    if (bb > 1.0e-290 && bb < 1.0e290 && aa < 1.0e300) {
-        const double t = 1.0e-6 * bb;
-        if (aa <= t * (1.0 - 0x1p-30)) return false;
-        if (aa >= t * (1.0 + 0x1p-30)) return true;
+__device__ __forceinline__ bool d3_above_tol(real a, real b) {
+    const real aa = fabs(a), bb = fabs(b);
+    if (bb > real(1.0e-290) && bb < real(1.0e290) && aa < real(1.0e300)) {
+        const real t = real(1.0e-6) * bb;
+        if (aa <= t * (real(1.0) - 0x1p-30)) return false;
+        if (aa >= t * (real(1.0) + 0x1p-30)) return true;
     }
-    return fabs(a / b) >= 1.0e-6;
+    return fabs(a / b) >= real(1.0e-6);
 }
 
 // d3_end per node column (local-memory arrays indexed 1..NS like the Fortran
@@ -40,93 +40,93 @@ __device__ __forceinline__ bool d3_above_tol(double a, double b) {
 //   * the convergence test forms the quotient only near the threshold.
 template <int ARR>
 __global__ void k_d3end(Dev d) {
-    const double t_inv = 1.0 / d.dt;
-    const double cka = d.cka;
-    const double B1cka2 = 16.6 * (cka * cka);
+    const real t_inv = real(1.0) / d.dt;
+    const real cka = d.cka;
+    const real B1cka2 = real(16.6) * (cka * cka);
     GRID_LOOP(ii, d.N) {
         const int node = (int)ii;
         const int NS = d.NS, L = d.L;
-        const double *bt = d.bt + (size_t)node * NS;
-        const double *snu = d.snu + (size_t)node * NS;
-        const double *Kv = d.Kv + (size_t)node * NS;
-        const double *Un = d.Unode + (size_t)node * L;
-        const double *Vn = d.Vnode + (size_t)node * L;
-        const double *T = d.TF + (size_t)node * L;
-        const double *S = d.SF + (size_t)node * L;
-        double *Ri = d.Ri + (size_t)node * NS;
-        double *tke = d.tke_dissip + (size_t)node * NS;
-        double xx1[ARR], yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
-        const double dmean = dmax(d.Dmin, d.depth[node] + d.eta_n[node]);
-        const double dmean2 = dmean * dmean;
-        const double ajac = jac_a(d, d.eta_jac, node);
+        const real *bt = d.bt + (size_t)node * NS;
+        const real *snu = d.snu + (size_t)node * NS;
+        const real *Kv = d.Kv + (size_t)node * NS;
+        const real *Un = d.Unode + (size_t)node * L;
+        const real *Vn = d.Vnode + (size_t)node * L;
+        const real *T = d.TF + (size_t)node * L;
+        const real *S = d.SF + (size_t)node * L;
+        real *Ri = d.Ri + (size_t)node * NS;
+        real *tke = d.tke_dissip + (size_t)node * NS;
+        real xx1[ARR], yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const real dmean2 = dmean * dmean;
+        const real ajac = jac_a(d, d.eta_jac, node);
         for (int nz = 1; nz <= NS; ++nz) {
             bA[nz] = bt[nz - 1];
             sn[nz] = snu[nz - 1];
         }
-        Ri[0] = 0.0;
-        Ri[NS - 1] = 0.0;
+        Ri[0] = real(0.0);
+        Ri[NS - 1] = real(0.0);
         for (int nz = 2; nz <= NS - 1; ++nz) {
-            const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
-            const double d1 = s_m - s_0;
-            const double d2 = s_0 - s_p;
-            const double dd = 0.5 * (d1 + d2);
-            double ap1 = Un[nz - 2] - Un[nz - 1];
-            const double ap2 = Vn[nz - 2] - Vn[nz - 1];
-            double b1 = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+            const real d1 = s_m - s_0;
+            const real d2 = s_0 - s_p;
+            const real dd = real(0.5) * (d1 + d2);
+            real ap1 = Un[nz - 2] - Un[nz - 1];
+            const real ap2 = Vn[nz - 2] - Vn[nz - 1];
+            real b1 = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
             b1 = b1 / dmean2;
-            const double zb = zbar_of(d, ajac, nz - 1);
-            const double rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
-            const double rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
+            const real zb = zbar_of(d, ajac, nz - 1);
+            const real rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
+            const real rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
             ap1 = (rho_up - rho_dn) / dd;
-            const double b2 = -0.5 * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
-            const double snu_p = 0.5 * (sn[nz - 1] + sn[nz]);
-            const double snu_m = 0.5 * (sn[nz] + sn[nz + 1]);
-            const double cc = 0.5 * 0.73 * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
+            const real b2 = -real(0.5) * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const real snu_p = real(0.5) * (sn[nz - 1] + sn[nz]);
+            const real snu_m = real(0.5) * (sn[nz] + sn[nz + 1]);
+            const real cc = real(0.5) * real(0.73) * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
             c2[nz] = cc / dmean2;
-            if (b1 > 0.0) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn[nz];
-            else Ri[nz - 1] = 10000.0;
+            if (b1 > real(0.0)) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn[nz];
+            else Ri[nz - 1] = real(10000.0);
             pb[nz] = -b1 - b2;
             qb[nz] = t_inv * bt[nz - 1];
         }
-        double y2;
+        real y2;
         {
-            const double d1 = 0.5 * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
-            const double wx = d.windx[node], wy = d.windy[node];
-            const double u_din_sur = 0.05 * (wx * wx + wy * wy);
-            const double snu_m = 0.5 * (sn[NS] + sn[NS - 1]);
-            y2 = (0.4e-3 * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * 0.76);
+            const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const real wx = d.windx[node], wy = d.windy[node];
+            const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+            const real snu_m = real(0.5) * (sn[NS] + sn[NS - 1]);
+            y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
         }
-        xx1[2] = 1.0;
+        xx1[2] = real(1.0);
         yy1[2] = y2;
         // bottom boundary value (independent of the iteration)
-        const double delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
-        const double lg = log(delta_b / d.z0b_min);
-        const double bott_R = B1cka2 / (lg * lg);
-        const double ubt = Un[L - 1], vbt = Vn[L - 1];
-        const double bot = bott_R * (ubt * ubt + vbt * vbt);
-        double *btr = bA, *btr1 = bB;
+        const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const real lg = log(delta_b / d.z0b_min);
+        const real bott_R = B1cka2 / (lg * lg);
+        const real ubt = Un[L - 1], vbt = Vn[L - 1];
+        const real bot = bott_R * (ubt * ubt + vbt * vbt);
+        real *btr = bA, *btr1 = bB;
         bool converged = false;
         for (int it = 1; it <= 200; ++it) {
-            double x = 1.0, y = y2;
-            double s_lo = sn[1], s_mid = sn[2];
+            real x = real(1.0), y = y2;
+            real s_lo = sn[1], s_mid = sn[2];
             for (int nz = 2; nz <= NS - 1; ++nz) {
-                const double s_hi = sn[nz + 1];
-                const double s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
-                const double dd1 = s_m - s_0;
-                const double dd2 = s_0 - s_p;
-                const double dd = 0.5 * (dd1 + dd2);
-                const double b = btr[nz];
-                const double c1 = 0.046 * (b * b) / s_mid;
+                const real s_hi = sn[nz + 1];
+                const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const real dd1 = s_m - s_0;
+                const real dd2 = s_0 - s_p;
+                const real dd = real(0.5) * (dd1 + dd2);
+                const real b = btr[nz];
+                const real c1 = real(0.046) * (b * b) / s_mid;
                 if (it == 200) tke[nz - 1] = c1;
-                const double fr = pb[nz] - c1 - qb[nz] - c2[nz];
-                const double snu_p = 0.5 * (s_lo + s_mid);
-                const double snu_mm = 0.5 * (s_mid + s_hi);
-                const double am = 0.5 * (snu_p * 0.73) / (dmean2 * dd1 * dd);
-                const double cm = 0.5 * (snu_mm * 0.73) / (dmean2 * dd2 * dd);
-                const double bm = am + cm + (2.0 * 0.046 * b) / s_mid + t_inv;
-                const double a = bm - am * x;
-                const double xn = cm / a;
-                const double yn = (am * y - fr) / a;
+                const real fr = pb[nz] - c1 - qb[nz] - c2[nz];
+                const real snu_p = real(0.5) * (s_lo + s_mid);
+                const real snu_mm = real(0.5) * (s_mid + s_hi);
+                const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+                const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
+                const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
+                const real a = bm - am * x;
+                const real xn = cm / a;
+                const real yn = (am * y - fr) / a;
                 xx1[nz + 1] = xn;
                 yy1[nz + 1] = yn;
                 x = xn;
@@ -134,37 +134,37 @@ __global__ void k_d3end(Dev d) {
                 s_lo = s_mid;
                 s_mid = s_hi;
             }
-            double b1v = bot;  // btr1(NS)
+            real b1v = bot;  // btr1(NS)
             btr1[NS] = b1v;
-            bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + 1.0e-8);
+            bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + real(1.0e-8));
             for (int nz = NS; nz >= 2; --nz) {
                 b1v = b1v * xx1[nz] + yy1[nz];  // btr1(nz-1)
                 btr1[nz - 1] = b1v;
-                above |= d3_above_tol(btr[nz - 1] - b1v, dmax(b1v, btr[nz - 1]) + 1.0e-8);
+                above |= d3_above_tol(btr[nz - 1] - b1v, dmax(b1v, btr[nz - 1]) + real(1.0e-8));
             }
             if (!above) { converged = true; break; }
-            double *t = btr;
+            real *t = btr;
             btr = btr1;
             btr1 = t;
         }
         if (converged) {
-            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = 0.046 * (btr[nz] * btr[nz]) / sn[nz];
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (btr[nz] * btr[nz]) / sn[nz];
         } else {
             atomicAdd(d.notconv, 1);
         }
-        double *btw = d.bt + (size_t)node * NS;
-        double *snw = d.snu + (size_t)node * NS;
-        double *Kvw = d.Kv + (size_t)node * NS;
+        real *btw = d.bt + (size_t)node * NS;
+        real *snw = d.snu + (size_t)node * NS;
+        real *Kvw = d.Kv + (size_t)node * NS;
         for (int nz = 1; nz <= NS; ++nz) {
-            const double btn = dmax(btr[nz], 1.0e-8);
+            const real btn = dmax(btr[nz], real(1.0e-8));
             btw[nz - 1] = btn;
-            const double zt = __ldg(d.sig + nz - 1) * dmean;
-            const double Zh = zt + d.z0b_min;
-            const double Zd = fabs(dmean - zt) + d.z0s_min;
-            const double Z0 = 1.0 - d.beta_scale * Zh * Zd / (dmean * dmean);
-            const double scale_t = cka * Zh * Zd * Z0 / dmean;
-            double s = scale_t * sqrt(btn) + d.snul;
-            if (s >= 0.2) s = 0.2;
+            const real zt = __ldg(d.sig + nz - 1) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = cka * Zh * Zd * Z0 / dmean;
+            real s = scale_t * sqrt(btn) + d.snul;
+            if (s >= real(0.2)) s = real(0.2);
             snw[nz - 1] = s;
             Kvw[nz - 1] = d.Pr_num * s;
         }
@@ -178,7 +178,7 @@ __global__ void k_av(Dev d) {
         const int e = (int)(ii / d.NS);
         const int z = (int)(ii % d.NS);
         const int4 en = d.elem_nodes[e];
-        const double4 w = d.w_cv[e];
+        const real4 w = d.w_cv[e];
         const int NS = d.NS;
         d.Av[ii] = wsum(w, d.snu[(size_t)en.x * NS + z], d.snu[(size_t)en.y * NS + z], d.snu[(size_t)en.z * NS + z],
                         d.snu[(size_t)en.w * NS + z]);
@@ -194,4 +194,4 @@ void launch_d3end(const Dev &d, cudaStream_t s) {
 }
 void launch_av(const Dev &d, cudaStream_t s) { k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d); }
 
-}  // namespace fesomc
+FESOMC_PREC_END

@@ -15,7 +15,7 @@
 //                 compensated deterministic two-pass reduction
 #include "device_common.cuh"
 
-namespace fesomc {
+FESOMC_PREC_BEGIN
 
 constexpr int kRedBlock = 256;
 constexpr int kRedGrid = 592;  // 4 x 148 SMs
@@ -24,11 +24,11 @@ constexpr int kRedGrid = 592;  // 4 x 148 SMs
 // global min / max of TF and SF
 // ---------------------------------------------------------------------------
 __global__ void k_minmax_part(Dev d) {
-    __shared__ double s[4][kRedBlock];
+    __shared__ real s[4][kRedBlock];
     const long long total = (long long)d.N * d.L;
-    double tmin = d.TF[0], tmax = d.TF[0], smin = d.SF[0], smax = d.SF[0];
+    real tmin = d.TF[0], tmax = d.TF[0], smin = d.SF[0], smax = d.SF[0];
     GRID_LOOP(i, total) {
-        const double t = d.TF[i], x = d.SF[i];
+        const real t = d.TF[i], x = d.SF[i];
         tmin = dmin(tmin, t); tmax = dmax(tmax, t);
         smin = dmin(smin, x); smax = dmax(smax, x);
     }
@@ -52,7 +52,7 @@ __global__ void k_minmax_part(Dev d) {
 __global__ void k_minmax_final(Dev d, int nparts) {
     if (blockIdx.x != 0) return;
     const int lane = threadIdx.x & 31;
-    double tmin = d.mm_part[0], tmax = d.mm_part[1], smin = d.mm_part[2], smax = d.mm_part[3];
+    real tmin = d.mm_part[0], tmax = d.mm_part[1], smin = d.mm_part[2], smax = d.mm_part[3];
     for (int b = lane; b < nparts; b += 32) {
         tmin = dmin(tmin, d.mm_part[4 * b + 0]);
         tmax = dmax(tmax, d.mm_part[4 * b + 1]);
@@ -66,27 +66,27 @@ __global__ void k_minmax_final(Dev d, int nparts) {
         smax = dmax(smax, __shfl_xor_sync(kFull, smax, o));
     }
     if (lane == 0) {
-        d.aver[0] = 0.5 * (tmin + tmax);
-        d.aver[1] = 0.5 * (smin + smax);
+        d.aver[0] = real(0.5) * (tmin + tmax);
+        d.aver[1] = real(0.5) * (smin + smax);
     }
 }
 
 // AB2 value of a tracer at (node, level) minus its mean (fv_tracer.F90:433)
-__device__ __forceinline__ double ab2(const Dev &d, const double *Tn, const double *To, size_t i, double aver) {
-    return -(0.5 + d.epsilon) * To[i] + (1.5 + d.epsilon) * Tn[i] - aver;
+__device__ __forceinline__ real ab2(const Dev &d, const real *Tn, const real *To, size_t i, real aver) {
+    return -(real(0.5) + d.epsilon) * To[i] + (real(1.5) + d.epsilon) * Tn[i] - aver;
 }
 
 // Vel_nor at node n from its boundary edges (fv_tracer.F90:862-873)
-__device__ __forceinline__ double vel_nor(const Dev &d, int n) {
-    double v = 0.0;
+__device__ __forceinline__ real vel_nor(const Dev &d, int n) {
+    real v = real(0.0);
     for (int p = d.node_bptr[n]; p < d.node_bptr[n + 1]; ++p) {
         const int code = d.node_bidx[p];
         const int ed = code >> 1;
         const int2 nn = d.edge_nodes[ed];
         const int e1 = d.edge_tri[ed].x;
-        const double dmean = dmax(d.Dmin, 0.5 * (d.eta_n[nn.x] + d.depth[nn.x] + d.eta_n[nn.y] + d.depth[nn.y]));
-        const double4 X = d.edge_cross[ed];
-        const double un1 = (d.V_filt_2D[e1] * X.x - d.U_filt_2D[e1] * X.y) * dmean;
+        const real dmean = dmax<real>(d.Dmin, real(0.5) * (d.eta_n[nn.x] + d.depth[nn.x] + d.eta_n[nn.y] + d.depth[nn.y]));
+        const real4 X = d.edge_cross[ed];
+        const real un1 = (d.V_filt_2D[e1] * X.x - d.U_filt_2D[e1] * X.y) * dmean;
         if (code & 1) v = v - un1 / d.area[n];
         else v = v + un1 / d.area[n];
     }
@@ -96,46 +96,46 @@ __device__ __forceinline__ double vel_nor(const Dev &d, int n) {
 // QUICK vertical flux tvert(k) of solve_tracer_upwind at interface k
 // (0-based, 0..NS-1) of node n; TO(m) returns the AB2 tracer of layer m.
 template <typename F>
-__device__ __forceinline__ double tvert_upwind(const Dev &d, int k, double a, const double *W, F TO) {
+__device__ __forceinline__ real tvert_upwind(const Dev &d, int k, real a, const real *W, F TO) {
     const int NS = d.NS;
-    if (k == NS - 1) return 0.0;
+    if (k == NS - 1) return real(0.0);
     if (k == 0) return -W[0] * TO(0);
     const int nz = k + 1;  // 1-based
     // Z(m), zbar(m) 1-based
     auto Z = [&](int m) { return z_of(d, a, m - 1); };
     auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
     auto T = [&](int m) { return TO(m - 1); };
-    const double w = W[nz - 1];
+    const real w = W[nz - 1];
     if (nz == 2) {
-        if (w > 0.0) {
-            const double dg = (ZB(2) - Z(1)) * (Z(2) - ZB(2)) / ((Z(3) - Z(1)) * (Z(2) - Z(3)));
-            const double db = -(ZB(2) - Z(1)) * (Z(3) - ZB(2)) / ((Z(2) - Z(1)) * (Z(2) - Z(3)));
-            return -(T(1) * (1.0 - dg - db) + T(2) * db + T(3) * dg) * w;
+        if (w > real(0.0)) {
+            const real dg = (ZB(2) - Z(1)) * (Z(2) - ZB(2)) / ((Z(3) - Z(1)) * (Z(2) - Z(3)));
+            const real db = -(ZB(2) - Z(1)) * (Z(3) - ZB(2)) / ((Z(2) - Z(1)) * (Z(2) - Z(3)));
+            return -(T(1) * (real(1.0) - dg - db) + T(2) * db + T(3) * dg) * w;
         }
         return -T(1) * w;
     }
     if (nz <= NS - 2) {
-        if (w >= 0.0) {
-            const double dg = (ZB(nz) - Z(nz - 1)) * (Z(nz) - ZB(nz)) / ((Z(nz + 1) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
-            const double db = -(ZB(nz) - Z(nz - 1)) * (Z(nz + 1) - ZB(nz)) / ((Z(nz) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
-            return -(T(nz - 1) * (1.0 - dg - db) + T(nz) * db + T(nz + 1) * dg) * w;
+        if (w >= real(0.0)) {
+            const real dg = (ZB(nz) - Z(nz - 1)) * (Z(nz) - ZB(nz)) / ((Z(nz + 1) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+            const real db = -(ZB(nz) - Z(nz - 1)) * (Z(nz + 1) - ZB(nz)) / ((Z(nz) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+            return -(T(nz - 1) * (real(1.0) - dg - db) + T(nz) * db + T(nz + 1) * dg) * w;
         }
-        const double dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
-        const double db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
-        return -(T(nz) * (1.0 - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
+        const real dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
+        const real db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
+        return -(T(nz) * (real(1.0) - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
     }
     // nz == NS-1
-    if (w >= 0.0) return -T(nz) * w;
-    const double dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
-    const double db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
-    return -(T(nz) * (1.0 - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
+    if (w >= real(0.0)) return -T(nz) * w;
+    const real dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
+    const real db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
+    return -(T(nz) * (real(1.0) - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
 }
 
 // AB2 tracers of this step minus their means, stored once per (node, level)
 // for the gathers below (fv_tracer.F90:433,435 and :39-47)
 __global__ void k_ab2_node(Dev d) {
     const long long total = (long long)d.N * d.L;
-    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    const real T_aver = d.aver[0], S_aver = d.aver[1];
     GRID_LOOP(i, total) {
         d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
         d.stfold[i] = ab2(d, d.SF, d.S_old, i, S_aver);
@@ -148,46 +148,46 @@ __global__ void k_ab2_node(Dev d) {
 // ---------------------------------------------------------------------------
 __global__ void k_upwind_h(Dev d) {
     const int lane = threadIdx.x & 31;
-    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
     WARP_LOOP(nn_, d.N) {
         const int n = (int)nn_;
-        const double a = jac_a(d, d.eta_jac, n);
-        const double *W = d.Wvel + (size_t)n * NS;
+        const real a = jac_a(d, d.eta_jac, n);
+        const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
-        const double area_inv = 1.0 / d.area[n];
+        const real area_inv = real(1.0) / d.area[n];
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
         const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const double vn = relax ? vel_nor(d, n) : 0.0;
+        const real vn = relax ? vel_nor(d, n) : real(0.0);
         for (int z0 = 0; z0 < L; z0 += 32) {
             const int z = z0 + lane;
             const int zc = z < L ? z : L - 1;
-            double acc_t = 0.0, acc_s = 0.0, acc_c = 0.0;
+            real acc_t = real(0.0), acc_s = real(0.0), acc_c = real(0.0);
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
                 const int2 nn = d.edge_nodes[ed];
                 const int2 et = d.edge_tri[ed];
-                const double4 X = d.edge_cross[ed];
+                const real4 X = d.edge_cross[ed];
                 const size_t i1 = (size_t)nn.x * L + zc, i2 = (size_t)nn.y * L + zc;
-                const double t1 = d.ttfold[i1], t2 = d.ttfold[i2];
-                const double s1 = d.stfold[i1], s2 = d.stfold[i2];
+                const real t1 = d.ttfold[i1], t2 = d.ttfold[i2];
+                const real s1 = d.stfold[i1], s2 = d.stfold[i2];
                 const size_t e1 = (size_t)et.x * L + zc;
-                const double J1 = d.Je[e1];
-                const double c1 = d.V_n_filt[e1] * X.x - d.U_n_filt[e1] * X.y;
-                double aux_c, t_aux, s_aux;
+                const real J1 = d.Je[e1];
+                const real c1 = d.V_n_filt[e1] * X.x - d.U_n_filt[e1] * X.y;
+                real aux_c, t_aux, s_aux;
                 if (ed < d.Ed_in) {
                     const size_t e2 = (size_t)et.y * L + zc;
-                    const double J2 = d.Je[e2];
-                    const double c2 = -d.V_n_filt[e2] * X.z + d.U_n_filt[e2] * X.w;
+                    const real J2 = d.Je[e2];
+                    const real c2 = -d.V_n_filt[e2] * X.z + d.U_n_filt[e2] * X.w;
                     aux_c = J1 * c1 + J2 * c2;
-                    if (c1 > 0.0 && c2 > 0.0) {
+                    if (c1 > real(0.0) && c2 > real(0.0)) {
                         t_aux = J1 * c1 * t2 + J2 * c2 * t2;
                         s_aux = J1 * c1 * s2 + J2 * c2 * s2;
-                    } else if (c1 > 0.0) {
+                    } else if (c1 > real(0.0)) {
                         t_aux = J1 * c1 * t2 + J2 * c2 * t1;
                         s_aux = J1 * c1 * s2 + J2 * c2 * s1;
-                    } else if (c2 > 0.0) {
+                    } else if (c2 > real(0.0)) {
                         t_aux = J1 * c1 * t1 + J2 * c2 * t2;
                         s_aux = J1 * c1 * s1 + J2 * c2 * s2;
                     } else {
@@ -196,7 +196,7 @@ __global__ void k_upwind_h(Dev d) {
                     }
                 } else {
                     aux_c = J1 * c1;
-                    if (c1 > 0.0) { t_aux = aux_c * t2; s_aux = aux_c * s2; }
+                    if (c1 > real(0.0)) { t_aux = aux_c * t2; s_aux = aux_c * s2; }
                     else { t_aux = aux_c * t1; s_aux = aux_c * s1; }
                 }
                 if (code & 1) { acc_c = acc_c - aux_c; acc_t = acc_t - t_aux; acc_s = acc_s - s_aux; }
@@ -204,20 +204,20 @@ __global__ void k_upwind_h(Dev d) {
             }
             auto TO = [&](int m) { return d.ttfold[base + m]; };
             auto SO = [&](int m) { return d.stfold[base + m]; };
-            const double tv0 = tvert_upwind(d, zc, a, W, TO), sv0 = tvert_upwind(d, zc, a, W, SO);
-            double tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
+            const real tv0 = tvert_upwind(d, zc, a, W, TO), sv0 = tvert_upwind(d, zc, a, W, SO);
+            real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
             if (lane == 31 || zc == L - 1) {
                 tv1 = tvert_upwind(d, zc + 1, a, W, TO);
                 sv1 = tvert_upwind(d, zc + 1, a, W, SO);
             }
             if (z < L) {
                 const size_t ii = base + z;
-                const double to = d.ttfold[ii], so = d.stfold[ii];
-                const double jc = jc_of(d, a, z);
-                double tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
-                double sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
+                const real to = d.ttfold[ii], so = d.stfold[ii];
+                const real jc = jc_of(d, a, z);
+                real tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
+                real sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
                 if (relax) {
-                    if (vn > 0.0) {
+                    if (vn > real(0.0)) {
                         tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (to + T_aver));
                         sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (so + S_aver));
                     } else {
@@ -225,7 +225,7 @@ __global__ void k_upwind_h(Dev d) {
                         sr = d.clim_relax * (d.Sclim[ii] - (so + S_aver));
                     }
                 }
-                const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+                const real ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
                 d.Told_new[ii] = ttf + T_aver;
                 d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
                 d.Sold_new[ii] = stf + S_aver;
@@ -248,9 +248,9 @@ __global__ void k_muscl_egrad(Dev d) {
         const int4 en = d.elem_nodes[e];
         const size_t i1 = (size_t)en.x * L + z, i2 = (size_t)en.y * L + z, i3 = (size_t)en.z * L + z,
                      i4 = (size_t)en.w * L + z;
-        const double t1 = d.ttfold[i1], t2 = d.ttfold[i2], t3 = d.ttfold[i3], t4 = d.ttfold[i4];
-        const double s1 = d.stfold[i1], s2 = d.stfold[i2], s3 = d.stfold[i3], s4 = d.stfold[i4];
-        const double4 gx = d.gs_x[e], gy = d.gs_y[e];
+        const real t1 = d.ttfold[i1], t2 = d.ttfold[i2], t3 = d.ttfold[i3], t4 = d.ttfold[i4];
+        const real s1 = d.stfold[i1], s2 = d.stfold[i2], s3 = d.stfold[i3], s4 = d.stfold[i4];
+        const real4 gx = d.gs_x[e], gy = d.gs_y[e];
         d.ttx[ii] = wsum(gx, t1, t2, t3, t4);
         d.tty[ii] = wsum(gy, t1, t2, t3, t4);
         d.stx[ii] = wsum(gx, s1, s2, s3, s4);
@@ -266,10 +266,10 @@ __global__ void k_muscl_ngrad(Dev d) {
         const int n = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
-        double tvol = 0.0, a = 0.0, b = 0.0, c = 0.0, e4 = 0.0;
+        real tvol = real(0.0), a = real(0.0), b = real(0.0), c = real(0.0), e4 = real(0.0);
         for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
             const int el = d.node_nidx[p];
-            const double ar = d.elem_area[el];
+            const real ar = d.elem_area[el];
             const size_t i = (size_t)el * L + z;
             tvol = tvol + ar;
             a = a + d.ttx[i] * ar;
@@ -290,35 +290,35 @@ __global__ void k_muscl_ngrad(Dev d) {
 // as in the reference.  MUSCL groups the weights as a*b/(c+a)/(b-c), Miura
 // as a*b/((c+a)*(b-c)).
 template <bool MUSCL, typename F>
-__device__ __forceinline__ double tvert_quick(const Dev &d, int k, double a, const double *W, F TO) {
+__device__ __forceinline__ real tvert_quick(const Dev &d, int k, real a, const real *W, F TO) {
     const int NS = d.NS;
-    if (k == NS - 1) return 0.0;
+    if (k == NS - 1) return real(0.0);
     if (k == 0) return -W[0] * TO(0);
-    double Tmean = 0.0;
+    real Tmean = real(0.0);
     // replay interfaces back to the last one with W /= 0 (carried Tmean)
     int start = k + 1;
-    while (start > 2 && W[start - 1] == 0.0) --start;
+    while (start > 2 && W[start - 1] == real(0.0)) --start;
     for (int nz = start; nz <= k + 1; ++nz) {
-        const double w = W[nz - 1];
+        const real w = W[nz - 1];
         auto Z = [&](int m) { return z_of(d, a, m - 1); };
         auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
-        if (w > 0.0) {
+        if (w > real(0.0)) {
             if (nz == NS - 1) Tmean = TO(nz - 1);
             else {
-                const double aa = ZB(nz) - Z(nz - 1), bb = Z(nz) - ZB(nz), cc = Z(nz + 1) - ZB(nz);
-                const double dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
-                const double db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
-                const double da = 1.0 - dg - db;
+                const real aa = ZB(nz) - Z(nz - 1), bb = Z(nz) - ZB(nz), cc = Z(nz + 1) - ZB(nz);
+                const real dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const real db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
+                const real da = real(1.0) - dg - db;
                 Tmean = TO(nz - 2) * da + TO(nz - 1) * db + TO(nz) * dg;
             }
         }
-        if (w < 0.0) {
+        if (w < real(0.0)) {
             if (nz == 2) Tmean = TO(nz - 2);
             else {
-                const double aa = Z(nz) - ZB(nz), bb = ZB(nz) - Z(nz - 1), cc = ZB(nz) - Z(nz - 2);
-                const double dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
-                const double db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
-                const double da = 1.0 - dg - db;
+                const real aa = Z(nz) - ZB(nz), bb = ZB(nz) - Z(nz - 1), cc = ZB(nz) - Z(nz - 2);
+                const real dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const real db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
+                const real da = real(1.0) - dg - db;
                 Tmean = TO(nz - 1) * da + TO(nz - 2) * db + TO(nz - 3) * dg;
             }
         }
@@ -326,12 +326,12 @@ __device__ __forceinline__ double tvert_quick(const Dev &d, int k, double a, con
     return -Tmean * W[k];
 }
 template <typename F>
-__device__ __forceinline__ double tvert_muscl(const Dev &d, int k, double a, const double *W, F TO) {
+__device__ __forceinline__ real tvert_muscl(const Dev &d, int k, real a, const real *W, F TO) {
     return tvert_quick<true>(d, k, a, W, TO);
 }
 
-__device__ __forceinline__ double muscl_mean(bool upw2, double Tm1, double Tm2) {
-    return upw2 ? 0.15 * Tm2 + 0.85 * (Tm1 + Tm2) / 2.0 : 0.15 * Tm1 + 0.85 * (Tm1 + Tm2) / 2.0;
+__device__ __forceinline__ real muscl_mean(bool upw2, real Tm1, real Tm2) {
+    return upw2 ? real(0.15) * Tm2 + real(0.85) * (Tm1 + Tm2) / real(2.0) : real(0.15) * Tm1 + real(0.85) * (Tm1 + Tm2) / real(2.0);
 }
 
 // MUSCL segment fluxes of one (edge, level) (fv_tracer.F90:59-170 for T and
@@ -347,12 +347,12 @@ __global__ void k_muscl_edge(Dev d) {
         const int2 nn = d.edge_nodes[ed];
         const int2 et = d.edge_tri[ed];
         const int2 ud = d.edge_updn[ed];
-        const double4 X = d.edge_cross[ed];
-        const double2 exy = d.edge_dxdy[ed];
+        const real4 X = d.edge_cross[ed];
+        const real2 exy = d.edge_dxdy[ed];
         const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
-        const double T1 = d.ttfold[i1], T2 = d.ttfold[i2];
-        const double S1 = d.stfold[i1], S2 = d.stfold[i2];
-        double g1, g2, g3, g4, h1, h2, h3, h4;
+        const real T1 = d.ttfold[i1], T2 = d.ttfold[i2];
+        const real S1 = d.stfold[i1], S2 = d.stfold[i2];
+        real g1, g2, g3, g4, h1, h2, h3, h4;
         if (ud.x >= 0 && ud.y >= 0) {
             const size_t u = (size_t)ud.x * L + z, w = (size_t)ud.y * L + z;
             g1 = d.ttx[u]; g2 = d.ttx[w]; g3 = d.tty[u]; g4 = d.tty[w];
@@ -361,42 +361,42 @@ __global__ void k_muscl_edge(Dev d) {
             g1 = d.tnx[i1]; g2 = d.tnx[i2]; g3 = d.tny[i1]; g4 = d.tny[i2];
             h1 = d.snx[i1]; h2 = d.snx[i2]; h3 = d.sny[i1]; h4 = d.sny[i2];
         }
-        double2 fT, fS, fC;
+        real2 fT, fS, fC;
         {
-            const double a = kREarth * d.elem_cos[et.x];
+            const real a = kREarth * d.elem_cos[et.x];
             const size_t e1 = (size_t)et.x * L + z;
-            const double J1 = d.Je[e1];
-            const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+            const real J1 = d.Je[e1];
+            const real U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
             const bool up1 = V1 * X.x - U1 * X.y > 0;
-            const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / 6.0;
-            const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / 6.0;
-            const double Tm = muscl_mean(up1, Tm1, Tm2);
+            const real Tm2 = T2 - (real(2.0) * (T2 - T1) + exy.x * a * g2 + exy.y * kREarth * g4) / real(6.0);
+            const real Tm1 = T1 + (real(2.0) * (T2 - T1) + exy.x * a * g1 + exy.y * kREarth * g3) / real(6.0);
+            const real Tm = muscl_mean(up1, Tm1, Tm2);
             fT.x = (J1 * V1 * Tm) * X.x - (J1 * U1 * Tm) * X.y;
-            const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / 6.0;
-            const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / 6.0;
-            const double Sm = muscl_mean(up1, Sm1, Sm2);
+            const real Sm2 = S2 - (real(2.0) * (S2 - S1) + exy.x * a * h2 + exy.y * kREarth * h4) / real(6.0);
+            const real Sm1 = S1 + (real(2.0) * (S2 - S1) + exy.x * a * h1 + exy.y * kREarth * h3) / real(6.0);
+            const real Sm = muscl_mean(up1, Sm1, Sm2);
             fS.x = (J1 * V1 * Sm) * X.x - (J1 * U1 * Sm) * X.y;
             fC.x = J1 * V1 * X.x - J1 * U1 * X.y;
         }
         if (et.y >= 0) {
-            const double b = kREarth * d.elem_cos[et.y];
+            const real b = kREarth * d.elem_cos[et.y];
             const size_t e2 = (size_t)et.y * L + z;
-            const double J2 = d.Je[e2];
-            const double U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
+            const real J2 = d.Je[e2];
+            const real U2f = d.U_n_filt[e2], V2f = d.V_n_filt[e2];
             const bool up2 = V2f * X.z - U2f * X.w < 0;
-            const double Tm2 = T2 - (2.0 * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / 6.0;
-            const double Tm1 = T1 + (2.0 * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / 6.0;
-            const double Tm = muscl_mean(up2, Tm1, Tm2);
-            const double Sm2 = S2 - (2.0 * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / 6.0;
-            const double Sm1 = S1 + (2.0 * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / 6.0;
-            const double Sm = muscl_mean(up2, Sm1, Sm2);
+            const real Tm2 = T2 - (real(2.0) * (T2 - T1) + exy.x * b * g2 + exy.y * kREarth * g4) / real(6.0);
+            const real Tm1 = T1 + (real(2.0) * (T2 - T1) + exy.x * b * g1 + exy.y * kREarth * g3) / real(6.0);
+            const real Tm = muscl_mean(up2, Tm1, Tm2);
+            const real Sm2 = S2 - (real(2.0) * (S2 - S1) + exy.x * b * h2 + exy.y * kREarth * h4) / real(6.0);
+            const real Sm1 = S1 + (real(2.0) * (S2 - S1) + exy.x * b * h1 + exy.y * kREarth * h3) / real(6.0);
+            const real Sm = muscl_mean(up2, Sm1, Sm2);
             // second segment uses U_n / V_n (fv_tracer.F90:158-159)
-            const double Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
+            const real Un2 = d.U_n[e2], Vn2 = d.V_n[e2];
             fT.y = -(J2 * Vn2 * Tm) * X.z + (J2 * Un2 * Tm) * X.w;
             fS.y = -(J2 * Vn2 * Sm) * X.z + (J2 * Un2 * Sm) * X.w;
             fC.y = -J2 * V2f * X.z + J2 * U2f * X.w;
         } else {
-            fT.y = 0.0; fS.y = 0.0; fC.y = 0.0;
+            fT.y = real(0.0); fS.y = real(0.0); fC.y = real(0.0);
         }
         d.mflT[ii] = fT;
         d.mflS[ii] = fS;
@@ -409,27 +409,27 @@ __global__ void k_muscl_edge(Dev d) {
 // of several edges are in flight together; the sums stay in edge order.
 __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
     const int lane = threadIdx.x & 31;
-    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
     WARP_LOOP(nn_, d.N) {
         const int n = (int)nn_;
-        const double an = jac_a(d, d.eta_jac, n);
-        const double *W = d.Wvel + (size_t)n * NS;
+        const real an = jac_a(d, d.eta_jac, n);
+        const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
         const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const double vn = relax ? vel_nor(d, n) : 0.0;
-        const double area = d.area[n];
+        const real vn = relax ? vel_nor(d, n) : real(0.0);
+        const real area = d.area[n];
         for (int z0 = 0; z0 < L; z0 += 32) {
             const int z = z0 + lane;
             const int zc = z < L ? z : L - 1;
-            double rt = 0.0, rs = 0.0, rc = 0.0;
+            real rt = real(0.0), rs = real(0.0), rc = real(0.0);
 #pragma unroll 4
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
                 const size_t i = (size_t)ed * L + zc;
-                const double2 fT = d.mflT[i], fS = d.mflS[i], fC = d.mflC[i];
+                const real2 fT = d.mflT[i], fS = d.mflS[i], fC = d.mflC[i];
                 const bool internal = ed < d.Ed_in;
                 if (code & 1) {
                     rt = rt - fT.x; rs = rs - fS.x; rc = rc - fC.x;
@@ -441,22 +441,22 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
             }
             auto TO = [&](int m) { return d.ttfold[base + m]; };
             auto SO = [&](int m) { return d.stfold[base + m]; };
-            const double tv0 = tvert_muscl(d, zc, an, W, TO), sv0 = tvert_muscl(d, zc, an, W, SO);
-            double tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
+            const real tv0 = tvert_muscl(d, zc, an, W, TO), sv0 = tvert_muscl(d, zc, an, W, SO);
+            real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
             if (lane == 31 || zc == L - 1) {
                 tv1 = tvert_muscl(d, zc + 1, an, W, TO);
                 sv1 = tvert_muscl(d, zc + 1, an, W, SO);
             }
             if (z < L) {
                 const size_t ii = base + z;
-                const double jc = jc_of(d, an, z);
-                const double aj = area * jc;
-                const double to = d.ttfold[ii], so = d.stfold[ii];
-                double tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
-                double sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
-                const double ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+                const real jc = jc_of(d, an, z);
+                const real aj = area * jc;
+                const real to = d.ttfold[ii], so = d.stfold[ii];
+                real tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
+                real sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
+                const real ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
                 if (relax) {
-                    if (vn > 0.0) {
+                    if (vn > real(0.0)) {
                         tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
                         sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
                     } else {
@@ -482,17 +482,17 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
 // H_advtr_crit = 0.1, H_advtr_min = 0)
 __global__ void k_miura_prep(Dev d) {
     const long long total = (long long)d.N * d.L;
-    const double T_aver = d.aver[0];
+    const real T_aver = d.aver[0];
     GRID_LOOP(i, total) {
         d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
         d.tnow[i] = d.TF[i] - T_aver;
         if (i % d.L == 0) {
             const int n = (int)(i / d.L);
-            const double crit = 0.1, hmin = 0.0;
-            const double dmean = dmax(d.Dmin, d.depth[n] + d.eta_n[n]);
-            double m;
-            if (dmean > crit) m = 1.0;
-            else if (dmean < hmin) m = 0.0;
+            const real crit = real(0.1), hmin = real(0.0);
+            const real dmean = dmax<real>(d.Dmin, d.depth[n] + d.eta_n[n]);
+            real m;
+            if (dmean > crit) m = real(1.0);
+            else if (dmean < hmin) m = real(0.0);
             else m = (dmean - hmin) / (crit - hmin);
             d.mask_ad[n] = m;
         }
@@ -507,8 +507,8 @@ __global__ void k_miura_egrad(Dev d) {
         const int z = (int)(ii % d.L);
         const int L = d.L;
         const int4 en = d.elem_nodes[e];
-        const double t1 = d.tnow[(size_t)en.x * L + z], t2 = d.tnow[(size_t)en.y * L + z];
-        const double t3 = d.tnow[(size_t)en.z * L + z], t4 = d.tnow[(size_t)en.w * L + z];
+        const real t1 = d.tnow[(size_t)en.x * L + z], t2 = d.tnow[(size_t)en.y * L + z];
+        const real t3 = d.tnow[(size_t)en.z * L + z], t4 = d.tnow[(size_t)en.w * L + z];
         d.ttx[ii] = wsum(d.gs_x[e], t1, t2, t3, t4);
         d.tty[ii] = wsum(d.gs_y[e], t1, t2, t3, t4);
     }
@@ -522,13 +522,13 @@ __global__ void k_miura_ngrad(Dev d) {
         const int n = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
-        double s = 0.0;
+        real s = real(0.0);
         for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) s = s + d.elem_area[d.node_nidx[p]];
-        const double tvol = 1.0 / s;
-        double tx = 0.0, ty = 0.0;
+        const real tvol = real(1.0) / s;
+        real tx = real(0.0), ty = real(0.0);
         for (int p = d.node_nptr[n]; p < d.node_nptr[n + 1]; ++p) {
             const int el = d.node_nidx[p];
-            const double ar = d.elem_area[el];
+            const real ar = d.elem_area[el];
             tx = tx + d.ttx[(size_t)el * L + z] * ar;
             ty = ty + d.tty[(size_t)el * L + z] * ar;
         }
@@ -542,60 +542,60 @@ __global__ void k_miura_ngrad(Dev d) {
 __global__ void k_miura_edge(Dev d) {
     const long long total = (long long)d.Ed * d.L;
     const int L = d.L;
-    const double dt = d.dt;
+    const real dt = d.dt;
     GRID_LOOP(ii, total) {
         const int ed = (int)(ii / L);
         const int z = (int)(ii % L);
         const int2 nn = d.edge_nodes[ed];
         const int2 et = d.edge_tri[ed];
-        const double4 X = d.edge_cross[ed];
-        const double2 exy = d.edge_dxdy[ed];
-        const double crt1 = 0.5 * (d.mask_ad[nn.x] + d.mask_ad[nn.y]);
+        const real4 X = d.edge_cross[ed];
+        const real2 exy = d.edge_dxdy[ed];
+        const real crt1 = real(0.5) * (d.mask_ad[nn.x] + d.mask_ad[nn.y]);
         const bool two = et.y >= 0;
-        const double a = 1.0, b = 1.0;
-        double Kh = d.elem_area[et.x];
-        if (two) Kh = 0.5 * (Kh + d.elem_area[et.y]);
+        const real a = real(1.0), b = real(1.0);
+        real Kh = d.elem_area[et.x];
+        if (two) Kh = real(0.5) * (Kh + d.elem_area[et.y]);
         Kh = d.K_hor * Kh / d.scale_area;
         const size_t e1 = (size_t)et.x * L + z;
         const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
-        double Tx, Ty;
+        real Tx, Ty;
         if (two) {
             const size_t e2 = (size_t)et.y * L + z;
-            Tx = 0.5 * Kh * (d.ttx[e1] + d.ttx[e2]);
-            Ty = 0.5 * Kh * (d.tty[e1] + d.tty[e2]);
+            Tx = real(0.5) * Kh * (d.ttx[e1] + d.ttx[e2]);
+            Ty = real(0.5) * Kh * (d.tty[e1] + d.tty[e2]);
         } else {
             Tx = Kh * d.ttx[e1];
             Ty = Kh * d.tty[e1];
         }
-        const double J1 = d.Je[e1];
-        const double U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
-        double Tmean;
+        const real J1 = d.Je[e1];
+        const real U1 = d.U_n_filt[e1], V1 = d.V_n_filt[e1];
+        real Tmean;
         if (V1 * X.x - U1 * X.y > 0) {
             // no dt on the V term in this branch (fv_tracer.F90:1057)
-            Tmean = d.tnow[i2] + (0.5 * (-exy.x * a + X.x - U1 * dt) * d.tnx[i2] +
-                                  0.5 * (-exy.y * kREarth + X.y - V1) * d.tny[i2]) * crt1;
+            Tmean = d.tnow[i2] + (real(0.5) * (-exy.x * a + X.x - U1 * dt) * d.tnx[i2] +
+                                  real(0.5) * (-exy.y * kREarth + X.y - V1) * d.tny[i2]) * crt1;
         } else {
-            Tmean = d.tnow[i1] + (0.5 * (exy.x * a + X.x - U1 * dt) * d.tnx[i1] +
-                                  0.5 * (exy.y * kREarth + X.y - V1 * dt) * d.tny[i1]) * crt1;
+            Tmean = d.tnow[i1] + (real(0.5) * (exy.x * a + X.x - U1 * dt) * d.tnx[i1] +
+                                  real(0.5) * (exy.y * kREarth + X.y - V1 * dt) * d.tny[i1]) * crt1;
         }
-        double2 fT, fC;
+        real2 fT, fC;
         fT.x = (J1 * V1 * Tmean - Ty) * X.x - (J1 * U1 * Tmean - Tx) * X.y;
         fC.x = J1 * V1 * X.x - J1 * U1 * X.y;
         if (two) {
             const size_t e2 = (size_t)et.y * L + z;
-            const double J2 = d.Je[e2];
-            const double U2 = d.U_n_filt[e2], V2 = d.V_n_filt[e2];
+            const real J2 = d.Je[e2];
+            const real U2 = d.U_n_filt[e2], V2 = d.V_n_filt[e2];
             if (V2 * X.z - U2 * X.w < 0) {
-                Tmean = d.tnow[i2] + (0.5 * (-exy.x * b + X.z - U2 * dt) * d.tnx[i2] +
-                                      0.5 * (-exy.y * kREarth + X.w - V2 * dt) * d.tny[i2]) * crt1;
+                Tmean = d.tnow[i2] + (real(0.5) * (-exy.x * b + X.z - U2 * dt) * d.tnx[i2] +
+                                      real(0.5) * (-exy.y * kREarth + X.w - V2 * dt) * d.tny[i2]) * crt1;
             } else {
-                Tmean = d.tnow[i1] + (0.5 * (exy.x * b + X.z - U2 * dt) * d.tnx[i1] +
-                                      0.5 * (exy.y * kREarth + X.w - V2 * dt) * d.tny[i1]) * crt1;
+                Tmean = d.tnow[i1] + (real(0.5) * (exy.x * b + X.z - U2 * dt) * d.tnx[i1] +
+                                      real(0.5) * (exy.y * kREarth + X.w - V2 * dt) * d.tny[i1]) * crt1;
             }
             fT.y = -(J2 * V2 * Tmean - Ty) * X.z + (J2 * U2 * Tmean - Tx) * X.w;
             fC.y = -J2 * V2 * X.z + J2 * U2 * X.w;
         } else {
-            fT.y = 0.0; fC.y = 0.0;
+            fT.y = real(0.0); fC.y = real(0.0);
         }
         d.mflT[ii] = fT;
         d.mflC[ii] = fC;
@@ -606,27 +606,27 @@ __global__ void k_miura_edge(Dev d) {
 // salinity passed through; one warp per node, lane = level
 __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
     const int lane = threadIdx.x & 31;
-    const double T_aver = d.aver[0];
+    const real T_aver = d.aver[0];
     const int L = d.L, NS = d.NS;
     WARP_LOOP(nn_, d.N) {
         const int n = (int)nn_;
-        const double an = jac_a(d, d.eta_jac, n);
-        const double *W = d.Wvel + (size_t)n * NS;
+        const real an = jac_a(d, d.eta_jac, n);
+        const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
         const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const double vn = relax ? vel_nor(d, n) : 0.0;
-        const double area = d.area[n];
+        const real vn = relax ? vel_nor(d, n) : real(0.0);
+        const real area = d.area[n];
         for (int z0 = 0; z0 < L; z0 += 32) {
             const int z = z0 + lane;
             const int zc = z < L ? z : L - 1;
-            double rt = 0.0, rc = 0.0;
+            real rt = real(0.0), rc = real(0.0);
 #pragma unroll 4
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
                 const int ed = code >> 1;
                 const size_t i = (size_t)ed * L + zc;
-                const double2 fT = d.mflT[i], fC = d.mflC[i];
+                const real2 fT = d.mflT[i], fC = d.mflC[i];
                 const bool internal = ed < d.Ed_in;
                 if (code & 1) {
                     rt = rt - fT.x; rc = rc - fC.x;
@@ -637,17 +637,17 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
                 }
             }
             auto TN = [&](int m) { return d.tnow[base + m]; };
-            const double tv0 = tvert_quick<false>(d, zc, an, W, TN);
-            double tv1 = __shfl_down_sync(kFull, tv0, 1);
+            const real tv0 = tvert_quick<false>(d, zc, an, W, TN);
+            real tv1 = __shfl_down_sync(kFull, tv0, 1);
             if (lane == 31 || zc == L - 1) tv1 = tvert_quick<false>(d, zc + 1, an, W, TN);
             if (z < L) {
                 const size_t ii = base + z;
-                const double jc = jc_of(d, an, z);
-                const double to = d.ttfold[ii];
-                const double ttf = d.tnow[ii];
-                double tr = ((rt - to * rc) / area + to * (W[z] - W[z + 1]) + tv0 - tv1) / jc;
+                const real jc = jc_of(d, an, z);
+                const real to = d.ttfold[ii];
+                const real ttf = d.tnow[ii];
+                real tr = ((rt - to * rc) / area + to * (W[z] - W[z + 1]) + tv0 - tv1) / jc;
                 if (relax) {
-                    if (vn > 0.0) tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                    if (vn > real(0.0)) tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
                     else tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
                 }
                 d.Told_new[ii] = ttf + T_aver;
@@ -662,13 +662,13 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
 // Tracer after advection and the river source, minus its mean: T(k) / S(k)
 // of tracer_impl_vert_diff.  The river source (fv_main.F90:1804-1823) adds
 // its terms to S in river-list order.
-__device__ __forceinline__ double vd_salt(const Dev &d, int n, size_t base, int z, double aj, double S_aver) {
-    double S = d.SF_adv[base + z];
+__device__ __forceinline__ real vd_salt(const Dev &d, int n, size_t base, int z, real aj, real S_aver) {
+    real S = d.SF_adv[base + z];
     if (d.key_rivers) {
         for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) {
-            const double r = d.runoff[d.node_ridx[p]];
-            const double coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
-            const double delta = (d.river_salinity - d.Sold_new[base + z]);
+            const real r = d.runoff[d.node_ridx[p]];
+            const real coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
+            const real delta = (d.river_salinity - d.Sold_new[base + z]);
             S = S + delta * coeff;
         }
     }
@@ -677,24 +677,24 @@ __device__ __forceinline__ double vd_salt(const Dev &d, int n, size_t base, int 
 
 // Tridiagonal coefficients a(k), b(k), c(k) of layer k (0-based) of node
 // column n (fv_tracer.F90:1380-1420).
-__device__ __forceinline__ void vd_coef(const Dev &d, const double *Kv, double aj, int k, double &a, double &b,
-                                        double &c) {
+__device__ __forceinline__ void vd_coef(const Dev &d, const real *Kv, real aj, int k, real &a, real &b,
+                                        real &c) {
     const int L = d.L, NS = d.NS;
-    const double dt = d.dt;
+    const real dt = d.dt;
     auto Zc = [&](int m) { return z_of(d, aj, m); };
     auto ZBc = [&](int m) { return zbar_of(d, aj, m); };
     if (k == 0) {
         c = -dt * Kv[1] / ((Zc(0) - Zc(1)) * (ZBc(0) - ZBc(1)));
-        a = 0.0;
-        b = -c + 1.0;
+        a = real(0.0);
+        b = -c + real(1.0);
     } else if (k == L - 1) {
         a = -dt * Kv[L - 1] / ((Zc(L - 2) - Zc(L - 1)) * (ZBc(L - 1) - ZBc(NS - 1)));
-        b = -a + 1.0;
-        c = 0.0;
+        b = -a + real(1.0);
+        c = real(0.0);
     } else {
         a = -dt * Kv[k] / ((Zc(k - 1) - Zc(k)) * (ZBc(k) - ZBc(k + 1)));
         c = -dt * Kv[k] / ((Zc(k) - Zc(k + 1)) * (ZBc(k) - ZBc(k + 1)));
-        b = -a - c + 1.0;
+        b = -a - c + real(1.0);
     }
 }
 
@@ -703,26 +703,27 @@ __device__ __forceinline__ void vd_coef(const Dev &d, const double *Kv, double a
 // ([array][level][thread]); T and S are re-read instead of stored.
 constexpr int kVdBlock = 128;
 __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
-    extern __shared__ double sm[];
-    const double T_aver = d.aver[0], S_aver = d.aver[1];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    real *sm = reinterpret_cast<real *>(sm_raw);
+    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
-    double *col = sm + threadIdx.x;
+    real *col = sm + threadIdx.x;
     const int bd = blockDim.x;
-    auto CP = [&](int k) -> double & { return col[((size_t)0 * L + k) * bd]; };
-    auto TP = [&](int k) -> double & { return col[((size_t)1 * L + k) * bd]; };
-    auto SP = [&](int k) -> double & { return col[((size_t)2 * L + k) * bd]; };
+    auto CP = [&](int k) -> real & { return col[((size_t)0 * L + k) * bd]; };
+    auto TP = [&](int k) -> real & { return col[((size_t)1 * L + k) * bd]; };
+    auto SP = [&](int k) -> real & { return col[((size_t)2 * L + k) * bd]; };
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
         const size_t base = (size_t)n * L;
-        const double aj = jac_a(d, d.eta_jac, n);
-        const double *Kv = d.Kv + (size_t)n * NS;
+        const real aj = jac_a(d, d.eta_jac, n);
+        const real *Kv = d.Kv + (size_t)n * NS;
         auto Tz = [&](int z) { return d.TF_adv[base + z] - T_aver; };
         auto Sz = [&](int z) { return vd_salt(d, n, base, z, aj, S_aver); };
         // forward elimination; the right-hand side of layer k uses T(k-1..k+1)
-        double Tm = 0.0, T0 = Tz(0), Tp = Tz(1);
-        double Sm = 0.0, S0 = Sz(0), Sp = Sz(1);
+        real Tm = real(0.0), T0 = Tz(0), Tp = Tz(1);
+        real Sm = real(0.0), S0 = Sz(0), Sp = Sz(1);
         for (int k = 0; k < L; ++k) {
-            double a, b, c, tr, sr;
+            real a, b, c, tr, sr;
             vd_coef(d, Kv, aj, k, a, b, c);
             if (k == 0) {
                 tr = c * (-Tp + T0);
@@ -739,7 +740,7 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
                 TP(0) = tr / b;
                 SP(0) = sr / b;
             } else {
-                const double m = 1.0 / (b - CP(k - 1) * a);
+                const real m = real(1.0) / (b - CP(k - 1) * a);
                 CP(k) = c * m;
                 TP(k) = (tr - TP(k - 1) * a) * m;
                 SP(k) = (sr - SP(k - 1) * a) * m;
@@ -750,16 +751,16 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
         }
         // back substitution and update, bottom to top
         unsigned int st = 0;
-        double tr = 0.0, sr = 0.0;
+        real tr = real(0.0), sr = real(0.0);
         for (int z = L - 1; z >= 0; --z) {
             if (z == L - 1) { tr = TP(z); sr = SP(z); }
             else { tr = TP(z) - CP(z) * tr; sr = SP(z) - CP(z) * sr; }
             const size_t i = base + z;
-            double t = Tz(z) + tr + T_aver;
-            double s = Sz(z) + sr + S_aver;
-            if (fabs(s) < 1.0e-12) s = fabs(s);
-            if (s < 0.0) st |= 0x1u;
-            if (t < -3.0) st |= 0x2u;
+            real t = Tz(z) + tr + T_aver;
+            real s = Sz(z) + sr + S_aver;
+            if (fabs(s) < real(1.0e-12)) s = fabs(s);
+            if (s < real(0.0)) st |= 0x1u;
+            if (t < -real(3.0)) st |= 0x2u;
             if (!isfinite(t) || !isfinite(s)) st |= 0x4u;
             d.TF[i] = t;
             d.SF[i] = s;
@@ -771,54 +772,57 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
     }
 }
 
+#if !FESOMC_FP32  // the energy diagnostic is FP64 only
 // ---------------------------------------------------------------------------
 // energy: compensated (Neumaier) partial sums per block, then one block
 // ---------------------------------------------------------------------------
 struct KSum {
-    double s, c;
-    __device__ void add(double x) {
-        double t = s + x;
+    real s, c;
+    __device__ void add(real x) {
+        real t = s + x;
         if (fabs(s) >= fabs(x)) c += (s - t) + x;
         else c += (x - t) + s;
         s = t;
     }
-    __device__ double value() const { return s + c; }
+    __device__ real value() const { return s + c; }
 };
 
-__global__ void k_energy_part(Dev d, double *part) {
-    __shared__ double sh[3][kRedBlock];
-    KSum pe{0.0, 0.0}, ke{0.0, 0.0}, ar{0.0, 0.0};
+__global__ void k_energy_part(Dev d, real *part) {
+    __shared__ real sh[3][kRedBlock];
+    KSum pe{real(0.0), real(0.0)}, ke{real(0.0), real(0.0)}, ar{real(0.0), real(0.0)};
     GRID_LOOP(i, d.N) {
-        const double e = d.eta_n[i];
-        pe.add(0.5 * kG * d.area[i] * (e * e));
+        const real e = d.eta_n[i];
+        pe.add(real(0.5) * kG * d.area[i] * (e * e));
         ar.add(d.area[i]);
     }
     GRID_LOOP(i, d.E) {
         const int4 en = d.elem_nodes[i];
-        const double4 w = d.w_cv[i];
-        const double s = wsum(w, dmax(d.Dmin, d.depth[en.x] + d.eta_n[en.x]), dmax(d.Dmin, d.depth[en.y] + d.eta_n[en.y]),
+        const real4 w = d.w_cv[i];
+        const real s = wsum(w, dmax(d.Dmin, d.depth[en.x] + d.eta_n[en.x]), dmax(d.Dmin, d.depth[en.y] + d.eta_n[en.y]),
                               dmax(d.Dmin, d.depth[en.z] + d.eta_n[en.z]), dmax(d.Dmin, d.depth[en.w] + d.eta_n[en.w]));
-        const double2 u = d.U_n_2D[i];
-        ke.add(0.5 * s * d.elem_area[i] * (u.x * u.x + u.y * u.y));
+        const real2 u = d.U_n_2D[i];
+        ke.add(real(0.5) * s * d.elem_area[i] * (u.x * u.x + u.y * u.y));
     }
     sh[0][threadIdx.x] = pe.value();
     sh[1][threadIdx.x] = ke.value();
     sh[2][threadIdx.x] = ar.value();
     __syncthreads();
     if (threadIdx.x < 3) {
-        KSum t{0.0, 0.0};
+        KSum t{real(0.0), real(0.0)};
         for (int k = 0; k < kRedBlock; ++k) t.add(sh[threadIdx.x][k]);
         part[(size_t)blockIdx.x * 3 + threadIdx.x] = t.value();
     }
 }
 
-__global__ void k_energy_final(const double *part, int nparts, double *out) {
+__global__ void k_energy_final(const real *part, int nparts, real *out) {
     if (threadIdx.x < 3 && blockIdx.x == 0) {
-        KSum t{0.0, 0.0};
+        KSum t{real(0.0), real(0.0)};
         for (int b = 0; b < nparts; ++b) t.add(part[(size_t)b * 3 + threadIdx.x]);
         out[threadIdx.x] = t.value();
     }
 }
+
+#endif
 
 // ---- launch wrappers --------------------------------------------------------
 void launch_minmax(const Dev &d, cudaStream_t s) {
@@ -846,7 +850,7 @@ void launch_muscl_edge(const Dev &d, cudaStream_t s) {
 }
 void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
-static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(double); }
+static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 int config_vdiff(const Dev &d) {
     return cudaFuncSetAttribute(k_vdiff_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vdiff_smem(d)) ==
                    cudaSuccess ? 0 : 1;
@@ -854,10 +858,12 @@ int config_vdiff(const Dev &d) {
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     k_vdiff_col<<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
 }
+#if !FESOMC_FP32
 int energy_parts() { return kRedGrid; }
-void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {
+void launch_energy(const Dev &d, real *part, real *out, cudaStream_t s) {
     k_energy_part<<<kRedGrid, kRedBlock, 0, s>>>(d, part);
     k_energy_final<<<1, 32, 0, s>>>(part, kRedGrid, out);
 }
+#endif
 
-}  // namespace fesomc
+FESOMC_PREC_END

@@ -13,44 +13,51 @@
 #include "fesomc_gpu.h"
 
 namespace fesomc {
-// kernels (k_*.cu)
-void launch_ab3_elem(const Dev &, cudaStream_t);
-void launch_ssh_node(const Dev &, int, cudaStream_t);
-void launch_puls_elem(const Dev &, cudaStream_t);
-void launch_el2nodes(const Dev &, const double *, const double *, double *, double *, cudaStream_t);
-void launch_p1_edge(const Dev &, cudaStream_t);
-void launch_p1_elem(const Dev &, cudaStream_t);
-void launch_adv2d_edge(const Dev &, cudaStream_t);
-void launch_u2d_elem(const Dev &, cudaStream_t);
-void launch_rot_nodes(const Dev &, cudaStream_t);
-void launch_zero_filt(const Dev &, cudaStream_t);
-void launch_pressure_col(const Dev &, cudaStream_t);
-void launch_bpg_elem(const Dev &, cudaStream_t);
-void launch_velgrad3d(const Dev &, cudaStream_t);
-void launch_adv3_edge(const Dev &, cudaStream_t);
-void launch_velrhs(const Dev &, double, cudaStream_t);
-void launch_implvisc(const Dev &, cudaStream_t);
-void launch_jac_swap(const Dev &, cudaStream_t);
-void launch_je(const Dev &, cudaStream_t);
-int config_d3end(const Dev &);
-int config_vdiff(const Dev &);
-int config_p1(const Dev &);
-int config_columns(const Dev &);
-void launch_ab2(const Dev &, cudaStream_t);
-void launch_update3d(const Dev &, double, cudaStream_t);
-void launch_wvel(const Dev &, cudaStream_t);
-void launch_d3end(const Dev &, cudaStream_t);
-void launch_av(const Dev &, cudaStream_t);
-void launch_minmax(const Dev &, cudaStream_t);
-void launch_upwind(const Dev &, cudaStream_t);
-void launch_muscl_egrad(const Dev &, cudaStream_t);
-void launch_muscl_ngrad(const Dev &, cudaStream_t);
-void launch_muscl_edge(const Dev &, cudaStream_t);
-void launch_miura(const Dev &, cudaStream_t);
-void launch_muscl_h(const Dev &, cudaStream_t);
-void launch_vdiff(const Dev &, cudaStream_t);
-int energy_parts();
-void launch_energy(const Dev &, double *, double *, cudaStream_t);
+// kernels (k_*.cu), compiled once per precision
+#define FESOMC_KERNEL_LAUNCHERS \
+    void launch_ab3_elem(const Dev &, cudaStream_t); \
+    void launch_ssh_node(const Dev &, int, cudaStream_t); \
+    void launch_puls_elem(const Dev &, cudaStream_t); \
+    void launch_el2nodes(const Dev &, const real *, const real *, real *, real *, cudaStream_t); \
+    void launch_p1_edge(const Dev &, cudaStream_t); \
+    void launch_p1_elem(const Dev &, cudaStream_t); \
+    void launch_adv2d_edge(const Dev &, cudaStream_t); \
+    void launch_u2d_elem(const Dev &, cudaStream_t); \
+    void launch_rot_nodes(const Dev &, cudaStream_t); \
+    void launch_zero_filt(const Dev &, cudaStream_t); \
+    void launch_pressure_col(const Dev &, cudaStream_t); \
+    void launch_bpg_elem(const Dev &, cudaStream_t); \
+    void launch_velgrad3d(const Dev &, cudaStream_t); \
+    void launch_adv3_edge(const Dev &, cudaStream_t); \
+    void launch_velrhs(const Dev &, real, cudaStream_t); \
+    void launch_implvisc(const Dev &, cudaStream_t); \
+    void launch_jac_swap(const Dev &, cudaStream_t); \
+    void launch_je(const Dev &, cudaStream_t); \
+    int config_d3end(const Dev &); \
+    int config_vdiff(const Dev &); \
+    int config_p1(const Dev &); \
+    int config_columns(const Dev &); \
+    void launch_ab2(const Dev &, cudaStream_t); \
+    void launch_update3d(const Dev &, real, cudaStream_t); \
+    void launch_wvel(const Dev &, cudaStream_t); \
+    void launch_d3end(const Dev &, cudaStream_t); \
+    void launch_av(const Dev &, cudaStream_t); \
+    void launch_minmax(const Dev &, cudaStream_t); \
+    void launch_upwind(const Dev &, cudaStream_t); \
+    void launch_muscl_egrad(const Dev &, cudaStream_t); \
+    void launch_muscl_ngrad(const Dev &, cudaStream_t); \
+    void launch_muscl_edge(const Dev &, cudaStream_t); \
+    void launch_miura(const Dev &, cudaStream_t); \
+    void launch_muscl_h(const Dev &, cudaStream_t); \
+    void launch_vdiff(const Dev &, cudaStream_t); \
+    int energy_parts(); \
+    void launch_energy(const Dev &, real *, real *, cudaStream_t);
+namespace f64 {
+FESOMC_KERNEL_LAUNCHERS
+}  // namespace f64
+namespace f32 {
+FESOMC_KERNEL_LAUNCHERS
+}  // namespace f32
 
 int grid_for(long long n, int block) {
     long long g = (n + block - 1) / block;
@@ -66,6 +73,7 @@ static const double kPi = 3.14159265358979;
 }  // namespace fesomc
 
 using namespace fesomc;
+using namespace fesomc::f64;
 
 struct fesomc_model {
     Dev d{};

@@ -18,6 +18,7 @@ CSRC = os.path.join(ROOT_DIR, "csrc")
 INC = os.path.join(REPO_DIR, "include")
 OBJ_DIR = os.path.join(ROOT_DIR, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+DUAL_PRECISION = ("k_baroclinic.cu", "k_barotropic.cu", "k_tracer.cu", "k_mixing.cu")
 
 
 def _nvcc():
@@ -41,6 +42,7 @@ def _stale(out, deps):
 def _headers():
     return (glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
             + glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
+            + glob.glob(os.path.join(CSRC, "**", "*.inc"), recursive=True)
             + glob.glob(os.path.join(INC, "*.h")))
 
 
@@ -63,14 +65,21 @@ def build_library(verbose=False, ptxas_v=False):
                          "-Wall", "-I", INC, "-I", CSRC, "-c", src, "-o", obj])
     nvcc = _nvcc()
     for src in sorted(glob.glob(os.path.join(CSRC, "**", "*.cu"), recursive=True)):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
-        objs.append(obj)
-        if _stale(obj, [src] + hdrs) or ptxas_v:
-            cmd = [nvcc] + ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-                                   "-ccbin", _cxx(), "-I", INC, "-I", CSRC, "-c", src, "-o", obj]
-            if ptxas_v:
-                cmd += ["-Xptxas", "-v"]
-            jobs.append(cmd)
+        # kernel sources with level fields are compiled once per arithmetic
+        # precision (fesomc::f64 and fesomc::f32)
+        variants = [("", "0")]
+        if os.path.basename(src) in DUAL_PRECISION:
+            variants.append((".f32", "1"))
+        for suffix, fp32 in variants:
+            obj = os.path.join(OBJ_DIR, os.path.basename(src) + suffix + ".o")
+            objs.append(obj)
+            if _stale(obj, [src] + hdrs) or ptxas_v:
+                cmd = [nvcc] + ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
+                                       "-ccbin", _cxx(), "-DFESOMC_FP32=" + fp32, "-I", INC, "-I", CSRC, "-c", src,
+                                       "-o", obj]
+                if ptxas_v:
+                    cmd += ["-Xptxas", "-v"]
+                jobs.append(cmd)
     logs = []
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
