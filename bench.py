@@ -204,6 +204,7 @@ def run_ours(args, ws, rank, local):
     abi.check(lib.fesomc_gpu_set_device(local), "fesomc_gpu_set_device")
     cfg = args.config
     case = build_case(cfg)
+    case.params.fp32_form = 1 if args.fp32_form else 0
     g = model.GpuModel(case)
     m = case.mesh
     units_per_step = m.N * m.L
@@ -282,8 +283,8 @@ def run_ours(args, ws, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(case, cfg),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.fp32_form else "f64",
+        "data": "synthetic", "config": workload_config(case, cfg),
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1000.0 * t_e2e / args.steps},
@@ -312,6 +313,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp32-form", action="store_true",
+                    help="run the FP32 form (level fields and 3D arithmetic in FP32, 2D sub-cycle in FP64)")
     args = ap.parse_args()
     ws, rank, local = dist_info()
     if args.impl == "reference":

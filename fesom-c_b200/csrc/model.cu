@@ -76,7 +76,10 @@ using namespace fesomc;
 using namespace fesomc::f64;
 
 struct fesomc_model {
-    Dev d{};
+    Dev d{};                    // FP64 view: 2D sub-cycle (always) and, in the FP64 form, everything
+    fesomc::f32::Dev d32{};     // FP32 form: level fields, geometry and 3D arithmetic in FP32
+    bool fp32 = false;
+    std::vector<float> h_f32;   // host staging for FP32 level fields
     fesomc_params p{};
     cudaStream_t stream = nullptr;
     std::vector<void *> allocs;
@@ -149,53 +152,82 @@ int upload(fesomc_model *m, const T **dst, const std::vector<T> &src) {
     return FESOMC_OK;
 }
 
-// field table for state sync: name of the fesomc_state member, device pointer, count, group
+// field table for state sync: name of the fesomc_state member, device
+// pointer, count, group, and whether the device copy is FP32 (level fields of
+// the FP32 form)
 struct FieldRef {
     double *fesomc_state::*host;
-    double *dev;
+    void *dev;
     size_t count;
     uint32_t group;
+    bool f32;
 };
 
 std::vector<FieldRef> field_table(fesomc_model *m) {
     Dev &d = m->d;
+    fesomc::f32::Dev &q = m->d32;
+    const bool f = m->fp32;
     const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
+#define LEV(name) (f ? (void *)q.name : (void *)d.name)
     return {
-        {&fesomc_state::eta_n, d.eta_n, N, FESOMC_F_ETA},
-        {&fesomc_state::eta_n_1, d.eta_n_1, N, FESOMC_F_ETA},
-        {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA},
-        {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA},
-        {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA},
-        {&fesomc_state::U_n_2D, reinterpret_cast<double *>(d.U_n_2D), 2 * E, FESOMC_F_UV2D},
-        {&fesomc_state::U_n_1, reinterpret_cast<double *>(d.U_n_1), 2 * E, FESOMC_F_UV2D},
-        {&fesomc_state::U_n_2, reinterpret_cast<double *>(d.U_n_2), 2 * E, FESOMC_F_UV2D},
-        {&fesomc_state::U_filt_2D, d.U_filt_2D, E, FESOMC_F_UV2D},
-        {&fesomc_state::V_filt_2D, d.V_filt_2D, E, FESOMC_F_UV2D},
-        {&fesomc_state::U_n, d.U_n, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::V_n, d.V_n, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::U_rhsAB, d.U_rhsAB, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::V_rhsAB, d.V_rhsAB, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::U_n_filt, d.U_n_filt, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::V_n_filt, d.V_n_filt, L * E, FESOMC_F_UV3D},
-        {&fesomc_state::TF, d.TF, L * N, FESOMC_F_TS},
-        {&fesomc_state::SF, d.SF, L * N, FESOMC_F_TS},
-        {&fesomc_state::T_old, d.T_old, L * N, FESOMC_F_TS},
-        {&fesomc_state::S_old, d.S_old, L * N, FESOMC_F_TS},
-        {&fesomc_state::Tclim, d.Tclim, L * N, FESOMC_F_CLIM},
-        {&fesomc_state::Sclim, d.Sclim, L * N, FESOMC_F_CLIM},
-        {&fesomc_state::bt, d.bt, NS * N, FESOMC_F_MIX},
-        {&fesomc_state::snu, d.snu, NS * N, FESOMC_F_MIX},
-        {&fesomc_state::Kv, d.Kv, NS * N, FESOMC_F_MIX},
-        {&fesomc_state::Ri, d.Ri, NS * N, FESOMC_F_MIX},
-        {&fesomc_state::tke_dissip, d.tke_dissip, NS * N, FESOMC_F_MIX},
-        {&fesomc_state::Av, d.Av, NS * E, FESOMC_F_MIX},
-        {&fesomc_state::Wvel, d.Wvel, NS * N, FESOMC_F_WVEL},
-        {&fesomc_state::mask_wd, d.mask_wd, E, FESOMC_F_MASK},
-        {&fesomc_state::mask_wd_node, d.mask_wd_node, N, FESOMC_F_MASK},
-        {&fesomc_state::rho_c, d.rho_c, L * N, FESOMC_F_DIAG},
-        {&fesomc_state::hpressure, d.hpressure, NS * N, FESOMC_F_DIAG},
-        {&fesomc_state::Bar_pr_2D, reinterpret_cast<double *>(d.Bar_pr_2D), 2 * E, FESOMC_F_DIAG},
+        {&fesomc_state::eta_n, d.eta_n, N, FESOMC_F_ETA, false},
+        {&fesomc_state::eta_n_1, d.eta_n_1, N, FESOMC_F_ETA, false},
+        {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA, false},
+        {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA, false},
+        {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA, false},
+        {&fesomc_state::U_n_2D, d.U_n_2D, 2 * E, FESOMC_F_UV2D, false},
+        {&fesomc_state::U_n_1, d.U_n_1, 2 * E, FESOMC_F_UV2D, false},
+        {&fesomc_state::U_n_2, d.U_n_2, 2 * E, FESOMC_F_UV2D, false},
+        {&fesomc_state::U_filt_2D, d.U_filt_2D, E, FESOMC_F_UV2D, false},
+        {&fesomc_state::V_filt_2D, d.V_filt_2D, E, FESOMC_F_UV2D, false},
+        {&fesomc_state::U_n, LEV(U_n), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::V_n, LEV(V_n), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::U_rhsAB, LEV(U_rhsAB), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::V_rhsAB, LEV(V_rhsAB), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::U_n_filt, LEV(U_n_filt), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::V_n_filt, LEV(V_n_filt), L * E, FESOMC_F_UV3D, f},
+        {&fesomc_state::TF, LEV(TF), L * N, FESOMC_F_TS, f},
+        {&fesomc_state::SF, LEV(SF), L * N, FESOMC_F_TS, f},
+        {&fesomc_state::T_old, LEV(T_old), L * N, FESOMC_F_TS, f},
+        {&fesomc_state::S_old, LEV(S_old), L * N, FESOMC_F_TS, f},
+        {&fesomc_state::Tclim, LEV(Tclim), L * N, FESOMC_F_CLIM, f},
+        {&fesomc_state::Sclim, LEV(Sclim), L * N, FESOMC_F_CLIM, f},
+        {&fesomc_state::bt, LEV(bt), NS * N, FESOMC_F_MIX, f},
+        {&fesomc_state::snu, LEV(snu), NS * N, FESOMC_F_MIX, f},
+        {&fesomc_state::Kv, LEV(Kv), NS * N, FESOMC_F_MIX, f},
+        {&fesomc_state::Ri, LEV(Ri), NS * N, FESOMC_F_MIX, f},
+        {&fesomc_state::tke_dissip, LEV(tke_dissip), NS * N, FESOMC_F_MIX, f},
+        {&fesomc_state::Av, LEV(Av), NS * E, FESOMC_F_MIX, f},
+        {&fesomc_state::Wvel, LEV(Wvel), NS * N, FESOMC_F_WVEL, f},
+        {&fesomc_state::mask_wd, d.mask_wd, E, FESOMC_F_MASK, false},
+        {&fesomc_state::mask_wd_node, d.mask_wd_node, N, FESOMC_F_MASK, false},
+        {&fesomc_state::rho_c, LEV(rho_c), L * N, FESOMC_F_DIAG, f},
+        {&fesomc_state::hpressure, LEV(hpressure), NS * N, FESOMC_F_DIAG, f},
+        {&fesomc_state::Bar_pr_2D, d.Bar_pr_2D, 2 * E, FESOMC_F_DIAG, false},
     };
+#undef LEV
+}
+
+// host double <-> device field (converting for FP32 level fields)
+int field_to_host(fesomc_model *m, const FieldRef &f, double *h) {
+    if (!f.f32) {
+        CK(cudaMemcpy(h, f.dev, f.count * sizeof(double), cudaMemcpyDeviceToHost));
+        return FESOMC_OK;
+    }
+    m->h_f32.resize(f.count);
+    CK(cudaMemcpy(m->h_f32.data(), f.dev, f.count * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < f.count; ++i) h[i] = (double)m->h_f32[i];
+    return FESOMC_OK;
+}
+int field_from_host(fesomc_model *m, void *dev, bool f32, size_t count, const double *h) {
+    if (!f32) {
+        CK(cudaMemcpy(dev, h, count * sizeof(double), cudaMemcpyHostToDevice));
+        return FESOMC_OK;
+    }
+    m->h_f32.resize(count);
+    for (size_t i = 0; i < count; ++i) m->h_f32[i] = (float)h[i];
+    CK(cudaMemcpy(dev, m->h_f32.data(), count * sizeof(float), cudaMemcpyHostToDevice));
+    return FESOMC_OK;
 }
 
 int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
@@ -344,9 +376,10 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
     return FESOMC_OK;
 }
 
-int alloc_state(fesomc_model *m) {
+// 2D (sub-cycle) state, forcing and diagnostics: FP64 in both forms
+int alloc_2d(fesomc_model *m) {
     Dev &d = m->d;
-    const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
+    const size_t N = d.N, E = d.E;
     int rc = 0;
     double **nodes[] = {&d.eta_n, &d.eta_n_1, &d.eta_n_2, &d.eta_new, &d.etaAB, &d.ssh_gp, &d.eta_jac,
                         &d.eta_jac_old, &d.mask_wd_node, &d.windx, &d.windy};
@@ -357,34 +390,9 @@ int alloc_state(fesomc_model *m) {
     for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
     if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
     if ((rc = dalloc(m, &d.bfric, E))) return rc;
-    if ((rc = dalloc(m, &d.Fp, E))) return rc;
-    if ((rc = dalloc(m, &d.adv3, L * (size_t)d.Ed_in))) return rc;
     if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
-    double **le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
-                     &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv, &d.Je, &d.Ze, &d.ZBe};
-    for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
-    double **ln[] = {&d.Unode, &d.Vnode, &d.Unode_p, &d.Vnode_p, &d.TF, &d.SF, &d.T_old, &d.S_old, &d.Tclim,
-                     &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new, &d.ttfold, &d.stfold};
-    for (auto p : ln) if ((rc = dalloc(m, p, L * N))) return rc;
-    if (m->p.tracer_adv == FESOMC_TRACER_MUSCL || m->p.tracer_adv == FESOMC_TRACER_MIURA) {
-        double **lg[] = {&d.ttx, &d.tty, &d.stx, &d.sty};
-        for (auto p : lg) if ((rc = dalloc(m, p, L * E))) return rc;
-        double **lgn[] = {&d.tnx, &d.tny, &d.snx, &d.sny};
-        for (auto p : lgn) if ((rc = dalloc(m, p, L * N))) return rc;
-        double2 **fl[] = {&d.mflT, &d.mflS, &d.mflC};
-        for (auto p : fl) if ((rc = dalloc(m, p, L * (size_t)d.Ed))) return rc;
-    }
-    if (m->p.tracer_adv == FESOMC_TRACER_MIURA) {
-        if ((rc = dalloc(m, &d.tnow, L * N))) return rc;
-        if ((rc = dalloc(m, &d.mask_ad, N))) return rc;
-    }
-    double **nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
-    for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
-    if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
     if ((rc = dalloc(m, &d.runoff, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1)))) return rc;
     if ((rc = dalloc(m, &d.ob_val, (size_t)(d.nobn > 0 ? d.nobn : 1) * (m->p.Mt > 0 ? m->p.Mt : 1)))) return rc;
-    if ((rc = dalloc(m, &d.mm_part, (size_t)4 * 1024))) return rc;
-    if ((rc = dalloc(m, &d.aver, 2))) return rc;
     if ((rc = dalloc(m, &d.status, 1))) return rc;
     if ((rc = dalloc(m, &d.notconv, 1))) return rc;
     if ((rc = dalloc(m, &m->d_epart, (size_t)3 * energy_parts()))) return rc;
@@ -392,7 +400,105 @@ int alloc_state(fesomc_model *m) {
     return FESOMC_OK;
 }
 
-void set_params(Dev &d, const fesomc_params &p) {
+// level fields and scratch of the 3D kernels, in the working precision of D
+template <typename D>
+int alloc_3d(fesomc_model *m, D &d) {
+    const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
+    int rc = 0;
+    if ((rc = dalloc(m, &d.Fp, E))) return rc;
+    if ((rc = dalloc(m, &d.adv3, L * (size_t)d.Ed_in))) return rc;
+    decltype(&d.U_n) le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
+                             &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv,
+                             &d.Je, &d.Ze, &d.ZBe};
+    for (auto p : le) if ((rc = dalloc(m, p, L * E))) return rc;
+    decltype(&d.U_n) ln[] = {&d.Unode, &d.Vnode, &d.Unode_p, &d.Vnode_p, &d.TF, &d.SF, &d.T_old, &d.S_old,
+                             &d.Tclim, &d.Sclim, &d.rho_c, &d.TF_adv, &d.SF_adv, &d.Told_new, &d.Sold_new,
+                             &d.ttfold, &d.stfold};
+    for (auto p : ln) if ((rc = dalloc(m, p, L * N))) return rc;
+    if (m->p.tracer_adv == FESOMC_TRACER_MUSCL || m->p.tracer_adv == FESOMC_TRACER_MIURA) {
+        decltype(&d.U_n) lg[] = {&d.ttx, &d.tty, &d.stx, &d.sty};
+        for (auto p : lg) if ((rc = dalloc(m, p, L * E))) return rc;
+        decltype(&d.U_n) lgn[] = {&d.tnx, &d.tny, &d.snx, &d.sny};
+        for (auto p : lgn) if ((rc = dalloc(m, p, L * N))) return rc;
+        decltype(&d.mflT) fl[] = {&d.mflT, &d.mflS, &d.mflC};
+        for (auto p : fl) if ((rc = dalloc(m, p, L * (size_t)d.Ed))) return rc;
+    }
+    if (m->p.tracer_adv == FESOMC_TRACER_MIURA) {
+        if ((rc = dalloc(m, &d.tnow, L * N))) return rc;
+        if ((rc = dalloc(m, &d.mask_ad, N))) return rc;
+    }
+    decltype(&d.U_n) nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
+    for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
+    if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
+    if ((rc = dalloc(m, &d.mm_part, (size_t)4 * 1024))) return rc;
+    if ((rc = dalloc(m, &d.aver, 2))) return rc;
+    return FESOMC_OK;
+}
+
+int alloc_state(fesomc_model *m) {
+    int rc = alloc_2d(m);
+    if (rc) return rc;
+    return m->fp32 ? alloc_3d(m, m->d32) : alloc_3d(m, m->d);
+}
+
+// FP32 form: the f32 view shares the sizes, flags, connectivity and the FP64
+// 2D state with the f64 view, and holds FP32 copies of the mesh geometry.
+template <typename TO>
+int geom_f32(fesomc_model *m, const void *src, size_t n_doubles, const TO **dst) {
+    std::vector<double> h(n_doubles);
+    CK(cudaMemcpy(h.data(), src, n_doubles * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<float> g(n_doubles);
+    for (size_t i = 0; i < n_doubles; ++i) g[i] = (float)h[i];
+    float *q = nullptr;
+    int rc = dalloc(m, &q, n_doubles);
+    if (rc) return rc;
+    CK(cudaMemcpy(q, g.data(), n_doubles * sizeof(float), cudaMemcpyHostToDevice));
+    *dst = reinterpret_cast<const TO *>(q);
+    return FESOMC_OK;
+}
+
+int setup_f32_view(fesomc_model *m) {
+    const Dev &a = m->d;
+    fesomc::f32::Dev &b = m->d32;
+    b.N = a.N; b.E = a.E; b.Ed = a.Ed; b.Ed_in = a.Ed_in; b.L = a.L; b.NS = a.NS;
+    b.nobn = a.nobn; b.n_rivers = a.n_rivers;
+    b.elem_nodes = a.elem_nodes; b.elem_nb = a.elem_nb; b.elem_edges = a.elem_edges; b.elem_iedges = a.elem_iedges;
+    b.edge_nodes = a.edge_nodes; b.edge_tri = a.edge_tri; b.edge_updn = a.edge_updn;
+    b.node_eptr = a.node_eptr; b.node_eidx = a.node_eidx; b.node_nptr = a.node_nptr; b.node_nidx = a.node_nidx;
+    b.node_bptr = a.node_bptr; b.node_bidx = a.node_bidx; b.node_rptr = a.node_rptr; b.node_ridx = a.node_ridx;
+    b.obn_of_node = a.obn_of_node; b.index_nod2D = a.index_nod2D;
+    const size_t N = a.N, E = a.E, Ed = a.Ed, L = a.L, NS = a.NS;
+    int rc;
+    if ((rc = geom_f32(m, a.sig, NS, &b.sig)) || (rc = geom_f32(m, a.dsig, L, &b.dsig)) ||
+        (rc = geom_f32(m, a.w_cv, 4 * E, &b.w_cv)) || (rc = geom_f32(m, a.gs_x, 4 * E, &b.gs_x)) ||
+        (rc = geom_f32(m, a.gs_y, 4 * E, &b.gs_y)) || (rc = geom_f32(m, a.gv_x, 4 * E, &b.gv_x)) ||
+        (rc = geom_f32(m, a.gv_y, 4 * E, &b.gv_y)) || (rc = geom_f32(m, a.elem_area, E, &b.elem_area)) ||
+        (rc = geom_f32(m, a.elem_cos, E, &b.elem_cos)) || (rc = geom_f32(m, a.coriolis, E, &b.coriolis)) ||
+        (rc = geom_f32(m, a.area, N, &b.area)) || (rc = geom_f32(m, a.depth, N, &b.depth)) ||
+        (rc = geom_f32(m, a.ac, N, &b.ac)) || (rc = geom_f32(m, a.atp1, N, &b.atp1)) ||
+        (rc = geom_f32(m, a.atp2, N, &b.atp2)) || (rc = geom_f32(m, a.elem_acc, E, &b.elem_acc)) ||
+        (rc = geom_f32(m, a.elem_bpfac, E, &b.elem_bpfac)) || (rc = geom_f32(m, a.edge_dxdy, 2 * Ed, &b.edge_dxdy)) ||
+        (rc = geom_f32(m, a.edge_cross, 4 * Ed, &b.edge_cross)) || (rc = geom_f32(m, a.node_tvol, N, &b.node_tvol)))
+        return rc;
+    return FESOMC_OK;
+}
+
+// share the FP64 2D state with the f32 view (after alloc_state)
+void share_2d(fesomc_model *m) {
+    const Dev &a = m->d;
+    fesomc::f32::Dev &b = m->d32;
+    b.eta_n = a.eta_n; b.eta_n_1 = a.eta_n_1; b.eta_n_2 = a.eta_n_2; b.eta_new = a.eta_new; b.etaAB = a.etaAB;
+    b.ssh_gp = a.ssh_gp; b.eta_jac = a.eta_jac; b.eta_jac_old = a.eta_jac_old;
+    b.U_n_2D = a.U_n_2D; b.U_n_1 = a.U_n_1; b.U_n_2 = a.U_n_2; b.UAB = a.UAB; b.U_rhs_2D_3D = a.U_rhs_2D_3D;
+    b.Bar_pr_2D = a.Bar_pr_2D; b.bfric = a.bfric;
+    b.aux_elem = a.aux_elem; b.dmean_n = a.dmean_n; b.U_filt_2D = a.U_filt_2D; b.V_filt_2D = a.V_filt_2D;
+    b.mask_wd = a.mask_wd; b.mask_wd_node = a.mask_wd_node; b.vel_grad = a.vel_grad;
+    b.taux = a.taux; b.tauy = a.tauy; b.windx = a.windx; b.windy = a.windy; b.runoff = a.runoff;
+    b.ob_val = a.ob_val; b.adv2d = a.adv2d; b.status = a.status; b.notconv = a.notconv;
+}
+
+template <typename D>
+void set_params(D &d, const fesomc_params &p) {
     d.dt = p.dt; d.dt_2D = p.dt_2D; d.Dmin = p.Dmin; d.C_d = p.C_d; d.beta = p.beta; d.epsilon = p.epsilon;
     d.density_0 = p.density_0; d.scale_area = p.scale_area; d.snul = p.snul; d.z0b_min = p.z0b_min;
     d.z0s_min = p.z0s_min; d.Pr_num = p.Pr_num; d.beta_scale = p.beta_scale; d.cka = p.cka;
@@ -408,7 +514,7 @@ void set_params(Dev &d, const fesomc_params &p) {
 // read or write counted once at its element size (connectivity and geometry
 // once), no credit for re-reads.  N nodes, E elements, Ed edges (Ei
 // internal), L layers, NS = L+1 interfaces.
-double kernel_bytes(const fesomc_model *m, const std::string &k) {
+double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     const Dev &d = m->d;
     const double N = d.N, E = d.E, Ed = d.Ed, Ei = d.Ed_in, L = d.L, NS = d.NS;
     const double nnz_ne = (double)(2 * d.Ed);  // node->edge incidences
@@ -469,6 +575,17 @@ double kernel_bytes(const fesomc_model *m, const std::string &k) {
     return 0.0;
 }
 
+// In the FP32 form the 3D kernels move their level fields (almost all of
+// their bytes) at half the size; the 2D sub-cycle kernels are unchanged.
+double kernel_bytes(const fesomc_model *m, const std::string &k) {
+    const double b = kernel_bytes_fp64(m, k);
+    if (!m->fp32) return b;
+    if (k == "ab3_elem" || k == "ssh_node" || k == "adv2d_edge" || k == "u2d_elem" || k == "rot_nodes" ||
+        k == "jac_swap")
+        return b;
+    return 0.5 * b;
+}
+
 // Runs fn() bracketed by profiling events when profiling is on.
 template <typename F>
 void rec(fesomc_model *m, const char *name, F fn) {
@@ -498,38 +615,45 @@ void rec(fesomc_model *m, const char *name, F fn) {
     P.used += 2;
 }
 
-// The kernel sequence of one internal step (oce_timestep case(3)).
+// The kernel sequence of one internal step (oce_timestep case(3)).  The 2D
+// sub-cycle kernels always run on the FP64 view; the 3D kernels on the view
+// of the model's form (K3).
 int enqueue_step(fesomc_model *m, double ff) {
     const Dev &d = m->d;
+    const fesomc::f32::Dev &q = m->d32;
+    const bool f = m->fp32;
     cudaStream_t s = m->stream;
     int n = 0;
-    rec(m, "pressure_col", [&] { launch_pressure_col(d, s); });
-    rec(m, "bpg_elem", [&] { launch_bpg_elem(d, s); });
+#define K3(fn, ...) (f ? fesomc::f32::fn(q, ##__VA_ARGS__) : fesomc::f64::fn(d, ##__VA_ARGS__))
+#define K3E2N(a, b, c, e) (f ? fesomc::f32::launch_el2nodes(q, q.a, q.b, q.c, q.e, s) \
+                             : fesomc::f64::launch_el2nodes(d, d.a, d.b, d.c, d.e, s))
+    rec(m, "pressure_col", [&] { K3(launch_pressure_col, s); });
+    rec(m, "bpg_elem", [&] { K3(launch_bpg_elem, s); });
     n += 2;
-    rec(m, "el2nodes", [&] { launch_el2nodes(d, d.U_n, d.V_n, d.Unode, d.Vnode, s); });
+    rec(m, "el2nodes", [&] { K3E2N(U_n, V_n, Unode, Vnode); });
     n += 1;
     if (d.ver_mix == 3) {
-        rec(m, "d3end", [&] { launch_d3end(d, s); });
-        rec(m, "av", [&] { launch_av(d, s); });
+        rec(m, "d3end", [&] { K3(launch_d3end, s); });
+        rec(m, "av", [&] { K3(launch_av, s); });
         n += 2;
     }
-    rec(m, "velgrad3d", [&] { launch_velgrad3d(d, s); });
+    rec(m, "velgrad3d", [&] { K3(launch_velgrad3d, s); });
     n += 1;
-    if (d.mom_adv_3D == 1) { rec(m, "adv3_edge", [&] { launch_adv3_edge(d, s); }); n += 1; }
-    rec(m, "velrhs", [&] { launch_velrhs(d, ff, s); });
+    if (d.mom_adv_3D == 1) { rec(m, "adv3_edge", [&] { K3(launch_adv3_edge, s); }); n += 1; }
+    rec(m, "velrhs", [&] { K3(launch_velrhs, ff, s); });
     n += 1;
-    if (d.im_vert_visc || d.im_vert_visc_fic) { rec(m, "implvisc", [&] { launch_implvisc(d, s); }); n += 1; }
-    rec(m, "zero_filt", [&] { launch_zero_filt(d, s); });
+    if (d.im_vert_visc || d.im_vert_visc_fic) { rec(m, "implvisc", [&] { K3(launch_implvisc, s); }); n += 1; }
+    rec(m, "zero_filt", [&] { K3(launch_zero_filt, s); });
     n += 1;
     for (int sub = 0; sub < d.Mt; ++sub) {
         rec(m, "ab3_elem", [&] { launch_ab3_elem(d, s); });
         rec(m, "ssh_node", [&] { launch_ssh_node(d, sub, s); });
         n += 2;
         if (sub == 0) {
-            rec(m, "puls_elem", [&] { launch_puls_elem(d, s); });
-            rec(m, "el2nodes_p", [&] { launch_el2nodes(d, d.U_puls, d.V_puls, d.Unode_p, d.Vnode_p, s); });
-            rec(m, "p1_edge", [&] { launch_p1_edge(d, s); });
-            rec(m, "p1_elem", [&] { launch_p1_elem(d, s); });
+            rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
+            rec(m, "el2nodes_p", [&] { K3E2N(U_puls, V_puls, Unode_p, Vnode_p); });
+            rec(m, "p1_edge", [&] { K3(launch_p1_edge, s); });
+            rec(m, "p1_elem", [&] { K3(launch_p1_elem, s); });
             n += 4;
         }
         if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { launch_adv2d_edge(d, s); }); n += 1; }
@@ -538,22 +662,24 @@ int enqueue_step(fesomc_model *m, double ff) {
         n += 2;
     }
     rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
-    rec(m, "update3d", [&] { launch_update3d(d, 1.0 / (double)d.Mt, s); });
-    rec(m, "wvel", [&] { launch_wvel(d, s); });
-    rec(m, "minmax", [&] { launch_minmax(d, s); });
+    rec(m, "update3d", [&] { K3(launch_update3d, 1.0 / (double)d.Mt, s); });
+    rec(m, "wvel", [&] { K3(launch_wvel, s); });
+    rec(m, "minmax", [&] { K3(launch_minmax, s); });
     n += 5;
-    if (d.tracer_adv != FESOMC_TRACER_MIURA) { rec(m, "ab2_node", [&] { launch_ab2(d, s); }); n += 1; }
-    if (d.tracer_adv == FESOMC_TRACER_MIURA) { rec(m, "miura", [&] { launch_miura(d, s); }); n += 5; }
+    if (d.tracer_adv != FESOMC_TRACER_MIURA) { rec(m, "ab2_node", [&] { K3(launch_ab2, s); }); n += 1; }
+    if (d.tracer_adv == FESOMC_TRACER_MIURA) { rec(m, "miura", [&] { K3(launch_miura, s); }); n += 5; }
     else if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
-        rec(m, "muscl_egrad", [&] { launch_muscl_egrad(d, s); });
-        rec(m, "muscl_ngrad", [&] { launch_muscl_ngrad(d, s); });
-        rec(m, "muscl_edge", [&] { launch_muscl_edge(d, s); });
-        rec(m, "muscl_h", [&] { launch_muscl_h(d, s); });
+        rec(m, "muscl_egrad", [&] { K3(launch_muscl_egrad, s); });
+        rec(m, "muscl_ngrad", [&] { K3(launch_muscl_ngrad, s); });
+        rec(m, "muscl_edge", [&] { K3(launch_muscl_edge, s); });
+        rec(m, "muscl_h", [&] { K3(launch_muscl_h, s); });
         n += 4;
     }
-    else { rec(m, "upwind_h", [&] { launch_upwind(d, s); }); n += 1; }
-    rec(m, "vdiff_col", [&] { launch_vdiff(d, s); });
+    else { rec(m, "upwind_h", [&] { K3(launch_upwind, s); }); n += 1; }
+    rec(m, "vdiff_col", [&] { K3(launch_vdiff, s); });
     n += 1;
+#undef K3E2N
+#undef K3
     m->launches_per_step = n;
     CK(cudaGetLastError());
     return FESOMC_OK;
@@ -673,11 +799,14 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (par->cl_solid_boder_relax) return FESOMC_EINVAL;
     if (par->mom_adv_2D != 2 && par->mom_adv_2D != 0) return FESOMC_EINVAL;
     if (par->mom_adv_3D != 1 && par->mom_adv_3D != 0) return FESOMC_EINVAL;
+    if (par->fp32_form != 0 && par->fp32_form != 1) return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;
     m->p = *par;
+    m->fp32 = par->fp32_form == 1;
     set_params(m->d, *par);
+    set_params(m->d32, *par);
     int rc = FESOMC_OK;
     auto fail = [&](int code) {
         fesomc_gpu_finalize(m);
@@ -685,9 +814,18 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     };
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(FESOMC_ECUDA);
     if ((rc = build_mesh(m, mesh))) return fail(rc);
+    if (m->fp32 && (rc = setup_f32_view(m))) return fail(rc);
     if ((rc = alloc_state(m))) return fail(rc);
+    if (m->fp32) share_2d(m);
     // kernels whose shared-memory scratch scales with the level count
-    if (config_d3end(m->d) || config_vdiff(m->d) || config_p1(m->d) || config_columns(m->d)) return fail(FESOMC_EINVAL);
+    if (m->fp32) {
+        const fesomc::f32::Dev &q = m->d32;
+        if (fesomc::f32::config_d3end(q) || fesomc::f32::config_vdiff(q) || fesomc::f32::config_p1(q) ||
+            fesomc::f32::config_columns(q))
+            return fail(FESOMC_EINVAL);
+    } else if (config_d3end(m->d) || config_vdiff(m->d) || config_p1(m->d) || config_columns(m->d)) {
+        return fail(FESOMC_EINVAL);
+    }
     const size_t nobn = (size_t)(mesh->nobn > 0 ? mesh->nobn : 0);
     m->ampt.assign(nobn * 12, 0.0);
     m->fazt.assign(nobn * 12, 0.0);
@@ -715,7 +853,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice) ||
         cudaMemcpy(m->d.eta_jac_old, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice))
         return fail(FESOMC_ECUDA);
-    launch_je(m->d, m->stream);
+    if (m->fp32) fesomc::f32::launch_je(m->d32, m->stream);
+    else launch_je(m->d, m->stream);
     if (cudaGetLastError() != cudaSuccess) return fail(FESOMC_ECUDA);
     m->lfirst = st->lfirst;
     m->time_jd = st->time_jd;
@@ -735,8 +874,12 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
     if (f->tauy) CK(cudaMemcpyAsync(d.tauy, f->tauy, E * 8, cudaMemcpyHostToDevice, s));
     if (f->windx) CK(cudaMemcpyAsync(d.windx, f->windx, N * 8, cudaMemcpyHostToDevice, s));
     if (f->windy) CK(cudaMemcpyAsync(d.windy, f->windy, N * 8, cudaMemcpyHostToDevice, s));
-    if (f->Tclim) CK(cudaMemcpyAsync(d.Tclim, f->Tclim, L * N * 8, cudaMemcpyHostToDevice, s));
-    if (f->Sclim) CK(cudaMemcpyAsync(d.Sclim, f->Sclim, L * N * 8, cudaMemcpyHostToDevice, s));
+    if (f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
+    int rc = FESOMC_OK;
+    if (f->Tclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Tclim : (void *)d.Tclim, m->fp32, L * N, f->Tclim)))
+        return rc;
+    if (f->Sclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Sclim : (void *)d.Sclim, m->fp32, L * N, f->Sclim)))
+        return rc;
     if (f->taux || f->tauy || f->windx || f->windy || f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
     if (f->runoff_rivers && d.n_rivers > 0) {
         std::memcpy(m->h_runoff, f->runoff_rivers, sizeof(double) * d.n_rivers);
@@ -773,7 +916,8 @@ int fesomc_gpu_sync_to_host(fesomc_model *m, uint32_t mask, fesomc_state *st) {
     CK(cudaStreamSynchronize(m->stream));
     for (const FieldRef &f : field_table(m)) {
         double *h = st->*(f.host);
-        if ((f.group & mask) && h) CK(cudaMemcpy(h, f.dev, f.count * sizeof(double), cudaMemcpyDeviceToHost));
+        int rc;
+        if ((f.group & mask) && h && (rc = field_to_host(m, f, h))) return rc;
     }
     st->lfirst = m->lfirst;
     st->time_jd = m->time_jd;
@@ -785,7 +929,8 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
     CK(cudaStreamSynchronize(m->stream));
     for (const FieldRef &f : field_table(m)) {
         const double *h = st->*(f.host);
-        if ((f.group & mask) && h) CK(cudaMemcpy(f.dev, h, f.count * sizeof(double), cudaMemcpyHostToDevice));
+        int rc;
+        if ((f.group & mask) && h && (rc = field_from_host(m, f.dev, f.f32, f.count, h))) return rc;
     }
     if (mask == FESOMC_F_ALL) {
         m->lfirst = st->lfirst;

@@ -145,6 +145,13 @@ typedef struct fesomc_params {
     int32_t temp_on, salinity_on; /* type_task 3 when either is set            */
     int32_t n_harm;               /* number of tidal harmonics in use (<=12)    */
     int32_t harm_index[12];       /* 0-based index into the 12 reference waves  */
+    /* Arithmetic form (no counterpart in the reference, which is FP64):
+     * 0 = plain FP64 (bit-exact with the reference algorithm);
+     * 1 = FP32 form: level fields, mesh geometry and the 3D arithmetic
+     *     (fluxes, advection, viscosity, tracers, mixing) in FP32; the
+     *     barotropic sub-cycle (SSH / total depth accumulation, wet/dry
+     *     tests) and the energy integral stay FP64.                        */
+    int32_t fp32_form;
 } fesomc_params;
 
 /*
