@@ -119,7 +119,7 @@ def workload_config(case, cfg):
     return {
         "workload": f"{cfg}: synthetic estuary {nx + 1}x{ny + 1} nodes ({case.meta['dx']:.0f} m), "
                     f"{m.NS} sigma levels, 30% quads split, MUSCL tracers, wetting/drying, "
-                    f"M2 open-boundary tide, river 500 m3/s, wind 0.1 N/m2; one step = one internal "
+                    f"M2 open-boundary tide, river 500 m3/s, cross-shore wind stress 0.1 N/m2; one step = one internal "
                     f"step (dt {case.params.dt:.0f} s) with {case.params.Mt} external sub-steps",
         "nodes": m.N, "elements": m.E, "edges": m.Ed, "levels": m.L,
         "dt_s": case.params.dt, "substeps": case.params.Mt,
@@ -305,6 +305,71 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+M2_PERIOD_S = 12.42 * 3600.0      # fv_var.F90:171
+TIDAL_DAY_S = 2.0 * M2_PERIOD_S    # two M2 periods
+
+
+def run_compare_forms(args):
+    """Chosen (FP32) form against the plain FP64 path on one GPU: both
+    models advance the same number of internal steps from the same state
+    (device-timed, forcing held), then the prognostic fields are compared.
+    Prints one JSON line with the wall time per simulated tidal day of each
+    form, their ratio, and the RMS / max differences."""
+    import numpy as np
+    from fesomc import abi, build, cases, model
+    if not os.path.exists(abi.LIB_PATH):
+        build.build_library()
+    lib = abi.load()
+    cfg = args.config
+    out = {}
+    states = {}
+    for form in (0, 1):
+        case = build_case(cfg)
+        case.params.fp32_form = form
+        g = model.GpuModel(case)
+        t_next = cases.advance_time(g.time_jd, case.params.dt)
+        g.set_forcing(case.forcing_fn(1, t_next))
+        ms = C.c_double()
+        abi.check(lib.fesomc_gpu_time_run(g.h, args.steps, C.byref(ms)), "fesomc_gpu_time_run")
+        st = g.state()
+        m = case.mesh
+        vol = float(np.sum(m.area * (m.depth + st["eta_n"])))
+        states[form] = (st, vol)
+        out[form] = ms.value / args.steps
+        dt = case.params.dt
+        wet = st["mask_wd_node"] > 0
+        g.close()
+    (a, va), (b, vb) = states[0], states[1]
+    wet = (a["mask_wd_node"] > 0) & (b["mask_wd_node"] > 0)
+
+    def rms(x):
+        return float(np.sqrt(np.mean(x * x)))
+
+    L = case.mesh.L
+    wetn = np.repeat(wet, L)
+    errors = {
+        "ssh_rms_m": rms(a["eta_n"][wet] - b["eta_n"][wet]),
+        "ssh_max_m": float(np.max(np.abs(a["eta_n"][wet] - b["eta_n"][wet]))),
+        "u_rms_m_s": rms(a["U_n"] - b["U_n"]), "u_max_m_s": float(np.max(np.abs(a["U_n"] - b["U_n"]))),
+        "v_rms_m_s": rms(a["V_n"] - b["V_n"]), "v_max_m_s": float(np.max(np.abs(a["V_n"] - b["V_n"]))),
+        "T_rms_C": rms(a["TF"][wetn] - b["TF"][wetn]), "T_max_C": float(np.max(np.abs(a["TF"][wetn] - b["TF"][wetn]))),
+        "S_rms_psu": rms(a["SF"][wetn] - b["SF"][wetn]),
+        "S_max_psu": float(np.max(np.abs(a["SF"][wetn] - b["SF"][wetn]))),
+        "volume_rel": abs(vb - va) / va,
+        "wet_nodes_differing": int(np.sum(a["mask_wd_node"] != b["mask_wd_node"])),
+    }
+    steps_per_day = TIDAL_DAY_S / dt
+    line = {
+        "metric": "chosen vs plain FP64 per simulated tidal day", "config": workload_config(case, cfg),
+        "steps": args.steps, "simulated_s": args.steps * dt, "m2_cycles": args.steps * dt / M2_PERIOD_S,
+        "plain_fp64": {"ms_per_step": out[0], "s_per_tidal_day": out[0] * steps_per_day / 1000.0},
+        "chosen_fp32": {"ms_per_step": out[1], "s_per_tidal_day": out[1] * steps_per_day / 1000.0},
+        "speedup": out[0] / out[1], "errors_vs_fp64": errors,
+        "notes": "device-timed graph replay, forcing of the first step held, both runs from the same initial state",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,10 +378,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--compare-forms", action="store_true",
+                    help="time the FP32 form against the plain FP64 path and report their differences")
     ap.add_argument("--fp32-form", action="store_true",
                     help="run the FP32 form (level fields and 3D arithmetic in FP32, 2D sub-cycle in FP64)")
     args = ap.parse_args()
     ws, rank, local = dist_info()
+    if args.compare_forms:
+        run_compare_forms(args)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
     else:

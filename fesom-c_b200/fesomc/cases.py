@@ -299,10 +299,14 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, **overrides)
     ampt[0, :] = 1.2                                      # M2 amplitude, m
     fazt = np.zeros((12, nobn))
     amp_factor, phy_factor = np.ones(12), np.zeros(12)
-    taux = np.full(E, tau)
-    tauy = np.zeros(E)
+    # uniform stress, cross-shore (+y, from the shore towards deep water); an
+    # along-channel stress towards the open boundary drives the shallow
+    # shore corner at the open boundary unstable in the reference scheme
+    # within a few hours of model time
+    taux = np.zeros(E)
+    tauy = np.full(E, tau)
     wspd = math.sqrt(tau / (1.3 * 1.3e-3)) if tau > 0 else 0.0
-    windx, windy = np.full(N, wspd), np.zeros(N)
+    windx, windy = np.zeros(N), np.full(N, wspd)
     nriv = mesh.c.n_rivers
     q_total = 500.0
 
