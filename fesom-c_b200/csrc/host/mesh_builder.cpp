@@ -18,6 +18,7 @@
 //   a_tp                 src/fv_ini.F90:94-107
 #include "fesomc_gpu.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -682,6 +683,49 @@ extern "C" int fesomc_mesh_set_rivers(fesomc_mesh_builder *b, int32_t n, const i
     for (int i = 0; i < n; ++i)
         if (nodes[i] < 1 || nodes[i] > b->nod2D) return FESOMC_EINVAL;
     b->nod_rivers.assign(nodes, nodes + n);
+    return FESOMC_OK;
+}
+
+// Sponge layer at the open boundary (ac_create_Xobn / ac_create /
+// Dist2in1, src/fv_utilit.F90:53-88,151-220): ac = distance to the nearest
+// open-boundary node / radius inside the radius, 1 elsewhere.  Open-boundary
+// nodes are those with index_nod2D = 2, in node order.
+extern "C" int fesomc_mesh_set_sponge(fesomc_mesh_builder *b, double radius) {
+    if (!b || !(radius > 0.0)) return FESOMC_EINVAL;
+    std::vector<double> x1, x2;
+    for (int n = 1; n <= b->nod2D; ++n)
+        if (b->index_nod2D[n - 1] == 2) {
+            x1.push_back(b->cx(n));
+            x2.push_back(b->cy(n));
+        }
+    b->ac.assign(b->nod2D, 1.0);
+    if (x1.empty()) return FESOMC_OK;
+    const size_t nob = x1.size();
+    for (int n = 1; n <= b->nod2D; ++n) {
+        const double X1 = b->cx(n), X2 = b->cy(n);
+        double d2obn;
+        if (b->cartesian) {
+            double d = (x1[0] - X1) * (x1[0] - X1) + (x2[0] - X2) * (x2[0] - X2);
+            for (size_t j = 1; j < nob; ++j) {
+                const double t = (x1[j] - X1) * (x1[j] - X1) + (x2[j] - X2) * (x2[j] - X2);
+                if (t < d) d = t;
+            }
+            d2obn = std::sqrt(d) * kREarth;
+        } else {
+            const double cos_X2 = std::cos(X2);
+            auto hav = [&](size_t j) {
+                const double s2 = std::sin((x2[j] - X2) * 0.5), s1 = std::sin((x1[j] - X1) * 0.5);
+                return s2 * s2 + cos_X2 * std::cos(x2[j]) * s1 * s1;
+            };
+            double a = hav(0);
+            for (size_t j = 1; j < nob; ++j) {
+                const double t = hav(j);
+                if (t < a) a = t;
+            }
+            d2obn = 2.0 * kREarth * std::asin(std::min(1.0, std::sqrt(a)));
+        }
+        if (d2obn < radius) b->ac[n - 1] = d2obn / radius;
+    }
     return FESOMC_OK;
 }
 

@@ -92,6 +92,7 @@ SIGNATURES = {
     "fesomc_mesh_view": (C.c_int, [C.c_void_p, C.POINTER(Mesh)]),
     "fesomc_mesh_scale_area": (C.c_double, [C.c_void_p]),
     "fesomc_mesh_set_rivers": (C.c_int, [C.c_void_p, C.c_int32, i32p]),
+    "fesomc_mesh_set_sponge": (C.c_int, [C.c_void_p, C.c_double]),
     "fesomc_mesh_free": (None, [C.c_void_p]),
     "fesomc_gpu_time_run": (C.c_int, [C.c_void_p, C.c_int32, f64p]),
     "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,

@@ -28,7 +28,7 @@ class HostMesh:
 
     def __init__(self, xy, index, elems, depth, *, cartesian, nsigma, coriolis_on=False, lat_deg=50.0,
                  ind_sigma=1, pow_sig=1.0, lev_bot=1.0, lev_sur=1.0, T_potential=False,
-                 with_up_dn_tri=True, rivers=None):
+                 with_up_dn_tri=True, rivers=None, sponge_radius=None):
         lib = abi.load()
         self.lib = lib
         xy = np.ascontiguousarray(xy, dtype=np.float64)
@@ -45,6 +45,8 @@ class HostMesh:
         if rivers is not None and len(rivers):
             r = np.ascontiguousarray(rivers, dtype=np.int32)
             abi.check(lib.fesomc_mesh_set_rivers(h, len(r), abi.iptr(r)), "fesomc_mesh_set_rivers")
+        if sponge_radius:
+            abi.check(lib.fesomc_mesh_set_sponge(h, float(sponge_radius)), "fesomc_mesh_set_sponge")
         self.c = abi.Mesh()
         abi.check(lib.fesomc_mesh_view(h, C.byref(self.c)), "fesomc_mesh_view")
         m = self.c
@@ -212,6 +214,11 @@ def le_medium(nsigma=40):
 # --------------------------------------------------------------------------
 # synthetic estuary
 # --------------------------------------------------------------------------
+# Sponge layer at the open boundary (SL_obn / SL_radius of fv_run.dat): the
+# clamped-elevation open boundary of the estuary grows spurious currents along
+# it within a few hours of model time without one.
+SPONGE_RADIUS = None
+
 ESTUARY_CFGS = {
     # name: (nx quads, ny quads, spacing m, nsigma, depth at y=0, depth at y=Ly, wind stress N/m2)
     "cfg0": (200, 80, 300.0, 11, 2.0, 25.0, 0.0),
@@ -270,12 +277,12 @@ def estuary_geometry(nx, ny, dx, seed=20261203, split_frac=0.3, h0=2.0, h1=25.0,
     return xy, index.ravel(), elems, depth, (nx + 1, ny + 1)
 
 
-def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, **overrides):
+def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS, **overrides):
     nx, ny, dx, nsigma, h0, h1, tau = ESTUARY_CFGS[cfg]
     xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1)
     rivers = np.arange(0, nyn) * nxn + 1                 # every node on x = 0 (1-based)
     mesh = HostMesh(xy, index, elems, depth, cartesian=True, nsigma=nsigma, coriolis_on=True,
-                    lat_deg=50.0, with_up_dn_tri=True, rivers=rivers)
+                    lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius)
     lib = abi.load()
     kw = dict(dt=20.0, dt_2D=2.0, Dmin=1.0, C_d=0.0025, tracer_adv=tracer_adv, wet_dry_on=1,
               key_rivers=1, TF_presence=1, temp_on=1, salinity_on=1, filt_2D=1, filt_3D=1,

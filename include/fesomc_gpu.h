@@ -254,6 +254,10 @@ int  fesomc_mesh_view(const fesomc_mesh_builder *b, fesomc_mesh *mesh);
 /* scale_area = sum(elem_area)/elem2D, sequential sum (fv_ini.F90:81). */
 double fesomc_mesh_scale_area(const fesomc_mesh_builder *b);
 int  fesomc_mesh_set_rivers(fesomc_mesh_builder *b, int32_t n, const int32_t *nodes);
+/* Sponge layer of radius (m) at the open boundary: ac_create
+ * (src/fv_utilit.F90:184-220, distance Dist2in1 :53-88), as the reference
+ * builds it when SL_obn is set (src/fv_main.F90:224-250). */
+int  fesomc_mesh_set_sponge(fesomc_mesh_builder *b, double radius);
 void fesomc_mesh_free(fesomc_mesh_builder *b);
 
 /* Jackett-McDougall density anomaly rho(t,s,pz) - density_0 on the host, as

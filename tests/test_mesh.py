@@ -58,6 +58,48 @@ def test_estuary_counts(built):
     assert (ud > 0).all(axis=1).mean() > 0.8
 
 
+def _sponge_restatement(m, radius, cartesian):
+    """ac_create / Dist2in1 (src/fv_utilit.F90:53-88,184-220) in numpy."""
+    p = m.coord_nod2D
+    ob = p[m.index_nod2D == 2]
+    r_earth = 6400000.0                                   # r_earth, src/fv_var.F90
+    if cartesian:
+        d = ((ob[None, :, 0] - p[:, None, 0]) ** 2 + (ob[None, :, 1] - p[:, None, 1]) ** 2).min(axis=1)
+        dist = np.sqrt(d) * r_earth
+    else:
+        a = (np.sin((ob[None, :, 1] - p[:, None, 1]) * 0.5) ** 2
+             + np.cos(p[:, None, 1]) * np.cos(ob[None, :, 1]) * np.sin((ob[None, :, 0] - p[:, None, 0]) * 0.5) ** 2)
+        dist = 2.0 * r_earth * np.arcsin(np.minimum(1.0, np.sqrt(a.min(axis=1))))
+    return np.where(dist < radius, dist / radius, 1.0)
+
+
+@pytest.mark.parametrize("cartesian", [True, False])
+def test_sponge_layer(built, cartesian):
+    from fesomc import cases
+    xy, idx, el, dep, (nxn, nyn) = cases.estuary_geometry(40, 16, 300.0)
+    if not cartesian:
+        xy = xy / 300.0 * 0.01 + np.array([5.0, 50.0])   # degrees, 0.01 degree spacing
+    radius = 2000.0
+    m = cases.HostMesh(xy, idx, el, dep, cartesian=cartesian, nsigma=5, with_up_dn_tri=False,
+                       sponge_radius=radius)
+    ac = m.ac
+    ob = m.index_nod2D == 2
+    assert ob.sum() == nyn
+    np.testing.assert_array_equal(ac[ob], 0.0)
+    assert ac.max() == 1.0 and 0.0 < ac[~ob].min() < 1.0
+    np.testing.assert_allclose(ac, _sponge_restatement(m, radius, cartesian), rtol=1e-13, atol=1e-15)
+    # without a sponge radius every node keeps the full terms
+    m0 = cases.HostMesh(xy, idx, el, dep, cartesian=cartesian, nsigma=5, with_up_dn_tri=False)
+    np.testing.assert_array_equal(m0.ac, 1.0)
+
+
+def test_sponge_rejects_bad_radius(built):
+    from fesomc import cases
+    xy, idx, el, dep, _ = cases.estuary_geometry(8, 4, 300.0)
+    with pytest.raises(RuntimeError, match="EINVAL"):
+        cases.HostMesh(xy, idx, el, dep, cartesian=True, nsigma=5, with_up_dn_tri=False, sponge_radius=-1.0)
+
+
 def test_orientation_fixed_and_bad_quad_rejected(built):
     from fesomc import cases
     xy = np.array([[0, 0], [1, 0], [1, 1], [0, 1], [2, 0], [2, 1]], float) * 100.0
