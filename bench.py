@@ -112,6 +112,11 @@ def build_case(cfg):
     return cases.estuary(cfg)
 
 
+def cases_sponge_km(case):
+    from fesomc import cases
+    return cases.SPONGE_RADIUS / 1000.0
+
+
 def workload_config(case, cfg):
     m = case.mesh
     state_gb = (m.N * m.L * 8 * 19 + m.E * m.L * 8 * 20 + m.N * m.NS * 8 * 7) / 1e9
@@ -119,7 +124,8 @@ def workload_config(case, cfg):
     return {
         "workload": f"{cfg}: synthetic estuary {nx + 1}x{ny + 1} nodes ({case.meta['dx']:.0f} m), "
                     f"{m.NS} sigma levels, 30% quads split, MUSCL tracers, wetting/drying, "
-                    f"M2 open-boundary tide, river 500 m3/s, cross-shore wind stress 0.1 N/m2; one step = one internal "
+                    f"M2 open-boundary tide, river 500 m3/s, cross-shore wind stress 0.1 N/m2, "
+                    f"{cases_sponge_km(case):.0f} km open-boundary sponge; one step = one internal "
                     f"step (dt {case.params.dt:.0f} s) with {case.params.Mt} external sub-steps",
         "nodes": m.N, "elements": m.E, "edges": m.Ed, "levels": m.L,
         "dt_s": case.params.dt, "substeps": case.params.Mt,

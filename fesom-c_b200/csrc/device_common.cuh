@@ -22,6 +22,12 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "fesomc_log.h"
+
+// FP32 form: the closure's logarithm is the device logf (the FP64 path uses
+// fesomc_log, bit-identical with the oracle's).
+static __device__ __forceinline__ float fesomc_log(float x) { return logf(x); }
+
 // Each kernel source is compiled twice: with FESOMC_FP32 = 0 into
 // fesomc::f64 (the FP64 path, bit-exact with the reference's algorithm) and
 // with FESOMC_FP32 = 1 into fesomc::f32 (the precision form: level fields,

@@ -100,7 +100,7 @@ __global__ void k_d3end(Dev d) {
         yy1[2] = y2;
         // bottom boundary value (independent of the iteration)
         const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
-        const real lg = log(delta_b / d.z0b_min);
+        const real lg = fesomc_log(delta_b / d.z0b_min);
         const real bott_R = B1cka2 / (lg * lg);
         const real ubt = Un[L - 1], vbt = Vn[L - 1];
         const real bot = bott_R * (ubt * ubt + vbt * vbt);

@@ -214,10 +214,18 @@ def le_medium(nsigma=40):
 # --------------------------------------------------------------------------
 # synthetic estuary
 # --------------------------------------------------------------------------
-# Sponge layer at the open boundary (SL_obn / SL_radius of fv_run.dat): the
-# clamped-elevation open boundary of the estuary grows spurious currents along
-# it within a few hours of model time without one.
-SPONGE_RADIUS = None
+# Open-boundary settings of the estuary, both run-file parameters of the
+# reference (fv_read_run.F90:877-898 and the SL_obn / SL_radius options).
+# Without them the 80 m estuary diverges within a few hours of model time:
+# an open-boundary node keeps its advective tracer tendency on inflow
+# (fv_tracer.F90:300-330) but gets no flux through the open edge itself, so
+# the tracer anomaly there grows exponentially (first at the shallow corner),
+# and currents along the clamped-elevation boundary grow next to the far
+# corner.  A relaxation to climatology on a 600 s time scale holds the
+# boundary tracers, and a 5 km sponge layer (ac scaling of advection and
+# viscosity, raised bottom drag) damps the boundary currents.
+SPONGE_RADIUS = 5000.0                                   # m
+OB_RELAX_S = 600.0                                       # clim_relax, relax2clim_ac time scale
 
 ESTUARY_CFGS = {
     # name: (nx quads, ny quads, spacing m, nsigma, depth at y=0, depth at y=Ly, wind stress N/m2)
@@ -286,7 +294,7 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
     lib = abi.load()
     kw = dict(dt=20.0, dt_2D=2.0, Dmin=1.0, C_d=0.0025, tracer_adv=tracer_adv, wet_dry_on=1,
               key_rivers=1, TF_presence=1, temp_on=1, salinity_on=1, filt_2D=1, filt_3D=1,
-              river_salinity=5.0)
+              river_salinity=5.0, clim_relax=1.0 / OB_RELAX_S, relax2clim_ac=1.0 / OB_RELAX_S)
     kw.update(overrides)
     p = default_params(**kw)
     p.n_harm = 1

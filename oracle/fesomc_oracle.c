@@ -12,6 +12,12 @@
  * (Fortran literals without _WP are REAL(4) constants promoted to REAL(8))
  * and its quirks.  Compile with -ffp-contract=off so no FMA is introduced.
  *
+ * One deliberate departure: the logarithm of the turbulence closure's bottom
+ * boundary value (fv_mixing.F90:238) is fesomc_log (an IEEE-only evaluation
+ * shared with the device kernels, within one ulp of the C library's log)
+ * rather than libm's log, so that the device path can be held to exact
+ * equality at every step count.
+ *
  * Parity pins: the mesh arrays it consumes are pinned against the
  * reference's edges.out / edge_tri.out (LE_medium test case); the whole time
  * step is pinned against the reference's energy_tocheck.dat series for the
@@ -28,6 +34,7 @@
 #include <string.h>
 
 #include "../include/fesomc_gpu.h"
+#include "../fesom-c_b200/csrc/fesomc_log.h"
 
 /* ---------------------------------------------------------------- consts */
 static const double WP_PI = 3.14159265358979;   /* fv_var.F90:8 */
@@ -135,6 +142,9 @@ static double densityJM(double t, double s, double pz, double density_0) {
                   + R4(4.8314e-4) * s * s;
     return rhopot * bulk / (bulk + 0.1 * pz) - density_0;
 }
+
+/* the shared logarithm, exported for its accuracy test */
+double oracle_log(double x) { return fesomc_log(x); }
 
 double oracle_densityJM(double t, double s, double pz, double density_0) {
     return densityJM(t, s, pz, density_0);
@@ -658,7 +668,9 @@ static void d3_end(oracle_model *m) {
                 yy1[nz + 1] = (am * yy1[nz] - fr) / a;
             }
             double delta_b = F3(m->Jc, NS - 1, node) + m->p.z0b_min;
-            double lg = log(delta_b / m->p.z0b_min);
+            /* dlog of fv_mixing.F90:238 through the shared IEEE-only log, so that
+               host and device agree bit for bit (within one ulp of libm's) */
+            double lg = fesomc_log(delta_b / m->p.z0b_min);
             double bott_R = B1cka2 / (lg * lg);
             double ub = F3(m->Unode, NS - 1, node), vb = F3(m->Vnode, NS - 1, node);
             btr1[NS] = bott_R * (ub * ub + vb * vb);

@@ -49,6 +49,8 @@ def load(abi):
         lib.oracle_T_aver.argtypes = [C.c_void_p]
         lib.oracle_densityJM.restype = C.c_double
         lib.oracle_densityJM.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
+        lib.oracle_log.restype = C.c_double
+        lib.oracle_log.argtypes = [C.c_double]
         _lib = lib
     return _lib
 

@@ -120,3 +120,26 @@ def test_estuary_oracle_low_temperature_flag(mods):
     rc = o.step(1)
     assert rc & abi.ST_LOWTEMP
     o.close()
+
+
+def test_shared_log_within_one_ulp_of_libm(mods):
+    """fesomc_log (the IEEE-only logarithm of d3_end's bottom boundary value,
+    shared by the oracle and the device kernels) against the C library's log:
+    at most one ulp apart, over the closure's argument range and beyond."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([np.exp(rng.uniform(-700.0, 700.0, 20000)),    # whole range
+                         1.0 + rng.uniform(-0.3, 0.3, 20000),          # near 1
+                         1.0 + rng.uniform(0.0, 2000.0, 20000),        # delta_b / z0b_min
+                         [1.0, 2.0, 0.5, 5e-324, 1e-310, 1.7976931348623157e308,
+                          np.nextafter(1.0, 2.0), np.nextafter(1.0, 0.0)]])
+    ours = np.array([lib.oracle_log(float(x)) for x in xs])
+    ref = np.array([math.log(float(x)) for x in xs])
+    ulps = np.abs(ours.view(np.int64) - ref.view(np.int64))
+    assert ulps.max() <= 1
+    assert np.mean(ulps != 0) < 0.01
+    assert lib.oracle_log(1.0) == 0.0
+    assert lib.oracle_log(0.0) == -math.inf
+    assert math.isnan(lib.oracle_log(-1.0)) and math.isnan(lib.oracle_log(math.nan))
+    assert lib.oracle_log(math.inf) == math.inf
