@@ -318,60 +318,142 @@ TIDAL_DAY_S = 2.0 * M2_PERIOD_S    # two M2 periods
 def run_compare_forms(args):
     """Chosen (FP32) form against the plain FP64 path on one GPU: both
     models advance the same number of internal steps from the same state
-    (device-timed, forcing held), then the prognostic fields are compared.
-    Prints one JSON line with the wall time per simulated tidal day of each
-    form, their ratio, and the RMS / max differences."""
+    (device-timed, forcing held), in chunks of --chunk steps; after each
+    chunk the prognostic fields are compared.  Prints one JSON line with the
+    wall time per simulated tidal day of each form, their ratio, the RMS /
+    max differences at the end and after every chunk."""
     import numpy as np
     from fesomc import abi, build, cases, model
     if not os.path.exists(abi.LIB_PATH):
         build.build_library()
     lib = abi.load()
     cfg = args.config
-    out = {}
-    states = {}
+    chunk = args.chunk if args.chunk > 0 else args.steps
+    models = []
     for form in (0, 1):
         case = build_case(cfg)
         case.params.fp32_form = form
         g = model.GpuModel(case)
         t_next = cases.advance_time(g.time_jd, case.params.dt)
         g.set_forcing(case.forcing_fn(1, t_next))
-        ms = C.c_double()
-        abi.check(lib.fesomc_gpu_time_run(g.h, args.steps, C.byref(ms)), "fesomc_gpu_time_run")
-        st = g.state()
-        m = case.mesh
-        vol = float(np.sum(m.area * (m.depth + st["eta_n"])))
-        states[form] = (st, vol)
-        out[form] = ms.value / args.steps
-        dt = case.params.dt
-        wet = st["mask_wd_node"] > 0
-        g.close()
-    (a, va), (b, vb) = states[0], states[1]
-    wet = (a["mask_wd_node"] > 0) & (b["mask_wd_node"] > 0)
+        models.append(g)
+    m = case.mesh
+    L = m.L
+    dt = case.params.dt
 
     def rms(x):
         return float(np.sqrt(np.mean(x * x)))
 
-    L = case.mesh.L
-    wetn = np.repeat(wet, L)
-    errors = {
-        "ssh_rms_m": rms(a["eta_n"][wet] - b["eta_n"][wet]),
-        "ssh_max_m": float(np.max(np.abs(a["eta_n"][wet] - b["eta_n"][wet]))),
-        "u_rms_m_s": rms(a["U_n"] - b["U_n"]), "u_max_m_s": float(np.max(np.abs(a["U_n"] - b["U_n"]))),
-        "v_rms_m_s": rms(a["V_n"] - b["V_n"]), "v_max_m_s": float(np.max(np.abs(a["V_n"] - b["V_n"]))),
-        "T_rms_C": rms(a["TF"][wetn] - b["TF"][wetn]), "T_max_C": float(np.max(np.abs(a["TF"][wetn] - b["TF"][wetn]))),
-        "S_rms_psu": rms(a["SF"][wetn] - b["SF"][wetn]),
-        "S_max_psu": float(np.max(np.abs(a["SF"][wetn] - b["SF"][wetn]))),
-        "volume_rel": abs(vb - va) / va,
-        "wet_nodes_differing": int(np.sum(a["mask_wd_node"] != b["mask_wd_node"])),
-    }
+    def compare():
+        (a, b) = (g.state() for g in models)
+        va, vb = (float(np.sum(m.area * (m.depth + s["eta_n"]))) for s in (a, b))
+        wet = (a["mask_wd_node"] > 0) & (b["mask_wd_node"] > 0)
+        wetn = np.repeat(wet, L)
+        return {
+            "ssh_rms_m": rms(a["eta_n"][wet] - b["eta_n"][wet]),
+            "ssh_max_m": float(np.max(np.abs(a["eta_n"][wet] - b["eta_n"][wet]))),
+            "u_rms_m_s": rms(a["U_n"] - b["U_n"]), "u_max_m_s": float(np.max(np.abs(a["U_n"] - b["U_n"]))),
+            "v_rms_m_s": rms(a["V_n"] - b["V_n"]), "v_max_m_s": float(np.max(np.abs(a["V_n"] - b["V_n"]))),
+            "T_rms_C": rms(a["TF"][wetn] - b["TF"][wetn]),
+            "T_max_C": float(np.max(np.abs(a["TF"][wetn] - b["TF"][wetn]))),
+            "S_rms_psu": rms(a["SF"][wetn] - b["SF"][wetn]),
+            "S_max_psu": float(np.max(np.abs(a["SF"][wetn] - b["SF"][wetn]))),
+            "volume_rel": abs(vb - va) / va,
+            "wet_nodes_differing": int(np.sum(a["mask_wd_node"] != b["mask_wd_node"])),
+        }
+
+    total_ms = [0.0, 0.0]
+    done = 0
+    per_chunk = []
+    failure = None
+    while done < args.steps and failure is None:
+        n = min(chunk, args.steps - done)
+        for form, g in enumerate(models):
+            ms = C.c_double()
+            rc = lib.fesomc_gpu_time_run(g.h, n, C.byref(ms))
+            if rc != abi.FESOMC_OK:
+                failure = f"form {form} stopped with {abi.ERRORS.get(rc, rc)} in steps {done + 1}-{done + n}"
+                break
+            total_ms[form] += ms.value
+        if failure is None:
+            done += n
+            e = compare()
+            per_chunk.append({"steps": done, "ssh_rms_m": e["ssh_rms_m"], "T_max_C": e["T_max_C"],
+                              "S_max_psu": e["S_max_psu"], "u_max_m_s": e["u_max_m_s"]})
+    errors = compare() if failure is None else None
+    for g in models:
+        g.close()
     steps_per_day = TIDAL_DAY_S / dt
+    ms0, ms1 = (t / max(done, 1) for t in total_ms)
     line = {
         "metric": "chosen vs plain FP64 per simulated tidal day", "config": workload_config(case, cfg),
-        "steps": args.steps, "simulated_s": args.steps * dt, "m2_cycles": args.steps * dt / M2_PERIOD_S,
-        "plain_fp64": {"ms_per_step": out[0], "s_per_tidal_day": out[0] * steps_per_day / 1000.0},
-        "chosen_fp32": {"ms_per_step": out[1], "s_per_tidal_day": out[1] * steps_per_day / 1000.0},
-        "speedup": out[0] / out[1], "errors_vs_fp64": errors,
+        "steps": done, "simulated_s": done * dt, "m2_cycles": done * dt / M2_PERIOD_S,
+        "plain_fp64": {"ms_per_step": ms0, "s_per_tidal_day": ms0 * steps_per_day / 1000.0},
+        "chosen_fp32": {"ms_per_step": ms1, "s_per_tidal_day": ms1 * steps_per_day / 1000.0},
+        "speedup": ms0 / ms1 if ms1 > 0 else None, "errors_vs_fp64": errors, "per_chunk": per_chunk,
         "notes": "device-timed graph replay, forcing of the first step held, both runs from the same initial state",
+    }
+    if failure:
+        line["failure"] = failure
+    print(json.dumps(line), flush=True)
+
+
+def run_ensemble(args, ws, rank, local):
+    """Perturbed estuary ensemble (--ensemble M members, FP32 form unless
+    --fp64): each rank takes its longest-processing-time share of the
+    members, advances them concurrently (fesomc_ensemble_run) for --steps
+    internal steps after --warmup, then the same steps member after member.
+    Prints one JSON line: aggregate node-level updates/s of both ways (max
+    device time over ranks) and their ratio."""
+    from fesomc import abi, build, cases, ensemble, replicas
+    if not os.path.exists(abi.LIB_PATH):
+        build.build_library()
+    lib = abi.load()
+    if ws > 1:
+        import torch
+        torch.cuda.set_device(local)
+    reps = replicas.Replicas(ws, "nccl")
+    abi.check(lib.fesomc_gpu_set_device(local), "fesomc_gpu_set_device")
+    draws = [cases.ensemble_draw(i) for i in range(args.ensemble)]
+    costs = [(d["nx"] + 1) * (d["ny"] + 1) * (d["nsigma"] - 1) for d in draws]
+    mine = ensemble.lpt_partition(costs, ws)[rank]
+    members = []
+    for i in mine:
+        c = cases.ensemble_member(i)
+        c.params.fp32_form = 0 if args.fp64 else 1
+        members.append(c)
+    ens = ensemble.Ensemble(members)
+    ens.run(args.warmup)
+    reps.barrier()
+    ms_conc, st_conc = ens.run(args.steps, timed=True)
+    t_conc = reps.max(ms_conc / 1000.0)
+    reps.barrier()
+    ms_seq, st_seq = ens.run_one_at_a_time(args.steps)
+    t_seq = reps.max(ms_seq / 1000.0)
+    ens.close()
+    reps.close()
+    ok = all(s == 0 for s in st_conc + st_seq)
+    total_units = sum(costs)                     # all members, all ranks
+    if rank != 0:
+        return
+    conc = total_units * args.steps / t_conc
+    seq = total_units * args.steps / t_seq
+    sizes = [(d["nx"] + 1) * (d["ny"] + 1) for d in draws]
+    line = {
+        "metric": "aggregate node\u00b7level updates/s, ensemble", "unit": "node-level updates/s",
+        "value": conc, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t_conc / args.steps, "higher_is_better": True, "scaling": "strong",
+        "dtype": "f64" if args.fp64 else "f32 (2D sub-cycle f64)", "data": "synthetic",
+        "config": {"workload": f"{args.ensemble} perturbed estuary members (cfg0 generator, 300 m), "
+                               f"{min(sizes)}-{max(sizes)} nodes, 11/21 sigma levels, M2 amplitude +-20 %, "
+                               f"phase +-15 deg, stress 0-0.2 N/m2 in random directions, noise 0-1 m",
+                   "members": args.ensemble, "nodes_total": sum(sizes), "node_levels_per_step": total_units,
+                   "this_rank_members": len(mine), "parallelism": f"LPT share of members per GPU ({ws})"},
+        "one_at_a_time": {"value": seq, "ms_per_step": 1000.0 * t_seq / args.steps},
+        "concurrent_over_one_at_a_time": conc / seq if seq > 0 else None,
+        "all_members_ok": ok,
+        "notes": "members on their own streams and step graphs, one step of every member per round; "
+                 "forcing of the first step held",
     }
     print(json.dumps(line), flush=True)
 
@@ -383,7 +465,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1")
+    ap.add_argument("--chunk", type=int, default=0, help="--compare-forms: steps between comparisons")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble", type=int, default=0, help="run the perturbed estuary ensemble of this many members")
+    ap.add_argument("--fp64", action="store_true", help="--ensemble: members in the plain FP64 path")
     ap.add_argument("--compare-forms", action="store_true",
                     help="time the FP32 form against the plain FP64 path and report their differences")
     ap.add_argument("--fp32-form", action="store_true",
@@ -392,6 +477,10 @@ def main():
     ws, rank, local = dist_info()
     if args.compare_forms:
         run_compare_forms(args)
+        return
+    if args.ensemble > 0:
+        ws, rank, local = dist_info()
+        run_ensemble(args, ws, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)

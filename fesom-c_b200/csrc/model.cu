@@ -1047,6 +1047,70 @@ int fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, int
     return status_code(m->status_acc);
 }
 
+int fesomc_ensemble_run(fesomc_model *const *members, int32_t n, int32_t nsteps, double *ms, int32_t *status) {
+    if (!members || n <= 0 || nsteps < 0) return FESOMC_EINVAL;
+    for (int i = 0; i < n; ++i) {
+        if (!members[i]) return FESOMC_EINVAL;
+        for (int j = 0; j < i; ++j)
+            if (members[j] == members[i]) return FESOMC_EINVAL;
+    }
+    cudaEvent_t fork = nullptr, join = nullptr;
+    std::vector<cudaEvent_t> done;
+    auto release = [&] {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        for (cudaEvent_t e : done) cudaEventDestroy(e);
+    };
+    cudaStream_t s0 = members[0]->stream;
+    if (ms) {
+        // start from idle streams, then fork every member stream from s0
+        for (int i = 0; i < n; ++i) CK(cudaStreamSynchronize(members[i]->stream));
+        if (cudaEventCreate(&fork) != cudaSuccess || cudaEventCreate(&join) != cudaSuccess) {
+            release();
+            return FESOMC_ECUDA;
+        }
+        done.assign(n, nullptr);
+        for (int i = 1; i < n; ++i)
+            if (cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming) != cudaSuccess) {
+                release();
+                return FESOMC_ECUDA;
+            }
+        CK(cudaEventRecord(fork, s0));
+        for (int i = 1; i < n; ++i) CK(cudaStreamWaitEvent(members[i]->stream, fork, 0));
+    }
+    // one internal step of every member per round: no member's host-side
+    // staging wait holds back the others' enqueues
+    for (int k = 0; k < nsteps; ++k)
+        for (int i = 0; i < n; ++i) {
+            const int rc = run_steps(members[i], 1);
+            if (rc) {
+                release();
+                return rc;
+            }
+        }
+    if (ms) {
+        for (int i = 1; i < n; ++i) {
+            CK(cudaEventRecord(done[i], members[i]->stream));
+            CK(cudaStreamWaitEvent(s0, done[i], 0));
+        }
+        CK(cudaEventRecord(join, s0));
+        CK(cudaEventSynchronize(join));
+        float f = 0.f;
+        CK(cudaEventElapsedTime(&f, fork, join));
+        *ms = f;
+    }
+    release();
+    int first = FESOMC_OK;
+    for (int i = 0; i < n; ++i) {
+        int rc = collect_status(members[i]);
+        if (rc) return rc;
+        rc = status_code(members[i]->status_acc);
+        if (status) status[i] = rc;
+        if (first == FESOMC_OK) first = rc;
+    }
+    return first;
+}
+
 int fesomc_gpu_set_device(int32_t device) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) return FESOMC_ECUDA;

@@ -97,6 +97,7 @@ SIGNATURES = {
     "fesomc_gpu_time_run": (C.c_int, [C.c_void_p, C.c_int32, f64p]),
     "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,
                                      C.POINTER(C.c_int64)]),
+    "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),
     "fesomc_gpu_set_device": (C.c_int, [C.c_int32]),
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),

@@ -286,8 +286,26 @@ def estuary_geometry(nx, ny, dx, seed=20261203, split_frac=0.3, h0=2.0, h1=25.0,
 
 
 def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS, **overrides):
+    """One of the named estuary configurations (ESTUARY_CFGS)."""
     nx, ny, dx, nsigma, h0, h1, tau = ESTUARY_CFGS[cfg]
-    xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1)
+    # uniform stress, cross-shore (+y, from the shore towards deep water); an
+    # along-channel stress towards the open boundary drives the shallow
+    # shore corner at the open boundary unstable in the reference scheme
+    # within a few hours of model time
+    return estuary_case(cfg, nx, ny, dx, nsigma, h0, h1, stress=(0.0, tau), seed=seed, tracer_adv=tracer_adv,
+                        sponge_radius=sponge_radius, **overrides)
+
+
+def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=1.2, m2_phase_deg=0.0,
+                 noise_sigma=0.5, seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS,
+                 **overrides):
+    """Synthetic estuary: nx x ny quads at dx metres, 30 % split into
+    triangles, depth h0 -> h1 across the channel plus smoothed noise of
+    noise_sigma metres, river at x = 0, M2 tide of m2_amp metres and phase
+    m2_phase_deg at the open boundary x = nx*dx, uniform wind stress
+    (taux, tauy) in N/m2.  Parameter overrides go to default_params."""
+    xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1,
+                                                            noise_sigma=noise_sigma)
     rivers = np.arange(0, nyn) * nxn + 1                 # every node on x = 0 (1-based)
     mesh = HostMesh(xy, index, elems, depth, cartesian=True, nsigma=nsigma, coriolis_on=True,
                     lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius)
@@ -311,17 +329,18 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
     st = initial_state(mesh, p, TF, SF, wet_dry_on=bool(p.wet_dry_on))
     nobn = mesh.c.nobn
     ampt = np.zeros((12, nobn))
-    ampt[0, :] = 1.2                                      # M2 amplitude, m
+    ampt[0, :] = m2_amp                                   # M2 amplitude, m
     fazt = np.zeros((12, nobn))
+    fazt[0, :] = m2_phase_deg * (math.pi / 180.0)         # radians, as the OB harmonics take it
     amp_factor, phy_factor = np.ones(12), np.zeros(12)
-    # uniform stress, cross-shore (+y, from the shore towards deep water); an
-    # along-channel stress towards the open boundary drives the shallow
-    # shore corner at the open boundary unstable in the reference scheme
-    # within a few hours of model time
-    taux = np.zeros(E)
-    tauy = np.full(E, tau)
+    sx, sy = stress
+    tau = math.hypot(sx, sy)
+    taux, tauy = np.full(E, float(sx)), np.full(E, float(sy))
+    # 10 m wind speed of the stress (rho_air 1.3, C_D 1.3e-3) for the surface
+    # TKE flux, in the direction of the stress
     wspd = math.sqrt(tau / (1.3 * 1.3e-3)) if tau > 0 else 0.0
-    windx, windy = np.zeros(N), np.full(N, wspd)
+    windx = np.full(N, wspd * (sx / tau) if tau > 0 else 0.0)
+    windy = np.full(N, wspd * (sy / tau) if tau > 0 else 0.0)
     nriv = mesh.c.n_rivers
     q_total = 500.0
 
@@ -334,7 +353,46 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
                 "ampt": ampt.reshape(-1).copy(), "fazt": fazt.reshape(-1).copy(),
                 "amp_factor": amp_factor, "phy_factor": phy_factor}
 
-    return Case(cfg, mesh, p, st, forcing, meta={"nx": nx, "ny": ny, "dx": dx})
+    meta = {"nx": nx, "ny": ny, "dx": dx, "stress": (float(sx), float(sy)), "m2_amp": m2_amp,
+            "m2_phase_deg": m2_phase_deg, "noise_sigma": noise_sigma}
+    return Case(name, mesh, p, st, forcing, meta=meta)
+
+
+# --------------------------------------------------------------------------
+# perturbed estuary ensemble
+# --------------------------------------------------------------------------
+ENSEMBLE_NODES = (20_000, 250_000)
+
+
+def ensemble_draw(index, seed=20261203, nodes_range=ENSEMBLE_NODES):
+    """Parameters of ensemble member `index`: the cfg0 generator (300 m
+    quads, 30 % split, depth 2 -> 25 m, aspect of the 200 x 80 grid) at a
+    node count drawn log-uniformly in nodes_range, 11 or 21 sigma levels, M2
+    amplitude 1.2 m +-20 %, phase +-15 degrees, uniform stress 0-0.2 N/m2 in
+    a random direction, bathymetry noise sigma 0-1 m.  Each member draws
+    from its own generator seeded by (seed, index)."""
+    rng = np.random.default_rng([seed, index])
+    lo, hi = nodes_range
+    nodes = math.exp(rng.uniform(math.log(lo), math.log(hi)))
+    ny1 = max(9, int(round(math.sqrt(nodes * 81.0 / 201.0))))
+    nx1 = max(9, int(round(nodes / ny1)))
+    nsigma = 11 if rng.random() < 0.5 else 21
+    amp = 1.2 * (1.0 + rng.uniform(-0.2, 0.2))
+    phase = rng.uniform(-15.0, 15.0)
+    tau = rng.uniform(0.0, 0.2)
+    th = rng.uniform(0.0, 2.0 * math.pi)
+    noise = rng.uniform(0.0, 1.0)
+    return {"nx": nx1 - 1, "ny": ny1 - 1, "nsigma": nsigma, "m2_amp": amp, "m2_phase_deg": phase,
+            "stress": (tau * math.cos(th), tau * math.sin(th)), "noise_sigma": noise,
+            "seed": seed + 7919 * (index + 1)}
+
+
+def ensemble_member(index, seed=20261203, nodes_range=ENSEMBLE_NODES, **overrides):
+    """Case of ensemble member `index` (ensemble_draw)."""
+    d = ensemble_draw(index, seed, nodes_range)
+    return estuary_case(f"member{index}", d["nx"], d["ny"], 300.0, d["nsigma"], 2.0, 25.0, stress=d["stress"],
+                        m2_amp=d["m2_amp"], m2_phase_deg=d["m2_phase_deg"], noise_sigma=d["noise_sigma"],
+                        seed=d["seed"], **overrides)
 
 
 def forcing_struct(fdict):

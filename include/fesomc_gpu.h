@@ -278,6 +278,21 @@ int  fesomc_gpu_time_run(fesomc_model *m, int32_t nsteps, double *ms);
 int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, int32_t *n_kernels,
                         char *names, double *ms_per_launch, double *bytes_per_launch, int64_t *launches);
 
+/* Ensemble: advances n_members independent model instances (meshes of any
+ * size, either precision form) by nsteps internal steps each, concurrently
+ * on one GPU.  Every member keeps its own stream and its own captured step
+ * graph; the call interleaves the members' steps (member order as given,
+ * largest first is best), then waits for all.  status[i] (may be NULL)
+ * receives member i's step status (FESOMC_OK, FESOMC_ENEGSALT, ...); the
+ * return value is the first non-OK member status, or a call error.  With
+ * ms != NULL the device time from the first enqueued step to the last
+ * finished one is measured with CUDA events (fork / join across the
+ * member streams).  Members must live on the current device and must not
+ * be used by another thread during the call.  No counterpart in the
+ * reference, which runs one mesh per executable. */
+int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_t nsteps, double *ms,
+                         int32_t *status);
+
 /* Selects the CUDA device used by subsequent fesomc_gpu_init calls of the
  * calling thread (one process per GPU).  No counterpart in the reference,
  * where each MPI rank owns a mesh partition instead. */
