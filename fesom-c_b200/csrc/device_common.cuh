@@ -41,6 +41,19 @@ namespace fesomc {
 
 constexpr double kG64 = 9.8;
 
+// Raises (never lowers) a kernel's dynamic shared-memory limit.  The
+// attribute belongs to the kernel, and every model instance of the process
+// (ensemble members of different level counts, both precision forms)
+// launches the same kernels, so one instance must not shrink another's.
+template <typename K>
+inline cudaError_t raise_smem_limit(K kernel, size_t bytes) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, kernel);
+    if (e != cudaSuccess) return e;
+    if (bytes <= (size_t)a.maxDynamicSharedSizeBytes) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // ---- max/min exactly as the Fortran MAX/MIN of two values -------------------
 template <typename T>
 __device__ __forceinline__ T dmax(T a, T b) { return a > b ? a : b; }

@@ -114,6 +114,15 @@ __global__ void k_bpg_elem(Dev d) {
             d.Bar_prv[(size_t)e * L + z] = bv;
             sm[cb.jl * S + z] = bu * je;
             sm[cb.jl * S + L + z] = bv * je;
+            // surface pressure force of the element (independent of the
+            // level sums): in this phase, off the serial path
+            if (z == 0) {
+                real pr[4];
+                for (int k = 0; k < 4; ++k)
+                    pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+                const real ar = d.elem_area[e];
+                d.Fp[e] = make_real2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
+            }
         }
         __syncthreads();
         const long long es = eb + threadIdx.x;
@@ -126,14 +135,6 @@ __global__ void k_bpg_elem(Dev d) {
                 b2 = b2 + row[L + k];
             }
             d.Bar_pr_2D[e] = make_double2(b1, b2);
-            const int4 en = d.elem_nodes[e];
-            const int nd[4] = {en.x, en.y, en.z, en.w};
-            const real4 gx = d.gs_x[e], gy = d.gs_y[e];
-            real pr[4];
-            for (int k = 0; k < 4; ++k)
-                pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
-            const real ar = d.elem_area[e];
-            d.Fp[e] = make_real2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
         }
         __syncthreads();
     }
@@ -280,17 +281,21 @@ __global__ void k_adv3_edge(Dev d) {
 
 // ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
-// level) with levels on consecutive lanes.  The loop runs over whole warps so
-// that the vertical flux at interface z+1 comes from the next lane.
+// level) with levels on consecutive threads.  The loop runs over whole
+// blocks; each thread computes the vertical flux at its interface z, and the
+// flux at z+1 comes from the next thread through shared memory (only the
+// block's last thread computes it itself).
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, real ff) {
+constexpr int kVelrhsBlock = 256;
+__global__ void __launch_bounds__(kVelrhsBlock, 3) k_velrhs(Dev d, real ff) {
+    __shared__ real s_fu[kVelrhsBlock], s_fv[kVelrhsBlock];
     const long long total = (long long)d.E * d.L;
-    const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
-        const bool valid = wbase + lane < total;
-        const long long ii = valid ? wbase + lane : total - 1;
+    const int t = (int)threadIdx.x;
+    const long long stride = (long long)gridDim.x * kVelrhsBlock;
+    for (long long bbase = (long long)blockIdx.x * kVelrhsBlock; bbase < total; bbase += stride) {
+        const bool valid = bbase + t < total;
+        const long long ii = valid ? bbase + t : total - 1;
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
@@ -340,9 +345,14 @@ __global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, real ff) {
         if (d.vert_adv == 1) {
             real fu0, fv0;
             uvert_at(d, e, z, w, en, ar, fu0, fv0);
-            real fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
+            s_fu[t] = fu0;
+            s_fv[t] = fv0;
+            __syncthreads();
+            real fu1, fv1;
             if (z == L - 1) { fu1 = real(0.0); fv1 = real(0.0); }
-            else if (lane == 31) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
+            else if (t == kVelrhsBlock - 1) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
+            else { fu1 = s_fu[t + 1]; fv1 = s_fv[t + 1]; }
+            __syncthreads();
             if (mwd != real(0.0)) {
                 const real acc = d.elem_acc[e];
                 uab = uab + (fu0 - fu1) * acc;
@@ -494,13 +504,14 @@ __global__ void k_je_elem(Dev d) {
 // per element.  Runs right after the jacobian call: the stored Je still holds
 // the previous jacobian (Jc_old), and is replaced here by the new Je / Ze /
 // ZBe.
+constexpr int kU3Sc = 14;  // per element: U2p, V2p, uf, vf, w_cv(4), a(4), U_n_2D(2)
 __global__ void k_update3d(Dev d, real Mt_inv) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L;
     const ColBlock cb(L);
     const int S = 2 * L + 1;
-    real *sc = sm + (size_t)cb.B * S;  // 4 scalars per element
+    real *sc = sm + (size_t)cb.B * S;  // kU3Sc scalars per element
     for (long long eb = (long long)blockIdx.x * cb.B; eb < d.E; eb += (long long)gridDim.x * cb.B) {
         const long long e_ = eb + cb.jl;
         const bool act = cb.jl < cb.B && e_ < d.E;
@@ -512,47 +523,55 @@ __global__ void k_update3d(Dev d, real Mt_inv) {
             vr = d.V_rhs[i];
             sm[cb.jl * S + cb.z] = ur * a_old;
             sm[cb.jl * S + L + cb.z] = vr * a_old;
+            // the element's scalars, here rather than in the serial sum or
+            // the level loop, so that both read shared memory only
+            if (cb.z == 0) {
+                const int e = (int)e_;
+                const int4 en = d.elem_nodes[e];
+                const real4 w = d.w_cv[e];
+                const real dmean_inv = real(1.0) / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
+                                                                d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
+                const real uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
+                const real vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
+                d.U_filt_2D[e] = uf;
+                d.V_filt_2D[e] = vf;
+                const real4 an = elem_jac_a(d, d.eta_jac, en);
+                const double2 u2d = d.U_n_2D[e];
+                real *o = sc + kU3Sc * cb.jl;
+                o[0] = dmean_inv;
+                o[2] = uf; o[3] = vf;
+                o[4] = w.x; o[5] = w.y; o[6] = w.z; o[7] = w.w;
+                o[8] = an.x; o[9] = an.y; o[10] = an.z; o[11] = an.w;
+                o[12] = (real)u2d.x; o[13] = (real)u2d.y;
+            }
         }
         __syncthreads();
         const long long es = eb + threadIdx.x;
         if ((int)threadIdx.x < cb.B && es < d.E) {
-            const int e = (int)es;
             const real *row = sm + threadIdx.x * S;
             real su = real(0.0), sv = real(0.0);
             for (int k = 0; k < L; ++k) {
                 su = su + row[k];
                 sv = sv + row[L + k];
             }
-            const int4 en = d.elem_nodes[e];
-            const real4 w = d.w_cv[e];
-            const real dmean_inv = real(1.0) / dmax(d.Dmin, wsum(w, d.depth[en.x] + d.eta_n[en.x], d.depth[en.y] + d.eta_n[en.y],
-                                                            d.depth[en.z] + d.eta_n[en.z], d.depth[en.w] + d.eta_n[en.w]));
-            const real uf = (d.U_filt_2D[e] * Mt_inv) * dmean_inv;
-            const real vf = (d.V_filt_2D[e] * Mt_inv) * dmean_inv;
-            d.U_filt_2D[e] = uf;
-            d.V_filt_2D[e] = vf;
-            real *o = sc + 4 * threadIdx.x;
+            real *o = sc + kU3Sc * threadIdx.x;
+            const real dmean_inv = o[0];
             o[0] = su * dmean_inv;
             o[1] = sv * dmean_inv;
-            o[2] = uf;
-            o[3] = vf;
         }
         __syncthreads();
         if (act) {
-            const int e = (int)e_, z = cb.z;
-            const real *o = sc + 4 * cb.jl;
+            const int z = cb.z;
+            const real *o = sc + kU3Sc * cb.jl;
             const real U2p = o[0], V2p = o[1], uf = o[2], vf = o[3];
-            const int4 en = d.elem_nodes[e];
-            const real4 w = d.w_cv[e];
-            const real4 an = elem_jac_a(d, d.eta_jac, en);
-            const double2 u2d = d.U_n_2D[e];
-            const real2 u2 = make_real2((real)u2d.x, (real)u2d.y);
+            const real4 w = make_real4(o[4], o[5], o[6], o[7]);
+            const real4 an = make_real4(o[8], o[9], o[10], o[11]);
             const real jn = je_of(d, w, an, z);
             const real az = a_old / jn;
             d.U_n_filt[i] = az * ur + uf - U2p;
             d.V_n_filt[i] = az * vr + vf - V2p;
-            d.U_n[i] = az * ur + u2.x - U2p;
-            d.V_n[i] = az * vr + u2.y - V2p;
+            d.U_n[i] = az * ur + o[12] - U2p;
+            d.V_n[i] = az * vr + o[13] - V2p;
             d.Je[i] = jn;
             d.Ze[i] = wsum_z(d, w, an, z);
             d.ZBe[i] = wsum_zbar(d, w, an, z);
@@ -570,11 +589,16 @@ __global__ void k_wvel(Dev d) {
     const int L = d.L, NS = d.NS;
     const ColBlock cb(L);
     const int S = L | 1;
+    real *sc = sm + (size_t)cb.B * S;  // per node: bottom Wvel, 1/area
     for (long long nb = (long long)blockIdx.x * cb.B; nb < d.N; nb += (long long)gridDim.x * cb.B) {
         const long long n_ = nb + cb.jl;
         const bool act = cb.jl < cb.B && n_ < d.N;
         if (act) {
             const int n = (int)n_, z = cb.z;
+            if (z == 0) {
+                sc[2 * cb.jl] = d.Wvel[(size_t)n * NS + NS - 1];
+                sc[2 * cb.jl + 1] = real(1.0) / d.area[n];
+            }
             const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
             real W = real(0.0);
 #pragma unroll 4
@@ -600,14 +624,14 @@ __global__ void k_wvel(Dev d) {
         const long long ns = nb + threadIdx.x;
         if ((int)threadIdx.x < cb.B && ns < d.N) {
             real *row = sm + threadIdx.x * S;
-            real below = d.Wvel[(size_t)ns * NS + NS - 1];
+            real below = sc[2 * threadIdx.x];
             for (int k = L - 1; k >= 0; --k) {
                 below = row[k] + below;
                 row[k] = below;
             }
         }
         __syncthreads();
-        if (act) d.Wvel[(size_t)n_ * NS + cb.z] = sm[cb.jl * S + cb.z] * (real(1.0) / d.area[n_]);
+        if (act) d.Wvel[(size_t)n_ * NS + cb.z] = sm[cb.jl * S + cb.z] * sc[2 * cb.jl + 1];
         __syncthreads();
     }
 }
@@ -624,11 +648,11 @@ static size_t col_smem(const Dev &d, int rows, int scalars) {
     return ((size_t)col_b(d) * S + (size_t)col_b(d) * scalars) * sizeof(real);
 }
 int config_columns(const Dev &d) {
-    const size_t big = col_smem(d, 2, 4);
-    cudaError_t e = cudaFuncSetAttribute(k_bpg_elem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update3d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_pressure_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_wvel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+    const size_t big = col_smem(d, 2, kU3Sc);
+    cudaError_t e = raise_smem_limit(k_bpg_elem, big);
+    if (e == cudaSuccess) e = raise_smem_limit(k_update3d, big);
+    if (e == cudaSuccess) e = raise_smem_limit(k_pressure_col, big);
+    if (e == cudaSuccess) e = raise_smem_limit(k_wvel, big);
     return e == cudaSuccess ? 0 : 1;
 }
 void launch_pressure_col(const Dev &d, cudaStream_t s) {
@@ -644,7 +668,7 @@ void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
-    k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
+    k_velrhs<<<grid_for((long long)d.E * d.L, kVelrhsBlock), kVelrhsBlock, 0, s>>>(d, ff);
 }
 #define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
     do {                                                                                   \
@@ -656,8 +680,8 @@ void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, g
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
 void launch_update3d(const Dev &d, real Mt_inv, cudaStream_t s) {
-    k_update3d<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, 4), s>>>(d, Mt_inv);
+    k_update3d<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, kU3Sc), s>>>(d, Mt_inv);
 }
-void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 0), s>>>(d); }
+void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 2), s>>>(d); }
 
 FESOMC_PREC_END

@@ -443,7 +443,7 @@ void launch_el2nodes(const Dev &d, const real *Ue, const real *Ve, real *Un, rea
 static int p1_elems(const Dev &d) { int b = 1024 / d.L; return b > 32 ? 32 : b; }
 static size_t p1_smem(const Dev &d) { return (size_t)p1_elems(d) * (2 * kP1Slots * d.L + 1) * sizeof(real); }
 int config_p1(const Dev &d) {
-    return cudaFuncSetAttribute(k_p1_elem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p1_smem(d)) == cudaSuccess
+    return raise_smem_limit(k_p1_elem, p1_smem(d)) == cudaSuccess
                ? 0 : 1;
 }
 void launch_p1_edge(const Dev &d, cudaStream_t s) {

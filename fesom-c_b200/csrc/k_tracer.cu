@@ -852,7 +852,7 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<warp_grid(d.N, 1
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 int config_vdiff(const Dev &d) {
-    return cudaFuncSetAttribute(k_vdiff_col, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vdiff_smem(d)) ==
+    return raise_smem_limit(k_vdiff_col, vdiff_smem(d)) ==
                    cudaSuccess ? 0 : 1;
 }
 void launch_vdiff(const Dev &d, cudaStream_t s) {

@@ -812,6 +812,9 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
         fesomc_gpu_finalize(m);
         return code;
     };
+    // the launch checks below read the thread's last CUDA error: start from
+    // a clean one (a non-sticky error of an earlier, unrelated call is not ours)
+    (void)cudaGetLastError();
     if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(FESOMC_ECUDA);
     if ((rc = build_mesh(m, mesh))) return fail(rc);
     if (m->fp32 && (rc = setup_f32_view(m))) return fail(rc);
@@ -1059,7 +1062,8 @@ int fesomc_ensemble_run(fesomc_model *const *members, int32_t n, int32_t nsteps,
     auto release = [&] {
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
-        for (cudaEvent_t e : done) cudaEventDestroy(e);
+        for (cudaEvent_t e : done)
+            if (e) cudaEventDestroy(e);
     };
     cudaStream_t s0 = members[0]->stream;
     if (ms) {

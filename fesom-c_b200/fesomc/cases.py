@@ -221,11 +221,12 @@ def le_medium(nsigma=40):
 # (fv_tracer.F90:300-330) but gets no flux through the open edge itself, so
 # the tracer anomaly there grows exponentially (first at the shallow corner),
 # and currents along the clamped-elevation boundary grow next to the far
-# corner.  A relaxation to climatology on a 600 s time scale holds the
-# boundary tracers, and a 5 km sponge layer (ac scaling of advection and
-# viscosity, raised bottom drag) damps the boundary currents.
+# corner.  A relaxation to climatology on a 60 s time scale (faster than
+# that growth, whose rate is of order u / dx) holds the boundary tracers,
+# and a 5 km sponge layer (ac scaling of advection and viscosity, raised
+# bottom drag) damps the boundary currents.
 SPONGE_RADIUS = 5000.0                                   # m
-OB_RELAX_S = 600.0                                       # clim_relax, relax2clim_ac time scale
+OB_RELAX_S = 60.0                                        # clim_relax, relax2clim_ac time scale
 
 ESTUARY_CFGS = {
     # name: (nx quads, ny quads, spacing m, nsigma, depth at y=0, depth at y=Ly, wind stress N/m2)
