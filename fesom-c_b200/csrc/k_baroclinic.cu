@@ -281,21 +281,20 @@ __global__ void k_adv3_edge(Dev d) {
 
 // ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
-// level) with levels on consecutive threads.  The loop runs over whole
-// blocks; each thread computes the vertical flux at its interface z, and the
-// flux at z+1 comes from the next thread through shared memory (only the
-// block's last thread computes it itself).
+// level) with levels on consecutive lanes.  The loop runs over whole warps so
+// that the vertical flux at interface z+1 comes from the next lane.
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
+// (Sharing the fluxes across the block through shared memory, so that only
+// one thread in 256 computes a second flux, was measured 16 % slower: the
+// block-wide barrier costs more than the lane-31 recomputation.)
 // ---------------------------------------------------------------------------
-constexpr int kVelrhsBlock = 256;
-__global__ void __launch_bounds__(kVelrhsBlock, 3) k_velrhs(Dev d, real ff) {
-    __shared__ real s_fu[kVelrhsBlock], s_fv[kVelrhsBlock];
+__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, real ff) {
     const long long total = (long long)d.E * d.L;
-    const int t = (int)threadIdx.x;
-    const long long stride = (long long)gridDim.x * kVelrhsBlock;
-    for (long long bbase = (long long)blockIdx.x * kVelrhsBlock; bbase < total; bbase += stride) {
-        const bool valid = bbase + t < total;
-        const long long ii = valid ? bbase + t : total - 1;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
+        const bool valid = wbase + lane < total;
+        const long long ii = valid ? wbase + lane : total - 1;
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
@@ -345,14 +344,9 @@ __global__ void __launch_bounds__(kVelrhsBlock, 3) k_velrhs(Dev d, real ff) {
         if (d.vert_adv == 1) {
             real fu0, fv0;
             uvert_at(d, e, z, w, en, ar, fu0, fv0);
-            s_fu[t] = fu0;
-            s_fv[t] = fv0;
-            __syncthreads();
-            real fu1, fv1;
+            real fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
             if (z == L - 1) { fu1 = real(0.0); fv1 = real(0.0); }
-            else if (t == kVelrhsBlock - 1) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
-            else { fu1 = s_fu[t + 1]; fv1 = s_fv[t + 1]; }
-            __syncthreads();
+            else if (lane == 31) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
             if (mwd != real(0.0)) {
                 const real acc = d.elem_acc[e];
                 uab = uab + (fu0 - fu1) * acc;
@@ -668,7 +662,7 @@ void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
-    k_velrhs<<<grid_for((long long)d.E * d.L, kVelrhsBlock), kVelrhsBlock, 0, s>>>(d, ff);
+    k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
 }
 #define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
     do {                                                                                   \
