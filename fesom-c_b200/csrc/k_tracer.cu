@@ -405,70 +405,72 @@ __global__ void k_muscl_edge(Dev d) {
 }
 
 // node gather of the edge fluxes in edge order + vertical + update, one
-// warp per node, lane = level.  The edge loop is unrolled so the flux loads
-// of several edges are in flight together; the sums stay in edge order.
+// thread per (node, level) with levels on consecutive lanes of a flat index
+// (no lane idles when L < 32; a warp may span two or three nodes).  The edge
+// loop is unrolled so the flux loads of several edges are in flight
+// together; the sums stay in edge order.  The vertical flux at interface
+// z+1 comes from the next lane when that lane holds the same node.
 __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
+    const long long total = (long long)d.N * d.L;
     const int lane = threadIdx.x & 31;
     const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
-    WARP_LOOP(nn_, d.N) {
-        const int n = (int)nn_;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
+        const bool valid = wbase + lane < total;
+        const long long i_ = valid ? wbase + lane : total - 1;
+        const int n = (int)(i_ / L);
+        const int z = (int)(i_ % L);
         const real an = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
-        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const real vn = relax ? vel_nor(d, n) : real(0.0);
-        const real area = d.area[n];
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            const int zc = z < L ? z : L - 1;
-            real rt = real(0.0), rs = real(0.0), rc = real(0.0);
+        real rt = real(0.0), rs = real(0.0), rc = real(0.0);
 #pragma unroll 4
-            for (int p = p0; p < p1; ++p) {
-                const int code = d.node_eidx[p];
-                const int ed = code >> 1;
-                const size_t i = (size_t)ed * L + zc;
-                const real2 fT = d.mflT[i], fS = d.mflS[i], fC = d.mflC[i];
-                const bool internal = ed < d.Ed_in;
-                if (code & 1) {
-                    rt = rt - fT.x; rs = rs - fS.x; rc = rc - fC.x;
-                    if (internal) { rt = rt - fT.y; rs = rs - fS.y; rc = rc - fC.y; }
+        for (int p = p0; p < p1; ++p) {
+            const int code = d.node_eidx[p];
+            const int ed = code >> 1;
+            const size_t i = (size_t)ed * L + z;
+            const real2 fT = d.mflT[i], fS = d.mflS[i], fC = d.mflC[i];
+            const bool internal = ed < d.Ed_in;
+            if (code & 1) {
+                rt = rt - fT.x; rs = rs - fS.x; rc = rc - fC.x;
+                if (internal) { rt = rt - fT.y; rs = rs - fS.y; rc = rc - fC.y; }
+            } else {
+                rt = rt + fT.x; rs = rs + fS.x; rc = rc + fC.x;
+                if (internal) { rt = rt + fT.y; rs = rs + fS.y; rc = rc + fC.y; }
+            }
+        }
+        auto TO = [&](int m) { return d.ttfold[base + m]; };
+        auto SO = [&](int m) { return d.stfold[base + m]; };
+        const real tv0 = tvert_muscl(d, z, an, W, TO), sv0 = tvert_muscl(d, z, an, W, SO);
+        real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
+        if (lane == 31 || z == L - 1) {
+            tv1 = tvert_muscl(d, z + 1, an, W, TO);
+            sv1 = tvert_muscl(d, z + 1, an, W, SO);
+        }
+        if (valid) {
+            const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
+            const size_t ii = base + z;
+            const real jc = jc_of(d, an, z);
+            const real aj = d.area[n] * jc;
+            const real to = d.ttfold[ii], so = d.stfold[ii];
+            real tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
+            real sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
+            const real ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
+            if (relax) {
+                if (vel_nor(d, n) > real(0.0)) {
+                    tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                    sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
                 } else {
-                    rt = rt + fT.x; rs = rs + fS.x; rc = rc + fC.x;
-                    if (internal) { rt = rt + fT.y; rs = rs + fS.y; rc = rc + fC.y; }
+                    tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
+                    sr = d.clim_relax * (d.Sclim[ii] - (stf + S_aver));
                 }
             }
-            auto TO = [&](int m) { return d.ttfold[base + m]; };
-            auto SO = [&](int m) { return d.stfold[base + m]; };
-            const real tv0 = tvert_muscl(d, zc, an, W, TO), sv0 = tvert_muscl(d, zc, an, W, SO);
-            real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
-            if (lane == 31 || zc == L - 1) {
-                tv1 = tvert_muscl(d, zc + 1, an, W, TO);
-                sv1 = tvert_muscl(d, zc + 1, an, W, SO);
-            }
-            if (z < L) {
-                const size_t ii = base + z;
-                const real jc = jc_of(d, an, z);
-                const real aj = area * jc;
-                const real to = d.ttfold[ii], so = d.stfold[ii];
-                real tr = rt / aj - to * rc / aj + to * (W[z] - W[z + 1]) / jc + (tv0 - tv1) / jc;
-                real sr = rs / aj - so * rc / aj + so * (W[z] - W[z + 1]) / jc + (sv0 - sv1) / jc;
-                const real ttf = d.TF[ii] - T_aver, stf = d.SF[ii] - S_aver;
-                if (relax) {
-                    if (vn > real(0.0)) {
-                        tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
-                        sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (stf + S_aver));
-                    } else {
-                        tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
-                        sr = d.clim_relax * (d.Sclim[ii] - (stf + S_aver));
-                    }
-                }
-                d.Told_new[ii] = ttf + T_aver;
-                d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
-                d.Sold_new[ii] = stf + S_aver;
-                d.SF_adv[ii] = stf + sr * d.dt + S_aver;
-            }
+            d.Told_new[ii] = ttf + T_aver;
+            d.TF_adv[ii] = ttf + tr * d.dt + T_aver;
+            d.Sold_new[ii] = stf + S_aver;
+            d.SF_adv[ii] = stf + sr * d.dt + S_aver;
         }
     }
 }
@@ -848,7 +850,9 @@ void launch_miura(const Dev &d, cudaStream_t s) {
 void launch_muscl_edge(const Dev &d, cudaStream_t s) {
     k_muscl_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
 }
-void launch_muscl_h(const Dev &d, cudaStream_t s) { k_muscl_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
+void launch_muscl_h(const Dev &d, cudaStream_t s) {
+    k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
+}
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 int config_vdiff(const Dev &d) {
