@@ -82,14 +82,8 @@ using real4 = float4;
 #include "dev_struct.inc"
 }  // namespace f32
 
-// ---- one warp per entity, lane = level ----------------------------------------
+// full-warp mask of the level shuffles (levels on consecutive lanes)
 constexpr unsigned kFull = 0xffffffffu;
-#define WARP_LOOP(ent, count)                                                                           \
-    for (long long ent = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; ent < (long long)(count); \
-         ent += ((long long)gridDim.x * blockDim.x) >> 5)
-
-// levels handled by the chunk of 32 starting at z0
-__device__ __forceinline__ int chunk_len(int L, int z0) { return L - z0 < 32 ? L - z0 : 32; }
 
 // grid-stride helper
 #define GRID_LOOP(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); \

@@ -143,25 +143,26 @@ __global__ void k_ab2_node(Dev d) {
 }
 
 // ---------------------------------------------------------------------------
-// solve_tracer_upwind: one warp per node, lane = level.  Edge data are
-// warp-uniform (broadcast loads), level data coalesced.
+// solve_tracer_upwind: one thread per (node, level), levels on consecutive
+// lanes of a flat index (no lane idles when L < 32); level data coalesced.
 // ---------------------------------------------------------------------------
 __global__ void k_upwind_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
-    WARP_LOOP(nn_, d.N) {
-        const int n = (int)nn_;
+    const long long total = (long long)d.N * L;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
+        const bool valid = wbase + lane < total;
+        const long long i_ = valid ? wbase + lane : total - 1;
+        const int n = (int)(i_ / L);
+        const int z = (int)(i_ % L), zc = z;
         const real a = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
         const real area_inv = real(1.0) / d.area[n];
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
-        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const real vn = relax ? vel_nor(d, n) : real(0.0);
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            const int zc = z < L ? z : L - 1;
+        {
             real acc_t = real(0.0), acc_s = real(0.0), acc_c = real(0.0);
             for (int p = p0; p < p1; ++p) {
                 const int code = d.node_eidx[p];
@@ -210,14 +211,15 @@ __global__ void k_upwind_h(Dev d) {
                 tv1 = tvert_upwind(d, zc + 1, a, W, TO);
                 sv1 = tvert_upwind(d, zc + 1, a, W, SO);
             }
-            if (z < L) {
+            if (valid) {
+                const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
                 const size_t ii = base + z;
                 const real to = d.ttfold[ii], so = d.stfold[ii];
                 const real jc = jc_of(d, a, z);
                 real tr = ((acc_t - to * acc_c) * area_inv + to * (W[z] - W[z + 1]) + (tv0 - tv1)) / jc;
                 real sr = ((acc_s - so * acc_c) * area_inv + so * (W[z] - W[z + 1]) + (sv0 - sv1)) / jc;
                 if (relax) {
-                    if (vn > real(0.0)) {
+                    if (vel_nor(d, n) > real(0.0)) {
                         tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (to + T_aver));
                         sr = sr + d.relax2clim_ac * (d.Sclim[ii] - (so + S_aver));
                     } else {
@@ -605,23 +607,24 @@ __global__ void k_miura_edge(Dev d) {
 }
 
 // node gather of the Miura fluxes in edge order + vertical + update (T),
-// salinity passed through; one warp per node, lane = level
+// salinity passed through; one thread per (node, level), levels on
+// consecutive lanes of a flat index
 __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const real T_aver = d.aver[0];
     const int L = d.L, NS = d.NS;
-    WARP_LOOP(nn_, d.N) {
-        const int n = (int)nn_;
+    const long long total = (long long)d.N * L;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
+        const bool valid = wbase + lane < total;
+        const long long i_ = valid ? wbase + lane : total - 1;
+        const int n = (int)(i_ / L);
+        const int z = (int)(i_ % L), zc = z;
         const real an = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
-        const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
-        const real vn = relax ? vel_nor(d, n) : real(0.0);
-        const real area = d.area[n];
-        for (int z0 = 0; z0 < L; z0 += 32) {
-            const int z = z0 + lane;
-            const int zc = z < L ? z : L - 1;
+        {
             real rt = real(0.0), rc = real(0.0);
 #pragma unroll 4
             for (int p = p0; p < p1; ++p) {
@@ -642,14 +645,16 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
             const real tv0 = tvert_quick<false>(d, zc, an, W, TN);
             real tv1 = __shfl_down_sync(kFull, tv0, 1);
             if (lane == 31 || zc == L - 1) tv1 = tvert_quick<false>(d, zc + 1, an, W, TN);
-            if (z < L) {
+            if (valid) {
+                const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
+                const real area = d.area[n];
                 const size_t ii = base + z;
                 const real jc = jc_of(d, an, z);
                 const real to = d.ttfold[ii];
                 const real ttf = d.tnow[ii];
                 real tr = ((rt - to * rc) / area + to * (W[z] - W[z + 1]) + tv0 - tv1) / jc;
                 if (relax) {
-                    if (vn > real(0.0)) tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
+                    if (vel_nor(d, n) > real(0.0)) tr = tr + d.relax2clim_ac * (d.Tclim[ii] - (ttf + T_aver));
                     else tr = d.clim_relax * (d.Tclim[ii] - (ttf + T_aver));
                 }
                 d.Told_new[ii] = ttf + T_aver;
@@ -831,9 +836,10 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
     k_minmax_part<<<kRedGrid, kRedBlock, 0, s>>>(d);
     k_minmax_final<<<1, 32, 0, s>>>(d, kRedGrid);
 }
-static int warp_grid(long long entities, int block) { return grid_for(entities * 32, block); }
 void launch_ab2(const Dev &d, cudaStream_t s) { k_ab2_node<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d); }
-void launch_upwind(const Dev &d, cudaStream_t s) { k_upwind_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d); }
+void launch_upwind(const Dev &d, cudaStream_t s) {
+    k_upwind_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
+}
 void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
     k_muscl_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
@@ -845,7 +851,7 @@ void launch_miura(const Dev &d, cudaStream_t s) {
     k_miura_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
     k_miura_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
     k_miura_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
-    k_miura_h<<<warp_grid(d.N, 128), 128, 0, s>>>(d);
+    k_miura_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
 }
 void launch_muscl_edge(const Dev &d, cudaStream_t s) {
     k_muscl_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
