@@ -134,7 +134,7 @@ __global__ void k_bpg_elem(Dev d) {
                 b1 = b1 + row[k];
                 b2 = b2 + row[L + k];
             }
-            d.Bar_pr_2D[e] = make_double2(b1, b2);
+            d.Bar_pr_2D[e] = make_real2(b1, b2);
         }
         __syncthreads();
     }
@@ -530,13 +530,13 @@ __global__ void k_update3d(Dev d, real Mt_inv) {
                 d.U_filt_2D[e] = uf;
                 d.V_filt_2D[e] = vf;
                 const real4 an = elem_jac_a(d, d.eta_jac, en);
-                const double2 u2d = d.U_n_2D[e];
+                const real2 u2d = d.U_n_2D[e];
                 real *o = sc + kU3Sc * cb.jl;
                 o[0] = dmean_inv;
                 o[2] = uf; o[3] = vf;
                 o[4] = w.x; o[5] = w.y; o[6] = w.z; o[7] = w.w;
                 o[8] = an.x; o[9] = an.y; o[10] = an.z; o[11] = an.w;
-                o[12] = (real)u2d.x; o[13] = (real)u2d.y;
+                o[12] = u2d.x; o[13] = u2d.y;
             }
         }
         __syncthreads();

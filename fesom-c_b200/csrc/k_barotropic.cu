@@ -10,15 +10,17 @@
 //               3D->2D forcing, implicit friction, wet/dry mask) fused with
 //               the time-level rotation of U and the U_filt accumulation
 //   rot_nodes : eta time-level rotation
-// All kernels are HBM-bandwidth bound.
+// All kernels are HBM-bandwidth bound.  Both precision forms compile them:
+// the elevation, total depths and the wet/dry tests are FP64 in both (the
+// *_d scalars, wsum_d / wexp_d), the 2D momentum follows 'real'.
 #include "device_common.cuh"
 
 FESOMC_PREC_BEGIN
 
-#if !FESOMC_FP32  // the 2D sub-cycle kernels exist in FP64 only
 // AB3 coefficients, timestep_AB_2D fv_main.F90:1403,1408
-__device__ __forceinline__ real ab3(real b, real x0, real x1, real x2) {
-    return (real(1.5) + b) * x0 - (real(0.5) + real(2.0) * b) * x1 + b * x2;
+template <typename T>
+__device__ __forceinline__ T ab3(T b, T x0, T x1, T x2) {
+    return (T(1.5) + b) * x0 - (T(0.5) + T(2.0) * b) * x1 + b * x2;
 }
 __device__ __forceinline__ real2 ab3v(real b, real2 x0, real2 x1, real2 x2) {
     return make_real2(ab3(b, x0.x, x1.x, x2.x), ab3(b, x0.y, x1.y, x2.y));
@@ -36,16 +38,16 @@ __global__ void k_ab3_elem(Dev d) {
         d.UAB[e] = uab;
         const int4 en = d.elem_nodes[e];
         const int nd[4] = {en.x, en.y, en.z, en.w};
-        real ad[4];
+        double ad[4];
         for (int i = 0; i < 4; ++i) {
             const int n = nd[i];
-            real etaab = ab3(b, d.eta_n[n], d.eta_n_1[n], d.eta_n_2[n]);
-            ad[i] = d.Dmin;
-            real ttl = etaab + d.depth[n];
-            if (ttl > d.Dmin) ad[i] = ttl;
+            const double etaab = ab3<double>(d.beta_d, d.eta_n[n], d.eta_n_1[n], d.eta_n_2[n]);
+            ad[i] = d.Dmin_d;
+            const double ttl = etaab + (double)d.depth[n];
+            if (ttl > d.Dmin_d) ad[i] = ttl;
         }
         const real4 w = d.w_cv[e];
-        d.aux_elem[e] = wexp(w, ad[0], ad[1], ad[2], ad[3]);
+        d.aux_elem[e] = (real)wexp_d(w, ad[0], ad[1], ad[2], ad[3]);
         // velocity gradients of UAB
         const int4 nb = d.elem_nb[e];
         const int4 ee = d.elem_edges[e];
@@ -101,15 +103,15 @@ __device__ __forceinline__ real ssh_edge_flux(const Dev &d, int ed) {
 // host with the reference formula (fv_average_dynamic.F90:190-216).
 // ---------------------------------------------------------------------------
 __global__ void k_ssh_node(Dev d, int sub) {
-    const real de = real(0.614), ga = real(0.088), ep = real(0.013), fe = real(1.0) - de - ga - ep;
+    const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
-        real acc = real(0.0);
+        double acc = 0.0;   // ssh_rhs: FP64 accumulation of the edge fluxes
         const int p0 = d.node_eptr[n], p1 = d.node_eptr[n + 1];
 #pragma unroll 4
         for (int p = p0; p < p1; ++p) {
             const int code = d.node_eidx[p];
-            const real c1 = ssh_edge_flux(d, code >> 1);
+            const double c1 = (double)ssh_edge_flux(d, code >> 1);
             if (code & 1) acc = acc - c1;
             else acc = acc + c1;
         }
@@ -118,17 +120,16 @@ __global__ void k_ssh_node(Dev d, int sub) {
         }
         const int q = d.obn_of_node[n];
         if (d.TF_presence && q >= 0) acc = d.ob_val[(size_t)sub * d.nobn + q];
-        const real en = d.eta_n[n];
-        real enew = acc;
-        if (d.index_nod2D[n] < 2) enew = en + d.dt_2D * acc / d.area[n];
+        const double en = d.eta_n[n];
+        double enew = acc;
+        if (d.index_nod2D[n] < 2) enew = en + d.dt_2D_d * acc / (double)d.area[n];
         d.eta_new[n] = enew;
-        const real eab = de * enew + fe * en + ga * d.eta_n_1[n] + ep * d.eta_n_2[n];
+        const double eab = de * enew + fe * en + ga * d.eta_n_1[n] + ep * d.eta_n_2[n];
         d.etaAB[n] = eab;
-        if (d.wet_dry_on) d.mask_wd_node[n] = (d.depth[n] + eab > d.Dmin) ? real(1.0) : real(0.0);
+        if (d.wet_dry_on) d.mask_wd_node[n] = ((double)d.depth[n] + eab > d.Dmin_d) ? real(1.0) : real(0.0);
     }
 }
 
-#endif
 // ---------------------------------------------------------------------------
 // sub-step 1 (fv_main.F90:1451-1520): dmean_n, compute_puls_vel
 // (fv_3D_vel.F90:257-307), one thread per (element, level).
@@ -143,8 +144,7 @@ __global__ void k_puls_elem(Dev d) {
                                               d.eta_n[en.z] + d.depth[en.z], d.eta_n[en.w] + d.depth[en.w]));
         const real a = dmn / dmax(d.Dmin, wsum(w, d.eta_new[en.x] + d.depth[en.x], d.eta_new[en.y] + d.depth[en.y],
                                                  d.eta_new[en.z] + d.depth[en.z], d.eta_new[en.w] + d.depth[en.w]));
-        const double2 u2d = d.U_n_2D[e];
-        const real2 u2 = make_real2((real)u2d.x, (real)u2d.y);
+        const real2 u2 = d.U_n_2D[e];
         d.U_puls[ii] = d.U_n[ii] - a * u2.x;
         d.V_puls[ii] = d.V_n[ii] - a * u2.y;
         if (ii % d.L == 0) d.dmean_n[e] = dmn;
@@ -278,18 +278,18 @@ __global__ void k_p1_elem(Dev d) {
                     ry = ry + T[(4 * 2 + 1) * L + k];
                 }
             const real dm = d.dmean_n[e];
-            d.U_rhs_2D_3D[e] = make_double2(rx / dm, ry / dm);
+            d.U_rhs_2D_3D[e] = make_real2(rx / dm, ry / dm);
         }
         __syncthreads();
     }
 }
 
-#if !FESOMC_FP32
 // One upwind edge flux of momentum_adv_upwind_2D (fv_advection.F90:589-643)
 __device__ __forceinline__ void adv2d_edge(const Dev &d, int ed, real &uu, real &vv) {
     const int2 nn = d.edge_nodes[ed];
     const int2 et = d.edge_tri[ed];
-    const real dmean = dmax(d.Dmin, real(0.5) * ((d.etaAB[nn.x] + d.depth[nn.x]) + (d.etaAB[nn.y] + d.depth[nn.y])));
+    const real dmean = (real)dmax(d.Dmin_d, 0.5 * ((d.etaAB[nn.x] + (double)d.depth[nn.x]) +
+                                                    (d.etaAB[nn.y] + (double)d.depth[nn.y])));
     const real acc = (d.ac[nn.x] + d.ac[nn.y]) * real(0.5);
     const real4 X = d.edge_cross[ed];
     const real2 U1 = d.UAB[et.x], U2 = d.UAB[et.y];
@@ -325,29 +325,31 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
         const int e = (int)ii;
         const int4 en = d.elem_nodes[e];
         const int nd[4] = {en.x, en.y, en.z, en.w};
-        real eab[4], dep[4], etag[4];
+        // elevations and total depths in FP64 (the elevation gradient and
+        // the wet/dry test with them); the momentum terms in 'real'
+        double eab[4], dep[4], etag[4];
         for (int k = 0; k < 4; ++k) {
             eab[k] = d.etaAB[nd[k]];
             dep[k] = d.depth[nd[k]];
-            etag[k] = kG * (d.atp1[nd[k]] * eab[k] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+            etag[k] = kG64 * ((double)d.atp1[nd[k]] * eab[k] - (double)d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
         }
         real mwd = d.mask_wd[e];
         if (d.wet_dry_on) {
-            const real dmin4 = dmin(dmin(dep[0], dep[1]), dmin(dep[2], dep[3]));
-            const real emax4 = dmax(dmax(eab[0], eab[1]), dmax(eab[2], eab[3]));
-            mwd = (dmin4 + emax4 > d.Dmin) ? real(1.0) : real(0.0);
+            const double dmin4 = dmin(dmin(dep[0], dep[1]), dmin(dep[2], dep[3]));
+            const double emax4 = dmax(dmax(eab[0], eab[1]), dmax(eab[2], eab[3]));
+            mwd = (dmin4 + emax4 > d.Dmin_d) ? real(1.0) : real(0.0);
             d.mask_wd[e] = mwd;
         }
         const real4 w = d.w_cv[e];
         const real ar = d.elem_area[e];
-        const real dmean = dmax(d.Dmin, wexp(w, eab[0] + dep[0], eab[1] + dep[1], eab[2] + dep[2], eab[3] + dep[3]));
+        const real dmean = (real)dmax(d.Dmin_d, wexp_d(w, eab[0] + dep[0], eab[1] + dep[1], eab[2] + dep[2], eab[3] + dep[3]));
         const real4 gx = d.gs_x[e], gy = d.gs_y[e];
+        const real gex = (real)((double)gx.x * etag[0] + (double)gx.y * etag[1] + (double)gx.z * etag[2] + (double)gx.w * etag[3]);
+        const real gey = (real)((double)gy.x * etag[0] + (double)gy.y * etag[1] + (double)gy.z * etag[2] + (double)gy.w * etag[3]);
         const real2 uab = d.UAB[e];
         const real cor = d.coriolis[e];
-        real rx = ar * (-dmean * (gx.x * etag[0] + gx.y * etag[1] + gx.z * etag[2] + gx.w * etag[3])
-                          + uab.y * dmean * cor + d.taux[e] * d0inv);
-        real ry = ar * (-dmean * (gy.x * etag[0] + gy.y * etag[1] + gy.z * etag[2] + gy.w * etag[3])
-                          - uab.x * dmean * cor + d.tauy[e] * d0inv);
+        real rx = ar * (-dmean * gex + uab.y * dmean * cor + d.taux[e] * d0inv);
+        real ry = ar * (-dmean * gey - uab.x * dmean * cor + d.tauy[e] * d0inv);
         if (d.mom_adv_2D == 2) {
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
                     u1 = u1 + un.x - uab.x;
                     u2 = u2 + un.y - uab.y;
                 }
-            const real sd = wsum(w, dep[0], dep[1], dep[2], dep[3]);
+            const real sd = (real)wsum_d(w, dep[0], dep[1], dep[2], dep[3]);
             rx = rx + d.tau_inv_filt * u1 * ar * sd;
             ry = ry + d.tau_inv_filt * u2 * ar * sd;
         }
@@ -379,12 +381,12 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
         rx = rx + r3.x;
         ry = ry + r3.y;
         // final update with implicit bottom drag
-        real eo[4], enw[4];
+        double eo[4], enw[4];
         for (int k = 0; k < 4; ++k) { eo[k] = d.eta_n[nd[k]]; enw[k] = d.eta_new[nd[k]]; }
-        const real dmo = dmax(d.Dmin, wsum(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
+        const real dmo = (real)dmax(d.Dmin_d, wsum_d(w, eo[0] + dep[0], eo[1] + dep[1], eo[2] + dep[2], eo[3] + dep[3]));
         const real4 bf = d.bfric[e];
         const real ub = bf.x, vb = bf.y, friction = bf.z;
-        const real ff = real(1.0) / (dmax(d.Dmin, wsum(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
+        const real ff = real(1.0) / ((real)dmax(d.Dmin_d, wsum_d(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]))
                                  + friction * d.dt_2D);
         const real dt2 = d.dt_2D;
         const real2 u0 = d.U_n_2D[e];
@@ -396,7 +398,7 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
         d.U_n_1[e] = u0;
         d.U_n_2D[e] = make_real2(nx, ny);
         // U_filt accumulation with the new elevation (fv_main.F90:1596-1605)
-        const real dmn = dmax(d.Dmin, wexp(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]));
+        const real dmn = (real)dmax(d.Dmin_d, wexp_d(w, enw[0] + dep[0], enw[1] + dep[1], enw[2] + dep[2], enw[3] + dep[3]));
         d.U_filt_2D[e] = d.U_filt_2D[e] + nx * dmn;
         d.V_filt_2D[e] = d.V_filt_2D[e] + ny * dmn;
     }
@@ -406,14 +408,13 @@ __global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
 __global__ void k_rot_nodes(Dev d) {
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
-        const real e0 = d.eta_n[n], e1 = d.eta_n_1[n];
+        const double e0 = d.eta_n[n], e1 = d.eta_n_1[n];
         d.eta_n_2[n] = e1;
         d.eta_n_1[n] = e0;
         d.eta_n[n] = d.eta_new[n];
     }
 }
 
-#endif
 // U_filt_2D = V_filt_2D = 0 at the start of the sub-cycle, and the bottom
 // velocity and quadratic drag a_Cd*|U_b| that update_2D_vel uses in every
 // sub-step (fv_average_dynamic.F90:262, 400-420; U_n is fixed during the
@@ -424,15 +425,13 @@ __global__ void k_zero_filt(Dev d) {
         d.V_filt_2D[ii] = real(0.0);
         const real a_Cd = d.C_d * ((real(1.0) - d.elem_acc[ii]) * d.Cd_bz + real(1.0));
         const real ub = d.U_n[(size_t)ii * d.L + d.L - 1], vb = d.V_n[(size_t)ii * d.L + d.L - 1];
-        d.bfric[ii] = make_double4(ub, vb, a_Cd * sqrt(ub * ub + vb * vb), 0.0);
+        d.bfric[ii] = make_real4(ub, vb, a_Cd * sqrt(ub * ub + vb * vb), real(0.0));
     }
 }
 
 // ---- launch wrappers --------------------------------------------------------
-#if !FESOMC_FP32
 void launch_ab3_elem(const Dev &d, cudaStream_t s) { k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) { k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub); }
-#endif
 void launch_puls_elem(const Dev &d, cudaStream_t s) {
     k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
@@ -454,11 +453,9 @@ void launch_p1_elem(const Dev &d, cudaStream_t s) {
     const long long blocks = ((long long)d.E + B - 1) / B;
     k_p1_elem<<<(int)(blocks < 148LL * 16 ? blocks : 148LL * 16), B * d.L, p1_smem(d), s>>>(d);
 }
-#if !FESOMC_FP32
 void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
 void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
-#endif
 void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 
 FESOMC_PREC_END

@@ -779,57 +779,59 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
     }
 }
 
-#if !FESOMC_FP32  // the energy diagnostic is FP64 only
 // ---------------------------------------------------------------------------
-// energy: compensated (Neumaier) partial sums per block, then one block
+// energy: compensated (Neumaier) partial sums per block, then one block.
+// FP64 accumulation in both precision forms.
 // ---------------------------------------------------------------------------
 struct KSum {
-    real s, c;
-    __device__ void add(real x) {
-        real t = s + x;
+    double s, c;
+    __device__ void add(double x) {
+        double t = s + x;
         if (fabs(s) >= fabs(x)) c += (s - t) + x;
         else c += (x - t) + s;
         s = t;
     }
-    __device__ real value() const { return s + c; }
+    __device__ double value() const { return s + c; }
 };
 
-__global__ void k_energy_part(Dev d, real *part) {
-    __shared__ real sh[3][kRedBlock];
-    KSum pe{real(0.0), real(0.0)}, ke{real(0.0), real(0.0)}, ar{real(0.0), real(0.0)};
+__global__ void k_energy_part(Dev d, double *part) {
+    __shared__ double sh[3][kRedBlock];
+    KSum pe{0.0, 0.0}, ke{0.0, 0.0}, ar{0.0, 0.0};
     GRID_LOOP(i, d.N) {
-        const real e = d.eta_n[i];
-        pe.add(real(0.5) * kG * d.area[i] * (e * e));
-        ar.add(d.area[i]);
+        const double e = d.eta_n[i];
+        const double a = d.area[i];
+        pe.add(0.5 * kG64 * a * (e * e));
+        ar.add(a);
     }
     GRID_LOOP(i, d.E) {
         const int4 en = d.elem_nodes[i];
         const real4 w = d.w_cv[i];
-        const real s = wsum(w, dmax(d.Dmin, d.depth[en.x] + d.eta_n[en.x]), dmax(d.Dmin, d.depth[en.y] + d.eta_n[en.y]),
-                              dmax(d.Dmin, d.depth[en.z] + d.eta_n[en.z]), dmax(d.Dmin, d.depth[en.w] + d.eta_n[en.w]));
+        const double s = wsum_d(w, dmax(d.Dmin_d, (double)d.depth[en.x] + d.eta_n[en.x]),
+                                dmax(d.Dmin_d, (double)d.depth[en.y] + d.eta_n[en.y]),
+                                dmax(d.Dmin_d, (double)d.depth[en.z] + d.eta_n[en.z]),
+                                dmax(d.Dmin_d, (double)d.depth[en.w] + d.eta_n[en.w]));
         const real2 u = d.U_n_2D[i];
-        ke.add(real(0.5) * s * d.elem_area[i] * (u.x * u.x + u.y * u.y));
+        const double ux = u.x, uy = u.y;
+        ke.add(0.5 * s * (double)d.elem_area[i] * (ux * ux + uy * uy));
     }
     sh[0][threadIdx.x] = pe.value();
     sh[1][threadIdx.x] = ke.value();
     sh[2][threadIdx.x] = ar.value();
     __syncthreads();
     if (threadIdx.x < 3) {
-        KSum t{real(0.0), real(0.0)};
+        KSum t{0.0, 0.0};
         for (int k = 0; k < kRedBlock; ++k) t.add(sh[threadIdx.x][k]);
         part[(size_t)blockIdx.x * 3 + threadIdx.x] = t.value();
     }
 }
 
-__global__ void k_energy_final(const real *part, int nparts, real *out) {
+__global__ void k_energy_final(const double *part, int nparts, double *out) {
     if (threadIdx.x < 3 && blockIdx.x == 0) {
-        KSum t{real(0.0), real(0.0)};
+        KSum t{0.0, 0.0};
         for (int b = 0; b < nparts; ++b) t.add(part[(size_t)b * 3 + threadIdx.x]);
         out[threadIdx.x] = t.value();
     }
 }
-
-#endif
 
 // ---- launch wrappers --------------------------------------------------------
 void launch_minmax(const Dev &d, cudaStream_t s) {
@@ -868,12 +870,10 @@ int config_vdiff(const Dev &d) {
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     k_vdiff_col<<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
 }
-#if !FESOMC_FP32
 int energy_parts() { return kRedGrid; }
-void launch_energy(const Dev &d, real *part, real *out, cudaStream_t s) {
+void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {
     k_energy_part<<<kRedGrid, kRedBlock, 0, s>>>(d, part);
     k_energy_final<<<1, 32, 0, s>>>(part, kRedGrid, out);
 }
-#endif
 
 FESOMC_PREC_END

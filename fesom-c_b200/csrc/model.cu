@@ -51,7 +51,7 @@ namespace fesomc {
     void launch_muscl_h(const Dev &, cudaStream_t); \
     void launch_vdiff(const Dev &, cudaStream_t); \
     int energy_parts(); \
-    void launch_energy(const Dev &, real *, real *, cudaStream_t);
+    void launch_energy(const Dev &, double *, double *, cudaStream_t);
 namespace f64 {
 FESOMC_KERNEL_LAUNCHERS
 }  // namespace f64
@@ -153,8 +153,8 @@ int upload(fesomc_model *m, const T **dst, const std::vector<T> &src) {
 }
 
 // field table for state sync: name of the fesomc_state member, device
-// pointer, count, group, and whether the device copy is FP32 (level fields of
-// the FP32 form)
+// pointer, count, group, and whether the device copy is FP32 (level fields
+// and 2D momentum of the FP32 form)
 struct FieldRef {
     double *fesomc_state::*host;
     void *dev;
@@ -175,11 +175,11 @@ std::vector<FieldRef> field_table(fesomc_model *m) {
         {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA, false},
         {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA, false},
         {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA, false},
-        {&fesomc_state::U_n_2D, d.U_n_2D, 2 * E, FESOMC_F_UV2D, false},
-        {&fesomc_state::U_n_1, d.U_n_1, 2 * E, FESOMC_F_UV2D, false},
-        {&fesomc_state::U_n_2, d.U_n_2, 2 * E, FESOMC_F_UV2D, false},
-        {&fesomc_state::U_filt_2D, d.U_filt_2D, E, FESOMC_F_UV2D, false},
-        {&fesomc_state::V_filt_2D, d.V_filt_2D, E, FESOMC_F_UV2D, false},
+        {&fesomc_state::U_n_2D, LEV(U_n_2D), 2 * E, FESOMC_F_UV2D, f},
+        {&fesomc_state::U_n_1, LEV(U_n_1), 2 * E, FESOMC_F_UV2D, f},
+        {&fesomc_state::U_n_2, LEV(U_n_2), 2 * E, FESOMC_F_UV2D, f},
+        {&fesomc_state::U_filt_2D, LEV(U_filt_2D), E, FESOMC_F_UV2D, f},
+        {&fesomc_state::V_filt_2D, LEV(V_filt_2D), E, FESOMC_F_UV2D, f},
         {&fesomc_state::U_n, LEV(U_n), L * E, FESOMC_F_UV3D, f},
         {&fesomc_state::V_n, LEV(V_n), L * E, FESOMC_F_UV3D, f},
         {&fesomc_state::U_rhsAB, LEV(U_rhsAB), L * E, FESOMC_F_UV3D, f},
@@ -199,11 +199,11 @@ std::vector<FieldRef> field_table(fesomc_model *m) {
         {&fesomc_state::tke_dissip, LEV(tke_dissip), NS * N, FESOMC_F_MIX, f},
         {&fesomc_state::Av, LEV(Av), NS * E, FESOMC_F_MIX, f},
         {&fesomc_state::Wvel, LEV(Wvel), NS * N, FESOMC_F_WVEL, f},
-        {&fesomc_state::mask_wd, d.mask_wd, E, FESOMC_F_MASK, false},
-        {&fesomc_state::mask_wd_node, d.mask_wd_node, N, FESOMC_F_MASK, false},
+        {&fesomc_state::mask_wd, LEV(mask_wd), E, FESOMC_F_MASK, f},
+        {&fesomc_state::mask_wd_node, LEV(mask_wd_node), N, FESOMC_F_MASK, f},
         {&fesomc_state::rho_c, LEV(rho_c), L * N, FESOMC_F_DIAG, f},
         {&fesomc_state::hpressure, LEV(hpressure), NS * N, FESOMC_F_DIAG, f},
-        {&fesomc_state::Bar_pr_2D, d.Bar_pr_2D, 2 * E, FESOMC_F_DIAG, false},
+        {&fesomc_state::Bar_pr_2D, LEV(Bar_pr_2D), 2 * E, FESOMC_F_DIAG, f},
     };
 #undef LEV
 }
@@ -376,27 +376,39 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
     return FESOMC_OK;
 }
 
-// 2D (sub-cycle) state, forcing and diagnostics: FP64 in both forms
+// elevation family, river / open-boundary inputs, status words and the
+// energy scratch: FP64 in both forms, held by the f64 view
 int alloc_2d(fesomc_model *m) {
     Dev &d = m->d;
-    const size_t N = d.N, E = d.E;
+    const size_t N = d.N;
     int rc = 0;
     double **nodes[] = {&d.eta_n, &d.eta_n_1, &d.eta_n_2, &d.eta_new, &d.etaAB, &d.ssh_gp, &d.eta_jac,
-                        &d.eta_jac_old, &d.mask_wd_node, &d.windx, &d.windy};
+                        &d.eta_jac_old};
     for (auto p : nodes) if ((rc = dalloc(m, p, N))) return rc;
-    double **elems[] = {&d.aux_elem, &d.dmean_n, &d.U_filt_2D, &d.V_filt_2D, &d.mask_wd, &d.taux, &d.tauy};
-    for (auto p : elems) if ((rc = dalloc(m, p, E))) return rc;
-    double2 **e2[] = {&d.U_n_2D, &d.U_n_1, &d.U_n_2, &d.UAB, &d.U_rhs_2D_3D, &d.Bar_pr_2D};
-    for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
-    if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
-    if ((rc = dalloc(m, &d.bfric, E))) return rc;
-    if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
     if ((rc = dalloc(m, &d.runoff, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1)))) return rc;
     if ((rc = dalloc(m, &d.ob_val, (size_t)(d.nobn > 0 ? d.nobn : 1) * (m->p.Mt > 0 ? m->p.Mt : 1)))) return rc;
     if ((rc = dalloc(m, &d.status, 1))) return rc;
     if ((rc = dalloc(m, &d.notconv, 1))) return rc;
     if ((rc = dalloc(m, &m->d_epart, (size_t)3 * energy_parts()))) return rc;
     if ((rc = dalloc(m, &m->d_eout, 4))) return rc;
+    return FESOMC_OK;
+}
+
+// 2D momentum, its forcing and the sub-cycle scratch, in the working
+// precision of D
+template <typename D>
+int alloc_mom2d(fesomc_model *m, D &d) {
+    const size_t N = d.N, E = d.E;
+    int rc = 0;
+    decltype(&d.mask_wd) nodes[] = {&d.mask_wd_node, &d.windx, &d.windy};
+    for (auto p : nodes) if ((rc = dalloc(m, p, N))) return rc;
+    decltype(&d.mask_wd) elems[] = {&d.aux_elem, &d.dmean_n, &d.U_filt_2D, &d.V_filt_2D, &d.mask_wd, &d.taux, &d.tauy};
+    for (auto p : elems) if ((rc = dalloc(m, p, E))) return rc;
+    decltype(&d.UAB) e2[] = {&d.U_n_2D, &d.U_n_1, &d.U_n_2, &d.UAB, &d.U_rhs_2D_3D, &d.Bar_pr_2D};
+    for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
+    if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
+    if ((rc = dalloc(m, &d.bfric, E))) return rc;
+    if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
     return FESOMC_OK;
 }
 
@@ -438,11 +450,13 @@ int alloc_3d(fesomc_model *m, D &d) {
 int alloc_state(fesomc_model *m) {
     int rc = alloc_2d(m);
     if (rc) return rc;
-    return m->fp32 ? alloc_3d(m, m->d32) : alloc_3d(m, m->d);
+    if (m->fp32) return (rc = alloc_mom2d(m, m->d32)) ? rc : alloc_3d(m, m->d32);
+    return (rc = alloc_mom2d(m, m->d)) ? rc : alloc_3d(m, m->d);
 }
 
 // FP32 form: the f32 view shares the sizes, flags, connectivity and the FP64
-// 2D state with the f64 view, and holds FP32 copies of the mesh geometry.
+// elevation family with the f64 view, and holds FP32 copies of the mesh
+// geometry and its own FP32 2D momentum.
 template <typename TO>
 int geom_f32(fesomc_model *m, const void *src, size_t n_doubles, const TO **dst) {
     std::vector<double> h(n_doubles);
@@ -483,18 +497,14 @@ int setup_f32_view(fesomc_model *m) {
     return FESOMC_OK;
 }
 
-// share the FP64 2D state with the f32 view (after alloc_state)
+// share the FP64 elevation family, inputs and status words with the f32
+// view (after alloc_state)
 void share_2d(fesomc_model *m) {
     const Dev &a = m->d;
     fesomc::f32::Dev &b = m->d32;
     b.eta_n = a.eta_n; b.eta_n_1 = a.eta_n_1; b.eta_n_2 = a.eta_n_2; b.eta_new = a.eta_new; b.etaAB = a.etaAB;
     b.ssh_gp = a.ssh_gp; b.eta_jac = a.eta_jac; b.eta_jac_old = a.eta_jac_old;
-    b.U_n_2D = a.U_n_2D; b.U_n_1 = a.U_n_1; b.U_n_2 = a.U_n_2; b.UAB = a.UAB; b.U_rhs_2D_3D = a.U_rhs_2D_3D;
-    b.Bar_pr_2D = a.Bar_pr_2D; b.bfric = a.bfric;
-    b.aux_elem = a.aux_elem; b.dmean_n = a.dmean_n; b.U_filt_2D = a.U_filt_2D; b.V_filt_2D = a.V_filt_2D;
-    b.mask_wd = a.mask_wd; b.mask_wd_node = a.mask_wd_node; b.vel_grad = a.vel_grad;
-    b.taux = a.taux; b.tauy = a.tauy; b.windx = a.windx; b.windy = a.windy; b.runoff = a.runoff;
-    b.ob_val = a.ob_val; b.adv2d = a.adv2d; b.status = a.status; b.notconv = a.notconv;
+    b.runoff = a.runoff; b.ob_val = a.ob_val; b.status = a.status; b.notconv = a.notconv;
 }
 
 template <typename D>
@@ -508,6 +518,7 @@ void set_params(D &d, const fesomc_params &p) {
     d.im_vert_visc = p.im_vert_visc; d.im_vert_visc_fic = p.im_vert_visc_fic; d.fic_point = p.fic_point;
     d.tracer_adv = p.tracer_adv; d.ver_mix = p.ver_mix; d.filt_2D = p.filt_2D; d.filt_3D = p.filt_3D;
     d.wet_dry_on = p.wet_dry_on; d.key_rivers = p.key_rivers; d.TF_presence = p.TF_presence; d.cl_relax = p.cl_relax;
+    d.beta_d = p.beta; d.Dmin_d = p.Dmin; d.dt_2D_d = p.dt_2D;
 }
 
 // Algorithmic bytes per launch of every kernel: each array the kernel must
@@ -575,14 +586,13 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     return 0.0;
 }
 
-// In the FP32 form the 3D kernels move their level fields (almost all of
-// their bytes) at half the size; the 2D sub-cycle kernels are unchanged.
+// In the FP32 form the 3D kernels and the 2D momentum kernels move their
+// fields (almost all of their bytes) at half the size; the elevation
+// kernels (ssh_node, rot_nodes, jac_swap) keep FP64 and are counted as such.
 double kernel_bytes(const fesomc_model *m, const std::string &k) {
     const double b = kernel_bytes_fp64(m, k);
     if (!m->fp32) return b;
-    if (k == "ab3_elem" || k == "ssh_node" || k == "adv2d_edge" || k == "u2d_elem" || k == "rot_nodes" ||
-        k == "jac_swap")
-        return b;
+    if (k == "ssh_node" || k == "rot_nodes" || k == "jac_swap") return b;
     return 0.5 * b;
 }
 
@@ -646,8 +656,8 @@ int enqueue_step(fesomc_model *m, double ff) {
     rec(m, "zero_filt", [&] { K3(launch_zero_filt, s); });
     n += 1;
     for (int sub = 0; sub < d.Mt; ++sub) {
-        rec(m, "ab3_elem", [&] { launch_ab3_elem(d, s); });
-        rec(m, "ssh_node", [&] { launch_ssh_node(d, sub, s); });
+        rec(m, "ab3_elem", [&] { K3(launch_ab3_elem, s); });
+        rec(m, "ssh_node", [&] { K3(launch_ssh_node, sub, s); });
         n += 2;
         if (sub == 0) {
             rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
@@ -656,9 +666,9 @@ int enqueue_step(fesomc_model *m, double ff) {
             rec(m, "p1_elem", [&] { K3(launch_p1_elem, s); });
             n += 4;
         }
-        if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { launch_adv2d_edge(d, s); }); n += 1; }
-        rec(m, "u2d_elem", [&] { launch_u2d_elem(d, s); });
-        rec(m, "rot_nodes", [&] { launch_rot_nodes(d, s); });
+        if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { K3(launch_adv2d_edge, s); }); n += 1; }
+        rec(m, "u2d_elem", [&] { K3(launch_u2d_elem, s); });
+        rec(m, "rot_nodes", [&] { K3(launch_rot_nodes, s); });
         n += 2;
     }
     rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
@@ -846,11 +856,13 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if ((rc = fesomc_gpu_sync_from_host(m, FESOMC_F_ALL, st))) return fail(rc);
     if (!st->mask_wd) {
         std::vector<double> ones(mesh->elem2D, 1.0);
-        if (cudaMemcpy(m->d.mask_wd, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice)) return fail(FESOMC_ECUDA);
+        void *dev = m->fp32 ? (void *)m->d32.mask_wd : (void *)m->d.mask_wd;
+        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data()))) return fail(rc);
     }
     if (!st->mask_wd_node) {
         std::vector<double> ones(mesh->nod2D, 1.0);
-        if (cudaMemcpy(m->d.mask_wd_node, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice)) return fail(FESOMC_ECUDA);
+        void *dev = m->fp32 ? (void *)m->d32.mask_wd_node : (void *)m->d.mask_wd_node;
+        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data()))) return fail(rc);
     }
     // jacobian state before the main loop: both calls see the initial eta
     if (cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice) ||
@@ -873,12 +885,22 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
     cudaStream_t s = m->stream;
     // large fields are copied synchronously with respect to the stream so the
     // caller may reuse its buffers on return
-    if (f->taux) CK(cudaMemcpyAsync(d.taux, f->taux, E * 8, cudaMemcpyHostToDevice, s));
-    if (f->tauy) CK(cudaMemcpyAsync(d.tauy, f->tauy, E * 8, cudaMemcpyHostToDevice, s));
-    if (f->windx) CK(cudaMemcpyAsync(d.windx, f->windx, N * 8, cudaMemcpyHostToDevice, s));
-    if (f->windy) CK(cudaMemcpyAsync(d.windy, f->windy, N * 8, cudaMemcpyHostToDevice, s));
-    if (f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
     int rc = FESOMC_OK;
+    if (!m->fp32) {
+        if (f->taux) CK(cudaMemcpyAsync(d.taux, f->taux, E * 8, cudaMemcpyHostToDevice, s));
+        if (f->tauy) CK(cudaMemcpyAsync(d.tauy, f->tauy, E * 8, cudaMemcpyHostToDevice, s));
+        if (f->windx) CK(cudaMemcpyAsync(d.windx, f->windx, N * 8, cudaMemcpyHostToDevice, s));
+        if (f->windy) CK(cudaMemcpyAsync(d.windy, f->windy, N * 8, cudaMemcpyHostToDevice, s));
+    } else if (f->taux || f->tauy || f->windx || f->windy) {
+        // FP32 form: converted on the host, written while the stream is idle
+        const fesomc::f32::Dev &q = m->d32;
+        CK(cudaStreamSynchronize(s));
+        if (f->taux && (rc = field_from_host(m, q.taux, true, E, f->taux))) return rc;
+        if (f->tauy && (rc = field_from_host(m, q.tauy, true, E, f->tauy))) return rc;
+        if (f->windx && (rc = field_from_host(m, q.windx, true, N, f->windx))) return rc;
+        if (f->windy && (rc = field_from_host(m, q.windy, true, N, f->windy))) return rc;
+    }
+    if (f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
     if (f->Tclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Tclim : (void *)d.Tclim, m->fp32, L * N, f->Tclim)))
         return rc;
     if (f->Sclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Sclim : (void *)d.Sclim, m->fp32, L * N, f->Sclim)))
@@ -944,7 +966,8 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
 
 int fesomc_gpu_energy(fesomc_model *m, double *eout) {
     if (!m || !eout) return FESOMC_EINVAL;
-    launch_energy(m->d, m->d_epart, m->d_eout, m->stream);
+    if (m->fp32) fesomc::f32::launch_energy(m->d32, m->d_epart, m->d_eout, m->stream);
+    else launch_energy(m->d, m->d_epart, m->d_eout, m->stream);
     m->launches += 2;
     double h[3];
     CK(cudaMemcpyAsync(h, m->d_eout, 3 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
