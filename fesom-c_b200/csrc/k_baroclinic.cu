@@ -288,7 +288,8 @@ __global__ void k_adv3_edge(Dev d) {
 // one thread in 256 computes a second flux, was measured 16 % slower: the
 // block-wide barrier costs more than the lane-31 recomputation.)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_velrhs(Dev d, real ff) {
+// FP32: 4 resident blocks (at most 64 registers); FP64: 3 (80 registers).
+__global__ void __launch_bounds__(256, FESOMC_FP32 ? 4 : 3) k_velrhs(Dev d, real ff) {
     const long long total = (long long)d.E * d.L;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;

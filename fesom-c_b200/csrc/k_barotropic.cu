@@ -319,7 +319,8 @@ __global__ void k_adv2d_edge(Dev d) {
 // key_atm off) + rotation of U time levels + U_filt accumulation
 // (fv_main.F90:1568-1606).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 6) k_u2d_elem(Dev d) {
+// FP32: 8 resident blocks (at most 64 registers); FP64: 6.
+__global__ void __launch_bounds__(128, FESOMC_FP32 ? 8 : 6) k_u2d_elem(Dev d) {
     const real d0inv = real(1.0) / d.density_0;
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
