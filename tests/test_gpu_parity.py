@@ -210,6 +210,15 @@ def test_sync_roundtrip(mods):
     g.close()
 
 
+def test_cfg0_bit_exact(mods):
+    """The reference's CPU-sized configuration (201 x 81 nodes at 300 m, 11
+    sigma levels, MUSCL, wetting/drying, tide, river), 100 internal steps."""
+    abi, cases, model, pyoracle = mods
+    bad, eg, eo = run_pair(mods, cases.estuary("cfg0"), 100)
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+
+
 def test_cfg1_scale_properties(mods):
     """The 1.05M-node, 21-level benchmark mesh: finite state, masks in {0,1},
     bit-identical repeat, and kernel launches counted."""
