@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include "fesomc_log.h"
+#include "fesomc_trig.h"
 
 // FP32 form: the closure's logarithm is the device logf (the FP64 path uses
 // fesomc_log, bit-identical with the oracle's).

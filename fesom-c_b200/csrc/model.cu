@@ -11,6 +11,7 @@
 
 #include "device_common.cuh"
 #include "fesomc_gpu.h"
+#include "forcing_dev.h"
 
 namespace fesomc {
 // kernels (k_*.cu), compiled once per precision
@@ -93,6 +94,10 @@ struct fesomc_model {
     size_t stage_len = 0;
     double *h_runoff = nullptr;  // host copy of current runoff
     bool runoff_dirty = false;
+    // forcing on the device (fesomc_gpu_set_device_forcing)
+    bool dev_forcing = false;
+    int river_ramp = 0;
+    double *d_clock = nullptr, *d_ampt = nullptr, *d_fazt = nullptr, *d_harm = nullptr, *d_runoff_base = nullptr;
     // diagnostics
     double *d_epart = nullptr, *d_eout = nullptr;
     unsigned int *h_status = nullptr;
@@ -529,6 +534,7 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     const Dev &d = m->d;
     const double N = d.N, E = d.E, Ed = d.Ed, Ei = d.Ed_in, L = d.L, NS = d.NS;
     const double nnz_ne = (double)(2 * d.Ed);  // node->edge incidences
+    if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
     if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
     // per internal edge: nodes (etaAB, depth, ac), elements (UAB, vel_grad,
@@ -592,7 +598,7 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
 double kernel_bytes(const fesomc_model *m, const std::string &k) {
     const double b = kernel_bytes_fp64(m, k);
     if (!m->fp32) return b;
-    if (k == "ssh_node" || k == "rot_nodes" || k == "jac_swap") return b;
+    if (k == "ssh_node" || k == "rot_nodes" || k == "jac_swap" || k == "forcing") return b;
     return 0.5 * b;
 }
 
@@ -628,6 +634,30 @@ void rec(fesomc_model *m, const char *name, F fn) {
 // The kernel sequence of one internal step (oce_timestep case(3)).  The 2D
 // sub-cycle kernels always run on the FP64 view; the 3D kernels on the view
 // of the model's form (K3).
+// device forcing view of the model (valid after fesomc_gpu_set_device_forcing)
+ForcingDev forcing_view(const fesomc_model *m) {
+    ForcingDev f{};
+    const Dev &d = m->d;
+    f.nobn = d.nobn;
+    f.n_rivers = d.n_rivers;
+    f.Mt = m->p.Mt;
+    f.restart = m->p.restart;
+    f.tides_on = m->p.TF_presence && d.nobn > 0;
+    f.rivers_on = m->p.key_rivers && d.n_rivers > 0 && m->d_runoff_base != nullptr;
+    f.river_ramp = m->river_ramp;
+    f.dt = m->p.dt;
+    f.dt_2D = m->p.dt_2D;
+    f.time_jd0 = m->p.time_jd0;
+    f.clock = m->d_clock;
+    f.ampt = m->d_ampt;
+    f.fazt = m->d_fazt;
+    f.harm = m->d_harm;
+    f.runoff_base = m->d_runoff_base;
+    f.ob_val = d.ob_val;
+    f.runoff = d.runoff;
+    return f;
+}
+
 int enqueue_step(fesomc_model *m, double ff) {
     const Dev &d = m->d;
     const fesomc::f32::Dev &q = m->d32;
@@ -637,6 +667,10 @@ int enqueue_step(fesomc_model *m, double ff) {
 #define K3(fn, ...) (f ? fesomc::f32::fn(q, ##__VA_ARGS__) : fesomc::f64::fn(d, ##__VA_ARGS__))
 #define K3E2N(a, b, c, e) (f ? fesomc::f32::launch_el2nodes(q, q.a, q.b, q.c, q.e, s) \
                              : fesomc::f64::launch_el2nodes(d, d.a, d.b, d.c, d.e, s))
+    if (m->dev_forcing) {
+        rec(m, "forcing", [&] { launch_forcing(forcing_view(m), s); });
+        n += 2;
+    }
     rec(m, "pressure_col", [&] { K3(launch_pressure_col, s); });
     rec(m, "bpg_elem", [&] { K3(launch_bpg_elem, s); });
     n += 2;
@@ -707,7 +741,7 @@ void ob_values(const fesomc_model *m, double time, double time_jd, double *out) 
             double v = 0.0;
             for (int j = 0; j < 12; ++j)
                 v = v + m->amp_factor[j] * m->ampt[(size_t)nobn * j + q] *
-                            std::cos((time_2D - p.time_jd0 * 86400.0) * 2.0 * kPi / (kHarmPeriod[j] * 3600.0) -
+                            fesomc_cos((time_2D - p.time_jd0 * 86400.0) * 2.0 * kPi / (kHarmPeriod[j] * 3600.0) -
                                      (m->fazt[(size_t)nobn * j + q] + m->phy_factor[j]));
             if (!p.restart)
                 if (time_jd - p.time_jd0 < 10.0) v = v * (time_jd - p.time_jd0) / 10.0;
@@ -764,7 +798,7 @@ int run_steps(fesomc_model *m, int nsteps) {
         // time update of the main loop (fv_main.F90:400-401)
         m->time_jd = m->time_jd + m->p.dt / 86400.0;
         const double time = m->time_jd * 86400.0;
-        int rc = upload_step_inputs(m, time, m->time_jd);
+        int rc = m->dev_forcing ? FESOMC_OK : upload_step_inputs(m, time, m->time_jd);
         if (rc) return rc;
         if (m->lfirst) {
             // first call of compute_vel_rhs: AB2 factor 1 (fv_3D_vel.F90:124-128)
@@ -789,6 +823,23 @@ int run_steps(fesomc_model *m, int nsteps) {
         }
         m->launches += m->launches_per_step;
     }
+    return FESOMC_OK;
+}
+
+// tide harmonics of the device forcing from the host copies
+int upload_tides(fesomc_model *m) {
+    const size_t nobn = (size_t)m->d.nobn;
+    if (nobn) {
+        CK(cudaMemcpy(m->d_ampt, m->ampt.data(), nobn * 12 * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(m->d_fazt, m->fazt.data(), nobn * 12 * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    double h[36];
+    for (int j = 0; j < 12; ++j) {
+        h[j] = m->amp_factor[j];
+        h[12 + j] = m->phy_factor[j];
+        h[24 + j] = kHarmPeriod[j];
+    }
+    CK(cudaMemcpy(m->d_harm, h, sizeof(h), cudaMemcpyHostToDevice));
     return FESOMC_OK;
 }
 
@@ -915,6 +966,37 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
     if (f->fazt && nobn) std::memcpy(m->fazt.data(), f->fazt, nobn * 12 * 8);
     if (f->amp_factor) std::memcpy(m->amp_factor, f->amp_factor, 12 * 8);
     if (f->phy_factor) std::memcpy(m->phy_factor, f->phy_factor, 12 * 8);
+    if (m->dev_forcing && ((f->ampt && nobn) || (f->fazt && nobn) || f->amp_factor || f->phy_factor)) {
+        CK(cudaStreamSynchronize(s));
+        if ((rc = upload_tides(m))) return rc;
+    }
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_set_device_forcing(fesomc_model *m, const double *runoff_base, int32_t river_ramp) {
+    if (!m) return FESOMC_EINVAL;
+    const Dev &d = m->d;
+    const bool rivers = m->p.key_rivers && d.n_rivers > 0;
+    if (rivers && !runoff_base) return FESOMC_EINVAL;
+    int rc;
+    CK(cudaStreamSynchronize(m->stream));
+    if (!m->d_clock) {
+        const size_t nobn = (size_t)(d.nobn > 0 ? d.nobn : 1);
+        if ((rc = dalloc(m, &m->d_clock, 1)) || (rc = dalloc(m, &m->d_ampt, 12 * nobn)) ||
+            (rc = dalloc(m, &m->d_fazt, 12 * nobn)) || (rc = dalloc(m, &m->d_harm, 36)) ||
+            (rc = dalloc(m, &m->d_runoff_base, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1))))
+            return rc;
+    }
+    if ((rc = upload_tides(m))) return rc;
+    if (rivers) CK(cudaMemcpy(m->d_runoff_base, runoff_base, sizeof(double) * d.n_rivers, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(m->d_clock, &m->time_jd, sizeof(double), cudaMemcpyHostToDevice));
+    m->river_ramp = river_ramp != 0;
+    if (!m->dev_forcing && m->graph) {
+        // the captured step has no forcing kernels: capture again
+        cudaGraphExecDestroy(m->graph);
+        m->graph = nullptr;
+    }
+    m->dev_forcing = true;
     return FESOMC_OK;
 }
 
@@ -960,6 +1042,7 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
     if (mask == FESOMC_F_ALL) {
         m->lfirst = st->lfirst;
         m->time_jd = st->time_jd;
+        if (m->d_clock) CK(cudaMemcpy(m->d_clock, &m->time_jd, sizeof(double), cudaMemcpyHostToDevice));
     }
     return FESOMC_OK;
 }

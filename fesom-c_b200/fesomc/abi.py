@@ -79,6 +79,7 @@ class MeshOpts(C.Structure):
 SIGNATURES = {
     "fesomc_gpu_init": (C.c_int, [C.POINTER(Mesh), C.POINTER(Params), C.POINTER(State), C.POINTER(C.c_void_p)]),
     "fesomc_gpu_set_forcing": (C.c_int, [C.c_void_p, C.POINTER(Forcing)]),
+    "fesomc_gpu_set_device_forcing": (C.c_int, [C.c_void_p, f64p, C.c_int32]),
     "fesomc_gpu_step": (C.c_int, [C.c_void_p, C.c_int32]),
     "fesomc_gpu_run": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "fesomc_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),

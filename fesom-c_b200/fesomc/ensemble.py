@@ -12,6 +12,8 @@ separate runs.
 """
 import ctypes as C
 
+import numpy as np
+
 from . import abi, cases, model
 
 # member step statuses that fesomc_ensemble_run reports per member
@@ -41,10 +43,10 @@ def lpt_partition(costs, bins):
 
 
 class Ensemble:
-    """Members (cases) on the current GPU, advanced together.  The forcing of
-    each member's first step is pushed once and held (the stress, wind and
-    river runoff of that step; the open-boundary tide is evaluated by the
-    library at every step)."""
+    """Members (cases) on the current GPU, advanced together.  Each member's
+    stress and wind are pushed once and held; its open-boundary tide and its
+    river runoff (ramped over the first 10 days) are evaluated on the GPU at
+    every step (fesomc_gpu_set_device_forcing)."""
 
     def __init__(self, member_cases):
         self.lib = abi.load()
@@ -58,6 +60,10 @@ class Ensemble:
                 t_next = cases.advance_time(g.time_jd, c.params.dt)
                 g.set_forcing(c.forcing_fn(1, t_next))
                 self.models.append(g)
+                base = np.ascontiguousarray(c.forcing_fn(1, c.params.time_jd0 + 20.0)["runoff_rivers"],
+                                            dtype=np.float64)
+                abi.check(self.lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base) if base.size else None, 1),
+                          "fesomc_gpu_set_device_forcing")
         except Exception:
             self.close()
             raise

@@ -212,6 +212,21 @@ typedef struct fesomc_model fesomc_model;
 int  fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par,
                      const fesomc_state *state, fesomc_model **out);
 int  fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f);
+/* Forcing on the device, replacing the per-step host side of rivers_do
+ * (src/fv_rivers.F90:263-299) and of the harmonic open-boundary elevation
+ * of compute_ssh_rhs_elem (src/fv_average_dynamic.F90:190-216).  After this
+ * call every internal step advances a device copy of time_jd (the main
+ * loop's time_jd + dt/86400, src/fv_main.F90:400) and evaluates on the
+ * device, with the same arithmetic as the host path, the open-boundary
+ * elevation of its Mt sub-steps (from the ampt / fazt / amp_factor /
+ * phy_factor last given to fesomc_gpu_set_forcing; later calls that change
+ * them are picked up) and the river runoff: runoff_base (n_rivers values,
+ * required when rivers are on), scaled by (time_jd - time_jd0)/10 during
+ * the first 10 days when river_ramp != 0.  Steps then copy nothing from
+ * the host; runoff given to fesomc_gpu_set_forcing is ignored.  The mode
+ * stays on for the life of the model.  Returns FESOMC_EINVAL when rivers
+ * are on and runoff_base is NULL. */
+int  fesomc_gpu_set_device_forcing(fesomc_model *m, const double *runoff_base, int32_t river_ramp);
 int  fesomc_gpu_step(fesomc_model *m, int32_t n_dt);
 int  fesomc_gpu_run(fesomc_model *m, int32_t n_dt0, int32_t nsteps);
 int  fesomc_gpu_sync_to_host(fesomc_model *m, uint32_t field_mask, fesomc_state *state);

@@ -12,11 +12,12 @@
  * (Fortran literals without _WP are REAL(4) constants promoted to REAL(8))
  * and its quirks.  Compile with -ffp-contract=off so no FMA is introduced.
  *
- * One deliberate departure: the logarithm of the turbulence closure's bottom
- * boundary value (fv_mixing.F90:238) is fesomc_log (an IEEE-only evaluation
- * shared with the device kernels, within one ulp of the C library's log)
- * rather than libm's log, so that the device path can be held to exact
- * equality at every step count.
+ * Two deliberate departures: the logarithm of the turbulence closure's
+ * bottom boundary value (fv_mixing.F90:238) is fesomc_log, and the cosine of
+ * the harmonic open-boundary elevation (fv_average_dynamic.F90:204-205) is
+ * fesomc_cos: IEEE-only evaluations shared with the device kernels, each
+ * within one ulp of the C library's function, rather than libm's, so that
+ * the device path can be held to exact equality at every step count.
  *
  * Parity pins: the mesh arrays it consumes are pinned against the
  * reference's edges.out / edge_tri.out (LE_medium test case); the whole time
@@ -35,6 +36,7 @@
 
 #include "../include/fesomc_gpu.h"
 #include "../fesom-c_b200/csrc/fesomc_log.h"
+#include "../fesom-c_b200/csrc/fesomc_trig.h"
 
 /* ---------------------------------------------------------------- consts */
 static const double WP_PI = 3.14159265358979;   /* fv_var.F90:8 */
@@ -143,8 +145,9 @@ static double densityJM(double t, double s, double pz, double density_0) {
     return rhopot * bulk / (bulk + 0.1 * pz) - density_0;
 }
 
-/* the shared logarithm, exported for its accuracy test */
+/* the shared logarithm and cosine, exported for their accuracy tests */
 double oracle_log(double x) { return fesomc_log(x); }
+double oracle_cos(double x) { return fesomc_cos(x); }
 
 double oracle_densityJM(double t, double s, double pz, double density_0) {
     return densityJM(t, s, pz, density_0);
@@ -274,7 +277,7 @@ static void compute_ssh_rhs_elem(oracle_model *m) {
             int n = m->in_obn[i - 1], q = i;
             for (int j = 1; j <= 12; ++j)
                 N1(m->ssh_rhs, n) = N1(m->ssh_rhs, n) + m->amp_factor[j - 1] * AMPT(q, j)
-                    * cos((m->time_2D - m->p.time_jd0 * 86400.0) * 2.0 * WP_PI / (HARM_PERIOD[j - 1] * 3600.0)
+                    * fesomc_cos((m->time_2D - m->p.time_jd0 * 86400.0) * 2.0 * WP_PI / (HARM_PERIOD[j - 1] * 3600.0)
                           - (FAZT(q, j) + m->phy_factor[j - 1]));
             if (!m->p.restart)
                 if (m->time_jd - m->p.time_jd0 < 10.0)

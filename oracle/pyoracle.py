@@ -51,6 +51,8 @@ def load(abi):
         lib.oracle_densityJM.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
         lib.oracle_log.restype = C.c_double
         lib.oracle_log.argtypes = [C.c_double]
+        lib.oracle_cos.restype = C.c_double
+        lib.oracle_cos.argtypes = [C.c_double]
         _lib = lib
     return _lib
 

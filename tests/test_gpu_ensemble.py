@@ -28,6 +28,8 @@ def _alone(case, steps):
     g = model.GpuModel(case)
     try:
         g.set_forcing(case.forcing_fn(1, cases.advance_time(g.time_jd, case.params.dt)))
+        base = np.ascontiguousarray(case.forcing_fn(1, case.params.time_jd0 + 20.0)["runoff_rivers"])
+        abi.check(g.lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base), 1), "fesomc_gpu_set_device_forcing")
         abi.check(g.lib.fesomc_gpu_run(g.h, 0, steps), "fesomc_gpu_run")
         return g.state()
     finally:

@@ -143,3 +143,24 @@ def test_shared_log_within_one_ulp_of_libm(mods):
     assert lib.oracle_log(0.0) == -math.inf
     assert math.isnan(lib.oracle_log(-1.0)) and math.isnan(lib.oracle_log(math.nan))
     assert lib.oracle_log(math.inf) == math.inf
+
+
+def test_shared_cos_within_one_ulp_of_libm(mods):
+    """fesomc_cos (the IEEE-only cosine of the harmonic open-boundary
+    elevation, shared by the oracle, the host forcing path and the device
+    forcing kernel) against the C library's cos: at most one ulp apart over
+    the phases a tide reaches, NaN beyond its range."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(-1000.0, 1000.0, 20000), rng.uniform(-4.0, 4.0, 20000),
+                         rng.uniform(-1.5e6, 1.5e6, 5000), [0.0, 1e-300, math.pi / 2, math.pi, -math.pi]])
+    ours = np.array([lib.oracle_cos(float(x)) for x in xs])
+    ref = np.array([math.cos(float(x)) for x in xs])
+    ulps = np.abs(ours.view(np.int64) - ref.view(np.int64))
+    # near a zero of cos an ulp of the result is tiny: compare those absolutely
+    ok = (ulps <= 1) | (np.abs(ours - ref) <= 2.3e-16)
+    assert ok.all()
+    assert np.mean(ulps != 0) < 0.1
+    assert lib.oracle_cos(0.0) == 1.0
+    assert math.isnan(lib.oracle_cos(2e6)) and math.isnan(lib.oracle_cos(math.inf))
