@@ -94,6 +94,23 @@ struct fesomc_model {
     size_t stage_len = 0;
     double *h_runoff = nullptr;  // host copy of current runoff
     bool runoff_dirty = false;
+    // asynchronous snapshots (fesomc_gpu_snapshot_begin / _end)
+    struct Snap {
+        double *dst;                  // caller's array (FP64)
+        void *dev_copy;
+        float *pinned32;              // FP32 fields: pinned staging, converted in _end
+        size_t count;
+    };
+    std::vector<Snap> snaps;          // fields of the snapshot in flight
+    std::vector<std::pair<void *, float *>> snap_bufs;  // (device copy, FP32 staging) per field slot
+    std::vector<size_t> snap_bytes;
+    std::vector<std::pair<void *, size_t>> registered;  // caller arrays page-locked for direct copies
+    fesomc_state *snap_state = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_taken = nullptr, snap_done = nullptr;
+    bool snap_pending = false;
+    double snap_time_jd = 0.0;
+    int snap_lfirst = 0;
     // forcing on the device (fesomc_gpu_set_device_forcing)
     bool dev_forcing = false;
     int river_ramp = 0;
@@ -1047,6 +1064,85 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
     return FESOMC_OK;
 }
 
+int fesomc_gpu_snapshot_begin(fesomc_model *m, uint32_t mask, fesomc_state *st) {
+    if (!m || !st) return FESOMC_EINVAL;
+    if (m->snap_pending) return FESOMC_ESTATE;
+    if (!m->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&m->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&m->snap_taken, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&m->snap_done, cudaEventDisableTiming));
+    }
+    const std::vector<FieldRef> table = field_table(m);
+    if (m->snap_bufs.size() < table.size()) {
+        m->snap_bufs.resize(table.size(), {nullptr, nullptr});
+        m->snap_bytes.resize(table.size(), 0);
+    }
+    m->snaps.clear();
+    // device-to-device copies on the step stream: the state after every step
+    // enqueued so far, taken without waiting for the host
+    for (size_t i = 0; i < table.size(); ++i) {
+        const FieldRef &f = table[i];
+        double *dst = st->*(f.host);
+        if (!(f.group & mask) || !dst) continue;
+        const size_t bytes = f.count * (f.f32 ? sizeof(float) : sizeof(double));
+        if (m->snap_bytes[i] != bytes) {
+            unsigned char *dc = nullptr;
+            int rc = dalloc(m, &dc, bytes);
+            if (rc) return rc;
+            float *hp = nullptr;
+            if (f.f32 && cudaMallocHost(&hp, bytes) != cudaSuccess) return FESOMC_ENOMEM;
+            m->snap_bufs[i] = {dc, hp};
+            m->snap_bytes[i] = bytes;
+        }
+        if (!f.f32) {
+            // the caller's array receives the copy directly: page-lock it once
+            bool known = false;
+            for (auto &r : m->registered) known |= (r.first == (void *)dst && r.second >= bytes);
+            if (!known) {
+                // an array that shares pages with one registered already
+                // cannot be registered; its copy then runs unlocked (the
+                // driver stages it), which is slower but correct
+                if (cudaHostRegister(dst, f.count * sizeof(double), cudaHostRegisterDefault) == cudaSuccess)
+                    m->registered.push_back({dst, f.count * sizeof(double)});
+                else
+                    (void)cudaGetLastError();
+            }
+        }
+        CK(cudaMemcpyAsync(m->snap_bufs[i].first, f.dev, bytes, cudaMemcpyDeviceToDevice, m->stream));
+        m->snaps.push_back({dst, m->snap_bufs[i].first, f.f32 ? m->snap_bufs[i].second : nullptr, f.count});
+    }
+    CK(cudaEventRecord(m->snap_taken, m->stream));
+    // device-to-host copies on the copy stream, overlapping the next steps
+    CK(cudaStreamWaitEvent(m->copy_stream, m->snap_taken, 0));
+    for (const auto &sn : m->snaps) {
+        if (sn.pinned32)
+            CK(cudaMemcpyAsync(sn.pinned32, sn.dev_copy, sn.count * sizeof(float), cudaMemcpyDeviceToHost,
+                               m->copy_stream));
+        else
+            CK(cudaMemcpyAsync(sn.dst, sn.dev_copy, sn.count * sizeof(double), cudaMemcpyDeviceToHost,
+                               m->copy_stream));
+    }
+    CK(cudaEventRecord(m->snap_done, m->copy_stream));
+    m->snap_state = st;
+    m->snap_time_jd = m->time_jd;
+    m->snap_lfirst = m->lfirst;
+    m->snap_pending = true;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_snapshot_end(fesomc_model *m) {
+    if (!m) return FESOMC_EINVAL;
+    if (!m->snap_pending) return FESOMC_ESTATE;
+    CK(cudaEventSynchronize(m->snap_done));
+    m->snap_pending = false;
+    for (const auto &sn : m->snaps)
+        if (sn.pinned32)
+            for (size_t i = 0; i < sn.count; ++i) sn.dst[i] = (double)sn.pinned32[i];
+    m->snap_state->time_jd = m->snap_time_jd;
+    m->snap_state->lfirst = m->snap_lfirst;
+    return FESOMC_OK;
+}
+
 int fesomc_gpu_energy(fesomc_model *m, double *eout) {
     if (!m || !eout) return FESOMC_EINVAL;
     if (m->fp32) fesomc::f32::launch_energy(m->d32, m->d_epart, m->d_eout, m->stream);
@@ -1078,6 +1174,13 @@ int fesomc_gpu_finalize(fesomc_model *m) {
         if (m->h_stage[i]) cudaFreeHost(m->h_stage[i]);
         if (m->stage_ev[i]) cudaEventDestroy(m->stage_ev[i]);
     }
+    if (m->copy_stream) cudaStreamSynchronize(m->copy_stream);
+    for (auto &b : m->snap_bufs)
+        if (b.second) cudaFreeHost(b.second);
+    for (auto &r : m->registered) cudaHostUnregister(r.first);
+    if (m->snap_taken) cudaEventDestroy(m->snap_taken);
+    if (m->snap_done) cudaEventDestroy(m->snap_done);
+    if (m->copy_stream) cudaStreamDestroy(m->copy_stream);
     if (m->h_runoff) cudaFreeHost(m->h_runoff);
     if (m->h_status) cudaFreeHost(m->h_status);
     if (m->h_notconv) cudaFreeHost(m->h_notconv);

@@ -84,6 +84,8 @@ SIGNATURES = {
     "fesomc_gpu_run": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "fesomc_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
     "fesomc_gpu_sync_from_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
+    "fesomc_gpu_snapshot_begin": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
+    "fesomc_gpu_snapshot_end": (C.c_int, [C.c_void_p]),
     "fesomc_gpu_energy": (C.c_int, [C.c_void_p, f64p]),
     "fesomc_gpu_last_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), i32p]),
     "fesomc_gpu_finalize": (C.c_int, [C.c_void_p]),

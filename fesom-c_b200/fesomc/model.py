@@ -70,6 +70,24 @@ class GpuModel:
         abi.check(self.lib.fesomc_gpu_energy(self.h, C.byref(e)), "fesomc_gpu_energy")
         return e.value
 
+    def snapshot_begin(self, mask=abi.F_ALL):
+        """Start an asynchronous copy of the masked fields (state after every
+        step enqueued so far) into host arrays this object keeps (page-locked
+        by the library on first use); stepping may go on meanwhile."""
+        if getattr(self, "_snap", None) is None:
+            arrays = {k: np.empty_like(v) for k, v in self.case.state0.items()}
+            self._snap = (arrays, self.case.state_struct(arrays, 0.0))
+        abi.check(self.lib.fesomc_gpu_snapshot_begin(self.h, mask, C.byref(self._snap[1])),
+                  "fesomc_gpu_snapshot_begin")
+
+    def snapshot_end(self):
+        """Wait for the snapshot started by snapshot_begin and return a copy."""
+        abi.check(self.lib.fesomc_gpu_snapshot_end(self.h), "fesomc_gpu_snapshot_end")
+        arrays, st = self._snap
+        out = {k: v.copy() for k, v in arrays.items()}
+        out["_time_jd"] = st.time_jd
+        return out
+
     def status(self):
         s, nc = C.c_uint32(), C.c_int32()
         self.lib.fesomc_gpu_last_status(self.h, C.byref(s), C.byref(nc))

@@ -230,6 +230,22 @@ int  fesomc_gpu_set_device_forcing(fesomc_model *m, const double *runoff_base, i
 int  fesomc_gpu_step(fesomc_model *m, int32_t n_dt);
 int  fesomc_gpu_run(fesomc_model *m, int32_t n_dt0, int32_t nsteps);
 int  fesomc_gpu_sync_to_host(fesomc_model *m, uint32_t field_mask, fesomc_state *state);
+/* Asynchronous output, the non-blocking counterpart of fesomc_gpu_sync_to_host
+ * for the output and restart writers (ncoutput(mpi)_do,
+ * src/fv_ncoutputmpi.F90:1164; write_restart_separate, src/fv_restart.F90:399):
+ * _begin takes a device-side copy of the masked fields after every step
+ * enqueued so far and starts copying it, on a second stream, into the
+ * non-NULL arrays of state (FP64, reference layout), then returns; the
+ * caller may keep stepping while the copy runs, and must not read or free
+ * those arrays before _end.  _end waits for the copy, converts the FP32
+ * fields of the FP32 form, and sets state's time_jd and lfirst to the
+ * snapshot's.  The destination arrays are page-locked (cudaHostRegister) on
+ * their first use and stay so until fesomc_gpu_finalize, so pass the same
+ * arrays each time (the driver's module arrays) and keep them allocated
+ * until then.  One snapshot at a time: _begin while one is pending, or _end
+ * without one, returns FESOMC_ESTATE. */
+int  fesomc_gpu_snapshot_begin(fesomc_model *m, uint32_t field_mask, fesomc_state *state);
+int  fesomc_gpu_snapshot_end(fesomc_model *m);
 int  fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t field_mask, const fesomc_state *state);
 int  fesomc_gpu_energy(fesomc_model *m, double *eout);
 int  fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv_columns);
