@@ -280,6 +280,127 @@ __global__ void k_adv3_edge(Dev d) {
 }
 
 // ---------------------------------------------------------------------------
+// biharmonic_viscosity (fv_viscosity.F90:104-334): two Laplacians of the
+// velocity, each an edge flux of the normal velocity gradient (the mean of
+// the two elements' gradients with its tangential part replaced by the
+// difference quotient) times Jd, gathered per element in edge order.
+// bih_edge: the flux of every (edge, level), internal and boundary edges;
+// pass 2 also scales it by the edge's sponge factor.
+// bih_uc: U_c = Ah * sum of the pass-1 fluxes (in U_puls / V_puls, free
+// until the sub-cycle).  bih_grad: vel_lapl_gradients (fv_gradients.F90:
+// 327-402) of U_c into the velocity-gradient arrays.  velrhs gathers the
+// pass-2 fluxes into U_rhs after the filter viscosity.
+// ---------------------------------------------------------------------------
+__global__ void k_bih_edge(Dev d, const real *U, const real *V, int pass2) {
+    const long long total = (long long)d.Ed * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const real2 dxy = d.edge_dxdy[ed];
+        const real jd = real(0.5) * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
+        const size_t i1 = (size_t)et.x * L + z;
+        real u1, v1;
+        if (ed < d.Ed_in) {
+            const size_t i2 = (size_t)et.y * L + z;
+            const real4 X = d.edge_cross[ed];
+            const real xe = dxy.x * kREarth * real(0.5) * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+            const real ye = dxy.y * kREarth;
+            real tx = -X.x + X.z;
+            real ty = -X.y + X.w;
+            const real tl = sqrt(tx * tx + ty * ty);
+            tx = tx / tl;
+            ty = ty / tl;
+            real g1 = real(0.5) * (d.vgux[i1] + d.vgux[i2]);
+            real g2 = real(0.5) * (d.vguy[i1] + d.vguy[i2]);
+            real tt = g1 * tx + g2 * ty - (U[i2] - U[i1]) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            u1 = (g1 * ye - g2 * xe);
+            g1 = real(0.5) * (d.vgvx[i1] + d.vgvx[i2]);
+            g2 = real(0.5) * (d.vgvy[i1] + d.vgvy[i2]);
+            tt = g1 * tx + g2 * ty - (V[i2] - V[i1]) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            v1 = (g1 * ye - g2 * xe);
+        } else {
+            const real xe = dxy.x * kREarth * d.elem_cos[et.x];
+            const real ye = dxy.y * kREarth;
+            u1 = (d.vgux[i1]) * ye - (d.vguy[i1]) * xe;
+            v1 = (d.vgvx[i1]) * ye - (d.vgvy[i1]) * xe;
+        }
+        real fu = u1 * jd, fv = v1 * jd;
+        if (pass2) {
+            const real acc = (d.ac[nn.x] + d.ac[nn.y]) / real(2.0);
+            fu = fu * acc;
+            fv = fv * acc;
+        }
+        d.bihfl[ii] = make_real2(fu, fv);
+    }
+}
+
+__global__ void k_bih_uc(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int4 se = d.elem_sedges[e];
+        const int codes[4] = {se.x, se.y, se.z, se.w};
+        real uc = real(0.0), vc = real(0.0);
+        for (int c = 0; c < 4; ++c) {
+            const int code = codes[c];
+            if (code < 0) break;
+            const real2 f = d.bihfl[(size_t)(code >> 1) * L + z];
+            if (code & 1) { uc = uc - f.x; vc = vc - f.y; }
+            else { uc = uc + f.x; vc = vc + f.y; }
+        }
+        const real Ah = -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
+        d.U_puls[ii] = uc * (Ah);
+        d.V_puls[ii] = vc * (Ah);
+    }
+}
+
+__global__ void k_bih_grad(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    const int L = d.L;
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int4 en = d.elem_nodes[e];
+        const int4 nb = d.elem_nb[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const real4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const int jend = (en.x == en.w) ? 3 : 4;
+        const real u0 = d.U_puls[ii], v0 = d.V_puls[ii];
+        real a1 = real(0.0), a2 = real(0.0), a3 = real(0.0), a4 = real(0.0);
+        for (int j = 0; j < jend; ++j) {
+            const int e2 = nbs[j];
+            real u, v;
+            if (e2 >= 0) {
+                u = d.U_puls[(size_t)e2 * L + z] - u0;
+                v = d.V_puls[(size_t)e2 * L + z] - v0;
+            } else {
+                u = -real(2.0) * u0;
+                v = -real(2.0) * v0;
+            }
+            a1 = a1 + gxa[j] * u;
+            a2 = a2 + gya[j] * u;
+            a3 = a3 + gxa[j] * v;
+            a4 = a4 + gya[j] * v;
+        }
+        d.vgux[ii] = a1;
+        d.vguy[ii] = a2;
+        d.vgvx[ii] = a3;
+        d.vgvy[ii] = a4;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
 // level) with levels on consecutive lanes.  The loop runs over whole warps so
 // that the vertical flux at interface z+1 comes from the next lane.
@@ -338,6 +459,19 @@ __global__ void __launch_bounds__(256, FESOMC_FP32 ? 4 : 3) k_velrhs(Dev d, real
                 }
             ur = ur + d.tau_inv_filt * u1 * ar * je;
             vr = vr + d.tau_inv_filt * v1 * ar * je;
+        }
+        // biharmonic viscosity (fv_viscosity.F90:248-330): the pass-2 edge
+        // fluxes in edge order, internal edges then boundary edges
+        if (d.bih_3D) {
+            const int4 se = d.elem_sedges[e];
+            const int codes[4] = {se.x, se.y, se.z, se.w};
+            for (int c = 0; c < 4; ++c) {
+                const int code = codes[c];
+                if (code < 0) break;
+                const real2 f = d.bihfl[(size_t)(code >> 1) * L + z];
+                if (code & 1) { ur = ur - f.x; vr = vr - f.y; }
+                else { ur = ur + f.x; vr = vr + f.y; }
+            }
         }
         // vertical advection (fv_advection.F90:354-469): flux at interface z
         // here, at z+1 from the next lane (same element) or computed
@@ -661,6 +795,12 @@ void launch_velgrad3d(const Dev &d, cudaStream_t s) {
 }
 void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_bih(const Dev &d, cudaStream_t s) {
+    k_bih_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d, d.U_n, d.V_n, 0);
+    k_bih_uc<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    k_bih_grad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    k_bih_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d, d.U_puls, d.V_puls, 1);
 }
 void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
     k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);

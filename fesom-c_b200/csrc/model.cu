@@ -31,6 +31,7 @@ namespace fesomc {
     void launch_velgrad3d(const Dev &, cudaStream_t); \
     void launch_adv3_edge(const Dev &, cudaStream_t); \
     void launch_velrhs(const Dev &, real, cudaStream_t); \
+    void launch_bih(const Dev &, cudaStream_t); \
     void launch_implvisc(const Dev &, cudaStream_t); \
     void launch_jac_swap(const Dev &, cudaStream_t); \
     void launch_je(const Dev &, cudaStream_t); \
@@ -262,7 +263,7 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
     for (int k = 0; k < L; ++k) dsig[k] = sig[k] - sig[k + 1];
     int rc;
     if ((rc = upload(m, &d.sig, sig)) || (rc = upload(m, &d.dsig, dsig))) return rc;
-    std::vector<int4> en(E), nb(E), ee(E), iel(E);
+    std::vector<int4> en(E), nb(E), ee(E), iel(E), sel(E);
     std::vector<double4> wcv(E), gsx(E), gsy(E), gvx(E), gvy(E);
     std::vector<double> eacc(E), bpf(E);
     for (int e = 0; e < E; ++e) {
@@ -305,6 +306,21 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
         int tmp[4] = {-1, -1, -1, -1};
         for (int t = 0; t < nl; ++t) tmp[t] = list[t];
         iel[e] = make_int4(tmp[0], tmp[1], tmp[2], tmp[3]);
+        // all edges of the element (boundary ones too, side 0), sorted
+        int all[4], na = 0;
+        for (int j = 0; j < q1; ++j) {
+            const int edg = g[j];
+            bool dup = false;
+            for (int t = 0; t < na; ++t) dup |= ((all[t] >> 1) == edg - 1);
+            if (dup) continue;
+            const int side = (msh->edge_tri[2 * (edg - 1)] == e + 1) ? 0 : 1;
+            all[na++] = ((edg - 1) << 1) | side;
+        }
+        for (int a = 1; a < na; ++a)
+            for (int b2 = a; b2 > 0 && all[b2 - 1] > all[b2]; --b2) std::swap(all[b2 - 1], all[b2]);
+        int tmp2[4] = {-1, -1, -1, -1};
+        for (int t = 0; t < na; ++t) tmp2[t] = all[t];
+        sel[e] = make_int4(tmp2[0], tmp2[1], tmp2[2], tmp2[3]);
     }
     std::vector<int2> edn(Ed), edt(Ed), eud(Ed);
     std::vector<double2> exy(Ed);
@@ -380,7 +396,8 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
     std::vector<double> ea(msh->elem_area, msh->elem_area + E), ec(msh->elem_cos, msh->elem_cos + E),
         cor(msh->coriolis, msh->coriolis + E);
     if ((rc = upload(m, &d.elem_nodes, en)) || (rc = upload(m, &d.elem_nb, nb)) || (rc = upload(m, &d.elem_edges, ee)) ||
-        (rc = upload(m, &d.elem_iedges, iel)) || (rc = upload(m, &d.edge_nodes, edn)) ||
+        (rc = upload(m, &d.elem_iedges, iel)) || (rc = upload(m, &d.elem_sedges, sel)) ||
+        (rc = upload(m, &d.edge_nodes, edn)) ||
         (rc = upload(m, &d.edge_tri, edt)) || (rc = upload(m, &d.edge_updn, eud)) ||
         (rc = upload(m, &d.node_eptr, eptr)) || (rc = upload(m, &d.node_eidx, eidx)) ||
         (rc = upload(m, &d.node_nptr, nptr)) || (rc = upload(m, &d.node_nidx, nidx)) ||
@@ -441,6 +458,7 @@ int alloc_3d(fesomc_model *m, D &d) {
     int rc = 0;
     if ((rc = dalloc(m, &d.Fp, E))) return rc;
     if ((rc = dalloc(m, &d.adv3, L * (size_t)d.Ed_in))) return rc;
+    if (m->p.bih_3D && (rc = dalloc(m, &d.bihfl, L * (size_t)d.Ed))) return rc;
     decltype(&d.U_n) le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
                              &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv,
                              &d.Je, &d.Ze, &d.ZBe};
@@ -499,6 +517,7 @@ int setup_f32_view(fesomc_model *m) {
     b.N = a.N; b.E = a.E; b.Ed = a.Ed; b.Ed_in = a.Ed_in; b.L = a.L; b.NS = a.NS;
     b.nobn = a.nobn; b.n_rivers = a.n_rivers;
     b.elem_nodes = a.elem_nodes; b.elem_nb = a.elem_nb; b.elem_edges = a.elem_edges; b.elem_iedges = a.elem_iedges;
+    b.elem_sedges = a.elem_sedges;
     b.edge_nodes = a.edge_nodes; b.edge_tri = a.edge_tri; b.edge_updn = a.edge_updn;
     b.node_eptr = a.node_eptr; b.node_eidx = a.node_eidx; b.node_nptr = a.node_nptr; b.node_nidx = a.node_nidx;
     b.node_bptr = a.node_bptr; b.node_bidx = a.node_bidx; b.node_rptr = a.node_rptr; b.node_ridx = a.node_ridx;
@@ -541,6 +560,7 @@ void set_params(D &d, const fesomc_params &p) {
     d.tracer_adv = p.tracer_adv; d.ver_mix = p.ver_mix; d.filt_2D = p.filt_2D; d.filt_3D = p.filt_3D;
     d.wet_dry_on = p.wet_dry_on; d.key_rivers = p.key_rivers; d.TF_presence = p.TF_presence; d.cl_relax = p.cl_relax;
     d.beta_d = p.beta; d.Dmin_d = p.Dmin; d.dt_2D_d = p.dt_2D;
+    d.bih_3D = p.bih_3D; d.Abh0 = p.Abh0;
 }
 
 // Algorithmic bytes per launch of every kernel: each array the kernel must
@@ -551,6 +571,9 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     const Dev &d = m->d;
     const double N = d.N, E = d.E, Ed = d.Ed, Ei = d.Ed_in, L = d.L, NS = d.NS;
     const double nnz_ne = (double)(2 * d.Ed);  // node->edge incidences
+    if (k == "biharmonic")   // two edge passes, U_c, its gradients
+        return 2 * (L * Ed * 16 + Ed * (8 + 8 + 16 + 32 + 16) + L * E * 32 + L * E * 16) + L * E * (16 + 16) +
+               E * 16 + L * E * (16 + 32) + E * (16 + 16 + 64) + N * 16;
     if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
     if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
@@ -701,6 +724,7 @@ int enqueue_step(fesomc_model *m, double ff) {
     rec(m, "velgrad3d", [&] { K3(launch_velgrad3d, s); });
     n += 1;
     if (d.mom_adv_3D == 1) { rec(m, "adv3_edge", [&] { K3(launch_adv3_edge, s); }); n += 1; }
+    if (d.bih_3D) { rec(m, "biharmonic", [&] { K3(launch_bih, s); }); n += 4; }
     rec(m, "velrhs", [&] { K3(launch_velrhs, ff, s); });
     n += 1;
     if (d.im_vert_visc || d.im_vert_visc_fic) { rec(m, "implvisc", [&] { K3(launch_implvisc, s); }); n += 1; }
@@ -878,6 +902,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (par->mom_adv_2D != 2 && par->mom_adv_2D != 0) return FESOMC_EINVAL;
     if (par->mom_adv_3D != 1 && par->mom_adv_3D != 0) return FESOMC_EINVAL;
     if (par->fp32_form != 0 && par->fp32_form != 1) return FESOMC_EINVAL;
+    if (par->bih_3D != 0 && par->bih_3D != 1) return FESOMC_EINVAL;
+    if (par->bih_3D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;

@@ -105,6 +105,7 @@ def default_params(**kw):
     p.snul, p.z0b_min, p.z0s_min = 7.5e-4, 0.01, 0.02
     p.Pr_num, p.beta_scale, p.cka = 0.0001, 3.9, 0.4   # fv_var.F90:44,130,16
     p.tau_inv_filt, p.K_hor = 0.000046296, 0.010
+    p.bih_3D, p.Abh0 = 0, 1000.0                  # LE_medium fv_run.dat:150,160
     p.Cd_bz, p.Bp_bz = 10.0, 5.0
     p.clim_relax = 1.0 / (15.0 * 3600.0 * 24.0)
     p.relax2clim_ac = 1.0 / (60.0 * 3600.0 * 24.0)

@@ -147,11 +147,16 @@ typedef struct fesomc_params {
     int32_t harm_index[12];       /* 0-based index into the 12 reference waves  */
     /* Arithmetic form (no counterpart in the reference, which is FP64):
      * 0 = plain FP64 (bit-exact with the reference algorithm);
-     * 1 = FP32 form: level fields, mesh geometry and the 3D arithmetic
-     *     (fluxes, advection, viscosity, tracers, mixing) in FP32; the
-     *     barotropic sub-cycle (SSH / total depth accumulation, wet/dry
-     *     tests) and the energy integral stay FP64.                        */
+     * 1 = FP32 form: level fields, the 2D momentum, mesh geometry and the
+     *     flux / advection / viscosity / tracer / mixing arithmetic in FP32;
+     *     the elevation, SSH and total-depth accumulation, wet/dry tests
+     *     and the energy integral stay FP64.                                */
     int32_t fp32_form;
+    /* biharmonic viscosity of the 3D momentum (bih_3D, Abh0 of fv_run.dat,
+     * src/fv_read_run.F90:320-326,396-401; biharmonic_viscosity,
+     * src/fv_viscosity.F90:104-334)                                        */
+    int32_t bih_3D;
+    double Abh0;
 } fesomc_params;
 
 /*

@@ -982,6 +982,133 @@ static void momentum_vert_impl_visc_tmp(oracle_model *m) {
     }
 }
 
+/* biharmonic_viscosity, fv_viscosity.F90:104-334 (serial build), with
+ * vel_lapl_gradients, fv_gradients.F90:327-402.  Overwrites the velocity
+ * gradients with those of the Laplacian, as the reference does. */
+static void biharmonic_viscosity(oracle_model *m) {
+    const int L = m->L;
+    double *U_c = calloc((size_t)L * m->E, sizeof(double));
+    double *V_c = calloc((size_t)L * m->E, sizeof(double));
+    /* first Laplacian of (U_n, V_n): internal edges, then boundary edges */
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double tx = -ECR(1, ed) + ECR(3, ed);
+        double ty = -ECR(2, ed) + ECR(4, ed);
+        double tl = sqrt(tx * tx + ty * ty);
+        tx = tx / tl;
+        ty = ty / tl;
+        for (int z = 1; z <= L; ++z) {
+            double g1 = 0.5 * (F3(m->vgux, z, e1) + F3(m->vgux, z, e2));
+            double g2 = 0.5 * (F3(m->vguy, z, e1) + F3(m->vguy, z, e2));
+            double tt = g1 * tx + g2 * ty - (F3(m->U_n, z, e2) - F3(m->U_n, z, e1)) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            double u1 = (g1 * ye - g2 * xe);
+            g1 = 0.5 * (F3(m->vgvx, z, e1) + F3(m->vgvx, z, e2));
+            g2 = 0.5 * (F3(m->vgvy, z, e1) + F3(m->vgvy, z, e2));
+            tt = g1 * tx + g2 * ty - (F3(m->V_n, z, e2) - F3(m->V_n, z, e1)) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            double v1 = (g1 * ye - g2 * xe);
+            F3(U_c, z, e1) = F3(U_c, z, e1) + u1 * F3(m->Jd, z, ed);
+            F3(V_c, z, e1) = F3(V_c, z, e1) + v1 * F3(m->Jd, z, ed);
+            F3(U_c, z, e2) = F3(U_c, z, e2) - u1 * F3(m->Jd, z, ed);
+            F3(V_c, z, e2) = F3(V_c, z, e2) - v1 * F3(m->Jd, z, ed);
+        }
+    }
+    for (int ed = m->Ed_in + 1; ed <= m->Ed; ++ed) {
+        int e1 = EDT(1, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH * N1(m->elem_cos, e1);
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        for (int z = 1; z <= L; ++z) {
+            double u1 = (F3(m->vgux, z, e1)) * ye - (F3(m->vguy, z, e1)) * xe;
+            double v1 = (F3(m->vgvx, z, e1)) * ye - (F3(m->vgvy, z, e1)) * xe;
+            F3(U_c, z, e1) = F3(U_c, z, e1) + u1 * F3(m->Jd, z, ed);
+            F3(V_c, z, e1) = F3(V_c, z, e1) + v1 * F3(m->Jd, z, ed);
+        }
+    }
+    for (int el = 1; el <= m->E; ++el) {
+        double Ah = -m->p.Abh0 * sqrt(N1(m->elem_area, el) / m->p.scale_area) / m->p.scale_area;
+        for (int z = 1; z <= L; ++z) {
+            F3(U_c, z, el) = F3(U_c, z, el) * (Ah);
+            F3(V_c, z, el) = F3(V_c, z, el) * (Ah);
+        }
+    }
+    /* vel_lapl_gradients(U_c, V_c) */
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        for (int z = 1; z <= L; ++z) {
+            double g[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int j = 1; j <= jend; ++j) {
+                int el2 = ELNB(j, el);
+                double u, v;
+                if (el2 > 0) {
+                    u = F3(U_c, z, el2) - F3(U_c, z, el);
+                    v = F3(V_c, z, el2) - F3(V_c, z, el);
+                } else {
+                    u = -2.0 * F3(U_c, z, el);
+                    v = -2.0 * F3(V_c, z, el);
+                }
+                g[0] = g[0] + GV(j, el) * u;
+                g[1] = g[1] + GV(j + 4, el) * u;
+                g[2] = g[2] + GV(j, el) * v;
+                g[3] = g[3] + GV(j + 4, el) * v;
+            }
+            F3(m->vgux, z, el) = g[0];
+            F3(m->vguy, z, el) = g[1];
+            F3(m->vgvx, z, el) = g[2];
+            F3(m->vgvy, z, el) = g[3];
+        }
+    }
+    /* second Laplacian into U_rhs, V_rhs, scaled by the sponge factor */
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double tx = -ECR(1, ed) + ECR(3, ed);
+        double ty = -ECR(2, ed) + ECR(4, ed);
+        double tl = sqrt(tx * tx + ty * ty);
+        tx = tx / tl;
+        ty = ty / tl;
+        double acc = (N1(m->ac, EDN(1, ed)) + N1(m->ac, EDN(2, ed))) / 2.0;
+        for (int z = 1; z <= L; ++z) {
+            double g1 = 0.5 * (F3(m->vgux, z, e1) + F3(m->vgux, z, e2));
+            double g2 = 0.5 * (F3(m->vguy, z, e1) + F3(m->vguy, z, e2));
+            double tt = g1 * tx + g2 * ty - (F3(U_c, z, e2) - F3(U_c, z, e1)) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            double u1 = (g1 * ye - g2 * xe);
+            g1 = 0.5 * (F3(m->vgvx, z, e1) + F3(m->vgvx, z, e2));
+            g2 = 0.5 * (F3(m->vgvy, z, e1) + F3(m->vgvy, z, e2));
+            tt = g1 * tx + g2 * ty - (F3(V_c, z, e2) - F3(V_c, z, e1)) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            double v1 = (g1 * ye - g2 * xe);
+            F3(m->U_rhs, z, e1) = F3(m->U_rhs, z, e1) + u1 * F3(m->Jd, z, ed) * acc;
+            F3(m->V_rhs, z, e1) = F3(m->V_rhs, z, e1) + v1 * F3(m->Jd, z, ed) * acc;
+            F3(m->U_rhs, z, e2) = F3(m->U_rhs, z, e2) - u1 * F3(m->Jd, z, ed) * acc;
+            F3(m->V_rhs, z, e2) = F3(m->V_rhs, z, e2) - v1 * F3(m->Jd, z, ed) * acc;
+        }
+    }
+    for (int ed = m->Ed_in + 1; ed <= m->Ed; ++ed) {
+        int e1 = EDT(1, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH * N1(m->elem_cos, e1);
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double acc = (N1(m->ac, EDN(1, ed)) + N1(m->ac, EDN(2, ed))) / 2.0;
+        for (int z = 1; z <= L; ++z) {
+            double u1 = (F3(m->vgux, z, e1)) * ye - (F3(m->vguy, z, e1)) * xe;
+            double v1 = (F3(m->vgvx, z, e1)) * ye - (F3(m->vgvy, z, e1)) * xe;
+            F3(m->U_rhs, z, e1) = F3(m->U_rhs, z, e1) + u1 * F3(m->Jd, z, ed) * acc;
+            F3(m->V_rhs, z, e1) = F3(m->V_rhs, z, e1) + v1 * F3(m->Jd, z, ed) * acc;
+        }
+    }
+    free(U_c);
+    free(V_c);
+}
+
 /* compute_vel_rhs, fv_3D_vel.F90:1-197 (key_atm off) */
 static void compute_vel_rhs(oracle_model *m) {
     const int L = m->L;
@@ -1009,6 +1136,7 @@ static void compute_vel_rhs(oracle_model *m) {
     vel_gradients(m);
     if (m->p.mom_adv_3D == 1) momentum_adv_upwind(m);
     if (m->p.filt_3D) viscosity_filt_3D(m);
+    if (m->p.bih_3D) biharmonic_viscosity(m);
     if (m->p.vert_adv == 1) momentum_vert_adv_upwind(m);
     double ff = 1.5 + eps;
     if (m->lfirst) { ff = 1.0; m->lfirst = 0; }

@@ -68,3 +68,10 @@ def test_fp32_form_other_tracer_schemes(mods, scheme):
     b, _ = run(mods, cases.estuary("small", tracer_adv=adv), 30, True)
     assert np.max(np.abs(a["TF"] - b["TF"])) < TS_MAX
     assert np.max(np.abs(a["SF"] - b["SF"])) < TS_MAX
+
+
+def test_fp32_form_biharmonic(mods):
+    a, _ = run(mods, mods[1].estuary("small", bih_3D=1, Abh0=1e4), 30, False)
+    b, _ = run(mods, mods[1].estuary("small", bih_3D=1, Abh0=1e4), 30, True)
+    assert np.max(np.abs(a["TF"] - b["TF"])) < TS_MAX
+    assert np.max(np.abs(a["U_n"] - b["U_n"])) < 1e-3

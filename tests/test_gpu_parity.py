@@ -210,6 +210,23 @@ def test_sync_roundtrip(mods):
     g.close()
 
 
+def test_estuary_biharmonic_bit_exact(mods):
+    """biharmonic_viscosity (two edge Laplacians, vel_lapl_gradients) on the
+    small estuary with the sponge factor, 30 steps."""
+    abi, cases, model, pyoracle = mods
+    bad, eg, eo = run_pair(mods, cases.estuary("small", bih_3D=1, Abh0=1e4), 30)
+    assert bad == []
+
+
+def test_le_biharmonic_bit_exact(mods):
+    abi, cases, model, pyoracle = mods
+    case = cases.le_medium()
+    case.params.Mt = 4
+    case.params.bih_3D = 1
+    bad, _, _ = run_pair(mods, case, 20)
+    assert bad == []
+
+
 def test_cfg0_bit_exact(mods):
     """The reference's CPU-sized configuration (201 x 81 nodes at 300 m, 11
     sigma levels, MUSCL, wetting/drying, tide, river), 100 internal steps."""

@@ -164,3 +164,21 @@ def test_shared_cos_within_one_ulp_of_libm(mods):
     assert np.mean(ulps != 0) < 0.1
     assert lib.oracle_cos(0.0) == 1.0
     assert math.isnan(lib.oracle_cos(2e6)) and math.isnan(lib.oracle_cos(math.inf))
+
+
+def test_estuary_biharmonic_oracle(mods):
+    """biharmonic_viscosity (bih_3D): active, finite, and linear in Abh0 for
+    a small viscosity (the damping of a fixed flow field doubles with it)."""
+    abi, cases, pyoracle = mods
+    out = {}
+    for ab in (0.0, 1e3, 1e4):
+        c = cases.estuary("small", bih_3D=1 if ab else 0, Abh0=ab if ab else 1000.0)
+        o = pyoracle.Oracle(c, abi, cases)
+        o.step(30)
+        out[ab] = o.state()
+        o.close()
+    d3 = np.abs(out[1e3]["U_n"] - out[0.0]["U_n"]).max()
+    d4 = np.abs(out[1e4]["U_n"] - out[0.0]["U_n"]).max()
+    assert np.isfinite(out[1e4]["U_n"]).all()
+    assert d3 > 0.0
+    assert 5.0 < d4 / d3 < 15.0
