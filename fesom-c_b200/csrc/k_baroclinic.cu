@@ -280,18 +280,24 @@ __global__ void k_adv3_edge(Dev d) {
 }
 
 // ---------------------------------------------------------------------------
-// biharmonic_viscosity (fv_viscosity.F90:104-334): two Laplacians of the
-// velocity, each an edge flux of the normal velocity gradient (the mean of
-// the two elements' gradients with its tangential part replaced by the
-// difference quotient) times Jd, gathered per element in edge order.
-// bih_edge: the flux of every (edge, level), internal and boundary edges;
-// pass 2 also scales it by the edge's sponge factor.
-// bih_uc: U_c = Ah * sum of the pass-1 fluxes (in U_puls / V_puls, free
-// until the sub-cycle).  bih_grad: vel_lapl_gradients (fv_gradients.F90:
-// 327-402) of U_c into the velocity-gradient arrays.  velrhs gathers the
-// pass-2 fluxes into U_rhs after the filter viscosity.
+// biharmonic_viscosity (fv_viscosity.F90:104-334) and its sub-step-1 twin
+// biharmonic_viscosity_3D_to_2D (:964-1219): two Laplacians of a velocity,
+// each an edge flux of the normal velocity gradient (the mean of the two
+// elements' gradients with its tangential part replaced by the difference
+// quotient), gathered per element in edge order (internal edges, then
+// boundary edges).
+// bih_edge: the flux of every (edge, level); mode 0 times Jd, mode 1 times
+// Jd and the edge's sponge factor, mode 2 plain.
+// bih_uc: U_c = Ah * sum of the mode-0 fluxes; Ah = -Abh0 sqrt(area/s)/s
+// (mode 0), -acc Abh0 sqrt(area/s)/s (mode 1, the 3D-to-2D form; its Visc
+// term is zero on this path, h_viscosity only runs with the sediment model).
+// bih_grad: vel_lapl_gradients (fv_gradients.F90:327-402) of U_c into the
+// velocity-gradient arrays.  velgrad_puls: vel_gradients_puls
+// (fv_gradients.F90:404-496, free slip) of U_puls.
+// velrhs gathers the mode-1 fluxes into U_rhs after the filter viscosity;
+// p1_elem gathers the mode-2 fluxes, times Je, into U_rhs_2D_3D.
 // ---------------------------------------------------------------------------
-__global__ void k_bih_edge(Dev d, const real *U, const real *V, int pass2) {
+__global__ void k_bih_edge(Dev d, const real *U, const real *V, int mode) {
     const long long total = (long long)d.Ed * d.L;
     const int L = d.L;
     GRID_LOOP(ii, total) {
@@ -300,7 +306,6 @@ __global__ void k_bih_edge(Dev d, const real *U, const real *V, int pass2) {
         const int2 nn = d.edge_nodes[ed];
         const int2 et = d.edge_tri[ed];
         const real2 dxy = d.edge_dxdy[ed];
-        const real jd = real(0.5) * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
         const size_t i1 = (size_t)et.x * L + z;
         real u1, v1;
         if (ed < d.Ed_in) {
@@ -331,39 +336,40 @@ __global__ void k_bih_edge(Dev d, const real *U, const real *V, int pass2) {
             u1 = (d.vgux[i1]) * ye - (d.vguy[i1]) * xe;
             v1 = (d.vgvx[i1]) * ye - (d.vgvy[i1]) * xe;
         }
-        real fu = u1 * jd, fv = v1 * jd;
-        if (pass2) {
-            const real acc = (d.ac[nn.x] + d.ac[nn.y]) / real(2.0);
-            fu = fu * acc;
-            fv = fv * acc;
+        real fu = u1, fv = v1;
+        if (mode != 2) {
+            const real jd = real(0.5) * (jc_of(d, jac_a(d, d.eta_jac, nn.x), z) + jc_of(d, jac_a(d, d.eta_jac, nn.y), z));
+            fu = u1 * jd;
+            fv = v1 * jd;
+            if (mode == 1) {
+                const real acc = (d.ac[nn.x] + d.ac[nn.y]) / real(2.0);
+                fu = fu * acc;
+                fv = fv * acc;
+            }
         }
         d.bihfl[ii] = make_real2(fu, fv);
     }
 }
 
-__global__ void k_bih_uc(Dev d) {
+__global__ void k_bih_uc(Dev d, int mode) {
     const long long total = (long long)d.E * d.L;
     const int L = d.L;
     GRID_LOOP(ii, total) {
         const int e = (int)(ii / L);
         const int z = (int)(ii % L);
-        const int4 se = d.elem_sedges[e];
-        const int codes[4] = {se.x, se.y, se.z, se.w};
-        real uc = real(0.0), vc = real(0.0);
-        for (int c = 0; c < 4; ++c) {
-            const int code = codes[c];
-            if (code < 0) break;
-            const real2 f = d.bihfl[(size_t)(code >> 1) * L + z];
-            if (code & 1) { uc = uc - f.x; vc = vc - f.y; }
-            else { uc = uc + f.x; vc = vc + f.y; }
-        }
-        const real Ah = -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
-        d.U_puls[ii] = uc * (Ah);
-        d.V_puls[ii] = vc * (Ah);
+        const real2 c = bih_gather(d, e, z);
+        const real Ah = (mode == 0) ? -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area
+                                    : -d.elem_acc[e] * d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
+        d.bihU[ii] = c.x * (Ah);
+        d.bihV[ii] = c.y * (Ah);
     }
 }
 
-__global__ void k_bih_grad(Dev d) {
+// least-squares gradients of (U, V) per (element, level); the boundary
+// neighbour is -2 U (vel_lapl_gradients) or the free-slip mirror
+// (vel_gradients_puls)
+template <bool FREE_SLIP>
+__global__ void k_bih_grad(Dev d, const real *U, const real *V) {
     const long long total = (long long)d.E * d.L;
     const int L = d.L;
     GRID_LOOP(ii, total) {
@@ -371,19 +377,29 @@ __global__ void k_bih_grad(Dev d) {
         const int z = (int)(ii % L);
         const int4 en = d.elem_nodes[e];
         const int4 nb = d.elem_nb[e];
+        const int4 ee = d.elem_edges[e];
         const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
         const real4 gx = d.gv_x[e], gy = d.gv_y[e];
         const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
         const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
         const int jend = (en.x == en.w) ? 3 : 4;
-        const real u0 = d.U_puls[ii], v0 = d.V_puls[ii];
+        const real u0 = U[ii], v0 = V[ii];
         real a1 = real(0.0), a2 = real(0.0), a3 = real(0.0), a4 = real(0.0);
         for (int j = 0; j < jend; ++j) {
             const int e2 = nbs[j];
             real u, v;
             if (e2 >= 0) {
-                u = d.U_puls[(size_t)e2 * L + z] - u0;
-                v = d.V_puls[(size_t)e2 * L + z] - v0;
+                u = U[(size_t)e2 * L + z] - u0;
+                v = V[(size_t)e2 * L + z] - v0;
+            } else if (FREE_SLIP) {
+                const real2 dxy = d.edge_dxdy[eds[j]];
+                const real zc1 = dxy.x * d.elem_cos[e], zc2 = dxy.y;
+                const real un = -real(2.0) * (u0 * zc2 - v0 * zc1) / (zc1 * zc1 + zc2 * zc2);
+                const real ua = u0 + un * zc2;
+                const real va = v0 - un * zc1;
+                u = ua - u0;
+                v = va - v0;
             } else {
                 u = -real(2.0) * u0;
                 v = -real(2.0) * v0;
@@ -797,10 +813,19 @@ void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_bih(const Dev &d, cudaStream_t s) {
-    k_bih_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d, d.U_n, d.V_n, 0);
-    k_bih_uc<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
-    k_bih_grad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
-    k_bih_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d, d.U_puls, d.V_puls, 1);
+    const int ge = grid_for((long long)d.Ed * d.L, 256), gl = grid_for((long long)d.E * d.L, 256);
+    k_bih_edge<<<ge, 256, 0, s>>>(d, d.U_n, d.V_n, 0);
+    k_bih_uc<<<gl, 256, 0, s>>>(d, 0);
+    k_bih_grad<false><<<gl, 256, 0, s>>>(d, d.bihU, d.bihV);
+    k_bih_edge<<<ge, 256, 0, s>>>(d, d.bihU, d.bihV, 1);
+}
+void launch_bih_puls(const Dev &d, cudaStream_t s) {
+    const int ge = grid_for((long long)d.Ed * d.L, 256), gl = grid_for((long long)d.E * d.L, 256);
+    k_bih_grad<true><<<gl, 256, 0, s>>>(d, d.U_puls, d.V_puls);
+    k_bih_edge<<<ge, 256, 0, s>>>(d, d.U_puls, d.V_puls, 0);
+    k_bih_uc<<<gl, 256, 0, s>>>(d, 1);
+    k_bih_grad<false><<<gl, 256, 0, s>>>(d, d.bihU, d.bihV);
+    k_bih_edge<<<ge, 256, 0, s>>>(d, d.bihU, d.bihV, 2);
 }
 void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
     k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);

@@ -208,7 +208,8 @@ __global__ void k_p1_elem(Dev d) {
     real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L;
     const int B = (int)blockDim.x / L;
-    const int S = 2 * kP1Slots * L + 1;  // per-element stride, odd: conflict-free
+    const int nsl = kP1Slots + (d.bih_3D ? 1 : 0);  // + biharmonic_viscosity_3D_to_2D
+    const int S = 2 * nsl * L + 1;  // per-element stride, odd: conflict-free
     const int jl = (int)threadIdx.x / L, z = (int)threadIdx.x % L;
     for (long long eb = (long long)blockIdx.x * B; eb < d.E; eb += (long long)gridDim.x * B) {
         const long long e_ = eb + jl;
@@ -246,6 +247,11 @@ __global__ void k_p1_elem(Dev d) {
                 T[(4 * 2 + 0) * L + z] = fu * je;
                 T[(4 * 2 + 1) * L + z] = fv * je;
             }
+            if (d.bih_3D) {
+                const real2 b = bih_gather(d, e, z);
+                T[(5 * 2 + 0) * L + z] = b.x * je;
+                T[(5 * 2 + 1) * L + z] = b.y * je;
+            }
         }
         __syncthreads();
         const long long es = eb + threadIdx.x;
@@ -276,6 +282,11 @@ __global__ void k_p1_elem(Dev d) {
                 for (int k = 0; k < L; ++k) {
                     rx = rx + T[(4 * 2 + 0) * L + k];
                     ry = ry + T[(4 * 2 + 1) * L + k];
+                }
+            if (d.bih_3D)
+                for (int k = 0; k < L; ++k) {
+                    rx = rx + T[(5 * 2 + 0) * L + k];
+                    ry = ry + T[(5 * 2 + 1) * L + k];
                 }
             const real dm = d.dmean_n[e];
             d.U_rhs_2D_3D[e] = make_real2(rx / dm, ry / dm);
@@ -441,7 +452,9 @@ void launch_el2nodes(const Dev &d, const real *Ue, const real *Ve, real *Un, rea
 }
 // B elements per block: B*L threads, at most 1024 and at most 32 elements
 static int p1_elems(const Dev &d) { int b = 1024 / d.L; return b > 32 ? 32 : b; }
-static size_t p1_smem(const Dev &d) { return (size_t)p1_elems(d) * (2 * kP1Slots * d.L + 1) * sizeof(real); }
+static size_t p1_smem(const Dev &d) {
+    return (size_t)p1_elems(d) * (2 * (kP1Slots + (d.bih_3D ? 1 : 0)) * d.L + 1) * sizeof(real);
+}
 int config_p1(const Dev &d) {
     return raise_smem_limit(k_p1_elem, p1_smem(d)) == cudaSuccess
                ? 0 : 1;

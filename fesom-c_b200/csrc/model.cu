@@ -32,6 +32,7 @@ namespace fesomc {
     void launch_adv3_edge(const Dev &, cudaStream_t); \
     void launch_velrhs(const Dev &, real, cudaStream_t); \
     void launch_bih(const Dev &, cudaStream_t); \
+    void launch_bih_puls(const Dev &, cudaStream_t); \
     void launch_implvisc(const Dev &, cudaStream_t); \
     void launch_jac_swap(const Dev &, cudaStream_t); \
     void launch_je(const Dev &, cudaStream_t); \
@@ -458,7 +459,9 @@ int alloc_3d(fesomc_model *m, D &d) {
     int rc = 0;
     if ((rc = dalloc(m, &d.Fp, E))) return rc;
     if ((rc = dalloc(m, &d.adv3, L * (size_t)d.Ed_in))) return rc;
-    if (m->p.bih_3D && (rc = dalloc(m, &d.bihfl, L * (size_t)d.Ed))) return rc;
+    if (m->p.bih_3D && ((rc = dalloc(m, &d.bihfl, L * (size_t)d.Ed)) || (rc = dalloc(m, &d.bihU, L * E)) ||
+                        (rc = dalloc(m, &d.bihV, L * E))))
+        return rc;
     decltype(&d.U_n) le[] = {&d.U_n, &d.V_n, &d.U_rhsAB, &d.V_rhsAB, &d.U_n_filt, &d.V_n_filt, &d.U_rhs, &d.V_rhs,
                              &d.U_puls, &d.V_puls, &d.vgux, &d.vguy, &d.vgvx, &d.vgvy, &d.Bar_pru, &d.Bar_prv,
                              &d.Je, &d.Ze, &d.ZBe};
@@ -574,6 +577,9 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     if (k == "biharmonic")   // two edge passes, U_c, its gradients
         return 2 * (L * Ed * 16 + Ed * (8 + 8 + 16 + 32 + 16) + L * E * 32 + L * E * 16) + L * E * (16 + 16) +
                E * 16 + L * E * (16 + 32) + E * (16 + 16 + 64) + N * 16;
+    if (k == "biharmonic_2d")   // pulsation gradients, two edge passes, U_c, its gradients
+        return L * E * (16 + 32) + E * (16 + 16 + 64 + 16) + 2 * (L * Ed * 16 + Ed * 48 + L * E * 48) +
+               L * E * (16 + 16) + E * 16 + L * E * (16 + 32);
     if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
     if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
@@ -738,6 +744,7 @@ int enqueue_step(fesomc_model *m, double ff) {
             rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
             rec(m, "el2nodes_p", [&] { K3E2N(U_puls, V_puls, Unode_p, Vnode_p); });
             rec(m, "p1_edge", [&] { K3(launch_p1_edge, s); });
+            if (d.bih_3D) { rec(m, "biharmonic_2d", [&] { K3(launch_bih_puls, s); }); n += 5; }
             rec(m, "p1_elem", [&] { K3(launch_p1_elem, s); });
             n += 4;
         }

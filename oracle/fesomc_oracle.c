@@ -468,6 +468,8 @@ static void momentum_adv_P1_3D_to_2D(oracle_model *m) {
     }
 }
 
+static void biharmonic_viscosity_3D_to_2D(oracle_model *m);
+
 /* viscosity_filt_3D_to_2D, fv_viscosity.F90:870-939 */
 static void viscosity_filt_3D_to_2D(oracle_model *m) {
     double tau_inv = m->p.tau_inv_filt;
@@ -522,6 +524,7 @@ static void timestep_AB_2D(oracle_model *m, int step) {
         compute_el2nodes_3D(m, m->U_puls, m->V_puls, m->Unode_p, m->Vnode_p);
         momentum_adv_P1_3D_to_2D(m);
         if (m->p.filt_3D) viscosity_filt_3D_to_2D(m);
+        if (m->p.bih_3D) biharmonic_viscosity_3D_to_2D(m);
         for (int el = 1; el <= m->E; ++el) {
             V2(m->U_rhs_2D_3D, 1, el) = V2(m->U_rhs_2D_3D, 1, el) / N1(m->dmean_n, el);
             V2(m->U_rhs_2D_3D, 2, el) = V2(m->U_rhs_2D_3D, 2, el) / N1(m->dmean_n, el);
@@ -982,14 +985,14 @@ static void momentum_vert_impl_visc_tmp(oracle_model *m) {
     }
 }
 
-/* biharmonic_viscosity, fv_viscosity.F90:104-334 (serial build), with
- * vel_lapl_gradients, fv_gradients.F90:327-402.  Overwrites the velocity
- * gradients with those of the Laplacian, as the reference does. */
-static void biharmonic_viscosity(oracle_model *m) {
+/* First Laplacian of (Uin, Vin) with the velocity gradients in vgux..vgvy:
+ * the edge loop of biharmonic_viscosity / biharmonic_viscosity_3D_to_2D
+ * (fv_viscosity.F90:135-212, 990-1087, serial build): internal edges, then
+ * boundary edges, each flux times Jd, into U_c, V_c (zeroed here). */
+static void bih_laplacian_jd(oracle_model *m, const double *Uin, const double *Vin, double *U_c, double *V_c) {
     const int L = m->L;
-    double *U_c = calloc((size_t)L * m->E, sizeof(double));
-    double *V_c = calloc((size_t)L * m->E, sizeof(double));
-    /* first Laplacian of (U_n, V_n): internal edges, then boundary edges */
+    memset(U_c, 0, sizeof(double) * (size_t)L * m->E);
+    memset(V_c, 0, sizeof(double) * (size_t)L * m->E);
     for (int ed = 1; ed <= m->Ed_in; ++ed) {
         int e1 = EDT(1, ed), e2 = EDT(2, ed);
         double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
@@ -1002,13 +1005,13 @@ static void biharmonic_viscosity(oracle_model *m) {
         for (int z = 1; z <= L; ++z) {
             double g1 = 0.5 * (F3(m->vgux, z, e1) + F3(m->vgux, z, e2));
             double g2 = 0.5 * (F3(m->vguy, z, e1) + F3(m->vguy, z, e2));
-            double tt = g1 * tx + g2 * ty - (F3(m->U_n, z, e2) - F3(m->U_n, z, e1)) / tl;
+            double tt = g1 * tx + g2 * ty - (F3(Uin, z, e2) - F3(Uin, z, e1)) / tl;
             g1 = g1 - tx * tt;
             g2 = g2 - ty * tt;
             double u1 = (g1 * ye - g2 * xe);
             g1 = 0.5 * (F3(m->vgvx, z, e1) + F3(m->vgvx, z, e2));
             g2 = 0.5 * (F3(m->vgvy, z, e1) + F3(m->vgvy, z, e2));
-            tt = g1 * tx + g2 * ty - (F3(m->V_n, z, e2) - F3(m->V_n, z, e1)) / tl;
+            tt = g1 * tx + g2 * ty - (F3(Vin, z, e2) - F3(Vin, z, e1)) / tl;
             g1 = g1 - tx * tt;
             g2 = g2 - ty * tt;
             double v1 = (g1 * ye - g2 * xe);
@@ -1029,14 +1032,11 @@ static void biharmonic_viscosity(oracle_model *m) {
             F3(V_c, z, e1) = F3(V_c, z, e1) + v1 * F3(m->Jd, z, ed);
         }
     }
-    for (int el = 1; el <= m->E; ++el) {
-        double Ah = -m->p.Abh0 * sqrt(N1(m->elem_area, el) / m->p.scale_area) / m->p.scale_area;
-        for (int z = 1; z <= L; ++z) {
-            F3(U_c, z, el) = F3(U_c, z, el) * (Ah);
-            F3(V_c, z, el) = F3(V_c, z, el) * (Ah);
-        }
-    }
-    /* vel_lapl_gradients(U_c, V_c) */
+}
+
+/* vel_lapl_gradients(U_c, V_c), fv_gradients.F90:327-402, into vgux..vgvy */
+static void vel_lapl_gradients(oracle_model *m, const double *U_c, const double *V_c) {
+    const int L = m->L;
 #pragma omp parallel for
     for (int el = 1; el <= m->E; ++el) {
         int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
@@ -1063,7 +1063,14 @@ static void biharmonic_viscosity(oracle_model *m) {
             F3(m->vgvy, z, el) = g[3];
         }
     }
-    /* second Laplacian into U_rhs, V_rhs, scaled by the sponge factor */
+}
+
+/* Second Laplacian of (U_c, V_c) with their gradients: per edge flux times
+ * Jd*acc (scale = 1, biharmonic_viscosity, fv_viscosity.F90:248-330) or
+ * plain (scale = 0, biharmonic_viscosity_3D_to_2D, :1116-1200), added to
+ * (Uo, Vo) in edge order. */
+static void bih_second(oracle_model *m, const double *U_c, const double *V_c, double *Uo, double *Vo, int scale) {
+    const int L = m->L;
     for (int ed = 1; ed <= m->Ed_in; ++ed) {
         int e1 = EDT(1, ed), e2 = EDT(2, ed);
         double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
@@ -1087,10 +1094,12 @@ static void biharmonic_viscosity(oracle_model *m) {
             g1 = g1 - tx * tt;
             g2 = g2 - ty * tt;
             double v1 = (g1 * ye - g2 * xe);
-            F3(m->U_rhs, z, e1) = F3(m->U_rhs, z, e1) + u1 * F3(m->Jd, z, ed) * acc;
-            F3(m->V_rhs, z, e1) = F3(m->V_rhs, z, e1) + v1 * F3(m->Jd, z, ed) * acc;
-            F3(m->U_rhs, z, e2) = F3(m->U_rhs, z, e2) - u1 * F3(m->Jd, z, ed) * acc;
-            F3(m->V_rhs, z, e2) = F3(m->V_rhs, z, e2) - v1 * F3(m->Jd, z, ed) * acc;
+            double fu = scale ? u1 * F3(m->Jd, z, ed) * acc : u1;
+            double fv = scale ? v1 * F3(m->Jd, z, ed) * acc : v1;
+            F3(Uo, z, e1) = F3(Uo, z, e1) + fu;
+            F3(Vo, z, e1) = F3(Vo, z, e1) + fv;
+            F3(Uo, z, e2) = F3(Uo, z, e2) - fu;
+            F3(Vo, z, e2) = F3(Vo, z, e2) - fv;
         }
     }
     for (int ed = m->Ed_in + 1; ed <= m->Ed; ++ed) {
@@ -1101,12 +1110,94 @@ static void biharmonic_viscosity(oracle_model *m) {
         for (int z = 1; z <= L; ++z) {
             double u1 = (F3(m->vgux, z, e1)) * ye - (F3(m->vguy, z, e1)) * xe;
             double v1 = (F3(m->vgvx, z, e1)) * ye - (F3(m->vgvy, z, e1)) * xe;
-            F3(m->U_rhs, z, e1) = F3(m->U_rhs, z, e1) + u1 * F3(m->Jd, z, ed) * acc;
-            F3(m->V_rhs, z, e1) = F3(m->V_rhs, z, e1) + v1 * F3(m->Jd, z, ed) * acc;
+            F3(Uo, z, e1) = F3(Uo, z, e1) + (scale ? u1 * F3(m->Jd, z, ed) * acc : u1);
+            F3(Vo, z, e1) = F3(Vo, z, e1) + (scale ? v1 * F3(m->Jd, z, ed) * acc : v1);
         }
     }
+}
+
+/* biharmonic_viscosity, fv_viscosity.F90:104-334 (serial build).  Leaves
+ * the Laplacian's gradients in vgux..vgvy, as the reference does. */
+static void biharmonic_viscosity(oracle_model *m) {
+    const int L = m->L;
+    double *U_c = malloc(sizeof(double) * (size_t)L * m->E), *V_c = malloc(sizeof(double) * (size_t)L * m->E);
+    bih_laplacian_jd(m, m->U_n, m->V_n, U_c, V_c);
+    for (int el = 1; el <= m->E; ++el) {
+        double Ah = -m->p.Abh0 * sqrt(N1(m->elem_area, el) / m->p.scale_area) / m->p.scale_area;
+        for (int z = 1; z <= L; ++z) {
+            F3(U_c, z, el) = F3(U_c, z, el) * (Ah);
+            F3(V_c, z, el) = F3(V_c, z, el) * (Ah);
+        }
+    }
+    vel_lapl_gradients(m, U_c, V_c);
+    bih_second(m, U_c, V_c, m->U_rhs, m->V_rhs, 1);
     free(U_c);
     free(V_c);
+}
+
+/* vel_gradients_puls, fv_gradients.F90:404-496 (free_slip = .true.) */
+static void vel_gradients_puls(oracle_model *m) {
+    const int L = m->L;
+#pragma omp parallel for
+    for (int el = 1; el <= m->E; ++el) {
+        int jend = (ELN(1, el) == ELN(4, el)) ? 3 : 4;
+        for (int z = 1; z <= L; ++z) {
+            double g[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int j = 1; j <= jend; ++j) {
+                int el2 = ELNB(j, el);
+                double u, v;
+                if (el2 > 0) {
+                    u = F3(m->U_puls, z, el2) - F3(m->U_puls, z, el);
+                    v = F3(m->V_puls, z, el2) - F3(m->V_puls, z, el);
+                } else {
+                    double zc1 = EDXY(1, ELE(j, el)), zc2 = EDXY(2, ELE(j, el));
+                    zc1 = zc1 * N1(m->elem_cos, el);
+                    double un = -2.0 * (F3(m->U_puls, z, el) * zc2 - F3(m->V_puls, z, el) * zc1) / (zc1 * zc1 + zc2 * zc2);
+                    double u_aux = F3(m->U_puls, z, el) + un * zc2;
+                    double v_aux = F3(m->V_puls, z, el) - un * zc1;
+                    u = u_aux - F3(m->U_puls, z, el);
+                    v = v_aux - F3(m->V_puls, z, el);
+                }
+                g[0] = g[0] + GV(j, el) * u;
+                g[1] = g[1] + GV(j + 4, el) * u;
+                g[2] = g[2] + GV(j, el) * v;
+                g[3] = g[3] + GV(j + 4, el) * v;
+            }
+            F3(m->vgux, z, el) = g[0];
+            F3(m->vguy, z, el) = g[1];
+            F3(m->vgvx, z, el) = g[2];
+            F3(m->vgvy, z, el) = g[3];
+        }
+    }
+}
+
+/* biharmonic_viscosity_3D_to_2D, fv_viscosity.F90:964-1219 (serial build).
+ * Visc is zero on this path (only h_viscosity, run by the sediment model,
+ * fills it). */
+static void biharmonic_viscosity_3D_to_2D(oracle_model *m) {
+    const int L = m->L;
+    const size_t n = (size_t)L * m->E;
+    double *U_c = malloc(sizeof(double) * n), *V_c = malloc(sizeof(double) * n);
+    double *Ub = calloc(n, sizeof(double)), *Vb = calloc(n, sizeof(double));
+    vel_gradients_puls(m);
+    bih_laplacian_jd(m, m->U_puls, m->V_puls, U_c, V_c);
+    for (int el = 1; el <= m->E; ++el) {
+        double acc = 0.0;
+        for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+        double Ah = -acc * m->p.Abh0 * sqrt(N1(m->elem_area, el) / m->p.scale_area) / m->p.scale_area;
+        for (int z = 1; z <= L; ++z) {
+            F3(U_c, z, el) = F3(U_c, z, el) * (Ah - 0.0);
+            F3(V_c, z, el) = F3(V_c, z, el) * (Ah - 0.0);
+        }
+    }
+    vel_lapl_gradients(m, U_c, V_c);
+    bih_second(m, U_c, V_c, Ub, Vb, 0);
+    for (int el = 1; el <= m->E; ++el)
+        for (int z = 1; z <= L; ++z) {
+            V2(m->U_rhs_2D_3D, 1, el) = V2(m->U_rhs_2D_3D, 1, el) + F3(Ub, z, el) * F3(m->Je, z, el);
+            V2(m->U_rhs_2D_3D, 2, el) = V2(m->U_rhs_2D_3D, 2, el) + F3(Vb, z, el) * F3(m->Je, z, el);
+        }
+    free(U_c); free(V_c); free(Ub); free(Vb);
 }
 
 /* compute_vel_rhs, fv_3D_vel.F90:1-197 (key_atm off) */
