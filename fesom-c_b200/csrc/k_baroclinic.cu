@@ -416,6 +416,39 @@ __global__ void k_bih_grad(Dev d, const real *U, const real *V) {
     }
 }
 
+// viscosity_filt2x_3D (fv_viscosity.F90:570-670), first half: U_c of every
+// (element, level) from the differences of U*Je with its neighbours
+// (neighbour 4 only when it differs from neighbour 1), times K_bi.  velrhs
+// forms UV_rhs from the neighbours' U_c.
+__global__ void k_filt2x_uc(Dev d) {
+    const long long total = (long long)d.E * d.L;
+    const int L = d.L;
+    const real tau_inv = d.dt * d.tau_c / real(3600.0) / real(24.0);
+    GRID_LOOP(ii, total) {
+        const int e = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int4 nb = d.elem_nb[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const real K_bi = tau_inv * sqrt(d.scale_area / d.elem_area[e]);
+        const real uj = d.U_n[ii] * d.Je[ii], vj = d.V_n[ii] * d.Je[ii];
+        real uc = real(0.0), vc = real(0.0);
+        for (int j = 0; j < 4; ++j) {
+            const int ne = nbs[j];
+            if (!(ne >= 0 && (j < 3 || ne != nbs[0]))) continue;
+            const size_t i2 = (size_t)ne * L + z;
+            if (j == 0) {
+                uc = uj - d.U_n[i2] * d.Je[i2];
+                vc = vj - d.V_n[i2] * d.Je[i2];
+            } else {
+                uc = uc + uj - d.U_n[i2] * d.Je[i2];
+                vc = vc + vj - d.V_n[i2] * d.Je[i2];
+            }
+        }
+        d.f2U[ii] = uc * K_bi;
+        d.f2V[ii] = vc * K_bi;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
 // level) with levels on consecutive lanes.  The loop runs over whole warps so
@@ -512,8 +545,22 @@ __global__ void __launch_bounds__(256, FESOMC_FP32 ? 4 : 3) k_velrhs(Dev d, real
             d.V_rhsAB[ii] = vab;
             const real area_inv = real(1.0) / ar;
             const real dt = d.dt;
-            d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + real(0.0)) / je);
-            d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + real(0.0)) / je);
+            // UV_rhs of viscosity_filt2x_3D (zero when it is off)
+            real uvx = real(0.0), uvy = real(0.0);
+            if (d.filt_bi_3D) {
+                const int4 nb = d.elem_nb[e];
+                const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+                const real uc = d.f2U[ii], vc = d.f2V[ii];
+                for (int j = 0; j < 4; ++j) {
+                    const int ne = nbs[j];
+                    if (!(ne >= 0 && (j < 3 || ne != nbs[0]))) continue;
+                    const size_t i2 = (size_t)ne * L + z;
+                    if (j == 0) { uvx = -uc + d.f2U[i2]; uvy = -vc + d.f2V[i2]; }
+                    else { uvx = uvx - uc + d.f2U[i2]; uvy = uvy - vc + d.f2V[i2]; }
+                }
+            }
+            d.U_rhs[ii] = mwd * (un0 + d.Bar_pru[ii] * dt + (dt * (ur + uab * ff) * area_inv + uvx) / je);
+            d.V_rhs[ii] = mwd * (vn0 + d.Bar_prv[ii] * dt + (dt * (vr + vab * ff) * area_inv + uvy) / je);
         }
     }
 }
@@ -811,6 +858,9 @@ void launch_velgrad3d(const Dev &d, cudaStream_t s) {
 }
 void launch_adv3_edge(const Dev &d, cudaStream_t s) {
     k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
+}
+void launch_filt2x(const Dev &d, cudaStream_t s) {
+    k_filt2x_uc<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }
 void launch_bih(const Dev &d, cudaStream_t s) {
     const int ge = grid_for((long long)d.Ed * d.L, 256), gl = grid_for((long long)d.E * d.L, 256);

@@ -325,6 +325,30 @@ __global__ void k_adv2d_edge(Dev d) {
     }
 }
 
+// viscosity_filt2x_2D (fv_viscosity.F90:672-767), first half: U_c of every
+// element from the differences of U_n_2D with its neighbours, times K_bi;
+// u2d_elem forms UV2_rhs from the neighbours' U_c.  Runs before u2d_elem,
+// which rotates U_n_2D.
+__global__ void k_filt2x_2d(Dev d) {
+    const real tau_inv = d.dt_2D * d.tau_c / real(3600.0) / real(24.0);
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int4 nb = d.elem_nb[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const real K_bi = tau_inv * sqrt(d.scale_area / d.elem_area[e]);
+        const real2 u0 = d.U_n_2D[e];
+        real uc = real(0.0), vc = real(0.0);
+        for (int j = 0; j < 4; ++j) {
+            const int ne = nbs[j];
+            if (!(ne >= 0 && (j < 3 || ne != nbs[0]))) continue;
+            const real2 u2 = d.U_n_2D[ne];
+            if (j == 0) { uc = u0.x - u2.x; vc = u0.y - u2.y; }
+            else { uc = uc + u0.x - u2.x; vc = vc + u0.y - u2.y; }
+        }
+        d.f2uv2d[e] = make_real2(uc * K_bi, vc * K_bi);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // u2d_elem: update_2D_vel (fv_average_dynamic.F90:228-443, type_task 3,
 // key_atm off) + rotation of U time levels + U_filt accumulation
@@ -403,8 +427,22 @@ __global__ void __launch_bounds__(128, FESOMC_FP32 ? 8 : 6) k_u2d_elem(Dev d) {
         const real dt2 = d.dt_2D;
         const real2 u0 = d.U_n_2D[e];
         const real2 bp = d.Bar_pr_2D[e];
-        const real nx = mwd * ((dmo * u0.x - dt2 * friction * (ub - u0.x) + dt2 * bp.x + dt2 * rx / ar) * ff + real(0.0));
-        const real ny = mwd * ((dmo * u0.y - dt2 * friction * (vb - u0.y) + dt2 * bp.y + dt2 * ry / ar) * ff + real(0.0));
+        // UV2_rhs of viscosity_filt2x_2D (zero when it is off)
+        real uvx = real(0.0), uvy = real(0.0);
+        if (d.filt_bi_2D) {
+            const int4 nb = d.elem_nb[e];
+            const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+            const real2 c0 = d.f2uv2d[e];
+            for (int j = 0; j < 4; ++j) {
+                const int ne = nbs[j];
+                if (!(ne >= 0 && (j < 3 || ne != nbs[0]))) continue;
+                const real2 c2 = d.f2uv2d[ne];
+                if (j == 0) { uvx = -c0.x + c2.x; uvy = -c0.y + c2.y; }
+                else { uvx = uvx - c0.x + c2.x; uvy = uvy - c0.y + c2.y; }
+            }
+        }
+        const real nx = mwd * ((dmo * u0.x - dt2 * friction * (ub - u0.x) + dt2 * bp.x + dt2 * rx / ar) * ff + uvx);
+        const real ny = mwd * ((dmo * u0.y - dt2 * friction * (vb - u0.y) + dt2 * bp.y + dt2 * ry / ar) * ff + uvy);
         // rotate U_n_2 <- U_n_1 <- U_n_2D <- new (fv_main.F90:1569-1578)
         d.U_n_2[e] = d.U_n_1[e];
         d.U_n_1[e] = u0;
@@ -468,6 +506,7 @@ void launch_p1_elem(const Dev &d, cudaStream_t s) {
     k_p1_elem<<<(int)(blocks < 148LL * 16 ? blocks : 148LL * 16), B * d.L, p1_smem(d), s>>>(d);
 }
 void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
+void launch_filt2x_2d(const Dev &d, cudaStream_t s) { k_filt2x_2d<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }

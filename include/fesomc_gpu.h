@@ -157,6 +157,11 @@ typedef struct fesomc_params {
      * src/fv_viscosity.F90:104-334)                                        */
     int32_t bih_3D;
     double Abh0;
+    /* filter-2x viscosities (filt_bi_3D / filt_bi_2D, tau_c of fv_run.dat,
+     * src/fv_read_run.F90:336-342; viscosity_filt2x_3D / _2D,
+     * src/fv_viscosity.F90:570-767)                                         */
+    int32_t filt_bi_3D, filt_bi_2D;
+    double tau_c;
 } fesomc_params;
 
 /*

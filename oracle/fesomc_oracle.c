@@ -73,6 +73,7 @@ typedef struct oracle_model {
     double *vgux, *vguy, *vgvx, *vgvy, *U_puls, *V_puls, *Unode, *Vnode, *Unode_p, *Vnode_p;
     double *TF, *SF, *T_old, *S_old, *Tclim, *Sclim, *rho_c, *hpressure;
     double *Bar_pru_3D, *Bar_prv_3D, *Bar_pr_2D;
+    double *UV_rhs_u, *UV_rhs_v, *UV2_rhs;   /* filter-2x terms (zero unless filt_bi_3D / _2D) */
     double *bt, *snu, *Kv, *Av, *Ri, *tke_dissip, *Wvel;
     /* forcing */
     double *runoff, *ampt, *fazt, amp_factor[12], phy_factor[12];
@@ -350,6 +351,49 @@ static inline double wsum2e(const oracle_model *m, int el, const double *x, cons
 }
 
 /* update_2D_vel, fv_average_dynamic.F90:228-443 (type_task 3, key_atm off) */
+/* viscosity_filt2x_2D, fv_viscosity.F90:672-767: UV2_rhs from U_n_2D */
+static void viscosity_filt2x_2D(oracle_model *m) {
+    double *U_c = malloc(sizeof(double) * (size_t)m->E), *V_c = malloc(sizeof(double) * (size_t)m->E);
+    const double tau_inv = m->p.dt_2D * m->p.tau_c / 3600.0 / 24.0;
+    for (int el = 1; el <= m->E; ++el) {
+        N1(U_c, el) = 0.0;
+        N1(V_c, el) = 0.0;
+        double K_bi = tau_inv * sqrt(m->p.scale_area / N1(m->elem_area, el));
+        for (int j = 1; j <= 4; ++j) {
+            int ne = ELNB(j, el);
+            if (ne > 0 && (j < 4 || ne != ELNB(1, el))) {
+                if (j == 1) {
+                    N1(U_c, el) = V2(m->U_n_2D, 1, el) - V2(m->U_n_2D, 1, ne);
+                    N1(V_c, el) = V2(m->U_n_2D, 2, el) - V2(m->U_n_2D, 2, ne);
+                } else {
+                    N1(U_c, el) = N1(U_c, el) + V2(m->U_n_2D, 1, el) - V2(m->U_n_2D, 1, ne);
+                    N1(V_c, el) = N1(V_c, el) + V2(m->U_n_2D, 2, el) - V2(m->U_n_2D, 2, ne);
+                }
+            }
+        }
+        N1(U_c, el) = N1(U_c, el) * K_bi;
+        N1(V_c, el) = N1(V_c, el) * K_bi;
+    }
+    for (int el = 1; el <= m->E; ++el) {
+        V2(m->UV2_rhs, 1, el) = 0.0;
+        V2(m->UV2_rhs, 2, el) = 0.0;
+        for (int j = 1; j <= 4; ++j) {
+            int ne = ELNB(j, el);
+            if (ne > 0 && (j < 4 || ne != ELNB(1, el))) {
+                if (j == 1) {
+                    V2(m->UV2_rhs, 1, el) = -N1(U_c, el) + N1(U_c, ne);
+                    V2(m->UV2_rhs, 2, el) = -N1(V_c, el) + N1(V_c, ne);
+                } else {
+                    V2(m->UV2_rhs, 1, el) = V2(m->UV2_rhs, 1, el) - N1(U_c, el) + N1(U_c, ne);
+                    V2(m->UV2_rhs, 2, el) = V2(m->UV2_rhs, 2, el) - N1(V_c, el) + N1(V_c, ne);
+                }
+            }
+        }
+    }
+    free(U_c);
+    free(V_c);
+}
+
 static void update_2D_vel(oracle_model *m, int step) {
     (void)step;
     const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
@@ -377,6 +421,7 @@ static void update_2D_vel(oracle_model *m, int step) {
     }
     if (m->p.mom_adv_2D == 2) momentum_adv_upwind_2D(m);
     if (m->p.filt_2D) viscosity_filt_2D(m);
+    if (m->p.filt_bi_2D) viscosity_filt2x_2D(m);
     for (int el = 1; el <= m->E; ++el) {
         V2(m->U_rhs_2D, 1, el) = V2(m->U_rhs_2D, 1, el) + V2(m->U_rhs_2D_3D, 1, el);
         V2(m->U_rhs_2D, 2, el) = V2(m->U_rhs_2D, 2, el) + V2(m->U_rhs_2D_3D, 2, el);
@@ -394,10 +439,10 @@ static void update_2D_vel(oracle_model *m, int step) {
         double dt2 = m->p.dt_2D;
         V2(m->U_rhs_2D, 1, el) = N1(m->mask_wd, el) * ((dmean * V2(m->U_n_2D, 1, el) -
             dt2 * friction * (ub - V2(m->U_n_2D, 1, el)) + dt2 * V2(m->Bar_pr_2D, 1, el) +
-            dt2 * V2(m->U_rhs_2D, 1, el) / N1(m->elem_area, el)) * ff + 0.0);
+            dt2 * V2(m->U_rhs_2D, 1, el) / N1(m->elem_area, el)) * ff + V2(m->UV2_rhs, 1, el));
         V2(m->U_rhs_2D, 2, el) = N1(m->mask_wd, el) * ((dmean * V2(m->U_n_2D, 2, el) -
             dt2 * friction * (vb - V2(m->U_n_2D, 2, el)) + dt2 * V2(m->Bar_pr_2D, 2, el) +
-            dt2 * V2(m->U_rhs_2D, 2, el) / N1(m->elem_area, el)) * ff + 0.0);
+            dt2 * V2(m->U_rhs_2D, 2, el) / N1(m->elem_area, el)) * ff + V2(m->UV2_rhs, 2, el));
     }
 }
 
@@ -1200,6 +1245,52 @@ static void biharmonic_viscosity_3D_to_2D(oracle_model *m) {
     free(U_c); free(V_c); free(Ub); free(Vb);
 }
 
+/* viscosity_filt2x_3D, fv_viscosity.F90:570-670: UV_rhs from U_n, V_n */
+static void viscosity_filt2x_3D(oracle_model *m) {
+    const int L = m->L;
+    double *U_c = malloc(sizeof(double) * (size_t)L * m->E), *V_c = malloc(sizeof(double) * (size_t)L * m->E);
+    const double tau_inv = m->p.dt * m->p.tau_c / 3600.0 / 24.0;
+    for (int el = 1; el <= m->E; ++el) {
+        double K_bi = tau_inv * sqrt(m->p.scale_area / N1(m->elem_area, el));
+        for (int z = 1; z <= L; ++z) {
+            double uj = F3(m->U_n, z, el) * F3(m->Je, z, el), vj = F3(m->V_n, z, el) * F3(m->Je, z, el);
+            double uc = 0.0, vc = 0.0;
+            for (int j = 1; j <= 4; ++j) {
+                int ne = ELNB(j, el);
+                if (!(ne > 0 && (j < 4 || ne != ELNB(1, el)))) continue;
+                if (j == 1) {
+                    uc = uj - F3(m->U_n, z, ne) * F3(m->Je, z, ne);
+                    vc = vj - F3(m->V_n, z, ne) * F3(m->Je, z, ne);
+                } else {
+                    uc = uc + uj - F3(m->U_n, z, ne) * F3(m->Je, z, ne);
+                    vc = vc + vj - F3(m->V_n, z, ne) * F3(m->Je, z, ne);
+                }
+            }
+            F3(U_c, z, el) = uc * K_bi;
+            F3(V_c, z, el) = vc * K_bi;
+        }
+    }
+    for (int el = 1; el <= m->E; ++el)
+        for (int z = 1; z <= L; ++z) {
+            double uv = 0.0, vv = 0.0;
+            for (int j = 1; j <= 4; ++j) {
+                int ne = ELNB(j, el);
+                if (!(ne > 0 && (j < 4 || ne != ELNB(1, el)))) continue;
+                if (j == 1) {
+                    uv = -F3(U_c, z, el) + F3(U_c, z, ne);
+                    vv = -F3(V_c, z, el) + F3(V_c, z, ne);
+                } else {
+                    uv = uv - F3(U_c, z, el) + F3(U_c, z, ne);
+                    vv = vv - F3(V_c, z, el) + F3(V_c, z, ne);
+                }
+            }
+            F3(m->UV_rhs_u, z, el) = uv;
+            F3(m->UV_rhs_v, z, el) = vv;
+        }
+    free(U_c);
+    free(V_c);
+}
+
 /* compute_vel_rhs, fv_3D_vel.F90:1-197 (key_atm off) */
 static void compute_vel_rhs(oracle_model *m) {
     const int L = m->L;
@@ -1227,6 +1318,7 @@ static void compute_vel_rhs(oracle_model *m) {
     vel_gradients(m);
     if (m->p.mom_adv_3D == 1) momentum_adv_upwind(m);
     if (m->p.filt_3D) viscosity_filt_3D(m);
+    if (m->p.filt_bi_3D) viscosity_filt2x_3D(m);
     if (m->p.bih_3D) biharmonic_viscosity(m);
     if (m->p.vert_adv == 1) momentum_vert_adv_upwind(m);
     double ff = 1.5 + eps;
@@ -1236,9 +1328,9 @@ static void compute_vel_rhs(oracle_model *m) {
         double area_inv = 1.0 / N1(m->elem_area, el);
         for (int z = 1; z <= L; ++z) {
             F3(m->U_rhs, z, el) = N1(m->mask_wd, el) * (F3(m->U_n, z, el) + F3(m->Bar_pru_3D, z, el) * m->p.dt +
-                (m->p.dt * (F3(m->U_rhs, z, el) + F3(m->U_rhsAB, z, el) * ff) * area_inv + 0.0) / F3(m->Je, z, el));
+                (m->p.dt * (F3(m->U_rhs, z, el) + F3(m->U_rhsAB, z, el) * ff) * area_inv + F3(m->UV_rhs_u, z, el)) / F3(m->Je, z, el));
             F3(m->V_rhs, z, el) = N1(m->mask_wd, el) * (F3(m->V_n, z, el) + F3(m->Bar_prv_3D, z, el) * m->p.dt +
-                (m->p.dt * (F3(m->V_rhs, z, el) + F3(m->V_rhsAB, z, el) * ff) * area_inv + 0.0) / F3(m->Je, z, el));
+                (m->p.dt * (F3(m->V_rhs, z, el) + F3(m->V_rhsAB, z, el) * ff) * area_inv + F3(m->UV_rhs_v, z, el)) / F3(m->Je, z, el));
         }
     }
     if (m->p.im_vert_visc) momentum_vert_impl_visc(m);
@@ -1978,6 +2070,7 @@ oracle_model *oracle_create(const fesomc_mesh *msh, const fesomc_params *par, co
     m->U_rhs = dalloc(L * E); m->V_rhs = dalloc(L * E);
     m->vgux = dalloc(L * E); m->vguy = dalloc(L * E); m->vgvx = dalloc(L * E); m->vgvy = dalloc(L * E);
     m->U_puls = dalloc(L * E); m->V_puls = dalloc(L * E);
+    m->UV_rhs_u = dalloc(L * E); m->UV_rhs_v = dalloc(L * E); m->UV2_rhs = dalloc(2 * (size_t)E);
     m->Unode = dalloc(L * N); m->Vnode = dalloc(L * N); m->Unode_p = dalloc(L * N); m->Vnode_p = dalloc(L * N);
     m->Bar_pru_3D = dalloc(L * E); m->Bar_prv_3D = dalloc(L * E);
     m->runoff = dalloc(msh->n_rivers);

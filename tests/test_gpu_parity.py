@@ -227,6 +227,20 @@ def test_le_biharmonic_bit_exact(mods):
     assert bad == []
 
 
+def test_estuary_filter2x_bit_exact(mods):
+    """viscosity_filt2x_3D and viscosity_filt2x_2D (filt_bi_3D / filt_bi_2D)
+    on the small estuary, 30 steps, and on LE, 20 steps."""
+    abi, cases, model, pyoracle = mods
+    bad, _, _ = run_pair(mods, cases.estuary("small", filt_bi_3D=1, filt_bi_2D=1, tau_c=0.4), 30)
+    assert bad == []
+    case = cases.le_medium()
+    case.params.Mt = 4
+    case.params.filt_bi_3D = 1
+    case.params.filt_bi_2D = 1
+    bad, _, _ = run_pair(mods, case, 20)
+    assert bad == []
+
+
 def test_cfg0_bit_exact(mods):
     """The reference's CPU-sized configuration (201 x 81 nodes at 300 m, 11
     sigma levels, MUSCL, wetting/drying, tide, river), 100 internal steps."""

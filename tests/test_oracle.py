@@ -182,3 +182,19 @@ def test_estuary_biharmonic_oracle(mods):
     assert np.isfinite(out[1e4]["U_n"]).all()
     assert d3 > 0.0
     assert 5.0 < d4 / d3 < 15.0
+
+
+def test_estuary_filter2x_oracle(mods):
+    """viscosity_filt2x_3D / _2D: each switch changes the run, which stays
+    finite."""
+    abi, cases, pyoracle = mods
+    out = {}
+    for key, kw in (("none", {}), ("3d", {"filt_bi_3D": 1}), ("2d", {"filt_bi_2D": 1})):
+        c = cases.estuary("small", tau_c=0.4, **kw)
+        o = pyoracle.Oracle(c, abi, cases)
+        o.step(20)
+        out[key] = o.state()
+        o.close()
+    for key in ("3d", "2d"):
+        assert np.isfinite(out[key]["U_n"]).all()
+        assert not np.array_equal(out[key]["U_n"], out["none"]["U_n"])
