@@ -325,6 +325,112 @@ __global__ void k_adv2d_edge(Dev d) {
     }
 }
 
+// biharmonic_2D (fv_viscosity.F90:338-568, free slip): two Laplacians of the
+// 2D velocity.  bih2d_edge: the flux of every edge from U and the gradients
+// in vel_grad (boundary edges with the free-slip projection, whose v uses
+// the projected u, as the reference); bih2d_ul: Ul = Ah acc sum of the
+// fluxes; bih2d_grad: vel_gradients_2D(Ul) into vel_grad (adv2d_edge has
+// used the gradients of UAB by then).  u2d_elem gathers the second pass.
+__global__ void k_bih2d_edge(Dev d, const real2 *U) {
+    GRID_LOOP(ii, d.Ed) {
+        const int ed = (int)ii;
+        const int2 et = d.edge_tri[ed];
+        const real2 dxy = d.edge_dxdy[ed];
+        real u1, v1;
+        if (ed < d.Ed_in) {
+            const real4 X = d.edge_cross[ed];
+            const real xe = dxy.x * kREarth * real(0.5) * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+            const real ye = dxy.y * kREarth;
+            real tx = -X.x + X.z;
+            real ty = -X.y + X.w;
+            const real tl = sqrt(tx * tx + ty * ty);
+            tx = tx / tl;
+            ty = ty / tl;
+            const real4 a = d.vel_grad[et.x], b = d.vel_grad[et.y];
+            const real2 U1 = U[et.x], U2 = U[et.y];
+            real g1 = real(0.5) * (a.x + b.x);
+            real g2 = real(0.5) * (a.y + b.y);
+            real tt = g1 * tx + g2 * ty - (U2.x - U1.x) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            u1 = (g1 * ye - g2 * xe);
+            g1 = real(0.5) * (a.z + b.z);
+            g2 = real(0.5) * (a.w + b.w);
+            tt = g1 * tx + g2 * ty - (U2.y - U1.y) / tl;
+            g1 = g1 - tx * tt;
+            g2 = g2 - ty * tt;
+            v1 = (g1 * ye - g2 * xe);
+        } else {
+            const real xe = dxy.x * kREarth;
+            const real xed = xe * d.elem_cos[et.x];
+            const real ye = dxy.y * kREarth;
+            const real4 a = d.vel_grad[et.x];
+            u1 = (a.x) * ye - (a.y) * xed;
+            v1 = (a.z) * ye - (a.w) * xed;
+            u1 = ye * (u1 * ye - v1 * xe) / (xe * xe + ye * ye);
+            v1 = -xe * (u1 * ye - v1 * xe) / (xe * xe + ye * ye);
+        }
+        d.b2fl[ed] = make_real2(u1, v1);
+    }
+}
+
+__global__ void k_bih2d_ul(Dev d) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int4 se = d.elem_sedges[e];
+        const int codes[4] = {se.x, se.y, se.z, se.w};
+        real ux = real(0.0), uy = real(0.0);
+        for (int c = 0; c < 4; ++c) {
+            const int code = codes[c];
+            if (code < 0) break;
+            const real2 f = d.b2fl[code >> 1];
+            if (code & 1) { ux = ux - f.x; uy = uy - f.y; }
+            else { ux = ux + f.x; uy = uy + f.y; }
+        }
+        const real Ah = -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
+        const real acc = d.elem_acc[e];
+        d.b2ul[e] = make_real2(ux * (Ah) * acc, uy * (Ah) * acc);
+    }
+}
+
+// vel_gradients_2D (fv_gradients.F90:97-176, free slip) of U into vel_grad
+__global__ void k_bih2d_grad(Dev d, const real2 *U) {
+    GRID_LOOP(ii, d.E) {
+        const int e = (int)ii;
+        const int4 en = d.elem_nodes[e];
+        const int4 nb = d.elem_nb[e];
+        const int4 ee = d.elem_edges[e];
+        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
+        const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
+        const real4 gx = d.gv_x[e], gy = d.gv_y[e];
+        const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
+        const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
+        const int jend = (en.x == en.w) ? 3 : 4;
+        const real2 u0 = U[e];
+        real g1 = real(0.0), g2 = real(0.0), g3 = real(0.0), g4 = real(0.0);
+        for (int j = 0; j < jend; ++j) {
+            const int e2 = nbs[j];
+            if (e2 >= 0) {
+                const real2 u2 = U[e2];
+                g1 = g1 + gxa[j] * (u2.x - u0.x);
+                g2 = g2 + gya[j] * (u2.x - u0.x);
+                g3 = g3 + gxa[j] * (u2.y - u0.y);
+                g4 = g4 + gya[j] * (u2.y - u0.y);
+            } else {
+                const real2 dxy = d.edge_dxdy[eds[j]];
+                const real zc1 = dxy.x * d.elem_cos[e];
+                const real zc2 = dxy.y;
+                const real un = -real(2.0) * (u0.x * zc2 - u0.y * zc1) / (zc1 * zc1 + zc2 * zc2);
+                g1 = g1 + gxa[j] * un * zc2;
+                g2 = g2 + gya[j] * un * zc2;
+                g3 = g3 - gxa[j] * un * zc1;
+                g4 = g4 - gya[j] * un * zc1;
+            }
+        }
+        d.vel_grad[e] = make_real4(g1, g2, g3, g4);
+    }
+}
+
 // viscosity_filt2x_2D (fv_viscosity.F90:672-767), first half: U_c of every
 // element from the differences of U_n_2D with its neighbours, times K_bi;
 // u2d_elem forms UV2_rhs from the neighbours' U_c.  Runs before u2d_elem,
@@ -412,6 +518,18 @@ __global__ void __launch_bounds__(128, FESOMC_FP32 ? 8 : 6) k_u2d_elem(Dev d) {
             const real sd = (real)wsum_d(w, dep[0], dep[1], dep[2], dep[3]);
             rx = rx + d.tau_inv_filt * u1 * ar * sd;
             ry = ry + d.tau_inv_filt * u2 * ar * sd;
+        }
+        // biharmonic_2D: the second-pass edge fluxes in edge order
+        if (d.bih_2D) {
+            const int4 se = d.elem_sedges[e];
+            const int codes[4] = {se.x, se.y, se.z, se.w};
+            for (int c = 0; c < 4; ++c) {
+                const int code = codes[c];
+                if (code < 0) break;
+                const real2 f = d.b2fl[code >> 1];
+                if (code & 1) { rx = rx - f.x; ry = ry - f.y; }
+                else { rx = rx + f.x; ry = ry + f.y; }
+            }
         }
         const real2 r3 = d.U_rhs_2D_3D[e];
         rx = rx + r3.x;
@@ -507,6 +625,12 @@ void launch_p1_elem(const Dev &d, cudaStream_t s) {
 }
 void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
 void launch_filt2x_2d(const Dev &d, cudaStream_t s) { k_filt2x_2d<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+void launch_bih_2d(const Dev &d, cudaStream_t s) {
+    k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.UAB);
+    k_bih2d_ul<<<grid_for(d.E, 256), 256, 0, s>>>(d);
+    k_bih2d_grad<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.b2ul);
+    k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.b2ul);
+}
 void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
 void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }

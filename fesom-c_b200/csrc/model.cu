@@ -34,6 +34,7 @@ namespace fesomc {
     void launch_bih(const Dev &, cudaStream_t); \
     void launch_filt2x(const Dev &, cudaStream_t); \
     void launch_filt2x_2d(const Dev &, cudaStream_t); \
+    void launch_bih_2d(const Dev &, cudaStream_t); \
     void launch_bih_puls(const Dev &, cudaStream_t); \
     void launch_implvisc(const Dev &, cudaStream_t); \
     void launch_jac_swap(const Dev &, cudaStream_t); \
@@ -452,6 +453,7 @@ int alloc_mom2d(fesomc_model *m, D &d) {
     if ((rc = dalloc(m, &d.bfric, E))) return rc;
     if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
     if (m->p.filt_bi_2D && (rc = dalloc(m, &d.f2uv2d, E))) return rc;
+    if (m->p.bih_2D && ((rc = dalloc(m, &d.b2fl, (size_t)d.Ed)) || (rc = dalloc(m, &d.b2ul, E)))) return rc;
     return FESOMC_OK;
 }
 
@@ -568,7 +570,7 @@ void set_params(D &d, const fesomc_params &p) {
     d.wet_dry_on = p.wet_dry_on; d.key_rivers = p.key_rivers; d.TF_presence = p.TF_presence; d.cl_relax = p.cl_relax;
     d.beta_d = p.beta; d.Dmin_d = p.Dmin; d.dt_2D_d = p.dt_2D;
     d.bih_3D = p.bih_3D; d.Abh0 = p.Abh0;
-    d.filt_bi_3D = p.filt_bi_3D; d.filt_bi_2D = p.filt_bi_2D; d.tau_c = p.tau_c;
+    d.filt_bi_3D = p.filt_bi_3D; d.filt_bi_2D = p.filt_bi_2D; d.tau_c = p.tau_c; d.bih_2D = p.bih_2D;
 }
 
 // Algorithmic bytes per launch of every kernel: each array the kernel must
@@ -587,6 +589,8 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
                L * E * (16 + 16) + E * 16 + L * E * (16 + 32);
     if (k == "filt2x") return L * E * (16 + 16 + 8 * 4) + E * (16 + 8) + L * E * 16;
     if (k == "filt2x_2d") return E * (16 + 16 + 8 + 16);
+    if (k == "bih_2d") return 2 * (Ed * (16 + 8 + 32 + 8 + 16) + E * 32 + Ed * 16) + E * (16 + 16 + 8 + 8 + 16) +
+                              E * (16 + 16 + 64 + 16 + 32);
     if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
     if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
@@ -758,6 +762,7 @@ int enqueue_step(fesomc_model *m, double ff) {
         }
         if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { K3(launch_adv2d_edge, s); }); n += 1; }
         if (d.filt_bi_2D) { rec(m, "filt2x_2d", [&] { K3(launch_filt2x_2d, s); }); n += 1; }
+        if (d.bih_2D) { rec(m, "bih_2d", [&] { K3(launch_bih_2d, s); }); n += 4; }
         rec(m, "u2d_elem", [&] { K3(launch_u2d_elem, s); });
         rec(m, "rot_nodes", [&] { K3(launch_rot_nodes, s); });
         n += 2;
@@ -920,8 +925,10 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (par->fp32_form != 0 && par->fp32_form != 1) return FESOMC_EINVAL;
     if (par->bih_3D != 0 && par->bih_3D != 1) return FESOMC_EINVAL;
     if (par->bih_3D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
-    if ((par->filt_bi_3D != 0 && par->filt_bi_3D != 1) || (par->filt_bi_2D != 0 && par->filt_bi_2D != 1))
+    if ((par->filt_bi_3D != 0 && par->filt_bi_3D != 1) || (par->filt_bi_2D != 0 && par->filt_bi_2D != 1) ||
+        (par->bih_2D != 0 && par->bih_2D != 1))
         return FESOMC_EINVAL;
+    if (par->bih_2D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;

@@ -107,6 +107,7 @@ def default_params(**kw):
     p.tau_inv_filt, p.K_hor = 0.000046296, 0.010
     p.bih_3D, p.Abh0 = 0, 1000.0                  # LE_medium fv_run.dat:150,160
     p.filt_bi_3D, p.filt_bi_2D, p.tau_c = 0, 0, 0.4   # fv_run.dat:153,156,159
+    p.bih_2D = 0                                   # fv_run.dat:157
     p.Cd_bz, p.Bp_bz = 10.0, 5.0
     p.clim_relax = 1.0 / (15.0 * 3600.0 * 24.0)
     p.relax2clim_ac = 1.0 / (60.0 * 3600.0 * 24.0)

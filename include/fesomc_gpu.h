@@ -162,6 +162,9 @@ typedef struct fesomc_params {
      * src/fv_viscosity.F90:570-767)                                         */
     int32_t filt_bi_3D, filt_bi_2D;
     double tau_c;
+    /* biharmonic viscosity of the 2D momentum (bih_2D; biharmonic_2D,
+     * src/fv_viscosity.F90:338-568), with Abh0                              */
+    int32_t bih_2D;
 } fesomc_params;
 
 /*

@@ -394,6 +394,67 @@ static void viscosity_filt2x_2D(oracle_model *m) {
     free(V_c);
 }
 
+/* one 2D Laplacian edge loop of biharmonic_2D (fv_viscosity.F90:338-568,
+ * serial build, free_slip): fluxes of (Uin) with the gradients in vel_grad,
+ * internal edges then boundary edges, added to out (2,E) */
+static void bih2d_pass(oracle_model *m, const double *Uin, double *out) {
+    for (int ed = 1; ed <= m->Ed_in; ++ed) {
+        int e1 = EDT(1, ed), e2 = EDT(2, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH * 0.5 * (N1(m->elem_cos, e1) + N1(m->elem_cos, e2));
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double tx = -ECR(1, ed) + ECR(3, ed);
+        double ty = -ECR(2, ed) + ECR(4, ed);
+        double tl = sqrt(tx * tx + ty * ty);
+        tx = tx / tl;
+        ty = ty / tl;
+        double g1 = 0.5 * (VG(1, e1) + VG(1, e2));
+        double g2 = 0.5 * (VG(2, e1) + VG(2, e2));
+        double tt = g1 * tx + g2 * ty - (V2(Uin, 1, e2) - V2(Uin, 1, e1)) / tl;
+        g1 = g1 - tx * tt;
+        g2 = g2 - ty * tt;
+        double u1 = (g1 * ye - g2 * xe);
+        g1 = 0.5 * (VG(3, e1) + VG(3, e2));
+        g2 = 0.5 * (VG(4, e1) + VG(4, e2));
+        tt = g1 * tx + g2 * ty - (V2(Uin, 2, e2) - V2(Uin, 2, e1)) / tl;
+        g1 = g1 - tx * tt;
+        g2 = g2 - ty * tt;
+        double v1 = (g1 * ye - g2 * xe);
+        V2(out, 1, e1) = V2(out, 1, e1) + u1;
+        V2(out, 2, e1) = V2(out, 2, e1) + v1;
+        V2(out, 1, e2) = V2(out, 1, e2) - u1;
+        V2(out, 2, e2) = V2(out, 2, e2) - v1;
+    }
+    for (int ed = m->Ed_in + 1; ed <= m->Ed; ++ed) {
+        int e1 = EDT(1, ed);
+        double xe = EDXY(1, ed) * WP_R_EARTH;
+        double xed = xe * N1(m->elem_cos, e1);
+        double ye = EDXY(2, ed) * WP_R_EARTH;
+        double u1 = (VG(1, e1)) * ye - (VG(2, e1)) * xed;
+        double v1 = (VG(3, e1)) * ye - (VG(4, e1)) * xed;
+        u1 = ye * (u1 * ye - v1 * xe) / (xe * xe + ye * ye);
+        v1 = -xe * (u1 * ye - v1 * xe) / (xe * xe + ye * ye);   /* with the new u1, as the reference */
+        V2(out, 1, e1) = V2(out, 1, e1) + u1;
+        V2(out, 2, e1) = V2(out, 2, e1) + v1;
+    }
+}
+
+/* biharmonic_2D, fv_viscosity.F90:338-568 (its h_viscosity_2D call only
+ * fills Visc2D, which the routine does not use) */
+static void biharmonic_2D(oracle_model *m) {
+    double *Ul = calloc(2 * (size_t)m->E, sizeof(double));
+    bih2d_pass(m, m->UAB, Ul);
+    for (int el = 1; el <= m->E; ++el) {
+        double acc = 0.0;
+        for (int k = 1; k <= 4; ++k) acc = acc + WCV(k, el) * N1(m->ac, ELN(k, el));
+        double Ah = -m->p.Abh0 * sqrt(N1(m->elem_area, el) / m->p.scale_area) / m->p.scale_area;
+        V2(Ul, 1, el) = V2(Ul, 1, el) * (Ah) * acc;
+        V2(Ul, 2, el) = V2(Ul, 2, el) * (Ah) * acc;
+    }
+    vel_gradients_2D(m, Ul);
+    bih2d_pass(m, Ul, m->U_rhs_2D);
+    free(Ul);
+}
+
 static void update_2D_vel(oracle_model *m, int step) {
     (void)step;
     const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
@@ -422,6 +483,7 @@ static void update_2D_vel(oracle_model *m, int step) {
     if (m->p.mom_adv_2D == 2) momentum_adv_upwind_2D(m);
     if (m->p.filt_2D) viscosity_filt_2D(m);
     if (m->p.filt_bi_2D) viscosity_filt2x_2D(m);
+    if (m->p.bih_2D) biharmonic_2D(m);
     for (int el = 1; el <= m->E; ++el) {
         V2(m->U_rhs_2D, 1, el) = V2(m->U_rhs_2D, 1, el) + V2(m->U_rhs_2D_3D, 1, el);
         V2(m->U_rhs_2D, 2, el) = V2(m->U_rhs_2D, 2, el) + V2(m->U_rhs_2D_3D, 2, el);

@@ -75,3 +75,7 @@ def test_fp32_form_biharmonic(mods):
     b, _ = run(mods, mods[1].estuary("small", bih_3D=1, Abh0=1e4), 30, True)
     assert np.max(np.abs(a["TF"] - b["TF"])) < TS_MAX
     assert np.max(np.abs(a["U_n"] - b["U_n"])) < 1e-3
+    a, _ = run(mods, mods[1].estuary("small", bih_2D=1, Abh0=1e4), 30, False)
+    b, _ = run(mods, mods[1].estuary("small", bih_2D=1, Abh0=1e4), 30, True)
+    assert np.max(np.abs(a["TF"] - b["TF"])) < TS_MAX
+    assert np.max(np.abs(a["U_n_2D"] - b["U_n_2D"])) < 1e-3

@@ -227,6 +227,20 @@ def test_le_biharmonic_bit_exact(mods):
     assert bad == []
 
 
+def test_biharmonic_2d_bit_exact(mods):
+    """biharmonic_2D (bih_2D: two 2D Laplacians per sub-step, the second
+    one's gradients from vel_gradients_2D) on the small estuary, 30 steps,
+    and on LE, 20 steps."""
+    abi, cases, model, pyoracle = mods
+    bad, _, _ = run_pair(mods, cases.estuary("small", bih_2D=1, Abh0=1e4), 30)
+    assert bad == []
+    case = cases.le_medium()
+    case.params.Mt = 4
+    case.params.bih_2D = 1
+    bad, _, _ = run_pair(mods, case, 20)
+    assert bad == []
+
+
 def test_estuary_filter2x_bit_exact(mods):
     """viscosity_filt2x_3D and viscosity_filt2x_2D (filt_bi_3D / filt_bi_2D)
     on the small estuary, 30 steps, and on LE, 20 steps."""

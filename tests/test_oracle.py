@@ -184,6 +184,23 @@ def test_estuary_biharmonic_oracle(mods):
     assert 5.0 < d4 / d3 < 15.0
 
 
+def test_estuary_biharmonic_2d_oracle(mods):
+    """biharmonic_2D (bih_2D): changes the barotropic velocity, stays finite,
+    and its effect grows with Abh0."""
+    abi, cases, pyoracle = mods
+    out = {}
+    for ab in (0.0, 1e3, 1e4):
+        c = cases.estuary("small", bih_2D=1 if ab else 0, Abh0=ab if ab else 1000.0)
+        o = pyoracle.Oracle(c, abi, cases)
+        o.step(20)
+        out[ab] = o.state()
+        o.close()
+    d3 = np.abs(out[1e3]["U_n_2D"] - out[0.0]["U_n_2D"]).max()
+    d4 = np.abs(out[1e4]["U_n_2D"] - out[0.0]["U_n_2D"]).max()
+    assert np.isfinite(out[1e4]["U_n_2D"]).all() and np.isfinite(out[1e4]["eta_n"]).all()
+    assert 0.0 < d3 < d4
+
+
 def test_estuary_filter2x_oracle(mods):
     """viscosity_filt2x_3D / _2D: each switch changes the run, which stays
     finite."""
