@@ -4,7 +4,8 @@
  * for the same argument.  It serves the harmonic open-boundary elevation of
  * compute_ssh_rhs_elem (src/fv_average_dynamic.F90:190-216), evaluated on
  * the device by the forcing kernel and on the host by the CPU oracle and the
- * host forcing path alike; plain C, includable from C and CUDA C++.
+ * host forcing path alike, and the equilibrium tide of potential
+ * (src/fv_tide_potential.F90:1-107); plain C, includable from C and CUDA C++.
  *
  * Method: Cody-Waite reduction by pi/2 and the Taylor series.
  *   n = rint(x * 2/pi),  r = ((x - n P1) - n P2) - n P3,  |r| <= pi/4 + tiny,
@@ -14,7 +15,7 @@
  *   sin r = r + r z (-1/3! + z/5! - ... + z^7/17!),       z = r^2
  *   cos r = 1 - z/2 + z^2 (1/4! - z/6! + ... - z^7/18!)
  * (the first omitted terms are below 1e-19), the quadrant n mod 4 picks
- * +-sin / +-cos.  The 1 - z/2 step keeps its rounding error (the difference
+ * +-sin / +-cos (for sin x the quadrant shifted by one).  The 1 - z/2 step keeps its rounding error (the difference
  * (1 - v) - z/2 is exact) and adds it back.  Within one ulp of cos x over
  * the range; against glibc's cos over 2e7 random arguments in [-1000, 1000]
  * it differs in 3 % of them, by one ulp (tests/test_oracle.py holds the
@@ -61,8 +62,8 @@ FESOMC_TRIG_FN double fesomc_cos_kernel(double rh, double rl) {
     return v + (((1.0 - v) - hz) + ((z * z) * q - rh * rl));
 }
 
-FESOMC_TRIG_FN double fesomc_cos(double x) {
-    if (!(fabs(x) < 1.6e6)) return (x - x) / (x - x);     /* out of range, inf or NaN: NaN */
+/* x = n pi/2 + (rh + rl); returns n mod 4 (|x| < 1.6e6) */
+FESOMC_TRIG_FN int fesomc_reduce_pio2(double x, double *rh_out, double *rl_out) {
     const double n = rint(x * FESOMC_2_OVER_PI);
     /* reduced argument as rh + rl: a is exact, a - b is split exactly (two-sum) */
     const double a = x - n * FESOMC_PIO2_1;
@@ -72,12 +73,30 @@ FESOMC_TRIG_FN double fesomc_cos(double x) {
     const double e = (a - (t - tb)) - (b + tb);
     const double c = n * FESOMC_PIO2_3;
     const double rh = t - c;
-    const double rl = ((t - rh) - c) + e;
-    switch (((long long)n) & 3) {
+    *rh_out = rh;
+    *rl_out = ((t - rh) - c) + e;
+    return (int)(((long long)n) & 3);
+}
+
+FESOMC_TRIG_FN double fesomc_cos(double x) {
+    if (!(fabs(x) < 1.6e6)) return (x - x) / (x - x);     /* out of range, inf or NaN: NaN */
+    double rh, rl;
+    switch (fesomc_reduce_pio2(x, &rh, &rl)) {
         case 0: return fesomc_cos_kernel(rh, rl);
         case 1: return -fesomc_sin_kernel(rh, rl);
         case 2: return -fesomc_cos_kernel(rh, rl);
         default: return fesomc_sin_kernel(rh, rl);
+    }
+}
+
+FESOMC_TRIG_FN double fesomc_sin(double x) {
+    if (!(fabs(x) < 1.6e6)) return (x - x) / (x - x);
+    double rh, rl;
+    switch (fesomc_reduce_pio2(x, &rh, &rl)) {
+        case 0: return fesomc_sin_kernel(rh, rl);
+        case 1: return fesomc_cos_kernel(rh, rl);
+        case 2: return -fesomc_sin_kernel(rh, rl);
+        default: return -fesomc_cos_kernel(rh, rl);
     }
 }
 

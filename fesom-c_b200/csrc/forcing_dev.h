@@ -22,4 +22,19 @@ struct ForcingDev {
 
 void launch_forcing(const ForcingDev &f, cudaStream_t s);
 
+// Inputs of the tidal potential kernel: the step's time_jd from 'clock'
+// (advanced by k_forcing_clock, or uploaded by the host path), node
+// coordinates (lon, lat) in radians, the harmonic switches a_th of the 11
+// equilibrium waves (M2, S2, N2, K2, K1, O1, P1, Q1, Mf, Mm, Ssa).
+struct PotentialDev {
+    int N;
+    double time_jd0;
+    double ath[11];
+    const double *clock;
+    const double2 *coord;
+    double *ssh_gp;
+};
+
+void launch_potential(const PotentialDev &p, cudaStream_t s);
+
 }  // namespace fesomc

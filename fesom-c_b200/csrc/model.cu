@@ -120,6 +120,7 @@ struct fesomc_model {
     bool dev_forcing = false;
     int river_ramp = 0;
     double *d_clock = nullptr, *d_ampt = nullptr, *d_fazt = nullptr, *d_harm = nullptr, *d_runoff_base = nullptr;
+    const double2 *d_coord = nullptr;       // node (lon, lat) for the tidal potential
     // diagnostics
     double *d_epart = nullptr, *d_eout = nullptr;
     unsigned int *h_status = nullptr;
@@ -589,6 +590,7 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
                L * E * (16 + 16) + E * 16 + L * E * (16 + 32);
     if (k == "filt2x") return L * E * (16 + 16 + 8 * 4) + E * (16 + 8) + L * E * 16;
     if (k == "filt2x_2d") return E * (16 + 16 + 8 + 16);
+    if (k == "potential") return N * (16 + 8);   // coordinates in, ssh_gp out
     if (k == "bih_2d") return 2 * (Ed * (16 + 8 + 32 + 8 + 16) + E * 32 + Ed * 16) + E * (16 + 16 + 8 + 8 + 16) +
                               E * (16 + 16 + 64 + 16 + 32);
     if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
@@ -655,7 +657,7 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
 double kernel_bytes(const fesomc_model *m, const std::string &k) {
     const double b = kernel_bytes_fp64(m, k);
     if (!m->fp32) return b;
-    if (k == "ssh_node" || k == "rot_nodes" || k == "jac_swap" || k == "forcing") return b;
+    if (k == "ssh_node" || k == "rot_nodes" || k == "jac_swap" || k == "forcing" || k == "potential") return b;
     return 0.5 * b;
 }
 
@@ -727,6 +729,19 @@ int enqueue_step(fesomc_model *m, double ff) {
     if (m->dev_forcing) {
         rec(m, "forcing", [&] { launch_forcing(forcing_view(m), s); });
         n += 2;
+    }
+    if (m->p.T_potential) {
+        // potential at the head of oce_timestep (fv_main.F90:1899)
+        PotentialDev pd{};
+        pd.N = d.N;
+        pd.time_jd0 = m->p.time_jd0;
+        for (int k = 0; k < m->p.n_harm; ++k)
+            if (m->p.harm_index[k] >= 0 && m->p.harm_index[k] < 11) pd.ath[m->p.harm_index[k]] = 1.0;
+        pd.clock = m->d_clock;
+        pd.coord = m->d_coord;
+        pd.ssh_gp = f ? q.ssh_gp : d.ssh_gp;
+        rec(m, "potential", [&] { launch_potential(pd, s); });
+        n += 1;
     }
     rec(m, "pressure_col", [&] { K3(launch_pressure_col, s); });
     rec(m, "bpg_elem", [&] { K3(launch_bpg_elem, s); });
@@ -816,7 +831,8 @@ int upload_step_inputs(fesomc_model *m, double time, double time_jd) {
     const int nobn = m->d.nobn, nr = m->d.n_rivers;
     const bool need_ob = m->p.TF_presence && nobn > 0;
     const bool need_r = m->p.key_rivers && nr > 0 && m->runoff_dirty;
-    if (!need_ob && !need_r) return FESOMC_OK;
+    const bool need_clock = m->p.T_potential != 0;
+    if (!need_ob && !need_r && !need_clock) return FESOMC_OK;
     const int i = m->stage_i;
     m->stage_i ^= 1;
     CK(cudaEventSynchronize(m->stage_ev[i]));
@@ -831,6 +847,12 @@ int upload_step_inputs(fesomc_model *m, double time, double time_jd) {
         std::memcpy(h + off, m->h_runoff, sizeof(double) * nr);
         CK(cudaMemcpyAsync(m->d.runoff, h + off, sizeof(double) * nr, cudaMemcpyHostToDevice, m->stream));
         m->runoff_dirty = false;
+        off += (size_t)nr;
+    }
+    if (need_clock) {
+        // the step's time_jd for the tidal potential kernel
+        h[off] = time_jd;
+        CK(cudaMemcpyAsync(m->d_clock, h + off, sizeof(double), cudaMemcpyHostToDevice, m->stream));
     }
     CK(cudaEventRecord(m->stage_ev[i], m->stream));
     return FESOMC_OK;
@@ -929,6 +951,7 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
         (par->bih_2D != 0 && par->bih_2D != 1))
         return FESOMC_EINVAL;
     if (par->bih_2D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
+    if (par->T_potential != 0 && par->T_potential != 1) return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;
@@ -970,6 +993,13 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (cudaMallocHost(&m->h_runoff, sizeof(double) * (mesh->n_rivers + 1)) != cudaSuccess) return fail(FESOMC_ENOMEM);
     std::memset(m->h_runoff, 0, sizeof(double) * (mesh->n_rivers + 1));
     if (cudaMallocHost(&m->h_status, sizeof(unsigned) * 2) != cudaSuccess) return fail(FESOMC_ENOMEM);
+    if (par->T_potential) {
+        if (!mesh->coord_nod2D) return fail(FESOMC_EINVAL);
+        std::vector<double2> lonlat((size_t)mesh->nod2D);
+        for (int i = 0; i < mesh->nod2D; ++i)
+            lonlat[i] = make_double2(mesh->coord_nod2D[2 * (size_t)i], mesh->coord_nod2D[2 * (size_t)i + 1]);
+        if ((rc = upload(m, &m->d_coord, lonlat)) || (rc = dalloc(m, &m->d_clock, 1))) return fail(rc);
+    }
     if (cudaMallocHost(&m->h_notconv, sizeof(int) * 2) != cudaSuccess) return fail(FESOMC_ENOMEM);
     // state upload (all groups that are provided)
     if ((rc = fesomc_gpu_sync_from_host(m, FESOMC_F_ALL, st))) return fail(rc);
@@ -1048,9 +1078,10 @@ int fesomc_gpu_set_device_forcing(fesomc_model *m, const double *runoff_base, in
     if (rivers && !runoff_base) return FESOMC_EINVAL;
     int rc;
     CK(cudaStreamSynchronize(m->stream));
-    if (!m->d_clock) {
+    if (!m->d_clock && (rc = dalloc(m, &m->d_clock, 1))) return rc;
+    if (!m->d_ampt) {
         const size_t nobn = (size_t)(d.nobn > 0 ? d.nobn : 1);
-        if ((rc = dalloc(m, &m->d_clock, 1)) || (rc = dalloc(m, &m->d_ampt, 12 * nobn)) ||
+        if ((rc = dalloc(m, &m->d_ampt, 12 * nobn)) ||
             (rc = dalloc(m, &m->d_fazt, 12 * nobn)) || (rc = dalloc(m, &m->d_harm, 36)) ||
             (rc = dalloc(m, &m->d_runoff_base, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1))))
             return rc;

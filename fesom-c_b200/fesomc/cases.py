@@ -108,6 +108,7 @@ def default_params(**kw):
     p.bih_3D, p.Abh0 = 0, 1000.0                  # LE_medium fv_run.dat:150,160
     p.filt_bi_3D, p.filt_bi_2D, p.tau_c = 0, 0, 0.4   # fv_run.dat:153,156,159
     p.bih_2D = 0                                   # fv_run.dat:157
+    p.T_potential = 0
     p.Cd_bz, p.Bp_bz = 10.0, 5.0
     p.clim_relax = 1.0 / (15.0 * 3600.0 * 24.0)
     p.relax2clim_ac = 1.0 / (60.0 * 3600.0 * 24.0)
@@ -311,8 +312,10 @@ def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=
     xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1,
                                                             noise_sigma=noise_sigma)
     rivers = np.arange(0, nyn) * nxn + 1                 # every node on x = 0 (1-based)
+    # T_potential switches both the potential and the mesh's a_tp weights
     mesh = HostMesh(xy, index, elems, depth, cartesian=True, nsigma=nsigma, coriolis_on=True,
-                    lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius)
+                    lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius,
+                    T_potential=bool(overrides.get("T_potential", 0)))
     lib = abi.load()
     kw = dict(dt=20.0, dt_2D=2.0, Dmin=1.0, C_d=0.0025, tracer_adv=tracer_adv, wet_dry_on=1,
               key_rivers=1, TF_presence=1, temp_on=1, salinity_on=1, filt_2D=1, filt_3D=1,

@@ -165,6 +165,13 @@ typedef struct fesomc_params {
     /* biharmonic viscosity of the 2D momentum (bih_2D; biharmonic_2D,
      * src/fv_viscosity.F90:338-568), with Abh0                              */
     int32_t bih_2D;
+    /* tidal potential (T_potential of fv_run.dat, src/fv_read_run.F90:651):
+     * potential (src/fv_tide_potential.F90:1-107, called at the head of
+     * oce_timestep, src/fv_main.F90:1899) writes the equilibrium tide of
+     * the harmonics in harm_index (M2..Ssa) into ssh_gp every step, on the
+     * device; build the mesh with the same flag for its a_tp
+     * (src/fv_ini.F90:94-107).                                              */
+    int32_t T_potential;
 } fesomc_params;
 
 /*

@@ -60,7 +60,7 @@ typedef struct oracle_model {
         *nod_in_elem2D_num, *nod_in_elem2D, *edge_up_dn_tri, *in_obn, *nod_rivers;
     int nobn, n_rivers;
     double *depth, *area, *elem_area, *elem_cos, *coriolis, *w_cv, *gradient_sca, *gradient_vec,
-        *edge_dxdy, *edge_cross_dxdy, *sigma, *a_tp, *ac;
+        *edge_dxdy, *edge_cross_dxdy, *sigma, *a_tp, *ac, *coord;
     /* 2D state */
     double *eta_n, *eta_n_1, *eta_n_2, *etaAB, *ssh_rhs, *ssh_gp, *eta_p, *eta_tmp;
     double *U_n_2D, *U_n_1, *U_n_2, *UAB, *U_rhs_2D, *U_rhs_2D_3D, *vel_grad, *dmean_n;
@@ -149,6 +149,7 @@ static double densityJM(double t, double s, double pz, double density_0) {
 /* the shared logarithm and cosine, exported for their accuracy tests */
 double oracle_log(double x) { return fesomc_log(x); }
 double oracle_cos(double x) { return fesomc_cos(x); }
+double oracle_sin(double x) { return fesomc_sin(x); }
 
 double oracle_densityJM(double t, double s, double pz, double density_0) {
     return densityJM(t, s, pz, density_0);
@@ -2043,11 +2044,74 @@ static void solve_tracers(oracle_model *m) {
     tracer_impl_vert_diff(m);
 }
 
+/* control_360, fv_tide_potential.F90:109-120 (float(iz) is exact here) */
+static double control_360(double fr) {
+    int iz = (int)(fr / 360.0);
+    if (iz >= 1) fr = fr - (double)iz * 360.0;
+    return fr;
+}
+
+/* potential, fv_tide_potential.F90:1-107: the equilibrium tide of 11
+ * harmonics (those of the harmonic list, a_th) into ssh_gp, ramped in over
+ * the first 5 days.  Sine and cosine are the shared IEEE-only ones. */
+static void potential(oracle_model *m) {
+    static const double Apt[11] = {0.242334, 0.112841, 0.046398, 0.030704, 0.141565, 0.100514,
+                                   0.046843, 0.019256, 0.041742, 0.022026, 0.019446};
+    static const double Fpt[11] = {1.40519e-4, 1.45444e-4, 1.37880e-4, 1.45842e-4, 0.72921e-4, 0.67598e-4,
+                                   0.72523e-4, 0.64959e-4, 0.53234e-5, 0.26392e-5, 0.03982e-5};
+    const double rad = WP_PI / 180.0;
+    double ath[11] = {0};
+    for (int k = 0; k < m->p.n_harm; ++k)
+        if (m->p.harm_index[k] >= 0 && m->p.harm_index[k] < 11) ath[m->p.harm_index[k]] = 1.0;
+    double DY = m->time_jd - 2442413.5;
+    double TY = (27392.500528 + 1.0000000356 * DY) / 36525.0;
+    double TY2 = TY * TY, TY3 = TY2 * TY;
+    double h0 = control_360(279.69668 + 36000.768930485 * TY + 3.03e-4 * TY2);
+    double s0 = control_360(270.434358 + 481267.88314137 * TY - 0.001133 * TY2 + 1.9e-6 * TY3);
+    double p0 = control_360(334.329653 + 4069.0340329575 * TY - 0.010325 * TY2 - 1.2e-5 * TY3);
+    double sxi[11];
+    sxi[0] = (h0 - s0) * 2.0 * rad;
+    sxi[1] = 0.0;
+    sxi[2] = (2.0 * h0 - 3.0 * s0 + p0) * rad;
+    sxi[3] = 2.0 * h0 * rad;
+    sxi[4] = (h0 + 90.0) * rad;
+    sxi[5] = (h0 - 2.0 * s0 - 90.0) * rad;
+    sxi[6] = (h0 - 90.0) * rad;
+    sxi[7] = (h0 - 3.0 * s0 + p0 - 90.0) * rad;
+    sxi[8] = 2.0 * s0 * rad;
+    sxi[9] = (s0 - p0) * rad;
+    sxi[10] = 2.0 * h0 * rad;
+    for (int n = 1; n <= m->N; ++n) {
+        double lon = m->coord[2 * (n - 1)], lat = m->coord[2 * (n - 1) + 1];
+        double ssh_sd = 0.0, ssh_d = 0.0, ssh_lp = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            double time_cor = DY * 86400.0 - sxi[j] / Fpt[j];
+            ssh_sd = ssh_sd + ath[j] * Apt[j] * fesomc_sin(0.5 * WP_PI - lat) * fesomc_sin(0.5 * WP_PI - lat)
+                              * fesomc_cos(Fpt[j] * time_cor + 2.0 * lon + sxi[j]);
+        }
+        for (int j = 4; j < 8; ++j) {
+            double time_cor = DY * 86400.0 - sxi[j] / Fpt[j];
+            ssh_d = ssh_d + ath[j] * Apt[j] * fesomc_sin(2.0 * (0.5 * WP_PI - lat))
+                            * fesomc_cos(Fpt[j] * time_cor + lon + sxi[j]);
+        }
+        for (int j = 8; j < 11; ++j) {
+            double time_cor = DY * 86400.0 - sxi[j] / Fpt[j];
+            double sl = fesomc_sin(0.5 * WP_PI - lat);
+            ssh_lp = ssh_lp + ath[j] * Apt[j] * (3.0 * (sl * sl) - 2.0) * fesomc_cos(Fpt[j] * time_cor + sxi[j]);
+        }
+        N1(m->ssh_gp, n) = ssh_sd + ssh_d + ssh_lp;
+        if (m->time_jd - m->p.time_jd0 < 5.0)
+            N1(m->ssh_gp, n) = N1(m->ssh_gp, n) * (m->time_jd - m->p.time_jd0) / 5.0;
+    }
+}
+
 /* oce_timestep case(3), fv_main.F90:1983-2095, preceded by the time update
- * of the main loop (fv_main.F90:400-401). */
+ * of the main loop (fv_main.F90:400-401) and, with T_potential, by the
+ * tidal potential (fv_main.F90:1899). */
 static void oce_timestep(oracle_model *m) {
     m->time_jd = m->time_jd + m->p.dt / 86400.0;
     m->time = m->time_jd * 86400.0;
+    if (m->p.T_potential) potential(m);
     pressure(m);
     compute_el2nodes_3D(m, m->U_n, m->V_n, m->Unode, m->Vnode);
     if (m->p.ver_mix == 3) d3_end(m);
@@ -2108,6 +2172,7 @@ oracle_model *oracle_create(const fesomc_mesh *msh, const fesomc_params *par, co
     m->gradient_sca = dcopy(msh->gradient_sca, 8 * E); m->gradient_vec = dcopy(msh->gradient_vec, 8 * E);
     m->edge_dxdy = dcopy(msh->edge_dxdy, 2 * Ed); m->edge_cross_dxdy = dcopy(msh->edge_cross_dxdy, 4 * Ed);
     m->sigma = dcopy(msh->sigma, NS); m->a_tp = dcopy(msh->a_tp, 2 * N); m->ac = dcopy(msh->ac, N);
+    m->coord = dcopy(msh->coord_nod2D, 2 * N);
 #define ST(field, n) m->field = dcopy(st->field, n)
     ST(eta_n, N); ST(eta_n_1, N); ST(eta_n_2, N); ST(etaAB, N); ST(ssh_gp, N);
     ST(U_n_2D, 2 * E); ST(U_n_1, 2 * E); ST(U_n_2, 2 * E); ST(U_filt_2D, E); ST(V_filt_2D, E);
@@ -2217,7 +2282,7 @@ void oracle_free(oracle_model *m) {
     void *ptrs[] = {m->index_nod2D, m->elem2D_nodes, m->edge_nodes, m->edge_tri, m->elem_edges, m->elem_neighbors,
                     m->nod_in_elem2D_num, m->nod_in_elem2D, m->edge_up_dn_tri, m->in_obn, m->nod_rivers,
                     m->depth, m->area, m->elem_area, m->elem_cos, m->coriolis, m->w_cv, m->gradient_sca,
-                    m->gradient_vec, m->edge_dxdy, m->edge_cross_dxdy, m->sigma, m->a_tp, m->ac,
+                    m->gradient_vec, m->edge_dxdy, m->edge_cross_dxdy, m->sigma, m->a_tp, m->ac, m->coord,
                     m->eta_n, m->eta_n_1, m->eta_n_2, m->etaAB, m->ssh_rhs, m->ssh_gp, m->eta_p, m->eta_tmp,
                     m->U_n_2D, m->U_n_1, m->U_n_2, m->UAB, m->U_rhs_2D, m->U_rhs_2D_3D, m->vel_grad, m->dmean_n,
                     m->U_filt_2D, m->V_filt_2D, m->taux, m->tauy, m->windx, m->windy, m->C_d_el,

@@ -53,6 +53,8 @@ def load(abi):
         lib.oracle_log.argtypes = [C.c_double]
         lib.oracle_cos.restype = C.c_double
         lib.oracle_cos.argtypes = [C.c_double]
+        lib.oracle_sin.restype = C.c_double
+        lib.oracle_sin.argtypes = [C.c_double]
         _lib = lib
     return _lib
 

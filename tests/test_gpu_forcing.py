@@ -10,13 +10,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 STEPS = 40
-FIELDS = ["eta_n", "eta_n_1", "etaAB", "U_n_2D", "U_n", "V_n", "TF", "SF", "Wvel", "Kv", "mask_wd_node"]
+FIELDS = ["eta_n", "eta_n_1", "etaAB", "U_n_2D", "U_n", "V_n", "TF", "SF", "Wvel", "Kv", "mask_wd_node",
+          "ssh_gp"]
 
 
-@pytest.mark.parametrize("fp32", [0, 1])
-def test_device_forcing_matches_host_forcing(built, fp32):
+@pytest.mark.parametrize("fp32,potential", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_device_forcing_matches_host_forcing(built, fp32, potential):
+    """With T_potential the potential kernel reads the device clock, which
+    the host path uploads each step and device forcing advances itself."""
     from fesomc import abi, cases, model
-    case = cases.estuary("small")
+    case = cases.estuary("small", T_potential=potential)
     case.params.fp32_form = fp32
     # host path: the forcing of every step pushed from the host
     g = model.GpuModel(case)

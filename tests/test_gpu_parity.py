@@ -241,6 +241,27 @@ def test_biharmonic_2d_bit_exact(mods):
     assert bad == []
 
 
+def test_tidal_potential_bit_exact(mods):
+    """T_potential: the potential kernel (all 11 equilibrium harmonics, the
+    shared IEEE-only sine and cosine) gives the oracle's ssh_gp, and the run
+    that feels it stays bit-exact, 30 steps."""
+    abi, cases, model, pyoracle = mods
+    case = cases.estuary("small", T_potential=1)
+    case.params.n_harm = 11
+    for j in range(11):
+        case.params.harm_index[j] = j
+    g = model.GpuModel(case)
+    o = pyoracle.Oracle(case, abi, cases)
+    g.step(30)
+    o.step(30)
+    sg, so = g.state(), o.state()
+    g.close()
+    o.close()
+    assert np.abs(so["ssh_gp"]).max() > 0.0
+    assert np.array_equal(sg["ssh_gp"], so["ssh_gp"])
+    assert compare(sg, so) == []
+
+
 def test_estuary_filter2x_bit_exact(mods):
     """viscosity_filt2x_3D and viscosity_filt2x_2D (filt_bi_3D / filt_bi_2D)
     on the small estuary, 30 steps, and on LE, 20 steps."""

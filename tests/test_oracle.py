@@ -166,6 +166,97 @@ def test_shared_cos_within_one_ulp_of_libm(mods):
     assert math.isnan(lib.oracle_cos(2e6)) and math.isnan(lib.oracle_cos(math.inf))
 
 
+def test_shared_sin_within_one_ulp_of_libm(mods):
+    """fesomc_sin (the equilibrium tide of the tidal potential) against the C
+    library's sin, as the cosine above."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    rng = np.random.default_rng(8)
+    xs = np.concatenate([rng.uniform(-4.0, 4.0, 20000), rng.uniform(-1000.0, 1000.0, 10000),
+                         [0.0, 1e-300, -1e-300, math.pi / 2, math.pi, 0.5 * 3.14159265358979]])
+    ours = np.array([lib.oracle_sin(float(x)) for x in xs])
+    ref = np.array([math.sin(float(x)) for x in xs])
+    ulps = np.abs(ours.view(np.int64) - ref.view(np.int64))
+    ok = (ulps <= 1) | (np.abs(ours - ref) <= 2.3e-16)
+    assert ok.all()
+    assert lib.oracle_sin(0.0) == 0.0 and lib.oracle_sin(1e-300) == 1e-300
+    assert math.isnan(lib.oracle_sin(2e6))
+
+
+def potential_numpy(time_jd, time_jd0, coord, ath):
+    """potential (fv_tide_potential.F90:1-107) in numpy with the C library's
+    sine and cosine: an independent restatement that pins the oracle's."""
+    pi = 3.14159265358979
+    rad = pi / 180.0
+    Apt = np.array([0.242334, 0.112841, 0.046398, 0.030704, 0.141565, 0.100514, 0.046843, 0.019256,
+                    0.041742, 0.022026, 0.019446])
+    Fpt = np.array([1.40519e-4, 1.45444e-4, 1.37880e-4, 1.45842e-4, 0.72921e-4, 0.67598e-4, 0.72523e-4,
+                    0.64959e-4, 0.53234e-5, 0.26392e-5, 0.03982e-5])
+
+    def c360(fr):
+        iz = int(fr / 360.0)
+        return fr - iz * 360.0 if iz >= 1 else fr
+
+    DY = time_jd - 2442413.5
+    TY = (27392.500528 + 1.0000000356 * DY) / 36525.0
+    h0 = c360(279.69668 + 36000.768930485 * TY + 3.03e-4 * TY ** 2)
+    s0 = c360(270.434358 + 481267.88314137 * TY - 0.001133 * TY ** 2 + 1.9e-6 * TY ** 3)
+    p0 = c360(334.329653 + 4069.0340329575 * TY - 0.010325 * TY ** 2 - 1.2e-5 * TY ** 3)
+    sxi = np.array([(h0 - s0) * 2 * rad, 0.0, (2 * h0 - 3 * s0 + p0) * rad, 2 * h0 * rad, (h0 + 90) * rad,
+                    (h0 - 2 * s0 - 90) * rad, (h0 - 90) * rad, (h0 - 3 * s0 + p0 - 90) * rad, 2 * s0 * rad,
+                    (s0 - p0) * rad, 2 * h0 * rad])
+    lon, lat = coord[:, 0], coord[:, 1]
+    colat = 0.5 * pi - lat
+    out = np.zeros(len(lon))
+    for j in range(11):
+        arg_t = Fpt[j] * (DY * 86400.0 - sxi[j] / Fpt[j]) + sxi[j]
+        if j < 4:
+            out += ath[j] * Apt[j] * np.sin(colat) ** 2 * np.cos(arg_t + 2 * lon)
+        elif j < 8:
+            out += ath[j] * Apt[j] * np.sin(2 * colat) * np.cos(arg_t + lon)
+        else:
+            out += ath[j] * Apt[j] * (3 * np.sin(colat) ** 2 - 2) * np.cos(arg_t)
+    if time_jd - time_jd0 < 5.0:
+        out = out * (time_jd - time_jd0) / 5.0
+    return out
+
+
+def test_tidal_potential_oracle(mods):
+    """T_potential: the oracle's ssh_gp after a step equals the numpy
+    restatement to rounding (the two use different sines and cosines), with
+    all 11 harmonics and with M2 alone, and the potential changes the run."""
+    abi, cases, pyoracle = mods
+    c = cases.estuary("small", T_potential=1)
+    c.params.n_harm = 11
+    for j in range(11):
+        c.params.harm_index[j] = j
+    coord = c.mesh.arr("coord_nod2D", (c.mesh.N, 2)).copy()
+    o = pyoracle.Oracle(c, abi, cases)
+    o.step(3)
+    s = o.state()
+    o.close()
+    ref = potential_numpy(o.time_jd, c.params.time_jd0, coord, np.ones(11))
+    assert np.abs(ref).max() > 0.0
+    assert np.allclose(s["ssh_gp"], ref, rtol=0.0, atol=1e-12 * np.abs(ref).max())
+    # only the listed harmonics
+    c1 = cases.estuary("small", T_potential=1)
+    o = pyoracle.Oracle(c1, abi, cases)
+    o.step(3)
+    s1 = o.state()
+    o.close()
+    ath = np.zeros(11)
+    ath[0] = 1.0
+    ref1 = potential_numpy(o.time_jd, c1.params.time_jd0, coord, ath)
+    assert np.allclose(s1["ssh_gp"], ref1, rtol=0.0, atol=1e-12 * np.abs(ref1).max())
+    c0 = cases.estuary("small")
+    o = pyoracle.Oracle(c0, abi, cases)
+    o.step(3)
+    s0 = o.state()
+    o.close()
+    assert not np.array_equal(s0["U_n_2D"], s1["U_n_2D"])
+    assert np.all(s0["ssh_gp"] == 0.0)
+
+
 def test_estuary_biharmonic_oracle(mods):
     """biharmonic_viscosity (bih_3D): active, finite, and linear in Abh0 for
     a small viscosity (the damping of a fixed flow field doubles with it)."""
