@@ -194,23 +194,31 @@ __global__ void k_p1_edge(Dev d) {
 }
 
 // Element part of momentum_adv_P1_3D_to_2D, optional
-// viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939), divided by dmean_n
-// (fv_main.F90:1504-1513).
+// viscosity_filt_3D_to_2D (fv_viscosity.F90:870-939) and
+// biharmonic_viscosity_3D_to_2D, divided by dmean_n (fv_main.F90:1504-1513).
 // A block takes B consecutive elements with one thread per (element, level)
-// (coalesced column loads).  Every thread writes its level's terms for the
-// element's edge slots and the filter into shared memory; then one thread
-// per element sums them in the reference's order: each slot's level sum
-// in level order (the slot sums are independent chains, interleaved), then
-// the slot contributions in slot order, then the filter terms.
+// (coalesced column loads); every thread writes its level's terms of the
+// element's edge slots and of the filter / biharmonic slots into shared
+// memory, and the first threads of each element also stage its edge codes,
+// the nodal factors acc of its edges and dmean_n.  Then, in the reference's
+// order of operations: one thread per (element, edge slot, component) sums
+// the slot over the levels in level order; one thread per (element,
+// component) adds the slot sums in slot order and the filter and
+// biharmonic terms level by level.
 constexpr int kP1Slots = 5;  // 4 internal-edge slots + the filter
 __global__ void k_p1_elem(Dev d) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L;
     const int B = (int)blockDim.x / L;
     const int nsl = kP1Slots + (d.bih_3D ? 1 : 0);  // + biharmonic_viscosity_3D_to_2D
     const int S = 2 * nsl * L + 1;  // per-element stride, odd: conflict-free
+    real *sm = reinterpret_cast<real *>(sm_raw);
+    real *sums = sm + (size_t)B * S;     // [B][8]: level sums of (slot, component)
+    real *accs = sums + (size_t)B * 8;   // [B][4]: acc of the edge slots
+    real *dms = accs + (size_t)B * 4;    // [B]: dmean_n
+    int *cds = reinterpret_cast<int *>(dms + B);  // [B][4]: edge codes
     const int jl = (int)threadIdx.x / L, z = (int)threadIdx.x % L;
+    const int nt = (int)blockDim.x;
     for (long long eb = (long long)blockIdx.x * B; eb < d.E; eb += (long long)gridDim.x * B) {
         const long long e_ = eb + jl;
         if (jl < B && e_ < d.E) {
@@ -219,6 +227,15 @@ __global__ void k_p1_elem(Dev d) {
             const real je = d.Je[(size_t)e * L + z];
             const int4 il = d.elem_iedges[e];
             const int codes[4] = {il.x, il.y, il.z, il.w};
+            for (int c = z; c < 4; c += L) {
+                const int code = c == 0 ? il.x : c == 1 ? il.y : c == 2 ? il.z : il.w;
+                cds[jl * 4 + c] = code;
+                if (code >= 0) {
+                    const int2 nn = d.edge_nodes[code >> 1];
+                    accs[jl * 4 + c] = (d.ac[nn.x] + d.ac[nn.y]) * real(.5);
+                }
+            }
+            if (z == 0) dms[jl] = d.dmean_n[e];
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 if (codes[c] >= 0) {
@@ -254,42 +271,38 @@ __global__ void k_p1_elem(Dev d) {
             }
         }
         __syncthreads();
-        const long long es = eb + threadIdx.x;
-        if ((int)threadIdx.x < B && es < d.E) {
-            const int e = (int)es;
-            const real *T = sm + (size_t)threadIdx.x * S;
-            const int4 il = d.elem_iedges[e];
-            const int codes[4] = {il.x, il.y, il.z, il.w};
-            real su[4] = {real(0.0), real(0.0), real(0.0), real(0.0)}, sv[4] = {real(0.0), real(0.0), real(0.0), real(0.0)};
-            for (int k = 0; k < L; ++k) {
+        // level sums of the edge slots, one thread per (element, slot, component)
+        for (int t = (int)threadIdx.x; t < B * 8; t += nt) {
+            const int j = t >> 3, ch = t & 7;
+            if (eb + j < d.E && cds[j * 4 + (ch >> 1)] >= 0) {
+                const real *T = sm + (size_t)j * S + (size_t)ch * L;
+                real sl = real(0.0);
+                for (int k = 0; k < L; ++k) sl = sl + T[k];
+                sums[j * 8 + ch] = sl;
+            }
+        }
+        __syncthreads();
+        // one thread per (element, component)
+        for (int t = (int)threadIdx.x; t < B * 2; t += nt) {
+            const int j = t >> 1, uv = t & 1;
+            const long long es = eb + j;
+            if (es < d.E) {
+                real r = real(0.0);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    su[c] = su[c] + T[(c * 2 + 0) * L + k];
-                    sv[c] = sv[c] + T[(c * 2 + 1) * L + k];
+                    const int code = cds[j * 4 + c];
+                    if (code < 0) break;
+                    const real a = accs[j * 4 + c], sc = sums[j * 8 + c * 2 + uv];
+                    if (code & 1) r = r + a * sc;
+                    else r = r - a * sc;
                 }
+                const real *T = sm + (size_t)j * S;
+                if (d.filt_3D)
+                    for (int k = 0; k < L; ++k) r = r + T[(4 * 2 + uv) * L + k];
+                if (d.bih_3D)
+                    for (int k = 0; k < L; ++k) r = r + T[(5 * 2 + uv) * L + k];
+                reinterpret_cast<real *>(d.U_rhs_2D_3D)[2 * es + uv] = r / dms[j];
             }
-            real rx = real(0.0), ry = real(0.0);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int code = codes[c];
-                if (code < 0) break;
-                const int2 nn = d.edge_nodes[code >> 1];
-                const real acc = (d.ac[nn.x] + d.ac[nn.y]) * real(.5);
-                if (code & 1) { rx = rx + acc * su[c]; ry = ry + acc * sv[c]; }
-                else { rx = rx - acc * su[c]; ry = ry - acc * sv[c]; }
-            }
-            if (d.filt_3D)
-                for (int k = 0; k < L; ++k) {
-                    rx = rx + T[(4 * 2 + 0) * L + k];
-                    ry = ry + T[(4 * 2 + 1) * L + k];
-                }
-            if (d.bih_3D)
-                for (int k = 0; k < L; ++k) {
-                    rx = rx + T[(5 * 2 + 0) * L + k];
-                    ry = ry + T[(5 * 2 + 1) * L + k];
-                }
-            const real dm = d.dmean_n[e];
-            d.U_rhs_2D_3D[e] = make_real2(rx / dm, ry / dm);
         }
         __syncthreads();
     }
@@ -606,10 +619,12 @@ void launch_puls_elem(const Dev &d, cudaStream_t s) {
 void launch_el2nodes(const Dev &d, const real *Ue, const real *Ve, real *Un, real *Vn, cudaStream_t s) {
     k_el2nodes<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d, Ue, Ve, Un, Vn);
 }
-// B elements per block: B*L threads, at most 1024 and at most 32 elements
+// B elements per block: B*L threads, at most 1024 and at most 32 elements;
+// per element its slot tile, 8 slot sums, 4 acc, dmean_n and 4 edge codes
 static int p1_elems(const Dev &d) { int b = 1024 / d.L; return b > 32 ? 32 : b; }
 static size_t p1_smem(const Dev &d) {
-    return (size_t)p1_elems(d) * (2 * (kP1Slots + (d.bih_3D ? 1 : 0)) * d.L + 1) * sizeof(real);
+    return (size_t)p1_elems(d) * ((2 * (kP1Slots + (d.bih_3D ? 1 : 0)) * d.L + 1 + 13) * sizeof(real) +
+                                  4 * sizeof(int));
 }
 int config_p1(const Dev &d) {
     return raise_smem_limit(k_p1_elem, p1_smem(d)) == cudaSuccess
