@@ -339,8 +339,9 @@ __device__ __forceinline__ real muscl_mean(bool upw2, real Tm1, real Tm2) {
 // MUSCL segment fluxes of one (edge, level) (fv_tracer.F90:59-170 for T and
 // S, :172-209 for the continuity term); thread per (edge, level), levels on
 // consecutive threads.  Each flux is computed once here and gathered by both
-// end nodes below.
-__global__ void k_muscl_edge(Dev d) {
+// end nodes below.  64 registers: 32 resident warps per SM instead of 24
+// (17 % faster).
+__global__ void __maxnreg__(64) k_muscl_edge(Dev d) {
     const long long total = (long long)d.Ed * d.L;
     const int L = d.L;
     GRID_LOOP(ii, total) {
