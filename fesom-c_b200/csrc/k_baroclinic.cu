@@ -32,7 +32,7 @@ struct ColBlock {
 // pressure (fv_pressure_new.F90:91-107): density per (node, level), the
 // hydrostatic sum per node in level order
 // ---------------------------------------------------------------------------
-__global__ void k_pressure_col(Dev d) {
+__global__ void __launch_bounds__(1024) k_pressure_col(Dev d) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     real *sm = reinterpret_cast<real *>(sm_raw);
     const real gd0 = kG / d.density_0;
@@ -72,8 +72,10 @@ __global__ void k_pressure_col(Dev d) {
 // baroclinic_pressure_gradient_3D (fv_pressure_new.F90:146-221) per
 // (element, level); Bar_pr_2D as a level-ordered sum per element.  Also the
 // element's surface pressure force of compute_vel_rhs (fv_3D_vel.F90:60-75),
-// the same for every level.
-__global__ void k_bpg_elem(Dev d) {
+// the same for every level.  Column blocks reach 1024 threads (B * L), so
+// the kernel is bounded to 64 registers (unbounded it takes 96, which a
+// block of more than 682 threads, i.e. L >= 43, could not launch with).
+__global__ void __launch_bounds__(1024) k_bpg_elem(Dev d) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     real *sm = reinterpret_cast<real *>(sm_raw);
     const int L = d.L, NS = d.NS;
