@@ -809,6 +809,8 @@ int enqueue_step(fesomc_model *m, double ff) {
 // Open-boundary elevation for the Mt sub-steps of the coming internal step
 // (compute_ssh_rhs_elem, fv_average_dynamic.F90:190-216), on the host with
 // the reference formula; 'time' is the internal-step time in seconds.
+// Harmonics with a zero amplitude are skipped: their term is a signed zero,
+// and adding it to the partial sum (which starts at +0) changes no bit.
 void ob_values(const fesomc_model *m, double time, double time_jd, double *out) {
     const fesomc_params &p = m->p;
     const int nobn = m->d.nobn;
@@ -816,10 +818,13 @@ void ob_values(const fesomc_model *m, double time, double time_jd, double *out) 
         const double time_2D = time + p.dt_2D * (sub + 1);
         for (int q = 0; q < nobn; ++q) {
             double v = 0.0;
-            for (int j = 0; j < 12; ++j)
-                v = v + m->amp_factor[j] * m->ampt[(size_t)nobn * j + q] *
+            for (int j = 0; j < 12; ++j) {
+                const double amp = m->amp_factor[j] * m->ampt[(size_t)nobn * j + q];
+                if (amp == 0.0) continue;
+                v = v + amp *
                             fesomc_cos((time_2D - p.time_jd0 * 86400.0) * 2.0 * kPi / (kHarmPeriod[j] * 3600.0) -
                                      (m->fazt[(size_t)nobn * j + q] + m->phy_factor[j]));
+            }
             if (!p.restart)
                 if (time_jd - p.time_jd0 < 10.0) v = v * (time_jd - p.time_jd0) / 10.0;
             out[(size_t)sub * nobn + q] = v;
