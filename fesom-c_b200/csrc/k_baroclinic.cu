@@ -611,20 +611,29 @@ __global__ void k_implvisc(Dev d) {
             const real friction = -a_Cd * sqrt(ub * ub + vb * vb);
             uu[L - 1] = uu[L - 1] + zinv * friction * ub;
             vv[L - 1] = vv[L - 1] + zinv * friction * vb;
-            cp[0] = c[0] / b[0];
-            up[0] = uu[0] / b[0];
-            vp[0] = vv[0] / b[0];
+            // the recurrences carry their last value in registers
+            real cpv = c[0] / b[0], upv = uu[0] / b[0], vpv = vv[0] / b[0];
+            cp[0] = cpv;
+            up[0] = upv;
+            vp[0] = vpv;
             for (int z = 1; z < L; ++z) {
-                const real m = b[z] - cp[z - 1] * a[z];
-                cp[z] = c[z] / m;
-                up[z] = (uu[z] - up[z - 1] * a[z]) / m;
-                vp[z] = (vv[z] - vp[z - 1] * a[z]) / m;
+                const real az = a[z];
+                const real m = b[z] - cpv * az;
+                cpv = c[z] / m;
+                upv = (uu[z] - upv * az) / m;
+                vpv = (vv[z] - vpv * az) / m;
+                cp[z] = cpv;
+                up[z] = upv;
+                vp[z] = vpv;
             }
-            uu[L - 1] = up[L - 1];
-            vv[L - 1] = vp[L - 1];
+            real un = upv, vn = vpv;
+            uu[L - 1] = un;
+            vv[L - 1] = vn;
             for (int z = L - 2; z >= 0; --z) {
-                uu[z] = up[z] - cp[z] * uu[z + 1];
-                vv[z] = vp[z] - cp[z] * vv[z + 1];
+                un = up[z] - cp[z] * un;
+                vn = vp[z] - cp[z] * vn;
+                uu[z] = un;
+                vv[z] = vn;
             }
             for (int z = 0; z < L; ++z) { ur[z] = uu[z] * mwd; vr[z] = vv[z] * mwd; }
         }
@@ -636,18 +645,37 @@ __global__ void k_implvisc(Dev d) {
                 const real rw = de / d.density_0;
                 yu[0] = d.taux[e] * rw;
                 yv[0] = d.tauy[e] * rw;
+                // the recurrences carry their last value in registers; the
+                // column values of the next level are loaded one level ahead
+                real xv = xx1[0], yuv = yu[0], yvv = yv[0];
+                real je_m = real(0.0), je_0 = je[0], je_p = L > 1 ? je[1] : real(0.0);
+                real av_0 = Av[0], av_p = Av[1];
+                real fx_n = ur[0], fy_n = vr[0];
                 for (int z = 0; z < L; ++z) {
-                    const real Fx = ur[z], Fy = vr[z];
-                    const real d1 = (z == 0) ? real(0.5) * je[z] : real(0.5) * (je[z] + je[z - 1]);
-                    const real d2 = (z == L - 1) ? real(0.5) * je[z] : real(0.5) * (je[z] + je[z + 1]);
-                    const real zt = dt / je[z];
-                    const real a = zt * Av[z] / d1;
-                    const real c = zt * Av[z + 1] / d2;
+                    const real Fx = fx_n, Fy = fy_n;
+                    const real jz = je_0, jm = je_m, jp = je_p, a0 = av_0, a1 = av_p;
+                    if (z + 1 < L) {
+                        fx_n = ur[z + 1];
+                        fy_n = vr[z + 1];
+                        je_m = je_0;
+                        je_0 = je_p;
+                        if (z + 2 < L) je_p = je[z + 2];
+                        av_0 = av_p;
+                        av_p = Av[z + 2];
+                    }
+                    const real d1 = (z == 0) ? real(0.5) * jz : real(0.5) * (jz + jm);
+                    const real d2 = (z == L - 1) ? real(0.5) * jz : real(0.5) * (jz + jp);
+                    const real zt = dt / jz;
+                    const real a = zt * a0 / d1;
+                    const real c = zt * a1 / d2;
                     const real b = a + c + real(1.0);
-                    const real dd = b - a * xx1[z];
-                    xx1[z + 1] = c / dd;
-                    yu[z + 1] = (a * yu[z] + Fx) / dd;
-                    yv[z + 1] = (a * yv[z] + Fy) / dd;
+                    const real dd = b - a * xv;
+                    xv = c / dd;
+                    yuv = (a * yuv + Fx) / dd;
+                    yvv = (a * yvv + Fy) / dd;
+                    xx1[z + 1] = xv;
+                    yu[z + 1] = yuv;
+                    yv[z + 1] = yvv;
                 }
                 de = je[L - 1] / (Av[NS - 1] + Av[L - 1]);
                 const real friction = de * a_Cd * sqrt(ub * ub + vb * vb);

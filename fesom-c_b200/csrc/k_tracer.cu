@@ -730,6 +730,7 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
         // forward elimination; the right-hand side of layer k uses T(k-1..k+1)
         real Tm = real(0.0), T0 = Tz(0), Tp = Tz(1);
         real Sm = real(0.0), S0 = Sz(0), Sp = Sz(1);
+        real cpv = real(0.0), tpv = real(0.0), spv = real(0.0);  // the recurrences, in registers
         for (int k = 0; k < L; ++k) {
             real a, b, c, tr, sr;
             vd_coef(d, Kv, aj, k, a, b, c);
@@ -744,15 +745,18 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
                 sr = -a * Sm - c * Sp + (a + c) * S0;
             }
             if (k == 0) {
-                CP(0) = c / b;
-                TP(0) = tr / b;
-                SP(0) = sr / b;
+                cpv = c / b;
+                tpv = tr / b;
+                spv = sr / b;
             } else {
-                const real m = real(1.0) / (b - CP(k - 1) * a);
-                CP(k) = c * m;
-                TP(k) = (tr - TP(k - 1) * a) * m;
-                SP(k) = (sr - SP(k - 1) * a) * m;
+                const real m = real(1.0) / (b - cpv * a);
+                cpv = c * m;
+                tpv = (tr - tpv * a) * m;
+                spv = (sr - spv * a) * m;
             }
+            CP(k) = cpv;
+            TP(k) = tpv;
+            SP(k) = spv;
             Tm = T0; T0 = Tp;
             Sm = S0; S0 = Sp;
             if (k + 2 < L) { Tp = Tz(k + 2); Sp = Sz(k + 2); }
