@@ -262,6 +262,17 @@ def test_tidal_potential_bit_exact(mods):
     assert compare(sg, so) == []
 
 
+@pytest.mark.parametrize("nsigma", [64, 127])
+def test_estuary_many_levels_bit_exact(mods, nsigma):
+    """Level counts far above the configurations (127 is the largest the
+    library takes): the generic d3_end, the column blocks with few entities
+    per block and the 128-level solver variants, 10 steps."""
+    abi, cases, model, pyoracle = mods
+    case = cases.estuary_case("small%d" % nsigma, 40, 16, 300.0, nsigma, 2.0, 25.0, stress=(0.0, 0.05))
+    bad, _, _ = run_pair(mods, case, 10)
+    assert bad == []
+
+
 def test_estuary_filter2x_bit_exact(mods):
     """viscosity_filt2x_3D and viscosity_filt2x_2D (filt_bi_3D / filt_bi_2D)
     on the small estuary, 30 steps, and on LE, 20 steps."""
