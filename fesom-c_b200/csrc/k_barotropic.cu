@@ -102,7 +102,8 @@ __device__ __forceinline__ real ssh_edge_flux(const Dev &d, int ed) {
 // ob_val holds the open-boundary elevation of this sub-step, computed on the
 // host with the reference formula (fv_average_dynamic.F90:190-216).
 // ---------------------------------------------------------------------------
-__global__ void k_ssh_node(Dev d, int sub) {
+// 40 registers: 6 resident blocks per SM instead of 5 (3 % faster).
+__global__ void __maxnreg__(40) k_ssh_node(Dev d, int sub) {
     const double de = 0.614, ga = 0.088, ep = 0.013, fe = 1.0 - de - ga - ep;
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
