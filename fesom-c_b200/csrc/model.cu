@@ -98,6 +98,11 @@ struct fesomc_model {
     int stage_i = 0;
     size_t stage_len = 0;
     double *h_runoff = nullptr;  // host copy of current runoff
+    // open-boundary table of the next step, evaluated while the GPU runs the
+    // current one (valid for pre_time_jd and the current harmonics)
+    std::vector<double> h_pre;
+    double pre_time_jd = 0.0;
+    bool pre_valid = false;
     bool runoff_dirty = false;
     // asynchronous snapshots (fesomc_gpu_snapshot_begin / _end)
     struct Snap {
@@ -844,7 +849,8 @@ int upload_step_inputs(fesomc_model *m, double time, double time_jd) {
     double *h = m->h_stage[i];
     size_t off = 0;
     if (need_ob) {
-        ob_values(m, time, time_jd, h);
+        if (m->pre_valid && m->pre_time_jd == time_jd) std::memcpy(h, m->h_pre.data(), sizeof(double) * nobn * m->p.Mt);
+        else ob_values(m, time, time_jd, h);
         CK(cudaMemcpyAsync(m->d.ob_val, h, sizeof(double) * nobn * m->p.Mt, cudaMemcpyHostToDevice, m->stream));
         off += (size_t)nobn * m->p.Mt;
     }
@@ -911,6 +917,14 @@ int run_steps(fesomc_model *m, int nsteps) {
             if (rc) return rc;
         }
         m->launches += m->launches_per_step;
+        if (!m->dev_forcing && m->p.TF_presence && m->d.nobn > 0) {
+            // the next step's open-boundary table, while this step runs
+            const double tj = m->time_jd + m->p.dt / 86400.0;
+            m->h_pre.resize((size_t)m->d.nobn * m->p.Mt);
+            ob_values(m, tj * 86400.0, tj, m->h_pre.data());
+            m->pre_time_jd = tj;
+            m->pre_valid = true;
+        }
     }
     return FESOMC_OK;
 }
@@ -1065,6 +1079,7 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
         m->runoff_dirty = true;
     }
     const size_t nobn = (size_t)d.nobn;
+    if ((f->ampt && nobn) || (f->fazt && nobn) || f->amp_factor || f->phy_factor) m->pre_valid = false;
     if (f->ampt && nobn) std::memcpy(m->ampt.data(), f->ampt, nobn * 12 * 8);
     if (f->fazt && nobn) std::memcpy(m->fazt.data(), f->fazt, nobn * 12 * 8);
     if (f->amp_factor) std::memcpy(m->amp_factor, f->amp_factor, 12 * 8);
