@@ -1162,6 +1162,16 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
         m->lfirst = st->lfirst;
         m->time_jd = st->time_jd;
         if (m->d_clock) CK(cudaMemcpy(m->d_clock, &m->time_jd, sizeof(double), cudaMemcpyHostToDevice));
+        // a restart: the jacobian state from the restart elevation, as the
+        // reference's jacobian call after reading a restart (fv_main.F90:364);
+        // a running model holds the same at every step boundary
+        const size_t N = (size_t)m->d.N;
+        CK(cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * N, cudaMemcpyDeviceToDevice));
+        CK(cudaMemcpy(m->d.eta_jac_old, m->d.eta_n, sizeof(double) * N, cudaMemcpyDeviceToDevice));
+        if (m->fp32) fesomc::f32::launch_je(m->d32, m->stream);
+        else launch_je(m->d, m->stream);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(m->stream));
     }
     return FESOMC_OK;
 }

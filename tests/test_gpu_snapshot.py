@@ -36,6 +36,37 @@ def test_snapshot_is_the_state_when_begun(built, fp32):
         b.close()
 
 
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_restart_from_snapshot_is_bit_exact(built, fp32):
+    """The restart path (write_restart_separate / a restart read): a full
+    snapshot taken while the run goes on, loaded into a fresh model, which
+    then continues exactly as the original run."""
+    import ctypes as C
+    from fesomc import abi, cases, model
+    case = cases.estuary("small")
+    case.params.fp32_form = fp32
+    a = model.GpuModel(case)
+    c = model.GpuModel(case)
+    try:
+        a.step(10)
+        a.snapshot_begin(abi.F_ALL)
+        a.step(10)
+        snap = a.snapshot_end()
+        ref = a.state()
+        arrays = {k: v for k, v in snap.items() if k != "_time_jd"}
+        st = case.state_struct(arrays, snap["_time_jd"], lfirst=0)
+        abi.check(c.lib.fesomc_gpu_sync_from_host(c.h, abi.F_ALL, C.byref(st)), "sync_from_host")
+        c.nstep, c.time_jd = 10, snap["_time_jd"]
+        c.step(10)
+        got = c.state()
+        assert got["_time_jd"] == ref["_time_jd"]
+        for f in FIELDS:
+            assert np.array_equal(got[f], ref[f]), f
+    finally:
+        a.close()
+        c.close()
+
+
 def test_snapshot_order_is_checked(built):
     from fesomc import abi, cases, model
     case = cases.estuary("small")
