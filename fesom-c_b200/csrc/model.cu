@@ -599,7 +599,9 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     if (k == "bih_2d") return 2 * (Ed * (16 + 8 + 32 + 8 + 16) + E * 32 + Ed * 16) + E * (16 + 16 + 8 + 8 + 16) +
                               E * (16 + 16 + 64 + 16 + 32);
     if (k == "forcing") return (double)d.nobn * (m->p.Mt * 8 + 12 * 16) + 36 * 8 + d.n_rivers * 16.0 + 16;
-    if (k == "ab3_elem") return E * (48 + 32 + 16 + 16 + 16 + 64 + 8) + N * 32 + E * (16 + 8 + 32);
+    // ab3_elem (AB3 levels, w_cv, nodes; eta levels and depth; UAB, aux out)
+    // and velgrad2d (UAB, neighbours, edges, gradients, cos; vel_grad out)
+    if (k == "ab3_elem") return E * (48 + 32 + 16) + N * 32 + E * (16 + 8) + E * (16 + 16 + 16 + 64 + 8) + E * 32;
     if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
     // per internal edge: nodes (etaAB, depth, ac), elements (UAB, vel_grad,
     // cos), geometry; one flux pair written
@@ -771,7 +773,7 @@ int enqueue_step(fesomc_model *m, double ff) {
     for (int sub = 0; sub < d.Mt; ++sub) {
         rec(m, "ab3_elem", [&] { K3(launch_ab3_elem, s); });
         rec(m, "ssh_node", [&] { K3(launch_ssh_node, sub, s); });
-        n += 2;
+        n += 3;
         if (sub == 0) {
             rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
             rec(m, "el2nodes_p", [&] { K3E2N(U_puls, V_puls, Unode_p, Vnode_p); });
