@@ -66,6 +66,12 @@ __device__ __forceinline__ real ssh_edge_flux(const Dev &d, int ed) {
     return c1;
 }
 
+// the SSH edge flux of every edge, once, for both end nodes to gather (the
+// flux array stays in L2; a quarter faster than forming it per node)
+__global__ void k_ssh_edge(Dev d) {
+    GRID_LOOP(ed, d.Ed) d.sshfl[ed] = ssh_edge_flux(d, (int)ed);
+}
+
 // ---------------------------------------------------------------------------
 // ssh_node: ssh_rhs gather (serial scatter order), rivers, open boundary,
 // eta_new = eta_n + dt_2D*rhs/area (fv_main.F90:1432-1435), then the AM4
@@ -84,7 +90,7 @@ __global__ void __maxnreg__(40) k_ssh_node(Dev d, int sub) {
 #pragma unroll 4
         for (int p = p0; p < p1; ++p) {
             const int code = d.node_eidx[p];
-            const double c1 = (double)ssh_edge_flux(d, code >> 1);
+            const double c1 = (double)d.sshfl[code >> 1];
             if (code & 1) acc = acc - c1;
             else acc = acc + c1;
         }
@@ -589,7 +595,10 @@ void launch_ab3_elem(const Dev &d, cudaStream_t s) {
     k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d);
     k_velgrad2d<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.UAB);
 }
-void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) { k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub); }
+void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) {
+    k_ssh_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d);
+    k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub);
+}
 void launch_puls_elem(const Dev &d, cudaStream_t s) {
     k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
 }

@@ -457,7 +457,7 @@ int alloc_mom2d(fesomc_model *m, D &d) {
     for (auto p : e2) if ((rc = dalloc(m, p, E))) return rc;
     if ((rc = dalloc(m, &d.vel_grad, E))) return rc;
     if ((rc = dalloc(m, &d.bfric, E))) return rc;
-    if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in))) return rc;
+    if ((rc = dalloc(m, &d.adv2d, (size_t)d.Ed_in)) || (rc = dalloc(m, &d.sshfl, (size_t)d.Ed))) return rc;
     if (m->p.filt_bi_2D && (rc = dalloc(m, &d.f2uv2d, E))) return rc;
     if (m->p.bih_2D && ((rc = dalloc(m, &d.b2fl, (size_t)d.Ed)) || (rc = dalloc(m, &d.b2ul, E)))) return rc;
     return FESOMC_OK;
@@ -602,7 +602,9 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     // ab3_elem (AB3 levels, w_cv, nodes; eta levels and depth; UAB, aux out)
     // and velgrad2d (UAB, neighbours, edges, gradients, cos; vel_grad out)
     if (k == "ab3_elem") return E * (48 + 32 + 16) + N * 32 + E * (16 + 8) + E * (16 + 16 + 16 + 64 + 8) + E * 32;
-    if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24;
+    // ssh_edge (edge geometry, UAB, aux; the flux out) and ssh_node (CSR,
+    // the fluxes, node fields)
+    if (k == "ssh_node") return N * (4 + 4 + 4 + 24 + 8 + 8 + 16) + 4 * nnz_ne + Ed * (8 + 32) + E * 24 + Ed * 16;
     // per internal edge: nodes (etaAB, depth, ac), elements (UAB, vel_grad,
     // cos), geometry; one flux pair written
     if (k == "adv2d_edge") return N * 24 + E * (16 + 32 + 8) + Ei * (8 + 8 + 32 + 16 + 16);
@@ -773,7 +775,7 @@ int enqueue_step(fesomc_model *m, double ff) {
     for (int sub = 0; sub < d.Mt; ++sub) {
         rec(m, "ab3_elem", [&] { K3(launch_ab3_elem, s); });
         rec(m, "ssh_node", [&] { K3(launch_ssh_node, sub, s); });
-        n += 3;
+        n += 4;
         if (sub == 0) {
             rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
             rec(m, "el2nodes_p", [&] { K3E2N(U_puls, V_puls, Unode_p, Vnode_p); });
