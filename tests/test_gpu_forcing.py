@@ -55,3 +55,33 @@ def test_device_forcing_needs_river_base(built):
         assert g.lib.fesomc_gpu_set_device_forcing(None, None, 0) == 1
     finally:
         g.close()
+
+
+def test_restart_with_device_forcing_and_potential(built):
+    """A restart into a fresh model on device forcing with the tidal
+    potential: the device clock follows the restart time, and the run
+    continues bit for bit."""
+    from fesomc import abi, cases, model
+    case = cases.estuary("small", T_potential=1)
+    base = np.ascontiguousarray(case.forcing_fn(1, case.params.time_jd0 + 20.0)["runoff_rivers"])
+    a = model.GpuModel(case)
+    c = model.GpuModel(case)
+    try:
+        for g in (a, c):
+            g.set_forcing(case.forcing_fn(1, cases.advance_time(g.time_jd, case.params.dt)))
+            abi.check(g.lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base), 1), "fesomc_gpu_set_device_forcing")
+        abi.check(a.lib.fesomc_gpu_run(a.h, 0, 10), "fesomc_gpu_run")
+        snap = a.state()
+        abi.check(a.lib.fesomc_gpu_run(a.h, 0, 10), "fesomc_gpu_run")
+        ref = a.state()
+        arrays = {k: v for k, v in snap.items() if k != "_time_jd"}
+        st = case.state_struct(arrays, snap["_time_jd"], lfirst=0)
+        abi.check(c.lib.fesomc_gpu_sync_from_host(c.h, abi.F_ALL, C.byref(st)), "sync_from_host")
+        abi.check(c.lib.fesomc_gpu_run(c.h, 0, 10), "fesomc_gpu_run")
+        got = c.state()
+    finally:
+        a.close()
+        c.close()
+    assert got["_time_jd"] == ref["_time_jd"]
+    for f in FIELDS:
+        assert np.array_equal(got[f], ref[f]), f
