@@ -77,8 +77,9 @@ __global__ void k_ssh_edge(Dev d) {
 // eta_new = eta_n + dt_2D*rhs/area (fv_main.F90:1432-1435), then the AM4
 // elevation of update_2D_vel (fv_average_dynamic.F90:290-295) into etaAB and
 // the node wet/dry mask (wad_mask, fv_main.F90:1302-1304).
-// ob_val holds the open-boundary elevation of this sub-step, computed on the
-// host with the reference formula (fv_average_dynamic.F90:190-216).
+// ob_val holds the open-boundary elevation of this sub-step (reference formula
+// fv_average_dynamic.F90:190-216), written before the step either by the host
+// (fesomc_gpu_set_forcing) or by k_forcing_values (device forcing).
 // ---------------------------------------------------------------------------
 // 40 registers: 6 resident blocks per SM instead of 5 (3 % faster).
 __global__ void __maxnreg__(40) k_ssh_node(Dev d, int sub) {

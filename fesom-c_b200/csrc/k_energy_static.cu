@@ -10,17 +10,21 @@
 // cudaMalloc, no cudaFree, no allocating library call.
 //
 // Scratch: g_energy_scratch holds kEsParts x 3 compensated partial sums (one
-// triple per block) and the 3 totals, 14,256 bytes.  The grid is fixed at
-// kEsParts blocks that stride over the mesh, so any mesh size fits; a launch
-// configuration that would need more partials than the array holds is
-// rejected with FESOMC_EINVAL.  Every call writes all the partials and totals
+// triple per block) and the 3 totals: 1,779 doubles, 14,232 bytes.  The grid
+// is fixed at kEsParts blocks that stride over the mesh, so any mesh size
+// fits (a static_assert ties the grid to the array size); node and element
+// counts below 1 are rejected with FESOMC_EINVAL.  Every call writes all the partials and totals
 // it later reads, so nothing in the array has to start at zero.  All calls on
 // a device share the one array: calls that overlap in time (different
 // streams or host threads) race on it and must be serialised by the caller.
 //
 // Set-up: the first call on a device (that device current) looks up the
-// array's device address once with cudaGetSymbolAddress and keeps it; make
-// that first call before any stream capture begins.
+// array's device address once with cudaGetSymbolAddress and keeps it for the
+// life of the process; make that first call before any stream capture
+// begins.  The kept address belongs to the device's primary context: after
+// cudaDeviceReset on that device the next context may place the array
+// elsewhere, so a process that resets a device must not call this entry
+// point on it again.
 #include <mutex>
 
 #include "device_common.cuh"
@@ -34,6 +38,7 @@ constexpr int kEsBlock = 256;
 constexpr int kEsParts = 592;                    // 4 blocks per SM on 148 SMs
 constexpr int kEsDoubles = kEsParts * 3 + 3;     // partial triples + totals
 constexpr int kEsMaxDevices = 64;
+static_assert(kEsDoubles * sizeof(double) == 14232, "documented scratch size");
 
 static __device__ __align__(256) double g_energy_scratch[kEsDoubles];
 
@@ -103,7 +108,7 @@ extern "C" int fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, 
         !eout)
         return FESOMC_EINVAL;
     const int nparts = kEsParts;
-    if (nparts * 3 + 3 > kEsDoubles) return FESOMC_EINVAL;  // more partials than the scratch holds
+    static_assert(kEsParts * 3 + 3 <= kEsDoubles, "one partial triple per block and the totals fit the scratch");
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess) return FESOMC_ECUDA;
     if (dev < 0 || dev >= kEsMaxDevices) return FESOMC_EINVAL;

@@ -975,6 +975,7 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
         return FESOMC_EINVAL;
     if (par->bih_2D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
     if (par->T_potential != 0 && par->T_potential != 1) return FESOMC_EINVAL;
+    if (par->npes < 0 || par->npes > 1) return FESOMC_EINVAL;   // one rank: no halo exchange
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;

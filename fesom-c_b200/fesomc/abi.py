@@ -52,7 +52,7 @@ class Params(C.Structure):
                                   "n_harm")] + \
         [("harm_index", C.c_int32 * 12), ("fp32_form", C.c_int32), ("bih_3D", C.c_int32), ("Abh0", C.c_double),
                                   ("filt_bi_3D", C.c_int32), ("filt_bi_2D", C.c_int32), ("tau_c", C.c_double),
-                                  ("bih_2D", C.c_int32), ("T_potential", C.c_int32)]
+                                  ("bih_2D", C.c_int32), ("T_potential", C.c_int32), ("npes", C.c_int32)]
 
 
 STATE_FIELDS = ["eta_n", "eta_n_1", "eta_n_2", "etaAB", "U_n_2D", "U_n_1", "U_n_2", "U_filt_2D",

@@ -21,8 +21,9 @@
  *    elem_neighbors <= 0) are kept.  The library converts on the host.
  *  - Every entry point returns 0 on success or one of FESOMC_E* (> 0).
  *  - The whole mesh lives on one GPU: there is no halo exchange (the MPI
- *    g_comm / exchange_* calls of the reference drop out).  A caller with
- *    npes > 1 must not call fesomc_gpu_init (it would return FESOMC_EINVAL).
+ *    g_comm / exchange_* calls of the reference drop out).  The caller passes
+ *    its MPI rank count in fesomc_params.npes; fesomc_gpu_init returns
+ *    FESOMC_EINVAL for npes > 1 (0 is read as 1).
  *  - Call from one host thread, outside any OpenMP parallel region.
  */
 #ifndef FESOMC_GPU_H
@@ -172,6 +173,10 @@ typedef struct fesomc_params {
      * device; build the mesh with the same flag for its a_tp
      * (src/fv_ini.F90:94-107).                                              */
     int32_t T_potential;
+    /* number of MPI ranks of the calling driver (npes, g_PARSUP).  The whole
+     * mesh lives on one GPU, so fesomc_gpu_init rejects npes > 1 with
+     * FESOMC_EINVAL; 0 (a zero-initialised struct) is read as 1.           */
+    int32_t npes;
 } fesomc_params;
 
 /*
@@ -349,19 +354,22 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * where each MPI rank owns a mesh partition instead. */
 int  fesomc_gpu_set_device(int32_t device);
 
-/* Domain energy (as fesomc_gpu_energy, src/fv_average_dynamic.F90:476-554)
- * of a state held in caller-owned DEVICE arrays, without creating a model
- * and without allocating device memory.  No counterpart in the reference.
- * It serves callers that own the state in their own device buffers or that
- * have reserved all device memory and may not allocate more.  Arrays use the
+/* No counterpart in the reference.  The domain energy (the same quantity
+ * fesomc_gpu_energy returns) of a state held in caller-owned DEVICE arrays,
+ * without creating a model and without allocating device memory.  It serves
+ * callers that own the state in their own device buffers (another
+ * framework's memory pool, whose allocator they must not bypass) or that
+ * have reserved all device memory up front and may not allocate more.  Arrays use the
  * reference shapes: eta_n, depth, area (nod2D); elem2D_nodes (4,elem2D),
  * 1-based; w_cv (4,elem2D); U_n_2D (2,elem2D); elem_area (elem2D).  stream
  * is a cudaStream_t (NULL = default stream); the call returns after the
- * result is on the host.  The reduction scratch is a fixed 14,256-byte
+ * result is on the host.  The reduction scratch is a fixed 14,232-byte
  * device array shared by all calls on a device: it needs no initial zeroing,
  * and calls that overlap in time race on it.  The first call on a device
- * (with that device current) looks up the array once; make it before any
- * stream capture begins.  Returns FESOMC_EINVAL for bad arguments. */
+ * (with that device current) looks up the array once and keeps its address
+ * for the life of the process; make it before any stream capture begins,
+ * and do not call it again on a device after cudaDeviceReset there.
+ * Returns FESOMC_EINVAL for bad arguments (counts below 1, NULL arrays). */
 int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const double *eta_n,
                           const double *depth, const double *area, const int32_t *elem2D_nodes,
                           const double *w_cv, const double *U_n_2D, const double *elem_area,

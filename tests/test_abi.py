@@ -50,6 +50,19 @@ def test_init_rejects_bad_arguments_without_gpu(built):
     assert built.fesomc_gpu_init(C.byref(m), C.byref(p), C.byref(s), C.byref(h)) == 1
 
 
+def test_init_rejects_more_than_one_rank_without_gpu(built):
+    """The whole mesh lives on one GPU (no halo exchange): a driver that runs
+    with npes > 1 ranks is refused before any CUDA call."""
+    from fesomc import abi, cases
+    case = cases.estuary("small")
+    arrays = case.new_state_arrays()
+    st = case.state_struct(arrays, case.params.time_jd0)
+    h = C.c_void_p()
+    case.params.npes = 2
+    assert built.fesomc_gpu_init(C.byref(case.mesh.c), C.byref(case.params), C.byref(st), C.byref(h)) == 1
+    assert not h.value
+
+
 def test_host_density_matches_oracle(built):
     import pyoracle
     from fesomc import abi

@@ -1,8 +1,11 @@
 """fesomc_energy_device: the energy diagnostic over caller-owned device arrays,
-with its reduction scratch in a fixed device array (no allocation by the
-library).  Checked through the C-ABI against fesomc_gpu_energy on the same
-state, on two calls in a row (the second call reuses the scratch the first
-one left behind)."""
+with its reduction scratch in a fixed device array, for callers that cannot
+allocate device memory (they hold their state in another framework's memory
+pool, or have reserved all device memory up front).  Checked through the
+C-ABI against fesomc_gpu_energy on the same state, on two calls in a row
+(the second call reuses the scratch the first one left behind), and checked
+to leave the device's free memory unchanged once its one-time set-up (the
+symbol lookup of the first call) is done."""
 import ctypes as C
 
 import numpy as np
@@ -42,17 +45,26 @@ def test_energy_device_matches_model_energy(built):
     earea = d(m.elem_area, np.float64)
     torch.cuda.synchronize()
     lib = abi.load()
-    out = []
-    for _ in range(2):
+
+    def call():
         e = C.c_double()
         rc = lib.fesomc_energy_device(m.N, m.E, case.params.Dmin, eta.data_ptr(), depth.data_ptr(), area.data_ptr(),
                                       nodes.data_ptr(), w_cv.data_ptr(), u2.data_ptr(), earea.data_ptr(), None,
                                       C.byref(e))
         abi.check(rc, "fesomc_energy_device")
-        out.append(e.value)
+        return e.value
+
+    out = [call()]                       # first call: one-time symbol lookup
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    out.append(call())
+    out.append(call())
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, "the entry point changed the device's free memory"
     for v in out:
         assert v == pytest.approx(e_model, rel=RTOL, abs=0.0)
-    assert out[0] == out[1]
+    assert out[0] == out[1] == out[2]
 
 
 def test_energy_device_rejects_bad_sizes(built):
