@@ -715,7 +715,8 @@ extern "C" int fesomc_mesh_set_sponge(fesomc_mesh_builder *b, double radius) {
             const double cos_X2 = std::cos(X2);
             auto hav = [&](size_t j) {
                 const double s2 = std::sin((x2[j] - X2) * 0.5), s1 = std::sin((x1[j] - X1) * 0.5);
-                return s2 * s2 + cos_X2 * std::cos(x2[j]) * s1 * s1;
+                // Fortran precedence: cos_X2 * cos(X2obn) * sin(..)**2 is (cos_X2 * cos) * (s1 * s1)
+                return s2 * s2 + cos_X2 * std::cos(x2[j]) * (s1 * s1);
             };
             double a = hav(0);
             for (size_t j = 1; j < nob; ++j) {

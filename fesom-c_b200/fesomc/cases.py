@@ -28,8 +28,10 @@ class HostMesh:
 
     def __init__(self, xy, index, elems, depth, *, cartesian, nsigma, coriolis_on=False, lat_deg=50.0,
                  ind_sigma=1, pow_sig=1.0, lev_bot=1.0, lev_sur=1.0, T_potential=False,
-                 with_up_dn_tri=True, rivers=None, sponge_radius=None):
-        lib = abi.load()
+                 with_up_dn_tri=True, rivers=None, sponge_radius=None, lib=None):
+        # lib: any object with the fesomc_mesh_* functions of the C-ABI (the
+        # product library by default)
+        lib = lib if lib is not None else abi.load()
         self.lib = lib
         xy = np.ascontiguousarray(xy, dtype=np.float64)
         index = np.ascontiguousarray(index, dtype=np.int32)
@@ -190,13 +192,14 @@ def _fixture_path():
     return os.path.join(abi.REPO_DIR, "tests", "golden", "le_medium.npz")
 
 
-def le_medium(nsigma=40):
-    """The reference's LE_medium lock-exchange case (fv_run.dat of the case)."""
+def le_medium(nsigma=40, lib=None):
+    """The reference's LE_medium lock-exchange case (fv_run.dat of the case).
+    lib: the mesh builder to use (default: the product library)."""
     d = np.load(_fixture_path())
     depth = np.full(len(d["nod_index"]), 20.0)          # title 'LE' (fv_main.F90:915-916)
     mesh = HostMesh(d["nod_xy"], d["nod_index"], d["elem_nodes"], depth, cartesian=False,
-                    nsigma=nsigma, coriolis_on=False, with_up_dn_tri=True)
-    lib = abi.load()
+                    nsigma=nsigma, coriolis_on=False, with_up_dn_tri=True, lib=lib)
+    lib = lib if lib is not None else abi.load()
     p = default_params()
     p.scale_area = mesh.scale_area
     p.density_0 = 1000.0 + lib.fesomc_host_density_jm(20.0, 30.0, 0.0, 1000.0)
@@ -291,7 +294,8 @@ def estuary_geometry(nx, ny, dx, seed=20261203, split_frac=0.3, h0=2.0, h1=25.0,
 
 
 def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS, **overrides):
-    """One of the named estuary configurations (ESTUARY_CFGS)."""
+    """One of the named estuary configurations (ESTUARY_CFGS).  lib=... (in
+    overrides) selects the mesh builder, default the product library."""
     nx, ny, dx, nsigma, h0, h1, tau = ESTUARY_CFGS[cfg]
     # uniform stress, cross-shore (+y, from the shore towards deep water); an
     # along-channel stress towards the open boundary drives the shallow
@@ -303,7 +307,7 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
 
 def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=1.2, m2_phase_deg=0.0,
                  noise_sigma=0.5, seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS,
-                 **overrides):
+                 lib=None, **overrides):
     """Synthetic estuary: nx x ny quads at dx metres, 30 % split into
     triangles, depth h0 -> h1 across the channel plus smoothed noise of
     noise_sigma metres, river at x = 0, M2 tide of m2_amp metres and phase
@@ -315,8 +319,8 @@ def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=
     # T_potential switches both the potential and the mesh's a_tp weights
     mesh = HostMesh(xy, index, elems, depth, cartesian=True, nsigma=nsigma, coriolis_on=True,
                     lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius,
-                    T_potential=bool(overrides.get("T_potential", 0)))
-    lib = abi.load()
+                    T_potential=bool(overrides.get("T_potential", 0)), lib=lib)
+    lib = lib if lib is not None else abi.load()
     kw = dict(dt=20.0, dt_2D=2.0, Dmin=1.0, C_d=0.0025, tracer_adv=tracer_adv, wet_dry_on=1,
               key_rivers=1, TF_presence=1, temp_on=1, salinity_on=1, filt_2D=1, filt_3D=1,
               river_salinity=5.0, clim_relax=1.0 / OB_RELAX_S, relax2clim_ac=1.0 / OB_RELAX_S)

@@ -55,8 +55,39 @@ def load(abi):
         lib.oracle_cos.argtypes = [C.c_double]
         lib.oracle_sin.restype = C.c_double
         lib.oracle_sin.argtypes = [C.c_double]
+        lib.oracle_mesh_build.restype = C.c_int
+        lib.oracle_mesh_build.argtypes = [C.c_int32, abi.f64p, abi.i32p, C.c_int32, abi.i32p, abi.f64p,
+                                          C.POINTER(abi.MeshOpts), C.POINTER(C.c_void_p)]
+        lib.oracle_mesh_view.restype = C.c_int
+        lib.oracle_mesh_view.argtypes = [C.c_void_p, C.POINTER(abi.Mesh)]
+        lib.oracle_mesh_scale_area.restype = C.c_double
+        lib.oracle_mesh_scale_area.argtypes = [C.c_void_p]
+        lib.oracle_mesh_set_rivers.restype = C.c_int
+        lib.oracle_mesh_set_rivers.argtypes = [C.c_void_p, C.c_int32, abi.i32p]
+        lib.oracle_mesh_set_sponge.restype = C.c_int
+        lib.oracle_mesh_set_sponge.argtypes = [C.c_void_p, C.c_double]
+        lib.oracle_mesh_free.restype = None
+        lib.oracle_mesh_free.argtypes = [C.c_void_p]
         _lib = lib
     return _lib
+
+
+class MeshLib:
+    """The oracle's own mesh restatement (oracle_mesh.c) under the names of
+    the product's host mesh builder, so that cases.* can build a case's mesh,
+    sigma levels and density_0 without loading the product library:
+    cases.estuary(cfg, lib=pyoracle.MeshLib(abi))."""
+
+    def __init__(self, abi):
+        lib = load(abi)
+        self.missing_symbols = []
+        self.fesomc_mesh_build = lib.oracle_mesh_build
+        self.fesomc_mesh_view = lib.oracle_mesh_view
+        self.fesomc_mesh_scale_area = lib.oracle_mesh_scale_area
+        self.fesomc_mesh_set_rivers = lib.oracle_mesh_set_rivers
+        self.fesomc_mesh_set_sponge = lib.oracle_mesh_set_sponge
+        self.fesomc_mesh_free = lib.oracle_mesh_free
+        self.fesomc_host_density_jm = lib.oracle_densityJM
 
 
 class Oracle:

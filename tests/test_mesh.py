@@ -117,3 +117,94 @@ def test_orientation_fixed_and_bad_quad_rejected(built):
     bad = np.array([[1, 3, 2, 4], [2, 5, 6, 3]], np.int32)
     with pytest.raises(RuntimeError, match="EMESH"):
         cases.HostMesh(xy, idx, bad, np.full(6, 10.0), cartesian=True, nsigma=5, with_up_dn_tri=False)
+
+
+MESH_ARRAYS = ["index_nod2D", "elem2D_nodes", "edge_nodes", "edge_tri", "elem_edges", "elem_neighbors",
+               "nod_in_elem2D_num", "nod_in_elem2D", "edge_up_dn_tri", "coord_nod2D", "depth", "area", "elem_area",
+               "elem_cos", "coriolis", "w_cv", "gradient_sca", "gradient_vec", "edge_dxdy", "edge_cross_dxdy",
+               "sigma", "a_tp", "ac", "in_obn", "nod_rivers"]
+
+
+def _same_mesh(a, b):
+    assert (a.N, a.E, a.Ed, a.Ed_in, a.NS) == (b.N, b.E, b.Ed, b.Ed_in, b.NS)
+    assert a.c.nod_in_elem2D_max == b.c.nod_in_elem2D_max
+    assert a.scale_area == b.scale_area
+    bad = [k for k in MESH_ARRAYS if not np.array_equal(getattr(a, k), getattr(b, k))]
+    assert bad == []
+
+
+@pytest.mark.parametrize("name", ["small", "cfg0"])
+def test_oracle_mesh_equals_product_mesh_estuary(built, name):
+    """The oracle's own restatement of the mesh set-up (oracle/oracle_mesh.c,
+    written from the Fortran alone) and the product's host builder give the
+    same arrays bit for bit on the estuary, whose 30 % triangles no reference
+    file pins; this makes the oracle's inputs independent of the product."""
+    import pyoracle
+    from fesomc import abi, cases
+    ol = pyoracle.MeshLib(abi)
+    p = cases.estuary(name)
+    o = cases.estuary(name, lib=ol)
+    _same_mesh(p.mesh, o.mesh)
+    assert p.params.density_0 == o.params.density_0
+    for k in p.state0:
+        assert np.array_equal(p.state0[k], o.state0[k]), k
+
+
+def test_oracle_mesh_equals_product_mesh_le_and_tidal_potential(built):
+    """LE (spherical coordinates, all quads), the a_tp weights of the tidal
+    potential, and on a spherical estuary the ind_sigma = 2 (tanh) levels,
+    rivers and the haversine sponge."""
+    import pyoracle
+    from fesomc import abi, cases
+    ol = pyoracle.MeshLib(abi)
+    _same_mesh(cases.le_medium().mesh, cases.le_medium(lib=ol).mesh)
+    _same_mesh(cases.estuary("small", T_potential=1).mesh, cases.estuary("small", T_potential=1, lib=ol).mesh)
+    xy, idx, el, dep, _ = cases.estuary_geometry(40, 16, 300.0)
+    xy = xy / 300.0 * 0.01 + np.array([5.0, 50.0])
+    kw = dict(cartesian=False, nsigma=21, ind_sigma=2, lev_bot=1.5, lev_sur=0.8, coriolis_on=True,
+              sponge_radius=2000.0, rivers=[1, 42])
+    _same_mesh(cases.HostMesh(xy, idx, el, dep, **kw), cases.HostMesh(xy, idx, el, dep, lib=ol, **kw))
+
+
+def test_estuary_triangle_gradients_exact_for_linear_fields(built):
+    """gradient_sca of a linear field is exact on every element of the
+    estuary, triangles and quads alike (mesh_arrays2, fv_mesh_array.F90:
+    1261-1302), and gradient_vec reproduces a linear velocity field exactly on
+    interior elements (least squares over the neighbour centres); for the
+    product's mesh builder and the oracle's."""
+    import pyoracle
+    from fesomc import abi, cases
+    for lib in (None, pyoracle.MeshLib(abi)):
+        m = cases.estuary("small", lib=lib).mesh
+        en = m.elem2D_nodes - 1
+        tri = en[:, 0] == en[:, 3]
+        assert tri.sum() > 100
+        p = m.coord_nod2D * cases.R_EARTH                  # metres (cartesian)
+        f = 3.0 * p[:, 0] - 2.0 * p[:, 1]
+        gx = (m.gradient_sca[:, :4] * f[en]).sum(axis=1)
+        gy = (m.gradient_sca[:, 4:] * f[en]).sum(axis=1)
+        # triangles carry a zero fourth weight, so the repeated node adds nothing
+        np.testing.assert_array_equal(m.gradient_sca[tri][:, [3, 7]], 0.0)
+        np.testing.assert_allclose(gx, 3.0, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(gy, -2.0, rtol=0, atol=1e-9)
+        # element centres as the reference computes them (elem_center)
+        xs, ys = p[:, 0], p[:, 1]
+        s1 = np.abs((xs[en[:, 2]] - xs[en[:, 3]]) * (ys[en[:, 0]] - ys[en[:, 3]])
+                    - (ys[en[:, 2]] - ys[en[:, 3]]) * (xs[en[:, 0]] - xs[en[:, 3]]))
+        s2 = np.abs((xs[en[:, 2]] - xs[en[:, 1]]) * (ys[en[:, 0]] - ys[en[:, 1]])
+                    - (ys[en[:, 2]] - ys[en[:, 1]]) * (xs[en[:, 0]] - xs[en[:, 1]]))
+        qx = ((xs[en[:, 0]] + xs[en[:, 2]] + xs[en[:, 3]]) * s1 + (xs[en[:, 0]] + xs[en[:, 1]] + xs[en[:, 2]]) * s2) \
+            / 3.0 / (s1 + s2)
+        qy = ((ys[en[:, 0]] + ys[en[:, 2]] + ys[en[:, 3]]) * s1 + (ys[en[:, 0]] + ys[en[:, 1]] + ys[en[:, 2]]) * s2) \
+            / 3.0 / (s1 + s2)
+        cx = np.where(tri, p[en[:, :3], 0].mean(axis=1), qx)
+        cy = np.where(tri, p[en[:, :3], 1].mean(axis=1), qy)
+        u = 0.5 * cx + 0.25 * cy
+        nb = m.elem_neighbors
+        interior = (nb > 0).all(axis=1)
+        for e in np.nonzero(interior)[0][::7]:
+            q = 3 if tri[e] else 4
+            du = u[nb[e, :q] - 1] - u[e]
+            gux = (m.gradient_vec[e, :q] * du).sum()
+            guy = (m.gradient_vec[e, 4:4 + q] * du).sum()
+            assert abs(gux - 0.5) < 1e-9 and abs(guy - 0.25) < 1e-9, e
