@@ -107,9 +107,47 @@ class ClockSampler:
                 "samples": len(sms)}
 
 
-def build_case(cfg):
+def build_case(cfg, lib=None):
     from fesomc import cases
-    return cases.estuary(cfg)
+    return cases.estuary(cfg, lib=lib)
+
+
+def oracle_case(cfg):
+    """The workload built by the oracle's own mesh restatement: the CPU legs
+    never load the product library."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from fesomc import abi
+    return build_case(cfg, lib=pyoracle.MeshLib(abi))
+
+
+def host_cpu():
+    """CPU model, physical cores and the hardware threads this process may use."""
+    model, cores = None, set()
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif not k and phys is not None:
+                    cores.add((phys, core))
+                    phys = core = None
+        if phys is not None:
+            cores.add((phys, core))
+    except OSError:
+        pass
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except AttributeError:
+        threads = os.cpu_count() or 1
+    return {"model": model, "physical_cores": len(cores) or None, "threads_available": threads}
 
 
 def cases_sponge_km(case):
@@ -134,14 +172,14 @@ def workload_config(case, cfg):
     }
 
 
-def cpu_oracle_rate(case, steps, budget_s=60.0):
+def cpu_oracle_rate(case, steps, budget_s=60.0, warmup=1):
     """Oracle restatement on all host cores: node*level updates/s over a
-    bounded number of internal steps (first step untimed)."""
+    bounded number of internal steps after `warmup` untimed ones."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from fesomc import abi, cases
     o = pyoracle.Oracle(case, abi, cases)
-    o.step(1)
+    o.step(max(warmup, 0))
     done, t0 = 0, time.perf_counter()
     while done < steps:
         o.step(1)
@@ -155,22 +193,30 @@ def cpu_oracle_rate(case, steps, budget_s=60.0):
 
 
 def run_reference(args, ws, rank):
+    """The reference arm: the oracle restatement of the time step (the
+    Fortran reference cannot be built in this image) on all host threads,
+    its case built by the oracle's own mesh restatement, so that no product
+    code is loaded.  --warmup untimed steps (at most 5), then up to --steps
+    timed steps within a time budget (a bounded sample of the workload)."""
     if rank != 0:
         return
     cfg = args.config
-    case = build_case(cfg)
-    cores = os.cpu_count() or 1
+    case = oracle_case(cfg)
+    cpu = host_cpu()
+    cores = cpu["threads_available"]
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     budget = min(150.0, 8.0 * max(args.steps, 1))
-    rate, done, dt = cpu_oracle_rate(case, max(args.steps, 1), budget_s=budget)
-    sample = (f"{done} internal steps of {cfg} after 1 untimed step ({dt:.1f} s), CPU restatement of the "
-              f"reference time step with OpenMP over {cores} threads")
+    warm = min(args.warmup, 5)
+    rate, done, dt = cpu_oracle_rate(case, max(args.steps, 1), budget_s=budget, warmup=warm)
+    sample = (f"{done} internal steps of {cfg} after {warm} untimed steps ({dt:.1f} s), CPU restatement of the "
+              f"reference time step (oracle port) with OpenMP over {cores} threads")
     line = {
         "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
-        "warmup": 1, "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
+        "warmup": warm, "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
         "config": workload_config(case, cfg),
-        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                         "cpu": cpu},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -294,10 +340,10 @@ def run_ours(args, ws, rank, local):
         "warmup": args.warmup, "ms_per_step": 1000.0 * t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.fp32_form else "f64",
         "data": "synthetic",
-        "config": dict(workload_config(case, cfg),
-                       forcing="timed region: open-boundary tide and ramped river runoff evaluated on the GPU "
-                               "each step (fesomc_gpu_set_device_forcing); e2e: host forcing path, the step's "
-                               "runoff and tide table copied from pinned host memory"),
+        "config": workload_config(case, cfg),
+        "forcing": "timed region: open-boundary tide and ramped river runoff evaluated on the GPU each step "
+                   "(fesomc_gpu_set_device_forcing); e2e: host forcing path, the step's runoff and tide table "
+                   "copied from pinned host memory",
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1000.0 * t_e2e / args.steps},
@@ -307,12 +353,14 @@ def run_ours(args, ws, rank, local):
     }
     g.close()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
+        cpu = host_cpu()
+        cores = cpu["threads_available"]
         os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-        rate, done, dt = cpu_oracle_rate(case, 4, budget_s=30.0)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+        rate, done, dt = cpu_oracle_rate(oracle_case(cfg), 8, budget_s=30.0)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "cpu": cpu,
                                 "sample": f"{done} internal steps of {cfg} after 1 untimed step "
-                                          f"({dt:.1f} s), CPU restatement with OpenMP"}
+                                          f"({dt:.1f} s), CPU restatement (oracle port, own mesh "
+                                          f"restatement) with OpenMP over {cores} threads"}
     reps.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -24,7 +24,7 @@ import sys
 
 import numpy as np
 
-ENERGY_ROWS = 400
+ENERGY_ROWS = 2000
 
 
 def _ints(path):

@@ -46,6 +46,37 @@ def test_device_forcing_matches_host_forcing(built, fp32, potential):
         assert np.array_equal(got[f], ref[f]), f
 
 
+@pytest.mark.parametrize("potential", [0, 1])
+def test_device_forcing_matches_oracle(built, potential):
+    """The forcing kernels (open-boundary tide of every sub-step, ramped river
+    runoff, and with T_potential the equilibrium tide) against the oracle,
+    which evaluates the same forcing on the host each step from the case's
+    forcing routines (rivers_do / obc harmonics, oracle_set_forcing); the
+    oracle runs on its own mesh restatement.  Exact."""
+    import pyoracle
+    from fesomc import abi, cases, model
+    case = cases.estuary("small", T_potential=potential)
+    ocase = cases.estuary("small", T_potential=potential, lib=pyoracle.MeshLib(abi))
+    g = model.GpuModel(case)
+    o = pyoracle.Oracle(ocase, abi, cases)
+    try:
+        g.set_forcing(case.forcing_fn(1, cases.advance_time(g.time_jd, case.params.dt)))
+        base = np.ascontiguousarray(case.forcing_fn(1, case.params.time_jd0 + 20.0)["runoff_rivers"])
+        abi.check(g.lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base), 1), "fesomc_gpu_set_device_forcing")
+        abi.check(g.lib.fesomc_gpu_run(g.h, 0, STEPS), "fesomc_gpu_run")
+        got = g.state()
+        assert o.step(STEPS) == 0
+        ref = o.state()
+    finally:
+        g.close()
+        o.close()
+    assert got["_time_jd"] == ref["_time_jd"]
+    if potential:
+        assert np.abs(ref["ssh_gp"]).max() > 0.0
+    for f in FIELDS:
+        assert np.array_equal(got[f], ref[f]), f
+
+
 def test_device_forcing_needs_river_base(built):
     from fesomc import cases, model
     case = cases.estuary("small")

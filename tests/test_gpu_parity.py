@@ -4,7 +4,12 @@ contraction, and the one transcendental of the step (the logarithm in
 d3_end's bottom boundary value) is the same IEEE-only evaluation on both
 (fesomc_log), so integer / mask results and every floating-point field are
 compared for exact equality at every step count.  This is stricter than the
-FP64 target of 1e-11 relative."""
+FP64 target of 1e-11 relative.
+
+Every case is built twice: with the product library's host mesh builder for
+the GPU run, and with the oracle's own restatement of the mesh set-up
+(oracle/oracle_mesh.c) for the oracle run, so that nothing the oracle reads
+comes from the product."""
 import math
 
 import numpy as np
@@ -39,10 +44,17 @@ def compare(sg, so):
     return bad
 
 
-def run_pair(mods, case, steps):
+def build_pair(mods, make):
+    """make(lib) -> case; returns (case for the GPU, case for the oracle)."""
     abi, cases, model, pyoracle = mods
-    g = model.GpuModel(case)
-    o = pyoracle.Oracle(case, abi, cases)
+    return make(None), make(pyoracle.MeshLib(abi))
+
+
+def run_pair(mods, make, steps):
+    abi, cases, model, pyoracle = mods
+    gcase, ocase = build_pair(mods, make)
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
     g.step(steps)
     o.step(steps)
     bad = compare(g.state(), o.state())
@@ -52,26 +64,41 @@ def run_pair(mods, case, steps):
     return bad, eg, eo
 
 
+def est(cases, *a, **kw):
+    """estuary case factory for build_pair / run_pair"""
+    return lambda lib: cases.estuary(*a, lib=lib, **kw)
+
+
+def le(cases, **params):
+    """LE_medium factory (Mt = 4, the golden series' sub-step count) with
+    parameter overrides"""
+    def make(lib):
+        c = cases.le_medium(lib=lib)
+        c.params.Mt = 4
+        for k, v in params.items():
+            setattr(c.params, k, v)
+        return c
+    return make
+
+
 def test_le_medium_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    case = cases.le_medium()
-    case.params.Mt = 4
-    bad, eg, eo = run_pair(mods, case, 20)
+    bad, eg, eo = run_pair(mods, le(cases), 20)
     assert bad == []
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
 
 def test_estuary_muscl_wetdry_tides_rivers_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    bad, eg, eo = run_pair(mods, cases.estuary("small"), 30)
+    bad, eg, eo = run_pair(mods, est(cases, "small"), 30)
     assert bad == []
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
 
 def test_estuary_upwind_implicit_visc_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    case = cases.estuary("small", tracer_adv=abi.TRACER_UPWIND, im_vert_visc=1, im_vert_visc_fic=0,
-                         filt_2D=0, filt_3D=0)
+    case = est(cases, "small", tracer_adv=abi.TRACER_UPWIND, im_vert_visc=1, im_vert_visc_fic=0,
+               filt_2D=0, filt_3D=0)
     bad, _, _ = run_pair(mods, case, 20)
     assert bad == []
 
@@ -80,41 +107,34 @@ def test_estuary_miura_bit_exact(mods):
     """solve_tracer_miura (temperature only, salinity passes through
     advection) with wetting/drying, tides and rivers."""
     abi, cases, model, pyoracle = mods
-    case = cases.estuary("small", tracer_adv=abi.TRACER_MIURA)
-    bad, eg, eo = run_pair(mods, case, 20)
+    bad, eg, eo = run_pair(mods, est(cases, "small", tracer_adv=abi.TRACER_MIURA), 20)
     assert bad == []
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
 
 def test_le_medium_miura_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    case = cases.le_medium()
-    case.params.Mt = 4
-    case.params.tracer_adv = abi.TRACER_MIURA
-    bad, _, _ = run_pair(mods, case, 20)
+    bad, _, _ = run_pair(mods, le(cases, tracer_adv=abi.TRACER_MIURA), 20)
     assert bad == []
 
 
 def test_estuary_both_vertical_viscosities_and_fic_points(mods):
     abi, cases, model, pyoracle = mods
     for fic in (0, 2):
-        case = cases.estuary("small", im_vert_visc=1, im_vert_visc_fic=1, fic_point=fic)
-        bad, _, _ = run_pair(mods, case, 10)
+        bad, _, _ = run_pair(mods, est(cases, "small", im_vert_visc=1, im_vert_visc_fic=1, fic_point=fic), 10)
         assert bad == [], fic
 
 
 def test_estuary_medium_21_levels(mods):
     """42k nodes x 20 layers, 20 internal steps, exact."""
     abi, cases, model, pyoracle = mods
-    bad, _, _ = run_pair(mods, cases.estuary("medium"), 20)
+    bad, _, _ = run_pair(mods, est(cases, "medium"), 20)
     assert bad == []
 
 
 def test_le_long_run_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    case = cases.le_medium()
-    case.params.Mt = 4
-    bad, eg, eo = run_pair(mods, case, 200)
+    bad, eg, eo = run_pair(mods, le(cases), 200)
     assert bad == []
     # the energy integral is a parallel compensated sum on the device and a
     # serial sum in the oracle: equal state, round-off-level difference
@@ -125,22 +145,97 @@ def test_estuary_upwind_implicit_visc_long_run(mods):
     """The configuration whose state first exposed a one-ulp difference of the
     device log against libm's, run ten times longer than the other cases."""
     abi, cases, model, pyoracle = mods
-    case = cases.estuary("small", tracer_adv=abi.TRACER_UPWIND, im_vert_visc=1, im_vert_visc_fic=0,
-                         filt_2D=0, filt_3D=0)
+    case = est(cases, "small", tracer_adv=abi.TRACER_UPWIND, im_vert_visc=1, im_vert_visc_fic=0,
+               filt_2D=0, filt_3D=0)
     bad, _, _ = run_pair(mods, case, 200)
     assert bad == []
 
 
-def test_le_golden_energy_on_gpu(mods):
+# the LE golden series (energy_tocheck.dat of the reference's LE_medium test
+# case, one row per 100 steps, 7 printed digits): rows the GPU must track,
+# and rows over which the oracle, on its own mesh, runs beside it
+GOLDEN_ROWS_GPU = 2000
+GOLDEN_ROWS_ORACLE = 150
+
+
+def test_le_golden_energy_series(mods):
+    """The GPU tracks the reference's printed energy over 2000 rows (200,000
+    steps, 1.16 model days); over the first 150 rows the oracle runs beside
+    it and both energies agree to 1e-12.  The first row whose energy no longer
+    rounds to the printed 7 digits (if any) is named in the failure."""
     abi, cases, model, pyoracle = mods
-    case = cases.le_medium()
-    case.params.Mt = 4
-    gold = case.meta["energy"]
-    g = model.GpuModel(case)
-    for row in range(3):
-        g.step(100)
-        assert abs(g.energy() - gold[row, 1]) <= half_unit_e16_7(gold[row, 1])
-    g.close()
+    gcase, ocase = build_pair(mods, le(cases))
+    gold = gcase.meta["energy"]
+    assert len(gold) >= GOLDEN_ROWS_GPU
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
+    off = []
+    try:
+        for row in range(GOLDEN_ROWS_GPU):
+            g.run(100)                       # LE has no forcing: graph replay
+            eg = g.energy()
+            if row < GOLDEN_ROWS_ORACLE:
+                o.step(100)
+                eo = o.energy()
+                assert abs(eg - eo) <= 1e-12 * abs(eo), row
+            if abs(eg - gold[row, 1]) > half_unit_e16_7(gold[row, 1]):
+                off.append((row, eg, float(gold[row, 1])))
+    finally:
+        g.close()
+        o.close()
+    assert off == [], "first departing row %d (%r), %d rows off" % (off[0][0], off[0][1:], len(off))
+
+
+def test_cfg0_two_tidal_days(mods):
+    """The reference's CPU-sized configuration (201 x 81 nodes at 300 m, 11
+    sigma levels, MUSCL, wetting/drying, M2 tide, river) over its stated run,
+    2 tidal days = 8,942 internal steps with the forcing of every step pushed
+    from the host, GPU against the oracle: wet/dry masks equal, and every
+    field within 1e-11 of its magnitude (the comparison is exact in practice;
+    the fields that differ at all are part of the failure text)."""
+    abi, cases, model, pyoracle = mods
+    steps = int(round(2 * 2 * 12.42 * 3600.0 / 20.0))        # 2 tidal days of 20 s steps
+    assert steps == 8942
+    gcase, ocase = build_pair(mods, est(cases, "cfg0"))
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
+    try:
+        assert g.step(steps) == 0
+        assert o.step(steps) == 0
+        sg, so = g.state(), o.state()
+        eg, eo = g.energy(), o.energy()
+    finally:
+        g.close()
+        o.close()
+    assert sg["_time_jd"] == so["_time_jd"]
+    for f in ("mask_wd", "mask_wd_node"):
+        assert np.array_equal(sg[f], so[f]), f
+    differing = compare(sg, so)
+    for f in FIELDS:
+        scale = max(float(np.abs(so[f]).max()), 1e-300)
+        assert float(np.abs(sg[f] - so[f]).max()) <= 1e-11 * scale, (f, differing)
+    assert differing == [], differing
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+
+
+def test_cfg1_bit_exact(mods):
+    """The 1.05M-node, 21-level benchmark mesh (1501 x 701 nodes at 80 m, 30 %
+    of quads split, MUSCL, wetting/drying, tide, river, 0.1 N/m2 wind),
+    4 internal steps, GPU against the oracle, exact."""
+    abi, cases, model, pyoracle = mods
+    gcase, ocase = build_pair(mods, est(cases, "cfg1"))
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
+    try:
+        g.step(4)
+        o.step(4)
+        bad = compare(g.state(), o.state())
+        eg, eo = g.energy(), o.energy()
+    finally:
+        g.close()
+        o.close()
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
 
 
 def test_graph_run_equals_stepwise(mods):
@@ -214,16 +309,13 @@ def test_estuary_biharmonic_bit_exact(mods):
     """biharmonic_viscosity (two edge Laplacians, vel_lapl_gradients) on the
     small estuary with the sponge factor, 30 steps."""
     abi, cases, model, pyoracle = mods
-    bad, eg, eo = run_pair(mods, cases.estuary("small", bih_3D=1, Abh0=1e4), 30)
+    bad, eg, eo = run_pair(mods, est(cases, "small", bih_3D=1, Abh0=1e4), 30)
     assert bad == []
 
 
 def test_le_biharmonic_bit_exact(mods):
     abi, cases, model, pyoracle = mods
-    case = cases.le_medium()
-    case.params.Mt = 4
-    case.params.bih_3D = 1
-    bad, _, _ = run_pair(mods, case, 20)
+    bad, _, _ = run_pair(mods, le(cases, bih_3D=1), 20)
     assert bad == []
 
 
@@ -232,12 +324,9 @@ def test_biharmonic_2d_bit_exact(mods):
     one's gradients from vel_gradients_2D) on the small estuary, 30 steps,
     and on LE, 20 steps."""
     abi, cases, model, pyoracle = mods
-    bad, _, _ = run_pair(mods, cases.estuary("small", bih_2D=1, Abh0=1e4), 30)
+    bad, _, _ = run_pair(mods, est(cases, "small", bih_2D=1, Abh0=1e4), 30)
     assert bad == []
-    case = cases.le_medium()
-    case.params.Mt = 4
-    case.params.bih_2D = 1
-    bad, _, _ = run_pair(mods, case, 20)
+    bad, _, _ = run_pair(mods, le(cases, bih_2D=1), 20)
     assert bad == []
 
 
@@ -246,12 +335,15 @@ def test_tidal_potential_bit_exact(mods):
     shared IEEE-only sine and cosine) gives the oracle's ssh_gp, and the run
     that feels it stays bit-exact, 30 steps."""
     abi, cases, model, pyoracle = mods
-    case = cases.estuary("small", T_potential=1)
-    case.params.n_harm = 11
-    for j in range(11):
-        case.params.harm_index[j] = j
-    g = model.GpuModel(case)
-    o = pyoracle.Oracle(case, abi, cases)
+    def make(lib):
+        case = cases.estuary("small", T_potential=1, lib=lib)
+        case.params.n_harm = 11
+        for j in range(11):
+            case.params.harm_index[j] = j
+        return case
+    gcase, ocase = build_pair(mods, make)
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
     g.step(30)
     o.step(30)
     sg, so = g.state(), o.state()
@@ -268,8 +360,9 @@ def test_estuary_many_levels_bit_exact(mods, nsigma):
     library takes): the generic d3_end, the column blocks with few entities
     per block and the 128-level solver variants, 10 steps."""
     abi, cases, model, pyoracle = mods
-    case = cases.estuary_case("small%d" % nsigma, 40, 16, 300.0, nsigma, 2.0, 25.0, stress=(0.0, 0.05))
-    bad, _, _ = run_pair(mods, case, 10)
+    def make(lib):
+        return cases.estuary_case("small%d" % nsigma, 40, 16, 300.0, nsigma, 2.0, 25.0, stress=(0.0, 0.05), lib=lib)
+    bad, _, _ = run_pair(mods, make, 10)
     assert bad == []
 
 
@@ -277,13 +370,9 @@ def test_estuary_filter2x_bit_exact(mods):
     """viscosity_filt2x_3D and viscosity_filt2x_2D (filt_bi_3D / filt_bi_2D)
     on the small estuary, 30 steps, and on LE, 20 steps."""
     abi, cases, model, pyoracle = mods
-    bad, _, _ = run_pair(mods, cases.estuary("small", filt_bi_3D=1, filt_bi_2D=1, tau_c=0.4), 30)
+    bad, _, _ = run_pair(mods, est(cases, "small", filt_bi_3D=1, filt_bi_2D=1, tau_c=0.4), 30)
     assert bad == []
-    case = cases.le_medium()
-    case.params.Mt = 4
-    case.params.filt_bi_3D = 1
-    case.params.filt_bi_2D = 1
-    bad, _, _ = run_pair(mods, case, 20)
+    bad, _, _ = run_pair(mods, le(cases, filt_bi_3D=1, filt_bi_2D=1), 20)
     assert bad == []
 
 
@@ -291,7 +380,7 @@ def test_cfg0_bit_exact(mods):
     """The reference's CPU-sized configuration (201 x 81 nodes at 300 m, 11
     sigma levels, MUSCL, wetting/drying, tide, river), 100 internal steps."""
     abi, cases, model, pyoracle = mods
-    bad, eg, eo = run_pair(mods, cases.estuary("cfg0"), 100)
+    bad, eg, eo = run_pair(mods, est(cases, "cfg0"), 100)
     assert bad == []
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
