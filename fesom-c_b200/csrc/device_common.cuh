@@ -41,6 +41,7 @@ static __device__ __forceinline__ float fesomc_log(float x) { return logf(x); }
 namespace fesomc {
 
 constexpr double kG64 = 9.8;
+constexpr double kPref = 101325.0;   // P_ref, reference atmospheric pressure (fv_var.F90:17)
 
 // Raises (never lowers) a kernel's dynamic shared-memory limit.  The
 // attribute belongs to the kernel, and every model instance of the process

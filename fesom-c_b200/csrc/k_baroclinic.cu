@@ -122,6 +122,16 @@ __global__ void __launch_bounds__(1024) k_bpg_elem(Dev d) {
                 real pr[4];
                 for (int k = 0; k < 4; ++k)
                     pr[k] = -kG * (d.atp1[nd[k]] * d.eta_n[nd[k]] - d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+                if (d.key_atm) {
+                    // sea-level pressure and E - P of the element (fv_3D_vel.F90:40-53)
+                    const real d0i = real(1.0) / d.density_0;
+                    const real atm_mean = wsum(w, (real)d.mslp[nd[0]], (real)d.mslp[nd[1]], (real)d.mslp[nd[2]],
+                                               (real)d.mslp[nd[3]]);
+                    const real emp_mean = wsum(w, (real)d.emp[nd[0]], (real)d.emp[nd[1]], (real)d.emp[nd[2]],
+                                               (real)d.emp[nd[3]]);
+                    for (int k = 0; k < 4; ++k)
+                        pr[k] = pr[k] - (real(kPref) - atm_mean) * d0i + kG * emp_mean * d0i;
+                }
                 const real ar = d.elem_area[e];
                 d.Fp[e] = make_real2(wsum(gx, pr[0], pr[1], pr[2], pr[3]) * ar, wsum(gy, pr[0], pr[1], pr[2], pr[3]) * ar);
             }

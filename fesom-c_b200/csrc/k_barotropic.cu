@@ -467,7 +467,15 @@ __global__ void __launch_bounds__(128, FESOMC_FP32 ? 8 : 6) k_u2d_elem(Dev d) {
         for (int k = 0; k < 4; ++k) {
             eab[k] = d.etaAB[nd[k]];
             dep[k] = d.depth[nd[k]];
-            etag[k] = kG64 * ((double)d.atp1[nd[k]] * eab[k] - (double)d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+            if (d.key_atm) {
+                // with atmospheric forcing: E - P and the sea-level pressure
+                // anomaly (fv_average_dynamic.F90:278-286)
+                const double d0i = 1.0 / d.density_0_d;
+                etag[k] = kG64 * ((double)d.atp1[nd[k]] * eab[k] - d.emp[nd[k]] * d0i -
+                                  (double)d.atp2[nd[k]] * d.ssh_gp[nd[k]]) + (kPref - d.mslp[nd[k]]) * d0i;
+            } else {
+                etag[k] = kG64 * ((double)d.atp1[nd[k]] * eab[k] - (double)d.atp2[nd[k]] * d.ssh_gp[nd[k]]);
+            }
         }
         real mwd = d.mask_wd[e];
         if (d.wet_dry_on) {

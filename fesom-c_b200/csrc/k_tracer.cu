@@ -14,6 +14,7 @@
 //   energy      : energy diagnostic (fv_average_dynamic.F90:476-554),
 //                 compensated deterministic two-pass reduction
 #include "device_common.cuh"
+#include "fesomc_exp.h"
 
 FESOMC_PREC_BEGIN
 
@@ -710,6 +711,102 @@ __device__ __forceinline__ void vd_coef(const Dev &d, const real *Kv, real aj, i
 // node column.  The sweep coefficients live in shared memory
 // ([array][level][thread]); T and S are re-read instead of stored.
 constexpr int kVdBlock = 128;
+// ---- atmospheric forcing of the column solve (key_atm) -------------------
+// sw_cp (fv_tracer.F90:1775-1908): heat capacity of sea water, UNESCO 1983
+// polynomial; literals without _WP in the Fortran are REAL(4) (R4).
+__device__ real sw_cp(real S, real Ti, real Pr) {
+    const real T = (Ti < real(0.0)) ? real(0.0) : Ti;
+    real S0, sS;
+    if (S < real(0.0)) { S0 = real(0.0); sS = real(0.0); }
+    else { S0 = S; sS = S * sqrt(S); }
+    const real P = Pr;
+    const real T68 = T * real(1.00024);
+    real c0 = real(4217.4), c1 = real(-3.720283), c2 = real(0.1412855), c3 = -R4(2.654387e-3), c4 = R4(2.093236e-5);
+    real a0 = real(-7.64357), a1 = real(0.1072763), a2 = -R4(1.38385e-3);
+    real b0 = real(0.1770383), b1 = -R4(4.07718e-3), b2 = R4(5.148e-5);
+    const real Cpst0 = (((c4 * T68 + c3) * T68 + c2) * T68 + c1) * T68 + c0 + (a0 + a1 * T68 + a2 * (T68 * T68)) * S0 +
+                       (b0 + b1 * T68 + b2 * (T68 * T68)) * sS;
+    a0 = -R4(4.9592e-1); a1 = R4(1.45747e-2); a2 = -R4(3.13885e-4);
+    const real a3 = R4(2.0357e-6), a4 = R4(1.7168e-8);
+    b0 = R4(2.4931e-4); b1 = -R4(1.08645e-5); b2 = R4(2.87533e-7);
+    const real b3 = -R4(4.0027e-9), b4 = R4(2.2956e-11);
+    c0 = -R4(5.422e-8); c1 = R4(2.6380e-9); c2 = -R4(6.5637e-11); c3 = R4(6.136e-13);
+    const real del_Cp0t0 = (((((c3 * T68 + c2) * T68 + c1) * T68 + c0) * P +
+                             ((((b4 * T68 + b3) * T68 + b2) * T68 + b1) * T68 + b0)) * P +
+                            ((((a4 * T68 + a3) * T68 + a2) * T68 + a1) * T68 + a0)) * P;
+    const real d0 = R4(4.9247e-3), d1 = -R4(1.28315e-4), d2 = R4(9.802e-7), d3 = R4(2.5941e-8), d4 = -R4(2.9179e-10);
+    const real e0 = -R4(1.2331e-4), e1 = -R4(1.517e-6), e2 = R4(3.122e-8);
+    const real f0 = -R4(2.9558e-6), f1 = R4(1.17054e-7), f2 = -R4(2.3905e-9), f3 = R4(1.8448e-11);
+    const real g0 = R4(9.971e-8);
+    const real h0 = R4(5.540e-10), h1 = -R4(1.7682e-11), h2 = R4(3.513e-13);
+    const real j1 = -R4(1.4300e-12);
+    const real S3_2 = sS;
+    // P**2 and P**3 as the products P*P and (P*P)*P
+    const real del_Cpstp = (((((d4 * T68 + d3) * T68 + d2) * T68 + d1) * T68 + d0) * S0 +
+                            ((e2 * T68 + e1) * T68 + e0) * S3_2) * P +
+                           ((((f3 * T68 + f2) * T68 + f1) * T68 + f0) * S0 + g0 * S3_2) * (P * P) +
+                           (((h2 * T68 + h1) * T68 + h0) * S0 + j1 * T68 * S3_2) * ((P * P) * P);
+    return Cpst0 + del_Cp0t0 + del_Cpstp;
+}
+
+// fraction of the surface shortwave left at depth z < 0: swr_paul_sim
+// (type_swr_body 1) or swr_soloviev (2), fv_tracer.F90:1566-1631
+__device__ __forceinline__ real swr_frac(const Dev &d, int n, real z) {
+    if (d.type_swr_body == 1) {
+        const real R = d.jer_const ? d.Rjc : (real)d.Rj[n];
+        const real a = d.jer_const ? d.ajc : (real)d.aj[n];
+        const real b = d.jer_const ? d.bjc : (real)d.bj[n];
+        return R * (real)fesomc_exp((double)(z / a)) + (real(1.0) - R) * (real)fesomc_exp((double)(z / b));
+    }
+    // a = (1, 0, 0), b = (10, 0, 0): sum(a*exp(b*z)), exp(0*z) = 1
+    return (real(1.0) * (real)fesomc_exp((double)(real(10.0) * z)) + real(0.0) * real(1.0)) + real(0.0) * real(1.0);
+}
+
+// calc_heat_flux_sw (fv_tracer.F90:1636-1697) for layer z (0-based) of node
+// n: the shortwave absorbed in the layer (and the non-solar flux in the top
+// one, the bottom-reflected rest in the lowest), as a temperature tendency.
+// As in the reference: T and S are T_old + T_aver and S_old + S_aver (the
+// tracers of the previous step, which are not shifted by their means at
+// this point), and sw_cp receives them in the order (T, S) against its
+// (S, T) arguments.
+__device__ real heat_source(const Dev &d, int n, size_t base, int z, real aj, real T_aver, real S_aver) {
+    const real d1 = zbar_of(d, aj, z), d2 = zbar_of(d, aj, z + 1);
+    const real T = d.Told_new[base + z] + T_aver;
+    const real S = d.Sold_new[base + z] + S_aver;
+    const real aux = (d1 + d2) * real(0.5);
+    const real rho = d.rho_c[base + z] + d.density_0;
+    const real ms = (real)d.mslp[n];
+    const real P = (ms == real(0.0)) ? (rho * kG * aux + real(kPref)) * real(10.0e-5) : (rho * kG * aux + ms) * real(10.0e-5);
+    const real c_p = sw_cp(T, S, P);
+    const real swr1 = swr_frac(d, n, -d1), swr2 = swr_frac(d, n, -d2);
+    const real jc = jc_of(d, aj, z);
+    const real qsr = (real)d.qsr[n];
+    real src;
+    if (z == 0) src = (qsr * (swr1 - swr2) + (real)d.qns[n]) / (jc * c_p * rho);
+    else src = qsr * (swr1 - swr2) / (jc * c_p * rho);
+    // the rest of the shortwave, 0.2 of it reflected by the bottom (REAL(4) 0.2)
+    if (z == d.L - 1) src = src + R4(0.2) * qsr * (swr2) / (jc * c_p * rho);
+    return src;
+}
+
+// calc_evap_precip (fv_tracer.F90:1699-1752): freshwater (E - P) source of
+// the top layer; T0 and S0 are the top layer minus their means.
+__device__ real evap_precip(const Dev &d, int n, real aj, real T0, real S0, real T_aver, real S_aver) {
+    const real T = T0 + T_aver;
+    const real S = S0 + S_aver;
+    const real rho = density_jm(T, real(0.0), -zbar_of(d, aj, 0), d.density_0);
+    const real den = (rho + d.density_0) * jc_of(d, aj, 0);
+    real frw = real(0.0);
+    if (den != real(0.0)) {
+        frw = S * (real)d.emp[n] / den;
+        if (S <= real(0.2) && frw < real(0.0)) frw = real(0.0);
+    }
+    return frw;
+}
+
+// kAtm: the atmospheric sources (key_atm) compiled in; the plain kernel keeps
+// its register count without them
+template <bool kAtm>
 __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     real *sm = reinterpret_cast<real *>(sm_raw);
@@ -731,6 +828,9 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
         real Tm = real(0.0), T0 = Tz(0), Tp = Tz(1);
         real Sm = real(0.0), S0 = Sz(0), Sp = Sz(1);
         real cpv = real(0.0), tpv = real(0.0), spv = real(0.0);  // the recurrences, in registers
+        // surface sources on wet nodes with atmospheric forcing (fv_tracer.F90:1376,1396-1418)
+        const bool atm = kAtm && d.mask_wd_node[n] != real(0.0);
+        const real frw = atm ? evap_precip(d, n, aj, T0, S0, T_aver, S_aver) : real(0.0);
         for (int k = 0; k < L; ++k) {
             real a, b, c, tr, sr;
             vd_coef(d, Kv, aj, k, a, b, c);
@@ -743,6 +843,10 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
             } else {
                 tr = -a * Tm - c * Tp + (a + c) * T0;
                 sr = -a * Sm - c * Sp + (a + c) * S0;
+            }
+            if (atm) {
+                tr = tr + d.dt * heat_source(d, n, base, k, aj, T_aver, S_aver);
+                if (k == 0) sr = sr + d.dt * frw;
             }
             if (k == 0) {
                 cpv = c / b;
@@ -869,11 +973,12 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) {
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 int config_vdiff(const Dev &d) {
-    return raise_smem_limit(k_vdiff_col, vdiff_smem(d)) ==
-                   cudaSuccess ? 0 : 1;
+    return (raise_smem_limit(k_vdiff_col<false>, vdiff_smem(d)) == cudaSuccess &&
+            raise_smem_limit(k_vdiff_col<true>, vdiff_smem(d)) == cudaSuccess) ? 0 : 1;
 }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
-    k_vdiff_col<<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
+    if (d.key_atm) k_vdiff_col<true><<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
+    else k_vdiff_col<false><<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);
 }
 int energy_parts() { return kRedGrid; }
 void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {

@@ -124,6 +124,7 @@ struct fesomc_model {
     // forcing on the device (fesomc_gpu_set_device_forcing)
     bool dev_forcing = false;
     int river_ramp = 0;
+    bool have_jer = false;                  // key_atm with jer_const = 0: Rj, aj, bj given
     double *d_clock = nullptr, *d_ampt = nullptr, *d_fazt = nullptr, *d_harm = nullptr, *d_runoff_base = nullptr;
     const double2 *d_coord = nullptr;       // node (lon, lat) for the tidal potential
     // diagnostics
@@ -436,6 +437,17 @@ int alloc_2d(fesomc_model *m) {
     for (auto p : nodes) if ((rc = dalloc(m, p, N))) return rc;
     if ((rc = dalloc(m, &d.runoff, (size_t)(d.n_rivers > 0 ? d.n_rivers : 1)))) return rc;
     if ((rc = dalloc(m, &d.ob_val, (size_t)(d.nobn > 0 ? d.nobn : 1) * (m->p.Mt > 0 ? m->p.Mt : 1)))) return rc;
+    if (m->p.key_atm) {
+        // array_setup: mslp = P_ref (fv_main.F90:1006); qns = qsr = emp = 0 (:1050-1053)
+        double **atm[] = {&d.mslp, &d.emp, &d.qsr, &d.qns};
+        for (auto p : atm) if ((rc = dalloc(m, p, N))) return rc;
+        std::vector<double> pref(N, kPref);
+        CK(cudaMemcpy(d.mslp, pref.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+        if (m->p.type_swr_body == 1 && !m->p.jer_const) {
+            double **jer[] = {&d.Rj, &d.aj, &d.bj};
+            for (auto p : jer) if ((rc = dalloc(m, p, N))) return rc;
+        }
+    }
     if ((rc = dalloc(m, &d.status, 1))) return rc;
     if ((rc = dalloc(m, &d.notconv, 1))) return rc;
     if ((rc = dalloc(m, &m->d_epart, (size_t)3 * energy_parts()))) return rc;
@@ -561,6 +573,7 @@ void share_2d(fesomc_model *m) {
     b.eta_n = a.eta_n; b.eta_n_1 = a.eta_n_1; b.eta_n_2 = a.eta_n_2; b.eta_new = a.eta_new; b.etaAB = a.etaAB;
     b.ssh_gp = a.ssh_gp; b.eta_jac = a.eta_jac; b.eta_jac_old = a.eta_jac_old;
     b.runoff = a.runoff; b.ob_val = a.ob_val; b.status = a.status; b.notconv = a.notconv;
+    b.mslp = a.mslp; b.emp = a.emp; b.qsr = a.qsr; b.qns = a.qns; b.Rj = a.Rj; b.aj = a.aj; b.bj = a.bj;
 }
 
 template <typename D>
@@ -577,6 +590,8 @@ void set_params(D &d, const fesomc_params &p) {
     d.beta_d = p.beta; d.Dmin_d = p.Dmin; d.dt_2D_d = p.dt_2D;
     d.bih_3D = p.bih_3D; d.Abh0 = p.Abh0;
     d.filt_bi_3D = p.filt_bi_3D; d.filt_bi_2D = p.filt_bi_2D; d.tau_c = p.tau_c; d.bih_2D = p.bih_2D;
+    d.key_atm = p.key_atm; d.type_swr_body = p.type_swr_body; d.jer_const = p.jer_const;
+    d.Rjc = p.Rjc; d.ajc = p.ajc; d.bjc = p.bjc; d.density_0_d = p.density_0;
 }
 
 // Algorithmic bytes per launch of every kernel: each array the kernel must
@@ -893,6 +908,8 @@ int status_code(unsigned st) {
 }
 
 int run_steps(fesomc_model *m, int nsteps) {
+    // per-node Jerlov water types must have come with the forcing
+    if (m->d.Rj && !m->have_jer) return FESOMC_ESTATE;
     for (int k = 0; k < nsteps; ++k) {
         // time update of the main loop (fv_main.F90:400-401)
         m->time_jd = m->time_jd + m->p.dt / 86400.0;
@@ -976,6 +993,10 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (par->bih_2D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
     if (par->T_potential != 0 && par->T_potential != 1) return FESOMC_EINVAL;
     if (par->npes < 0 || par->npes > 1) return FESOMC_EINVAL;   // one rank: no halo exchange
+    if (par->key_atm != 0 && par->key_atm != 1) return FESOMC_EINVAL;
+    if (par->key_atm && (par->type_swr_body < 1 || par->type_swr_body > 2 ||   // fv_read_run.F90:799-803
+                         (par->jer_const != 0 && par->jer_const != 1)))
+        return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;
@@ -1079,6 +1100,14 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
     if (f->Sclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Sclim : (void *)d.Sclim, m->fp32, L * N, f->Sclim)))
         return rc;
     if (f->taux || f->tauy || f->windx || f->windy || f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
+    if (d.mslp) {   // key_atm: FP64 node fields in both forms
+        const double *src[] = {f->mslp, f->emp, f->qsr, f->qns, f->Rj, f->aj, f->bj};
+        double *dst[] = {d.mslp, d.emp, d.qsr, d.qns, d.Rj, d.aj, d.bj};
+        for (int k = 0; k < 7; ++k)
+            if (src[k] && dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], N * 8, cudaMemcpyHostToDevice, s));
+        if (d.Rj && f->Rj && f->aj && f->bj) m->have_jer = true;
+        CK(cudaStreamSynchronize(s));
+    }
     if (f->runoff_rivers && d.n_rivers > 0) {
         std::memcpy(m->h_runoff, f->runoff_rivers, sizeof(double) * d.n_rivers);
         m->runoff_dirty = true;

@@ -52,7 +52,9 @@ class Params(C.Structure):
                                   "n_harm")] + \
         [("harm_index", C.c_int32 * 12), ("fp32_form", C.c_int32), ("bih_3D", C.c_int32), ("Abh0", C.c_double),
                                   ("filt_bi_3D", C.c_int32), ("filt_bi_2D", C.c_int32), ("tau_c", C.c_double),
-                                  ("bih_2D", C.c_int32), ("T_potential", C.c_int32), ("npes", C.c_int32)]
+                                  ("bih_2D", C.c_int32), ("T_potential", C.c_int32), ("npes", C.c_int32),
+                                  ("key_atm", C.c_int32), ("type_swr_body", C.c_int32), ("jer_const", C.c_int32),
+                                  ("Rjc", C.c_double), ("ajc", C.c_double), ("bjc", C.c_double)]
 
 
 STATE_FIELDS = ["eta_n", "eta_n_1", "eta_n_2", "etaAB", "U_n_2D", "U_n_1", "U_n_2", "U_filt_2D",
@@ -67,7 +69,8 @@ class State(C.Structure):
 
 class Forcing(C.Structure):
     _fields_ = [(n, f64p) for n in ("taux", "tauy", "windx", "windy", "runoff_rivers", "Tclim", "Sclim",
-                                    "ampt", "fazt", "amp_factor", "phy_factor")]
+                                    "ampt", "fazt", "amp_factor", "phy_factor", "mslp", "emp", "qsr", "qns",
+                                    "Rj", "aj", "bj")]
 
 
 class MeshOpts(C.Structure):

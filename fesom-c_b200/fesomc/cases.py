@@ -111,6 +111,10 @@ def default_params(**kw):
     p.filt_bi_3D, p.filt_bi_2D, p.tau_c = 0, 0, 0.4   # fv_run.dat:153,156,159
     p.bih_2D = 0                                   # fv_run.dat:157
     p.T_potential = 0
+    # atmospheric forcing off; its shortwave settings as in LE_medium's
+    # fv_run.dat:280-286 (type_swr_body 1, jer_const, R a b = 0.78 1.4 7.9)
+    p.key_atm, p.type_swr_body, p.jer_const = 0, 1, 1
+    p.Rjc, p.ajc, p.bjc = 0.78, 1.4, 7.9
     p.Cd_bz, p.Bp_bz = 10.0, 5.0
     p.clim_relax = 1.0 / (15.0 * 3600.0 * 24.0)
     p.relax2clim_ac = 1.0 / (60.0 * 3600.0 * 24.0)
@@ -307,12 +311,16 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
 
 def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=1.2, m2_phase_deg=0.0,
                  noise_sigma=0.5, seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS,
-                 lib=None, **overrides):
+                 lib=None, atm=None, **overrides):
     """Synthetic estuary: nx x ny quads at dx metres, 30 % split into
     triangles, depth h0 -> h1 across the channel plus smoothed noise of
     noise_sigma metres, river at x = 0, M2 tide of m2_amp metres and phase
     m2_phase_deg at the open boundary x = nx*dx, uniform wind stress
-    (taux, tauy) in N/m2.  Parameter overrides go to default_params."""
+    (taux, tauy) in N/m2.  atm: atmospheric forcing (turns key_atm on), a
+    dict of node fields or constants among qns, qsr (W/m2, downward), emp
+    (E - P), mslp (Pa) and Rj, aj, bj (jer_const = 0), or a callable
+    (mesh) -> such a dict, pushed with every step's forcing.  Parameter
+    overrides go to default_params."""
     xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1,
                                                             noise_sigma=noise_sigma)
     rivers = np.arange(0, nyn) * nxn + 1                 # every node on x = 0 (1-based)
@@ -325,6 +333,8 @@ def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=
               key_rivers=1, TF_presence=1, temp_on=1, salinity_on=1, filt_2D=1, filt_3D=1,
               river_salinity=5.0, clim_relax=1.0 / OB_RELAX_S, relax2clim_ac=1.0 / OB_RELAX_S)
     kw.update(overrides)
+    if atm is not None:
+        kw["key_atm"] = 1
     p = default_params(**kw)
     p.n_harm = 1
     p.harm_index[0] = 0                                  # M2
@@ -354,15 +364,22 @@ def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=
     windy = np.full(N, wspd * (sy / tau) if tau > 0 else 0.0)
     nriv = mesh.c.n_rivers
     q_total = 500.0
+    atm_fields = {}
+    if atm is not None:
+        a = atm(mesh) if callable(atm) else atm
+        for k, v in a.items():
+            atm_fields[k] = np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), (N,)))
 
     def forcing(step, time_jd):
         # rivers_do (fv_rivers.F90:263-299): constant runoff, 10-day ramp
         r = np.full(nriv, q_total / max(nriv, 1))
         if time_jd - p.time_jd0 < 10.0:
             r = r * (time_jd - p.time_jd0) / 10.0
-        return {"taux": taux, "tauy": tauy, "windx": windx, "windy": windy, "runoff_rivers": r,
-                "ampt": ampt.reshape(-1).copy(), "fazt": fazt.reshape(-1).copy(),
-                "amp_factor": amp_factor, "phy_factor": phy_factor}
+        f = {"taux": taux, "tauy": tauy, "windx": windx, "windy": windy, "runoff_rivers": r,
+             "ampt": ampt.reshape(-1).copy(), "fazt": fazt.reshape(-1).copy(),
+             "amp_factor": amp_factor, "phy_factor": phy_factor}
+        f.update(atm_fields)
+        return f
 
     meta = {"nx": nx, "ny": ny, "dx": dx, "stress": (float(sx), float(sy)), "m2_amp": m2_amp,
             "m2_phase_deg": m2_phase_deg, "noise_sigma": noise_sigma}
@@ -410,7 +427,7 @@ def forcing_struct(fdict):
     """fesomc_forcing pointing at the arrays of fdict (kept alive by caller)."""
     f = abi.Forcing()
     for k in ("taux", "tauy", "windx", "windy", "runoff_rivers", "Tclim", "Sclim", "ampt", "fazt",
-              "amp_factor", "phy_factor"):
+              "amp_factor", "phy_factor", "mslp", "emp", "qsr", "qns", "Rj", "aj", "bj"):
         a = fdict.get(k)
         if a is not None:
             a = np.ascontiguousarray(a, dtype=np.float64)

@@ -177,6 +177,23 @@ typedef struct fesomc_params {
      * mesh lives on one GPU, so fesomc_gpu_init rejects npes > 1 with
      * FESOMC_EINVAL; 0 (a zero-initialised struct) is read as 1.           */
     int32_t npes;
+    /* atmospheric forcing (key_atm of fv_run.dat, src/fv_read_run.F90:768):
+     * the sea-level pressure and E - P in the elevation gradient of
+     * update_2D_vel (src/fv_average_dynamic.F90:278-286) and in the surface
+     * pressure force of compute_vel_rhs (src/fv_3D_vel.F90:40-53), and the
+     * shortwave / non-solar heat source and the E - P freshwater source of
+     * tracer_impl_vert_diff (src/fv_tracer.F90:1376,1396-1418;
+     * calc_heat_flux_sw :1636-1697, calc_evap_precip :1699-1752, sw_cp
+     * :1775-1908) from the fesomc_forcing fields mslp, emp, qsr, qns.
+     * type_swr_body: 1 = Paulson-Simpson / Jerlov two-band profile, 2 =
+     * Soloviev (src/fv_read_run.F90:793-803); with type_swr_body 1 and
+     * jer_const = 1 the water type is Rjc, ajc, bjc (the R, a, b keys,
+     * :825-856), with jer_const = 0 the per-node Rj, aj, bj of the forcing
+     * (required before the first step, else FESOMC_ESTATE).               */
+    int32_t key_atm;
+    int32_t type_swr_body;
+    int32_t jer_const;
+    double Rjc, ajc, bjc;
 } fesomc_params;
 
 /*
@@ -215,6 +232,14 @@ typedef struct fesomc_forcing {
     const double *Tclim, *Sclim;    /* (nsigma-1,nod2D)                        */
     const double *ampt, *fazt;      /* (nobn,12) OB tidal amplitude / phase    */
     const double *amp_factor, *phy_factor; /* (12)                             */
+    /* key_atm only (what sbc_do leaves in o_ARRAYS, src/fv_main.F90:419);
+     * before the first one the library holds mslp = P_ref = 101325 Pa
+     * (src/fv_main.F90:1006) and zero emp, qsr, qns (:1050-1053)         */
+    const double *mslp;             /* (nod2D) sea-level pressure, Pa          */
+    const double *emp;              /* (nod2D) evaporation - precipitation     */
+    const double *qsr;              /* (nod2D) downward shortwave, W/m^2       */
+    const double *qns;              /* (nod2D) downward non-solar heat, W/m^2  */
+    const double *Rj, *aj, *bj;     /* (nod2D) Jerlov water type per node (jer_const = 0) */
 } fesomc_forcing;
 
 /* Opaque model instance. */

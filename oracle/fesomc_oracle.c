@@ -36,6 +36,7 @@
 
 #include "../include/fesomc_gpu.h"
 #include "../fesom-c_b200/csrc/fesomc_log.h"
+#include "../fesom-c_b200/csrc/fesomc_exp.h"
 #include "../fesom-c_b200/csrc/fesomc_trig.h"
 
 /* ---------------------------------------------------------------- consts */
@@ -77,6 +78,7 @@ typedef struct oracle_model {
     double *bt, *snu, *Kv, *Av, *Ri, *tke_dissip, *Wvel;
     /* forcing */
     double *runoff, *ampt, *fazt, amp_factor[12], phy_factor[12];
+    double *mslp, *emp, *qsr, *qns, *Rj, *aj, *bj;   /* key_atm (sbc_do fields, jer_const = 0 water types) */
     /* scratch */
     double *s_e1, *s_e2, *s_e3, *s_e4, *s_n1, *s_n2, *s_n3, *s_n4, *s_ed1, *s_ed2, *s_ed3, *s_ed4;
     double *s_gr;
@@ -148,6 +150,7 @@ static double densityJM(double t, double s, double pz, double density_0) {
 
 /* the shared logarithm and cosine, exported for their accuracy tests */
 double oracle_log(double x) { return fesomc_log(x); }
+double oracle_exp(double x) { return fesomc_exp(x); }
 double oracle_cos(double x) { return fesomc_cos(x); }
 double oracle_sin(double x) { return fesomc_sin(x); }
 
@@ -351,7 +354,9 @@ static inline double wsum2e(const oracle_model *m, int el, const double *x, cons
          + WCV(3, el) * (N1(x, ELN(3, el)) + N1(y, ELN(3, el))) + WCV(4, el) * (N1(x, ELN(4, el)) + N1(y, ELN(4, el)));
 }
 
-/* update_2D_vel, fv_average_dynamic.F90:228-443 (type_task 3, key_atm off) */
+/* update_2D_vel, fv_average_dynamic.F90:228-443 (type_task 3).  density0_inv
+ * is 1/density_0 as set at :272 (the reference lists it PRIVATE in the
+ * OpenMP region of :277, which a serial build does not see) */
 /* viscosity_filt2x_2D, fv_viscosity.F90:672-767: UV2_rhs from U_n_2D */
 static void viscosity_filt2x_2D(oracle_model *m) {
     double *U_c = malloc(sizeof(double) * (size_t)m->E), *V_c = malloc(sizeof(double) * (size_t)m->E);
@@ -467,7 +472,11 @@ static void update_2D_vel(oracle_model *m, int step) {
     for (int n = 1; n <= m->N; ++n) {
         N1(m->eta_n_2, n) = de * N1(m->ssh_rhs, n) + fe * N1(m->eta_n, n) + ga * N1(m->eta_n_1, n) + ep * N1(m->eta_n_2, n);
         N1(m->etaAB, n) = N1(m->eta_n_2, n);
-        N1(eta, n) = WP_G * (ATP(n, 1) * N1(m->eta_n_2, n) - ATP(n, 2) * N1(m->ssh_gp, n));
+        if (m->p.key_atm)   /* fv_average_dynamic.F90:278-286 */
+            N1(eta, n) = WP_G * (ATP(n, 1) * N1(m->eta_n_2, n) - N1(m->emp, n) * density0_inv - ATP(n, 2) * N1(m->ssh_gp, n))
+                       + (WP_P_REF - N1(m->mslp, n)) * density0_inv;
+        else
+            N1(eta, n) = WP_G * (ATP(n, 1) * N1(m->eta_n_2, n) - ATP(n, 2) * N1(m->ssh_gp, n));
     }
     if (m->p.wet_dry_on) wad_mask(m);
 #pragma omp parallel for
@@ -1354,7 +1363,7 @@ static void viscosity_filt2x_3D(oracle_model *m) {
     free(V_c);
 }
 
-/* compute_vel_rhs, fv_3D_vel.F90:1-197 (key_atm off) */
+/* compute_vel_rhs, fv_3D_vel.F90:1-197 */
 static void compute_vel_rhs(oracle_model *m) {
     const int L = m->L;
     const double eps = m->p.epsilon;
@@ -1364,6 +1373,15 @@ static void compute_vel_rhs(oracle_model *m) {
         for (int k = 1; k <= 4; ++k) {
             int nk = ELN(k, el);
             pre[k - 1] = -WP_G * (ATP(nk, 1) * N1(m->eta_n, nk) - ATP(nk, 2) * N1(m->ssh_gp, nk));
+        }
+        if (m->p.key_atm) {   /* fv_3D_vel.F90:40-53 */
+            const double density0_inv = 1.0 / m->p.density_0;
+            double Atm_mean = WCV(1, el) * N1(m->mslp, ELN(1, el)) + WCV(2, el) * N1(m->mslp, ELN(2, el))
+                            + WCV(3, el) * N1(m->mslp, ELN(3, el)) + WCV(4, el) * N1(m->mslp, ELN(4, el));
+            double emp_mean = WCV(1, el) * N1(m->emp, ELN(1, el)) + WCV(2, el) * N1(m->emp, ELN(2, el))
+                            + WCV(3, el) * N1(m->emp, ELN(3, el)) + WCV(4, el) * N1(m->emp, ELN(4, el));
+            for (int k = 0; k < 4; ++k)
+                pre[k] = pre[k] - (WP_P_REF - Atm_mean) * density0_inv + WP_G * emp_mean * density0_inv;
         }
         double sx = 0, sy = 0;
         for (int k = 1; k <= 4; ++k) sx = sx + GS(k, el) * pre[k - 1];
@@ -1942,7 +1960,111 @@ static void solve_tracer_muscl(oracle_model *m, double *ttf, double *ttfold, int
 #undef UDG
 }
 
-/* tracer_impl_vert_diff, fv_tracer.F90:1319-1494 (key_atm off) */
+/* ---- surface sources of the column solve with key_atm --------------------- */
+
+/* sw_cp, fv_tracer.F90:1775-1908 (UNESCO 1983 heat capacity); literals
+ * without _WP are REAL(4) */
+static double sw_cp(double S, double Ti, double Pr) {
+    double T, S0, sS;
+    if (Ti < 0) T = 0.0; else T = Ti;
+    if (S < 0) { S0 = 0.0; sS = 0.0; } else { S0 = S; sS = S * sqrt(S); }
+    double P = Pr;
+    double T68 = T * 1.00024;
+    double c0 = 4217.4, c1 = -3.720283, c2 = 0.1412855, c3 = R4(-2.654387e-3f), c4 = R4(2.093236e-5f);
+    double a0 = -7.64357, a1 = 0.1072763, a2 = R4(-1.38385e-3f);
+    double b0 = 0.1770383, b1 = R4(-4.07718e-3f), b2 = R4(5.148e-5f);
+    double Cpst0 = (((c4 * T68 + c3) * T68 + c2) * T68 + c1) * T68 + c0 +
+                   (a0 + a1 * T68 + a2 * (T68 * T68)) * S0 +
+                   (b0 + b1 * T68 + b2 * (T68 * T68)) * sS;
+    a0 = R4(-4.9592e-1f); a1 = R4(1.45747e-2f); a2 = R4(-3.13885e-4f);
+    double a3 = R4(2.0357e-6f), a4 = R4(1.7168e-8f);
+    b0 = R4(2.4931e-4f); b1 = R4(-1.08645e-5f); b2 = R4(2.87533e-7f);
+    double b3 = R4(-4.0027e-9f), b4 = R4(2.2956e-11f);
+    c0 = R4(-5.422e-8f); c1 = R4(2.6380e-9f); c2 = R4(-6.5637e-11f); c3 = R4(6.136e-13f);
+    double del_Cp0t0 = (((((c3 * T68 + c2) * T68 + c1) * T68 + c0) * P +
+                        ((((b4 * T68 + b3) * T68 + b2) * T68 + b1) * T68 + b0)) * P +
+                        ((((a4 * T68 + a3) * T68 + a2) * T68 + a1) * T68 + a0)) * P;
+    double d0 = R4(4.9247e-3f), d1 = R4(-1.28315e-4f), d2 = R4(9.802e-7f), d3 = R4(2.5941e-8f), d4 = R4(-2.9179e-10f);
+    double e0 = R4(-1.2331e-4f), e1 = R4(-1.517e-6f), e2 = R4(3.122e-8f);
+    double f0 = R4(-2.9558e-6f), f1 = R4(1.17054e-7f), f2 = R4(-2.3905e-9f), f3 = R4(1.8448e-11f);
+    double g0 = R4(9.971e-8f);
+    double h0 = R4(5.540e-10f), h1 = R4(-1.7682e-11f), h2 = R4(3.513e-13f);
+    double j1 = R4(-1.4300e-12f);
+    double S3_2 = sS;
+    /* P**2 and P**3 as the products P*P and (P*P)*P */
+    double del_Cpstp = (((((d4 * T68 + d3) * T68 + d2) * T68 + d1) * T68 + d0) * S0 +
+                        ((e2 * T68 + e1) * T68 + e0) * S3_2) * P +
+                       ((((f3 * T68 + f2) * T68 + f1) * T68 + f0) * S0 + g0 * S3_2) * (P * P) +
+                       (((h2 * T68 + h1) * T68 + h0) * S0 + j1 * T68 * S3_2) * ((P * P) * P);
+    return Cpst0 + del_Cp0t0 + del_Cpstp;
+}
+
+/* swr_paul_sim (fv_tracer.F90:1611-1631) and swr_soloviev (:1566-1609) */
+static double swr_paul_sim(double z, double R, double a, double b) {
+    return R * fesomc_exp(z / a) + (1 - R) * fesomc_exp(z / b);
+}
+static double swr_soloviev(double z) {
+    const double a[3] = {1.0, 0.0, 0.0}, b[3] = {10.0, 0.0, 0.0};
+    double s = a[0] * fesomc_exp(b[0] * z);
+    s = s + a[1] * fesomc_exp(b[1] * z);
+    s = s + a[2] * fesomc_exp(b[2] * z);
+    return s;
+}
+
+/* calc_heat_flux_sw, fv_tracer.F90:1636-1697: num_sig 1-based */
+static double calc_heat_flux_sw(oracle_model *m, int num_sig, int i) {
+    double d1 = W3(m->zbar, num_sig, i);
+    double d2 = W3(m->zbar, num_sig + 1, i);
+    double T = F3(m->T_old, num_sig, i) + m->T_aver;
+    double S = F3(m->S_old, num_sig, i) + m->S_aver;
+    double aux = (d1 + d2) * 0.5;
+    double rho = F3(m->rho_c, num_sig, i) + m->p.density_0;
+    double P;
+    if (N1(m->mslp, i) == 0.0) P = (rho * WP_G * aux + WP_P_REF) * 10.0e-5;
+    else P = (rho * WP_G * aux + N1(m->mslp, i)) * 10.0e-5;
+    double c_p = sw_cp(T, S, P);   /* called as sw_cp(T, S, P, c_p) against sw_cp(S, Ti, Pr, cp0) */
+    double swr1 = 0.0, swr2 = 0.0;
+    if (m->p.type_swr_body == 1) {
+        if (m->p.jer_const) {
+            swr1 = swr_paul_sim(-d1, m->p.Rjc, m->p.ajc, m->p.bjc);
+            swr2 = swr_paul_sim(-d2, m->p.Rjc, m->p.ajc, m->p.bjc);
+        } else {
+            swr1 = swr_paul_sim(-d1, N1(m->Rj, i), N1(m->aj, i), N1(m->bj, i));
+            swr2 = swr_paul_sim(-d2, N1(m->Rj, i), N1(m->aj, i), N1(m->bj, i));
+        }
+    } else if (m->p.type_swr_body == 2) {
+        swr1 = swr_soloviev(-d1);
+        swr2 = swr_soloviev(-d2);
+    }
+    double swr_source;
+    if (num_sig == 1) swr_source = (N1(m->qsr, i) * (swr1 - swr2) + N1(m->qns, i)) / (F3(m->Jc, num_sig, i) * c_p * rho);
+    else swr_source = N1(m->qsr, i) * (swr1 - swr2) / (F3(m->Jc, num_sig, i) * c_p * rho);
+    if (num_sig == m->NS - 1)
+        swr_source = swr_source + R4(0.2f) * N1(m->qsr, i) * (swr2) / (F3(m->Jc, num_sig, i) * c_p * rho);
+    return swr_source;
+}
+
+/* calc_evap_precip, fv_tracer.F90:1699-1752 (TF, SF here shifted by their means) */
+static double calc_evap_precip(oracle_model *m, int i) {
+    double T = F3(m->TF, 1, i) + m->T_aver;
+    double S = F3(m->SF, 1, i) + m->S_aver;
+    double rho = densityJM(T, 0.0, -W3(m->zbar, 1, i), m->p.density_0);
+    double frw;
+    if ((rho + m->p.density_0) * F3(m->Jc, 1, i) != 0) {
+        frw = S * N1(m->emp, i) / ((rho + m->p.density_0) * F3(m->Jc, 1, i));
+        if (S <= 0.2) {
+            if (frw < 0) frw = 0.0;
+        }
+    } else {
+        frw = 0.0;
+    }
+    return frw;
+}
+
+/* exported for the CPU tests */
+double oracle_sw_cp(double S, double T, double P) { return sw_cp(S, T, P); }
+
+/* tracer_impl_vert_diff, fv_tracer.F90:1319-1494 */
 static void tracer_impl_vert_diff(oracle_model *m) {
     const int L = m->L, NS = m->NS;
     const double dt = m->p.dt, T_aver = m->T_aver, S_aver = m->S_aver;
@@ -1966,14 +2088,27 @@ static void tracer_impl_vert_diff(oracle_model *m) {
         a[L] = -dt * W3(m->Kv, L, n) / ((ZZ(L - 1) - ZZ(L)) * (ZB(L) - ZB(NS)));
         b[L] = -a[L] + 1.0;
         c[L] = 0.0;
-        tr[1] = c[1] * (-TT(2) + TT(1));
-        sr[1] = c[1] * (-SS(2) + SS(1));
-        for (int nz = 2; nz <= NS - 2; ++nz) {
-            tr[nz] = -a[nz] * TT(nz - 1) - c[nz] * TT(nz + 1) + (a[nz] + c[nz]) * TT(nz);
-            sr[nz] = -a[nz] * SS(nz - 1) - c[nz] * SS(nz + 1) + (a[nz] + c[nz]) * SS(nz);
+        if (m->p.key_atm && N1(m->mask_wd_node, n) != 0.0) {
+            /* heat and freshwater sources (fv_tracer.F90:1376,1396-1418) */
+            double frw = calc_evap_precip(m, n);
+            tr[1] = c[1] * (-TT(2) + TT(1)) + dt * calc_heat_flux_sw(m, 1, n);
+            sr[1] = c[1] * (-SS(2) + SS(1)) + dt * frw;
+            for (int nz = 2; nz <= NS - 2; ++nz) {
+                tr[nz] = -a[nz] * TT(nz - 1) - c[nz] * TT(nz + 1) + (a[nz] + c[nz]) * TT(nz) + dt * calc_heat_flux_sw(m, nz, n);
+                sr[nz] = -a[nz] * SS(nz - 1) - c[nz] * SS(nz + 1) + (a[nz] + c[nz]) * SS(nz);
+            }
+            tr[L] = a[L] * (TT(L) - TT(L - 1)) + dt * calc_heat_flux_sw(m, L, n);
+            sr[L] = a[L] * (SS(L) - SS(L - 1));
+        } else {
+            tr[1] = c[1] * (-TT(2) + TT(1));
+            sr[1] = c[1] * (-SS(2) + SS(1));
+            for (int nz = 2; nz <= NS - 2; ++nz) {
+                tr[nz] = -a[nz] * TT(nz - 1) - c[nz] * TT(nz + 1) + (a[nz] + c[nz]) * TT(nz);
+                sr[nz] = -a[nz] * SS(nz - 1) - c[nz] * SS(nz + 1) + (a[nz] + c[nz]) * SS(nz);
+            }
+            tr[L] = a[L] * (TT(L) - TT(L - 1));
+            sr[L] = a[L] * (SS(L) - SS(L - 1));
         }
-        tr[L] = a[L] * (TT(L) - TT(L - 1));
-        sr[L] = a[L] * (SS(L) - SS(L - 1));
         cp[1] = c[1] / b[1];
         tp[1] = tr[1] / b[1];
         sp[1] = sr[1] / b[1];
@@ -2201,6 +2336,10 @@ oracle_model *oracle_create(const fesomc_mesh *msh, const fesomc_params *par, co
     m->Unode = dalloc(L * N); m->Vnode = dalloc(L * N); m->Unode_p = dalloc(L * N); m->Vnode_p = dalloc(L * N);
     m->Bar_pru_3D = dalloc(L * E); m->Bar_prv_3D = dalloc(L * E);
     m->runoff = dalloc(msh->n_rivers);
+    /* array_setup: mslp = P_ref (fv_main.F90:1006), qns = qsr = emp = 0 (:1050-1053) */
+    m->mslp = dalloc(N); m->emp = dalloc(N); m->qsr = dalloc(N); m->qns = dalloc(N);
+    m->Rj = dalloc(N); m->aj = dalloc(N); m->bj = dalloc(N);
+    for (size_t i = 0; i < N; ++i) m->mslp[i] = WP_P_REF;
     m->ampt = dalloc((size_t)msh->nobn * 12); m->fazt = dalloc((size_t)msh->nobn * 12);
     for (int j = 0; j < 12; ++j) { m->amp_factor[j] = 1.0; m->phy_factor[j] = 0.0; }
     size_t big = L * (E > N ? E : N);
@@ -2230,6 +2369,13 @@ int oracle_set_forcing(oracle_model *m, const fesomc_forcing *f) {
     if (f->fazt && m->nobn) memcpy(m->fazt, f->fazt, (size_t)m->nobn * 12 * 8);
     if (f->amp_factor) memcpy(m->amp_factor, f->amp_factor, 12 * 8);
     if (f->phy_factor) memcpy(m->phy_factor, f->phy_factor, 12 * 8);
+    if (f->mslp) memcpy(m->mslp, f->mslp, N * 8);
+    if (f->emp) memcpy(m->emp, f->emp, N * 8);
+    if (f->qsr) memcpy(m->qsr, f->qsr, N * 8);
+    if (f->qns) memcpy(m->qns, f->qns, N * 8);
+    if (f->Rj) memcpy(m->Rj, f->Rj, N * 8);
+    if (f->aj) memcpy(m->aj, f->aj, N * 8);
+    if (f->bj) memcpy(m->bj, f->bj, N * 8);
     return 0;
 }
 

@@ -55,6 +55,10 @@ def load(abi):
         lib.oracle_cos.argtypes = [C.c_double]
         lib.oracle_sin.restype = C.c_double
         lib.oracle_sin.argtypes = [C.c_double]
+        lib.oracle_exp.restype = C.c_double
+        lib.oracle_exp.argtypes = [C.c_double]
+        lib.oracle_sw_cp.restype = C.c_double
+        lib.oracle_sw_cp.argtypes = [C.c_double, C.c_double, C.c_double]
         lib.oracle_mesh_build.restype = C.c_int
         lib.oracle_mesh_build.argtypes = [C.c_int32, abi.f64p, abi.i32p, C.c_int32, abi.i32p, abi.f64p,
                                           C.POINTER(abi.MeshOpts), C.POINTER(C.c_void_p)]

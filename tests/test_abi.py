@@ -73,3 +73,17 @@ def test_host_density_matches_oracle(built):
     # pure water near 17.9 C and 35.7 C (independent sanity of the EOS restatement)
     assert abs(built.fesomc_host_density_jm(17.857142857142858, 0.0, 0.0, 0.0) - 998.62) < 0.01
     assert abs(built.fesomc_host_density_jm(35.714285714285715, 0.0, 0.0, 0.0) - 993.79) < 0.01
+
+
+def test_init_rejects_bad_atmospheric_options_without_gpu(built):
+    """key_atm must be 0/1, type_swr_body 1 or 2 and jer_const 0/1
+    (fv_read_run.F90:799-803)."""
+    from fesomc import cases
+    case = cases.estuary("small")
+    arrays = case.new_state_arrays()
+    st = case.state_struct(arrays, case.params.time_jd0)
+    h = C.c_void_p()
+    for bad in ({"key_atm": 2}, {"key_atm": 1, "type_swr_body": 3}, {"key_atm": 1, "jer_const": 2}):
+        p = cases.default_params(**bad)
+        p.scale_area, p.density_0 = case.params.scale_area, case.params.density_0
+        assert built.fesomc_gpu_init(C.byref(case.mesh.c), C.byref(p), C.byref(st), C.byref(h)) == 1, bad

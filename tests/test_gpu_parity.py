@@ -403,3 +403,73 @@ def test_cfg1_scale_properties(mods):
         assert np.all(np.isfinite(s[k]))
         assert np.array_equal(out[0][k], out[1][k])
     assert set(np.unique(s["mask_wd"])) <= {0.0, 1.0}
+
+
+def _atm_varied(mesh):
+    """Shortwave, non-solar flux, E - P and a sea-level pressure gradient
+    that vary over the estuary (seeded)."""
+    rng = np.random.default_rng(11)
+    x = mesh.coord_nod2D[:, 0] / mesh.coord_nod2D[:, 0].max()
+    return {"qsr": 250.0 + 50.0 * rng.random(mesh.N), "qns": -60.0 + 20.0 * x,
+            "emp": 2.0e-5 * (x - 0.5), "mslp": 101325.0 + 400.0 * x}
+
+
+def _atm_per_node(mesh):
+    f = _atm_varied(mesh)
+    rng = np.random.default_rng(12)
+    f.update(Rj=0.58 + 0.2 * rng.random(mesh.N), aj=0.35 + rng.random(mesh.N), bj=5.0 + 20.0 * rng.random(mesh.N))
+    return f
+
+
+@pytest.mark.parametrize("variant", ["cfg4_heat_loss", "jerlov_const", "soloviev", "jerlov_per_node"])
+def test_key_atm_bit_exact(mods, variant):
+    """Atmospheric forcing (key_atm): the sea-level pressure and E - P in
+    the elevation gradient of the sub-cycle and in the surface pressure force
+    of the 3D step, and the shortwave / non-solar heat and E - P freshwater
+    sources of the tracer column solve, 20 steps on the small estuary, exact.
+    cfg4_heat_loss is the learned-closure configuration's -100 W/m2 surface
+    heat flux; the others exercise both shortwave profiles and per-node
+    Jerlov water types."""
+    abi, cases, model, pyoracle = mods
+    atm, kw = {
+        "cfg4_heat_loss": ({"qns": -100.0, "qsr": 0.0, "emp": 0.0}, {}),
+        "jerlov_const": (_atm_varied, {}),
+        "soloviev": (_atm_varied, {"type_swr_body": 2}),
+        "jerlov_per_node": (_atm_per_node, {"jer_const": 0}),
+    }[variant]
+    bad, eg, eo = run_pair(mods, est(cases, "small", atm=atm, **kw), 20)
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+
+
+def test_key_atm_changes_the_run_and_fp32_form_runs(mods):
+    """The surface heat loss cools the estuary against the run without it,
+    and the FP32 form runs the same forcing (finite, within 0.01 C of FP64)."""
+    abi, cases, model, pyoracle = mods
+    heat = {"qns": -100.0, "qsr": 0.0, "emp": 0.0}
+    out = {}
+    for name, atm, fp32 in (("off", None, 0), ("on", heat, 0), ("on32", heat, 1)):
+        c = cases.estuary("small", atm=atm)
+        c.params.fp32_form = fp32
+        g = model.GpuModel(c)
+        g.step(20)
+        out[name] = g.state()
+        g.close()
+    wet = out["on"]["mask_wd_node"] > 0
+    L = c.mesh.L
+    top = lambda s: s["TF"].reshape(-1, L)[wet, 0]
+    assert np.mean(top(out["on"]) - top(out["off"])) < -1e-4
+    assert np.all(np.isfinite(out["on32"]["TF"]))
+    assert np.max(np.abs(out["on32"]["TF"] - out["on"]["TF"])) < 0.01
+
+
+def test_key_atm_per_node_water_types_required(mods):
+    """With jer_const = 0 the per-node Rj, aj, bj must come with the forcing
+    before the first step (FESOMC_ESTATE otherwise)."""
+    abi, cases, model, pyoracle = mods
+    c = cases.estuary("small", atm={"qns": -100.0}, jer_const=0)
+    g = model.GpuModel(c)
+    try:
+        assert g.step(1, check=False) == 4
+    finally:
+        g.close()

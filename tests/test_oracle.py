@@ -331,3 +331,72 @@ def test_estuary_filter2x_oracle(mods):
     for key in ("3d", "2d"):
         assert np.isfinite(out[key]["U_n"]).all()
         assert not np.array_equal(out[key]["U_n"], out["none"]["U_n"])
+
+
+def test_shared_exp_within_one_ulp_of_libm(mods):
+    """fesomc_exp (the IEEE-only exponential of the shortwave absorption
+    profiles, shared by the oracle and the device kernels) against the C
+    library's exp: at most one ulp apart over the normal range; subnormal
+    results and the over/underflow ends included."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    rng = np.random.default_rng(6)
+    xs = np.concatenate([rng.uniform(-700.0, 700.0, 20000),         # whole normal range
+                         rng.uniform(-60.0, 0.0, 20000),            # z / a of the profiles
+                         rng.uniform(-1e-3, 1e-3, 5000),
+                         [0.0, -0.0, 1.0, -1.0, 709.78, -708.3, 1e-300, -1e-300]])
+    ours = np.array([lib.oracle_exp(float(x)) for x in xs])
+    ref = np.array([math.exp(float(x)) for x in xs])
+    ulps = np.abs(ours.view(np.int64) - ref.view(np.int64))
+    assert ulps.max() <= 1
+    assert np.mean(ulps != 0) < 0.1
+    assert lib.oracle_exp(0.0) == 1.0
+    for x in (-710.0, -720.0, -740.0):
+        assert abs(lib.oracle_exp(x) - math.exp(x)) <= 2 * 5e-324 + 2e-16 * math.exp(x)
+    assert lib.oracle_exp(-800.0) == 0.0 and lib.oracle_exp(800.0) == math.inf
+    assert math.isnan(lib.oracle_exp(math.nan))
+
+
+def test_sw_cp_unesco_check_value(mods):
+    """sw_cp (fv_tracer.F90:1775-1908) against the UNESCO 1983 check value
+    (Fofonoff and Millard, Unesco Tech. Pap. Mar. Sci. 44): cp = 3849.500
+    J/(kg K) at S = 40, T68 = 40 C, p = 10000 dbar (1000 bar, the routine's
+    unit); and pure water at the surface at 0 C: the polynomial's 4217.4."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    assert abs(lib.oracle_sw_cp(40.0, 40.0 / 1.00024, 1000.0) - 3849.500) < 0.01
+    assert abs(lib.oracle_sw_cp(0.0, 0.0, 0.0) - 4217.4) < 1e-9
+    # the routine clamps negative temperature and salinity to zero
+    assert lib.oracle_sw_cp(-1.0, -2.0, 0.0) == lib.oracle_sw_cp(0.0, 0.0, 0.0)
+
+
+def test_surface_heat_flux_cools_the_top_layer(mods):
+    """key_atm with a -100 W/m2 non-solar flux (the learned-closure forcing):
+    after one step the wet top layer is cooler than in the same run with a
+    zero flux, by up to dt * qns / (rho c_p Jc) (the heat source of the top
+    layer, fv_tracer.F90:1686-1690, spread down by the implicit diffusion),
+    and the domain heat content drops by about dt * qns * wet area / (rho
+    c_p)."""
+    abi, cases, pyoracle = mods
+    runs = []
+    for qns in (0.0, -100.0):
+        c = cases.estuary("small", atm={"qns": qns, "qsr": 0.0, "emp": 0.0})
+        o = pyoracle.Oracle(c, abi, cases)
+        o.step(1)
+        runs.append((c, o.state()))
+        o.close()
+    (c, s0), (_, s1) = runs
+    m, L, dt = c.mesh, c.mesh.L, c.params.dt
+    T0 = s0["TF"].reshape(m.N, L)
+    T1 = s1["TF"].reshape(m.N, L)
+    wet = s0["mask_wd_node"] > 0
+    dT = T1 - T0
+    assert np.all(dT[wet, 0] < 0.0)
+    H = np.maximum(m.depth + s0["eta_n"], c.params.Dmin)
+    jc = H * (m.sigma[0] - m.sigma[1])
+    rho_cp = 1025.0 * 3990.0
+    expect = dt * (-100.0) / (rho_cp * jc)
+    ratio = dT[wet, 0] / expect[wet]
+    assert np.median(ratio) > 0.3 and ratio.max() < 1.1
+    heat = np.sum(m.area[wet, None] * (dT[wet] * (H[wet, None] * (m.sigma[:-1] - m.sigma[1:])[None, :])))
+    assert abs(heat / (dt * -100.0 * m.area[wet].sum() / rho_cp) - 1.0) < 0.05
