@@ -1,0 +1,193 @@
+// Learned vertical-mixing closure, the model side: per node column the
+// network's inputs (from the same state d3_end reads, src/fv_mixing.F90:
+// 109-196), the training-envelope test that hands a column to the plain
+// closure, the training-set harvest, the application of the network's
+// output to snu, Kv and bt, and the judge statistics.  Compiled once per
+// arithmetic precision like the other state kernels.  No counterpart in the
+// reference.
+#include "closure.h"
+#include "device_common.cuh"
+
+FESOMC_PREC_BEGIN
+
+// Raw (transformed, not normalised) inputs of node column 'node', written to
+// f[0..IN) with stride 1 (layout in closure.h).
+__device__ void lc_inputs(const Dev &d, int node, float *f) {
+    const int NS = d.NS, L = d.L;
+    const real *Un = d.Unode + (size_t)node * L;
+    const real *Vn = d.Vnode + (size_t)node * L;
+    const real *T = d.TF + (size_t)node * L;
+    const real *S = d.SF + (size_t)node * L;
+    const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+    const real dmean2 = dmean * dmean;
+    const real ajac = jac_a(d, d.eta_jac, node);
+    for (int k = 0; k < NS; ++k) {
+        real sh = real(0.0), n2 = real(0.0);
+        if (k >= 1 && k <= NS - 2) {
+            const real d1 = __ldg(d.sig + k - 1) - __ldg(d.sig + k);
+            const real d2 = __ldg(d.sig + k) - __ldg(d.sig + k + 1);
+            const real dd = real(0.5) * (d1 + d2);
+            const real ap1 = Un[k - 1] - Un[k], ap2 = Vn[k - 1] - Vn[k];
+            sh = (ap1 * ap1 + ap2 * ap2) / (dd * dd) / dmean2;
+            const real zb = zbar_of(d, ajac, k);
+            const real rho_up = density_jm(T[k - 1], S[k - 1], -zb, d.density_0);
+            const real rho_dn = density_jm(T[k], S[k], -zb, d.density_0);
+            n2 = -kG * (rho_up - rho_dn) / dd / (d.density_0 * dmean);
+        }
+        f[k] = asinhf((float)sh / kLcX0);
+        f[NS + k] = asinhf((float)n2 / kLcX0);
+        f[2 * NS + k] = (float)zbar_of(d, ajac, k);
+    }
+    const real wx = d.windx[node], wy = d.windy[node];
+    const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+    const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+    const real lg = log(delta_b / d.z0b_min);
+    const real bott_R = real(16.6) * (d.cka * d.cka) / (lg * lg);
+    const real bot = bott_R * (Un[L - 1] * Un[L - 1] + Vn[L - 1] * Vn[L - 1]);
+    f[3 * NS] = asinhf((float)u_din_sur / kLcX0);
+    f[3 * NS + 1] = asinhf((float)bot / kLcX0);
+    f[3 * NS + 2] = (float)dmean;
+}
+
+// warp-aggregated append of 'take' lanes to a list counter
+__device__ __forceinline__ unsigned long long warp_append(bool take, unsigned long long *ctr) {
+    const unsigned mask = __activemask();
+    const unsigned b = __ballot_sync(mask, take);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned long long base = 0;
+    if (lane == leader && b) base = atomicAdd(ctr, (unsigned long long)__popc(b));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(b & ((1u << lane) - 1u));
+}
+
+// Inputs of every column, normalised into X; the envelope test; the list of
+// columns the plain closure takes (dry or outside the envelope); counters.
+__global__ void k_lc_features(Dev d, LcView c) {
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        float *x = c.X + (size_t)node * c.IN;
+        lc_inputs(d, node, x);
+        const bool wet = d.mask_wd_node[node] != real(0.0);
+        bool in = true;
+        for (int j = 0; j < c.IN; ++j) {
+            const float v = (x[j] - c.mu_x[j]) / c.sd_x[j];
+            x[j] = v;
+            in = in && (v >= c.lo_x[j]) && (v <= c.hi_x[j]);
+        }
+        const bool net = wet && in;
+        c.flag[node] = net ? 1 : 0;
+        const unsigned long long slot = warp_append(!net, c.count);
+        if (!net) c.list[slot] = node;
+        if (wet) atomicAdd(&c.acc[0], 1ULL);
+        if (wet && !in) atomicAdd(&c.acc[1], 1ULL);
+        if (!wet) atomicAdd(&c.acc[2], 1ULL);
+    }
+}
+
+// the closure's viscosity from the network output (clamped to the range the
+// plain closure can give: snul .. 0.2, fv_mixing.F90:291-295)
+__device__ __forceinline__ real lc_snu(const Dev &d, const LcView &c, int node, int k) {
+    const float ls = c.Y[(size_t)node * c.OUT + k] * c.sd_y[k] + c.mu_y[k];
+    real s = (real)expf(ls);
+    if (!(s >= d.snul)) s = d.snul;
+    if (s > real(0.2)) s = real(0.2);
+    return s;
+}
+
+// Network columns: snu and Kv from the outputs, and bt from the closure's
+// own relation snu = scale_t sqrt(bt) + snul (fv_mixing.F90:280-295), so that
+// the plain closure, when it next runs on the column (fallback or judge),
+// starts from the turbulence energy that matches the viscosity in use.
+__global__ void k_lc_apply(Dev d, LcView c) {
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        if (!c.flag[node]) continue;
+        const int NS = d.NS;
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        real *bt = d.bt + (size_t)node * NS;
+        real *sn = d.snu + (size_t)node * NS;
+        real *kv = d.Kv + (size_t)node * NS;
+        for (int k = 0; k < NS; ++k) {
+            const real s = lc_snu(d, c, node, k);
+            const float lk = c.Y[(size_t)node * c.OUT + NS + k] * c.sd_y[NS + k] + c.mu_y[NS + k];
+            real K = (real)expf(lk);
+            const real klo = d.Pr_num * d.snul, khi = d.Pr_num * real(0.2);
+            if (!(K >= klo)) K = klo;
+            if (K > khi) K = khi;
+            const real zt = __ldg(d.sig + k) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = d.cka * Zh * Zd * Z0 / dmean;
+            real b = real(1.0e-8);
+            if (scale_t > real(0.0)) {
+                const real r = (s - d.snul) / scale_t;
+                b = dmax(r * r, real(1.0e-8));
+            }
+            bt[k] = b;
+            sn[k] = s;
+            kv[k] = K;
+        }
+    }
+}
+
+// training pairs: raw inputs and log snu / log Kv of wet columns, after the
+// plain closure has run on the step
+__global__ void k_lc_harvest(Dev d, LcView c) {
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        const bool wet = d.mask_wd_node[node] != real(0.0);
+        const unsigned long long slot = warp_append(wet, c.hcount);
+        if (!wet || slot >= (unsigned long long)c.hcap) continue;
+        lc_inputs(d, node, c.hx + slot * c.IN);
+        const int NS = d.NS;
+        float *y = c.hy + slot * c.OUT;
+        for (int k = 0; k < NS; ++k) {
+            y[k] = logf((float)d.snu[(size_t)node * NS + k]);
+            y[NS + k] = logf((float)d.Kv[(size_t)node * NS + k]);
+        }
+    }
+}
+
+// judge: the plain closure ran on every column; compare the network's
+// viscosity on the columns it would have taken (log difference)
+__global__ void k_lc_judge(Dev d, LcView c) {
+    double s2 = 0.0, n = 0.0, mx = 0.0;
+    GRID_LOOP(ii, d.N) {
+        const int node = (int)ii;
+        if (!c.flag[node]) continue;
+        for (int k = 0; k < d.NS; ++k) {
+            const double e = log((double)lc_snu(d, c, node, k)) - log((double)d.snu[(size_t)node * d.NS + k]);
+            s2 += e * e;
+            n += 1.0;
+            mx = fmax(mx, fabs(e));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+        n += __shfl_down_sync(0xffffffffu, n, o);
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0 && n > 0.0) {
+        atomicAdd(&c.judge[0], s2);
+        atomicAdd(&c.judge[1], n);
+        // max of non-negative doubles through their ordered bit patterns
+        atomicMax(reinterpret_cast<unsigned long long *>(&c.judge[2]), (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+void launch_lc_features(const Dev &d, const LcView &c, cudaStream_t s) {
+    k_lc_features<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
+}
+void launch_lc_apply(const Dev &d, const LcView &c, cudaStream_t s) {
+    k_lc_apply<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
+}
+void launch_lc_harvest(const Dev &d, const LcView &c, cudaStream_t s) {
+    k_lc_harvest<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
+}
+void launch_lc_judge(const Dev &d, const LcView &c, cudaStream_t s) {
+    k_lc_judge<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
+}
+
+FESOMC_PREC_END

@@ -41,13 +41,17 @@ __device__ __forceinline__ bool d3_above_tol(real a, real b) {
 //   * both sweeps load the next level's array values one level ahead, so
 //     that their latency overlaps the current level's division chain (3 %
 //     faster; unrolling by 4 instead was 9 % slower).
-template <int ARR>
-__global__ void k_d3end(Dev d) {
+//
+// kList: the columns are list[0 .. *count) instead of every node (the
+// columns the learned closure hands back to the plain one).
+template <int ARR, bool kList>
+__global__ void k_d3end(Dev d, const int *list, const unsigned long long *count) {
     const real t_inv = real(1.0) / d.dt;
     const real cka = d.cka;
     const real B1cka2 = real(16.6) * (cka * cka);
-    GRID_LOOP(ii, d.N) {
-        const int node = (int)ii;
+    const long long ncol = kList ? (long long)*count : (long long)d.N;
+    GRID_LOOP(ii, ncol) {
+        const int node = kList ? list[ii] : (int)ii;
         const int NS = d.NS, L = d.L;
         const real *bt = d.bt + (size_t)node * NS;
         const real *snu = d.snu + (size_t)node * NS;
@@ -197,10 +201,18 @@ __global__ void k_av(Dev d) {
 
 int config_d3end(const Dev &d) { return d.NS <= 127 ? 0 : 1; }
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.NS <= 11) k_d3end<12><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    else if (d.NS <= 21) k_d3end<22><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    else if (d.NS <= 40) k_d3end<41><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    else k_d3end<128><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    if (d.NS <= 11) k_d3end<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 21) k_d3end<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 40) k_d3end<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else k_d3end<128, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+}
+// the plain closure on the listed columns (count read on the device, so the
+// launch covers every node and the grid-stride loop stops at the count)
+void launch_d3end_list(const Dev &d, const int *list, const unsigned long long *count, cudaStream_t s) {
+    if (d.NS <= 11) k_d3end<12, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else if (d.NS <= 21) k_d3end<22, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else if (d.NS <= 40) k_d3end<41, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else k_d3end<128, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
 }
 void launch_av(const Dev &d, cudaStream_t s) { k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d); }
 

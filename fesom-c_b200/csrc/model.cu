@@ -9,9 +9,11 @@
 #include <string>
 #include <vector>
 
+#include "closure.h"
 #include "device_common.cuh"
 #include "fesomc_gpu.h"
 #include "forcing_dev.h"
+#include "mlp.h"
 
 namespace fesomc {
 // kernels (k_*.cu), compiled once per precision
@@ -56,6 +58,11 @@ namespace fesomc {
     void launch_miura(const Dev &, cudaStream_t); \
     void launch_muscl_h(const Dev &, cudaStream_t); \
     void launch_vdiff(const Dev &, cudaStream_t); \
+    void launch_d3end_list(const Dev &, const int *, const unsigned long long *, cudaStream_t); \
+    void launch_lc_features(const Dev &, const LcView &, cudaStream_t); \
+    void launch_lc_apply(const Dev &, const LcView &, cudaStream_t); \
+    void launch_lc_harvest(const Dev &, const LcView &, cudaStream_t); \
+    void launch_lc_judge(const Dev &, const LcView &, cudaStream_t); \
     int energy_parts(); \
     void launch_energy(const Dev &, double *, double *, cudaStream_t);
 namespace f64 {
@@ -136,6 +143,17 @@ struct fesomc_model {
     // time
     double time_jd = 0.0;
     int lfirst = 1;
+    // learned closure (fesomc_closure_attach / _harvest): the network in use,
+    // its per-column buffers, and what the coming step does with it
+    fesomc::LcNet *lc = nullptr;
+    fesomc::LcView lcv{};
+    float *lc_bufA = nullptr, *lc_bufB = nullptr;
+    bool lc_on = false;               // the network stands in for d3_end
+    bool lc_judge_now = false;        // this step: plain closure on every column, compared
+    bool lc_harvest_now = false;      // this step: plain closure, columns harvested
+    int lc_judge_every = 0;
+    long long lc_steps = 0, lc_judges = 0;
+    void *lc_owner = nullptr;         // fesomc_closure the per-column buffers were made for
     // graph
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;
@@ -772,8 +790,28 @@ int enqueue_step(fesomc_model *m, double ff) {
     n += 2;
     rec(m, "el2nodes", [&] { K3E2N(U_n, V_n, Unode, Vnode); });
     n += 1;
-    if (d.ver_mix == 3) {
+    if (d.ver_mix == 3 && m->lc_on) {
+        // learned closure: inputs, envelope test and fallback list; the
+        // network on every column; its viscosity where it applies and the
+        // plain closure on the listed columns, or (judge step) the plain
+        // closure everywhere, compared with the network
+        const LcView &c = m->lcv;
+        CK(cudaMemsetAsync(c.count, 0, sizeof(unsigned long long), s));
+        rec(m, "lc_features", [&] { K3(launch_lc_features, c, s); });
+        rec(m, "lc_infer", [&] { lc_forward_full(m->lc, c.X, d.N, c.Y, m->lc_bufA, m->lc_bufB, s); });
+        n += 5;
+        if (m->lc_judge_now) {
+            rec(m, "d3end", [&] { K3(launch_d3end, s); });
+            rec(m, "lc_judge", [&] { K3(launch_lc_judge, c, s); });
+        } else {
+            rec(m, "lc_apply", [&] { K3(launch_lc_apply, c, s); });
+            rec(m, "d3end_list", [&] { K3(launch_d3end_list, c.list, c.count, s); });
+        }
+        rec(m, "av", [&] { K3(launch_av, s); });
+        n += 3;
+    } else if (d.ver_mix == 3) {
         rec(m, "d3end", [&] { K3(launch_d3end, s); });
+        if (m->lc_harvest_now) { rec(m, "lc_harvest", [&] { K3(launch_lc_harvest, m->lcv, s); }); n += 1; }
         rec(m, "av", [&] { K3(launch_av, s); });
         n += 2;
     }
@@ -916,11 +954,21 @@ int run_steps(fesomc_model *m, int nsteps) {
         const double time = m->time_jd * 86400.0;
         int rc = m->dev_forcing ? FESOMC_OK : upload_step_inputs(m, time, m->time_jd);
         if (rc) return rc;
+        // learned closure: every lc_judge_every-th step is a judge step
+        if (m->lc_on) {
+            m->lc_steps += 1;
+            m->lc_judge_now = m->lc_judge_every > 0 && m->lc_steps % m->lc_judge_every == 0;
+            if (m->lc_judge_now) m->lc_judges += 1;
+        }
+        const bool eager = m->lc_judge_now || m->lc_harvest_now;
         if (m->lfirst) {
             // first call of compute_vel_rhs: AB2 factor 1 (fv_3D_vel.F90:124-128)
             rc = enqueue_step(m, 1.0);
             if (rc) return rc;
             m->lfirst = 0;
+        } else if (eager) {
+            rc = enqueue_step(m, 1.5 + m->p.epsilon);
+            if (rc) return rc;
         } else if (m->use_graph) {
             if (!m->graph) {
                 cudaGraph_t g;
@@ -1312,6 +1360,7 @@ int fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv) 
 
 int fesomc_gpu_finalize(fesomc_model *m) {
     if (!m) return FESOMC_OK;
+    if (m->lc && m->lc->stream == m->stream) m->lc->stream = nullptr;
     if (m->stream) cudaStreamSynchronize(m->stream);
     if (m->graph) cudaGraphExecDestroy(m->graph);
     for (cudaEvent_t e : m->prof.ev) cudaEventDestroy(e);
@@ -1468,6 +1517,195 @@ int fesomc_ensemble_run(fesomc_model *const *members, int32_t n, int32_t nsteps,
         if (first == FESOMC_OK) first = rc;
     }
     return first;
+}
+
+// ---- learned vertical-mixing closure ---------------------------------------
+struct fesomc_closure {
+    fesomc::LcNet *net = nullptr;
+};
+
+namespace {
+constexpr int kLcBatch = 8192;
+
+// the per-column buffers of model m for closure c (made once per pairing)
+int lc_model_buffers(fesomc_model *m, fesomc_closure *c) {
+    LcNet *n = c->net;
+    LcView &v = m->lcv;
+    const int W = std::max(n->IN, n->OUT);
+    v.NS = n->NS;
+    v.IN = n->IN;
+    v.OUT = n->OUT;
+    v.mu_x = n->stats;
+    v.sd_x = n->stats + W;
+    v.mu_y = n->stats + 2 * W;
+    v.sd_y = n->stats + 3 * W;
+    v.lo_x = n->stats + 4 * W;
+    v.hi_x = n->stats + 5 * W;
+    v.hx = n->hx;
+    v.hy = n->hy;
+    v.hcap = n->hcap;
+    v.hcount = n->hcount;
+    if (m->lc_owner == c) return FESOMC_OK;
+    const size_t N = m->d.N;
+    int rc;
+    if ((rc = dalloc(m, &v.X, N * n->IN)) || (rc = dalloc(m, &v.Y, N * n->OUT)) || (rc = dalloc(m, &v.flag, N)) ||
+        (rc = dalloc(m, &v.list, N)) || (rc = dalloc(m, &v.count, 1)) || (rc = dalloc(m, &v.acc, 4)) ||
+        (rc = dalloc(m, &v.judge, 3)) || (rc = dalloc(m, &m->lc_bufA, N * kLcHidden)) ||
+        (rc = dalloc(m, &m->lc_bufB, N * kLcHidden)))
+        return rc;
+    m->lc_owner = c;
+    return FESOMC_OK;
+}
+
+void drop_graph(fesomc_model *m) {
+    if (m->graph) {
+        cudaStreamSynchronize(m->stream);
+        cudaGraphExecDestroy(m->graph);
+        m->graph = nullptr;
+    }
+}
+}  // namespace
+
+int fesomc_closure_create(int32_t nsigma, int64_t capacity, uint64_t seed, fesomc_closure **out) {
+    if (!out || nsigma < 5 || nsigma > 32 || capacity < 0 || capacity >= (1LL << 31)) return FESOMC_EINVAL;
+    *out = nullptr;
+    fesomc_closure *c = new (std::nothrow) fesomc_closure();
+    if (!c) return FESOMC_ENOMEM;
+    int rc = 0;
+    c->net = lc_create(nsigma, capacity, seed, kLcBatch, nullptr, &rc);
+    if (!c->net) {
+        delete c;
+        return rc ? rc : FESOMC_ENOMEM;
+    }
+    *out = c;
+    return FESOMC_OK;
+}
+
+void fesomc_closure_free(fesomc_closure *c) {
+    if (!c) return;
+    cudaDeviceSynchronize();
+    lc_free(c->net);
+    delete c;
+}
+
+int fesomc_closure_info(const fesomc_closure *c, int64_t *harvested, int64_t *nparams, int32_t *n_in, int32_t *n_out) {
+    if (!c) return FESOMC_EINVAL;
+    unsigned long long h = 0;
+    CK(cudaMemcpy(&h, c->net->hcount, sizeof(h), cudaMemcpyDeviceToHost));
+    if (harvested) *harvested = (int64_t)std::min<unsigned long long>(h, (unsigned long long)c->net->hcap);
+    if (nparams) *nparams = c->net->np;
+    if (n_in) *n_in = c->net->IN;
+    if (n_out) *n_out = c->net->OUT;
+    return FESOMC_OK;
+}
+
+int fesomc_closure_harvest(fesomc_closure *c, fesomc_model *m, int32_t nsteps, int32_t every) {
+    if (!c || !m || nsteps < 0 || every < 1) return FESOMC_EINVAL;
+    if (c->net->NS != m->d.NS || m->lc_on || m->p.ver_mix != 3) return FESOMC_ESTATE;
+    int rc = lc_model_buffers(m, c);
+    if (rc) return rc;
+    for (int k = 0; k < nsteps; ++k) {
+        m->lc_harvest_now = (k + 1) % every == 0;
+        rc = run_steps(m, 1);
+        m->lc_harvest_now = false;
+        if (rc) return rc;
+    }
+    if ((rc = collect_status(m))) return rc;
+    return status_code(m->status_acc);
+}
+
+int fesomc_closure_fit(fesomc_closure *c) {
+    if (!c) return FESOMC_EINVAL;
+    return lc_fit_stats(c->net);
+}
+
+int fesomc_closure_train(fesomc_closure *c, int32_t epochs, int32_t batch, float lr, uint64_t seed, float *losses) {
+    if (!c || !(lr > 0.0f)) return FESOMC_EINVAL;
+    return lc_train(c->net, epochs, batch, lr, seed, losses);
+}
+
+int fesomc_closure_params(fesomc_closure *c, float *get, const float *set) {
+    if (!c) return FESOMC_EINVAL;
+    const size_t b = sizeof(float) * (size_t)c->net->np;
+    if (set) CK(cudaMemcpy(c->net->params, set, b, cudaMemcpyHostToDevice));
+    if (get) CK(cudaMemcpy(get, c->net->params, b, cudaMemcpyDeviceToHost));
+    return FESOMC_OK;
+}
+
+int fesomc_closure_norm(fesomc_closure *c, float *get, const float *set) {
+    if (!c) return FESOMC_EINVAL;
+    const size_t b = sizeof(float) * 6 * (size_t)std::max(c->net->IN, c->net->OUT);
+    if (set) CK(cudaMemcpy(c->net->stats, set, b, cudaMemcpyHostToDevice));
+    if (get) CK(cudaMemcpy(get, c->net->stats, b, cudaMemcpyDeviceToHost));
+    return FESOMC_OK;
+}
+
+int fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y) {
+    if (!c || !X || !Y || n < 1) return FESOMC_EINVAL;
+    LcNet *net = c->net;
+    float *dx = nullptr, *dy = nullptr;
+    if (cudaMalloc(&dx, sizeof(float) * n * net->IN) != cudaSuccess) return FESOMC_ENOMEM;
+    if (cudaMalloc(&dy, sizeof(float) * n * net->OUT) != cudaSuccess) { cudaFree(dx); return FESOMC_ENOMEM; }
+    int rc = FESOMC_OK;
+    if (cudaMemcpy(dx, X, sizeof(float) * n * net->IN, cudaMemcpyHostToDevice) != cudaSuccess) rc = FESOMC_ECUDA;
+    if (!rc) rc = lc_forward(net, dx, n, dy);
+    if (!rc && cudaMemcpy(Y, dy, sizeof(float) * n * net->OUT, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FESOMC_ECUDA;
+    cudaFree(dx);
+    cudaFree(dy);
+    return rc;
+}
+
+int fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32_t n, double *loss, float *grads) {
+    if (!c || !X || !T || !loss || n < 1 || n > c->net->Bmax) return FESOMC_EINVAL;
+    LcNet *net = c->net;
+    CK(cudaMemcpy(net->Xb, X, sizeof(float) * (size_t)n * net->IN, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(net->Tb, T, sizeof(float) * (size_t)n * net->OUT, cudaMemcpyHostToDevice));
+    int rc = lc_grad(net, net->Xb, net->Tb, n, loss);
+    if (rc) return rc;
+    if (grads) CK(cudaMemcpy(grads, net->grads, sizeof(float) * net->np, cudaMemcpyDeviceToHost));
+    return FESOMC_OK;
+}
+
+int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every) {
+    if (!m || judge_every < 0) return FESOMC_EINVAL;
+    drop_graph(m);
+    if (!c) {
+        m->lc_on = false;
+        m->lc = nullptr;
+        return FESOMC_OK;
+    }
+    if (c->net->NS != m->d.NS || m->p.ver_mix != 3) return FESOMC_EINVAL;
+    if (c->net->n_train < 1) return FESOMC_ESTATE;   // no statistics: fesomc_closure_fit first
+    int rc = lc_model_buffers(m, c);
+    if (rc) return rc;
+    CK(cudaMemset(m->lcv.acc, 0, 4 * sizeof(unsigned long long)));
+    CK(cudaMemset(m->lcv.judge, 0, 3 * sizeof(double)));
+    m->lc = c->net;
+    m->lc_on = true;
+    m->lc_judge_every = judge_every;
+    m->lc_steps = 0;
+    m->lc_judges = 0;
+    return FESOMC_OK;
+}
+
+int fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r) {
+    if (!m || !r) return FESOMC_EINVAL;
+    std::memset(r, 0, sizeof(*r));
+    r->steps = m->lc_steps;
+    r->judge_steps = m->lc_judges;
+    if (!m->lcv.acc) return FESOMC_OK;
+    unsigned long long acc[4];
+    double j[3];
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaMemcpy(acc, m->lcv.acc, sizeof(acc), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(j, m->lcv.judge, sizeof(j), cudaMemcpyDeviceToHost));
+    r->wet_columns = (int64_t)acc[0];
+    r->out_of_envelope = (int64_t)acc[1];
+    r->dry_columns = (int64_t)acc[2];
+    r->judge_values = (int64_t)j[1];
+    r->judge_rms_log = j[1] > 0 ? std::sqrt(j[0] / j[1]) : 0.0;
+    r->judge_max_log = j[2];
+    return FESOMC_OK;
 }
 
 int fesomc_gpu_set_device(int32_t device) {

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(ROOT_DIR, "libfesomc_gpu.so")
 
 i32p = C.POINTER(C.c_int32)
 f64p = C.POINTER(C.c_double)
+f32p = C.POINTER(C.c_float)
 
 FESOMC_OK = 0
 ERRORS = {1: "EINVAL", 2: "ENOMEM", 3: "ECUDA", 4: "ESTATE", 5: "ENEGSALT", 6: "ELOWTEMP",
@@ -80,6 +81,11 @@ class MeshOpts(C.Structure):
                 ("T_potential", C.c_int32), ("with_up_dn_tri", C.c_int32)]
 
 
+class ClosureReport(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("steps", "judge_steps", "wet_columns", "out_of_envelope", "dry_columns",
+                                         "judge_values")] + [("judge_rms_log", C.c_double), ("judge_max_log", C.c_double)]
+
+
 # Every symbol include/fesomc_gpu.h declares, with its ctypes signature.
 SIGNATURES = {
     "fesomc_gpu_init": (C.c_int, [C.POINTER(Mesh), C.POINTER(Params), C.POINTER(State), C.POINTER(C.c_void_p)]),
@@ -107,6 +113,18 @@ SIGNATURES = {
                                      C.POINTER(C.c_int64)]),
     "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),
     "fesomc_gpu_set_device": (C.c_int, [C.c_int32]),
+    "fesomc_closure_create": (C.c_int, [C.c_int32, C.c_int64, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "fesomc_closure_free": (None, [C.c_void_p]),
+    "fesomc_closure_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), i32p, i32p]),
+    "fesomc_closure_harvest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
+    "fesomc_closure_fit": (C.c_int, [C.c_void_p]),
+    "fesomc_closure_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_uint64, f32p]),
+    "fesomc_closure_params": (C.c_int, [C.c_void_p, f32p, f32p]),
+    "fesomc_closure_norm": (C.c_int, [C.c_void_p, f32p, f32p]),
+    "fesomc_closure_forward": (C.c_int, [C.c_void_p, f32p, C.c_int64, f32p]),
+    "fesomc_closure_grad": (C.c_int, [C.c_void_p, f32p, f32p, C.c_int32, f64p, f32p]),
+    "fesomc_closure_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "fesomc_closure_stats": (C.c_int, [C.c_void_p, C.POINTER(ClosureReport)]),
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),
     "fesomc_host_density_jm": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),
@@ -151,6 +169,14 @@ def dptr(a):
         return None
     assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(f64p)
+
+
+def fptr(a):
+    """float* to a C-contiguous float32 numpy array (or NULL)."""
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(f32p)
 
 
 def iptr(a):

@@ -18,7 +18,7 @@ CSRC = os.path.join(ROOT_DIR, "csrc")
 INC = os.path.join(REPO_DIR, "include")
 OBJ_DIR = os.path.join(ROOT_DIR, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-DUAL_PRECISION = ("k_baroclinic.cu", "k_barotropic.cu", "k_tracer.cu", "k_mixing.cu")
+DUAL_PRECISION = ("k_baroclinic.cu", "k_barotropic.cu", "k_tracer.cu", "k_mixing.cu", "k_closure.cu")
 
 
 def _nvcc():

@@ -1,0 +1,108 @@
+"""Host driver of the learned vertical-mixing closure (fesomc_closure_* in
+include/fesomc_gpu.h): harvest columns from the plain closure d3_end
+(src/fv_mixing.F90:73-347) while a model steps, fit the normalisation and the
+training envelope, train on the GPU, and attach the network to a model's
+time step.  No counterpart in the reference."""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class Closure:
+    """One network (and its training set) for meshes with nsigma levels."""
+
+    def __init__(self, nsigma, capacity=0, seed=20261204):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        abi.check(self.lib.fesomc_closure_create(nsigma, int(capacity), seed, C.byref(h)), "fesomc_closure_create")
+        self.h = h
+        n_in, n_out = C.c_int32(), C.c_int32()
+        np_ = C.c_int64()
+        abi.check(self.lib.fesomc_closure_info(h, None, C.byref(np_), C.byref(n_in), C.byref(n_out)))
+        self.nsigma, self.n_in, self.n_out, self.nparams = nsigma, n_in.value, n_out.value, np_.value
+
+    def harvested(self):
+        n = C.c_int64()
+        abi.check(self.lib.fesomc_closure_info(self.h, C.byref(n), None, None, None))
+        return n.value
+
+    def harvest(self, model, nsteps, every=1):
+        """Advance model (a fesomc.model.GpuModel, forcing as last set) by
+        nsteps with the plain closure, harvesting every 'every'-th step."""
+        rc = self.lib.fesomc_closure_harvest(self.h, model.h, nsteps, every)
+        for _ in range(nsteps):
+            model.time_jd += model.case.params.dt / 86400.0
+        model.nstep += nsteps
+        abi.check(rc, "fesomc_closure_harvest")
+
+    def fit(self):
+        abi.check(self.lib.fesomc_closure_fit(self.h), "fesomc_closure_fit")
+
+    def train(self, epochs, batch=4096, lr=1e-3, seed=1):
+        losses = np.zeros(max(epochs, 1), dtype=np.float32)
+        abi.check(self.lib.fesomc_closure_train(self.h, epochs, batch, lr, seed, abi.fptr(losses)),
+                  "fesomc_closure_train")
+        return losses[:epochs]
+
+    def params(self, value=None):
+        if value is not None:
+            v = np.ascontiguousarray(value, dtype=np.float32)
+            assert v.size == self.nparams
+            abi.check(self.lib.fesomc_closure_params(self.h, None, abi.fptr(v)))
+            return v
+        out = np.empty(self.nparams, dtype=np.float32)
+        abi.check(self.lib.fesomc_closure_params(self.h, abi.fptr(out), None))
+        return out
+
+    def norm(self, value=None):
+        w = max(self.n_in, self.n_out)
+        if value is not None:
+            v = np.ascontiguousarray(value, dtype=np.float32).reshape(-1)
+            assert v.size == 6 * w
+            abi.check(self.lib.fesomc_closure_norm(self.h, None, abi.fptr(v)))
+            return v.reshape(6, w)
+        out = np.empty(6 * w, dtype=np.float32)
+        abi.check(self.lib.fesomc_closure_norm(self.h, abi.fptr(out), None))
+        return out.reshape(6, w)
+
+    def forward(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.empty((X.shape[0], self.n_out), dtype=np.float32)
+        abi.check(self.lib.fesomc_closure_forward(self.h, abi.fptr(X), X.shape[0], abi.fptr(Y)),
+                  "fesomc_closure_forward")
+        return Y
+
+    def grad(self, X, T):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        T = np.ascontiguousarray(T, dtype=np.float32)
+        g = np.empty(self.nparams, dtype=np.float32)
+        loss = C.c_double()
+        abi.check(self.lib.fesomc_closure_grad(self.h, abi.fptr(X), abi.fptr(T), X.shape[0], C.byref(loss),
+                                               abi.fptr(g)), "fesomc_closure_grad")
+        return loss.value, g
+
+    def attach(self, model, judge_every=0):
+        abi.check(self.lib.fesomc_closure_attach(model.h, self.h, judge_every), "fesomc_closure_attach")
+
+    @staticmethod
+    def detach(model):
+        abi.check(abi.load().fesomc_closure_attach(model.h, None, 0), "fesomc_closure_attach")
+
+    @staticmethod
+    def stats(model):
+        r = abi.ClosureReport()
+        abi.check(abi.load().fesomc_closure_stats(model.h, C.byref(r)), "fesomc_closure_stats")
+        return {k: getattr(r, k) for k, _ in abi.ClosureReport._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fesomc_closure_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

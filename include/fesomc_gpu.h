@@ -400,6 +400,64 @@ int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const doub
                           const double *w_cv, const double *U_n_2D, const double *elem_area,
                           void *stream, double *eout);
 
+/* ---- learned vertical-mixing closure ----------------------------------------
+ * No counterpart in the reference.  A per-column network stands in for the
+ * turbulence closure d3_end (src/fv_mixing.F90:73-347): inputs per node
+ * column are, at the nsigma interfaces, the squared shear, the buoyancy
+ * frequency squared and the interface depth, plus the surface TKE flux term,
+ * the bottom TKE value and the total depth (3*nsigma + 3 values; shear, N^2
+ * and the boundary terms through asinh(x/1e-6), then normalised by the
+ * training set); three hidden layers of 256 with SiLU; outputs log snu and
+ * log Kv at the interfaces (2*nsigma, normalised).  It is trained on the
+ * GPU, on columns harvested from the plain closure, by FP32 forward /
+ * backward / Adam kernels.  In the time step (fesomc_closure_attach) a wet
+ * column whose inputs lie inside the training envelope takes the network's
+ * snu and Kv, and bt from the closure's own relation snu = scale_t sqrt(bt)
+ * + snul; dry columns and columns outside the envelope take the plain
+ * closure; every judge_every-th step the plain closure runs on all columns
+ * and the network's viscosity is compared with it.
+ *
+ * _create: nsigma 5..32, room for 'capacity' harvested columns.
+ * _harvest: advances the model nsteps internal steps (forcing as last set,
+ *   like fesomc_gpu_run) with the plain closure, appending the wet columns of
+ *   every 'every'-th step to the training set.
+ * _fit: normalisation and envelope (per-input min / max) of the training set.
+ * _train: epochs of Adam over the training set in minibatches of 'batch'
+ *   (<= 8192); losses (may be NULL) receives the mean loss per epoch.
+ * _params / _norm: copy the parameters (W1 b1 W2 b2 W3 b3 W4 b4, W row-major
+ *   out x in) / the statistics (6 arrays of max(in, out) floats: input mean,
+ *   input sd, output mean, output sd, envelope low, envelope high of the
+ *   normalised inputs) out of (get) and into (set) the closure.
+ * _forward / _grad: the network on host arrays of normalised inputs (tests);
+ *   _grad takes n <= 8192 samples and returns the mean squared error and its
+ *   gradient in the parameter layout.
+ * _attach: the model's steps use the closure (NULL: the plain closure
+ *   again); judge_every 0 never judges.  _stats: counts since attach.     */
+typedef struct fesomc_closure fesomc_closure;
+typedef struct fesomc_closure_report {
+    int64_t steps, judge_steps;       /* steps since attach, of which judge steps */
+    int64_t wet_columns;              /* wet column-steps seen                   */
+    int64_t out_of_envelope;          /* wet column-steps given to the plain closure */
+    int64_t dry_columns;              /* dry column-steps (plain closure)        */
+    int64_t judge_values;             /* interface values compared by the judge  */
+    double judge_rms_log, judge_max_log; /* network vs plain closure, log snu   */
+} fesomc_closure_report;
+int  fesomc_closure_create(int32_t nsigma, int64_t capacity, uint64_t seed, fesomc_closure **out);
+void fesomc_closure_free(fesomc_closure *c);
+int  fesomc_closure_info(const fesomc_closure *c, int64_t *harvested, int64_t *nparams, int32_t *n_in,
+                         int32_t *n_out);
+int  fesomc_closure_harvest(fesomc_closure *c, fesomc_model *m, int32_t nsteps, int32_t every);
+int  fesomc_closure_fit(fesomc_closure *c);
+int  fesomc_closure_train(fesomc_closure *c, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                          float *losses);
+int  fesomc_closure_params(fesomc_closure *c, float *get, const float *set);
+int  fesomc_closure_norm(fesomc_closure *c, float *get, const float *set);
+int  fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y);
+int  fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32_t n, double *loss,
+                         float *grads);
+int  fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every);
+int  fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r);
+
 /* ---- version / introspection --------------------------------------------- */
 const char *fesomc_gpu_version(void);
 /* Number of kernels launched by this instance since init. */

@@ -72,6 +72,17 @@ def load(abi):
         lib.oracle_mesh_set_sponge.argtypes = [C.c_void_p, C.c_double]
         lib.oracle_mesh_free.restype = None
         lib.oracle_mesh_free.argtypes = [C.c_void_p]
+        f32p = C.POINTER(C.c_float)
+        lib.oracle_mlp_nparams.restype = C.c_int64
+        lib.oracle_mlp_nparams.argtypes = [C.c_int]
+        lib.oracle_mlp_forward.restype = C.c_int
+        lib.oracle_mlp_forward.argtypes = [C.c_int, f32p, f32p, C.c_int, f32p]
+        lib.oracle_mlp_grad.restype = C.c_int
+        lib.oracle_mlp_grad.argtypes = [C.c_int, f32p, f32p, f32p, C.c_int, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double)]
+        lib.oracle_mlp_adam.restype = None
+        lib.oracle_mlp_adam.argtypes = [C.c_int64, f32p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.c_int, C.c_double]
         _lib = lib
     return _lib
 
@@ -147,3 +158,35 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def mlp_nparams(abi, nsigma):
+    return load(abi).oracle_mlp_nparams(nsigma)
+
+
+def mlp_forward(abi, nsigma, params, X):
+    """The closure network on the CPU (double accumulation): Y = net(X)."""
+    lib = load(abi)
+    p, X = _f32(params), _f32(X)
+    Y = np.empty((X.shape[0], 2 * nsigma), dtype=np.float32)
+    f = C.POINTER(C.c_float)
+    if lib.oracle_mlp_forward(nsigma, p.ctypes.data_as(f), X.ctypes.data_as(f), X.shape[0], Y.ctypes.data_as(f)):
+        raise RuntimeError("oracle_mlp_forward failed")
+    return Y
+
+
+def mlp_grad(abi, nsigma, params, X, T):
+    """Mean squared error of the closure network and its exact gradient."""
+    lib = load(abi)
+    p, X, T = _f32(params), _f32(X), _f32(T)
+    g = np.empty(p.size, dtype=np.float64)
+    loss = C.c_double()
+    f = C.POINTER(C.c_float)
+    if lib.oracle_mlp_grad(nsigma, p.ctypes.data_as(f), X.ctypes.data_as(f), T.ctypes.data_as(f), X.shape[0],
+                           C.byref(loss), g.ctypes.data_as(C.POINTER(C.c_double))):
+        raise RuntimeError("oracle_mlp_grad failed")
+    return loss.value, g
