@@ -417,6 +417,7 @@ int lc_train(LcNet *n, int epochs, int B, float lr, unsigned long long seed, flo
     const float *mu_x = n->stats, *sd_x = n->stats + W, *mu_y = n->stats + 2 * W, *sd_y = n->stats + 3 * W;
     std::mt19937_64 rng(seed);
     const long long nb = (long long)(cnt / B);
+    n->tc_ready = false;   // the BF16 copies no longer match
     for (int ep = 0; ep < epochs; ++ep) {
         unsigned long long a;
         do { a = (rng() % cnt) | 1ULL; } while (std::gcd(a, cnt) != 1ULL);

@@ -2,6 +2,7 @@
 // training state on the device and the functions model.cu builds the C-ABI
 // entry points from.  No counterpart in the reference.
 #pragma once
+#include <cstdint>
 #include <vector>
 
 #include "closure.h"
@@ -33,6 +34,11 @@ struct LcNet {
     float *hx = nullptr, *hy = nullptr;
     long long hcap = 0;
     unsigned long long *hcount = nullptr;
+    // BF16 weights for the tensor-core kernel (chunk-major operand layout),
+    // valid after lc_tc_prepare until the parameters change
+    uint16_t *wtc = nullptr;
+    unsigned int *tc_err = nullptr;
+    bool tc_ready = false;
     cudaStream_t stream = nullptr;
     std::vector<void *> allocs;
 };
@@ -50,5 +56,10 @@ int lc_grad(LcNet *n, const float *X, const float *T, int B, double *loss);
 int lc_fit_stats(LcNet *n);
 // epochs of Adam over the harvested set in minibatches of B; mean loss per epoch
 int lc_train(LcNet *n, int epochs, int B, float lr, unsigned long long seed, float *losses);
+// BF16 tensor-core inference (k_mlp_tc.cu): whether the network's size fits
+// the kernel, the BF16 weight copies, and Y = network(X) on stream s
+bool lc_tc_supported(const LcNet *n);
+int lc_tc_prepare(LcNet *n);
+int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStream_t s);
 
 }  // namespace fesomc

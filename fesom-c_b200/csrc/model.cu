@@ -149,6 +149,7 @@ struct fesomc_model {
     fesomc::LcView lcv{};
     float *lc_bufA = nullptr, *lc_bufB = nullptr;
     bool lc_on = false;               // the network stands in for d3_end
+    bool lc_bf16 = false;             // inference on the tensor cores (BF16) instead of FP32
     bool lc_judge_now = false;        // this step: plain closure on every column, compared
     bool lc_harvest_now = false;      // this step: plain closure, columns harvested
     int lc_judge_every = 0;
@@ -798,7 +799,8 @@ int enqueue_step(fesomc_model *m, double ff) {
         const LcView &c = m->lcv;
         CK(cudaMemsetAsync(c.count, 0, sizeof(unsigned long long), s));
         rec(m, "lc_features", [&] { K3(launch_lc_features, c, s); });
-        rec(m, "lc_infer", [&] { lc_forward_full(m->lc, c.X, d.N, c.Y, m->lc_bufA, m->lc_bufB, s); });
+        if (m->lc_bf16) rec(m, "lc_infer_tc", [&] { lc_forward_tc(m->lc, c.X, d.N, c.Y, s); });
+        else rec(m, "lc_infer", [&] { lc_forward_full(m->lc, c.X, d.N, c.Y, m->lc_bufA, m->lc_bufB, s); });
         n += 5;
         if (m->lc_judge_now) {
             rec(m, "d3end", [&] { K3(launch_d3end, s); });
@@ -1550,10 +1552,18 @@ int lc_model_buffers(fesomc_model *m, fesomc_closure *c) {
     int rc;
     if ((rc = dalloc(m, &v.X, N * n->IN)) || (rc = dalloc(m, &v.Y, N * n->OUT)) || (rc = dalloc(m, &v.flag, N)) ||
         (rc = dalloc(m, &v.list, N)) || (rc = dalloc(m, &v.count, 1)) || (rc = dalloc(m, &v.acc, 4)) ||
-        (rc = dalloc(m, &v.judge, 3)) || (rc = dalloc(m, &m->lc_bufA, N * kLcHidden)) ||
-        (rc = dalloc(m, &m->lc_bufB, N * kLcHidden)))
+        (rc = dalloc(m, &v.judge, 3)))
         return rc;
+    m->lc_bufA = m->lc_bufB = nullptr;   // FP32 inference activations: made when first needed
     m->lc_owner = c;
+    return FESOMC_OK;
+}
+
+int lc_fp32_buffers(fesomc_model *m) {
+    if (m->lc_bufA) return FESOMC_OK;
+    const size_t N = m->d.N;
+    int rc;
+    if ((rc = dalloc(m, &m->lc_bufA, N * kLcHidden)) || (rc = dalloc(m, &m->lc_bufB, N * kLcHidden))) return rc;
     return FESOMC_OK;
 }
 
@@ -1640,15 +1650,25 @@ int fesomc_closure_norm(fesomc_closure *c, float *get, const float *set) {
     return FESOMC_OK;
 }
 
-int fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y) {
+int fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y, int32_t bf16) {
     if (!c || !X || !Y || n < 1) return FESOMC_EINVAL;
     LcNet *net = c->net;
+    if (bf16 && !lc_tc_supported(net)) return FESOMC_EINVAL;
+    if (bf16 && !net->tc_ready) {
+        int rc = lc_tc_prepare(net);
+        if (rc) return rc;
+    }
     float *dx = nullptr, *dy = nullptr;
     if (cudaMalloc(&dx, sizeof(float) * n * net->IN) != cudaSuccess) return FESOMC_ENOMEM;
     if (cudaMalloc(&dy, sizeof(float) * n * net->OUT) != cudaSuccess) { cudaFree(dx); return FESOMC_ENOMEM; }
     int rc = FESOMC_OK;
     if (cudaMemcpy(dx, X, sizeof(float) * n * net->IN, cudaMemcpyHostToDevice) != cudaSuccess) rc = FESOMC_ECUDA;
-    if (!rc) rc = lc_forward(net, dx, n, dy);
+    if (!rc) rc = bf16 ? lc_forward_tc(net, dx, n, dy, nullptr) : lc_forward(net, dx, n, dy);
+    if (!rc && bf16) {
+        unsigned int err = 0;
+        if (cudaMemcpy(&err, net->tc_err, sizeof(err), cudaMemcpyDeviceToHost) != cudaSuccess) rc = FESOMC_ECUDA;
+        else if (err) rc = FESOMC_ECUDA;
+    }
     if (!rc && cudaMemcpy(Y, dy, sizeof(float) * n * net->OUT, cudaMemcpyDeviceToHost) != cudaSuccess) rc = FESOMC_ECUDA;
     cudaFree(dx);
     cudaFree(dy);
@@ -1666,7 +1686,7 @@ int fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32
     return FESOMC_OK;
 }
 
-int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every) {
+int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every, int32_t bf16) {
     if (!m || judge_every < 0) return FESOMC_EINVAL;
     drop_graph(m);
     if (!c) {
@@ -1676,8 +1696,12 @@ int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_ever
     }
     if (c->net->NS != m->d.NS || m->p.ver_mix != 3) return FESOMC_EINVAL;
     if (c->net->n_train < 1) return FESOMC_ESTATE;   // no statistics: fesomc_closure_fit first
+    if (bf16 && !lc_tc_supported(c->net)) return FESOMC_EINVAL;
     int rc = lc_model_buffers(m, c);
     if (rc) return rc;
+    if (bf16 && (rc = lc_tc_prepare(c->net))) return rc;
+    if (!bf16 && (rc = lc_fp32_buffers(m))) return rc;
+    m->lc_bf16 = bf16 != 0;
     CK(cudaMemset(m->lcv.acc, 0, 4 * sizeof(unsigned long long)));
     CK(cudaMemset(m->lcv.judge, 0, 3 * sizeof(double)));
     m->lc = c->net;

@@ -121,9 +121,9 @@ SIGNATURES = {
     "fesomc_closure_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_uint64, f32p]),
     "fesomc_closure_params": (C.c_int, [C.c_void_p, f32p, f32p]),
     "fesomc_closure_norm": (C.c_int, [C.c_void_p, f32p, f32p]),
-    "fesomc_closure_forward": (C.c_int, [C.c_void_p, f32p, C.c_int64, f32p]),
+    "fesomc_closure_forward": (C.c_int, [C.c_void_p, f32p, C.c_int64, f32p, C.c_int32]),
     "fesomc_closure_grad": (C.c_int, [C.c_void_p, f32p, f32p, C.c_int32, f64p, f32p]),
-    "fesomc_closure_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "fesomc_closure_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "fesomc_closure_stats": (C.c_int, [C.c_void_p, C.POINTER(ClosureReport)]),
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),

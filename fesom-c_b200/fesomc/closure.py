@@ -67,10 +67,11 @@ class Closure:
         abi.check(self.lib.fesomc_closure_norm(self.h, abi.fptr(out), None))
         return out.reshape(6, w)
 
-    def forward(self, X):
+    def forward(self, X, bf16=False):
+        """The network on normalised inputs; bf16: on the tensor cores."""
         X = np.ascontiguousarray(X, dtype=np.float32)
         Y = np.empty((X.shape[0], self.n_out), dtype=np.float32)
-        abi.check(self.lib.fesomc_closure_forward(self.h, abi.fptr(X), X.shape[0], abi.fptr(Y)),
+        abi.check(self.lib.fesomc_closure_forward(self.h, abi.fptr(X), X.shape[0], abi.fptr(Y), int(bf16)),
                   "fesomc_closure_forward")
         return Y
 
@@ -83,12 +84,15 @@ class Closure:
                                                abi.fptr(g)), "fesomc_closure_grad")
         return loss.value, g
 
-    def attach(self, model, judge_every=0):
-        abi.check(self.lib.fesomc_closure_attach(model.h, self.h, judge_every), "fesomc_closure_attach")
+    def attach(self, model, judge_every=0, bf16=True):
+        """The model's steps use this network (inference on the tensor cores
+        unless bf16 is False); every judge_every-th step runs the plain
+        closure and compares."""
+        abi.check(self.lib.fesomc_closure_attach(model.h, self.h, judge_every, int(bf16)), "fesomc_closure_attach")
 
     @staticmethod
     def detach(model):
-        abi.check(abi.load().fesomc_closure_attach(model.h, None, 0), "fesomc_closure_attach")
+        abi.check(abi.load().fesomc_closure_attach(model.h, None, 0, 0), "fesomc_closure_attach")
 
     @staticmethod
     def stats(model):

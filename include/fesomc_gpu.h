@@ -428,11 +428,14 @@ int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const doub
  *   out x in) / the statistics (6 arrays of max(in, out) floats: input mean,
  *   input sd, output mean, output sd, envelope low, envelope high of the
  *   normalised inputs) out of (get) and into (set) the closure.
- * _forward / _grad: the network on host arrays of normalised inputs (tests);
+ * _forward / _grad: the network on host arrays of normalised inputs (tests),
+ *   _forward with bf16 = 1 on the tensor cores (BF16 weights and
+ *   activations, FP32 accumulation; nsigma <= 25), else in FP32;
  *   _grad takes n <= 8192 samples and returns the mean squared error and its
  *   gradient in the parameter layout.
  * _attach: the model's steps use the closure (NULL: the plain closure
- *   again); judge_every 0 never judges.  _stats: counts since attach.     */
+ *   again), its inference on the tensor cores when bf16 = 1 (else FP32);
+ *   judge_every 0 never judges.  _stats: counts since attach.             */
 typedef struct fesomc_closure fesomc_closure;
 typedef struct fesomc_closure_report {
     int64_t steps, judge_steps;       /* steps since attach, of which judge steps */
@@ -452,10 +455,10 @@ int  fesomc_closure_train(fesomc_closure *c, int32_t epochs, int32_t batch, floa
                           float *losses);
 int  fesomc_closure_params(fesomc_closure *c, float *get, const float *set);
 int  fesomc_closure_norm(fesomc_closure *c, float *get, const float *set);
-int  fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y);
+int  fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float *Y, int32_t bf16);
 int  fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32_t n, double *loss,
                          float *grads);
-int  fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every);
+int  fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every, int32_t bf16);
 int  fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r);
 
 /* ---- version / introspection --------------------------------------------- */

@@ -52,6 +52,54 @@ def test_gradients_match_oracle(mods, nsigma, batch):
         c.close()
 
 
+def _bf16(a):
+    """Round float32 values to bfloat16 (nearest even), returned as float32."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32)
+
+
+def _net_bf16_reference(p, X, n_in, n_out):
+    """The network with BF16 inputs, weights and hidden activations and FP32
+    (here float64) accumulation, as the tensor-core kernel computes it."""
+    dims = [n_in, 256, 256, 256, n_out]
+    o, a = 0, _bf16(X).astype(np.float64)
+    for l in range(4):
+        W = _bf16(p[o:o + dims[l + 1] * dims[l]]).reshape(dims[l + 1], dims[l]).astype(np.float64)
+        o += dims[l + 1] * dims[l]
+        b = p[o:o + dims[l + 1]].astype(np.float64)
+        o += dims[l + 1]
+        z = a @ W.T + b
+        a = _bf16((z / (1.0 + np.exp(-z))).astype(np.float32)).astype(np.float64) if l < 3 else z
+    return a
+
+
+@pytest.mark.parametrize("nsigma,ncol", [(21, 1000), (11, 300), (21, 5)])
+def test_tensor_core_inference(mods, nsigma, ncol):
+    """The BF16 tensor-core kernel (tcgen05.mma, TMEM accumulators) against
+    the same network with the same BF16 roundings on the CPU (relative 2e-3:
+    FP32 accumulation order and the SiLU's exp), and against the FP32
+    network (relative 3e-2, the BF16 rounding itself); partial last tiles
+    included."""
+    abi, cases, closure, model, pyoracle = mods
+    c = closure.Closure(nsigma)
+    try:
+        p = _rand(c.nparams, 7, 0.06)
+        c.params(p)
+        X = _rand((ncol, c.n_in), 8)
+        Yt = c.forward(X, bf16=True).astype(np.float64)
+        Yb = _net_bf16_reference(p, X, c.n_in, c.n_out)
+        Yf = pyoracle.mlp_forward(abi, nsigma, p, X).astype(np.float64)
+        scale = np.max(np.abs(Yf))
+        assert np.max(np.abs(Yt - Yb)) <= 2e-3 * scale
+        assert np.max(np.abs(Yt - Yf)) <= 3e-2 * scale
+        # repeatable, and agrees with the FP32 GPU kernels to the BF16 level
+        assert np.array_equal(Yt, c.forward(X, bf16=True).astype(np.float64))
+        assert np.max(np.abs(Yt - c.forward(X).astype(np.float64))) <= 3e-2 * scale
+    finally:
+        c.close()
+
+
 def _harvested(mods, steps=40, every=4, **kw):
     abi, cases, closure, model, pyoracle = mods
     case = cases.estuary("small", **kw)
