@@ -524,6 +524,125 @@ def run_ensemble(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def stress_forcing(case, tau, theta):
+    """Uniform stress tau (N/m2) towards angle theta and the 10 m wind that
+    carries it (rho_air 1.3, C_D 1.3e-3), as the estuary cases set them."""
+    import math
+    import numpy as np
+    m = case.mesh
+    w = math.sqrt(tau / (1.3 * 1.3e-3)) if tau > 0 else 0.0
+    return {"taux": np.full(m.E, tau * math.cos(theta)), "tauy": np.full(m.E, tau * math.sin(theta)),
+            "windx": np.full(m.N, w * math.cos(theta)), "windy": np.full(m.N, w * math.sin(theta))}
+
+
+def mixed_layer_depth(case, state, dT=0.2):
+    """Depth (m) where temperature first differs from the top layer by dT
+    (temperature criterion), per wet node; the column depth if nowhere."""
+    import numpy as np
+    m = case.mesh
+    L = m.L
+    H = np.maximum(m.depth + state["eta_n"], case.params.Dmin)
+    zmid = 0.5 * ((1.0 - m.sigma[:-1]) + (1.0 - m.sigma[1:]))
+    T = state["TF"].reshape(-1, L)
+    off = np.abs(T - T[:, :1]) > dT
+    first = np.where(off.any(axis=1), off.argmax(axis=1), L - 1)
+    return zmid[first] * H
+
+
+def run_closure(args):
+    """Learned closure on the cfg1 mesh (cfg4): columns harvested from the
+    plain closure under seeded forcing draws (stress 0-0.3 N/m2 in a random
+    direction, surface heat flux -200..+100 W/m2), trained on the GPU, then
+    one tidal day of cfg4 forcing (0.15 N/m2, -100 W/m2) with the FP32 form +
+    learned closure against the plain FP64 path.  One JSON line: training,
+    fallback rate, judge error, mixed-layer depth, SSH / T / S errors and time
+    per simulated tidal day of both."""
+    import math
+    import numpy as np
+    from fesomc import abi, build, cases, closure, model
+    if not os.path.exists(abi.LIB_PATH):
+        build.build_library()
+    lib = abi.load()
+    rng = np.random.default_rng(20261204)
+    heat = {"qns": -100.0, "qsr": 0.0, "emp": 0.0}
+    case = cases.estuary(args.config, atm=heat)
+    m = case.mesh
+    base = np.ascontiguousarray(case.forcing_fn(1, case.params.time_jd0 + 20.0)["runoff_rivers"], dtype=np.float64)
+
+    def new_model(fp32, forcing):
+        case.params.fp32_form = 1 if fp32 else 0
+        g = model.GpuModel(case)
+        f = case.forcing_fn(1, cases.advance_time(g.time_jd, case.params.dt))
+        f.update(forcing)
+        g.set_forcing(f)
+        abi.check(lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base), 1), "fesomc_gpu_set_device_forcing")
+        return g
+
+    c = closure.Closure(m.NS, capacity=args.lc_capacity)
+    t0 = time.perf_counter()
+    draws = []
+    for k in range(args.lc_draws):
+        tau, th, qns = rng.uniform(0.0, 0.3), rng.uniform(0.0, 2 * math.pi), rng.uniform(-200.0, 100.0)
+        draws.append({"tau": tau, "theta": th, "qns": qns})
+        f = stress_forcing(case, tau, th)
+        f["qns"] = np.full(m.N, qns)
+        g = new_model(True, f)
+        c.harvest(g, args.lc_spinup, args.lc_spinup + 1)          # spin-up, nothing harvested
+        c.harvest(g, args.lc_harvest_steps, args.lc_every)
+        g.close()
+    harvest_s = time.perf_counter() - t0
+    c.fit()
+    t0 = time.perf_counter()
+    losses = c.train(args.lc_epochs, batch=8192, lr=args.lc_lr, seed=3)
+    train_s = time.perf_counter() - t0
+    steps = args.steps
+    cfg4 = stress_forcing(case, 0.15, 0.5 * math.pi)
+    runs = {}
+    for name, fp32, lc in (("plain_fp64", False, False), ("fp32_plain", True, False), ("fp32_learned", True, True)):
+        g = new_model(fp32, cfg4)
+        if lc:
+            c.attach(g, judge_every=args.lc_judge, bf16=True)
+        ms = C.c_double()
+        rc = lib.fesomc_gpu_time_run(g.h, steps, C.byref(ms))
+        st = g.state()
+        rep = closure.Closure.stats(g) if lc else None
+        g.close()
+        runs[name] = {"rc": rc, "ms_per_step": ms.value / steps, "state": st, "stats": rep}
+    ref = runs["plain_fp64"]["state"]
+    wet = ref["mask_wd_node"] > 0
+    wetn = np.repeat(wet, m.L)
+    mld_ref = mixed_layer_depth(case, ref)
+
+    def errors(s):
+        mld = mixed_layer_depth(case, s)
+        return {"ssh_rms_m": float(np.sqrt(np.mean((s["eta_n"][wet] - ref["eta_n"][wet]) ** 2))),
+                "T_rms_C": float(np.sqrt(np.mean((s["TF"][wetn] - ref["TF"][wetn]) ** 2))),
+                "T_max_C": float(np.max(np.abs(s["TF"][wetn] - ref["TF"][wetn]))),
+                "S_rms_psu": float(np.sqrt(np.mean((s["SF"][wetn] - ref["SF"][wetn]) ** 2))),
+                "S_max_psu": float(np.max(np.abs(s["SF"][wetn] - ref["SF"][wetn]))),
+                "mld_mean_m": float(np.mean(mld[wet])), "mld_rms_diff_m": float(np.sqrt(np.mean((mld[wet] - mld_ref[wet]) ** 2)))}
+
+    day = TIDAL_DAY_S / case.params.dt
+    out = {"metric": "learned closure (cfg4) vs plain FP64 per simulated tidal day", "config": workload_config(case, args.config),
+           "forcing": "cfg4: uniform cross-shore stress 0.15 N/m2, non-solar surface heat flux -100 W/m2, tide and ramped river on the GPU",
+           "training": {"draws": draws, "columns": c.harvested(), "harvest_s": harvest_s, "epochs": args.lc_epochs,
+                        "train_s": train_s, "loss_per_epoch": [float(x) for x in losses], "parameters": c.nparams},
+           "steps": steps, "simulated_s": steps * case.params.dt, "mld_mean_plain_m": float(np.mean(mld_ref[wet]))}
+    for name, r in runs.items():
+        e = {"rc": r["rc"], "ms_per_step": r["ms_per_step"], "s_per_tidal_day": r["ms_per_step"] * day / 1000.0}
+        if name != "plain_fp64":
+            e["errors_vs_plain_fp64"] = errors(r["state"])
+            e["speedup_vs_plain_fp64"] = runs["plain_fp64"]["ms_per_step"] / r["ms_per_step"]
+        if r["stats"]:
+            st = r["stats"]
+            e["closure"] = dict(st, fallback_rate=(st["out_of_envelope"] + st["dry_columns"]) /
+                                max(1, st["wet_columns"] + st["dry_columns"]),
+                                envelope_fallback_rate=st["out_of_envelope"] / max(1, st["wet_columns"]))
+        out[name] = e
+    c.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -539,8 +658,21 @@ def main():
                     help="time the FP32 form against the plain FP64 path and report their differences")
     ap.add_argument("--fp32-form", action="store_true",
                     help="run the FP32 form (level fields and 3D arithmetic in FP32, 2D sub-cycle in FP64)")
+    ap.add_argument("--closure", action="store_true",
+                    help="learned closure report (cfg4): harvest, train, one tidal day against plain FP64")
+    ap.add_argument("--lc-draws", type=int, default=6)
+    ap.add_argument("--lc-spinup", type=int, default=90)
+    ap.add_argument("--lc-harvest-steps", type=int, default=60)
+    ap.add_argument("--lc-every", type=int, default=20)
+    ap.add_argument("--lc-capacity", type=int, default=20_000_000)
+    ap.add_argument("--lc-epochs", type=int, default=4)
+    ap.add_argument("--lc-lr", type=float, default=1e-3)
+    ap.add_argument("--lc-judge", type=int, default=100)
     args = ap.parse_args()
     ws, rank, local = dist_info()
+    if args.closure:
+        run_closure(args)
+        return
     if args.compare_forms:
         run_compare_forms(args)
         return

@@ -62,7 +62,9 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
         const real *S = d.SF + (size_t)node * L;
         real *Ri = d.Ri + (size_t)node * NS;
         real *tke = d.tke_dissip + (size_t)node * NS;
-        real xx1[ARR], yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
+        // bA / bB alternate as btr and as xx1: the back substitution writes
+        // btr1(k) into the xx1(k) slot it has just read (seven arrays, not eight)
+        real yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
         const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
         const real dmean2 = dmean * dmean;
         const real ajac = jac_a(d, d.eta_jac, node);
@@ -103,15 +105,14 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
             const real snu_m = real(0.5) * (sn[NS] + sn[NS - 1]);
             y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
         }
-        xx1[2] = real(1.0);
-        yy1[2] = y2;
+        // xx1(2) = 1 and yy1(2) = y2 (the surface condition) are used as constants
         // bottom boundary value (independent of the iteration)
         const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
         const real lg = fesomc_log(delta_b / d.z0b_min);
         const real bott_R = B1cka2 / (lg * lg);
         const real ubt = Un[L - 1], vbt = Vn[L - 1];
         const real bot = bott_R * (ubt * ubt + vbt * vbt);
-        real *btr = bA, *btr1 = bB;
+        real *btr = bA, *xq = bB;   // xq: this iteration's xx1, then its btr1
         bool converged = false;
         for (int it = 1; it <= 200; ++it) {
             real x = real(1.0), y = y2;
@@ -138,7 +139,7 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
                 const real a = bm - am * x;
                 const real xn = cm / a;
                 const real yn = (am * y - fr) / a;
-                xx1[nz + 1] = xn;
+                xq[nz + 1] = xn;
                 yy1[nz + 1] = yn;
                 x = xn;
                 y = yn;
@@ -146,20 +147,21 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
                 s_mid = s_hi;
             }
             real b1v = bot;  // btr1(NS)
-            btr1[NS] = b1v;
+            real x_n = xq[NS], y_n = yy1[NS], o_n = btr[NS - 1];
+            xq[NS] = b1v;
             bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + real(1.0e-8));
-            real x_n = xx1[NS], y_n = yy1[NS], o_n = btr[NS - 1];
             for (int nz = NS; nz >= 2; --nz) {
                 const real xv = x_n, yv = y_n, ov = o_n;
-                if (nz - 1 >= 2) { x_n = xx1[nz - 1]; y_n = yy1[nz - 1]; o_n = btr[nz - 2]; }
-                b1v = b1v * xv + yv;  // btr1(nz-1)
-                btr1[nz - 1] = b1v;
+                if (nz - 1 >= 3) { x_n = xq[nz - 1]; y_n = yy1[nz - 1]; o_n = btr[nz - 2]; }
+                else if (nz - 1 == 2) { x_n = real(1.0); y_n = y2; o_n = btr[nz - 2]; }
+                b1v = b1v * xv + yv;  // btr1(nz-1), into the xx1(nz-1) slot already read
+                xq[nz - 1] = b1v;
                 above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
             }
             if (!above) { converged = true; break; }
             real *t = btr;
-            btr = btr1;
-            btr1 = t;
+            btr = xq;
+            xq = t;
         }
         if (converged) {
             for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (btr[nz] * btr[nz]) / sn[nz];

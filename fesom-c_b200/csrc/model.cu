@@ -2,6 +2,7 @@
 // gather lists in reference edge order), device state, the per-step launch
 // sequence of oce_timestep case(3) (src/fv_main.F90:1983-2095) and its
 // capture into one CUDA graph, forcing upload, state sync and diagnostics.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -155,6 +156,12 @@ struct fesomc_model {
     int lc_judge_every = 0;
     long long lc_steps = 0, lc_judges = 0;
     void *lc_owner = nullptr;         // fesomc_closure the per-column buffers were made for
+    // storage order (fesomc_params.sfc_order): device index -> reference
+    // index of nodes and elements, used by every transfer of a field
+    bool perm = false;
+    const int *d_nd_ref = nullptr, *d_el_ref = nullptr;
+    void *d_perm_buf = nullptr;       // staging of one field in reference order
+    size_t perm_buf_bytes = 0;
     // graph
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;
@@ -205,15 +212,67 @@ int upload(fesomc_model *m, const T **dst, const std::vector<T> &src) {
     return FESOMC_OK;
 }
 
+// Storage order: fields live on the device in the order of the model's
+// nodes / elements, which with fesomc_params.sfc_order is a Hilbert-curve
+// order of the mesh; callers always see the reference order.  A field of an
+// entity kind holds 'lev' consecutive values per entity.
+template <typename T>
+__global__ void k_perm_gather(const T *ref, T *dev, const int *ref_of, long long n_ent, int lev) {
+    const long long total = n_ent * lev;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long e = i / lev, k = i % lev;
+        dev[i] = ref[(size_t)ref_of[e] * lev + k];
+    }
+}
+template <typename T>
+__global__ void k_perm_scatter(const T *dev, T *ref, const int *ref_of, long long n_ent, int lev) {
+    const long long total = n_ent * lev;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long e = i / lev, k = i % lev;
+        ref[(size_t)ref_of[e] * lev + k] = dev[i];
+    }
+}
+
+enum { ENT_NODE = 0, ENT_ELEM = 1 };
+
+// the permutation of an entity kind and the values per entity of a field
+inline const int *perm_of(const fesomc_model *m, int ent) { return ent == ENT_NODE ? m->d_nd_ref : m->d_el_ref; }
+inline long long ents(const fesomc_model *m, int ent) { return ent == ENT_NODE ? m->d.N : m->d.E; }
+
+int perm_buf(fesomc_model *m, size_t bytes) {
+    if (m->perm_buf_bytes >= bytes) return FESOMC_OK;
+    unsigned char *q = nullptr;
+    int rc = dalloc(m, &q, bytes);
+    if (rc) return rc;
+    m->d_perm_buf = q;
+    m->perm_buf_bytes = bytes;
+    return FESOMC_OK;
+}
+
+// device field (device order) -> buffer in reference order, on stream s
+template <typename T>
+void unpermute_to(const fesomc_model *m, int ent, const T *dev, T *ref, size_t count, cudaStream_t s) {
+    const long long n = ents(m, ent);
+    const int lev = (int)(count / n);
+    k_perm_scatter<<<grid_for(count, 256), 256, 0, s>>>(dev, ref, perm_of(m, ent), n, lev);
+}
+template <typename T>
+void permute_from(const fesomc_model *m, int ent, const T *ref, T *dev, size_t count, cudaStream_t s) {
+    const long long n = ents(m, ent);
+    const int lev = (int)(count / n);
+    k_perm_gather<<<grid_for(count, 256), 256, 0, s>>>(ref, dev, perm_of(m, ent), n, lev);
+}
+
 // field table for state sync: name of the fesomc_state member, device
-// pointer, count, group, and whether the device copy is FP32 (level fields
-// and 2D momentum of the FP32 form)
+// pointer, count, group, whether the device copy is FP32 (level fields and
+// 2D momentum of the FP32 form), and the entity kind it is stored per
 struct FieldRef {
     double *fesomc_state::*host;
     void *dev;
     size_t count;
     uint32_t group;
     bool f32;
+    int ent;
 };
 
 std::vector<FieldRef> field_table(fesomc_model *m) {
@@ -223,64 +282,153 @@ std::vector<FieldRef> field_table(fesomc_model *m) {
     const size_t N = d.N, E = d.E, L = d.L, NS = d.NS;
 #define LEV(name) (f ? (void *)q.name : (void *)d.name)
     return {
-        {&fesomc_state::eta_n, d.eta_n, N, FESOMC_F_ETA, false},
-        {&fesomc_state::eta_n_1, d.eta_n_1, N, FESOMC_F_ETA, false},
-        {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA, false},
-        {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA, false},
-        {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA, false},
-        {&fesomc_state::U_n_2D, LEV(U_n_2D), 2 * E, FESOMC_F_UV2D, f},
-        {&fesomc_state::U_n_1, LEV(U_n_1), 2 * E, FESOMC_F_UV2D, f},
-        {&fesomc_state::U_n_2, LEV(U_n_2), 2 * E, FESOMC_F_UV2D, f},
-        {&fesomc_state::U_filt_2D, LEV(U_filt_2D), E, FESOMC_F_UV2D, f},
-        {&fesomc_state::V_filt_2D, LEV(V_filt_2D), E, FESOMC_F_UV2D, f},
-        {&fesomc_state::U_n, LEV(U_n), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::V_n, LEV(V_n), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::U_rhsAB, LEV(U_rhsAB), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::V_rhsAB, LEV(V_rhsAB), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::U_n_filt, LEV(U_n_filt), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::V_n_filt, LEV(V_n_filt), L * E, FESOMC_F_UV3D, f},
-        {&fesomc_state::TF, LEV(TF), L * N, FESOMC_F_TS, f},
-        {&fesomc_state::SF, LEV(SF), L * N, FESOMC_F_TS, f},
-        {&fesomc_state::T_old, LEV(T_old), L * N, FESOMC_F_TS, f},
-        {&fesomc_state::S_old, LEV(S_old), L * N, FESOMC_F_TS, f},
-        {&fesomc_state::Tclim, LEV(Tclim), L * N, FESOMC_F_CLIM, f},
-        {&fesomc_state::Sclim, LEV(Sclim), L * N, FESOMC_F_CLIM, f},
-        {&fesomc_state::bt, LEV(bt), NS * N, FESOMC_F_MIX, f},
-        {&fesomc_state::snu, LEV(snu), NS * N, FESOMC_F_MIX, f},
-        {&fesomc_state::Kv, LEV(Kv), NS * N, FESOMC_F_MIX, f},
-        {&fesomc_state::Ri, LEV(Ri), NS * N, FESOMC_F_MIX, f},
-        {&fesomc_state::tke_dissip, LEV(tke_dissip), NS * N, FESOMC_F_MIX, f},
-        {&fesomc_state::Av, LEV(Av), NS * E, FESOMC_F_MIX, f},
-        {&fesomc_state::Wvel, LEV(Wvel), NS * N, FESOMC_F_WVEL, f},
-        {&fesomc_state::mask_wd, LEV(mask_wd), E, FESOMC_F_MASK, f},
-        {&fesomc_state::mask_wd_node, LEV(mask_wd_node), N, FESOMC_F_MASK, f},
-        {&fesomc_state::rho_c, LEV(rho_c), L * N, FESOMC_F_DIAG, f},
-        {&fesomc_state::hpressure, LEV(hpressure), NS * N, FESOMC_F_DIAG, f},
-        {&fesomc_state::Bar_pr_2D, LEV(Bar_pr_2D), 2 * E, FESOMC_F_DIAG, f},
+        {&fesomc_state::eta_n, d.eta_n, N, FESOMC_F_ETA, false, ENT_NODE},
+        {&fesomc_state::eta_n_1, d.eta_n_1, N, FESOMC_F_ETA, false, ENT_NODE},
+        {&fesomc_state::eta_n_2, d.eta_n_2, N, FESOMC_F_ETA, false, ENT_NODE},
+        {&fesomc_state::etaAB, d.etaAB, N, FESOMC_F_ETA, false, ENT_NODE},
+        {&fesomc_state::ssh_gp, d.ssh_gp, N, FESOMC_F_ETA, false, ENT_NODE},
+        {&fesomc_state::U_n_2D, LEV(U_n_2D), 2 * E, FESOMC_F_UV2D, f, ENT_ELEM},
+        {&fesomc_state::U_n_1, LEV(U_n_1), 2 * E, FESOMC_F_UV2D, f, ENT_ELEM},
+        {&fesomc_state::U_n_2, LEV(U_n_2), 2 * E, FESOMC_F_UV2D, f, ENT_ELEM},
+        {&fesomc_state::U_filt_2D, LEV(U_filt_2D), E, FESOMC_F_UV2D, f, ENT_ELEM},
+        {&fesomc_state::V_filt_2D, LEV(V_filt_2D), E, FESOMC_F_UV2D, f, ENT_ELEM},
+        {&fesomc_state::U_n, LEV(U_n), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::V_n, LEV(V_n), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::U_rhsAB, LEV(U_rhsAB), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::V_rhsAB, LEV(V_rhsAB), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::U_n_filt, LEV(U_n_filt), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::V_n_filt, LEV(V_n_filt), L * E, FESOMC_F_UV3D, f, ENT_ELEM},
+        {&fesomc_state::TF, LEV(TF), L * N, FESOMC_F_TS, f, ENT_NODE},
+        {&fesomc_state::SF, LEV(SF), L * N, FESOMC_F_TS, f, ENT_NODE},
+        {&fesomc_state::T_old, LEV(T_old), L * N, FESOMC_F_TS, f, ENT_NODE},
+        {&fesomc_state::S_old, LEV(S_old), L * N, FESOMC_F_TS, f, ENT_NODE},
+        {&fesomc_state::Tclim, LEV(Tclim), L * N, FESOMC_F_CLIM, f, ENT_NODE},
+        {&fesomc_state::Sclim, LEV(Sclim), L * N, FESOMC_F_CLIM, f, ENT_NODE},
+        {&fesomc_state::bt, LEV(bt), NS * N, FESOMC_F_MIX, f, ENT_NODE},
+        {&fesomc_state::snu, LEV(snu), NS * N, FESOMC_F_MIX, f, ENT_NODE},
+        {&fesomc_state::Kv, LEV(Kv), NS * N, FESOMC_F_MIX, f, ENT_NODE},
+        {&fesomc_state::Ri, LEV(Ri), NS * N, FESOMC_F_MIX, f, ENT_NODE},
+        {&fesomc_state::tke_dissip, LEV(tke_dissip), NS * N, FESOMC_F_MIX, f, ENT_NODE},
+        {&fesomc_state::Av, LEV(Av), NS * E, FESOMC_F_MIX, f, ENT_ELEM},
+        {&fesomc_state::Wvel, LEV(Wvel), NS * N, FESOMC_F_WVEL, f, ENT_NODE},
+        {&fesomc_state::mask_wd, LEV(mask_wd), E, FESOMC_F_MASK, f, ENT_ELEM},
+        {&fesomc_state::mask_wd_node, LEV(mask_wd_node), N, FESOMC_F_MASK, f, ENT_NODE},
+        {&fesomc_state::rho_c, LEV(rho_c), L * N, FESOMC_F_DIAG, f, ENT_NODE},
+        {&fesomc_state::hpressure, LEV(hpressure), NS * N, FESOMC_F_DIAG, f, ENT_NODE},
+        {&fesomc_state::Bar_pr_2D, LEV(Bar_pr_2D), 2 * E, FESOMC_F_DIAG, f, ENT_ELEM},
     };
 #undef LEV
 }
 
-// host double <-> device field (converting for FP32 level fields)
+// host double <-> device field (converting for FP32 level fields, and
+// between the reference and the storage order)
 int field_to_host(fesomc_model *m, const FieldRef &f, double *h) {
+    const size_t bytes = f.count * (f.f32 ? sizeof(float) : sizeof(double));
+    const void *src = f.dev;
+    if (m->perm) {
+        int rc = perm_buf(m, bytes);
+        if (rc) return rc;
+        if (f.f32) unpermute_to(m, f.ent, (const float *)f.dev, (float *)m->d_perm_buf, f.count, m->stream);
+        else unpermute_to(m, f.ent, (const double *)f.dev, (double *)m->d_perm_buf, f.count, m->stream);
+        CK(cudaStreamSynchronize(m->stream));
+        src = m->d_perm_buf;
+    }
     if (!f.f32) {
-        CK(cudaMemcpy(h, f.dev, f.count * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(h, src, bytes, cudaMemcpyDeviceToHost));
         return FESOMC_OK;
     }
     m->h_f32.resize(f.count);
-    CK(cudaMemcpy(m->h_f32.data(), f.dev, f.count * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(m->h_f32.data(), src, bytes, cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < f.count; ++i) h[i] = (double)m->h_f32[i];
     return FESOMC_OK;
 }
-int field_from_host(fesomc_model *m, void *dev, bool f32, size_t count, const double *h) {
-    if (!f32) {
-        CK(cudaMemcpy(dev, h, count * sizeof(double), cudaMemcpyHostToDevice));
-        return FESOMC_OK;
+int field_from_host(fesomc_model *m, void *dev, bool f32, size_t count, const double *h, int ent) {
+    const size_t bytes = count * (f32 ? sizeof(float) : sizeof(double));
+    void *dst = dev;
+    if (m->perm) {
+        int rc = perm_buf(m, bytes);
+        if (rc) return rc;
+        dst = m->d_perm_buf;
     }
-    m->h_f32.resize(count);
-    for (size_t i = 0; i < count; ++i) m->h_f32[i] = (float)h[i];
-    CK(cudaMemcpy(dev, m->h_f32.data(), count * sizeof(float), cudaMemcpyHostToDevice));
+    if (!f32) {
+        CK(cudaMemcpy(dst, h, bytes, cudaMemcpyHostToDevice));
+    } else {
+        m->h_f32.resize(count);
+        for (size_t i = 0; i < count; ++i) m->h_f32[i] = (float)h[i];
+        CK(cudaMemcpy(dst, m->h_f32.data(), bytes, cudaMemcpyHostToDevice));
+    }
+    if (m->perm) {
+        if (f32) permute_from(m, ent, (const float *)m->d_perm_buf, (float *)dev, count, m->stream);
+        else permute_from(m, ent, (const double *)m->d_perm_buf, (double *)dev, count, m->stream);
+        CK(cudaStreamSynchronize(m->stream));
+    }
     return FESOMC_OK;
+}
+
+// Hilbert-curve index of (x, y) on an n x n grid, n a power of two
+uint64_t hilbert_index(uint32_t n, uint32_t x, uint32_t y) {
+    uint64_t d = 0;
+    for (uint32_t s = n / 2; s > 0; s /= 2) {
+        const uint32_t rx = (x & s) > 0, ry = (y & s) > 0;
+        d += (uint64_t)s * s * ((3 * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) { x = n - 1 - x; y = n - 1 - y; }
+            std::swap(x, y);
+        }
+    }
+    return d;
+}
+
+// Storage order of nodes, elements and edges: identity, or (sfc_order) the
+// order of a Hilbert curve through the node positions, element centroids and
+// edge midpoints, internal and boundary edges each kept in their own range
+// (the kernels tell them apart by index).  *_ref maps a device index to the
+// reference one, *_dev the reverse.
+void storage_order(const fesomc_mesh *msh, bool sfc, std::vector<int> &nd_ref, std::vector<int> &el_ref,
+                   std::vector<int> &ed_ref) {
+    const int N = msh->nod2D, E = msh->elem2D, Ed = msh->edge2D, Ed_in = msh->edge2D_in;
+    nd_ref.resize(N); el_ref.resize(E); ed_ref.resize(Ed);
+    for (int i = 0; i < N; ++i) nd_ref[i] = i;
+    for (int i = 0; i < E; ++i) el_ref[i] = i;
+    for (int i = 0; i < Ed; ++i) ed_ref[i] = i;
+    if (!sfc || !msh->coord_nod2D) return;
+    const double *c = msh->coord_nod2D;
+    double x0 = c[0], x1 = c[0], y0 = c[1], y1 = c[1];
+    for (int i = 0; i < N; ++i) {
+        x0 = std::min(x0, c[2 * i]); x1 = std::max(x1, c[2 * i]);
+        y0 = std::min(y0, c[2 * i + 1]); y1 = std::max(y1, c[2 * i + 1]);
+    }
+    const uint32_t G = 1u << 16;
+    const double sx = (x1 > x0) ? (G - 1) / (x1 - x0) : 0.0, sy = (y1 > y0) ? (G - 1) / (y1 - y0) : 0.0;
+    auto key = [&](double x, double y) {
+        return hilbert_index(G, (uint32_t)((x - x0) * sx), (uint32_t)((y - y0) * sy));
+    };
+    auto order = [](std::vector<int> &idx, int lo, int hi, const std::vector<uint64_t> &k) {
+        std::sort(idx.begin() + lo, idx.begin() + hi, [&](int a, int b) { return k[a] != k[b] ? k[a] < k[b] : a < b; });
+    };
+    std::vector<uint64_t> kn(N), ke(E), kd(Ed);
+    for (int i = 0; i < N; ++i) kn[i] = key(c[2 * i], c[2 * i + 1]);
+    for (int e = 0; e < E; ++e) {
+        const int32_t *q = msh->elem2D_nodes + 4 * e;
+        const int q1 = (q[0] == q[3]) ? 3 : 4;
+        double x = 0.0, y = 0.0;
+        for (int k = 0; k < q1; ++k) { x += c[2 * (q[k] - 1)]; y += c[2 * (q[k] - 1) + 1]; }
+        ke[e] = key(x / q1, y / q1);
+    }
+    for (int ed = 0; ed < Ed; ++ed) {
+        const int a = msh->edge_nodes[2 * ed] - 1, b = msh->edge_nodes[2 * ed + 1] - 1;
+        kd[ed] = key(0.5 * (c[2 * a] + c[2 * b]), 0.5 * (c[2 * a + 1] + c[2 * b + 1]));
+    }
+    order(nd_ref, 0, N, kn);
+    order(el_ref, 0, E, ke);
+    order(ed_ref, 0, Ed_in, kd);
+    order(ed_ref, Ed_in, Ed, kd);
+}
+
+std::vector<int> inverse(const std::vector<int> &ref) {
+    std::vector<int> dev(ref.size());
+    for (size_t i = 0; i < ref.size(); ++i) dev[ref[i]] = (int)i;
+    return dev;
 }
 
 int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
@@ -293,138 +441,154 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
     for (int k = 0; k < L; ++k) dsig[k] = sig[k] - sig[k + 1];
     int rc;
     if ((rc = upload(m, &d.sig, sig)) || (rc = upload(m, &d.dsig, dsig))) return rc;
+    // connectivity checks, in reference numbering
+    for (int e = 0; e < E; ++e)
+        for (int k = 0; k < 4; ++k) {
+            const int32_t q = msh->elem2D_nodes[4 * e + k], g = msh->elem_edges[4 * e + k];
+            if (q < 1 || q > N) return FESOMC_EINVAL;
+            if (k < ((msh->elem2D_nodes[4 * e] == msh->elem2D_nodes[4 * e + 3]) ? 3 : 4) && (g < 1 || g > Ed))
+                return FESOMC_EINVAL;
+        }
+    for (int ed = 0; ed < Ed; ++ed) {
+        const int n1 = msh->edge_nodes[2 * ed], n2 = msh->edge_nodes[2 * ed + 1];
+        if (n1 < 1 || n1 > N || n2 < 1 || n2 > N) return FESOMC_EINVAL;
+        const int t1 = msh->edge_tri[2 * ed], t2 = msh->edge_tri[2 * ed + 1];
+        if (t1 < 1 || t1 > E) return FESOMC_EINVAL;
+        if ((ed < Ed_in) != (t2 > 0)) return FESOMC_EINVAL;
+    }
+    std::vector<int> nd_ref, el_ref, ed_ref;
+    storage_order(msh, m->p.sfc_order != 0, nd_ref, el_ref, ed_ref);
+    const std::vector<int> nd_dev = inverse(nd_ref), el_dev = inverse(el_ref), ed_dev = inverse(ed_ref);
+    m->perm = m->p.sfc_order != 0;
+    if (m->perm && ((rc = upload(m, &m->d_nd_ref, nd_ref)) || (rc = upload(m, &m->d_el_ref, el_ref)))) return rc;
+    auto ndv = [&](int ref1) { return nd_dev[ref1 - 1]; };        // 1-based reference node -> device
+    auto elv = [&](int ref1) { return ref1 > 0 ? el_dev[ref1 - 1] : -1; };
+    // an edge list entry: device edge and side, sorted by the reference edge number
+    auto edge_codes = [&](const int *refcodes, int n, int *out) {
+        int tmp[4];
+        for (int t = 0; t < n; ++t) tmp[t] = refcodes[t];
+        for (int a = 1; a < n; ++a)
+            for (int b2 = a; b2 > 0 && tmp[b2 - 1] > tmp[b2]; --b2) std::swap(tmp[b2 - 1], tmp[b2]);
+        for (int t = 0; t < 4; ++t) out[t] = t < n ? ((ed_dev[tmp[t] >> 1] << 1) | (tmp[t] & 1)) : -1;
+    };
     std::vector<int4> en(E), nb(E), ee(E), iel(E), sel(E);
     std::vector<double4> wcv(E), gsx(E), gsy(E), gvx(E), gvy(E);
     std::vector<double> eacc(E), bpf(E);
-    for (int e = 0; e < E; ++e) {
+    for (int ei = 0; ei < E; ++ei) {
+        const int e = el_ref[ei];
         const int32_t *q = msh->elem2D_nodes + 4 * e;
-        for (int k = 0; k < 4; ++k)
-            if (q[k] < 1 || q[k] > N) return FESOMC_EINVAL;
-        en[e] = make_int4(q[0] - 1, q[1] - 1, q[2] - 1, q[3] - 1);
+        en[ei] = make_int4(ndv(q[0]), ndv(q[1]), ndv(q[2]), ndv(q[3]));
         const int32_t *b = msh->elem_neighbors + 4 * e;
-        nb[e] = make_int4(b[0] > 0 ? b[0] - 1 : -1, b[1] > 0 ? b[1] - 1 : -1, b[2] > 0 ? b[2] - 1 : -1,
-                          b[3] > 0 ? b[3] - 1 : -1);
+        nb[ei] = make_int4(elv(b[0]), elv(b[1]), elv(b[2]), elv(b[3]));
         const int32_t *g = msh->elem_edges + 4 * e;
-        ee[e] = make_int4(g[0] - 1, g[1] - 1, g[2] - 1, g[3] - 1);
+        ee[ei] = make_int4(g[0] > 0 ? ed_dev[g[0] - 1] : -1, g[1] > 0 ? ed_dev[g[1] - 1] : -1,
+                           g[2] > 0 ? ed_dev[g[2] - 1] : -1, g[3] > 0 ? ed_dev[g[3] - 1] : -1);
         const double *w = msh->w_cv + 4 * e;
-        wcv[e] = make_double4(w[0], w[1], w[2], w[3]);
-        const double *s = msh->gradient_sca + 8 * e;
-        gsx[e] = make_double4(s[0], s[1], s[2], s[3]);
-        gsy[e] = make_double4(s[4], s[5], s[6], s[7]);
+        wcv[ei] = make_double4(w[0], w[1], w[2], w[3]);
+        const double *sg = msh->gradient_sca + 8 * e;
+        gsx[ei] = make_double4(sg[0], sg[1], sg[2], sg[3]);
+        gsy[ei] = make_double4(sg[4], sg[5], sg[6], sg[7]);
         const double *v = msh->gradient_vec + 8 * e;
-        gvx[e] = make_double4(v[0], v[1], v[2], v[3]);
-        gvy[e] = make_double4(v[4], v[5], v[6], v[7]);
+        gvx[ei] = make_double4(v[0], v[1], v[2], v[3]);
+        gvy[ei] = make_double4(v[4], v[5], v[6], v[7]);
         double acc = 0.0;
         for (int k = 0; k < 4; ++k) acc = acc + w[k] * msh->ac[q[k] - 1];
-        eacc[e] = acc;
-        bpf[e] = std::pow(acc, m->p.Bp_bz) * 1.0;
-        // internal edges of this element, in edge order, with the side
+        eacc[ei] = acc;
+        bpf[ei] = std::pow(acc, m->p.Bp_bz) * 1.0;
+        // internal edges of this element, in reference edge order, with the
+        // side; and all its edges (boundary ones too)
         const int q1 = (q[0] == q[3]) ? 3 : 4;
-        int list[4], nl = 0;
+        int list[4], nl = 0, all[4], na = 0;
         for (int j = 0; j < q1; ++j) {
             const int edg = g[j];
-            if (edg < 1 || edg > Ed) return FESOMC_EINVAL;
-            if (edg > Ed_in) continue;
-            bool dup = false;
-            for (int t = 0; t < nl; ++t) dup |= ((list[t] >> 1) == edg - 1);
-            if (dup) continue;
-            const int side = (msh->edge_tri[2 * (edg - 1)] == e + 1) ? 0 : 1;
-            list[nl++] = ((edg - 1) << 1) | side;
-        }
-        for (int a = 1; a < nl; ++a)
-            for (int b2 = a; b2 > 0 && list[b2 - 1] > list[b2]; --b2) std::swap(list[b2 - 1], list[b2]);
-        int tmp[4] = {-1, -1, -1, -1};
-        for (int t = 0; t < nl; ++t) tmp[t] = list[t];
-        iel[e] = make_int4(tmp[0], tmp[1], tmp[2], tmp[3]);
-        // all edges of the element (boundary ones too, side 0), sorted
-        int all[4], na = 0;
-        for (int j = 0; j < q1; ++j) {
-            const int edg = g[j];
+            const int code = ((edg - 1) << 1) | ((msh->edge_tri[2 * (edg - 1)] == e + 1) ? 0 : 1);
             bool dup = false;
             for (int t = 0; t < na; ++t) dup |= ((all[t] >> 1) == edg - 1);
             if (dup) continue;
-            const int side = (msh->edge_tri[2 * (edg - 1)] == e + 1) ? 0 : 1;
-            all[na++] = ((edg - 1) << 1) | side;
+            all[na++] = code;
+            if (edg <= Ed_in) list[nl++] = code;
         }
-        for (int a = 1; a < na; ++a)
-            for (int b2 = a; b2 > 0 && all[b2 - 1] > all[b2]; --b2) std::swap(all[b2 - 1], all[b2]);
-        int tmp2[4] = {-1, -1, -1, -1};
-        for (int t = 0; t < na; ++t) tmp2[t] = all[t];
-        sel[e] = make_int4(tmp2[0], tmp2[1], tmp2[2], tmp2[3]);
+        int o1[4], o2[4];
+        edge_codes(list, nl, o1);
+        edge_codes(all, na, o2);
+        iel[ei] = make_int4(o1[0], o1[1], o1[2], o1[3]);
+        sel[ei] = make_int4(o2[0], o2[1], o2[2], o2[3]);
     }
     std::vector<int2> edn(Ed), edt(Ed), eud(Ed);
     std::vector<double2> exy(Ed);
     std::vector<double4> ecr(Ed);
     std::vector<int> ecount(N + 1, 0), bcount(N + 1, 0);
-    for (int ed = 0; ed < Ed; ++ed) {
+    for (int di = 0; di < Ed; ++di) {
+        const int ed = ed_ref[di];
         const int n1 = msh->edge_nodes[2 * ed], n2 = msh->edge_nodes[2 * ed + 1];
-        if (n1 < 1 || n1 > N || n2 < 1 || n2 > N) return FESOMC_EINVAL;
-        edn[ed] = make_int2(n1 - 1, n2 - 1);
-        const int t1 = msh->edge_tri[2 * ed], t2 = msh->edge_tri[2 * ed + 1];
-        if (t1 < 1 || t1 > E) return FESOMC_EINVAL;
-        if ((ed < Ed_in) != (t2 > 0)) return FESOMC_EINVAL;
-        edt[ed] = make_int2(t1 - 1, t2 > 0 ? t2 - 1 : -1);
+        edn[di] = make_int2(ndv(n1), ndv(n2));
+        edt[di] = make_int2(elv(msh->edge_tri[2 * ed]), elv(msh->edge_tri[2 * ed + 1]));
         if (msh->edge_up_dn_tri) {
             const int u = msh->edge_up_dn_tri[2 * ed], w = msh->edge_up_dn_tri[2 * ed + 1];
-            eud[ed] = make_int2(u > 0 ? u - 1 : -1, w > 0 ? w - 1 : -1);
+            eud[di] = make_int2(elv(u), elv(w));
         } else {
-            eud[ed] = make_int2(-1, -1);
+            eud[di] = make_int2(-1, -1);
         }
-        exy[ed] = make_double2(msh->edge_dxdy[2 * ed], msh->edge_dxdy[2 * ed + 1]);
-        const double *c = msh->edge_cross_dxdy + 4 * ed;
-        ecr[ed] = make_double4(c[0], c[1], c[2], c[3]);
-        ecount[n1]++; ecount[n2]++;
-        if (ed >= Ed_in) { bcount[n1]++; bcount[n2]++; }
+        exy[di] = make_double2(msh->edge_dxdy[2 * ed], msh->edge_dxdy[2 * ed + 1]);
+        const double *cc = msh->edge_cross_dxdy + 4 * ed;
+        ecr[di] = make_double4(cc[0], cc[1], cc[2], cc[3]);
+        ecount[edn[di].x + 1]++; ecount[edn[di].y + 1]++;
+        if (ed >= Ed_in) { bcount[edn[di].x + 1]++; bcount[edn[di].y + 1]++; }
     }
-    // CSR node -> edges (appending in edge order keeps each list sorted)
+    // CSR node -> edges, each list in reference edge order
     std::vector<int> eptr(N + 1, 0), bptr(N + 1, 0);
     for (int n = 0; n < N; ++n) { eptr[n + 1] = eptr[n] + ecount[n + 1]; bptr[n + 1] = bptr[n] + bcount[n + 1]; }
     std::vector<int> eidx(eptr[N]), bidx(bptr[N]), efill(eptr.begin(), eptr.end() - 1), bfill(bptr.begin(), bptr.end() - 1);
     for (int ed = 0; ed < Ed; ++ed) {
-        eidx[efill[edn[ed].x]++] = (ed << 1) | 0;
-        eidx[efill[edn[ed].y]++] = (ed << 1) | 1;
+        const int di = ed_dev[ed];
+        eidx[efill[edn[di].x]++] = (di << 1) | 0;
+        eidx[efill[edn[di].y]++] = (di << 1) | 1;
         if (ed >= Ed_in) {
-            bidx[bfill[edn[ed].x]++] = (ed << 1) | 0;
-            bidx[bfill[edn[ed].y]++] = (ed << 1) | 1;
+            bidx[bfill[edn[di].x]++] = (di << 1) | 0;
+            bidx[bfill[edn[di].y]++] = (di << 1) | 1;
         }
     }
     // CSR node -> elements (nod_in_elem2D order) and the summed area
     std::vector<int> nptr(N + 1, 0), nidx;
     std::vector<double> tvol(N);
-    for (int n = 0; n < N; ++n) {
+    for (int ni = 0; ni < N; ++ni) {
+        const int n = nd_ref[ni];
         const int num = msh->nod_in_elem2D_num[n];
-        double s = 0.0;
+        double sum = 0.0;
         for (int k = 0; k < num; ++k) {
             const int el = msh->nod_in_elem2D[(size_t)msh->nod_in_elem2D_max * n + k];
             if (el < 1 || el > E) return FESOMC_EINVAL;
-            nidx.push_back(el - 1);
-            s = s + msh->elem_area[el - 1];
+            nidx.push_back(el_dev[el - 1]);
+            sum = sum + msh->elem_area[el - 1];
         }
-        nptr[n + 1] = (int)nidx.size();
-        tvol[n] = s;
+        nptr[ni + 1] = (int)nidx.size();
+        tvol[ni] = sum;
     }
     // rivers and open boundary
     std::vector<int> rcount(N + 1, 0);
     for (int i = 0; i < msh->n_rivers; ++i) {
         const int nd = msh->nod_rivers[i];
         if (nd < 1 || nd > N) return FESOMC_EINVAL;
-        rcount[nd]++;
+        rcount[ndv(nd) + 1]++;
     }
     std::vector<int> rptr(N + 1, 0);
     for (int n = 0; n < N; ++n) rptr[n + 1] = rptr[n] + rcount[n + 1];
     std::vector<int> ridx(rptr[N]), rfill(rptr.begin(), rptr.end() - 1);
-    for (int i = 0; i < msh->n_rivers; ++i) ridx[rfill[msh->nod_rivers[i] - 1]++] = i;
+    for (int i = 0; i < msh->n_rivers; ++i) ridx[rfill[ndv(msh->nod_rivers[i])]++] = i;
     std::vector<int> obn(N, -1);
     for (int i = 0; i < msh->nobn; ++i) {
         const int nd = msh->in_obn[i];
         if (nd < 1 || nd > N) return FESOMC_EINVAL;
-        obn[nd - 1] = i;
+        obn[ndv(nd)] = i;
     }
-    std::vector<int> idx(msh->index_nod2D, msh->index_nod2D + N);
-    std::vector<double> dep(msh->depth, msh->depth + N), area(msh->area, msh->area + N), ac(msh->ac, msh->ac + N);
-    std::vector<double> atp1(msh->a_tp, msh->a_tp + N), atp2(msh->a_tp + N, msh->a_tp + 2 * (size_t)N);
-    std::vector<double> ea(msh->elem_area, msh->elem_area + E), ec(msh->elem_cos, msh->elem_cos + E),
-        cor(msh->coriolis, msh->coriolis + E);
+    // per-node and per-element mesh arrays in storage order
+    auto gather_n = [&](const double *src) { std::vector<double> v(N); for (int i = 0; i < N; ++i) v[i] = src[nd_ref[i]]; return v; };
+    auto gather_e = [&](const double *src) { std::vector<double> v(E); for (int i = 0; i < E; ++i) v[i] = src[el_ref[i]]; return v; };
+    std::vector<int> idx(N);
+    for (int i = 0; i < N; ++i) idx[i] = msh->index_nod2D[nd_ref[i]];
+    std::vector<double> dep = gather_n(msh->depth), area = gather_n(msh->area), ac = gather_n(msh->ac);
+    std::vector<double> atp1 = gather_n(msh->a_tp), atp2 = gather_n(msh->a_tp + N);
+    std::vector<double> ea = gather_e(msh->elem_area), ec = gather_e(msh->elem_cos), cor = gather_e(msh->coriolis);
     if ((rc = upload(m, &d.elem_nodes, en)) || (rc = upload(m, &d.elem_nb, nb)) || (rc = upload(m, &d.elem_edges, ee)) ||
         (rc = upload(m, &d.elem_iedges, iel)) || (rc = upload(m, &d.elem_sedges, sel)) ||
         (rc = upload(m, &d.edge_nodes, edn)) ||
@@ -1043,6 +1207,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (par->bih_2D && !std::isfinite(par->Abh0)) return FESOMC_EINVAL;
     if (par->T_potential != 0 && par->T_potential != 1) return FESOMC_EINVAL;
     if (par->npes < 0 || par->npes > 1) return FESOMC_EINVAL;   // one rank: no halo exchange
+    if (par->sfc_order != 0 && par->sfc_order != 1) return FESOMC_EINVAL;
+    if (par->sfc_order && !mesh->coord_nod2D) return FESOMC_EINVAL;
     if (par->key_atm != 0 && par->key_atm != 1) return FESOMC_EINVAL;
     if (par->key_atm && (par->type_swr_body < 1 || par->type_swr_body > 2 ||   // fv_read_run.F90:799-803
                          (par->jer_const != 0 && par->jer_const != 1)))
@@ -1094,6 +1260,14 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
         for (int i = 0; i < mesh->nod2D; ++i)
             lonlat[i] = make_double2(mesh->coord_nod2D[2 * (size_t)i], mesh->coord_nod2D[2 * (size_t)i + 1]);
         if ((rc = upload(m, &m->d_coord, lonlat)) || (rc = dalloc(m, &m->d_clock, 1))) return fail(rc);
+        if (m->perm) {   // coordinates in storage order
+            if ((rc = perm_buf(m, lonlat.size() * sizeof(double2)))) return fail(rc);
+            if (cudaMemcpy(m->d_perm_buf, lonlat.data(), lonlat.size() * sizeof(double2), cudaMemcpyHostToDevice) !=
+                cudaSuccess)
+                return fail(FESOMC_ECUDA);
+            permute_from(m, ENT_NODE, (const double *)m->d_perm_buf, (double *)m->d_coord, 2 * lonlat.size(), m->stream);
+            if (cudaStreamSynchronize(m->stream) != cudaSuccess) return fail(FESOMC_ECUDA);
+        }
     }
     if (cudaMallocHost(&m->h_notconv, sizeof(int) * 2) != cudaSuccess) return fail(FESOMC_ENOMEM);
     // state upload (all groups that are provided)
@@ -1101,12 +1275,12 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
     if (!st->mask_wd) {
         std::vector<double> ones(mesh->elem2D, 1.0);
         void *dev = m->fp32 ? (void *)m->d32.mask_wd : (void *)m->d.mask_wd;
-        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data()))) return fail(rc);
+        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data(), ENT_ELEM))) return fail(rc);
     }
     if (!st->mask_wd_node) {
         std::vector<double> ones(mesh->nod2D, 1.0);
         void *dev = m->fp32 ? (void *)m->d32.mask_wd_node : (void *)m->d.mask_wd_node;
-        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data()))) return fail(rc);
+        if ((rc = field_from_host(m, dev, m->fp32, ones.size(), ones.data(), ENT_NODE))) return fail(rc);
     }
     // jacobian state before the main loop: both calls see the initial eta
     if (cudaMemcpy(m->d.eta_jac, m->d.eta_n, sizeof(double) * mesh->nod2D, cudaMemcpyDeviceToDevice) ||
@@ -1130,7 +1304,13 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
     // large fields are copied synchronously with respect to the stream so the
     // caller may reuse its buffers on return
     int rc = FESOMC_OK;
-    if (!m->fp32) {
+    if (!m->fp32 && m->perm) {
+        CK(cudaStreamSynchronize(s));
+        if (f->taux && (rc = field_from_host(m, d.taux, false, E, f->taux, ENT_ELEM))) return rc;
+        if (f->tauy && (rc = field_from_host(m, d.tauy, false, E, f->tauy, ENT_ELEM))) return rc;
+        if (f->windx && (rc = field_from_host(m, d.windx, false, N, f->windx, ENT_NODE))) return rc;
+        if (f->windy && (rc = field_from_host(m, d.windy, false, N, f->windy, ENT_NODE))) return rc;
+    } else if (!m->fp32) {
         if (f->taux) CK(cudaMemcpyAsync(d.taux, f->taux, E * 8, cudaMemcpyHostToDevice, s));
         if (f->tauy) CK(cudaMemcpyAsync(d.tauy, f->tauy, E * 8, cudaMemcpyHostToDevice, s));
         if (f->windx) CK(cudaMemcpyAsync(d.windx, f->windx, N * 8, cudaMemcpyHostToDevice, s));
@@ -1139,22 +1319,25 @@ int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
         // FP32 form: converted on the host, written while the stream is idle
         const fesomc::f32::Dev &q = m->d32;
         CK(cudaStreamSynchronize(s));
-        if (f->taux && (rc = field_from_host(m, q.taux, true, E, f->taux))) return rc;
-        if (f->tauy && (rc = field_from_host(m, q.tauy, true, E, f->tauy))) return rc;
-        if (f->windx && (rc = field_from_host(m, q.windx, true, N, f->windx))) return rc;
-        if (f->windy && (rc = field_from_host(m, q.windy, true, N, f->windy))) return rc;
+        if (f->taux && (rc = field_from_host(m, q.taux, true, E, f->taux, ENT_ELEM))) return rc;
+        if (f->tauy && (rc = field_from_host(m, q.tauy, true, E, f->tauy, ENT_ELEM))) return rc;
+        if (f->windx && (rc = field_from_host(m, q.windx, true, N, f->windx, ENT_NODE))) return rc;
+        if (f->windy && (rc = field_from_host(m, q.windy, true, N, f->windy, ENT_NODE))) return rc;
     }
     if (f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
-    if (f->Tclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Tclim : (void *)d.Tclim, m->fp32, L * N, f->Tclim)))
+    if (f->Tclim &&
+        (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Tclim : (void *)d.Tclim, m->fp32, L * N, f->Tclim, ENT_NODE)))
         return rc;
-    if (f->Sclim && (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Sclim : (void *)d.Sclim, m->fp32, L * N, f->Sclim)))
+    if (f->Sclim &&
+        (rc = field_from_host(m, m->fp32 ? (void *)m->d32.Sclim : (void *)d.Sclim, m->fp32, L * N, f->Sclim, ENT_NODE)))
         return rc;
     if (f->taux || f->tauy || f->windx || f->windy || f->Tclim || f->Sclim) CK(cudaStreamSynchronize(s));
     if (d.mslp) {   // key_atm: FP64 node fields in both forms
         const double *src[] = {f->mslp, f->emp, f->qsr, f->qns, f->Rj, f->aj, f->bj};
         double *dst[] = {d.mslp, d.emp, d.qsr, d.qns, d.Rj, d.aj, d.bj};
+        CK(cudaStreamSynchronize(s));
         for (int k = 0; k < 7; ++k)
-            if (src[k] && dst[k]) CK(cudaMemcpyAsync(dst[k], src[k], N * 8, cudaMemcpyHostToDevice, s));
+            if (src[k] && dst[k] && (rc = field_from_host(m, dst[k], false, N, src[k], ENT_NODE))) return rc;
         if (d.Rj && f->Rj && f->aj && f->bj) m->have_jer = true;
         CK(cudaStreamSynchronize(s));
     }
@@ -1240,7 +1423,7 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
     for (const FieldRef &f : field_table(m)) {
         const double *h = st->*(f.host);
         int rc;
-        if ((f.group & mask) && h && (rc = field_from_host(m, f.dev, f.f32, f.count, h))) return rc;
+        if ((f.group & mask) && h && (rc = field_from_host(m, f.dev, f.f32, f.count, h, f.ent))) return rc;
     }
     if (mask == FESOMC_F_ALL) {
         m->lfirst = st->lfirst;
@@ -1304,7 +1487,12 @@ int fesomc_gpu_snapshot_begin(fesomc_model *m, uint32_t mask, fesomc_state *st) 
                     (void)cudaGetLastError();
             }
         }
-        CK(cudaMemcpyAsync(m->snap_bufs[i].first, f.dev, bytes, cudaMemcpyDeviceToDevice, m->stream));
+        if (!m->perm)
+            CK(cudaMemcpyAsync(m->snap_bufs[i].first, f.dev, bytes, cudaMemcpyDeviceToDevice, m->stream));
+        else if (f.f32)   // the copy in reference order
+            unpermute_to(m, f.ent, (const float *)f.dev, (float *)m->snap_bufs[i].first, f.count, m->stream);
+        else
+            unpermute_to(m, f.ent, (const double *)f.dev, (double *)m->snap_bufs[i].first, f.count, m->stream);
         m->snaps.push_back({dst, m->snap_bufs[i].first, f.f32 ? m->snap_bufs[i].second : nullptr, f.count});
     }
     CK(cudaEventRecord(m->snap_taken, m->stream));

@@ -55,7 +55,8 @@ class Params(C.Structure):
                                   ("filt_bi_3D", C.c_int32), ("filt_bi_2D", C.c_int32), ("tau_c", C.c_double),
                                   ("bih_2D", C.c_int32), ("T_potential", C.c_int32), ("npes", C.c_int32),
                                   ("key_atm", C.c_int32), ("type_swr_body", C.c_int32), ("jer_const", C.c_int32),
-                                  ("Rjc", C.c_double), ("ajc", C.c_double), ("bjc", C.c_double)]
+                                  ("Rjc", C.c_double), ("ajc", C.c_double), ("bjc", C.c_double),
+                                  ("sfc_order", C.c_int32)]
 
 
 STATE_FIELDS = ["eta_n", "eta_n_1", "eta_n_2", "etaAB", "U_n_2D", "U_n_1", "U_n_2", "U_filt_2D",

@@ -311,7 +311,7 @@ def estuary(cfg="cfg0", seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radiu
 
 def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=1.2, m2_phase_deg=0.0,
                  noise_sigma=0.5, seed=20261203, tracer_adv=abi.TRACER_MUSCL, sponge_radius=SPONGE_RADIUS,
-                 lib=None, atm=None, **overrides):
+                 lib=None, atm=None, shuffle=None, **overrides):
     """Synthetic estuary: nx x ny quads at dx metres, 30 % split into
     triangles, depth h0 -> h1 across the channel plus smoothed noise of
     noise_sigma metres, river at x = 0, M2 tide of m2_amp metres and phase
@@ -319,11 +319,21 @@ def estuary_case(name, nx, ny, dx, nsigma, h0, h1, *, stress=(0.0, 0.0), m2_amp=
     (taux, tauy) in N/m2.  atm: atmospheric forcing (turns key_atm on), a
     dict of node fields or constants among qns, qsr (W/m2, downward), emp
     (E - P), mslp (Pa) and Rj, aj, bj (jer_const = 0), or a callable
-    (mesh) -> such a dict, pushed with every step's forcing.  Parameter
-    overrides go to default_params."""
+    (mesh) -> such a dict, pushed with every step's forcing.  shuffle: a
+    seed that numbers the nodes and lists the elements in random order (a
+    mesh as it may come from a mesh generator's file, not row by row).
+    Parameter overrides go to default_params."""
     xy, index, elems, depth, (nxn, nyn) = estuary_geometry(nx, ny, dx, seed=seed, h0=h0, h1=h1,
                                                             noise_sigma=noise_sigma)
     rivers = np.arange(0, nyn) * nxn + 1                 # every node on x = 0 (1-based)
+    if shuffle is not None:
+        rs = np.random.default_rng([seed, shuffle])
+        pn = rs.permutation(len(index))                  # new node j is old node pn[j]
+        new_of_old = np.empty(len(index), dtype=np.int64)
+        new_of_old[pn] = np.arange(len(index))
+        xy, index, depth = xy[pn], index[pn], depth[pn]
+        elems = (new_of_old[elems - 1] + 1).astype(np.int32)[rs.permutation(len(elems))]
+        rivers = new_of_old[rivers - 1] + 1
     # T_potential switches both the potential and the mesh's a_tp weights
     mesh = HostMesh(xy, index, elems, depth, cartesian=True, nsigma=nsigma, coriolis_on=True,
                     lat_deg=50.0, with_up_dn_tri=True, rivers=rivers, sponge_radius=sponge_radius,

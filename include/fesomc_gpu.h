@@ -194,6 +194,16 @@ typedef struct fesomc_params {
     int32_t type_swr_body;
     int32_t jer_const;
     double Rjc, ajc, bjc;
+    /* Storage order on the device (no counterpart in the reference):
+     * 0 = the reference numbering; 1 = nodes, elements and edges stored
+     * along a Hilbert curve through their positions (internal and boundary
+     * edges each in their own range), so that neighbour gathers of meshes
+     * numbered in file order touch nearby memory.  The permutation is kept
+     * by the library: every array crossing the C-ABI stays in the reference
+     * numbering, and every edge-ordered sum still runs in reference edge
+     * order, so results are the same bits in both orders.  Needs
+     * coord_nod2D.                                                          */
+    int32_t sfc_order;
 } fesomc_params;
 
 /*

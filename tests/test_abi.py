@@ -83,7 +83,7 @@ def test_init_rejects_bad_atmospheric_options_without_gpu(built):
     arrays = case.new_state_arrays()
     st = case.state_struct(arrays, case.params.time_jd0)
     h = C.c_void_p()
-    for bad in ({"key_atm": 2}, {"key_atm": 1, "type_swr_body": 3}, {"key_atm": 1, "jer_const": 2}):
+    for bad in ({"key_atm": 2}, {"key_atm": 1, "type_swr_body": 3}, {"key_atm": 1, "jer_const": 2}, {"sfc_order": 2}):
         p = cases.default_params(**bad)
         p.scale_area, p.density_0 = case.params.scale_area, case.params.density_0
         assert built.fesomc_gpu_init(C.byref(case.mesh.c), C.byref(p), C.byref(st), C.byref(h)) == 1, bad

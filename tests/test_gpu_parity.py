@@ -473,3 +473,45 @@ def test_key_atm_per_node_water_types_required(mods):
         assert g.step(1, check=False) == 4
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("shuffle", [None, 5])
+def test_sfc_storage_order_bit_exact(mods, shuffle):
+    """Nodes, elements and edges stored along a Hilbert curve (sfc_order = 1)
+    give the oracle's bits, on the estuary as generated (row by row) and with
+    its nodes and elements numbered at random (a mesh in file order); the
+    oracle runs in the reference numbering of the same mesh."""
+    abi, cases, model, pyoracle = mods
+    bad, eg, eo = run_pair(mods, est(cases, "small", shuffle=shuffle, sfc_order=1), 30)
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+    if shuffle is not None:
+        bad, _, _ = run_pair(mods, est(cases, "small", shuffle=shuffle), 30)
+        assert bad == []
+
+
+def test_sfc_storage_order_le_potential_snapshot_fp32(mods):
+    """Storage order on LE (spherical), with the tidal potential and device
+    forcing, through the asynchronous snapshot, and in the FP32 form (which
+    gives the same bits in both orders)."""
+    abi, cases, model, pyoracle = mods
+    bad, _, _ = run_pair(mods, le(cases, sfc_order=1), 20)
+    assert bad == []
+    out = []
+    for sfc in (0, 1):
+        case = cases.estuary("small", T_potential=1, sfc_order=sfc)
+        case.params.fp32_form = 1
+        g = model.GpuModel(case)
+        g.set_forcing(case.forcing_fn(1, cases.advance_time(g.time_jd, case.params.dt)))
+        base = np.ascontiguousarray(case.forcing_fn(1, case.params.time_jd0 + 20.0)["runoff_rivers"])
+        abi.check(g.lib.fesomc_gpu_set_device_forcing(g.h, abi.dptr(base), 1))
+        g.run(15)
+        g.snapshot_begin()
+        snap = g.snapshot_end()
+        st = g.state()
+        g.close()
+        for f in FIELDS:
+            assert np.array_equal(snap[f], st[f]), f
+        out.append(st)
+    for f in FIELDS:
+        assert np.array_equal(out[0][f], out[1][f]), f
