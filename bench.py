@@ -643,6 +643,33 @@ def run_closure(args):
     print(json.dumps(out), flush=True)
 
 
+def run_lc_infer(args):
+    """The learned closure's inference alone: the BF16 tensor-core kernel and
+    the FP32 kernels on --lc-infer device-resident columns of the cfg1 shape
+    (21 levels: 66 inputs, 42 outputs), random weights, device-timed; FLOP
+    per column 2 (66*256 + 2*256*256 + 256*42)."""
+    from fesomc import closure
+    c = closure.Closure(21)
+    n = args.lc_infer
+    flop = 2.0 * (66 * 256 + 2 * 256 * 256 + 256 * 42) * n
+    ms_tc = c.time(n, reps=max(args.steps, 1), bf16=True)
+    ms_32 = c.time(n, reps=max(min(args.steps, 5), 1), bf16=False)
+    c.close()
+    peak = None
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    kind = "fallback"
+    if os.path.exists(pk):
+        with open(pk) as f:
+            peak = json.load(f).get("bf16_tflops")
+            kind = "measured"
+    peak = peak or 1590.0
+    tf = flop / (ms_tc * 1e-3) / 1e12
+    print(json.dumps({"metric": "learned-closure inference", "columns": n, "flop_per_pass": flop,
+                      "bf16_tcgen05": {"ms": ms_tc, "tflops": tf, "frac_of_peak": tf / peak, "peak_tflops": peak,
+                                       "peak_source": kind},
+                      "fp32_simt": {"ms": ms_32, "tflops": flop / (ms_32 * 1e-3) / 1e12}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -668,8 +695,12 @@ def main():
     ap.add_argument("--lc-epochs", type=int, default=4)
     ap.add_argument("--lc-lr", type=float, default=1e-3)
     ap.add_argument("--lc-judge", type=int, default=100)
+    ap.add_argument("--lc-infer", type=int, default=0, help="time the closure inference on this many columns")
     args = ap.parse_args()
     ws, rank, local = dist_info()
+    if args.lc_infer > 0:
+        run_lc_infer(args)
+        return
     if args.closure:
         run_closure(args)
         return

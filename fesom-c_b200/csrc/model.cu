@@ -1874,6 +1874,57 @@ int fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32
     return FESOMC_OK;
 }
 
+namespace {
+// deterministic pseudo-random normalised inputs for the timing entry point
+__global__ void k_lc_fill(long long n, float *x, unsigned long long seed) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + seed;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        z ^= z >> 31;
+        x[i] = (float)((double)(z >> 11) * (1.0 / 9007199254740992.0) * 4.0 - 2.0);
+    }
+}
+}  // namespace
+
+int fesomc_closure_time(fesomc_closure *c, int64_t n, int32_t reps, int32_t bf16, double *ms) {
+    if (!c || n < 1 || reps < 1 || !ms) return FESOMC_EINVAL;
+    LcNet *net = c->net;
+    if (bf16 && !lc_tc_supported(net)) return FESOMC_EINVAL;
+    if (bf16 && !net->tc_ready) {
+        int rc = lc_tc_prepare(net);
+        if (rc) return rc;
+    }
+    float *dx = nullptr, *dy = nullptr, *ba = nullptr, *bb = nullptr;
+    int rc = FESOMC_OK;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaMalloc(&dx, sizeof(float) * n * net->IN) || cudaMalloc(&dy, sizeof(float) * n * net->OUT) ||
+        (!bf16 && (cudaMalloc(&ba, sizeof(float) * n * kLcHidden) || cudaMalloc(&bb, sizeof(float) * n * kLcHidden))))
+        rc = FESOMC_ENOMEM;
+    if (!rc && (cudaEventCreate(&e0) || cudaEventCreate(&e1))) rc = FESOMC_ECUDA;
+    if (!rc) {
+        k_lc_fill<<<grid_for(n * net->IN, 256), 256>>>(n * net->IN, dx, 12345ULL);
+        auto once = [&]() {
+            return bf16 ? lc_forward_tc(net, dx, n, dy, nullptr) : lc_forward_full(net, dx, n, dy, ba, bb, nullptr);
+        };
+        rc = once();   // warm-up
+        if (!rc && cudaEventRecord(e0) != cudaSuccess) rc = FESOMC_ECUDA;
+        for (int r = 0; r < reps && !rc; ++r) rc = once();
+        if (!rc && (cudaEventRecord(e1) || cudaEventSynchronize(e1))) rc = FESOMC_ECUDA;
+        float t = 0.0f;
+        if (!rc && cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) rc = FESOMC_ECUDA;
+        *ms = t / reps;
+        if (!rc && bf16) {
+            unsigned int err = 0;
+            if (cudaMemcpy(&err, net->tc_err, sizeof(err), cudaMemcpyDeviceToHost) != cudaSuccess || err) rc = FESOMC_ECUDA;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(dx); cudaFree(dy); cudaFree(ba); cudaFree(bb);
+    return rc;
+}
+
 int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every, int32_t bf16) {
     if (!m || judge_every < 0) return FESOMC_EINVAL;
     drop_graph(m);

@@ -126,6 +126,7 @@ SIGNATURES = {
     "fesomc_closure_grad": (C.c_int, [C.c_void_p, f32p, f32p, C.c_int32, f64p, f32p]),
     "fesomc_closure_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "fesomc_closure_stats": (C.c_int, [C.c_void_p, C.POINTER(ClosureReport)]),
+    "fesomc_closure_time": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.c_int32, f64p]),
     "fesomc_gpu_version": (C.c_char_p, []),
     "fesomc_gpu_kernel_launches": (C.c_int64, [C.c_void_p]),
     "fesomc_host_density_jm": (C.c_double, [C.c_double, C.c_double, C.c_double, C.c_double]),

@@ -94,6 +94,12 @@ class Closure:
     def detach(model):
         abi.check(abi.load().fesomc_closure_attach(model.h, None, 0, 0), "fesomc_closure_attach")
 
+    def time(self, ncol, reps=10, bf16=True):
+        """Mean device ms of one pass over ncol device-resident columns."""
+        ms = C.c_double()
+        abi.check(self.lib.fesomc_closure_time(self.h, int(ncol), reps, int(bf16), C.byref(ms)), "fesomc_closure_time")
+        return ms.value
+
     @staticmethod
     def stats(model):
         r = abi.ClosureReport()

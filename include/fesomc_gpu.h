@@ -469,6 +469,10 @@ int  fesomc_closure_forward(fesomc_closure *c, const float *X, int64_t n, float 
 int  fesomc_closure_grad(fesomc_closure *c, const float *X, const float *T, int32_t n, double *loss,
                          float *grads);
 int  fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_every, int32_t bf16);
+/* measurement: the network on n device-resident pseudo-random columns,
+ * reps times after one warm-up, *ms = mean device time per pass (CUDA
+ * events); bf16 selects the tensor-core kernel. */
+int  fesomc_closure_time(fesomc_closure *c, int64_t n, int32_t reps, int32_t bf16, double *ms);
 int  fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r);
 
 /* ---- version / introspection --------------------------------------------- */
