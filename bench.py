@@ -107,9 +107,12 @@ class ClockSampler:
                 "samples": len(sms)}
 
 
+BUILD_OPTS = {}   # storage-order options of the run (--sfc-order, --shuffle)
+
+
 def build_case(cfg, lib=None):
     from fesomc import cases
-    return cases.estuary(cfg, lib=lib)
+    return cases.estuary(cfg, lib=lib, **BUILD_OPTS)
 
 
 def oracle_case(cfg):
@@ -169,6 +172,9 @@ def workload_config(case, cfg):
         "dt_s": case.params.dt, "substeps": case.params.Mt,
         "l2": f"inputs larger than L2 (device state ~{state_gb:.1f} GB per replica, no flush needed)",
         "parallelism": "replicas (one independent mesh per GPU)",
+        "numbering": ("nodes and elements numbered at random (seed %d)" % BUILD_OPTS["shuffle"]
+                      if BUILD_OPTS.get("shuffle") is not None else "generator order (row by row)"),
+        "storage_order": "Hilbert curve" if BUILD_OPTS.get("sfc_order") else "mesh numbering",
     }
 
 
@@ -696,7 +702,13 @@ def main():
     ap.add_argument("--lc-lr", type=float, default=1e-3)
     ap.add_argument("--lc-judge", type=int, default=100)
     ap.add_argument("--lc-infer", type=int, default=0, help="time the closure inference on this many columns")
+    ap.add_argument("--sfc-order", action="store_true", help="store the mesh along a Hilbert curve on the device")
+    ap.add_argument("--shuffle", type=int, default=None, help="number the mesh's nodes and elements at random (seed)")
     args = ap.parse_args()
+    if args.sfc_order:
+        BUILD_OPTS["sfc_order"] = 1
+    if args.shuffle is not None:
+        BUILD_OPTS["shuffle"] = args.shuffle
     ws, rank, local = dist_info()
     if args.lc_infer > 0:
         run_lc_infer(args)
