@@ -357,6 +357,17 @@ def run_ours(args, ws, rank, local):
         "roofline": roof,
         "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in kk.items()} for kk in kernels],
     }
+    # d3_end sweeps per column in one more step: the mean, and the mean over
+    # warps (32 consecutive columns) of their largest count, which a warp
+    # waits for
+    import numpy as np
+    its = np.empty(m.N, dtype=np.int32)
+    if lib.fesomc_gpu_d3end_iterations(g.h, 1, its.ctypes.data_as(C.POINTER(C.c_int32))) == 0:
+        w = its[: (m.N // 32) * 32].reshape(-1, 32)
+        line["d3end_iterations"] = {"mean": float(its.mean()), "max": int(its.max()),
+                                    "warp_max_mean": float(w.max(axis=1).mean()),
+                                    "lane_efficiency": float(its[: w.size].mean() / w.max(axis=1).mean()),
+                                    "step": "the step after the timed region"}
     g.close()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = host_cpu()

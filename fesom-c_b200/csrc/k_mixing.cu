@@ -114,6 +114,7 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
         const real bot = bott_R * (ubt * ubt + vbt * vbt);
         real *btr = bA, *xq = bB;   // xq: this iteration's xx1, then its btr1
         bool converged = false;
+        int iters = 200;
         for (int it = 1; it <= 200; ++it) {
             real x = real(1.0), y = y2;
             real s_lo = sn[1], s_mid = sn[2];
@@ -158,11 +159,12 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
                 xq[nz - 1] = b1v;
                 above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
             }
-            if (!above) { converged = true; break; }
+            if (!above) { converged = true; iters = it; break; }
             real *t = btr;
             btr = xq;
             xq = t;
         }
+        if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
         if (converged) {
             for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (btr[nz] * btr[nz]) / sn[nz];
         } else {

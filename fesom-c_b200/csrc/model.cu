@@ -1971,6 +1971,24 @@ int fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r) {
     return FESOMC_OK;
 }
 
+int fesomc_gpu_d3end_iterations(fesomc_model *m, int32_t nsteps, int32_t *iters) {
+    if (!m || nsteps < 1 || !iters || m->p.ver_mix != 3) return FESOMC_EINVAL;
+    int *buf = nullptr;
+    int rc = dalloc(m, &buf, (size_t)m->d.N);
+    if (rc) return rc;
+    drop_graph(m);                   // the graph holds the kernels' parameters: capture again
+    m->d.d3_iters = buf;
+    m->d32.d3_iters = buf;
+    rc = run_steps(m, nsteps);
+    m->d.d3_iters = nullptr;
+    m->d32.d3_iters = nullptr;
+    drop_graph(m);
+    if (rc) return rc;
+    if ((rc = collect_status(m))) return rc;
+    CK(cudaMemcpy(iters, buf, sizeof(int) * (size_t)m->d.N, cudaMemcpyDeviceToHost));
+    return status_code(m->status_acc);
+}
+
 int fesomc_gpu_set_device(int32_t device) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) return FESOMC_ECUDA;

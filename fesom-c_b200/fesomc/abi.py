@@ -110,6 +110,7 @@ SIGNATURES = {
     "fesomc_mesh_set_sponge": (C.c_int, [C.c_void_p, C.c_double]),
     "fesomc_mesh_free": (None, [C.c_void_p]),
     "fesomc_gpu_time_run": (C.c_int, [C.c_void_p, C.c_int32, f64p]),
+    "fesomc_gpu_d3end_iterations": (C.c_int, [C.c_void_p, C.c_int32, i32p]),
     "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,
                                      C.POINTER(C.c_int64)]),
     "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),

@@ -366,6 +366,13 @@ double fesomc_host_density_jm(double t, double s, double pz, double density_0);
  * Neither has a counterpart in the reference; they replace its per-routine
  * omp_get_wtime prints (src/fv_main.F90:2084-2095). */
 int  fesomc_gpu_time_run(fesomc_model *m, int32_t nsteps, double *ms);
+/* fesomc_gpu_d3end_iterations: advances nsteps internal steps (forcing as
+ * last set) and returns in iters (nod2D values) the number of sweeps the
+ * turbulence closure d3_end needed on each node column in the last of them
+ * (200 = not converged), in the device's storage order, i.e. in the order
+ * consecutive GPU threads take the columns (32 consecutive values share a
+ * warp).  Measurement only; no counterpart in the reference. */
+int  fesomc_gpu_d3end_iterations(fesomc_model *m, int32_t nsteps, int32_t *iters);
 int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, int32_t *n_kernels,
                         char *names, double *ms_per_launch, double *bytes_per_launch, int64_t *launches);
 
