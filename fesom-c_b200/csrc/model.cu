@@ -330,15 +330,17 @@ int field_to_host(fesomc_model *m, const FieldRef &f, double *h) {
         if (rc) return rc;
         if (f.f32) unpermute_to(m, f.ent, (const float *)f.dev, (float *)m->d_perm_buf, f.count, m->stream);
         else unpermute_to(m, f.ent, (const double *)f.dev, (double *)m->d_perm_buf, f.count, m->stream);
-        CK(cudaStreamSynchronize(m->stream));
         src = m->d_perm_buf;
     }
+    // the model's stream is non-blocking: copy on it, then wait for it
     if (!f.f32) {
-        CK(cudaMemcpy(h, src, bytes, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(h, src, bytes, cudaMemcpyDeviceToHost, m->stream));
+        CK(cudaStreamSynchronize(m->stream));
         return FESOMC_OK;
     }
     m->h_f32.resize(f.count);
-    CK(cudaMemcpy(m->h_f32.data(), src, bytes, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(m->h_f32.data(), src, bytes, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
     for (size_t i = 0; i < f.count; ++i) h[i] = (double)m->h_f32[i];
     return FESOMC_OK;
 }
@@ -350,18 +352,20 @@ int field_from_host(fesomc_model *m, void *dev, bool f32, size_t count, const do
         if (rc) return rc;
         dst = m->d_perm_buf;
     }
+    // on the model's (non-blocking) stream, so that the permutation below
+    // reads the staging buffer after the copy into it has landed
     if (!f32) {
-        CK(cudaMemcpy(dst, h, bytes, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, m->stream));
     } else {
         m->h_f32.resize(count);
         for (size_t i = 0; i < count; ++i) m->h_f32[i] = (float)h[i];
-        CK(cudaMemcpy(dst, m->h_f32.data(), bytes, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(dst, m->h_f32.data(), bytes, cudaMemcpyHostToDevice, m->stream));
     }
     if (m->perm) {
         if (f32) permute_from(m, ent, (const float *)m->d_perm_buf, (float *)dev, count, m->stream);
         else permute_from(m, ent, (const double *)m->d_perm_buf, (double *)dev, count, m->stream);
-        CK(cudaStreamSynchronize(m->stream));
     }
+    CK(cudaStreamSynchronize(m->stream));
     return FESOMC_OK;
 }
 
@@ -1262,8 +1266,8 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
         if ((rc = upload(m, &m->d_coord, lonlat)) || (rc = dalloc(m, &m->d_clock, 1))) return fail(rc);
         if (m->perm) {   // coordinates in storage order
             if ((rc = perm_buf(m, lonlat.size() * sizeof(double2)))) return fail(rc);
-            if (cudaMemcpy(m->d_perm_buf, lonlat.data(), lonlat.size() * sizeof(double2), cudaMemcpyHostToDevice) !=
-                cudaSuccess)
+            if (cudaMemcpyAsync(m->d_perm_buf, lonlat.data(), lonlat.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                                m->stream) != cudaSuccess)
                 return fail(FESOMC_ECUDA);
             permute_from(m, ENT_NODE, (const double *)m->d_perm_buf, (double *)m->d_coord, 2 * lonlat.size(), m->stream);
             if (cudaStreamSynchronize(m->stream) != cudaSuccess) return fail(FESOMC_ECUDA);

