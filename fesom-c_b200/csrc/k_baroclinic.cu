@@ -371,8 +371,9 @@ __global__ void k_bih_uc(Dev d, int mode) {
         const int e = (int)(ii / L);
         const int z = (int)(ii % L);
         const real2 c = bih_gather(d, e, z);
-        const real Ah = (mode == 0) ? -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area
-                                    : -d.elem_acc[e] * d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
+        const real sa = scale_area_of(d, e);
+        const real Ah = (mode == 0) ? -d.Abh0 * sqrt(d.elem_area[e] / sa) / sa
+                                    : -d.elem_acc[e] * d.Abh0 * sqrt(d.elem_area[e] / sa) / sa;
         d.bihU[ii] = c.x * (Ah);
         d.bihV[ii] = c.y * (Ah);
     }
@@ -442,7 +443,7 @@ __global__ void k_filt2x_uc(Dev d) {
         const int z = (int)(ii % L);
         const int4 nb = d.elem_nb[e];
         const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
-        const real K_bi = tau_inv * sqrt(d.scale_area / d.elem_area[e]);
+        const real K_bi = tau_inv * sqrt(scale_area_of(d, e) / d.elem_area[e]);
         const real uj = d.U_n[ii] * d.Je[ii], vj = d.V_n[ii] * d.Je[ii];
         real uc = real(0.0), vc = real(0.0);
         for (int j = 0; j < 4; ++j) {

@@ -380,7 +380,8 @@ __global__ void k_bih2d_ul(Dev d) {
             if (code & 1) { ux = ux - f.x; uy = uy - f.y; }
             else { ux = ux + f.x; uy = uy + f.y; }
         }
-        const real Ah = -d.Abh0 * sqrt(d.elem_area[e] / d.scale_area) / d.scale_area;
+        const real sa = scale_area_of(d, e);
+        const real Ah = -d.Abh0 * sqrt(d.elem_area[e] / sa) / sa;
         const real acc = d.elem_acc[e];
         d.b2ul[e] = make_real2(ux * (Ah) * acc, uy * (Ah) * acc);
     }
@@ -435,7 +436,7 @@ __global__ void k_filt2x_2d(Dev d) {
         const int e = (int)ii;
         const int4 nb = d.elem_nb[e];
         const int nbs[4] = {nb.x, nb.y, nb.z, nb.w};
-        const real K_bi = tau_inv * sqrt(d.scale_area / d.elem_area[e]);
+        const real K_bi = tau_inv * sqrt(scale_area_of(d, e) / d.elem_area[e]);
         const real2 u0 = d.U_n_2D[e];
         real uc = real(0.0), vc = real(0.0);
         for (int j = 0; j < 4; ++j) {

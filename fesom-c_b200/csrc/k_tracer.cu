@@ -24,11 +24,17 @@ constexpr int kRedGrid = 592;  // 4 x 148 SMs
 // ---------------------------------------------------------------------------
 // global min / max of TF and SF
 // ---------------------------------------------------------------------------
+// One partial per (block, member): blockIdx.y is the member, whose nodes
+// are member_node_off[m] .. member_node_off[m+1] (all nodes for one member).
 __global__ void k_minmax_part(Dev d) {
     __shared__ real s[4][kRedBlock];
-    const long long total = (long long)d.N * d.L;
-    real tmin = d.TF[0], tmax = d.TF[0], smin = d.SF[0], smax = d.SF[0];
-    GRID_LOOP(i, total) {
+    const int mb = blockIdx.y;
+    const long long n0 = d.member_node_off ? d.member_node_off[mb] : 0;
+    const long long n1 = d.member_node_off ? d.member_node_off[mb + 1] : d.N;
+    const long long first = n0 * d.L, total = (n1 - n0) * d.L;
+    real tmin = d.TF[first], tmax = d.TF[first], smin = d.SF[first], smax = d.SF[first];
+    GRID_LOOP(j, total) {
+        const long long i = first + j;
         const real t = d.TF[i], x = d.SF[i];
         tmin = dmin(tmin, t); tmax = dmax(tmax, t);
         smin = dmin(smin, x); smax = dmax(smax, x);
@@ -45,20 +51,20 @@ __global__ void k_minmax_part(Dev d) {
         __syncthreads();
     }
     if (threadIdx.x == 0)
-        for (int k = 0; k < 4; ++k) d.mm_part[(size_t)blockIdx.x * 4 + k] = s[k][0];
+        for (int k = 0; k < 4; ++k) d.mm_part[((size_t)mb * gridDim.x + blockIdx.x) * 4 + k] = s[k][0];
 }
 
-// min / max are exact, so the order in which the partials are combined does
-// not change the result
+// one warp per member; min / max are exact, so the order in which the
+// partials are combined does not change the result
 __global__ void k_minmax_final(Dev d, int nparts) {
-    if (blockIdx.x != 0) return;
     const int lane = threadIdx.x & 31;
-    real tmin = d.mm_part[0], tmax = d.mm_part[1], smin = d.mm_part[2], smax = d.mm_part[3];
+    const real *part = d.mm_part + (size_t)blockIdx.x * nparts * 4;
+    real tmin = part[0], tmax = part[1], smin = part[2], smax = part[3];
     for (int b = lane; b < nparts; b += 32) {
-        tmin = dmin(tmin, d.mm_part[4 * b + 0]);
-        tmax = dmax(tmax, d.mm_part[4 * b + 1]);
-        smin = dmin(smin, d.mm_part[4 * b + 2]);
-        smax = dmax(smax, d.mm_part[4 * b + 3]);
+        tmin = dmin(tmin, part[4 * b + 0]);
+        tmax = dmax(tmax, part[4 * b + 1]);
+        smin = dmin(smin, part[4 * b + 2]);
+        smax = dmax(smax, part[4 * b + 3]);
     }
     for (int o = 16; o > 0; o >>= 1) {
         tmin = dmin(tmin, __shfl_xor_sync(kFull, tmin, o));
@@ -67,8 +73,8 @@ __global__ void k_minmax_final(Dev d, int nparts) {
         smax = dmax(smax, __shfl_xor_sync(kFull, smax, o));
     }
     if (lane == 0) {
-        d.aver[0] = real(0.5) * (tmin + tmax);
-        d.aver[1] = real(0.5) * (smin + smax);
+        d.aver[2 * blockIdx.x] = real(0.5) * (tmin + tmax);
+        d.aver[2 * blockIdx.x + 1] = real(0.5) * (smin + smax);
     }
 }
 
@@ -136,10 +142,10 @@ __device__ __forceinline__ real tvert_upwind(const Dev &d, int k, real a, const 
 // for the gathers below (fv_tracer.F90:433,435 and :39-47)
 __global__ void k_ab2_node(Dev d) {
     const long long total = (long long)d.N * d.L;
-    const real T_aver = d.aver[0], S_aver = d.aver[1];
     GRID_LOOP(i, total) {
-        d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
-        d.stfold[i] = ab2(d, d.SF, d.S_old, i, S_aver);
+        const int n = (int)(i / d.L);
+        d.ttfold[i] = ab2(d, d.TF, d.T_old, i, t_aver_of(d, n));
+        d.stfold[i] = ab2(d, d.SF, d.S_old, i, s_aver_of(d, n));
     }
 }
 
@@ -149,7 +155,6 @@ __global__ void k_ab2_node(Dev d) {
 // ---------------------------------------------------------------------------
 __global__ void k_upwind_h(Dev d) {
     const int lane = threadIdx.x & 31;
-    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
     const long long total = (long long)d.N * L;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -158,6 +163,7 @@ __global__ void k_upwind_h(Dev d) {
         const long long i_ = valid ? wbase + lane : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L), zc = z;
+        const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
         const real a = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
@@ -417,7 +423,6 @@ __global__ void __maxnreg__(64) k_muscl_edge(Dev d) {
 __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
     const long long total = (long long)d.N * d.L;
     const int lane = threadIdx.x & 31;
-    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
@@ -425,6 +430,7 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
         const long long i_ = valid ? wbase + lane : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L);
+        const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
         const real an = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
@@ -488,8 +494,8 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
 // H_advtr_crit = 0.1, H_advtr_min = 0)
 __global__ void k_miura_prep(Dev d) {
     const long long total = (long long)d.N * d.L;
-    const real T_aver = d.aver[0];
     GRID_LOOP(i, total) {
+        const real T_aver = t_aver_of(d, (int)(i / d.L));
         d.ttfold[i] = ab2(d, d.TF, d.T_old, i, T_aver);
         d.tnow[i] = d.TF[i] - T_aver;
         if (i % d.L == 0) {
@@ -561,7 +567,7 @@ __global__ void k_miura_edge(Dev d) {
         const real a = real(1.0), b = real(1.0);
         real Kh = d.elem_area[et.x];
         if (two) Kh = real(0.5) * (Kh + d.elem_area[et.y]);
-        Kh = d.K_hor * Kh / d.scale_area;
+        Kh = d.K_hor * Kh / scale_area_of(d, et.x);
         const size_t e1 = (size_t)et.x * L + z;
         const size_t i1 = (size_t)nn.x * L + z, i2 = (size_t)nn.y * L + z;
         real Tx, Ty;
@@ -613,7 +619,6 @@ __global__ void k_miura_edge(Dev d) {
 // consecutive lanes of a flat index
 __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
     const int lane = threadIdx.x & 31;
-    const real T_aver = d.aver[0];
     const int L = d.L, NS = d.NS;
     const long long total = (long long)d.N * L;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -622,6 +627,7 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
         const long long i_ = valid ? wbase + lane : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L), zc = z;
+        const real T_aver = t_aver_of(d, n);
         const real an = jac_a(d, d.eta_jac, n);
         const real *W = d.Wvel + (size_t)n * NS;
         const size_t base = (size_t)n * L;
@@ -810,7 +816,6 @@ template <bool kAtm>
 __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     real *sm = reinterpret_cast<real *>(sm_raw);
-    const real T_aver = d.aver[0], S_aver = d.aver[1];
     const int L = d.L, NS = d.NS;
     real *col = sm + threadIdx.x;
     const int bd = blockDim.x;
@@ -819,6 +824,7 @@ __global__ void __launch_bounds__(kVdBlock) k_vdiff_col(Dev d) {
     auto SP = [&](int k) -> real & { return col[((size_t)2 * L + k) * bd]; };
     GRID_LOOP(ii, d.N) {
         const int n = (int)ii;
+        const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
         const size_t base = (size_t)n * L;
         const real aj = jac_a(d, d.eta_jac, n);
         const real *Kv = d.Kv + (size_t)n * NS;
@@ -943,9 +949,13 @@ __global__ void k_energy_final(const double *part, int nparts, double *out) {
 }
 
 // ---- launch wrappers --------------------------------------------------------
+// partials per member of the tracer min / max: kRedGrid for one mesh, fewer
+// per member for packed members (at least 8)
+int minmax_parts(int n_members) { return n_members <= 1 ? kRedGrid : (kRedGrid / n_members > 8 ? kRedGrid / n_members : 8); }
 void launch_minmax(const Dev &d, cudaStream_t s) {
-    k_minmax_part<<<kRedGrid, kRedBlock, 0, s>>>(d);
-    k_minmax_final<<<1, 32, 0, s>>>(d, kRedGrid);
+    const int parts = minmax_parts(d.n_members);
+    k_minmax_part<<<dim3(parts, d.n_members), kRedBlock, 0, s>>>(d);
+    k_minmax_final<<<d.n_members, 32, 0, s>>>(d, parts);
 }
 void launch_ab2(const Dev &d, cudaStream_t s) { k_ab2_node<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d); }
 void launch_upwind(const Dev &d, cudaStream_t s) {

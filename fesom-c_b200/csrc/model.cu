@@ -65,6 +65,7 @@ namespace fesomc {
     void launch_lc_harvest(const Dev &, const LcView &, cudaStream_t); \
     void launch_lc_judge(const Dev &, const LcView &, cudaStream_t); \
     int energy_parts(); \
+    int minmax_parts(int); \
     void launch_energy(const Dev &, double *, double *, cudaStream_t);
 namespace f64 {
 FESOMC_KERNEL_LAUNCHERS
@@ -156,6 +157,11 @@ struct fesomc_model {
     int lc_judge_every = 0;
     long long lc_steps = 0, lc_judges = 0;
     void *lc_owner = nullptr;         // fesomc_closure the per-column buffers were made for
+    // packed members (fesomc_gpu_init_packed): node and element ranges of
+    // each member in the reference numbering of the packed mesh
+    int n_members = 1;
+    std::vector<int> member_node_off, member_elem_off;
+    std::vector<double> member_scale_area;
     // storage order (fesomc_params.sfc_order): device index -> reference
     // index of nodes and elements, used by every transfer of a field
     bool perm = false;
@@ -388,7 +394,12 @@ uint64_t hilbert_index(uint32_t n, uint32_t x, uint32_t y) {
 // edge midpoints, internal and boundary edges each kept in their own range
 // (the kernels tell them apart by index).  *_ref maps a device index to the
 // reference one, *_dev the reverse.
-void storage_order(const fesomc_mesh *msh, bool sfc, std::vector<int> &nd_ref, std::vector<int> &el_ref,
+//
+// Packed members (node_member / elem_member non-empty, reference numbering):
+// each member's nodes and elements stay in its own contiguous range, the
+// curve ordering them within it, and edges are ordered by their member first.
+void storage_order(const fesomc_mesh *msh, bool sfc, const std::vector<int> &node_member,
+                   const std::vector<int> &elem_member, std::vector<int> &nd_ref, std::vector<int> &el_ref,
                    std::vector<int> &ed_ref) {
     const int N = msh->nod2D, E = msh->elem2D, Ed = msh->edge2D, Ed_in = msh->edge2D_in;
     nd_ref.resize(N); el_ref.resize(E); ed_ref.resize(Ed);
@@ -407,21 +418,23 @@ void storage_order(const fesomc_mesh *msh, bool sfc, std::vector<int> &nd_ref, s
     auto key = [&](double x, double y) {
         return hilbert_index(G, (uint32_t)((x - x0) * sx), (uint32_t)((y - y0) * sy));
     };
+    const bool packed = !node_member.empty();
+    auto mkey = [&](int member) { return packed ? (uint64_t)member << 40 : (uint64_t)0; };
     auto order = [](std::vector<int> &idx, int lo, int hi, const std::vector<uint64_t> &k) {
         std::sort(idx.begin() + lo, idx.begin() + hi, [&](int a, int b) { return k[a] != k[b] ? k[a] < k[b] : a < b; });
     };
     std::vector<uint64_t> kn(N), ke(E), kd(Ed);
-    for (int i = 0; i < N; ++i) kn[i] = key(c[2 * i], c[2 * i + 1]);
+    for (int i = 0; i < N; ++i) kn[i] = mkey(packed ? node_member[i] : 0) | key(c[2 * i], c[2 * i + 1]);
     for (int e = 0; e < E; ++e) {
         const int32_t *q = msh->elem2D_nodes + 4 * e;
         const int q1 = (q[0] == q[3]) ? 3 : 4;
         double x = 0.0, y = 0.0;
         for (int k = 0; k < q1; ++k) { x += c[2 * (q[k] - 1)]; y += c[2 * (q[k] - 1) + 1]; }
-        ke[e] = key(x / q1, y / q1);
+        ke[e] = mkey(packed ? elem_member[e] : 0) | key(x / q1, y / q1);
     }
     for (int ed = 0; ed < Ed; ++ed) {
         const int a = msh->edge_nodes[2 * ed] - 1, b = msh->edge_nodes[2 * ed + 1] - 1;
-        kd[ed] = key(0.5 * (c[2 * a] + c[2 * b]), 0.5 * (c[2 * a + 1] + c[2 * b + 1]));
+        kd[ed] = mkey(packed ? node_member[a] : 0) | key(0.5 * (c[2 * a] + c[2 * b]), 0.5 * (c[2 * a + 1] + c[2 * b + 1]));
     }
     order(nd_ref, 0, N, kn);
     order(el_ref, 0, E, ke);
@@ -460,8 +473,18 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
         if (t1 < 1 || t1 > E) return FESOMC_EINVAL;
         if ((ed < Ed_in) != (t2 > 0)) return FESOMC_EINVAL;
     }
+    // packed members: the member of every node and element (reference numbering)
+    std::vector<int> nmem, emem;
+    if (m->n_members > 1) {
+        nmem.resize(N);
+        emem.resize(E);
+        for (int k = 0; k < m->n_members; ++k) {
+            for (int i = m->member_node_off[k]; i < m->member_node_off[k + 1]; ++i) nmem[i] = k;
+            for (int i = m->member_elem_off[k]; i < m->member_elem_off[k + 1]; ++i) emem[i] = k;
+        }
+    }
     std::vector<int> nd_ref, el_ref, ed_ref;
-    storage_order(msh, m->p.sfc_order != 0, nd_ref, el_ref, ed_ref);
+    storage_order(msh, m->p.sfc_order != 0, nmem, emem, nd_ref, el_ref, ed_ref);
     const std::vector<int> nd_dev = inverse(nd_ref), el_dev = inverse(el_ref), ed_dev = inverse(ed_ref);
     m->perm = m->p.sfc_order != 0;
     if (m->perm && ((rc = upload(m, &m->d_nd_ref, nd_ref)) || (rc = upload(m, &m->d_el_ref, el_ref)))) return rc;
@@ -610,6 +633,18 @@ int build_mesh(fesomc_model *m, const fesomc_mesh *msh) {
         (rc = upload(m, &d.elem_bpfac, bpf)) || (rc = upload(m, &d.edge_dxdy, exy)) ||
         (rc = upload(m, &d.edge_cross, ecr)) || (rc = upload(m, &d.node_tvol, tvol)))
         return rc;
+    // packed members, in storage order (each member's range is the same
+    // there, the storage order keeping members apart)
+    d.n_members = m->n_members;
+    if (m->n_members > 1) {
+        std::vector<int> nm(N), em(E);
+        for (int i = 0; i < N; ++i) nm[i] = nmem[nd_ref[i]];
+        for (int i = 0; i < E; ++i) em[i] = emem[el_ref[i]];
+        if ((rc = upload(m, &d.node_member, nm)) || (rc = upload(m, &d.elem_member, em)) ||
+            (rc = upload(m, &d.member_node_off, m->member_node_off)) ||
+            (rc = upload(m, &d.member_scale_area, m->member_scale_area)))
+            return rc;
+    }
     return FESOMC_OK;
 }
 
@@ -696,8 +731,9 @@ int alloc_3d(fesomc_model *m, D &d) {
     decltype(&d.U_n) nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
     for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
-    if ((rc = dalloc(m, &d.mm_part, (size_t)4 * 1024))) return rc;
-    if ((rc = dalloc(m, &d.aver, 2))) return rc;
+    const size_t nm = (size_t)m->n_members;
+    if ((rc = dalloc(m, &d.mm_part, (size_t)4 * nm * fesomc::f64::minmax_parts((int)nm)))) return rc;
+    if ((rc = dalloc(m, &d.aver, 2 * nm))) return rc;
     return FESOMC_OK;
 }
 
@@ -736,8 +772,11 @@ int setup_f32_view(fesomc_model *m) {
     b.node_eptr = a.node_eptr; b.node_eidx = a.node_eidx; b.node_nptr = a.node_nptr; b.node_nidx = a.node_nidx;
     b.node_bptr = a.node_bptr; b.node_bidx = a.node_bidx; b.node_rptr = a.node_rptr; b.node_ridx = a.node_ridx;
     b.obn_of_node = a.obn_of_node; b.index_nod2D = a.index_nod2D;
+    b.n_members = a.n_members; b.node_member = a.node_member; b.elem_member = a.elem_member;
+    b.member_node_off = a.member_node_off;
     const size_t N = a.N, E = a.E, Ed = a.Ed, L = a.L, NS = a.NS;
     int rc;
+    if (a.member_scale_area && (rc = geom_f32(m, a.member_scale_area, a.n_members, &b.member_scale_area))) return rc;
     if ((rc = geom_f32(m, a.sig, NS, &b.sig)) || (rc = geom_f32(m, a.dsig, L, &b.dsig)) ||
         (rc = geom_f32(m, a.w_cv, 4 * E, &b.w_cv)) || (rc = geom_f32(m, a.gs_x, 4 * E, &b.gs_x)) ||
         (rc = geom_f32(m, a.gs_y, 4 * E, &b.gs_y)) || (rc = geom_f32(m, a.gv_x, 4 * E, &b.gv_x)) ||
@@ -1189,7 +1228,54 @@ int upload_tides(fesomc_model *m) {
 
 extern "C" {
 
+namespace {
+// A packed member table: ranges that start at 0, grow strictly and end at
+// the mesh's counts, and connectivity that never crosses from one member to
+// another (elements' nodes, edges' nodes and elements, nodes' elements).
+bool members_valid(const fesomc_mesh *msh, const fesomc_members *mb) {
+    const int n = mb->n, N = msh->nod2D, E = msh->elem2D;
+    if (n < 1 || !mb->node_off || !mb->elem_off || !mb->scale_area) return false;
+    if (mb->node_off[0] != 0 || mb->elem_off[0] != 0 || mb->node_off[n] != N || mb->elem_off[n] != E) return false;
+    for (int k = 0; k < n; ++k) {
+        if (mb->node_off[k + 1] <= mb->node_off[k] || mb->elem_off[k + 1] <= mb->elem_off[k]) return false;
+        if (!(mb->scale_area[k] > 0.0) || !std::isfinite(mb->scale_area[k])) return false;
+    }
+    std::vector<int> nm(N), em(E);
+    for (int k = 0; k < n; ++k) {
+        for (int i = mb->node_off[k]; i < mb->node_off[k + 1]; ++i) nm[i] = k;
+        for (int i = mb->elem_off[k]; i < mb->elem_off[k + 1]; ++i) em[i] = k;
+    }
+    auto node_in = [&](int32_t ref1, int k) { return ref1 >= 1 && ref1 <= N && nm[ref1 - 1] == k; };
+    auto elem_in = [&](int32_t ref1, int k) { return ref1 >= 1 && ref1 <= E && em[ref1 - 1] == k; };
+    for (int e = 0; e < E; ++e)
+        for (int j = 0; j < 4; ++j) {
+            if (!node_in(msh->elem2D_nodes[4 * e + j], em[e])) return false;
+            const int32_t nb = msh->elem_neighbors[4 * e + j];
+            if (nb > 0 && !elem_in(nb, em[e])) return false;
+        }
+    for (int ed = 0; ed < msh->edge2D; ++ed) {
+        const int32_t a = msh->edge_nodes[2 * ed];
+        if (a < 1 || a > N) return false;
+        const int k = nm[a - 1];
+        if (!node_in(msh->edge_nodes[2 * ed + 1], k) || !elem_in(msh->edge_tri[2 * ed], k)) return false;
+        if (msh->edge_tri[2 * ed + 1] > 0 && !elem_in(msh->edge_tri[2 * ed + 1], k)) return false;
+        if (msh->edge_up_dn_tri)
+            for (int j = 0; j < 2; ++j)
+                if (msh->edge_up_dn_tri[2 * ed + j] > 0 && !elem_in(msh->edge_up_dn_tri[2 * ed + j], k)) return false;
+    }
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < msh->nod_in_elem2D_num[i]; ++j)
+            if (!elem_in(msh->nod_in_elem2D[(size_t)msh->nod_in_elem2D_max * i + j], nm[i])) return false;
+    return true;
+}
+}  // namespace
+
 int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fesomc_state *st, fesomc_model **out) {
+    return fesomc_gpu_init_packed(mesh, par, st, nullptr, out);
+}
+
+int fesomc_gpu_init_packed(const fesomc_mesh *mesh, const fesomc_params *par, const fesomc_state *st,
+                           const fesomc_members *members, fesomc_model **out) {
     if (!mesh || !par || !st || !out) return FESOMC_EINVAL;
     *out = nullptr;
     if (mesh->nsigma < 5 || mesh->nsigma > 127 || mesh->nod2D < 3 || mesh->elem2D < 1) return FESOMC_EINVAL;
@@ -1218,8 +1304,15 @@ int fesomc_gpu_init(const fesomc_mesh *mesh, const fesomc_params *par, const fes
                          (par->jer_const != 0 && par->jer_const != 1)))
         return FESOMC_EINVAL;
     if (!st->eta_n || !st->TF || !st->SF || !st->U_n || !st->V_n) return FESOMC_EINVAL;
+    if (members && !members_valid(mesh, members)) return FESOMC_EINVAL;
     fesomc_model *m = new (std::nothrow) fesomc_model();
     if (!m) return FESOMC_ENOMEM;
+    if (members && members->n > 1) {
+        m->n_members = members->n;
+        m->member_node_off.assign(members->node_off, members->node_off + members->n + 1);
+        m->member_elem_off.assign(members->elem_off, members->elem_off + members->n + 1);
+        m->member_scale_area.assign(members->scale_area, members->scale_area + members->n);
+    }
     m->p = *par;
     m->fp32 = par->fp32_form == 1;
     set_params(m->d, *par);

@@ -82,6 +82,10 @@ class MeshOpts(C.Structure):
                 ("T_potential", C.c_int32), ("with_up_dn_tri", C.c_int32)]
 
 
+class Members(C.Structure):
+    _fields_ = [("n", C.c_int32), ("node_off", i32p), ("elem_off", i32p), ("scale_area", f64p)]
+
+
 class ClosureReport(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("steps", "judge_steps", "wet_columns", "out_of_envelope", "dry_columns",
                                          "judge_values")] + [("judge_rms_log", C.c_double), ("judge_max_log", C.c_double)]
@@ -114,6 +118,8 @@ SIGNATURES = {
     "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,
                                      C.POINTER(C.c_int64)]),
     "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),
+    "fesomc_gpu_init_packed": (C.c_int, [C.POINTER(Mesh), C.POINTER(Params), C.POINTER(State), C.POINTER(Members),
+                                         C.POINTER(C.c_void_p)]),
     "fesomc_gpu_set_device": (C.c_int, [C.c_int32]),
     "fesomc_closure_create": (C.c_int, [C.c_int32, C.c_int64, C.c_uint64, C.POINTER(C.c_void_p)]),
     "fesomc_closure_free": (None, [C.c_void_p]),

@@ -14,7 +14,7 @@ import ctypes as C
 
 import numpy as np
 
-from . import abi, cases, model
+from . import abi, cases, model, packed
 
 # member step statuses that fesomc_ensemble_run reports per member
 STEP_STATUSES = {k for k, v in abi.ERRORS.items() if v in ("ENEGSALT", "ELOWTEMP", "ENONFINITE")}
@@ -111,3 +111,44 @@ class Ensemble:
         for g in self.models:
             g.close()
         self.models = []
+
+
+class PackedEnsemble(Ensemble):
+    """The members packed into one model per level count (packed.PackedCase):
+    every kernel of a step covers all members of a pack in one launch, and
+    the packs (at most two here: 11 and 21 levels) run side by side as in
+    Ensemble.  Statuses and states are reported per member."""
+
+    def __init__(self, member_cases):
+        groups = {}
+        for i, c in enumerate(member_cases):
+            groups.setdefault(c.mesh.NS, []).append(i)
+        self.groups = [groups[k] for k in sorted(groups)]
+        self.n_members = len(member_cases)
+        self.packs = [packed.PackedCase([member_cases[i] for i in g], name="pack%d" % k)
+                      for k, g in enumerate(self.groups)]
+        super().__init__(self.packs)
+
+    def _spread(self, pack_status):
+        status = [0] * self.n_members
+        for g, st in zip(self.groups, pack_status):
+            for i in g:
+                status[i] = st
+        return status
+
+    def run(self, nsteps, timed=False):
+        ms, st = super().run(nsteps, timed)
+        return ms, self._spread(st)
+
+    def run_one_at_a_time(self, nsteps):
+        ms, st = super().run_one_at_a_time(nsteps)
+        return ms, self._spread(st)
+
+    def member_state(self, i, mask=abi.F_ALL):
+        """State of the caller's member i, split from its pack."""
+        for k, g in enumerate(self.groups):
+            if i in g:
+                pack = self.packs[k]
+                return pack.split_state(Ensemble.member(self, k).state(mask))[g.index(i)]
+        raise IndexError(i)
+

@@ -21,8 +21,13 @@ class GpuModel:
         self.arrays = case.new_state_arrays()
         st = case.state_struct(self.arrays, case.params.time_jd0, lfirst=1)
         h = C.c_void_p()
-        abi.check(self.lib.fesomc_gpu_init(C.byref(case.mesh.c), C.byref(case.params), C.byref(st), C.byref(h)),
-                  "fesomc_gpu_init")
+        members = getattr(case, "members", None)   # packed members (packed.PackedCase)
+        if members is not None:
+            abi.check(self.lib.fesomc_gpu_init_packed(C.byref(case.mesh.c), C.byref(case.params), C.byref(st),
+                                                      C.byref(members), C.byref(h)), "fesomc_gpu_init_packed")
+        else:
+            abi.check(self.lib.fesomc_gpu_init(C.byref(case.mesh.c), C.byref(case.params), C.byref(st), C.byref(h)),
+                      "fesomc_gpu_init")
         self.h = h
         self.time_jd = case.params.time_jd0
         self.nstep = 0

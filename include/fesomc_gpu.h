@@ -391,6 +391,30 @@ int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, in
 int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_t nsteps, double *ms,
                          int32_t *status);
 
+/* Packed members: several meshes advanced as one model, so that every
+ * kernel of a step covers all members in one launch.  The caller
+ * concatenates the members' fesomc_mesh arrays (indices offset; all
+ * members' internal edges first, then all boundary edges), fesomc_state
+ * and fesomc_forcing arrays in member order; the members share nsigma,
+ * sigma and every fesomc_params field except scale_area, given per member
+ * here.  Each member then advances bit for bit as it does alone: the tracer
+ * means of solve_tracers (fv_tracer.F90:18-27) and scale_area are taken per
+ * member.  No counterpart in the reference, which runs one mesh per
+ * executable. */
+typedef struct fesomc_members {
+    int32_t n;                    /* members                                       */
+    const int32_t *node_off;      /* (n+1) first node of each member, 0-based; node_off[n] = nod2D */
+    const int32_t *elem_off;      /* (n+1) first element of each member; elem_off[n] = elem2D */
+    const double *scale_area;     /* (n) sum(elem_area)/elem2D of each member (fv_ini.F90:81) */
+} fesomc_members;
+
+/* fesomc_gpu_init for a packed mesh; members = NULL or n = 1 is one mesh.
+ * Returns FESOMC_EINVAL when the ranges do not start at 0, grow strictly and
+ * end at nod2D / elem2D, when a scale_area is not positive, or when an
+ * element, edge or node-element list reaches into another member. */
+int  fesomc_gpu_init_packed(const fesomc_mesh *mesh, const fesomc_params *par, const fesomc_state *st,
+                            const fesomc_members *members, fesomc_model **out);
+
 /* Selects the CUDA device used by subsequent fesomc_gpu_init calls of the
  * calling thread (one process per GPU).  No counterpart in the reference,
  * where each MPI rank owns a mesh partition instead. */
