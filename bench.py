@@ -263,7 +263,13 @@ def run_ours(args, ws, rank, local):
     cfg = args.config
     case = build_case(cfg)
     case.params.fp32_form = 1 if args.fp32_form else 0
+    shapes, tune_rep = None, None
+    if args.launch_shapes != "default":
+        from fesomc import autotune
+        shapes, tune_rep = autotune.shapes_for(case, refresh=args.launch_shapes == "search")
     g = model.GpuModel(case)
+    if shapes:
+        autotune.apply(g, shapes)
     m = case.mesh
     units_per_step = m.N * m.L
     barrier, max_over_ranks = reps.barrier, reps.max
@@ -354,6 +360,7 @@ def run_ours(args, ws, rank, local):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1000.0 * t_e2e / args.steps},
         "gpu_launches": int(timed_launches),
+        "launch_shapes": {"source": args.launch_shapes, "shapes": shapes, "tuning": tune_rep},
         "roofline": roof,
         "kernels": [{k: (round(v, 6) if isinstance(v, float) else v) for k, v in kk.items()} for kk in kernels],
     }
@@ -730,6 +737,9 @@ def main():
     ap.add_argument("--lc-judge", type=int, default=100)
     ap.add_argument("--lc-infer", type=int, default=0, help="time the closure inference on this many columns")
     ap.add_argument("--sfc-order", action="store_true", help="store the mesh along a Hilbert curve on the device")
+    ap.add_argument("--launch-shapes", default="tuned", choices=["default", "tuned", "search"],
+                    help="kernel launch shapes: built-in defaults, the autotuner's (cached, searched when "
+                         "absent), or a fresh search")
     ap.add_argument("--shuffle", type=int, default=None, help="number the mesh's nodes and elements at random (seed)")
     args = ap.parse_args()
     if args.sfc_order:

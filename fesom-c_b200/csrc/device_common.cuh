@@ -1,6 +1,7 @@
 // Shared device-side definitions of the B200 FESOM-C time step.
 //
-// Layout in HBM (device order == reference order in this version):
+// Layout in HBM (device order: the reference order, or with sfc_order the
+// order of a Hilbert curve through the mesh, every index translated):
 //   * 2D node / element fields: one double per entity.
 //   * 2D vectors (U_n_2D, UAB, ...): double2 per element (u, v interleaved,
 //     as the Fortran (2,E) arrays).
@@ -70,6 +71,17 @@ __host__ __device__ __forceinline__ double4 make_real4(double x, double y, doubl
 __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z, float w) {
     return make_float4(x, y, z, w);
 }
+
+// Launch-shape knobs (fesomc_gpu_tune_*): threads per block of the kernels
+// whose results do not depend on the block shape (one thread per entity or
+// per (entity, level), grid-stride, no block-level reduction), and entities
+// per block of the column kernels (pressure_col, bpg_elem, update3d, wvel).
+// A value of 0 selects the built-in default.
+enum TuneKnob : int {
+    TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_P1EDGE, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
+    TK_SSHNODE, TK_ADV2D, TK_U2D, TK_ROT, TK_ZEROFILT, TK_AB2, TK_MEGRAD, TK_MNGRAD, TK_MEDGE, TK_MH,
+    TK_UPWIND, TK_AV, TK_COLUMNS, kTuneKnobs
+};
 
 namespace f64 {
 using real = double;

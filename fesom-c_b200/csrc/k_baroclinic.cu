@@ -875,7 +875,11 @@ __global__ void k_wvel(Dev d) {
 
 // ---- launch wrappers --------------------------------------------------------
 // column blocks: B = min(16, 1024 / L) entities, B * L threads
-static int col_b(const Dev &d) { int b = 1024 / d.L; return b > 16 ? 16 : b; }
+static int col_b(const Dev &d) {
+    if (d.tune[TK_COLUMNS] > 0) return d.tune[TK_COLUMNS];
+    int b = 1024 / d.L;
+    return b > 16 ? 16 : b;
+}
 static int col_grid(const Dev &d, long long count) {
     const long long blocks = (count + col_b(d) - 1) / col_b(d);
     return (int)(blocks < 148LL * 8 ? blocks : 148LL * 8);
@@ -899,10 +903,12 @@ void launch_bpg_elem(const Dev &d, cudaStream_t s) {
     k_bpg_elem<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, 0), s>>>(d);
 }
 void launch_velgrad3d(const Dev &d, cudaStream_t s) {
-    k_velgrad3d<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_VELGRAD3D, 256);
+    k_velgrad3d<<<grid_for((long long)d.E * d.L, b), b, 0, s>>>(d);
 }
 void launch_adv3_edge(const Dev &d, cudaStream_t s) {
-    k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_ADV3, 256);
+    k_adv3_edge<<<grid_for((long long)d.Ed_in * d.L, b), b, 0, s>>>(d);
 }
 void launch_filt2x(const Dev &d, cudaStream_t s) {
     k_filt2x_uc<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
@@ -923,7 +929,8 @@ void launch_bih_puls(const Dev &d, cudaStream_t s) {
     k_bih_edge<<<ge, 256, 0, s>>>(d, d.bihU, d.bihV, 2);
 }
 void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
-    k_velrhs<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d, ff);
+    const int b = tuned(d, TK_VELRHS, 256);
+    k_velrhs<<<grid_for((long long)d.E * d.L, b), b, 0, s>>>(d, ff);
 }
 #define MAXL_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                                   \
     do {                                                                                   \
@@ -938,5 +945,18 @@ void launch_update3d(const Dev &d, real Mt_inv, cudaStream_t s) {
     k_update3d<<<col_grid(d, d.E), col_b(d) * d.L, col_smem(d, 2, kU3Sc), s>>>(d, Mt_inv);
 }
 void launch_wvel(const Dev &d, cudaStream_t s) { k_wvel<<<col_grid(d, d.N), col_b(d) * d.L, col_smem(d, 1, 2), s>>>(d); }
+
+
+// Largest block (threads) each tunable kernel of this file can launch with
+// (its registers and launch bounds): lim[knob] lowered to that.
+static void tune_lower(int *lim, int knob, const void *k) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k) == cudaSuccess && a.maxThreadsPerBlock < lim[knob]) lim[knob] = a.maxThreadsPerBlock;
+}
+void tune_limits_baroclinic(int *lim) {
+    tune_lower(lim, TK_VELRHS, (const void *)k_velrhs);
+    tune_lower(lim, TK_VELGRAD3D, (const void *)k_velgrad3d);
+    tune_lower(lim, TK_ADV3, (const void *)k_adv3_edge);
+}
 
 FESOMC_PREC_END

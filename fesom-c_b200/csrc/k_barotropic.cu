@@ -602,18 +602,22 @@ __global__ void k_zero_filt(Dev d) {
 
 // ---- launch wrappers --------------------------------------------------------
 void launch_ab3_elem(const Dev &d, cudaStream_t s) {
-    k_ab3_elem<<<grid_for(d.E, 256), 256, 0, s>>>(d);
-    k_velgrad2d<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.UAB);
+    const int b1 = tuned(d, TK_AB3, 256), b2 = tuned(d, TK_VELGRAD2D, 256);
+    k_ab3_elem<<<grid_for(d.E, b1), b1, 0, s>>>(d);
+    k_velgrad2d<<<grid_for(d.E, b2), b2, 0, s>>>(d, d.UAB);
 }
 void launch_ssh_node(const Dev &d, int sub, cudaStream_t s) {
-    k_ssh_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d);
-    k_ssh_node<<<grid_for(d.N, 256), 256, 0, s>>>(d, sub);
+    const int b1 = tuned(d, TK_SSHEDGE, 256), b2 = tuned(d, TK_SSHNODE, 256);
+    k_ssh_edge<<<grid_for(d.Ed, b1), b1, 0, s>>>(d);
+    k_ssh_node<<<grid_for(d.N, b2), b2, 0, s>>>(d, sub);
 }
 void launch_puls_elem(const Dev &d, cudaStream_t s) {
-    k_puls_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_PULS, 256);
+    k_puls_elem<<<grid_for((long long)d.E * d.L, b), b, 0, s>>>(d);
 }
 void launch_el2nodes(const Dev &d, const real *Ue, const real *Ve, real *Un, real *Vn, cudaStream_t s) {
-    k_el2nodes<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d, Ue, Ve, Un, Vn);
+    const int b = tuned(d, TK_EL2NODES, 256);
+    k_el2nodes<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d, Ue, Ve, Un, Vn);
 }
 // B elements per block: B*L threads, at most 1024 and at most 32 elements;
 // per element its slot tile, 8 slot sums, 4 acc, dmean_n and 4 edge codes
@@ -627,14 +631,18 @@ int config_p1(const Dev &d) {
                ? 0 : 1;
 }
 void launch_p1_edge(const Dev &d, cudaStream_t s) {
-    k_p1_edge<<<grid_for((long long)d.Ed_in * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_P1EDGE, 256);
+    k_p1_edge<<<grid_for((long long)d.Ed_in * d.L, b), b, 0, s>>>(d);
 }
 void launch_p1_elem(const Dev &d, cudaStream_t s) {
     const int B = p1_elems(d);
     const long long blocks = ((long long)d.E + B - 1) / B;
     k_p1_elem<<<(int)(blocks < 148LL * 16 ? blocks : 148LL * 16), B * d.L, p1_smem(d), s>>>(d);
 }
-void launch_adv2d_edge(const Dev &d, cudaStream_t s) { k_adv2d_edge<<<grid_for(d.Ed_in, 256), 256, 0, s>>>(d); }
+void launch_adv2d_edge(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_ADV2D, 256);
+    k_adv2d_edge<<<grid_for(d.Ed_in, b), b, 0, s>>>(d);
+}
 void launch_filt2x_2d(const Dev &d, cudaStream_t s) { k_filt2x_2d<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
 void launch_bih_2d(const Dev &d, cudaStream_t s) {
     k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.UAB);
@@ -642,8 +650,38 @@ void launch_bih_2d(const Dev &d, cudaStream_t s) {
     k_velgrad2d<<<grid_for(d.E, 256), 256, 0, s>>>(d, d.b2ul);
     k_bih2d_edge<<<grid_for(d.Ed, 256), 256, 0, s>>>(d, d.b2ul);
 }
-void launch_u2d_elem(const Dev &d, cudaStream_t s) { k_u2d_elem<<<grid_for(d.E, 128), 128, 0, s>>>(d); }
-void launch_rot_nodes(const Dev &d, cudaStream_t s) { k_rot_nodes<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
-void launch_zero_filt(const Dev &d, cudaStream_t s) { k_zero_filt<<<grid_for(d.E, 256), 256, 0, s>>>(d); }
+void launch_u2d_elem(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_U2D, 128);
+    k_u2d_elem<<<grid_for(d.E, b), b, 0, s>>>(d);
+}
+void launch_rot_nodes(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_ROT, 256);
+    k_rot_nodes<<<grid_for(d.N, b), b, 0, s>>>(d);
+}
+void launch_zero_filt(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_ZEROFILT, 256);
+    k_zero_filt<<<grid_for(d.E, b), b, 0, s>>>(d);
+}
+
+
+// Largest block (threads) each tunable kernel of this file can launch with
+// (its registers and launch bounds): lim[knob] lowered to that.
+static void tune_lower(int *lim, int knob, const void *k) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k) == cudaSuccess && a.maxThreadsPerBlock < lim[knob]) lim[knob] = a.maxThreadsPerBlock;
+}
+void tune_limits_barotropic(int *lim) {
+    tune_lower(lim, TK_AB3, (const void *)k_ab3_elem);
+    tune_lower(lim, TK_VELGRAD2D, (const void *)k_velgrad2d);
+    tune_lower(lim, TK_SSHEDGE, (const void *)k_ssh_edge);
+    tune_lower(lim, TK_SSHNODE, (const void *)k_ssh_node);
+    tune_lower(lim, TK_PULS, (const void *)k_puls_elem);
+    tune_lower(lim, TK_EL2NODES, (const void *)k_el2nodes);
+    tune_lower(lim, TK_P1EDGE, (const void *)k_p1_edge);
+    tune_lower(lim, TK_ADV2D, (const void *)k_adv2d_edge);
+    tune_lower(lim, TK_U2D, (const void *)k_u2d_elem);
+    tune_lower(lim, TK_ROT, (const void *)k_rot_nodes);
+    tune_lower(lim, TK_ZEROFILT, (const void *)k_zero_filt);
+}
 
 FESOMC_PREC_END

@@ -241,6 +241,20 @@ void launch_d3end(const Dev &d, cudaStream_t s) {
 void launch_d3end_list(const Dev &d, const int *list, const unsigned long long *count, cudaStream_t s) {
     k_d3end<true><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, list, count);
 }
-void launch_av(const Dev &d, cudaStream_t s) { k_av<<<grid_for((long long)d.E * d.NS, 256), 256, 0, s>>>(d); }
+void launch_av(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_AV, 256);
+    k_av<<<grid_for((long long)d.E * d.NS, b), b, 0, s>>>(d);
+}
+
+
+// Largest block (threads) each tunable kernel of this file can launch with
+// (its registers and launch bounds): lim[knob] lowered to that.
+static void tune_lower(int *lim, int knob, const void *k) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k) == cudaSuccess && a.maxThreadsPerBlock < lim[knob]) lim[knob] = a.maxThreadsPerBlock;
+}
+void tune_limits_mixing(int *lim) {
+    tune_lower(lim, TK_AV, (const void *)k_av);
+}
 
 FESOMC_PREC_END

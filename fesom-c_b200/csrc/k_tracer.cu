@@ -957,15 +957,21 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
     k_minmax_part<<<dim3(parts, d.n_members), kRedBlock, 0, s>>>(d);
     k_minmax_final<<<d.n_members, 32, 0, s>>>(d, parts);
 }
-void launch_ab2(const Dev &d, cudaStream_t s) { k_ab2_node<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d); }
+void launch_ab2(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_AB2, 256);
+    k_ab2_node<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
+}
 void launch_upwind(const Dev &d, cudaStream_t s) {
-    k_upwind_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
+    const int b = tuned(d, TK_UPWIND, 128);
+    k_upwind_h<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
 }
 void launch_muscl_egrad(const Dev &d, cudaStream_t s) {
-    k_muscl_egrad<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_MEGRAD, 256);
+    k_muscl_egrad<<<grid_for((long long)d.E * d.L, b), b, 0, s>>>(d);
 }
 void launch_muscl_ngrad(const Dev &d, cudaStream_t s) {
-    k_muscl_ngrad<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_MNGRAD, 256);
+    k_muscl_ngrad<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
 }
 void launch_miura(const Dev &d, cudaStream_t s) {
     k_miura_prep<<<grid_for((long long)d.N * d.L, 256), 256, 0, s>>>(d);
@@ -975,10 +981,12 @@ void launch_miura(const Dev &d, cudaStream_t s) {
     k_miura_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
 }
 void launch_muscl_edge(const Dev &d, cudaStream_t s) {
-    k_muscl_edge<<<grid_for((long long)d.Ed * d.L, 256), 256, 0, s>>>(d);
+    const int b = tuned(d, TK_MEDGE, 256);
+    k_muscl_edge<<<grid_for((long long)d.Ed * d.L, b), b, 0, s>>>(d);
 }
 void launch_muscl_h(const Dev &d, cudaStream_t s) {
-    k_muscl_h<<<grid_for((long long)d.N * d.L, 128), 128, 0, s>>>(d);
+    const int b = tuned(d, TK_MH, 128);
+    k_muscl_h<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
 }
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
@@ -994,6 +1002,22 @@ int energy_parts() { return kRedGrid; }
 void launch_energy(const Dev &d, double *part, double *out, cudaStream_t s) {
     k_energy_part<<<kRedGrid, kRedBlock, 0, s>>>(d, part);
     k_energy_final<<<1, 32, 0, s>>>(part, kRedGrid, out);
+}
+
+
+// Largest block (threads) each tunable kernel of this file can launch with
+// (its registers and launch bounds): lim[knob] lowered to that.
+static void tune_lower(int *lim, int knob, const void *k) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, k) == cudaSuccess && a.maxThreadsPerBlock < lim[knob]) lim[knob] = a.maxThreadsPerBlock;
+}
+void tune_limits_tracer(int *lim) {
+    tune_lower(lim, TK_AB2, (const void *)k_ab2_node);
+    tune_lower(lim, TK_MEGRAD, (const void *)k_muscl_egrad);
+    tune_lower(lim, TK_MNGRAD, (const void *)k_muscl_ngrad);
+    tune_lower(lim, TK_MEDGE, (const void *)k_muscl_edge);
+    tune_lower(lim, TK_MH, (const void *)k_muscl_h);
+    tune_lower(lim, TK_UPWIND, (const void *)k_upwind_h);
 }
 
 FESOMC_PREC_END

@@ -66,6 +66,10 @@ namespace fesomc {
     void launch_lc_judge(const Dev &, const LcView &, cudaStream_t); \
     int energy_parts(); \
     int minmax_parts(int); \
+    void tune_limits_baroclinic(int *); \
+    void tune_limits_barotropic(int *); \
+    void tune_limits_tracer(int *); \
+    void tune_limits_mixing(int *); \
     void launch_energy(const Dev &, double *, double *, cudaStream_t);
 namespace f64 {
 FESOMC_KERNEL_LAUNCHERS
@@ -1804,6 +1808,77 @@ int fesomc_ensemble_run(fesomc_model *const *members, int32_t n, int32_t nsteps,
         if (first == FESOMC_OK) first = rc;
     }
     return first;
+}
+
+// ---- launch-shape knobs -----------------------------------------------------
+namespace {
+struct KnobInfo {
+    const char *name;      // the kernel (or kernel group) the knob shapes
+    const char *records;   // the fesomc_gpu_profile records that time it
+    int def;               // default threads per block (0: column entities per block)
+};
+const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
+    {"velrhs", "velrhs", 256}, {"velgrad3d", "velgrad3d", 256}, {"adv3_edge", "adv3_edge", 256},
+    {"puls_elem", "puls_elem", 256}, {"el2nodes", "el2nodes,el2nodes_p", 256}, {"p1_edge", "p1_edge", 256},
+    {"ab3_elem", "ab3_elem", 256}, {"velgrad2d", "ab3_elem", 256}, {"ssh_edge", "ssh_node", 256},
+    {"ssh_node", "ssh_node", 256}, {"adv2d_edge", "adv2d_edge", 256}, {"u2d_elem", "u2d_elem", 128},
+    {"rot_nodes", "rot_nodes", 256}, {"zero_filt", "zero_filt", 256}, {"ab2_node", "ab2_node", 256},
+    {"muscl_egrad", "muscl_egrad", 256}, {"muscl_ngrad", "muscl_ngrad", 256}, {"muscl_edge", "muscl_edge", 256},
+    {"muscl_h", "muscl_h", 128}, {"upwind_h", "upwind_h", 128}, {"av", "av", 256},
+    {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
+};
+int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
+void drop_graph(fesomc_model *m);
+int copy_str(const char *src, char *dst, int32_t len) {
+    if (!dst) return FESOMC_OK;
+    if (len < 1 || (int32_t)std::strlen(src) >= len) return FESOMC_EINVAL;
+    std::strcpy(dst, src);
+    return FESOMC_OK;
+}
+}  // namespace
+
+int fesomc_gpu_tune_knobs(void) { return fesomc::kTuneKnobs; }
+
+int fesomc_gpu_tune_knob(int32_t k, char *name, int32_t name_len, char *records, int32_t records_len) {
+    if (k < 0 || k >= fesomc::kTuneKnobs) return FESOMC_EINVAL;
+    int rc = copy_str(kKnobs[k].name, name, name_len);
+    return rc ? rc : copy_str(kKnobs[k].records, records, records_len);
+}
+
+int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
+    if (!m || (!values && !limits)) return FESOMC_EINVAL;
+    int lim[fesomc::kTuneKnobs];
+    for (int k = 0; k < fesomc::kTuneKnobs; ++k) lim[k] = 1024;
+    fesomc::f64::tune_limits_baroclinic(lim); fesomc::f64::tune_limits_barotropic(lim);
+    fesomc::f64::tune_limits_tracer(lim); fesomc::f64::tune_limits_mixing(lim);
+    fesomc::f32::tune_limits_baroclinic(lim); fesomc::f32::tune_limits_barotropic(lim);
+    fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
+    lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
+    for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
+        if (values) {
+            const int v = m->d.tune[k];
+            values[k] = v > 0 ? v : (kKnobs[k].def > 0 ? kKnobs[k].def : default_columns(m->d.L));
+        }
+        if (limits) limits[k] = k == fesomc::TK_COLUMNS ? lim[k] : (lim[k] / 32) * 32;
+    }
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_tune_set(fesomc_model *m, const int32_t *values) {
+    if (!m || !values) return FESOMC_EINVAL;
+    int32_t lim[fesomc::kTuneKnobs];
+    int rc = fesomc_gpu_tune_get(m, nullptr, lim);
+    if (rc) return rc;
+    for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
+        const int v = values[k];
+        if (v < 0 || v > lim[k]) return FESOMC_EINVAL;
+        if (k != fesomc::TK_COLUMNS && v != 0 && (v < 32 || v % 32 != 0)) return FESOMC_EINVAL;
+    }
+    drop_graph(m);   // the captured step holds the old launch shapes
+    for (int k = 0; k < fesomc::kTuneKnobs; ++k) m->d.tune[k] = m->d32.tune[k] = values[k];
+    // the column kernels' shared memory follows their entities per block
+    const int bad = m->fp32 ? fesomc::f32::config_columns(m->d32) : fesomc::f64::config_columns(m->d);
+    return bad ? FESOMC_EINVAL : FESOMC_OK;
 }
 
 // ---- learned vertical-mixing closure ---------------------------------------

@@ -118,6 +118,10 @@ SIGNATURES = {
     "fesomc_gpu_profile": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, i32p, C.c_char_p, f64p, f64p,
                                      C.POINTER(C.c_int64)]),
     "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),
+    "fesomc_gpu_tune_knobs": (C.c_int, []),
+    "fesomc_gpu_tune_knob": (C.c_int, [C.c_int32, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32]),
+    "fesomc_gpu_tune_get": (C.c_int, [C.c_void_p, i32p, i32p]),
+    "fesomc_gpu_tune_set": (C.c_int, [C.c_void_p, i32p]),
     "fesomc_gpu_init_packed": (C.c_int, [C.POINTER(Mesh), C.POINTER(Params), C.POINTER(State), C.POINTER(Members),
                                          C.POINTER(C.c_void_p)]),
     "fesomc_gpu_set_device": (C.c_int, [C.c_int32]),

@@ -391,6 +391,26 @@ int  fesomc_gpu_profile(fesomc_model *m, int32_t nsteps, int32_t max_kernels, in
 int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_t nsteps, double *ms,
                          int32_t *status);
 
+/* Launch shapes.  A knob is the threads per block of one kernel whose
+ * results do not depend on the block shape (one thread per entity or per
+ * (entity, level), grid-stride, no block-level reduction), or ("columns")
+ * the nodes / elements per block of the column kernels; any setting gives
+ * the same bits.  fesomc_gpu_tune_knobs returns the number of knobs;
+ * fesomc_gpu_tune_knob their names and the fesomc_gpu_profile records that
+ * time each (comma-separated; buffers of *_len bytes, NULL to skip).
+ * fesomc_gpu_tune_get fills values (the shapes in use) and limits (the
+ * largest each knob accepts on this device), either may be NULL.
+ * fesomc_gpu_tune_set takes one value per knob (0 = the default) and
+ * returns FESOMC_EINVAL, changing nothing, when a thread count is not a
+ * multiple of 32 or a value exceeds its limit; the next step captures its
+ * graph again.  The search over the knobs and its cache per mesh size and
+ * level count live with the host driver (fesomc/autotune.py).  No
+ * counterpart in the reference. */
+int  fesomc_gpu_tune_knobs(void);
+int  fesomc_gpu_tune_knob(int32_t k, char *name, int32_t name_len, char *records, int32_t records_len);
+int  fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits);
+int  fesomc_gpu_tune_set(fesomc_model *m, const int32_t *values);
+
 /* Packed members: several meshes advanced as one model, so that every
  * kernel of a step covers all members in one launch.  The caller
  * concatenates the members' fesomc_mesh arrays (indices offset; all
