@@ -266,7 +266,10 @@ def run_ours(args, ws, rank, local):
     shapes, tune_rep = None, None
     if args.launch_shapes != "default":
         from fesomc import autotune
-        shapes, tune_rep = autotune.shapes_for(case, refresh=args.launch_shapes == "search")
+        try:
+            shapes, tune_rep = autotune.shapes_for(case, refresh=args.launch_shapes == "search")
+        except Exception as ex:        # timing stays valid with the default shapes
+            shapes, tune_rep = None, {"error": repr(ex)}
     g = model.GpuModel(case)
     if shapes:
         autotune.apply(g, shapes)

@@ -25,6 +25,8 @@ namespace fesomc {
 
 constexpr int kLcHidden = 256;
 constexpr float kLcX0 = 1.0e-6f;
+// fallback rules beyond the training envelope (fesomc_closure_set_rules)
+constexpr int kLcRuleUnstable = 1;   // N^2 < 0 at an interior interface: the plain closure
 
 inline int lc_in(int NS) { return 3 * NS + 3; }
 inline int lc_out(int NS) { return 2 * NS; }
@@ -34,6 +36,7 @@ inline int lc_out(int NS) { return 2 * NS; }
 // precision and read these through a plain struct
 struct LcView {
     int NS, IN, OUT;
+    int rules;                                // kLcRule* bits
     const float *mu_x, *sd_x, *mu_y, *sd_y;   // normalisation (IN / OUT)
     const float *lo_x, *hi_x;                 // training envelope of the normalised inputs
     float *X;                                 // per node: normalised inputs (N x IN), FP32

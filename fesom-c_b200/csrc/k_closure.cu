@@ -70,6 +70,9 @@ __global__ void k_lc_features(Dev d, LcView c) {
         lc_inputs(d, node, x);
         const bool wet = d.mask_wd_node[node] != real(0.0);
         bool in = true;
+        // statically unstable column (a negative N^2 input, sign kept by asinh)
+        if (c.rules & kLcRuleUnstable)
+            for (int k = 1; k <= c.NS - 2; ++k) in = in && !(x[c.NS + k] < 0.0f);
         for (int j = 0; j < c.IN; ++j) {
             const float v = (x[j] - c.mu_x[j]) / c.sd_x[j];
             x[j] = v;

@@ -22,6 +22,7 @@ struct LcNet {
     long long np = 0;             // parameters
     float *params = nullptr, *grads = nullptr, *mom = nullptr, *var = nullptr;
     int adam_t = 0;
+    int rules = 0;                // fallback rules (kLcRule*) the model applies with this network
     // statistics, W = max(IN, OUT)-strided: mu_x, sd_x, mu_y, sd_y, lo_x, hi_x
     float *stats = nullptr;
     std::vector<float> h_stats;

@@ -2113,6 +2113,7 @@ int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_ever
     if (bf16 && (rc = lc_tc_prepare(c->net))) return rc;
     if (!bf16 && (rc = lc_fp32_buffers(m))) return rc;
     m->lc_bf16 = bf16 != 0;
+    m->lcv.rules = c->net->rules;
     CK(cudaMemset(m->lcv.acc, 0, 4 * sizeof(unsigned long long)));
     CK(cudaMemset(m->lcv.judge, 0, 3 * sizeof(double)));
     m->lc = c->net;
@@ -2120,6 +2121,12 @@ int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_ever
     m->lc_judge_every = judge_every;
     m->lc_steps = 0;
     m->lc_judges = 0;
+    return FESOMC_OK;
+}
+
+int fesomc_closure_set_rules(fesomc_closure *c, int32_t rules) {
+    if (!c || (rules & ~fesomc::kLcRuleUnstable)) return FESOMC_EINVAL;
+    c->net->rules = rules;
     return FESOMC_OK;
 }
 

@@ -119,6 +119,7 @@ SIGNATURES = {
                                      C.POINTER(C.c_int64)]),
     "fesomc_ensemble_run": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, f64p, i32p]),
     "fesomc_gpu_tune_knobs": (C.c_int, []),
+    "fesomc_closure_set_rules": (C.c_int, [C.c_void_p, C.c_int32]),
     "fesomc_gpu_tune_knob": (C.c_int, [C.c_int32, C.c_char_p, C.c_int32, C.c_char_p, C.c_int32]),
     "fesomc_gpu_tune_get": (C.c_int, [C.c_void_p, i32p, i32p]),
     "fesomc_gpu_tune_set": (C.c_int, [C.c_void_p, i32p]),

@@ -37,6 +37,11 @@ class Closure:
         model.nstep += nsteps
         abi.check(rc, "fesomc_closure_harvest")
 
+    def set_rules(self, unstable=False):
+        """Fallback rules beyond the envelope, used from the next attach on:
+        unstable -- statically unstable columns (N^2 < 0) to the plain closure."""
+        abi.check(self.lib.fesomc_closure_set_rules(self.h, 1 if unstable else 0), "fesomc_closure_set_rules")
+
     def fit(self):
         abi.check(self.lib.fesomc_closure_fit(self.h), "fesomc_closure_fit")
 

@@ -525,6 +525,14 @@ int  fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_eve
  * events); bf16 selects the tensor-core kernel. */
 int  fesomc_closure_time(fesomc_closure *c, int64_t n, int32_t reps, int32_t bf16, double *ms);
 int  fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r);
+/* fesomc_closure_set_rules: fallback rules the model applies, beyond the
+ * training envelope, with this network from the next fesomc_closure_attach
+ * on.  FESOMC_LC_RULE_UNSTABLE (1): a column with N^2 < 0 at an interior
+ * interface (statically unstable, convecting) goes to the plain closure;
+ * such columns are counted as out of the envelope.  Other bits:
+ * FESOMC_EINVAL. */
+#define FESOMC_LC_RULE_UNSTABLE 1
+int  fesomc_closure_set_rules(fesomc_closure *c, int32_t rules);
 
 /* ---- version / introspection --------------------------------------------- */
 const char *fesomc_gpu_version(void);
