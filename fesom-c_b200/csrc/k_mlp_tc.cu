@@ -3,27 +3,38 @@
 // counterpart in the reference; the network stands in for d3_end
 // (src/fv_mixing.F90:73-347).
 //
-// One persistent CTA per SM (128 threads, 4 warps) walks 128-column tiles.
-// Per tile: the normalised inputs (FP32) are converted to BF16 into shared
-// memory; four layers of tcgen05.mma (M = 128 columns, N = output neurons,
-// K = 16 per instruction) accumulate in TMEM (256 of the SM's 512 columns);
-// after each layer the four warps read their 32 TMEM lanes (tcgen05.ld),
-// add the bias, apply SiLU and write the BF16 activations back to shared
-// memory as the next layer's A operand; the last layer's FP32 outputs go to
-// global memory.  W1 and W4 stay in shared memory for the kernel's life;
-// W2 and W3 (128 KB each) stream through one 64 KB buffer in halves of 128
-// output neurons (they stay in L2, every CTA reads the same 256 KB).
+// One persistent CTA per SM walks 128-column tiles with specialised warps:
+//   warp 0       producer: streams the weights, unit by unit, from global
+//                memory (L2-resident: every CTA reads the same ~330 KB) into
+//                a ring of kSlots shared-memory slots with bulk copies
+//                (cp.async.bulk, completion counted on the slot's mbarrier);
+//   warp 1       MMA issuer (one lane): per layer and unit, K/16
+//                tcgen05.mma (M = 128 columns, N = 64 neurons, K = 16) into
+//                tensor memory, a commit that frees the slot, and after the
+//                layer's last unit a commit that hands the accumulator over;
+//   warps 4..    epilogue (kEpiWarps warps, kEpiWarps/4 per TMEM lane
+//                quarter, each a share of the accumulator columns): the
+//                tile's normalised FP32 inputs to BF16 in shared memory,
+//                then per hidden layer bias + SiLU of the accumulator
+//                (tcgen05.ld) back to shared memory as the next layer's A
+//                operand, and the last layer's FP32 outputs to global memory.
+// The weight units are 64 output neurons x the layer's whole K (W1: 4 units,
+// W2, W3: 4 each, W4: 1 of N4p neurons), so the producer runs up to kSlots
+// units ahead of the MMAs and fetches the next tile's first layer while the
+// epilogue finishes the current tile.
 //
 // Operands use the no-swizzle K-major canonical layout: 8-row x 16-byte
 // core matrices, an operand of R rows stored as K/8 slabs of R x 16 bytes
 // ("chunk-major"): element (r, k) at byte (k/8)*R*16 + r*16 + (k%8)*2.  The
 // descriptor of the k-th 16-wide slice starts at slab 2k, with LBO = R*16
 // (the next 8-wide chunk) and SBO = 128 (the next 8 rows).  The host lays
-// the BF16 weights out the same way, so their copies are contiguous.
+// every weight unit out the same way (R = 64, or N4p for W4), so a unit is
+// one contiguous bulk copy.
 //
-// Every wait on the MMA-completion barrier is bounded; a CTA whose MMAs do
-// not complete in about a second sets the error word, frees its tensor
-// memory and returns.
+// Every wait on an mbarrier is bounded (about a second); a role that gives
+// up sets the CTA's failure flag and the error word, the others see the flag
+// and stop, and the CTA waits (bounded) for its own copies and MMAs in
+// flight before it frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -37,21 +48,37 @@
 namespace fesomc {
 namespace {
 
-constexpr int kTM = 128;                 // columns per tile (MMA M)
-constexpr int kThreads = 128;
-constexpr int kSlab = kTM * 16;          // bytes of one 8-wide K chunk of a 128-row operand
+constexpr int kTM = 128;                  // columns per tile (MMA M)
+constexpr int kUnitN = 64;                // output neurons per weight unit (MMA N)
+constexpr int kSlots = 4;                 // weight slots in shared memory
+constexpr int kSlotBytes = kUnitN * 256 * 2;
+constexpr int kEpiWarps = 8;              // 2 per TMEM lane quarter
+constexpr int kEpiThreads = 32 * kEpiWarps;
+constexpr int kThreads = 128 + kEpiThreads;
+constexpr int kSlab = kTM * 16;           // bytes of one 8-wide K chunk of the 128-row A operand
 constexpr uint32_t kTmemCols = 256;
+constexpr int kMaxUnits = 16;
+constexpr uint32_t kSpin = 1u << 25;
+// barriers: full[kSlots], empty[kSlots], acc_full, a_ready, drain
+constexpr int kBars = 2 * kSlots + 3;
 
 struct TcParams {
     int IN, OUT, K1p, N4p;
     long long ncol;
     const float *X;                      // ncol x IN, normalised FP32
     float *Y;                            // ncol x OUT, FP32
-    const uint4 *W1, *W2, *W3, *W4;      // BF16, chunk-major
+    const unsigned char *W;              // BF16 weight units, chunk-major, back to back
+    int n_units;
+    int unit_off[kMaxUnits];             // byte offset of unit u in W
+    int unit_bytes[kMaxUnits];
+    int unit_rows[kMaxUnits];            // N of the unit's MMAs
+    int unit_k[kMaxUnits];               // K of the unit (K1p or 256)
+    int unit_col[kMaxUnits];             // first accumulator column of the unit
+    int unit_last[kMaxUnits];            // 1: the last unit of its layer
     const float *b1, *b2, *b3, *b4;
     unsigned int *err;
     // shared-memory offsets (bytes)
-    int oX, oH, oW1, oW4, oWB, oB, oBar;
+    int oH, oW, oB, oBar;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -86,18 +113,37 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 __device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// bounded wait for the barrier phase; false on timeout (about a second)
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase) {
-    for (uint32_t it = 0; it < (1u << 25); ++it) {
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// bulk copy global -> this CTA's shared memory (no multicast), completion
+// counted on bar
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// bounded wait for the completion of the barrier phase of the given parity;
+// false on timeout, or when fail (if given) is set
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, const volatile int *fail) {
+    for (uint32_t it = 0; it < kSpin; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}\n"
             : "=r"(done)
-            : "r"(bar), "r"(phase)
+            : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((it & 255u) == 255u && fail && *fail) return false;
         __nanosleep(32);
     }
     return false;
@@ -120,50 +166,32 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float silu_dev(float z) { return z / (1.0f + expf(-z)); }
+// SiLU with the fast exponential and division (BF16 output: their error,
+// about 1e-6 relative, is far below the BF16 rounding)
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t *>(&h);
 }
 
-// copy n16 16-byte words from global to shared
-__device__ __forceinline__ void copy_words(uint4 *dst, const uint4 *src, int n16) {
-    for (int i = threadIdx.x; i < n16; i += kThreads) dst[i] = __ldg(src + i);
+__device__ __forceinline__ void fail_now(volatile int *fail, unsigned int *err) {
+    *fail = 1;
+    atomicOr(err, 1u);
 }
 
-// bias + SiLU of the 256 accumulator columns of this thread's row, to the
-// BF16 activation operand (row r, chunk-major, 128 rows)
-__device__ __forceinline__ void epi_hidden(uint32_t tbase, unsigned char *H, const float *bias) {
-    const int w = threadIdx.x >> 5, r = threadIdx.x;
-    for (int c0 = 0; c0 < 256; c0 += 32) {
-        float v[32];
-        tmem_ld32(tbase + ((uint32_t)(32 * w) << 16) + (uint32_t)c0, v);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint4 o;
-            o.x = pack_bf16(silu_dev(v[8 * q + 0] + bias[c0 + 8 * q + 0]), silu_dev(v[8 * q + 1] + bias[c0 + 8 * q + 1]));
-            o.y = pack_bf16(silu_dev(v[8 * q + 2] + bias[c0 + 8 * q + 2]), silu_dev(v[8 * q + 3] + bias[c0 + 8 * q + 3]));
-            o.z = pack_bf16(silu_dev(v[8 * q + 4] + bias[c0 + 8 * q + 4]), silu_dev(v[8 * q + 5] + bias[c0 + 8 * q + 5]));
-            o.w = pack_bf16(silu_dev(v[8 * q + 6] + bias[c0 + 8 * q + 6]), silu_dev(v[8 * q + 7] + bias[c0 + 8 * q + 7]));
-            *reinterpret_cast<uint4 *>(H + (size_t)(c0 / 8 + q) * kSlab + (size_t)r * 16) = o;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(TcParams p) {
+__global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char *sX = sm + p.oX, *sH = sm + p.oH, *sW1 = sm + p.oW1, *sW4 = sm + p.oW4, *sWB = sm + p.oWB;
+    unsigned char *sH = sm + p.oH;
     float *sb = reinterpret_cast<float *>(sm + p.oB);          // b1 b2 b3 (256 each), b4 (N4p)
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + p.oBar);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + p.oBar + 8);
-    int *sfail = reinterpret_cast<int *>(sm + p.oBar + 12);
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t bar_a = smem_u32(bar);
+    const uint32_t bar0 = smem_u32(sm + p.oBar);
+    auto full_bar = [&](int s) { return bar0 + 8u * (uint32_t)s; };
+    auto empty_bar = [&](int s) { return bar0 + 8u * (uint32_t)(kSlots + s); };
+    const uint32_t acc_bar = bar0 + 8u * (2 * kSlots), a_bar = acc_bar + 8u, drain_bar = acc_bar + 16u;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + p.oBar + 8 * kBars);
+    volatile int *sfail = reinterpret_cast<volatile int *>(sm + p.oBar + 8 * kBars + 4);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // resident weights and biases
-    copy_words(reinterpret_cast<uint4 *>(sW1), p.W1, 256 * p.K1p * 2 / 16);
-    copy_words(reinterpret_cast<uint4 *>(sW4), p.W4, p.N4p * 256 * 2 / 16);
     for (int i = tid; i < 256; i += kThreads) {
         sb[i] = p.b1[i];
         sb[256 + i] = p.b2[i];
@@ -172,7 +200,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(TcParams p) {
     for (int i = tid; i < p.N4p; i += kThreads) sb[768 + i] = i < p.OUT ? p.b4[i] : 0.0f;
     if (tid == 0) {
         *sfail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+        for (int s = 0; s < kSlots; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        mbar_init(acc_bar, 1);
+        mbar_init(a_bar, kEpiWarps);
+        mbar_init(drain_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -181,117 +215,154 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(TcParams p) {
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    fence_proxy();
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tbase = *tslot;
-    uint32_t phase = 0;
     const long long ntiles = (p.ncol + kTM - 1) / kTM;
-    const uint32_t id256 = idesc_bf16(256), id128 = idesc_bf16(128), idN4 = idesc_bf16(p.N4p);
-    const uint32_t aX = smem_u32(sX), aH = smem_u32(sH), aW1 = smem_u32(sW1), aW4 = smem_u32(sW4), aWB = smem_u32(sWB);
-    bool ok = true;
+    const int U = p.n_units;
 
-    // wait for the MMAs committed so far; all threads agree on the outcome
-    auto wait_mma = [&]() {
-        const bool done = bar_wait(bar_a, phase);
-        phase ^= 1u;
-        if (!done) atomicOr(sfail, 1);
-        __syncthreads();
-        ok = ok && (*sfail == 0);
-        fence_after();
-    };
-
-    for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const long long row0 = tile * kTM;
-        // inputs of this tile to BF16 (zero rows beyond ncol, zero K padding)
-        {
-            const long long row = row0 + tid;
-            const bool valid = row < p.ncol;
-            const float *x = p.X + (valid ? row : 0) * p.IN;
-            for (int kc = 0; kc < p.K1p / 8; ++kc) {
-                float v[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int k = kc * 8 + j;
-                    v[j] = (valid && k < p.IN) ? x[k] : 0.0f;
+    if (warp == 0) {
+        // ---- producer: every unit of every tile of this CTA, in order ----
+        if (lane == 0) {
+            long long g = 0;   // units issued
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+                for (int u = 0; u < U; ++u) {
+                    const int s = (int)(g % kSlots);
+                    const long long n = g / kSlots;
+                    if (n >= 1 && !bar_wait(empty_bar(s), (uint32_t)((n - 1) & 1), sfail)) {
+                        fail_now(sfail, p.err);
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(full_bar(s), (uint32_t)p.unit_bytes[u]);
+                    bulk_g2s(smem_u32(sm + p.oW + s * kSlotBytes), p.W + p.unit_off[u], (uint32_t)p.unit_bytes[u],
+                             full_bar(s));
+                    ++g;
                 }
-                uint4 o;
-                o.x = pack_bf16(v[0], v[1]);
-                o.y = pack_bf16(v[2], v[3]);
-                o.z = pack_bf16(v[4], v[5]);
-                o.w = pack_bf16(v[6], v[7]);
-                *reinterpret_cast<uint4 *>(sX + (size_t)kc * kSlab + (size_t)tid * 16) = o;
+            // every copy issued lands before the CTA may leave: wait for the
+            // phase of each slot's last use (already complete when the MMAs
+            // consumed it)
+            for (int s = 0; s < kSlots; ++s) {
+                const long long uses = g > s ? (g - 1 - s) / kSlots + 1 : 0;
+                if (uses > 0) bar_wait(full_bar(s), (uint32_t)((uses - 1) & 1), nullptr);
             }
         }
-        fence_proxy();
-        fence_before();
-        __syncthreads();
-        // layer 1: [128 x K1p] x [K1p x 256]
-        if (tid == 0) {
-            fence_after();
-            for (int s = 0; s < p.K1p / 16; ++s)
-                mma_bf16(tbase, sdesc(aX + 2 * s * kSlab, kSlab, 128), sdesc(aW1 + 2 * s * 256 * 16, 256 * 16, 128),
-                         id256, s > 0);
-            mma_commit(bar_a);
-        }
-        wait_mma();
-        if (!ok) break;
-        epi_hidden(tbase, sH, sb);
-        // layers 2 and 3: [128 x 256] x [256 x 256], W in two halves of 128 neurons
-        for (int l = 0; l < 2 && ok; ++l) {
-            const uint4 *W = l == 0 ? p.W2 : p.W3;
-            for (int half = 0; half < 2; ++half) {
-                copy_words(reinterpret_cast<uint4 *>(sWB), W + (size_t)half * (128 * 256 * 2 / 16), 128 * 256 * 2 / 16);
-                fence_proxy();
-                wait_ld();
-                fence_before();
-                __syncthreads();
-                if (tid == 0) {
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            long long g = 0, a_uses = 0;
+            bool ok = true;
+            const uint32_t aH = smem_u32(sH);
+            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+                for (int u = 0; u < U; ++u) {
+                    if (u == 0 || p.unit_last[u - 1]) {
+                        // a new layer: its A operand (inputs or activations) is in H
+                        if (!bar_wait(a_bar, (uint32_t)(a_uses & 1), sfail)) {
+                            fail_now(sfail, p.err);
+                            ok = false;
+                            break;
+                        }
+                        ++a_uses;
+                    }
+                    const int s = (int)(g % kSlots);
+                    if (!bar_wait(full_bar(s), (uint32_t)((g / kSlots) & 1), sfail)) {
+                        fail_now(sfail, p.err);
+                        ok = false;
+                        break;
+                    }
                     fence_after();
-                    for (int s = 0; s < 16; ++s)
-                        mma_bf16(tbase + (uint32_t)(128 * half), sdesc(aH + 2 * s * kSlab, kSlab, 128),
-                                 sdesc(aWB + 2 * s * 128 * 16, 128 * 16, 128), id128, s > 0);
-                    mma_commit(bar_a);
+                    const uint32_t aW = smem_u32(sm + p.oW + s * kSlotBytes);
+                    const int R = p.unit_rows[u];
+                    const uint32_t id = idesc_bf16(R);
+                    for (int ks = 0; ks < p.unit_k[u] / 16; ++ks)
+                        mma_bf16(tbase + (uint32_t)p.unit_col[u], sdesc(aH + 2 * ks * kSlab, kSlab, 128),
+                                 sdesc(aW + 2 * ks * R * 16, (uint32_t)R * 16, 128), id, ks > 0);
+                    mma_commit(empty_bar(s));
+                    if (p.unit_last[u]) mma_commit(acc_bar);
+                    ++g;
                 }
-                wait_mma();
-                if (!ok) break;
+            // every MMA issued completes before the tensor memory is freed
+            mma_commit(drain_bar);
+            bar_wait(drain_bar, 0, nullptr);
+        }
+    } else if (warp >= 4) {
+        // ---- epilogue ----
+        const int e = tid - 128;
+        const int q = warp & 3;                     // TMEM lane quarter
+        const int part = (warp - 4) >> 2;           // share of the columns
+        constexpr int nparts = kEpiWarps / 4;
+        const int r = 32 * q + lane;                // tile row of this thread
+        long long acc_uses = 0;
+        bool ok = true;
+        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            const long long row0 = tile * kTM;
+            const long long left = p.ncol - row0;
+            const int nr = left < kTM ? (int)left : kTM;
+            // inputs to BF16 (coalesced over the tile's contiguous rows),
+            // zero K padding; rows beyond ncol keep stale values (their
+            // outputs are not stored)
+            const float *x = p.X + row0 * p.IN;
+            for (int i = e; i < nr * p.IN; i += kEpiThreads) {
+                const int rr = i / p.IN, k = i - rr * p.IN;
+                *reinterpret_cast<__nv_bfloat16 *>(sH + (size_t)(k >> 3) * kSlab + (size_t)rr * 16 + (k & 7) * 2) =
+                    __float2bfloat16_rn(__ldg(x + i));
             }
-            if (!ok) break;
-            epi_hidden(tbase, sH, sb + 256 * (l + 1));
-        }
-        if (!ok) break;
-        fence_proxy();
-        fence_before();
-        __syncthreads();
-        // layer 4: [128 x 256] x [256 x N4p]
-        if (tid == 0) {
-            fence_after();
-            for (int s = 0; s < 16; ++s)
-                mma_bf16(tbase, sdesc(aH + 2 * s * kSlab, kSlab, 128), sdesc(aW4 + 2 * s * p.N4p * 16, p.N4p * 16, 128),
-                         idN4, s > 0);
-            mma_commit(bar_a);
-        }
-        wait_mma();
-        if (!ok) break;
-        {
-            const long long row = row0 + tid;
-            for (int c0 = 0; c0 < p.N4p; c0 += 32) {
-                float v[32];
-                tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-                if (row < p.ncol)
-                    for (int j = 0; j < 32 && c0 + j < p.OUT; ++j) p.Y[row * p.OUT + c0 + j] = v[j] + sb[768 + c0 + j];
+            for (int i = e; i < (p.K1p - p.IN) * kTM; i += kEpiThreads) {
+                const int k = p.IN + i / kTM, rr = i % kTM;
+                *reinterpret_cast<__nv_bfloat16 *>(sH + (size_t)(k >> 3) * kSlab + (size_t)rr * 16 + (k & 7) * 2) =
+                    __float2bfloat16_rn(0.0f);
+            }
+            fence_proxy();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(a_bar);
+            for (int l = 0; l < 4; ++l) {
+                if (!bar_wait(acc_bar, (uint32_t)(acc_uses & 1), sfail)) {
+                    fail_now(sfail, p.err);
+                    ok = false;
+                    break;
+                }
+                ++acc_uses;
+                fence_after();
+                if (l < 3) {
+                    const float *bias = sb + 256 * l;
+                    for (int c0 = 32 * part; c0 < 256; c0 += 32 * nparts) {
+                        float v[32];
+                        tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            uint4 o;
+                            o.x = pack_bf16(silu_fast(v[8 * j + 0] + bias[c0 + 8 * j + 0]),
+                                            silu_fast(v[8 * j + 1] + bias[c0 + 8 * j + 1]));
+                            o.y = pack_bf16(silu_fast(v[8 * j + 2] + bias[c0 + 8 * j + 2]),
+                                            silu_fast(v[8 * j + 3] + bias[c0 + 8 * j + 3]));
+                            o.z = pack_bf16(silu_fast(v[8 * j + 4] + bias[c0 + 8 * j + 4]),
+                                            silu_fast(v[8 * j + 5] + bias[c0 + 8 * j + 5]));
+                            o.w = pack_bf16(silu_fast(v[8 * j + 6] + bias[c0 + 8 * j + 6]),
+                                            silu_fast(v[8 * j + 7] + bias[c0 + 8 * j + 7]));
+                            *reinterpret_cast<uint4 *>(sH + (size_t)(c0 / 8 + j) * kSlab + (size_t)r * 16) = o;
+                        }
+                    }
+                    fence_before();
+                    fence_proxy();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(a_bar);
+                } else {
+                    const long long row = row0 + r;
+                    for (int c0 = 32 * part; c0 < p.N4p; c0 += 32 * nparts) {
+                        float v[32];
+                        tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (row < p.ncol && c0 + j < p.OUT) p.Y[row * p.OUT + c0 + j] = v[j] + sb[768 + c0 + j];
+                    }
+                    fence_before();
+                }
             }
         }
-        fence_before();
-        __syncthreads();
     }
-    if (!ok) {
-        if (tid == 0) atomicOr(p.err, 1u);
-        // a commit that timed out may still complete: wait for it once more
-        // (bounded) before the tensor memory is given back
-        bar_wait(bar_a, phase ^ 1u);
-    }
+    __syncwarp();
     fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -311,56 +382,83 @@ uint16_t bf16_bits(float f) {
     return (uint16_t)(u >> 16);
 }
 
-}  // namespace
+// the weight units of the network, in the order the kernel consumes them
+struct UnitPlan {
+    int n = 0;
+    int off[kMaxUnits], bytes[kMaxUnits], rows[kMaxUnits], k[kMaxUnits], col[kMaxUnits], last[kMaxUnits];
+    int layer[kMaxUnits], first_neuron[kMaxUnits];
+    size_t total = 0;
+};
 
-static size_t tc_smem(int K1p, int N4p, TcParams *o);
-
-// the kernel's shared-memory plan fits one SM (227 KB): nsigma <= 25
-bool lc_tc_supported(const LcNet *n) {
-    const int K1p = (n->IN + 15) / 16 * 16, N4p = (n->OUT + 15) / 16 * 16;
-    return N4p <= 64 && tc_smem(K1p, N4p, nullptr) <= 232448;
+UnitPlan unit_plan(int K1p, int N4p) {
+    UnitPlan u;
+    auto add = [&](int layer, int rows, int k, int col, int first, bool last) {
+        const int i = u.n++;
+        u.off[i] = (int)u.total;
+        u.bytes[i] = rows * k * 2;
+        u.rows[i] = rows;
+        u.k[i] = k;
+        u.col[i] = col;
+        u.last[i] = last ? 1 : 0;
+        u.layer[i] = layer;
+        u.first_neuron[i] = first;
+        u.total += (size_t)u.bytes[i];
+    };
+    for (int j = 0; j < 4; ++j) add(0, kUnitN, K1p, kUnitN * j, kUnitN * j, j == 3);
+    for (int l = 1; l <= 2; ++l)
+        for (int j = 0; j < 4; ++j) add(l, kUnitN, 256, kUnitN * j, kUnitN * j, j == 3);
+    add(3, N4p, 256, 0, 0, true);
+    return u;
 }
 
-static size_t tc_smem(int K1p, int N4p, TcParams *o) {
+size_t tc_smem(TcParams *o) {
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t at = off;
         off += (bytes + 1023) / 1024 * 1024;
         return (int)at;
     };
-    const int oX = take((size_t)kTM * K1p * 2), oH = take((size_t)kTM * 256 * 2), oW1 = take((size_t)256 * K1p * 2),
-              oW4 = take((size_t)N4p * 256 * 2), oWB = take((size_t)128 * 256 * 2),
-              oB = take((size_t)(768 + 64) * 4), oBar = take(64);
+    const int oH = take((size_t)kTM * 256 * 2), oW = take((size_t)kSlots * kSlotBytes),
+              oB = take((size_t)(768 + 64) * 4), oBar = take(8 * kBars + 8);
     if (o) {
-        o->oX = oX; o->oH = oH; o->oW1 = oW1; o->oW4 = oW4; o->oWB = oWB; o->oB = oB; o->oBar = oBar;
+        o->oH = oH; o->oW = oW; o->oB = oB; o->oBar = oBar;
     }
     return off;
 }
 
-// BF16 copies of the weights in the chunk-major operand layout (after every
-// parameter change)
+int k1p_of(const LcNet *n) { return (n->IN + 15) / 16 * 16; }
+int n4p_of(const LcNet *n) { return (n->OUT + 15) / 16 * 16; }
+
+}  // namespace
+
+// the kernel's plan: the first layer's K fits a weight slot and the outputs
+// one unit (nsigma <= 32 at 3*nsigma + 3 inputs and 2*nsigma outputs), the
+// shared memory fits one SM
+bool lc_tc_supported(const LcNet *n) {
+    return k1p_of(n) <= 256 && n4p_of(n) <= kUnitN && tc_smem(nullptr) <= 232448;
+}
+
+// BF16 copies of the weights as the kernel's units (after every parameter
+// change)
 int lc_tc_prepare(LcNet *n) {
     if (!lc_tc_supported(n)) return FESOMC_EINVAL_LC;
-    const int K1p = (n->IN + 15) / 16 * 16, N4p = (n->OUT + 15) / 16 * 16;
+    const int K1p = k1p_of(n), N4p = n4p_of(n);
     std::vector<float> p(n->np);
     if (cudaMemcpy(p.data(), n->params, sizeof(float) * n->np, cudaMemcpyDeviceToHost) != cudaSuccess)
         return FESOMC_ECUDA_LC;
-    const size_t s1 = (size_t)256 * K1p, s2 = (size_t)256 * 256, s4 = (size_t)N4p * 256;
-    std::vector<uint16_t> w(s1 + 2 * s2 + s4, 0);
-    // W1: 256 rows (neurons) x K1p
-    for (int r = 0; r < 256; ++r)
-        for (int k = 0; k < n->IN; ++k) w[cm_index(256, r, k)] = bf16_bits(p[n->off[0] + (size_t)r * n->IN + k]);
-    // W2, W3: two halves of 128 neurons, each a 128-row operand
-    for (int l = 1; l <= 2; ++l) {
-        uint16_t *base = w.data() + s1 + (size_t)(l - 1) * s2;
-        for (int r = 0; r < 256; ++r)
-            for (int k = 0; k < 256; ++k)
-                base[(size_t)(r / 128) * 128 * 256 + cm_index(128, r % 128, k)] =
-                    bf16_bits(p[n->off[l] + (size_t)r * 256 + k]);
+    const UnitPlan up = unit_plan(K1p, N4p);
+    std::vector<uint16_t> w(up.total / 2, 0);
+    const int fan_in[4] = {n->IN, 256, 256, 256}, fan_out[4] = {256, 256, 256, n->OUT};
+    for (int i = 0; i < up.n; ++i) {
+        const int l = up.layer[i], R = up.rows[i];
+        uint16_t *base = w.data() + up.off[i] / 2;
+        for (int r = 0; r < R; ++r) {
+            const int neuron = up.first_neuron[i] + r;
+            if (neuron >= fan_out[l]) continue;   // zero padding of W4
+            for (int k = 0; k < fan_in[l]; ++k)
+                base[cm_index(R, r, k)] = bf16_bits(p[n->off[l] + (size_t)neuron * fan_in[l] + k]);
+        }
     }
-    uint16_t *b4 = w.data() + s1 + 2 * s2;
-    for (int r = 0; r < n->OUT; ++r)
-        for (int k = 0; k < 256; ++k) b4[cm_index(N4p, r, k)] = bf16_bits(p[n->off[3] + (size_t)r * 256 + k]);
     if (!n->wtc) {
         void *q = nullptr;
         if (cudaMalloc(&q, w.size() * 2) != cudaSuccess) return FESOMC_ENOMEM_LC;
@@ -379,25 +477,32 @@ int lc_tc_prepare(LcNet *n) {
 // Y (B x OUT) = network(X (B x IN)) with the BF16 tensor-core kernel
 int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStream_t s) {
     if (!n->tc_ready) return FESOMC_ESTATE_LC;
+    if (B < 1) return 0;
     TcParams p{};
     p.IN = n->IN;
     p.OUT = n->OUT;
-    p.K1p = (n->IN + 15) / 16 * 16;
-    p.N4p = (n->OUT + 15) / 16 * 16;
+    p.K1p = k1p_of(n);
+    p.N4p = n4p_of(n);
     p.ncol = B;
     p.X = X;
     p.Y = Y;
-    const size_t s1 = (size_t)256 * p.K1p, s2 = (size_t)256 * 256;
-    p.W1 = reinterpret_cast<const uint4 *>(n->wtc);
-    p.W2 = reinterpret_cast<const uint4 *>(n->wtc + s1);
-    p.W3 = reinterpret_cast<const uint4 *>(n->wtc + s1 + s2);
-    p.W4 = reinterpret_cast<const uint4 *>(n->wtc + s1 + 2 * s2);
+    p.W = reinterpret_cast<const unsigned char *>(n->wtc);
+    const UnitPlan up = unit_plan(p.K1p, p.N4p);
+    p.n_units = up.n;
+    for (int i = 0; i < up.n; ++i) {
+        p.unit_off[i] = up.off[i];
+        p.unit_bytes[i] = up.bytes[i];
+        p.unit_rows[i] = up.rows[i];
+        p.unit_k[i] = up.k[i];
+        p.unit_col[i] = up.col[i];
+        p.unit_last[i] = up.last[i];
+    }
     p.b1 = n->params + n->off[0] + (long long)256 * n->IN;
     p.b2 = n->params + n->off[1] + (long long)256 * 256;
     p.b3 = n->params + n->off[2] + (long long)256 * 256;
     p.b4 = n->params + n->off[3] + (long long)n->OUT * 256;
     p.err = n->tc_err;
-    const size_t smem = tc_smem(p.K1p, p.N4p, &p);
+    const size_t smem = tc_smem(&p);
     static size_t raised = 0;
     if (smem > raised) {
         if (cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -413,8 +518,6 @@ int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStr
     return cudaGetLastError() == cudaSuccess ? 0 : FESOMC_ECUDA_LC;
 }
 
-size_t lc_tc_smem_bytes(const LcNet *n) {
-    return tc_smem((n->IN + 15) / 16 * 16, (n->OUT + 15) / 16 * 16, nullptr);
-}
+size_t lc_tc_smem_bytes(const LcNet *) { return tc_smem(nullptr); }
 
 }  // namespace fesomc
