@@ -689,12 +689,12 @@ def run_closure(args):
 def run_lc_infer(args):
     """The learned closure's inference alone: the BF16 tensor-core kernel and
     the FP32 kernels on --lc-infer device-resident columns of the cfg1 shape
-    (21 levels: 66 inputs, 42 outputs), random weights, device-timed; FLOP
-    per column 2 (66*256 + 2*256*256 + 256*42)."""
+    (21 levels: 66 inputs, 21 outputs), random weights, device-timed; FLOP
+    per column 2 (66*256 + 2*256*256 + 256*21)."""
     from fesomc import closure
     c = closure.Closure(21)
     n = args.lc_infer
-    flop = 2.0 * (66 * 256 + 2 * 256 * 256 + 256 * 42) * n
+    flop = 2.0 * (c.n_in * 256 + 2 * 256 * 256 + 256 * c.n_out) * n
     ms_tc = c.time(n, reps=max(args.steps, 1), bf16=True)
     ms_32 = c.time(n, reps=max(min(args.steps, 5), 1), bf16=False)
     c.close()

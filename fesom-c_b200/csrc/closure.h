@@ -2,7 +2,7 @@
 // d3_end (src/fv_mixing.F90:73-347).  No counterpart in the reference.
 //
 // Network: IN = 3*NS + 3 inputs, three hidden layers of 256 with SiLU,
-// OUT = 2*NS outputs; layer l computes Z = A W^T + b with W row-major
+// OUT = NS outputs; layer l computes Z = A W^T + b with W row-major
 // (out x in); the flat parameter vector is W1 b1 W2 b2 W3 b3 W4 b4.
 //
 // Inputs per node column (NS interfaces, 0-based k; before the transform):
@@ -15,7 +15,11 @@
 // Shear, N^2 and the two boundary terms enter as asinh(x / x0) with x0 =
 // 1e-6 (they span many decades and N^2 changes sign); every input is then
 // normalised by the training set's mean and standard deviation.
-// Outputs: log snu and log Kv per interface, normalised the same way.
+// Outputs: log bt (the turbulence energy d3_end advances) per interface,
+// normalised the same way.  snu and Kv follow from bt exactly as d3_end
+// forms them (snu = scale_t sqrt(bt) + snul, capped at 0.2; Kv = Pr_num snu),
+// so the network's bt, snu and Kv are one consistent closure state, and the
+// plain closure restarts from a bt inside its own range.
 #pragma once
 #include <cstdint>
 
@@ -29,7 +33,9 @@ constexpr float kLcX0 = 1.0e-6f;
 constexpr int kLcRuleUnstable = 1;   // N^2 < 0 at an interior interface: the plain closure
 
 inline int lc_in(int NS) { return 3 * NS + 3; }
-inline int lc_out(int NS) { return 2 * NS; }
+inline int lc_out(int NS) { return NS; }
+// rows of the statistics array (each max(IN, OUT) floats)
+constexpr int kLcStatRows = 8;
 
 // the device-side pieces the step kernels need (features, application,
 // envelope test and judge statistics); the state kernels are compiled per
@@ -39,6 +45,7 @@ struct LcView {
     int rules;                                // kLcRule* bits
     const float *mu_x, *sd_x, *mu_y, *sd_y;   // normalisation (IN / OUT)
     const float *lo_x, *hi_x;                 // training envelope of the normalised inputs
+    const float *lo_y, *hi_y;                 // range of the training targets (log bt, not normalised)
     float *X;                                 // per node: normalised inputs (N x IN), FP32
     float *Y;                                 // per node: network outputs (N x OUT), normalised
     int *flag;                                // per node: 1 = network, 0 = plain closure

@@ -88,20 +88,27 @@ __global__ void k_lc_features(Dev d, LcView c) {
     }
 }
 
-// the closure's viscosity from the network output (clamped to the range the
-// plain closure can give: snul .. 0.2, fv_mixing.F90:291-295)
-__device__ __forceinline__ real lc_snu(const Dev &d, const LcView &c, int node, int k) {
-    const float ls = c.Y[(size_t)node * c.OUT + k] * c.sd_y[k] + c.mu_y[k];
-    real s = (real)expf(ls);
-    if (!(s >= d.snul)) s = d.snul;
-    if (s > real(0.2)) s = real(0.2);
-    return s;
+// The network's closure state of interface k: bt from its output, held to
+// the range of the training targets, and snu, Kv from bt exactly as d3_end
+// forms them (fv_mixing.F90:280-300).
+__device__ __forceinline__ void lc_state(const Dev &d, const LcView &c, int node, int k, real dmean, real &bt,
+                                         real &snu) {
+    float lb = c.Y[(size_t)node * c.OUT + k] * c.sd_y[k] + c.mu_y[k];
+    if (!(lb >= c.lo_y[k])) lb = c.lo_y[k];   // NaN too
+    if (lb > c.hi_y[k]) lb = c.hi_y[k];
+    const real btn = dmax((real)expf(lb), real(1.0e-8));
+    const real zt = __ldg(d.sig + k) * dmean;
+    const real Zh = zt + d.z0b_min;
+    const real Zd = fabs(dmean - zt) + d.z0s_min;
+    const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+    const real scale_t = d.cka * Zh * Zd * Z0 / dmean;
+    real s = scale_t * sqrt(btn) + d.snul;
+    if (s >= real(0.2)) s = real(0.2);
+    bt = btn;
+    snu = s;
 }
 
-// Network columns: snu and Kv from the outputs, and bt from the closure's
-// own relation snu = scale_t sqrt(bt) + snul (fv_mixing.F90:280-295), so that
-// the plain closure, when it next runs on the column (fallback or judge),
-// starts from the turbulence energy that matches the viscosity in use.
+// Network columns: bt, snu and Kv of the network's closure state.
 __global__ void k_lc_apply(Dev d, LcView c) {
     GRID_LOOP(ii, d.N) {
         const int node = (int)ii;
@@ -112,31 +119,17 @@ __global__ void k_lc_apply(Dev d, LcView c) {
         real *sn = d.snu + (size_t)node * NS;
         real *kv = d.Kv + (size_t)node * NS;
         for (int k = 0; k < NS; ++k) {
-            const real s = lc_snu(d, c, node, k);
-            const float lk = c.Y[(size_t)node * c.OUT + NS + k] * c.sd_y[NS + k] + c.mu_y[NS + k];
-            real K = (real)expf(lk);
-            const real klo = d.Pr_num * d.snul, khi = d.Pr_num * real(0.2);
-            if (!(K >= klo)) K = klo;
-            if (K > khi) K = khi;
-            const real zt = __ldg(d.sig + k) * dmean;
-            const real Zh = zt + d.z0b_min;
-            const real Zd = fabs(dmean - zt) + d.z0s_min;
-            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
-            const real scale_t = d.cka * Zh * Zd * Z0 / dmean;
-            real b = real(1.0e-8);
-            if (scale_t > real(0.0)) {
-                const real r = (s - d.snul) / scale_t;
-                b = dmax(r * r, real(1.0e-8));
-            }
+            real b, s;
+            lc_state(d, c, node, k, dmean, b, s);
             bt[k] = b;
             sn[k] = s;
-            kv[k] = K;
+            kv[k] = d.Pr_num * s;
         }
     }
 }
 
-// training pairs: raw inputs and log snu / log Kv of wet columns, after the
-// plain closure has run on the step
+// training pairs: raw inputs and log bt of wet columns, after the plain
+// closure has run on the step
 __global__ void k_lc_harvest(Dev d, LcView c) {
     GRID_LOOP(ii, d.N) {
         const int node = (int)ii;
@@ -146,10 +139,7 @@ __global__ void k_lc_harvest(Dev d, LcView c) {
         lc_inputs(d, node, c.hx + slot * c.IN);
         const int NS = d.NS;
         float *y = c.hy + slot * c.OUT;
-        for (int k = 0; k < NS; ++k) {
-            y[k] = logf((float)d.snu[(size_t)node * NS + k]);
-            y[NS + k] = logf((float)d.Kv[(size_t)node * NS + k]);
-        }
+        for (int k = 0; k < NS; ++k) y[k] = logf((float)d.bt[(size_t)node * NS + k]);   // bt >= 1e-8
     }
 }
 
@@ -160,8 +150,13 @@ __global__ void k_lc_judge(Dev d, LcView c) {
     GRID_LOOP(ii, d.N) {
         const int node = (int)ii;
         if (!c.flag[node]) continue;
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
         for (int k = 0; k < d.NS; ++k) {
-            const double e = log((double)lc_snu(d, c, node, k)) - log((double)d.snu[(size_t)node * d.NS + k]);
+            real b, s;
+            lc_state(d, c, node, k, dmean, b, s);
+            const real sp = d.snu[(size_t)node * d.NS + k];
+            if (!(s > real(0.0) && sp > real(0.0))) continue;   // log of a non-positive viscosity
+            const double e = log((double)s) - log((double)sp);
             s2 += e * e;
             n += 1.0;
             mx = fmax(mx, fabs(e));

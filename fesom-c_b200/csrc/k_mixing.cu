@@ -24,56 +24,39 @@ __device__ __forceinline__ bool d3_above_tol(real a, real b) {
     return fabs(a / b) >= real(1.0e-6);
 }
 
-// d3_end per node column.  The column's arrays live in shared memory, laid
-// out [array][level][thread] so that a warp's access to one level is 32
-// consecutive words: the iterated sweep never leaves the SM.  (As local
-// memory their working set over the resident columns exceeded L2 and every
-// iteration streamed it through DRAM, 6.6x the kernel's algorithmic bytes.)
-// Arrays, by the Fortran index nz they hold:
-//   sn        snu(nz), nz = 1..NS                 (constant over the iteration)
-//   bA, bB    btr / btr1 / xx1, nz = 1..NS        (alternating, see below)
-//   yy1       yy1(nz), nz = 3..NS
-//   pb, qb, c2  -b1-b2, t_inv*bt and c2, nz = 2..NS-1 (constant)
-// i.e. 7*NS - 8 values per column (d3end_smem).  Beyond that:
-//   * am and cm are recomputed in each iteration from snu(k-1..k+1) held in
-//     registers (the reference recomputes them the same way);
+// d3_end per node column (local-memory arrays indexed 1..NS like the Fortran
+// ones, ARR >= NS + 1 entries each).  The kernel is bound by the traffic of
+// those arrays: the working set of the resident columns does not fit in L2,
+// so each iteration streams them through DRAM.  It therefore keeps the
+// array count and the accesses per level low:
+//   * -b1-b2, t_inv*bo and c2 are formed once per level; am and cm are
+//     recomputed in each iteration from snu(k-1..k+1) held in registers (the
+//     reference recomputes them the same way);
 //   * xx1(k), yy1(k) feed the next level from registers, the arrays only
 //     carry them to the back substitution;
-//   * btr and btr1 alternate between bA and bB, and the back substitution
-//     writes btr1(k) into the xx1(k) slot it has just read, so xx1 needs no
-//     array of its own; xx1(2) = 1 and yy1(2) = y2 are constants;
+//   * btr and btr1 alternate between two arrays instead of being copied;
 //   * tke_dissip, which the reference overwrites in every iteration, is
 //     written once from the btr of the last iteration;
 //   * the convergence test forms the quotient only near the threshold;
-//   * both sweeps load the next level's values one level ahead.
+//   * both sweeps load the next level's array values one level ahead, so
+//     that their latency overlaps the current level's division chain (3 %
+//     faster; unrolling by 4 instead was 9 % slower).
+// (The same arrays in shared memory, [array][level][thread], take the DRAM
+// traffic down to the algorithmic bytes but leave room for 6 warps per SM
+// only, and the kernel then waits on its FP64 chains: 3.85 against 2.54 ms
+// on cfg1.)
 //
 // kList: the columns are list[0 .. *count) instead of every node (the
 // columns the learned closure hands back to the plain one).
-constexpr int kD3Block = 32;
-
-__host__ __device__ inline int d3end_values(int NS) { return 7 * NS - 8; }
-
-template <bool kList>
-__global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, const unsigned long long *count) {
-    extern __shared__ unsigned char d3_smem[];
-    constexpr int B = kD3Block;
-    const int NS = d.NS, L = d.L;
-    real *const base = reinterpret_cast<real *>(d3_smem) + threadIdx.x;
-    // per-array views: element nz of an array at [(nz - first) * B]
-    real *const s_sn = base - 1 * B;                     // nz = 1..NS
-    real *const s_bA = base + (NS - 1) * B;              // nz = 1..NS
-    real *const s_bB = base + (2 * NS - 1) * B;          // nz = 1..NS
-    real *const s_yy = base + (3 * NS - 3) * B;          // nz = 3..NS
-    real *const s_pb = base + (4 * NS - 4) * B;          // nz = 2..NS-1
-    real *const s_qb = base + (5 * NS - 6) * B;          // nz = 2..NS-1
-    real *const s_c2 = base + (6 * NS - 8) * B;          // nz = 2..NS-1
-#define D3(a, nz) a[(size_t)(nz) * B]
+template <int ARR, bool kList>
+__global__ void k_d3end(Dev d, const int *list, const unsigned long long *count) {
     const real t_inv = real(1.0) / d.dt;
     const real cka = d.cka;
     const real B1cka2 = real(16.6) * (cka * cka);
     const long long ncol = kList ? (long long)*count : (long long)d.N;
     GRID_LOOP(ii, ncol) {
         const int node = kList ? list[ii] : (int)ii;
+        const int NS = d.NS, L = d.L;
         const real *bt = d.bt + (size_t)node * NS;
         const real *snu = d.snu + (size_t)node * NS;
         const real *Kv = d.Kv + (size_t)node * NS;
@@ -83,12 +66,13 @@ __global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, cons
         const real *S = d.SF + (size_t)node * L;
         real *Ri = d.Ri + (size_t)node * NS;
         real *tke = d.tke_dissip + (size_t)node * NS;
+        real xx1[ARR], yy1[ARR], bA[ARR], bB[ARR], pb[ARR], qb[ARR], c2[ARR], sn[ARR];
         const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
         const real dmean2 = dmean * dmean;
         const real ajac = jac_a(d, d.eta_jac, node);
         for (int nz = 1; nz <= NS; ++nz) {
-            D3(s_bA, nz) = bt[nz - 1];
-            D3(s_sn, nz) = snu[nz - 1];
+            bA[nz] = bt[nz - 1];
+            sn[nz] = snu[nz - 1];
         }
         Ri[0] = real(0.0);
         Ri[NS - 1] = real(0.0);
@@ -99,50 +83,50 @@ __global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, cons
             const real dd = real(0.5) * (d1 + d2);
             real ap1 = Un[nz - 2] - Un[nz - 1];
             const real ap2 = Vn[nz - 2] - Vn[nz - 1];
-            const real sn_m = snu[nz - 2], sn_0 = snu[nz - 1], sn_p = snu[nz];
-            real b1 = sn_0 * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            real b1 = sn[nz] * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
             b1 = b1 / dmean2;
             const real zb = zbar_of(d, ajac, nz - 1);
             const real rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
             const real rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
             ap1 = (rho_up - rho_dn) / dd;
             const real b2 = -real(0.5) * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
-            const real snu_p = real(0.5) * (sn_m + sn_0);
-            const real snu_m = real(0.5) * (sn_0 + sn_p);
+            const real snu_p = real(0.5) * (sn[nz - 1] + sn[nz]);
+            const real snu_m = real(0.5) * (sn[nz] + sn[nz + 1]);
             const real cc = real(0.5) * real(0.73) * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
-            D3(s_c2, nz) = cc / dmean2;
-            if (b1 > real(0.0)) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn_0;
+            c2[nz] = cc / dmean2;
+            if (b1 > real(0.0)) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn[nz];
             else Ri[nz - 1] = real(10000.0);
-            D3(s_pb, nz) = -b1 - b2;
-            D3(s_qb, nz) = t_inv * bt[nz - 1];
+            pb[nz] = -b1 - b2;
+            qb[nz] = t_inv * bt[nz - 1];
         }
         real y2;
         {
             const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
             const real wx = d.windx[node], wy = d.windy[node];
             const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
-            const real snu_m = real(0.5) * (snu[NS - 1] + snu[NS - 2]);
+            const real snu_m = real(0.5) * (sn[NS] + sn[NS - 1]);
             y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
         }
+        xx1[2] = real(1.0);
+        yy1[2] = y2;
         // bottom boundary value (independent of the iteration)
         const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
         const real lg = fesomc_log(delta_b / d.z0b_min);
         const real bott_R = B1cka2 / (lg * lg);
         const real ubt = Un[L - 1], vbt = Vn[L - 1];
         const real bot = bott_R * (ubt * ubt + vbt * vbt);
-        real *btr = s_bA, *xq = s_bB;   // xq: this iteration's xx1, then its btr1
+        real *btr = bA, *btr1 = bB;
         bool converged = false;
         int iters = 200;
         for (int it = 1; it <= 200; ++it) {
             real x = real(1.0), y = y2;
-            real s_lo = D3(s_sn, 1), s_mid = D3(s_sn, 2);
-            real b_n = D3(btr, 2), pb_n = D3(s_pb, 2), qb_n = D3(s_qb, 2), c2_n = D3(s_c2, 2), sh_n = D3(s_sn, 3);
+            real s_lo = sn[1], s_mid = sn[2];
+            real b_n = btr[2], pb_n = pb[2], qb_n = qb[2], c2_n = c2[2], sh_n = sn[3];
             for (int nz = 2; nz <= NS - 1; ++nz) {
                 const real s_hi = sh_n;
                 const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n;
                 if (nz + 1 <= NS - 1) {
-                    b_n = D3(btr, nz + 1); pb_n = D3(s_pb, nz + 1); qb_n = D3(s_qb, nz + 1);
-                    c2_n = D3(s_c2, nz + 1); sh_n = D3(s_sn, nz + 2);
+                    b_n = btr[nz + 1]; pb_n = pb[nz + 1]; qb_n = qb[nz + 1]; c2_n = c2[nz + 1]; sh_n = sn[nz + 2];
                 }
                 const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
                 const real dd1 = s_m - s_0;
@@ -159,37 +143,32 @@ __global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, cons
                 const real a = bm - am * x;
                 const real xn = cm / a;
                 const real yn = (am * y - fr) / a;
-                D3(xq, nz + 1) = xn;
-                D3(s_yy, nz + 1) = yn;
+                xx1[nz + 1] = xn;
+                yy1[nz + 1] = yn;
                 x = xn;
                 y = yn;
                 s_lo = s_mid;
                 s_mid = s_hi;
             }
             real b1v = bot;  // btr1(NS)
-            real x_n = D3(xq, NS), y_n = D3(s_yy, NS), o_n = D3(btr, NS - 1);
-            const real top = D3(btr, NS);
-            D3(xq, NS) = b1v;
-            bool above = d3_above_tol(top - b1v, dmax(b1v, top) + real(1.0e-8));
+            btr1[NS] = b1v;
+            bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + real(1.0e-8));
+            real x_n = xx1[NS], y_n = yy1[NS], o_n = btr[NS - 1];
             for (int nz = NS; nz >= 2; --nz) {
                 const real xv = x_n, yv = y_n, ov = o_n;
-                if (nz - 1 >= 3) { x_n = D3(xq, nz - 1); y_n = D3(s_yy, nz - 1); o_n = D3(btr, nz - 2); }
-                else if (nz - 1 == 2) { x_n = real(1.0); y_n = y2; o_n = D3(btr, nz - 2); }
-                b1v = b1v * xv + yv;  // btr1(nz-1), into the xx1(nz-1) slot already read
-                D3(xq, nz - 1) = b1v;
+                if (nz - 1 >= 2) { x_n = xx1[nz - 1]; y_n = yy1[nz - 1]; o_n = btr[nz - 2]; }
+                b1v = b1v * xv + yv;  // btr1(nz-1)
+                btr1[nz - 1] = b1v;
                 above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
             }
             if (!above) { converged = true; iters = it; break; }
             real *t = btr;
-            btr = xq;
-            xq = t;
+            btr = btr1;
+            btr1 = t;
         }
         if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
         if (converged) {
-            for (int nz = 2; nz <= NS - 1; ++nz) {
-                const real b = D3(btr, nz);
-                tke[nz - 1] = real(0.046) * (b * b) / D3(s_sn, nz);
-            }
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (btr[nz] * btr[nz]) / sn[nz];
         } else {
             atomicAdd(d.notconv, 1);
         }
@@ -197,7 +176,7 @@ __global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, cons
         real *snw = d.snu + (size_t)node * NS;
         real *Kvw = d.Kv + (size_t)node * NS;
         for (int nz = 1; nz <= NS; ++nz) {
-            const real btn = dmax(D3(btr, nz), real(1.0e-8));
+            const real btn = dmax(btr[nz], real(1.0e-8));
             btw[nz - 1] = btn;
             const real zt = __ldg(d.sig + nz - 1) * dmean;
             const real Zh = zt + d.z0b_min;
@@ -210,7 +189,6 @@ __global__ void __launch_bounds__(kD3Block) k_d3end(Dev d, const int *list, cons
             Kvw[nz - 1] = d.Pr_num * s;
         }
     }
-#undef D3
 }
 
 // Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
@@ -227,19 +205,20 @@ __global__ void k_av(Dev d) {
     }
 }
 
-static size_t d3end_smem(const Dev &d) { return (size_t)d3end_values(d.NS) * kD3Block * sizeof(real); }
-int config_d3end(const Dev &d) {
-    if (d.NS < 3 || d.NS > 127) return 1;
-    return (raise_smem_limit(k_d3end<false>, d3end_smem(d)) == cudaSuccess &&
-            raise_smem_limit(k_d3end<true>, d3end_smem(d)) == cudaSuccess) ? 0 : 1;
-}
+int config_d3end(const Dev &d) { return d.NS <= 127 ? 0 : 1; }
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    k_d3end<false><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, nullptr, nullptr);
+    if (d.NS <= 11) k_d3end<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 21) k_d3end<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 40) k_d3end<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else k_d3end<128, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
 }
 // the plain closure on the listed columns (count read on the device, so the
 // launch covers every node and the grid-stride loop stops at the count)
 void launch_d3end_list(const Dev &d, const int *list, const unsigned long long *count, cudaStream_t s) {
-    k_d3end<true><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, list, count);
+    if (d.NS <= 11) k_d3end<12, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else if (d.NS <= 21) k_d3end<22, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else if (d.NS <= 40) k_d3end<41, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    else k_d3end<128, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
 }
 void launch_av(const Dev &d, cudaStream_t s) {
     const int b = tuned(d, TK_AV, 256);

@@ -246,7 +246,7 @@ LcNet *lc_create(int NS, long long hcap, unsigned long long seed, int Bmax, cuda
     int r = 0;
     if ((r = lc_alloc(n, &n->params, n->np)) || (r = lc_alloc(n, &n->grads, n->np)) ||
         (r = lc_alloc(n, &n->mom, n->np)) || (r = lc_alloc(n, &n->var, n->np)) ||
-        (r = lc_alloc(n, &n->stats, 6 * (size_t)std::max(n->IN, n->OUT))) || (r = lc_alloc(n, &n->dloss, 2)) ||
+        (r = lc_alloc(n, &n->stats, kLcStatRows * (size_t)std::max(n->IN, n->OUT))) || (r = lc_alloc(n, &n->dloss, 2)) ||
         (r = lc_alloc(n, &n->Xb, (size_t)Bmax * n->IN)) || (r = lc_alloc(n, &n->Tb, (size_t)Bmax * n->OUT)) ||
         (r = lc_alloc(n, &n->part, (size_t)((Bmax + kColChunk - 1) / kColChunk) * kLcHidden)) ||
         (r = lc_alloc(n, &n->hcount, 1)) || (hcap > 0 && ((r = lc_alloc(n, &n->hx, (size_t)hcap * n->IN)) ||
@@ -262,12 +262,14 @@ LcNet *lc_create(int NS, long long hcap, unsigned long long seed, int Bmax, cuda
             lc_free(n);
             return nullptr;
         }
-    // normalisation starts as the identity (mean 0, sd 1, envelope +-inf)
-    std::vector<float> st(6 * (size_t)std::max(n->IN, n->OUT));
+    // normalisation starts as the identity (mean 0, sd 1, envelope and
+    // target range +-inf)
+    std::vector<float> st(kLcStatRows * (size_t)std::max(n->IN, n->OUT));
     const int W = std::max(n->IN, n->OUT);
     for (int j = 0; j < W; ++j) {
         st[0 * W + j] = 0.0f; st[1 * W + j] = 1.0f; st[2 * W + j] = 0.0f; st[3 * W + j] = 1.0f;
         st[4 * W + j] = -INFINITY; st[5 * W + j] = INFINITY;
+        st[6 * W + j] = -INFINITY; st[7 * W + j] = INFINITY;
     }
     cudaMemcpy(n->stats, st.data(), st.size() * sizeof(float), cudaMemcpyHostToDevice);
     // He-uniform weights (bound sqrt(6 / fan_in)), zero biases
@@ -386,7 +388,7 @@ int lc_fit_stats(LcNet *n) {
     cudaStreamSynchronize(n->stream);
     cudaFree(d);
     LCK(e);
-    std::vector<float> st(6 * (size_t)W, 0.0f);
+    std::vector<float> st(kLcStatRows * (size_t)W, 0.0f);
     for (int j = 0; j < n->IN + n->OUT; ++j) {
         const double *q = &h[4 * j];
         const double mean = q[0] / cnt;
@@ -401,6 +403,8 @@ int lc_fit_stats(LcNet *n) {
         } else {
             st[2 * W + (j - n->IN)] = (float)mean;
             st[3 * W + (j - n->IN)] = (float)sd;
+            st[6 * W + (j - n->IN)] = (float)q[2];
+            st[7 * W + (j - n->IN)] = (float)q[3];
         }
     }
     n->h_stats = st;

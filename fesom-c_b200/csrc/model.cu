@@ -1903,6 +1903,8 @@ int lc_model_buffers(fesomc_model *m, fesomc_closure *c) {
     v.sd_y = n->stats + 3 * W;
     v.lo_x = n->stats + 4 * W;
     v.hi_x = n->stats + 5 * W;
+    v.lo_y = n->stats + 6 * W;
+    v.hi_y = n->stats + 7 * W;
     v.hx = n->hx;
     v.hy = n->hy;
     v.hcap = n->hcap;
@@ -2004,7 +2006,7 @@ int fesomc_closure_params(fesomc_closure *c, float *get, const float *set) {
 
 int fesomc_closure_norm(fesomc_closure *c, float *get, const float *set) {
     if (!c) return FESOMC_EINVAL;
-    const size_t b = sizeof(float) * 6 * (size_t)std::max(c->net->IN, c->net->OUT);
+    const size_t b = sizeof(float) * kLcStatRows * (size_t)std::max(c->net->IN, c->net->OUT);
     if (set) CK(cudaMemcpy(c->net->stats, set, b, cudaMemcpyHostToDevice));
     if (get) CK(cudaMemcpy(get, c->net->stats, b, cudaMemcpyDeviceToHost));
     return FESOMC_OK;

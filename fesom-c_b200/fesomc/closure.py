@@ -9,6 +9,11 @@ import numpy as np
 
 from . import abi
 
+# rows of the statistics (norm): input mean, input sd, target mean, target
+# sd, envelope low, envelope high (normalised inputs), lowest and highest
+# target (log bt)
+STAT_ROWS = 8
+
 
 class Closure:
     """One network (and its training set) for meshes with nsigma levels."""
@@ -65,12 +70,12 @@ class Closure:
         w = max(self.n_in, self.n_out)
         if value is not None:
             v = np.ascontiguousarray(value, dtype=np.float32).reshape(-1)
-            assert v.size == 6 * w
+            assert v.size == STAT_ROWS * w
             abi.check(self.lib.fesomc_closure_norm(self.h, None, abi.fptr(v)))
-            return v.reshape(6, w)
-        out = np.empty(6 * w, dtype=np.float32)
+            return v.reshape(STAT_ROWS, w)
+        out = np.empty(STAT_ROWS * w, dtype=np.float32)
         abi.check(self.lib.fesomc_closure_norm(self.h, abi.fptr(out), None))
-        return out.reshape(6, w)
+        return out.reshape(STAT_ROWS, w)
 
     def forward(self, X, bf16=False):
         """The network on normalised inputs; bf16: on the tensor cores."""

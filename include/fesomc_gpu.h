@@ -468,15 +468,17 @@ int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const doub
  * frequency squared and the interface depth, plus the surface TKE flux term,
  * the bottom TKE value and the total depth (3*nsigma + 3 values; shear, N^2
  * and the boundary terms through asinh(x/1e-6), then normalised by the
- * training set); three hidden layers of 256 with SiLU; outputs log snu and
- * log Kv at the interfaces (2*nsigma, normalised).  It is trained on the
- * GPU, on columns harvested from the plain closure, by FP32 forward /
- * backward / Adam kernels.  In the time step (fesomc_closure_attach) a wet
- * column whose inputs lie inside the training envelope takes the network's
- * snu and Kv, and bt from the closure's own relation snu = scale_t sqrt(bt)
- * + snul; dry columns and columns outside the envelope take the plain
- * closure; every judge_every-th step the plain closure runs on all columns
- * and the network's viscosity is compared with it.
+ * training set); three hidden layers of 256 with SiLU; outputs log bt, the
+ * turbulence energy d3_end advances, at the interfaces (nsigma, normalised).
+ * It is trained on the GPU, on columns harvested from the plain closure, by
+ * FP32 forward / backward / Adam kernels.  In the time step
+ * (fesomc_closure_attach) a wet column whose inputs lie inside the training
+ * envelope takes the network's bt, held to the range of the training
+ * targets, and snu and Kv formed from it as d3_end forms them (snu =
+ * scale_t sqrt(bt) + snul, at most 0.2; Kv = Pr_num snu); dry columns and
+ * columns outside the envelope take the plain closure; every judge_every-th
+ * step the plain closure runs on all columns and the network's viscosity is
+ * compared with it.
  *
  * _create: nsigma 5..32, room for 'capacity' harvested columns.
  * _harvest: advances the model nsteps internal steps (forcing as last set,
@@ -486,12 +488,13 @@ int  fesomc_energy_device(int32_t nod2D, int32_t elem2D, double Dmin, const doub
  * _train: epochs of Adam over the training set in minibatches of 'batch'
  *   (<= 8192); losses (may be NULL) receives the mean loss per epoch.
  * _params / _norm: copy the parameters (W1 b1 W2 b2 W3 b3 W4 b4, W row-major
- *   out x in) / the statistics (6 arrays of max(in, out) floats: input mean,
+ *   out x in) / the statistics (8 arrays of max(in, out) floats: input mean,
  *   input sd, output mean, output sd, envelope low, envelope high of the
- *   normalised inputs) out of (get) and into (set) the closure.
+ *   normalised inputs, lowest and highest training target) out of (get) and
+ *   into (set) the closure.
  * _forward / _grad: the network on host arrays of normalised inputs (tests),
  *   _forward with bf16 = 1 on the tensor cores (BF16 weights and
- *   activations, FP32 accumulation; nsigma <= 25), else in FP32;
+ *   activations, FP32 accumulation; nsigma <= 32), else in FP32;
  *   _grad takes n <= 8192 samples and returns the mean squared error and its
  *   gradient in the parameter layout.
  * _attach: the model's steps use the closure (NULL: the plain closure

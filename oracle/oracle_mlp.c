@@ -8,7 +8,7 @@
  * column: IN = 3*NS + 3 inputs (per interface the squared shear, the
  * buoyancy frequency squared and the interface depth; then the surface
  * forcing term, the bottom friction term and the total depth, all
- * normalised), three hidden layers of 256 with SiLU, OUT = 2*NS outputs
+ * normalised), three hidden layers of 256 with SiLU, OUT = NS outputs
  * (log of the viscosity snu and of the diffusivity Kv per interface,
  * normalised).  Layer l computes Z_l = A_{l-1} W_l^T + b_l with W_l stored
  * row-major (out x in); the flat parameter vector is W1 b1 W2 b2 W3 b3 W4 b4.
@@ -30,7 +30,7 @@ static void mlp_dims(int NS, int d[5]) {
     d[1] = MLP_H;
     d[2] = MLP_H;
     d[3] = MLP_H;
-    d[4] = 2 * NS;
+    d[4] = NS;
 }
 
 int64_t oracle_mlp_nparams(int NS) {

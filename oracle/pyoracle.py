@@ -172,7 +172,7 @@ def mlp_forward(abi, nsigma, params, X):
     """The closure network on the CPU (double accumulation): Y = net(X)."""
     lib = load(abi)
     p, X = _f32(params), _f32(X)
-    Y = np.empty((X.shape[0], 2 * nsigma), dtype=np.float32)
+    Y = np.empty((X.shape[0], nsigma), dtype=np.float32)
     f = C.POINTER(C.c_float)
     if lib.oracle_mlp_forward(nsigma, p.ctypes.data_as(f), X.ctypes.data_as(f), X.shape[0], Y.ctypes.data_as(f)):
         raise RuntimeError("oracle_mlp_forward failed")

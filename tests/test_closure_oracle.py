@@ -22,7 +22,7 @@ def _random_net(nparams, seed):
 @pytest.mark.parametrize("nsigma", [5, 11])
 def test_mlp_gradient_matches_finite_differences(mods, nsigma):
     abi, pyoracle = mods
-    n_in, n_out = 3 * nsigma + 3, 2 * nsigma
+    n_in, n_out = 3 * nsigma + 3, nsigma
     npar = pyoracle.mlp_nparams(abi, nsigma)
     assert npar == n_in * 256 + 256 + 2 * (256 * 256 + 256) + 256 * n_out + n_out
     rng = np.random.default_rng(3)

@@ -142,6 +142,9 @@ def test_harvest_and_envelope(mods):
         st = c.norm()
         assert np.all(np.isfinite(st[:4])) and np.all(st[1, :c.n_in] > 0) and np.all(st[3, :c.n_out] > 0)
         assert np.all(st[4, :c.n_in] <= 0.0) and np.all(st[5, :c.n_in] >= 0.0)
+        # targets: log bt of the plain closure (bt >= 1e-8), their range kept
+        lo, hi = st[6, :c.n_out], st[7, :c.n_out]
+        assert np.all(np.isfinite(lo)) and np.all(lo <= hi) and np.all(lo >= np.log(1e-8) - 1e-4)
     finally:
         c.close()
 
