@@ -465,12 +465,13 @@ __global__ void k_filt2x_uc(Dev d) {
 
 // ---------------------------------------------------------------------------
 // velrhs: compute_vel_rhs (fv_3D_vel.F90:1-180), one thread per (element,
-// level) with levels on consecutive lanes.  The loop runs over whole warps so
-// that the vertical flux at interface z+1 comes from the next lane.
+// level) with levels on consecutive lanes.  Each warp takes 31 outputs and
+// its lane 31 forms the vertical flux at its own index, the interface below
+// lane 30's layer, so the flux at interface z+1 comes from the next lane
+// for every output and no lane forms a second flux.
 // ff = 1 on the very first call (lfirst), 1.5+epsilon afterwards.
-// (Sharing the fluxes across the block through shared memory, so that only
-// one thread in 256 computes a second flux, was measured 16 % slower: the
-// block-wide barrier costs more than the lane-31 recomputation.)
+// (Sharing the fluxes across the block through shared memory was measured
+// 16 % slower than recomputing them: the block-wide barrier costs more.)
 // ---------------------------------------------------------------------------
 // 4 resident blocks (at most 64 registers) in both forms: in FP64 the few
 // spilled registers cost less than the lost warps (11 % faster than 3
@@ -478,10 +479,11 @@ __global__ void k_filt2x_uc(Dev d) {
 __global__ void __launch_bounds__(256, 4) k_velrhs(Dev d, real ff) {
     const long long total = (long long)d.E * d.L;
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
-        const bool valid = wbase + lane < total;
-        const long long ii = valid ? wbase + lane : total - 1;
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 31 < total; c += nwarp) {
+        const long long iw = c * 31 + lane;
+        const bool valid = lane < 31 && iw < total;
+        const long long ii = iw < total ? iw : total - 1;
         const int e = (int)(ii / d.L);
         const int z = (int)(ii % d.L);
         const int L = d.L;
@@ -545,8 +547,7 @@ __global__ void __launch_bounds__(256, 4) k_velrhs(Dev d, real ff) {
             real fu0, fv0;
             uvert_at(d, e, z, w, en, ar, fu0, fv0);
             real fu1 = __shfl_down_sync(kFull, fu0, 1), fv1 = __shfl_down_sync(kFull, fv0, 1);
-            if (z == L - 1) { fu1 = real(0.0); fv1 = real(0.0); }
-            else if (lane == 31) uvert_at(d, e, z + 1, w, en, ar, fu1, fv1);
+            if (z == L - 1) { fu1 = real(0.0); fv1 = real(0.0); }   // the bottom interface carries no flux
             if (mwd != real(0.0)) {
                 const real acc = d.elem_acc[e];
                 uab = uab + (fu0 - fu1) * acc;

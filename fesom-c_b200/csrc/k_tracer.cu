@@ -138,6 +138,51 @@ __device__ __forceinline__ real tvert_upwind(const Dev &d, int k, real a, const 
     return -(T(nz) * (real(1.0) - dg - db) + T(nz - 1) * db + T(nz - 2) * dg) * w;
 }
 
+// tvert_upwind of T and S of the same column: the interface weights, the
+// same for both tracers, are formed once (same expressions, same bits)
+template <typename F, typename G>
+__device__ __forceinline__ void tvert_upwind2(const Dev &d, int k, real a, const real *W, F TO, G SO, real &tv,
+                                              real &sv) {
+    const int NS = d.NS;
+    if (k == NS - 1) { tv = real(0.0); sv = real(0.0); return; }
+    if (k == 0) { tv = -W[0] * TO(0); sv = -W[0] * SO(0); return; }
+    const int nz = k + 1;  // 1-based
+    auto Z = [&](int m) { return z_of(d, a, m - 1); };
+    auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
+    const real w = W[nz - 1];
+    // a quadratic over layers m0, m1, m2 (1-based) with weights 1-dg-db, db,
+    // dg, or the single layer m0
+    int m0, m1 = 0, m2 = 0;
+    real dg = real(0.0), db = real(0.0);
+    bool quad = true;
+    if (nz == 2) {
+        if (w > real(0.0)) {
+            dg = (ZB(2) - Z(1)) * (Z(2) - ZB(2)) / ((Z(3) - Z(1)) * (Z(2) - Z(3)));
+            db = -(ZB(2) - Z(1)) * (Z(3) - ZB(2)) / ((Z(2) - Z(1)) * (Z(2) - Z(3)));
+            m0 = 1; m1 = 2; m2 = 3;
+        } else {
+            m0 = 1; quad = false;
+        }
+    } else if (nz <= NS - 2 && w >= real(0.0)) {
+        dg = (ZB(nz) - Z(nz - 1)) * (Z(nz) - ZB(nz)) / ((Z(nz + 1) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+        db = -(ZB(nz) - Z(nz - 1)) * (Z(nz + 1) - ZB(nz)) / ((Z(nz) - Z(nz - 1)) * (Z(nz) - Z(nz + 1)));
+        m0 = nz - 1; m1 = nz; m2 = nz + 1;
+    } else if (nz == NS - 1 && w >= real(0.0)) {
+        m0 = nz; quad = false;
+    } else {
+        dg = (Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 1)) / ((Z(nz) - Z(nz - 2)) * (Z(nz - 2) - Z(nz - 1)));
+        db = -(Z(nz) - ZB(nz)) * (ZB(nz) - Z(nz - 2)) / ((Z(nz) - Z(nz - 1)) * (Z(nz - 2) - Z(nz - 1)));
+        m0 = nz; m1 = nz - 1; m2 = nz - 2;
+    }
+    if (quad) {
+        tv = -(TO(m0 - 1) * (real(1.0) - dg - db) + TO(m1 - 1) * db + TO(m2 - 1) * dg) * w;
+        sv = -(SO(m0 - 1) * (real(1.0) - dg - db) + SO(m1 - 1) * db + SO(m2 - 1) * dg) * w;
+    } else {
+        tv = -TO(m0 - 1) * w;
+        sv = -SO(m0 - 1) * w;
+    }
+}
+
 // AB2 tracers of this step minus their means, stored once per (node, level)
 // for the gathers below (fv_tracer.F90:433,435 and :39-47)
 __global__ void k_ab2_node(Dev d) {
@@ -157,10 +202,14 @@ __global__ void k_upwind_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const int L = d.L, NS = d.NS;
     const long long total = (long long)d.N * L;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
-        const bool valid = wbase + lane < total;
-        const long long i_ = valid ? wbase + lane : total - 1;
+    // each warp takes 31 (node, level) outputs; lane 31 forms the flux at its
+    // own index, the interface below lane 30's layer, for the shuffle, so no
+    // lane forms a second flux
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 31 < total; c += nwarp) {
+        const long long iw = c * 31 + lane;
+        const bool valid = lane < 31 && iw < total;
+        const long long i_ = iw < total ? iw : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L), zc = z;
         const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
@@ -212,12 +261,10 @@ __global__ void k_upwind_h(Dev d) {
             }
             auto TO = [&](int m) { return d.ttfold[base + m]; };
             auto SO = [&](int m) { return d.stfold[base + m]; };
-            const real tv0 = tvert_upwind(d, zc, a, W, TO), sv0 = tvert_upwind(d, zc, a, W, SO);
+            real tv0, sv0;
+            tvert_upwind2(d, zc, a, W, TO, SO, tv0, sv0);
             real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
-            if (lane == 31 || zc == L - 1) {
-                tv1 = tvert_upwind(d, zc + 1, a, W, TO);
-                sv1 = tvert_upwind(d, zc + 1, a, W, SO);
-            }
+            if (zc == L - 1) { tv1 = real(0.0); sv1 = real(0.0); }   // the bottom interface carries no flux
             if (valid) {
                 const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
                 const size_t ii = base + z;
@@ -334,9 +381,51 @@ __device__ __forceinline__ real tvert_quick(const Dev &d, int k, real a, const r
     }
     return -Tmean * W[k];
 }
-template <typename F>
-__device__ __forceinline__ real tvert_muscl(const Dev &d, int k, real a, const real *W, F TO) {
-    return tvert_quick<true>(d, k, a, W, TO);
+
+// tvert_quick of T and S of the same column: the weights, the same for both
+// tracers, are formed once (same expressions, same bits)
+template <bool MUSCL, typename F, typename G>
+__device__ __forceinline__ void tvert_quick2(const Dev &d, int k, real a, const real *W, F TO, G SO, real &tv,
+                                             real &sv) {
+    const int NS = d.NS;
+    if (k == NS - 1) { tv = real(0.0); sv = real(0.0); return; }
+    if (k == 0) { tv = -W[0] * TO(0); sv = -W[0] * SO(0); return; }
+    real Tmean = real(0.0), Smean = real(0.0);
+    int start = k + 1;
+    while (start > 2 && W[start - 1] == real(0.0)) --start;
+    for (int nz = start; nz <= k + 1; ++nz) {
+        const real w = W[nz - 1];
+        auto Z = [&](int m) { return z_of(d, a, m - 1); };
+        auto ZB = [&](int m) { return zbar_of(d, a, m - 1); };
+        if (w > real(0.0)) {
+            if (nz == NS - 1) {
+                Tmean = TO(nz - 1);
+                Smean = SO(nz - 1);
+            } else {
+                const real aa = ZB(nz) - Z(nz - 1), bb = Z(nz) - ZB(nz), cc = Z(nz + 1) - ZB(nz);
+                const real dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const real db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
+                const real da = real(1.0) - dg - db;
+                Tmean = TO(nz - 2) * da + TO(nz - 1) * db + TO(nz) * dg;
+                Smean = SO(nz - 2) * da + SO(nz - 1) * db + SO(nz) * dg;
+            }
+        }
+        if (w < real(0.0)) {
+            if (nz == 2) {
+                Tmean = TO(nz - 2);
+                Smean = SO(nz - 2);
+            } else {
+                const real aa = Z(nz) - ZB(nz), bb = ZB(nz) - Z(nz - 1), cc = ZB(nz) - Z(nz - 2);
+                const real dg = MUSCL ? aa * bb / (cc + aa) / (bb - cc) : aa * bb / ((cc + aa) * (bb - cc));
+                const real db = MUSCL ? -aa * cc / (bb + aa) / (bb - cc) : -aa * cc / ((bb + aa) * (bb - cc));
+                const real da = real(1.0) - dg - db;
+                Tmean = TO(nz - 1) * da + TO(nz - 2) * db + TO(nz - 3) * dg;
+                Smean = SO(nz - 1) * da + SO(nz - 2) * db + SO(nz - 3) * dg;
+            }
+        }
+    }
+    tv = -Tmean * W[k];
+    sv = -Smean * W[k];
 }
 
 __device__ __forceinline__ real muscl_mean(bool upw2, real Tm1, real Tm2) {
@@ -424,10 +513,14 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
     const long long total = (long long)d.N * d.L;
     const int lane = threadIdx.x & 31;
     const int L = d.L, NS = d.NS;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
-        const bool valid = wbase + lane < total;
-        const long long i_ = valid ? wbase + lane : total - 1;
+    // each warp takes 31 (node, level) outputs; lane 31 forms the flux at its
+    // own index, the interface below lane 30's layer, for the shuffle, so no
+    // lane forms a second flux
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 31 < total; c += nwarp) {
+        const long long iw = c * 31 + lane;
+        const bool valid = lane < 31 && iw < total;
+        const long long i_ = iw < total ? iw : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L);
         const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
@@ -453,12 +546,10 @@ __global__ void __launch_bounds__(128, 8) k_muscl_h(Dev d) {
         }
         auto TO = [&](int m) { return d.ttfold[base + m]; };
         auto SO = [&](int m) { return d.stfold[base + m]; };
-        const real tv0 = tvert_muscl(d, z, an, W, TO), sv0 = tvert_muscl(d, z, an, W, SO);
+        real tv0, sv0;
+        tvert_quick2<true>(d, z, an, W, TO, SO, tv0, sv0);
         real tv1 = __shfl_down_sync(kFull, tv0, 1), sv1 = __shfl_down_sync(kFull, sv0, 1);
-        if (lane == 31 || z == L - 1) {
-            tv1 = tvert_muscl(d, z + 1, an, W, TO);
-            sv1 = tvert_muscl(d, z + 1, an, W, SO);
-        }
+        if (z == L - 1) { tv1 = real(0.0); sv1 = real(0.0); }   // the bottom interface carries no flux
         if (valid) {
             const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
             const size_t ii = base + z;
@@ -621,10 +712,14 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
     const int lane = threadIdx.x & 31;
     const int L = d.L, NS = d.NS;
     const long long total = (long long)d.N * L;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long wbase = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; wbase < total; wbase += stride) {
-        const bool valid = wbase + lane < total;
-        const long long i_ = valid ? wbase + lane : total - 1;
+    // each warp takes 31 (node, level) outputs; lane 31 forms the flux at its
+    // own index, the interface below lane 30's layer, for the shuffle, so no
+    // lane forms a second flux
+    const long long nwarp = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c * 31 < total; c += nwarp) {
+        const long long iw = c * 31 + lane;
+        const bool valid = lane < 31 && iw < total;
+        const long long i_ = iw < total ? iw : total - 1;
         const int n = (int)(i_ / L);
         const int z = (int)(i_ % L), zc = z;
         const real T_aver = t_aver_of(d, n);
@@ -652,7 +747,7 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
             auto TN = [&](int m) { return d.tnow[base + m]; };
             const real tv0 = tvert_quick<false>(d, zc, an, W, TN);
             real tv1 = __shfl_down_sync(kFull, tv0, 1);
-            if (lane == 31 || zc == L - 1) tv1 = tvert_quick<false>(d, zc + 1, an, W, TN);
+            if (zc == L - 1) tv1 = real(0.0);   // the bottom interface carries no flux
             if (valid) {
                 const bool relax = d.cl_relax && d.index_nod2D[n] == 2;
                 const real area = d.area[n];
