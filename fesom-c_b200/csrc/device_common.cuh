@@ -75,12 +75,13 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // Launch-shape knobs (fesomc_gpu_tune_*): threads per block of the kernels
 // whose results do not depend on the block shape (one thread per entity or
 // per (entity, level), grid-stride, no block-level reduction), and entities
-// per block of the column kernels (pressure_col, bpg_elem, update3d, wvel).
-// A value of 0 selects the built-in default.
+// per block of the column kernels (pressure_col, bpg_elem, update3d, wvel),
+// and where d3_end keeps its column arrays (1 local memory, 2 shared
+// memory).  A value of 0 selects the built-in default.
 enum TuneKnob : int {
     TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_P1EDGE, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
     TK_SSHNODE, TK_ADV2D, TK_U2D, TK_ROT, TK_ZEROFILT, TK_AB2, TK_MEGRAD, TK_MNGRAD, TK_MEDGE, TK_MH,
-    TK_UPWIND, TK_AV, TK_COLUMNS, kTuneKnobs
+    TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, kTuneKnobs
 };
 
 namespace f64 {

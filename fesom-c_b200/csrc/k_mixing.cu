@@ -191,6 +191,185 @@ __global__ void k_d3end(Dev d, const int *list, const unsigned long long *count)
     }
 }
 
+// The same closure with the column arrays in shared memory, laid out
+// [array][level][thread] so that a warp's access to one level is 32
+// consecutive words (launch-shape knob "d3end_arrays" = 2):
+//   sn        snu(nz), nz = 1..NS                 (constant over the iteration)
+//   bA, bB    btr / btr1 / xx1, nz = 1..NS        (alternating; the back
+//             substitution writes btr1(k) into the xx1(k) slot it has just
+//             read, xx1(2) = 1 and yy1(2) = y2 being constants)
+//   yy1       yy1(nz), nz = 3..NS
+//   pb, qb, c2  -b1-b2, t_inv*bt and c2, nz = 2..NS-1 (constant)
+// i.e. 7*NS - 8 values per column: its DRAM traffic is the algorithmic
+// bytes, but only 6 warps of 32 columns fit an SM, so the set-up and final
+// level loops are unrolled for independent work per thread.  The same
+// arithmetic as k_d3end, in the same order.
+constexpr int kD3Block = 32;
+
+__host__ __device__ inline int d3end_values(int NS) { return 7 * NS - 8; }
+
+template <bool kList>
+__global__ void __launch_bounds__(kD3Block, 6) k_d3end_sm(Dev d, const int *list, const unsigned long long *count) {
+    extern __shared__ unsigned char d3_smem[];
+    constexpr int B = kD3Block;
+    const int NS = d.NS, L = d.L;
+    real *const base = reinterpret_cast<real *>(d3_smem) + threadIdx.x;
+    // per-array views: element nz of an array at [(nz - first) * B]
+    real *const s_sn = base - 1 * B;                     // nz = 1..NS
+    real *const s_bA = base + (NS - 1) * B;              // nz = 1..NS
+    real *const s_bB = base + (2 * NS - 1) * B;          // nz = 1..NS
+    real *const s_yy = base + (3 * NS - 3) * B;          // nz = 3..NS
+    real *const s_pb = base + (4 * NS - 4) * B;          // nz = 2..NS-1
+    real *const s_qb = base + (5 * NS - 6) * B;          // nz = 2..NS-1
+    real *const s_c2 = base + (6 * NS - 8) * B;          // nz = 2..NS-1
+#define D3(a, nz) a[(size_t)(nz) * B]
+    const real t_inv = real(1.0) / d.dt;
+    const real cka = d.cka;
+    const real B1cka2 = real(16.6) * (cka * cka);
+    const long long ncol = kList ? (long long)*count : (long long)d.N;
+    GRID_LOOP(ii, ncol) {
+        const int node = kList ? list[ii] : (int)ii;
+        const real *bt = d.bt + (size_t)node * NS;
+        const real *snu = d.snu + (size_t)node * NS;
+        const real *Kv = d.Kv + (size_t)node * NS;
+        const real *Un = d.Unode + (size_t)node * L;
+        const real *Vn = d.Vnode + (size_t)node * L;
+        const real *T = d.TF + (size_t)node * L;
+        const real *S = d.SF + (size_t)node * L;
+        real *Ri = d.Ri + (size_t)node * NS;
+        real *tke = d.tke_dissip + (size_t)node * NS;
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const real dmean2 = dmean * dmean;
+        const real ajac = jac_a(d, d.eta_jac, node);
+        for (int nz = 1; nz <= NS; ++nz) {
+            D3(s_bA, nz) = bt[nz - 1];
+            D3(s_sn, nz) = snu[nz - 1];
+        }
+        Ri[0] = real(0.0);
+        Ri[NS - 1] = real(0.0);
+#pragma unroll 4
+        for (int nz = 2; nz <= NS - 1; ++nz) {
+            const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+            const real d1 = s_m - s_0;
+            const real d2 = s_0 - s_p;
+            const real dd = real(0.5) * (d1 + d2);
+            real ap1 = Un[nz - 2] - Un[nz - 1];
+            const real ap2 = Vn[nz - 2] - Vn[nz - 1];
+            const real sn_m = snu[nz - 2], sn_0 = snu[nz - 1], sn_p = snu[nz];
+            real b1 = sn_0 * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            b1 = b1 / dmean2;
+            const real zb = zbar_of(d, ajac, nz - 1);
+            const real rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
+            const real rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
+            ap1 = (rho_up - rho_dn) / dd;
+            const real b2 = -real(0.5) * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const real snu_p = real(0.5) * (sn_m + sn_0);
+            const real snu_m = real(0.5) * (sn_0 + sn_p);
+            const real cc = real(0.5) * real(0.73) * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
+            D3(s_c2, nz) = cc / dmean2;
+            if (b1 > real(0.0)) Ri[nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn_0;
+            else Ri[nz - 1] = real(10000.0);
+            D3(s_pb, nz) = -b1 - b2;
+            D3(s_qb, nz) = t_inv * bt[nz - 1];
+        }
+        real y2;
+        {
+            const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const real wx = d.windx[node], wy = d.windy[node];
+            const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+            const real snu_m = real(0.5) * (snu[NS - 1] + snu[NS - 2]);
+            y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
+        }
+        // bottom boundary value (independent of the iteration)
+        const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const real lg = fesomc_log(delta_b / d.z0b_min);
+        const real bott_R = B1cka2 / (lg * lg);
+        const real ubt = Un[L - 1], vbt = Vn[L - 1];
+        const real bot = bott_R * (ubt * ubt + vbt * vbt);
+        real *btr = s_bA, *xq = s_bB;   // xq: this iteration's xx1, then its btr1
+        bool converged = false;
+        int iters = 200;
+        for (int it = 1; it <= 200; ++it) {
+            real x = real(1.0), y = y2;
+            real s_lo = D3(s_sn, 1), s_mid = D3(s_sn, 2);
+            real b_n = D3(btr, 2), pb_n = D3(s_pb, 2), qb_n = D3(s_qb, 2), c2_n = D3(s_c2, 2), sh_n = D3(s_sn, 3);
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const real s_hi = sh_n;
+                const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n;
+                if (nz + 1 <= NS - 1) {
+                    b_n = D3(btr, nz + 1); pb_n = D3(s_pb, nz + 1); qb_n = D3(s_qb, nz + 1);
+                    c2_n = D3(s_c2, nz + 1); sh_n = D3(s_sn, nz + 2);
+                }
+                const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const real dd1 = s_m - s_0;
+                const real dd2 = s_0 - s_p;
+                const real dd = real(0.5) * (dd1 + dd2);
+                const real c1 = real(0.046) * (b * b) / s_mid;
+                if (it == 200) tke[nz - 1] = c1;
+                const real fr = pbv - c1 - qbv - c2v;
+                const real snu_p = real(0.5) * (s_lo + s_mid);
+                const real snu_mm = real(0.5) * (s_mid + s_hi);
+                const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+                const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
+                const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
+                const real a = bm - am * x;
+                const real xn = cm / a;
+                const real yn = (am * y - fr) / a;
+                D3(xq, nz + 1) = xn;
+                D3(s_yy, nz + 1) = yn;
+                x = xn;
+                y = yn;
+                s_lo = s_mid;
+                s_mid = s_hi;
+            }
+            real b1v = bot;  // btr1(NS)
+            real x_n = D3(xq, NS), y_n = D3(s_yy, NS), o_n = D3(btr, NS - 1);
+            const real top = D3(btr, NS);
+            D3(xq, NS) = b1v;
+            bool above = d3_above_tol(top - b1v, dmax(b1v, top) + real(1.0e-8));
+            for (int nz = NS; nz >= 2; --nz) {
+                const real xv = x_n, yv = y_n, ov = o_n;
+                if (nz - 1 >= 3) { x_n = D3(xq, nz - 1); y_n = D3(s_yy, nz - 1); o_n = D3(btr, nz - 2); }
+                else if (nz - 1 == 2) { x_n = real(1.0); y_n = y2; o_n = D3(btr, nz - 2); }
+                b1v = b1v * xv + yv;  // btr1(nz-1), into the xx1(nz-1) slot already read
+                D3(xq, nz - 1) = b1v;
+                above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
+            }
+            if (!above) { converged = true; iters = it; break; }
+            real *t = btr;
+            btr = xq;
+            xq = t;
+        }
+        if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
+        if (converged) {
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const real b = D3(btr, nz);
+                tke[nz - 1] = real(0.046) * (b * b) / D3(s_sn, nz);
+            }
+        } else {
+            atomicAdd(d.notconv, 1);
+        }
+        real *btw = d.bt + (size_t)node * NS;
+        real *snw = d.snu + (size_t)node * NS;
+        real *Kvw = d.Kv + (size_t)node * NS;
+#pragma unroll 4
+        for (int nz = 1; nz <= NS; ++nz) {
+            const real btn = dmax(D3(btr, nz), real(1.0e-8));
+            btw[nz - 1] = btn;
+            const real zt = __ldg(d.sig + nz - 1) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = cka * Zh * Zd * Z0 / dmean;
+            real s = scale_t * sqrt(btn) + d.snul;
+            if (s >= real(0.2)) s = real(0.2);
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+#undef D3
+}
+
 // Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
 __global__ void k_av(Dev d) {
     const long long total = (long long)d.E * d.NS;
@@ -205,9 +384,15 @@ __global__ void k_av(Dev d) {
     }
 }
 
-int config_d3end(const Dev &d) { return d.NS <= 127 ? 0 : 1; }
+static size_t d3end_smem(const Dev &d) { return (size_t)d3end_values(d.NS) * kD3Block * sizeof(real); }
+int config_d3end(const Dev &d) {
+    if (d.NS > 127) return 1;
+    return (raise_smem_limit(k_d3end_sm<false>, d3end_smem(d)) == cudaSuccess &&
+            raise_smem_limit(k_d3end_sm<true>, d3end_smem(d)) == cudaSuccess) ? 0 : 1;
+}
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.NS <= 11) k_d3end<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    if (d.tune[TK_D3END] == 2) k_d3end_sm<false><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 11) k_d3end<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 21) k_d3end<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 40) k_d3end<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else k_d3end<128, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
@@ -215,7 +400,8 @@ void launch_d3end(const Dev &d, cudaStream_t s) {
 // the plain closure on the listed columns (count read on the device, so the
 // launch covers every node and the grid-stride loop stops at the count)
 void launch_d3end_list(const Dev &d, const int *list, const unsigned long long *count, cudaStream_t s) {
-    if (d.NS <= 11) k_d3end<12, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
+    if (d.tune[TK_D3END] == 2) k_d3end_sm<true><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, list, count);
+    else if (d.NS <= 11) k_d3end<12, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
     else if (d.NS <= 21) k_d3end<22, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
     else if (d.NS <= 40) k_d3end<41, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);
     else k_d3end<128, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);

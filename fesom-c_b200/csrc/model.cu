@@ -1826,6 +1826,7 @@ const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"muscl_egrad", "muscl_egrad", 256}, {"muscl_ngrad", "muscl_ngrad", 256}, {"muscl_edge", "muscl_edge", 256},
     {"muscl_h", "muscl_h", 128}, {"upwind_h", "upwind_h", 128}, {"av", "av", 256},
     {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
+    {"d3end_arrays", "d3end,d3end_list", 1},
 };
 int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
 void drop_graph(fesomc_model *m);
@@ -1854,12 +1855,13 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     fesomc::f32::tune_limits_baroclinic(lim); fesomc::f32::tune_limits_barotropic(lim);
     fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
+    lim[fesomc::TK_D3END] = 2;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         if (values) {
             const int v = m->d.tune[k];
             values[k] = v > 0 ? v : (kKnobs[k].def > 0 ? kKnobs[k].def : default_columns(m->d.L));
         }
-        if (limits) limits[k] = k == fesomc::TK_COLUMNS ? lim[k] : (lim[k] / 32) * 32;
+        if (limits) limits[k] = (k == fesomc::TK_COLUMNS || k == fesomc::TK_D3END) ? lim[k] : (lim[k] / 32) * 32;
     }
     return FESOMC_OK;
 }
@@ -1872,7 +1874,7 @@ int fesomc_gpu_tune_set(fesomc_model *m, const int32_t *values) {
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         const int v = values[k];
         if (v < 0 || v > lim[k]) return FESOMC_EINVAL;
-        if (k != fesomc::TK_COLUMNS && v != 0 && (v < 32 || v % 32 != 0)) return FESOMC_EINVAL;
+        if (k != fesomc::TK_COLUMNS && k != fesomc::TK_D3END && v != 0 && (v < 32 || v % 32 != 0)) return FESOMC_EINVAL;
     }
     drop_graph(m);   // the captured step holds the old launch shapes
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) m->d.tune[k] = m->d32.tune[k] = values[k];

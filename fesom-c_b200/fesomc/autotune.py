@@ -28,6 +28,7 @@ from . import abi, cases, model
 
 THREADS = (64, 128, 256, 512, 1024)
 COLUMNS = (1, 2, 4, 8, 16, 32)
+D3END_ARRAYS = (1, 2)   # d3_end's column arrays: local memory, shared memory
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "launch_shapes_b200.json")
 
 
@@ -129,7 +130,7 @@ def search(case, steps=3, warmup=2, margin=0.02, log=None):
         before = profile(g, steps)
         trials = 0
         for name, recs in ks:
-            cands = COLUMNS if name == "columns" else THREADS
+            cands = COLUMNS if name == "columns" else (D3END_ARRAYS if name == "d3end_arrays" else THREADS)
             cands = [c for c in cands if c <= lim[name]]
 
             def t_of(v):
