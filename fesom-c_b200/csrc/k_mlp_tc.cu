@@ -166,9 +166,19 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// SiLU with the fast exponential and division (BF16 output: their error,
-// about 1e-6 relative, is far below the BF16 rounding)
-__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
+// SiLU as z/2 (1 + tanh(z/2)) with the hardware tanh approximation (one
+// special-function operation per activation instead of an exponential and a
+// reciprocal: the epilogue is bound by that pipe; the approximation's error,
+// about 2^-11 relative, is below the BF16 rounding of the result)
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float silu_fast(float z) {
+    const float h = 0.5f * z;
+    return fmaf(h, tanh_approx(h), h);
+}
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -300,19 +310,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
             const long long row0 = tile * kTM;
             const long long left = p.ncol - row0;
             const int nr = left < kTM ? (int)left : kTM;
-            // inputs to BF16 (coalesced over the tile's contiguous rows),
-            // zero K padding; rows beyond ncol keep stale values (their
-            // outputs are not stored)
+            // inputs to BF16, one (8-wide K chunk, row) per item with the row
+            // fastest: each item is one 16-byte store (consecutive threads,
+            // consecutive rows: no bank conflicts), the K padding zero; rows
+            // beyond ncol keep stale values (their outputs are not stored)
             const float *x = p.X + row0 * p.IN;
-            for (int i = e; i < nr * p.IN; i += kEpiThreads) {
-                const int rr = i / p.IN, k = i - rr * p.IN;
-                *reinterpret_cast<__nv_bfloat16 *>(sH + (size_t)(k >> 3) * kSlab + (size_t)rr * 16 + (k & 7) * 2) =
-                    __float2bfloat16_rn(__ldg(x + i));
-            }
-            for (int i = e; i < (p.K1p - p.IN) * kTM; i += kEpiThreads) {
-                const int k = p.IN + i / kTM, rr = i % kTM;
-                *reinterpret_cast<__nv_bfloat16 *>(sH + (size_t)(k >> 3) * kSlab + (size_t)rr * 16 + (k & 7) * 2) =
-                    __float2bfloat16_rn(0.0f);
+            for (int i = e; i < (p.K1p / 8) * kTM; i += kEpiThreads) {
+                const int kc = i / kTM, rr = i - kc * kTM;
+                if (rr >= nr) continue;
+                const float *xr = x + (size_t)rr * p.IN + 8 * kc;
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) v[j] = (8 * kc + j < p.IN) ? __ldg(xr + j) : 0.0f;
+                uint4 o;
+                o.x = pack_bf16(v[0], v[1]);
+                o.y = pack_bf16(v[2], v[3]);
+                o.z = pack_bf16(v[4], v[5]);
+                o.w = pack_bf16(v[6], v[7]);
+                *reinterpret_cast<uint4 *>(sH + (size_t)kc * kSlab + (size_t)rr * 16) = o;
             }
             fence_proxy();
             __syncwarp();
