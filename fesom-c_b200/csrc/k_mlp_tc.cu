@@ -7,14 +7,16 @@
 //   warp 0       producer: streams the weights, unit by unit, from global
 //                memory (L2-resident: every CTA reads the same ~330 KB) into
 //                a ring of kSlots shared-memory slots with bulk copies
-//                (cp.async.bulk, completion counted on the slot's mbarrier);
+//                (cp.async.bulk, completion counted on the slot's mbarrier),
+//                and the next tile's inputs (its rows are contiguous) into an
+//                FP32 staging buffer one tile ahead;
 //   warp 1       MMA issuer (one lane): per layer and unit, K/16
 //                tcgen05.mma (M = 128 columns, N = 64 neurons, K = 16) into
 //                tensor memory, a commit that frees the slot, and after the
 //                layer's last unit a commit that hands the accumulator over;
 //   warps 4..    epilogue (kEpiWarps warps, kEpiWarps/4 per TMEM lane
 //                quarter, each a share of the accumulator columns): the
-//                tile's normalised FP32 inputs to BF16 in shared memory,
+//                tile's staged FP32 inputs to BF16 in shared memory,
 //                then per hidden layer bias + SiLU of the accumulator
 //                (tcgen05.ld) back to shared memory as the next layer's A
 //                operand, and the last layer's FP32 outputs to global memory.
@@ -50,7 +52,7 @@ namespace {
 
 constexpr int kTM = 128;                  // columns per tile (MMA M)
 constexpr int kUnitN = 64;                // output neurons per weight unit (MMA N)
-constexpr int kSlots = 4;                 // weight slots in shared memory
+constexpr int kSlots = 3;                 // weight slots in shared memory
 constexpr int kSlotBytes = kUnitN * 256 * 2;
 constexpr int kEpiWarps = 8;              // 2 per TMEM lane quarter
 constexpr int kEpiThreads = 32 * kEpiWarps;
@@ -59,8 +61,8 @@ constexpr int kSlab = kTM * 16;           // bytes of one 8-wide K chunk of the 
 constexpr uint32_t kTmemCols = 256;
 constexpr int kMaxUnits = 16;
 constexpr uint32_t kSpin = 1u << 25;
-// barriers: full[kSlots], empty[kSlots], acc_full, a_ready, drain
-constexpr int kBars = 2 * kSlots + 3;
+// barriers: full[kSlots], empty[kSlots], acc_full, a_ready, drain, x_full, x_empty
+constexpr int kBars = 2 * kSlots + 5;
 
 struct TcParams {
     int IN, OUT, K1p, N4p;
@@ -78,7 +80,7 @@ struct TcParams {
     const float *b1, *b2, *b3, *b4;
     unsigned int *err;
     // shared-memory offsets (bytes)
-    int oH, oW, oB, oBar;
+    int oH, oW, oX, oB, oBar;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -198,6 +200,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
     auto full_bar = [&](int s) { return bar0 + 8u * (uint32_t)s; };
     auto empty_bar = [&](int s) { return bar0 + 8u * (uint32_t)(kSlots + s); };
     const uint32_t acc_bar = bar0 + 8u * (2 * kSlots), a_bar = acc_bar + 8u, drain_bar = acc_bar + 16u;
+    const uint32_t xfull_bar = acc_bar + 24u, xempty_bar = acc_bar + 32u;
+    const float *sX = reinterpret_cast<const float *>(sm + p.oX);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + p.oBar + 8 * kBars);
     volatile int *sfail = reinterpret_cast<volatile int *>(sm + p.oBar + 8 * kBars + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -217,6 +221,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
         mbar_init(acc_bar, 1);
         mbar_init(a_bar, kEpiWarps);
         mbar_init(drain_bar, 1);
+        mbar_init(xfull_bar, 1);
+        mbar_init(xempty_bar, kEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -236,8 +242,30 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
         // ---- producer: every unit of every tile of this CTA, in order ----
         if (lane == 0) {
             long long g = 0;   // units issued
+            long long xk = 0;  // input tiles issued
             bool ok = true;
-            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
+            // the inputs of tile t: its rows are contiguous; the bulk copy
+            // takes the whole 16-byte multiple, the epilogue the rest
+            auto issue_x = [&](long long t) {
+                const long long left = p.ncol - t * kTM;
+                const int nr = left < kTM ? (int)left : kTM;
+                const uint32_t bytes = (uint32_t)((size_t)nr * p.IN * 4) & ~15u;
+                mbar_expect_tx(xfull_bar, bytes);
+                if (bytes) bulk_g2s(smem_u32(sm + p.oX), p.X + t * kTM * p.IN, bytes, xfull_bar);
+                ++xk;
+            };
+            if (blockIdx.x < ntiles) issue_x(blockIdx.x);
+            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                const long long nxt = tile + gridDim.x;
+                if (nxt < ntiles) {
+                    // the staging buffer is free once this tile's inputs are converted
+                    if (!bar_wait(xempty_bar, (uint32_t)((xk - 1) & 1), sfail)) {
+                        fail_now(sfail, p.err);
+                        ok = false;
+                        break;
+                    }
+                    issue_x(nxt);
+                }
                 for (int u = 0; u < U; ++u) {
                     const int s = (int)(g % kSlots);
                     const long long n = g / kSlots;
@@ -251,13 +279,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
                              full_bar(s));
                     ++g;
                 }
+            }
             // every copy issued lands before the CTA may leave: wait for the
             // phase of each slot's last use (already complete when the MMAs
-            // consumed it)
+            // consumed it) and of the last input tile
             for (int s = 0; s < kSlots; ++s) {
                 const long long uses = g > s ? (g - 1 - s) / kSlots + 1 : 0;
                 if (uses > 0) bar_wait(full_bar(s), (uint32_t)((uses - 1) & 1), nullptr);
             }
+            if (xk > 0) bar_wait(xfull_bar, (uint32_t)((xk - 1) & 1), nullptr);
         }
     } else if (warp == 1) {
         // ---- MMA issuer ----
@@ -304,12 +334,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
         const int part = (warp - 4) >> 2;           // share of the columns
         constexpr int nparts = kEpiWarps / 4;
         const int r = 32 * q + lane;                // tile row of this thread
-        long long acc_uses = 0;
+        long long acc_uses = 0, x_uses = 0;
         bool ok = true;
         for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
             const long long row0 = tile * kTM;
             const long long left = p.ncol - row0;
             const int nr = left < kTM ? (int)left : kTM;
+            if (!bar_wait(xfull_bar, (uint32_t)(x_uses & 1), sfail)) {
+                fail_now(sfail, p.err);
+                break;
+            }
+            ++x_uses;
+            const int staged = (int)(((uint32_t)((size_t)nr * p.IN * 4) & ~15u) / 4);   // floats in sX
             // inputs to BF16, one (8-wide K chunk, row) per item with the row
             // fastest: each item is one 16-byte store (consecutive threads,
             // consecutive rows: no bank conflicts), the K padding zero; rows
@@ -318,10 +354,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
             for (int i = e; i < (p.K1p / 8) * kTM; i += kEpiThreads) {
                 const int kc = i / kTM, rr = i - kc * kTM;
                 if (rr >= nr) continue;
-                const float *xr = x + (size_t)rr * p.IN + 8 * kc;
                 float v[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) v[j] = (8 * kc + j < p.IN) ? __ldg(xr + j) : 0.0f;
+                for (int j = 0; j < 8; ++j) {
+                    const int k = 8 * kc + j, f = rr * p.IN + k;
+                    v[j] = k < p.IN ? (f < staged ? sX[f] : __ldg(x + f)) : 0.0f;
+                }
                 uint4 o;
                 o.x = pack_bf16(v[0], v[1]);
                 o.y = pack_bf16(v[2], v[3]);
@@ -331,7 +369,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
             }
             fence_proxy();
             __syncwarp();
-            if (lane == 0) mbar_arrive(a_bar);
+            if (lane == 0) {
+                mbar_arrive(xempty_bar);   // the staging buffer may take the next tile
+                mbar_arrive(a_bar);
+            }
             for (int l = 0; l < 4; ++l) {
                 if (!bar_wait(acc_bar, (uint32_t)(acc_uses & 1), sfail)) {
                     fail_now(sfail, p.err);
@@ -426,7 +467,7 @@ UnitPlan unit_plan(int K1p, int N4p) {
     return u;
 }
 
-size_t tc_smem(TcParams *o) {
+size_t tc_smem(int IN, TcParams *o) {
     size_t off = 0;
     auto take = [&](size_t bytes) {
         const size_t at = off;
@@ -434,9 +475,9 @@ size_t tc_smem(TcParams *o) {
         return (int)at;
     };
     const int oH = take((size_t)kTM * 256 * 2), oW = take((size_t)kSlots * kSlotBytes),
-              oB = take((size_t)(768 + 64) * 4), oBar = take(8 * kBars + 8);
+              oX = take((size_t)kTM * IN * 4), oB = take((size_t)(768 + 64) * 4), oBar = take(8 * kBars + 8);
     if (o) {
-        o->oH = oH; o->oW = oW; o->oB = oB; o->oBar = oBar;
+        o->oH = oH; o->oW = oW; o->oX = oX; o->oB = oB; o->oBar = oBar;
     }
     return off;
 }
@@ -450,7 +491,7 @@ int n4p_of(const LcNet *n) { return (n->OUT + 15) / 16 * 16; }
 // one unit (nsigma <= 32 at 3*nsigma + 3 inputs and 2*nsigma outputs), the
 // shared memory fits one SM
 bool lc_tc_supported(const LcNet *n) {
-    return k1p_of(n) <= 256 && n4p_of(n) <= kUnitN && tc_smem(nullptr) <= 232448;
+    return k1p_of(n) <= 256 && n4p_of(n) <= kUnitN && tc_smem(n->IN, nullptr) <= 232448;
 }
 
 // BF16 copies of the weights as the kernel's units (after every parameter
@@ -517,7 +558,7 @@ int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStr
     p.b3 = n->params + n->off[2] + (long long)256 * 256;
     p.b4 = n->params + n->off[3] + (long long)n->OUT * 256;
     p.err = n->tc_err;
-    const size_t smem = tc_smem(&p);
+    const size_t smem = tc_smem(p.IN, &p);
     static size_t raised = 0;
     if (smem > raised) {
         if (cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -533,6 +574,6 @@ int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStr
     return cudaGetLastError() == cudaSuccess ? 0 : FESOMC_ECUDA_LC;
 }
 
-size_t lc_tc_smem_bytes(const LcNet *) { return tc_smem(nullptr); }
+size_t lc_tc_smem_bytes(const LcNet *n) { return tc_smem(n->IN, nullptr); }
 
 }  // namespace fesomc
