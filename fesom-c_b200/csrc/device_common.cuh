@@ -79,7 +79,7 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // and where d3_end keeps its column arrays (1 local memory, 2 shared
 // memory).  A value of 0 selects the built-in default.
 enum TuneKnob : int {
-    TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
+    TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_P1EDGE, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
     TK_SSHNODE, TK_ADV2D, TK_U2D, TK_ROT, TK_ZEROFILT, TK_AB2, TK_MEGRAD, TK_MNGRAD, TK_MEDGE, TK_MH,
     TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, kTuneKnobs
 };

@@ -151,24 +151,26 @@ __global__ void k_el2nodes(Dev d, const real *Ue, const real *Ve, real *Un, real
 }
 
 // momentum_adv_P1_3D_to_2D (fv_advection.F90:676-793): the edge part
-// uu*un, vv*un of internal edge ed at level z.  Each of the edge's two
-// elements forms it in p1_elem from the nodes' velocities (the same
-// expressions give the same bits twice), instead of a per-(edge, level)
-// array written once and read by both elements (2.2x its bytes in DRAM
-// traffic: the second element's read missed L2).
-__device__ __forceinline__ real2 p1_edge_flux(const Dev &d, int ed, int z) {
+// uu*un, vv*un of every (internal edge, level), thread per (edge, level).
+// Stored in the adv3 buffer, which velrhs has finished with.
+__global__ void k_p1_edge(Dev d) {
+    const long long total = (long long)d.Ed_in * d.L;
     const int L = d.L;
-    const int2 nn = d.edge_nodes[ed];
-    const int2 et = d.edge_tri[ed];
-    const real2 dxy = d.edge_dxdy[ed];
-    const real xe = dxy.x * kREarth * real(0.5) * (d.elem_cos[et.x] + d.elem_cos[et.y]);
-    const real ye = dxy.y * kREarth;
-    const real a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
-    const real uu = real(0.5) * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
-    const real vv = real(0.5) * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
-    const real jd = real(0.5) * (jc_of(d, a1, z) + jc_of(d, a2, z));
-    const real un = (uu * ye - vv * xe) * jd;
-    return make_real2(uu * un, vv * un);
+    GRID_LOOP(ii, total) {
+        const int ed = (int)(ii / L);
+        const int z = (int)(ii % L);
+        const int2 nn = d.edge_nodes[ed];
+        const int2 et = d.edge_tri[ed];
+        const real2 dxy = d.edge_dxdy[ed];
+        const real xe = dxy.x * kREarth * real(0.5) * (d.elem_cos[et.x] + d.elem_cos[et.y]);
+        const real ye = dxy.y * kREarth;
+        const real a1 = jac_a(d, d.eta_jac, nn.x), a2 = jac_a(d, d.eta_jac, nn.y);
+        const real uu = real(0.5) * (d.Unode_p[(size_t)nn.x * L + z] + d.Unode_p[(size_t)nn.y * L + z]);
+        const real vv = real(0.5) * (d.Vnode_p[(size_t)nn.x * L + z] + d.Vnode_p[(size_t)nn.y * L + z]);
+        const real jd = real(0.5) * (jc_of(d, a1, z) + jc_of(d, a2, z));
+        const real un = (uu * ye - vv * xe) * jd;
+        d.adv3[ii] = make_real2(uu * un, vv * un);
+    }
 }
 
 // Element part of momentum_adv_P1_3D_to_2D, optional
@@ -217,7 +219,7 @@ __global__ void k_p1_elem(Dev d) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
                 if (codes[c] >= 0) {
-                    const real2 pq = p1_edge_flux(d, codes[c] >> 1, z);
+                    const real2 pq = d.adv3[(size_t)(codes[c] >> 1) * L + z];
                     T[(c * 2 + 0) * L + z] = pq.x * je;
                     T[(c * 2 + 1) * L + z] = pq.y * je;
                 }
@@ -628,6 +630,10 @@ int config_p1(const Dev &d) {
     return raise_smem_limit(k_p1_elem, p1_smem(d)) == cudaSuccess
                ? 0 : 1;
 }
+void launch_p1_edge(const Dev &d, cudaStream_t s) {
+    const int b = tuned(d, TK_P1EDGE, 256);
+    k_p1_edge<<<grid_for((long long)d.Ed_in * d.L, b), b, 0, s>>>(d);
+}
 void launch_p1_elem(const Dev &d, cudaStream_t s) {
     const int B = p1_elems(d);
     const long long blocks = ((long long)d.E + B - 1) / B;
@@ -671,6 +677,7 @@ void tune_limits_barotropic(int *lim) {
     tune_lower(lim, TK_SSHNODE, (const void *)k_ssh_node);
     tune_lower(lim, TK_PULS, (const void *)k_puls_elem);
     tune_lower(lim, TK_EL2NODES, (const void *)k_el2nodes);
+    tune_lower(lim, TK_P1EDGE, (const void *)k_p1_edge);
     tune_lower(lim, TK_ADV2D, (const void *)k_adv2d_edge);
     tune_lower(lim, TK_U2D, (const void *)k_u2d_elem);
     tune_lower(lim, TK_ROT, (const void *)k_rot_nodes);

@@ -23,6 +23,7 @@ namespace fesomc {
     void launch_ssh_node(const Dev &, int, cudaStream_t); \
     void launch_puls_elem(const Dev &, cudaStream_t); \
     void launch_el2nodes(const Dev &, const real *, const real *, real *, real *, cudaStream_t); \
+    void launch_p1_edge(const Dev &, cudaStream_t); \
     void launch_p1_elem(const Dev &, cudaStream_t); \
     void launch_adv2d_edge(const Dev &, cudaStream_t); \
     void launch_u2d_elem(const Dev &, cudaStream_t); \
@@ -870,10 +871,9 @@ double kernel_bytes_fp64(const fesomc_model *m, const std::string &k) {
     if (k == "implvisc") return L * E * 16 + NS * E * 8 + E * (16 + 16 + 16) + L * E * 16 + L * E * 16;
     if (k == "zero_filt") return E * 16 + E * 8 + E * 16 + E * 32;
     if (k == "puls_elem") return L * E * 16 + E * 16 + N * 24 + E * 48 + L * E * 16 + E * 8;
-    // p1_elem: the edge fluxes from Unode_p / Vnode_p, eta_jac, depth and
-    // the edge geometry; Je, the edge codes and acc, dmean_n, the output
+    if (k == "p1_edge") return L * N * 16 + N * 16 + Ei * 32 + E * 8 + L * Ei * 16;
     if (k == "p1_elem")
-        return L * N * 16 + N * 16 + Ei * 32 + E * 8 + E * (16 + 16 + 16) + Ei * 8 + N * 8 + L * E * 8 +
+        return L * Ei * 16 + E * (16 + 16 + 16) + Ei * 8 + N * 8 + L * E * 8 +
                (d.filt_3D ? L * E * 16 + E * 24 : 0.0);
     if (k == "jac_swap") return N * 32;
     if (k == "update3d") return L * E * (16 + 8 + 32 + 24) + N * 24 + E * 48 + E * 32 + E * 16;
@@ -1045,9 +1045,10 @@ int enqueue_step(fesomc_model *m, double ff) {
         if (sub == 0) {
             rec(m, "puls_elem", [&] { K3(launch_puls_elem, s); });
             rec(m, "el2nodes_p", [&] { K3E2N(U_puls, V_puls, Unode_p, Vnode_p); });
+            rec(m, "p1_edge", [&] { K3(launch_p1_edge, s); });
             if (d.bih_3D) { rec(m, "biharmonic_2d", [&] { K3(launch_bih_puls, s); }); n += 5; }
             rec(m, "p1_elem", [&] { K3(launch_p1_elem, s); });
-            n += 3;
+            n += 4;
         }
         if (d.mom_adv_2D == 2) { rec(m, "adv2d_edge", [&] { K3(launch_adv2d_edge, s); }); n += 1; }
         if (d.filt_bi_2D) { rec(m, "filt2x_2d", [&] { K3(launch_filt2x_2d, s); }); n += 1; }
@@ -1818,7 +1819,7 @@ struct KnobInfo {
 };
 const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"velrhs", "velrhs", 256}, {"velgrad3d", "velgrad3d", 256}, {"adv3_edge", "adv3_edge", 256},
-    {"puls_elem", "puls_elem", 256}, {"el2nodes", "el2nodes,el2nodes_p", 256},
+    {"puls_elem", "puls_elem", 256}, {"el2nodes", "el2nodes,el2nodes_p", 256}, {"p1_edge", "p1_edge", 256},
     {"ab3_elem", "ab3_elem", 256}, {"velgrad2d", "ab3_elem", 256}, {"ssh_edge", "ssh_node", 256},
     {"ssh_node", "ssh_node", 256}, {"adv2d_edge", "adv2d_edge", 256}, {"u2d_elem", "u2d_elem", 128},
     {"rot_nodes", "rot_nodes", 256}, {"zero_filt", "zero_filt", 256}, {"ab2_node", "ab2_node", 256},
