@@ -31,6 +31,7 @@ constexpr int kLcHidden = 256;
 constexpr float kLcX0 = 1.0e-6f;
 // fallback rules beyond the training envelope (fesomc_closure_set_rules)
 constexpr int kLcRuleUnstable = 1;   // N^2 < 0 at an interior interface: the plain closure
+constexpr int kLcRuleBoundary = 2;   // solid or open boundary node (index_nod2D != 0): the plain closure
 
 inline int lc_in(int NS) { return 3 * NS + 3; }
 inline int lc_out(int NS) { return NS; }

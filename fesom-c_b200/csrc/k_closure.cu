@@ -73,6 +73,8 @@ __global__ void k_lc_features(Dev d, LcView c) {
         // statically unstable column (a negative N^2 input, sign kept by asinh)
         if (c.rules & kLcRuleUnstable)
             for (int k = 1; k <= c.NS - 2; ++k) in = in && !(x[c.NS + k] < 0.0f);
+        // coastline and open-boundary columns
+        if ((c.rules & kLcRuleBoundary) && d.index_nod2D[node] != 0) in = false;
         for (int j = 0; j < c.IN; ++j) {
             const float v = (x[j] - c.mu_x[j]) / c.sd_x[j];
             x[j] = v;

@@ -14,8 +14,8 @@
 //                tcgen05.mma (M = 128 columns, N = 64 neurons, K = 16) into
 //                tensor memory, a commit that frees the slot, and after the
 //                layer's last unit a commit that hands the accumulator over;
-//   warps 4..    epilogue (kEpiWarps warps, kEpiWarps/4 per TMEM lane
-//                quarter, each a share of the accumulator columns): the
+//   warps 4..    epilogue (16 warps, four per TMEM lane quarter, each 64 of
+//                the 256 accumulator columns, read 64 at a time): the
 //                tile's staged FP32 inputs to BF16 in shared memory,
 //                then per hidden layer bias + SiLU of the accumulator
 //                (tcgen05.ld) back to shared memory as the next layer's A
@@ -54,7 +54,7 @@ constexpr int kTM = 128;                  // columns per tile (MMA M)
 constexpr int kUnitN = 64;                // output neurons per weight unit (MMA N)
 constexpr int kSlots = 3;                 // weight slots in shared memory
 constexpr int kSlotBytes = kUnitN * 256 * 2;
-constexpr int kEpiWarps = 8;              // 2 per TMEM lane quarter
+constexpr int kEpiWarps = 16;             // 4 per TMEM lane quarter
 constexpr int kEpiThreads = 32 * kEpiWarps;
 constexpr int kThreads = 128 + kEpiThreads;
 constexpr int kSlab = kTM * 16;           // bytes of one 8-wide K chunk of the 128-row A operand
@@ -167,6 +167,29 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// 32 consecutive TMEM columns of this warp's 32 lanes, without the wait:
+// two of these are in flight before tmem_wait2
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+// the wait for the loads in flight; the registers pass through it, so no
+// use of them is scheduled before it
+#define R16(a, o) "+r"(a[o + 0]), "+r"(a[o + 1]), "+r"(a[o + 2]), "+r"(a[o + 3]), "+r"(a[o + 4]), "+r"(a[o + 5]), \
+    "+r"(a[o + 6]), "+r"(a[o + 7]), "+r"(a[o + 8]), "+r"(a[o + 9]), "+r"(a[o + 10]), "+r"(a[o + 11]),          \
+    "+r"(a[o + 12]), "+r"(a[o + 13]), "+r"(a[o + 14]), "+r"(a[o + 15])
+__device__ __forceinline__ void tmem_wait2(uint32_t (&a)[32], uint32_t (&b)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : R16(a, 0), R16(a, 16), R16(b, 0), R16(b, 16)::"memory");
+}
+#undef R16
 
 // SiLU as z/2 (1 + tanh(z/2)) with the hardware tanh approximation (one
 // special-function operation per activation instead of an exponential and a
@@ -383,21 +406,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
                 fence_after();
                 if (l < 3) {
                     const float *bias = sb + 256 * l;
-                    for (int c0 = 32 * part; c0 < 256; c0 += 32 * nparts) {
-                        float v[32];
-                        tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                    // this warp's 64 columns: both loads in flight, one wait
+                    const int c0 = 64 * part;
+                    uint32_t ra[32], rb[32];
+                    tmem_ld32_async(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, ra);
+                    tmem_ld32_async(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + 32), rb);
+                    tmem_wait2(ra, rb);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t *rv = h == 0 ? ra : rb;
+                        const int cb = c0 + 32 * h;
 #pragma unroll
                         for (int j = 0; j < 4; ++j) {
+                            float v[8];
+#pragma unroll
+                            for (int t = 0; t < 8; ++t) v[t] = silu_fast(__uint_as_float(rv[8 * j + t]) + bias[cb + 8 * j + t]);
                             uint4 o;
-                            o.x = pack_bf16(silu_fast(v[8 * j + 0] + bias[c0 + 8 * j + 0]),
-                                            silu_fast(v[8 * j + 1] + bias[c0 + 8 * j + 1]));
-                            o.y = pack_bf16(silu_fast(v[8 * j + 2] + bias[c0 + 8 * j + 2]),
-                                            silu_fast(v[8 * j + 3] + bias[c0 + 8 * j + 3]));
-                            o.z = pack_bf16(silu_fast(v[8 * j + 4] + bias[c0 + 8 * j + 4]),
-                                            silu_fast(v[8 * j + 5] + bias[c0 + 8 * j + 5]));
-                            o.w = pack_bf16(silu_fast(v[8 * j + 6] + bias[c0 + 8 * j + 6]),
-                                            silu_fast(v[8 * j + 7] + bias[c0 + 8 * j + 7]));
-                            *reinterpret_cast<uint4 *>(sH + (size_t)(c0 / 8 + j) * kSlab + (size_t)r * 16) = o;
+                            o.x = pack_bf16(v[0], v[1]);
+                            o.y = pack_bf16(v[2], v[3]);
+                            o.z = pack_bf16(v[4], v[5]);
+                            o.w = pack_bf16(v[6], v[7]);
+                            *reinterpret_cast<uint4 *>(sH + (size_t)(cb / 8 + j) * kSlab + (size_t)r * 16) = o;
                         }
                     }
                     fence_before();

@@ -2129,7 +2129,7 @@ int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_ever
 }
 
 int fesomc_closure_set_rules(fesomc_closure *c, int32_t rules) {
-    if (!c || (rules & ~fesomc::kLcRuleUnstable)) return FESOMC_EINVAL;
+    if (!c || (rules & ~(fesomc::kLcRuleUnstable | fesomc::kLcRuleBoundary))) return FESOMC_EINVAL;
     c->net->rules = rules;
     return FESOMC_OK;
 }

@@ -42,10 +42,12 @@ class Closure:
         model.nstep += nsteps
         abi.check(rc, "fesomc_closure_harvest")
 
-    def set_rules(self, unstable=False):
+    def set_rules(self, unstable=False, boundary=False):
         """Fallback rules beyond the envelope, used from the next attach on:
-        unstable -- statically unstable columns (N^2 < 0) to the plain closure."""
-        abi.check(self.lib.fesomc_closure_set_rules(self.h, 1 if unstable else 0), "fesomc_closure_set_rules")
+        unstable -- statically unstable columns (N^2 < 0) to the plain closure;
+        boundary -- columns at solid / open boundary nodes to the plain closure."""
+        rules = (1 if unstable else 0) | (2 if boundary else 0)
+        abi.check(self.lib.fesomc_closure_set_rules(self.h, rules), "fesomc_closure_set_rules")
 
     def fit(self):
         abi.check(self.lib.fesomc_closure_fit(self.h), "fesomc_closure_fit")

@@ -533,9 +533,11 @@ int  fesomc_closure_stats(fesomc_model *m, fesomc_closure_report *r);
  * training envelope, with this network from the next fesomc_closure_attach
  * on.  FESOMC_LC_RULE_UNSTABLE (1): a column with N^2 < 0 at an interior
  * interface (statically unstable, convecting) goes to the plain closure;
- * such columns are counted as out of the envelope.  Other bits:
- * FESOMC_EINVAL. */
+ * FESOMC_LC_RULE_BOUNDARY (2): a column at a solid or open boundary node
+ * (index_nod2D != 0) goes to the plain closure.  Such columns are counted
+ * as out of the envelope.  Other bits: FESOMC_EINVAL. */
 #define FESOMC_LC_RULE_UNSTABLE 1
+#define FESOMC_LC_RULE_BOUNDARY 2
 int  fesomc_closure_set_rules(fesomc_closure *c, int32_t rules);
 
 /* ---- version / introspection --------------------------------------------- */
