@@ -107,7 +107,7 @@ class ClockSampler:
                 "samples": len(sms)}
 
 
-BUILD_OPTS = {}   # storage-order options of the run (--sfc-order, --shuffle)
+BUILD_OPTS = {}   # storage-order options of the run (--mesh-order, --shuffle)
 
 
 def build_case(cfg, lib=None):
@@ -739,13 +739,14 @@ def main():
     ap.add_argument("--lc-lr", type=float, default=1e-3)
     ap.add_argument("--lc-judge", type=int, default=100)
     ap.add_argument("--lc-infer", type=int, default=0, help="time the closure inference on this many columns")
-    ap.add_argument("--sfc-order", action="store_true", help="store the mesh along a Hilbert curve on the device")
+    ap.add_argument("--mesh-order", action="store_true",
+                    help="store the mesh in its own numbering on the device (default: along a Hilbert curve)")
     ap.add_argument("--launch-shapes", default="tuned", choices=["default", "tuned", "search"],
                     help="kernel launch shapes: built-in defaults, the autotuner's (cached, searched when "
                          "absent), or a fresh search")
     ap.add_argument("--shuffle", type=int, default=None, help="number the mesh's nodes and elements at random (seed)")
     args = ap.parse_args()
-    if args.sfc_order:
+    if not args.mesh_order:
         BUILD_OPTS["sfc_order"] = 1
     if args.shuffle is not None:
         BUILD_OPTS["shuffle"] = args.shuffle

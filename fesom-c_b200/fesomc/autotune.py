@@ -11,7 +11,7 @@ than `margin`.  Any setting gives the same bits, so tuning changes speed
 only.
 
 Results are cached per mesh size (nodes, elements, edges), level count,
-precision form and tracer scheme in a JSON file: the user's cache
+precision form, tracer scheme and storage order in a JSON file: the user's cache
 (FESOMC_LAUNCH_SHAPES, default ~/.cache/fesomc/launch_shapes.json), seeded
 by the shapes measured on a B200 that ship with the package
 (launch_shapes_b200.json).
@@ -39,8 +39,8 @@ def cache_path():
 
 def cache_key(case):
     m, p = case.mesh, case.params
-    return "N%d-E%d-Ed%d-NS%d-%s-adv%d-mix%d" % (m.N, m.E, m.Ed, m.NS, "f32" if p.fp32_form else "f64",
-                                                 p.tracer_adv, p.ver_mix)
+    return "N%d-E%d-Ed%d-NS%d-%s-adv%d-mix%d-sfc%d" % (m.N, m.E, m.Ed, m.NS, "f32" if p.fp32_form else "f64",
+                                                       p.tracer_adv, p.ver_mix, p.sfc_order)
 
 
 def load_cache(path=None):

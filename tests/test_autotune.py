@@ -27,7 +27,7 @@ def test_cache_roundtrip(tmp_path, built):
     from fesomc import autotune, cases
     case = cases.estuary("small")
     key = autotune.cache_key(case)
-    assert re.fullmatch(r"N\d+-E\d+-Ed\d+-NS\d+-f(32|64)-adv\d+-mix\d+", key)
+    assert re.fullmatch(r"N\d+-E\d+-Ed\d+-NS\d+-f(32|64)-adv\d+-mix\d+-sfc\d", key)
     path = str(tmp_path / "shapes.json")
     assert key not in autotune.load_cache(path)
     autotune.save_entry(key, {"velrhs": 128, "columns": 4}, path)
@@ -44,5 +44,5 @@ def test_shipped_table_is_valid_json():
     if os.path.exists(autotune.SHIPPED):
         data = json.load(open(autotune.SHIPPED))
         for k, v in data.items():
-            assert re.fullmatch(r"N\d+-E\d+-Ed\d+-NS\d+-f(32|64)-adv\d+-mix\d+", k)
+            assert re.fullmatch(r"N\d+-E\d+-Ed\d+-NS\d+-f(32|64)-adv\d+-mix\d+-sfc\d", k)
             assert all(isinstance(x, int) and x >= 0 for x in v.values())
