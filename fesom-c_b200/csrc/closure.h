@@ -35,6 +35,8 @@ constexpr int kLcRuleBoundary = 2;   // solid or open boundary node (index_nod2D
 
 inline int lc_in(int NS) { return 3 * NS + 3; }
 inline int lc_out(int NS) { return NS; }
+// nodes per block of the harvest's ordered compaction
+constexpr int kLcHarvestBlock = 256;
 // rows of the statistics array (each max(IN, OUT) floats)
 constexpr int kLcStatRows = 8;
 
@@ -51,7 +53,7 @@ struct LcView {
     float *Y;                                 // per node: network outputs (N x OUT), normalised
     int *flag;                                // per node: 1 = network, 0 = plain closure
     int *list;                                // nodes handed to the plain closure
-    int *blk;                                 // scan scratch (per-block counts)
+    int *blk;                                 // harvest: per block of kLcHarvestBlock nodes, its wet count, then its first slot
     unsigned long long *count;                // [0] list length
     unsigned long long *acc;                  // [0] wet columns [1] out of envelope [2] dry [3] steps
     double *judge;                            // [0] sum of squared log-errors [1] count [2] max

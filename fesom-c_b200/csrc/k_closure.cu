@@ -130,19 +130,71 @@ __global__ void k_lc_apply(Dev d, LcView c) {
     }
 }
 
-// training pairs: raw inputs and log bt of wet columns, after the plain
-// closure has run on the step
-__global__ void k_lc_harvest(Dev d, LcView c) {
-    GRID_LOOP(ii, d.N) {
-        const int node = (int)ii;
-        const bool wet = d.mask_wd_node[node] != real(0.0);
-        const unsigned long long slot = warp_append(wet, c.hcount);
-        if (!wet || slot >= (unsigned long long)c.hcap) continue;
-        lc_inputs(d, node, c.hx + slot * c.IN);
-        const int NS = d.NS;
-        float *y = c.hy + slot * c.OUT;
-        for (int k = 0; k < NS; ++k) y[k] = logf((float)d.bt[(size_t)node * NS + k]);   // bt >= 1e-8
+// Training pairs: raw inputs and log bt of the wet columns, after the plain
+// closure has run on the step, appended in node order (the order of the
+// training set, hence the minibatches, does not depend on scheduling):
+// each block of kLcHarvestBlock consecutive nodes counts its wet columns,
+// one block turns the counts into first slots (an ordered scan from the
+// current count), and each block writes its columns at its slots.
+__global__ void k_lc_wetcount(Dev d, LcView c) {
+    const int node = blockIdx.x * kLcHarvestBlock + threadIdx.x;
+    const bool wet = node < d.N && d.mask_wd_node[node] != real(0.0);
+    const int n = __syncthreads_count(wet);
+    if (threadIdx.x == 0) c.blk[blockIdx.x] = n;
+}
+
+// blk[b] <- the slot of block b's first wet column (capped at hcap);
+// hcount <- hcount + all wet columns.  One block of 1024 threads.
+__global__ void k_lc_slots(int nblk, LcView c) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long base;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) base = *c.hcount;
+    __syncthreads();
+    for (int c0 = 0; c0 < nblk; c0 += 1024) {
+        const int i = c0 + (int)threadIdx.x;
+        const unsigned long long v = i < nblk ? (unsigned long long)c.blk[i] : 0ULL;
+        unsigned long long incl = v;   // inclusive scan within the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            unsigned long long t = wsum[lane], ti = t;
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long u = __shfl_up_sync(0xffffffffu, ti, o);
+                if (lane >= o) ti += u;
+            }
+            wsum[lane] = ti - t;   // exclusive over warps
+        }
+        __syncthreads();
+        const unsigned long long slot = base + wsum[w] + incl - v;
+        if (i < nblk) c.blk[i] = (int)(slot < (unsigned long long)c.hcap ? slot : (unsigned long long)c.hcap);
+        __syncthreads();
+        if (threadIdx.x == 1023) base = slot + v;   // the last thread holds the chunk's end
+        __syncthreads();
     }
+    if (threadIdx.x == 0) *c.hcount = base;
+}
+
+__global__ void k_lc_harvest(Dev d, LcView c) {
+    __shared__ int wcount[kLcHarvestBlock / 32];
+    const int node = blockIdx.x * kLcHarvestBlock + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const bool wet = node < d.N && d.mask_wd_node[node] != real(0.0);
+    const unsigned b = __ballot_sync(0xffffffffu, wet);
+    if (lane == 0) wcount[w] = __popc(b);
+    __syncthreads();
+    int before = 0;
+    for (int k = 0; k < w; ++k) before += wcount[k];
+    const long long slot = (long long)c.blk[blockIdx.x] + before + __popc(b & ((1u << lane) - 1u));
+    if (!wet || slot >= c.hcap) return;
+    lc_inputs(d, node, c.hx + slot * c.IN);
+    const int NS = d.NS;
+    float *y = c.hy + slot * c.OUT;
+    for (int k = 0; k < NS; ++k) y[k] = logf((float)d.bt[(size_t)node * NS + k]);   // bt >= 1e-8
 }
 
 // judge: the plain closure ran on every column; compare the network's
@@ -183,8 +235,12 @@ void launch_lc_features(const Dev &d, const LcView &c, cudaStream_t s) {
 void launch_lc_apply(const Dev &d, const LcView &c, cudaStream_t s) {
     k_lc_apply<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
 }
+int lc_harvest_blocks(int N) { return (N + kLcHarvestBlock - 1) / kLcHarvestBlock; }
 void launch_lc_harvest(const Dev &d, const LcView &c, cudaStream_t s) {
-    k_lc_harvest<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);
+    const int nblk = lc_harvest_blocks(d.N);
+    k_lc_wetcount<<<nblk, kLcHarvestBlock, 0, s>>>(d, c);
+    k_lc_slots<<<1, 1024, 0, s>>>(nblk, c);
+    k_lc_harvest<<<nblk, kLcHarvestBlock, 0, s>>>(d, c);
 }
 void launch_lc_judge(const Dev &d, const LcView &c, cudaStream_t s) {
     k_lc_judge<<<grid_for(d.N, 128), 128, 0, s>>>(d, c);

@@ -1024,7 +1024,7 @@ int enqueue_step(fesomc_model *m, double ff) {
         n += 3;
     } else if (d.ver_mix == 3) {
         rec(m, "d3end", [&] { K3(launch_d3end, s); });
-        if (m->lc_harvest_now) { rec(m, "lc_harvest", [&] { K3(launch_lc_harvest, m->lcv, s); }); n += 1; }
+        if (m->lc_harvest_now) { rec(m, "lc_harvest", [&] { K3(launch_lc_harvest, m->lcv, s); }); n += 3; }
         rec(m, "av", [&] { K3(launch_av, s); });
         n += 2;
     }
@@ -1916,7 +1916,7 @@ int lc_model_buffers(fesomc_model *m, fesomc_closure *c) {
     int rc;
     if ((rc = dalloc(m, &v.X, N * n->IN)) || (rc = dalloc(m, &v.Y, N * n->OUT)) || (rc = dalloc(m, &v.flag, N)) ||
         (rc = dalloc(m, &v.list, N)) || (rc = dalloc(m, &v.count, 1)) || (rc = dalloc(m, &v.acc, 4)) ||
-        (rc = dalloc(m, &v.judge, 3)))
+        (rc = dalloc(m, &v.judge, 3)) || (rc = dalloc(m, &v.blk, (N + kLcHarvestBlock - 1) / kLcHarvestBlock)))
         return rc;
     m->lc_bufA = m->lc_bufB = nullptr;   // FP32 inference activations: made when first needed
     m->lc_owner = c;
