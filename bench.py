@@ -622,6 +622,7 @@ def run_closure(args):
         return g
 
     c = closure.Closure(m.NS, capacity=args.lc_capacity)
+    rules = [r for r in args.lc_rules.split(",") if r]
     t0 = time.perf_counter()
     draws = []
     for k in range(args.lc_draws):
@@ -644,6 +645,7 @@ def run_closure(args):
     for name, fp32, lc in (("plain_fp64", False, False), ("fp32_plain", True, False), ("fp32_learned", True, True)):
         g = new_model(fp32, cfg4)
         if lc:
+            c.set_rules(unstable="unstable" in rules, boundary="boundary" in rules)
             c.attach(g, judge_every=args.lc_judge, bf16=True)
         ms = C.c_double()
         rc = lib.fesomc_gpu_time_run(g.h, steps, C.byref(ms))
@@ -670,6 +672,7 @@ def run_closure(args):
            "forcing": "cfg4: uniform cross-shore stress 0.15 N/m2, non-solar surface heat flux -100 W/m2, tide and ramped river on the GPU",
            "training": {"draws": draws, "columns": c.harvested(), "harvest_s": harvest_s, "epochs": args.lc_epochs,
                         "train_s": train_s, "loss_per_epoch": [float(x) for x in losses], "parameters": c.nparams},
+           "fallback_rules": rules or ["envelope only"],
            "steps": steps, "simulated_s": steps * case.params.dt, "mld_mean_plain_m": float(np.mean(mld_ref[wet]))}
     for name, r in runs.items():
         e = {"rc": r["rc"], "ms_per_step": r["ms_per_step"], "s_per_tidal_day": r["ms_per_step"] * day / 1000.0}
@@ -738,6 +741,8 @@ def main():
     ap.add_argument("--lc-epochs", type=int, default=4)
     ap.add_argument("--lc-lr", type=float, default=1e-3)
     ap.add_argument("--lc-judge", type=int, default=100)
+    ap.add_argument("--lc-rules", default="unstable,boundary",
+                    help="closure fallback rules beyond the envelope: comma-separated of unstable, boundary")
     ap.add_argument("--lc-infer", type=int, default=0, help="time the closure inference on this many columns")
     ap.add_argument("--mesh-order", action="store_true",
                     help="store the mesh in its own numbering on the device (default: along a Hilbert curve)")

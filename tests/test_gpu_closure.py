@@ -214,3 +214,27 @@ def test_training_learns_and_beats_no_closure(mods):
             assert e_lc < e_none, (f, e_lc, e_none)
     finally:
         c.close()
+
+
+def test_fallback_rules_take_their_columns(mods):
+    """The boundary and convective-column rules hand more columns to the
+    plain closure than the envelope alone (counted as out of the envelope);
+    judging every step keeps the plain closure's state, so the three runs
+    see the same columns.  Unknown rule bits are refused."""
+    abi, cases, closure, model, pyoracle = mods
+    case, c = _harvested(mods)
+    try:
+        assert c.lib.fesomc_closure_set_rules(c.h, 8) == 1
+        counts = {}
+        for name, kw in (("none", {}), ("boundary", {"boundary": True}), ("unstable", {"unstable": True})):
+            c.set_rules(**kw)
+            _, rep = _run(mods, case, 4, c, judge=1)
+            counts[name] = rep["out_of_envelope"]
+            assert rep["wet_columns"] > 0
+        nb = int(np.count_nonzero(case.mesh.index_nod2D != 0))
+        assert counts["boundary"] > counts["none"]
+        assert counts["boundary"] - counts["none"] <= 4 * nb
+        assert counts["unstable"] >= counts["none"]
+    finally:
+        c.set_rules()
+        c.close()
