@@ -3,27 +3,32 @@
 // counterpart in the reference; the network stands in for d3_end
 // (src/fv_mixing.F90:73-347).
 //
-// One persistent CTA per SM walks 128-column tiles with specialised warps:
+// One persistent CTA per SM walks 128-column tiles, two at a time in
+// alternation (tile slots 0 and 1: the CTA's even and odd tiles), with
+// specialised warps:
 //   warp 0       producer: streams the weights, unit by unit, from global
 //                memory (L2-resident: every CTA reads the same ~330 KB) into
 //                a ring of kSlots shared-memory slots with bulk copies
 //                (cp.async.bulk, completion counted on the slot's mbarrier),
-//                and the next tile's inputs (its rows are contiguous) into an
-//                FP32 staging buffer one tile ahead;
-//   warp 1       MMA issuer (one lane): per layer and unit, K/16
-//                tcgen05.mma (M = 128 columns, N = 64 neurons, K = 16) into
-//                tensor memory, a commit that frees the slot, and after the
-//                layer's last unit a commit that hands the accumulator over;
-//   warps 4..    epilogue (16 warps, four per TMEM lane quarter, each 64 of
-//                the 256 accumulator columns, read 64 at a time): the
-//                tile's staged FP32 inputs to BF16 in shared memory,
-//                then per hidden layer bias + SiLU of the accumulator
-//                (tcgen05.ld) back to shared memory as the next layer's A
-//                operand, and the last layer's FP32 outputs to global memory.
-// The weight units are 64 output neurons x the layer's whole K (W1: 4 units,
-// W2, W3: 4 each, W4: 1 of N4p neurons), so the producer runs up to kSlots
-// units ahead of the MMAs and fetches the next tile's first layer while the
-// epilogue finishes the current tile.
+//                in the order the MMAs take them;
+//   warp 1       MMA issuer (one lane): layer by layer, alternating between
+//                the two tiles, per weight unit K/16 tcgen05.mma (M = 128
+//                columns, N = 64 neurons, K = 16) into the tile slot's 256
+//                tensor-memory columns, a commit that frees the weight slot,
+//                and after the layer's last unit a commit that hands the
+//                slot's accumulator over;
+//   warps 4-11   epilogue of tile slot 0, warps 12-19 of tile slot 1 (two
+//                warps per TMEM lane quarter, 128 of the 256 accumulator
+//                columns each, read 64 at a time): the tile's normalised
+//                FP32 inputs to BF16 in the slot's shared-memory operand
+//                buffer, then per hidden layer bias + SiLU of the
+//                accumulator (tcgen05.ld) back into that buffer as the next
+//                layer's A operand, and the last layer's FP32 outputs to
+//                global memory.
+// While one slot's epilogue works, the MMAs run the other slot's layer, so
+// the tensor pipe and the epilogue overlap instead of taking turns.  The
+// weight units are 64 output neurons x the layer's whole K (W1: 4 units,
+// W2, W3: 4 each, W4: 1 of N4p neurons).
 //
 // Operands use the no-swizzle K-major canonical layout: 8-row x 16-byte
 // core matrices, an operand of R rows stored as K/8 slabs of R x 16 bytes
@@ -52,16 +57,17 @@ namespace {
 
 constexpr int kTM = 128;                  // columns per tile (MMA M)
 constexpr int kUnitN = 64;                // output neurons per weight unit (MMA N)
-constexpr int kSlots = 3;                 // weight slots in shared memory
+constexpr int kSlots = 2;                 // weight slots in shared memory
 constexpr int kSlotBytes = kUnitN * 256 * 2;
-constexpr int kEpiWarps = 16;             // 4 per TMEM lane quarter
-constexpr int kEpiThreads = 32 * kEpiWarps;
-constexpr int kThreads = 128 + kEpiThreads;
+constexpr int kGroupWarps = 8;            // epilogue warps per tile slot: 2 per TMEM lane quarter
+constexpr int kGroupThreads = 32 * kGroupWarps;
+constexpr int kThreads = 128 + 2 * kGroupThreads;
 constexpr int kSlab = kTM * 16;           // bytes of one 8-wide K chunk of the 128-row A operand
-constexpr uint32_t kTmemCols = 256;
+constexpr int kHBytes = kTM * 256 * 2;    // one tile slot's A operand buffer
+constexpr uint32_t kTmemCols = 512;       // two accumulators of 256 columns
 constexpr int kMaxUnits = 16;
 constexpr uint32_t kSpin = 1u << 25;
-// barriers: full[kSlots], empty[kSlots], acc_full, a_ready, drain, x_full, x_empty
+// barriers: full[kSlots], empty[kSlots], acc[2], a[2], drain
 constexpr int kBars = 2 * kSlots + 5;
 
 struct TcParams {
@@ -77,10 +83,11 @@ struct TcParams {
     int unit_k[kMaxUnits];               // K of the unit (K1p or 256)
     int unit_col[kMaxUnits];             // first accumulator column of the unit
     int unit_last[kMaxUnits];            // 1: the last unit of its layer
+    int layer_start[5];                  // units of layer l: layer_start[l] .. layer_start[l+1]-1
     const float *b1, *b2, *b3, *b4;
     unsigned int *err;
     // shared-memory offsets (bytes)
-    int oH, oW, oX, oB, oBar;
+    int oH, oW, oB, oBar;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -217,14 +224,13 @@ __device__ __forceinline__ void fail_now(volatile int *fail, unsigned int *err) 
 
 __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ TcParams p) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char *sH = sm + p.oH;
     float *sb = reinterpret_cast<float *>(sm + p.oB);          // b1 b2 b3 (256 each), b4 (N4p)
     const uint32_t bar0 = smem_u32(sm + p.oBar);
     auto full_bar = [&](int s) { return bar0 + 8u * (uint32_t)s; };
     auto empty_bar = [&](int s) { return bar0 + 8u * (uint32_t)(kSlots + s); };
-    const uint32_t acc_bar = bar0 + 8u * (2 * kSlots), a_bar = acc_bar + 8u, drain_bar = acc_bar + 16u;
-    const uint32_t xfull_bar = acc_bar + 24u, xempty_bar = acc_bar + 32u;
-    const float *sX = reinterpret_cast<const float *>(sm + p.oX);
+    auto acc_bar = [&](int g) { return bar0 + 8u * (uint32_t)(2 * kSlots + g); };
+    auto a_bar = [&](int g) { return bar0 + 8u * (uint32_t)(2 * kSlots + 2 + g); };
+    const uint32_t drain_bar = bar0 + 8u * (uint32_t)(2 * kSlots + 4);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + p.oBar + 8 * kBars);
     volatile int *sfail = reinterpret_cast<volatile int *>(sm + p.oBar + 8 * kBars + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -241,11 +247,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
             mbar_init(full_bar(s), 1);
             mbar_init(empty_bar(s), 1);
         }
-        mbar_init(acc_bar, 1);
-        mbar_init(a_bar, kEpiWarps);
+        for (int g = 0; g < 2; ++g) {
+            mbar_init(acc_bar(g), 1);
+            mbar_init(a_bar(g), kGroupWarps);
+        }
         mbar_init(drain_bar, 1);
-        mbar_init(xfull_bar, 1);
-        mbar_init(xempty_bar, kEpiWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -259,130 +265,110 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
     fence_after();
     const uint32_t tbase = *tslot;
     const long long ntiles = (p.ncol + kTM - 1) / kTM;
-    const int U = p.n_units;
+    // this CTA's tiles: k = 0 .. K-1 is tile blockIdx.x + k * gridDim.x, in
+    // tile slot k % 2; the k-th pair is tiles 2k (slot 0) and 2k+1 (slot 1)
+    const long long K = ntiles > (long long)blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp == 0) {
-        // ---- producer: every unit of every tile of this CTA, in order ----
+        // ---- producer: the units in the order the MMAs take them ----
         if (lane == 0) {
-            long long g = 0;   // units issued
-            long long xk = 0;  // input tiles issued
+            long long gu = 0;   // units issued
             bool ok = true;
-            // the inputs of tile t: its rows are contiguous; the bulk copy
-            // takes the whole 16-byte multiple, the epilogue the rest
-            auto issue_x = [&](long long t) {
-                const long long left = p.ncol - t * kTM;
-                const int nr = left < kTM ? (int)left : kTM;
-                const uint32_t bytes = (uint32_t)((size_t)nr * p.IN * 4) & ~15u;
-                mbar_expect_tx(xfull_bar, bytes);
-                if (bytes) bulk_g2s(smem_u32(sm + p.oX), p.X + t * kTM * p.IN, bytes, xfull_bar);
-                ++xk;
-            };
-            if (blockIdx.x < ntiles) issue_x(blockIdx.x);
-            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-                const long long nxt = tile + gridDim.x;
-                if (nxt < ntiles) {
-                    // the staging buffer is free once this tile's inputs are converted
-                    if (!bar_wait(xempty_bar, (uint32_t)((xk - 1) & 1), sfail)) {
-                        fail_now(sfail, p.err);
-                        ok = false;
-                        break;
+            for (long long pr = 0; 2 * pr < K && ok; ++pr)
+                for (int l = 0; l < 4 && ok; ++l)
+                    for (int g = 0; g < 2 && ok; ++g) {
+                        if (2 * pr + g >= K) continue;
+                        for (int u = p.layer_start[l]; u < p.layer_start[l + 1]; ++u) {
+                            const int s = (int)(gu % kSlots);
+                            const long long n = gu / kSlots;
+                            if (n >= 1 && !bar_wait(empty_bar(s), (uint32_t)((n - 1) & 1), sfail)) {
+                                fail_now(sfail, p.err);
+                                ok = false;
+                                break;
+                            }
+                            mbar_expect_tx(full_bar(s), (uint32_t)p.unit_bytes[u]);
+                            bulk_g2s(smem_u32(sm + p.oW + s * kSlotBytes), p.W + p.unit_off[u],
+                                     (uint32_t)p.unit_bytes[u], full_bar(s));
+                            ++gu;
+                        }
                     }
-                    issue_x(nxt);
-                }
-                for (int u = 0; u < U; ++u) {
-                    const int s = (int)(g % kSlots);
-                    const long long n = g / kSlots;
-                    if (n >= 1 && !bar_wait(empty_bar(s), (uint32_t)((n - 1) & 1), sfail)) {
-                        fail_now(sfail, p.err);
-                        ok = false;
-                        break;
-                    }
-                    mbar_expect_tx(full_bar(s), (uint32_t)p.unit_bytes[u]);
-                    bulk_g2s(smem_u32(sm + p.oW + s * kSlotBytes), p.W + p.unit_off[u], (uint32_t)p.unit_bytes[u],
-                             full_bar(s));
-                    ++g;
-                }
-            }
             // every copy issued lands before the CTA may leave: wait for the
             // phase of each slot's last use (already complete when the MMAs
-            // consumed it) and of the last input tile
+            // consumed it)
             for (int s = 0; s < kSlots; ++s) {
-                const long long uses = g > s ? (g - 1 - s) / kSlots + 1 : 0;
+                const long long uses = gu > s ? (gu - 1 - s) / kSlots + 1 : 0;
                 if (uses > 0) bar_wait(full_bar(s), (uint32_t)((uses - 1) & 1), nullptr);
             }
-            if (xk > 0) bar_wait(xfull_bar, (uint32_t)((xk - 1) & 1), nullptr);
         }
     } else if (warp == 1) {
-        // ---- MMA issuer ----
+        // ---- MMA issuer: layer by layer, alternating between the tile slots ----
         if (lane == 0) {
-            long long g = 0, a_uses = 0;
+            long long gu = 0, a_uses[2] = {0, 0};
             bool ok = true;
-            const uint32_t aH = smem_u32(sH);
-            for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x)
-                for (int u = 0; u < U; ++u) {
-                    if (u == 0 || p.unit_last[u - 1]) {
-                        // a new layer: its A operand (inputs or activations) is in H
-                        if (!bar_wait(a_bar, (uint32_t)(a_uses & 1), sfail)) {
+            for (long long pr = 0; 2 * pr < K && ok; ++pr)
+                for (int l = 0; l < 4 && ok; ++l)
+                    for (int g = 0; g < 2 && ok; ++g) {
+                        if (2 * pr + g >= K) continue;
+                        // the slot's A operand (inputs or activations) is ready
+                        if (!bar_wait(a_bar(g), (uint32_t)(a_uses[g] & 1), sfail)) {
                             fail_now(sfail, p.err);
                             ok = false;
                             break;
                         }
-                        ++a_uses;
+                        ++a_uses[g];
+                        const uint32_t aH = smem_u32(sm + p.oH + g * kHBytes);
+                        const uint32_t dcol = tbase + (uint32_t)(256 * g);
+                        for (int u = p.layer_start[l]; u < p.layer_start[l + 1]; ++u) {
+                            const int s = (int)(gu % kSlots);
+                            if (!bar_wait(full_bar(s), (uint32_t)((gu / kSlots) & 1), sfail)) {
+                                fail_now(sfail, p.err);
+                                ok = false;
+                                break;
+                            }
+                            fence_after();
+                            const uint32_t aW = smem_u32(sm + p.oW + s * kSlotBytes);
+                            const int R = p.unit_rows[u];
+                            const uint32_t id = idesc_bf16(R);
+                            for (int ks = 0; ks < p.unit_k[u] / 16; ++ks)
+                                mma_bf16(dcol + (uint32_t)p.unit_col[u], sdesc(aH + 2 * ks * kSlab, kSlab, 128),
+                                         sdesc(aW + 2 * ks * R * 16, (uint32_t)R * 16, 128), id, ks > 0);
+                            mma_commit(empty_bar(s));
+                            ++gu;
+                        }
+                        if (ok) mma_commit(acc_bar(g));
                     }
-                    const int s = (int)(g % kSlots);
-                    if (!bar_wait(full_bar(s), (uint32_t)((g / kSlots) & 1), sfail)) {
-                        fail_now(sfail, p.err);
-                        ok = false;
-                        break;
-                    }
-                    fence_after();
-                    const uint32_t aW = smem_u32(sm + p.oW + s * kSlotBytes);
-                    const int R = p.unit_rows[u];
-                    const uint32_t id = idesc_bf16(R);
-                    for (int ks = 0; ks < p.unit_k[u] / 16; ++ks)
-                        mma_bf16(tbase + (uint32_t)p.unit_col[u], sdesc(aH + 2 * ks * kSlab, kSlab, 128),
-                                 sdesc(aW + 2 * ks * R * 16, (uint32_t)R * 16, 128), id, ks > 0);
-                    mma_commit(empty_bar(s));
-                    if (p.unit_last[u]) mma_commit(acc_bar);
-                    ++g;
-                }
             // every MMA issued completes before the tensor memory is freed
             mma_commit(drain_bar);
             bar_wait(drain_bar, 0, nullptr);
         }
     } else if (warp >= 4) {
-        // ---- epilogue ----
-        const int e = tid - 128;
+        // ---- epilogue of tile slot g ----
+        const int g = (warp - 4) / kGroupWarps;
+        const int gw = (warp - 4) % kGroupWarps;
         const int q = warp & 3;                     // TMEM lane quarter
-        const int part = (warp - 4) >> 2;           // share of the columns
-        constexpr int nparts = kEpiWarps / 4;
+        const int part = gw >> 2;                   // half of the accumulator columns
         const int r = 32 * q + lane;                // tile row of this thread
-        long long acc_uses = 0, x_uses = 0;
+        const int e = tid - 128 - g * kGroupThreads;
+        unsigned char *sH = sm + p.oH + g * kHBytes;
+        const uint32_t tcol = tbase + (uint32_t)(256 * g) + ((uint32_t)(32 * q) << 16);
+        long long acc_uses = 0;
         bool ok = true;
-        for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-            const long long row0 = tile * kTM;
+        for (long long k = g; k < K && ok; k += 2) {
+            const long long row0 = ((long long)blockIdx.x + k * gridDim.x) * kTM;
             const long long left = p.ncol - row0;
             const int nr = left < kTM ? (int)left : kTM;
-            if (!bar_wait(xfull_bar, (uint32_t)(x_uses & 1), sfail)) {
-                fail_now(sfail, p.err);
-                break;
-            }
-            ++x_uses;
-            const int staged = (int)(((uint32_t)((size_t)nr * p.IN * 4) & ~15u) / 4);   // floats in sX
             // inputs to BF16, one (8-wide K chunk, row) per item with the row
             // fastest: each item is one 16-byte store (consecutive threads,
             // consecutive rows: no bank conflicts), the K padding zero; rows
             // beyond ncol keep stale values (their outputs are not stored)
             const float *x = p.X + row0 * p.IN;
-            for (int i = e; i < (p.K1p / 8) * kTM; i += kEpiThreads) {
+            for (int i = e; i < (p.K1p / 8) * kTM; i += kGroupThreads) {
                 const int kc = i / kTM, rr = i - kc * kTM;
                 if (rr >= nr) continue;
+                const float *xr = x + (size_t)rr * p.IN + 8 * kc;
                 float v[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int k = 8 * kc + j, f = rr * p.IN + k;
-                    v[j] = k < p.IN ? (f < staged ? sX[f] : __ldg(x + f)) : 0.0f;
-                }
+                for (int j = 0; j < 8; ++j) v[j] = (8 * kc + j < p.IN) ? __ldg(xr + j) : 0.0f;
                 uint4 o;
                 o.x = pack_bf16(v[0], v[1]);
                 o.y = pack_bf16(v[2], v[3]);
@@ -392,12 +378,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
             }
             fence_proxy();
             __syncwarp();
-            if (lane == 0) {
-                mbar_arrive(xempty_bar);   // the staging buffer may take the next tile
-                mbar_arrive(a_bar);
-            }
+            if (lane == 0) mbar_arrive(a_bar(g));
             for (int l = 0; l < 4; ++l) {
-                if (!bar_wait(acc_bar, (uint32_t)(acc_uses & 1), sfail)) {
+                if (!bar_wait(acc_bar(g), (uint32_t)(acc_uses & 1), sfail)) {
                     fail_now(sfail, p.err);
                     ok = false;
                     break;
@@ -406,38 +389,41 @@ __global__ void __launch_bounds__(kThreads, 1) k_mlp_tc(const __grid_constant__ 
                 fence_after();
                 if (l < 3) {
                     const float *bias = sb + 256 * l;
-                    // this warp's 64 columns: both loads in flight, one wait
-                    const int c0 = 64 * part;
-                    uint32_t ra[32], rb[32];
-                    tmem_ld32_async(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, ra);
-                    tmem_ld32_async(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(c0 + 32), rb);
-                    tmem_wait2(ra, rb);
+                    // this warp's 128 columns, 64 at a time: both loads in flight, one wait
+#pragma unroll 1
+                    for (int c0 = 128 * part; c0 < 128 * part + 128; c0 += 64) {
+                        uint32_t ra[32], rb[32];
+                        tmem_ld32_async(tcol + (uint32_t)c0, ra);
+                        tmem_ld32_async(tcol + (uint32_t)(c0 + 32), rb);
+                        tmem_wait2(ra, rb);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const uint32_t *rv = h == 0 ? ra : rb;
-                        const int cb = c0 + 32 * h;
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t *rv = h == 0 ? ra : rb;
+                            const int cb = c0 + 32 * h;
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) {
-                            float v[8];
+                            for (int j = 0; j < 4; ++j) {
+                                float v[8];
 #pragma unroll
-                            for (int t = 0; t < 8; ++t) v[t] = silu_fast(__uint_as_float(rv[8 * j + t]) + bias[cb + 8 * j + t]);
-                            uint4 o;
-                            o.x = pack_bf16(v[0], v[1]);
-                            o.y = pack_bf16(v[2], v[3]);
-                            o.z = pack_bf16(v[4], v[5]);
-                            o.w = pack_bf16(v[6], v[7]);
-                            *reinterpret_cast<uint4 *>(sH + (size_t)(cb / 8 + j) * kSlab + (size_t)r * 16) = o;
+                                for (int t = 0; t < 8; ++t)
+                                    v[t] = silu_fast(__uint_as_float(rv[8 * j + t]) + bias[cb + 8 * j + t]);
+                                uint4 o;
+                                o.x = pack_bf16(v[0], v[1]);
+                                o.y = pack_bf16(v[2], v[3]);
+                                o.z = pack_bf16(v[4], v[5]);
+                                o.w = pack_bf16(v[6], v[7]);
+                                *reinterpret_cast<uint4 *>(sH + (size_t)(cb / 8 + j) * kSlab + (size_t)r * 16) = o;
+                            }
                         }
                     }
                     fence_before();
                     fence_proxy();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(a_bar);
+                    if (lane == 0) mbar_arrive(a_bar(g));
                 } else {
                     const long long row = row0 + r;
-                    for (int c0 = 32 * part; c0 < p.N4p; c0 += 32 * nparts) {
+                    for (int c0 = 32 * part; c0 < p.N4p; c0 += 64) {
                         float v[32];
-                        tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
+                        tmem_ld32(tcol + (uint32_t)c0, v);
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
                             if (row < p.ncol && c0 + j < p.OUT) p.Y[row * p.OUT + c0 + j] = v[j] + sb[768 + c0 + j];
@@ -503,10 +489,11 @@ size_t tc_smem(int IN, TcParams *o) {
         off += (bytes + 1023) / 1024 * 1024;
         return (int)at;
     };
-    const int oH = take((size_t)kTM * 256 * 2), oW = take((size_t)kSlots * kSlotBytes),
-              oX = take((size_t)kTM * IN * 4), oB = take((size_t)(768 + 64) * 4), oBar = take(8 * kBars + 8);
+    (void)IN;
+    const int oH = take((size_t)2 * kHBytes), oW = take((size_t)kSlots * kSlotBytes),
+              oB = take((size_t)(768 + 64) * 4), oBar = take(8 * kBars + 8);
     if (o) {
-        o->oH = oH; o->oW = oW; o->oX = oX; o->oB = oB; o->oBar = oBar;
+        o->oH = oH; o->oW = oW; o->oB = oB; o->oBar = oBar;
     }
     return off;
 }
@@ -581,6 +568,11 @@ int lc_forward_tc(const LcNet *n, const float *X, long long B, float *Y, cudaStr
         p.unit_k[i] = up.k[i];
         p.unit_col[i] = up.col[i];
         p.unit_last[i] = up.last[i];
+    }
+    for (int l = 0, i = 0; l < 4; ++l) {
+        p.layer_start[l] = i;
+        while (i < up.n && up.layer[i] == l) ++i;
+        p.layer_start[l + 1] = i;
     }
     p.b1 = n->params + n->off[0] + (long long)256 * n->IN;
     p.b2 = n->params + n->off[1] + (long long)256 * 256;
