@@ -370,6 +370,216 @@ __global__ void __launch_bounds__(kD3Block, 6) k_d3end_sm(Dev d, const int *list
 #undef D3
 }
 
+// ---- d3_end in two kernels (launch-shape knob "d3end_arrays" = 3) ----------
+// The set-up of a column (its per-interface constants, which take most of the
+// FP64 work: two densityJM per interface and the divisions of b1, b2, c2,
+// Ri) does not depend on the sweep, and its interfaces are independent.  The
+// set-up kernel takes blocks of kD3Tile consecutive nodes, stages their
+// columns in shared memory with coalesced loads, forms the constants with
+// one thread per (node, interface) exactly as k_d3end's first loop does, and
+// writes -b1-b2, t_inv*bt, c2 and snu level-major ([interface][node]: a warp
+// of 32 consecutive nodes reads 256 contiguous bytes of one interface) and
+// Ri in the column layout.  The sweep kernel then keeps only xx1, yy1 and
+// the btr pair in local memory (4 arrays instead of 8: the working set of
+// the resident columns fits in L2) and reads the constants level-major.
+constexpr int kD3Tile = 32;
+constexpr int kD3SetupThreads = 256;
+
+__global__ void __launch_bounds__(kD3SetupThreads) k_d3end_setup(Dev d) {
+    extern __shared__ unsigned char d3s_smem[];
+    const int NS = d.NS, L = d.L, N = d.N;
+    real *sm = reinterpret_cast<real *>(d3s_smem);
+    // per node j of the tile, stride NS: U, V, T, S (L levels), bt, snu, Kv, Ri (NS)
+    real *sU = sm, *sV = sm + 1 * kD3Tile * NS, *sT = sm + 2 * kD3Tile * NS, *sS = sm + 3 * kD3Tile * NS;
+    real *sB = sm + 4 * kD3Tile * NS, *sN = sm + 5 * kD3Tile * NS, *sK = sm + 6 * kD3Tile * NS;
+    real *sR = sm + 7 * kD3Tile * NS;
+    real *sDm = sm + 8 * kD3Tile * NS, *sAj = sDm + kD3Tile;
+    const real t_inv = real(1.0) / d.dt;
+    for (long long n0 = (long long)blockIdx.x * kD3Tile; n0 < N; n0 += (long long)gridDim.x * kD3Tile) {
+        const int nt = (int)(N - n0 < kD3Tile ? N - n0 : kD3Tile);
+        for (int i = threadIdx.x; i < nt * L; i += blockDim.x) {
+            const int j = i / L, k = i - j * L;
+            const size_t g = (size_t)n0 * L + i;
+            sU[j * NS + k] = d.Unode[g];
+            sV[j * NS + k] = d.Vnode[g];
+            sT[j * NS + k] = d.TF[g];
+            sS[j * NS + k] = d.SF[g];
+        }
+        for (int i = threadIdx.x; i < nt * NS; i += blockDim.x) {
+            const size_t g = (size_t)n0 * NS + i;
+            sB[i] = d.bt[g];
+            sN[i] = d.snu[g];
+            sK[i] = d.Kv[g];
+        }
+        if ((int)threadIdx.x < nt) {
+            const int node = (int)n0 + threadIdx.x;
+            sDm[threadIdx.x] = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+            sAj[threadIdx.x] = jac_a(d, d.eta_jac, node);
+        }
+        __syncthreads();
+        // snu level-major, and Ri(1) = Ri(NS) = 0
+        for (int i = threadIdx.x; i < kD3Tile * NS; i += blockDim.x) {
+            const int j = i % kD3Tile, k = i / kD3Tile;   // node fastest
+            if (j < nt) d.d3_sn[(size_t)k * N + n0 + j] = sN[j * NS + k];
+        }
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+            sR[j * NS] = real(0.0);
+            sR[j * NS + NS - 1] = real(0.0);
+        }
+        // the interfaces nz = 2..NS-1, node fastest (k_d3end's first loop)
+        for (int i = threadIdx.x; i < kD3Tile * (NS - 2); i += blockDim.x) {
+            const int j = i % kD3Tile, nz = 2 + i / kD3Tile;
+            if (j >= nt) continue;
+            const real *Un = sU + j * NS, *Vn = sV + j * NS, *T = sT + j * NS, *S = sS + j * NS;
+            const real *bt = sB + j * NS, *Kv = sK + j * NS, *snc = sN + j * NS;
+            const real dmean = sDm[j], dmean2 = dmean * dmean, ajac = sAj[j];
+            const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+            const real d1 = s_m - s_0;
+            const real d2 = s_0 - s_p;
+            const real dd = real(0.5) * (d1 + d2);
+            real ap1 = Un[nz - 2] - Un[nz - 1];
+            const real ap2 = Vn[nz - 2] - Vn[nz - 1];
+            const real sn_m = snc[nz - 2], sn_0 = snc[nz - 1], sn_p = snc[nz];
+            real b1 = sn_0 * (ap1 * ap1 + ap2 * ap2) / (dd * dd);
+            b1 = b1 / dmean2;
+            const real zb = zbar_of(d, ajac, nz - 1);
+            const real rho_up = density_jm(T[nz - 2], S[nz - 2], -zb, d.density_0);
+            const real rho_dn = density_jm(T[nz - 1], S[nz - 1], -zb, d.density_0);
+            ap1 = (rho_up - rho_dn) / dd;
+            const real b2 = -real(0.5) * kG * Kv[nz - 1] * ap1 / (d.density_0 * dmean);
+            const real snu_p = real(0.5) * (sn_m + sn_0);
+            const real snu_m = real(0.5) * (sn_0 + sn_p);
+            const real cc = real(0.5) * real(0.73) * (snu_p * (bt[nz - 2] - bt[nz - 1]) / d1 - snu_m * (bt[nz - 1] - bt[nz]) / d2) / dd;
+            const size_t o = (size_t)(nz - 2) * N + n0 + j;
+            d.d3_c2[o] = cc / dmean2;
+            if (b1 > real(0.0)) sR[j * NS + nz - 1] = -kG * ap1 / (d.density_0 * dmean) / b1 * sn_0;
+            else sR[j * NS + nz - 1] = real(10000.0);
+            d.d3_pb[o] = -b1 - b2;
+            d.d3_qb[o] = t_inv * bt[nz - 1];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt * NS; i += blockDim.x) d.Ri[(size_t)n0 * NS + i] = sR[i];
+        __syncthreads();
+    }
+}
+
+// The sweeps of d3_end per node column, from the set-up's level-major
+// constants; the same arithmetic as k_d3end, in the same order.
+template <int ARR, bool kList>
+__global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *count) {
+    const real t_inv = real(1.0) / d.dt;
+    const real cka = d.cka;
+    const real B1cka2 = real(16.6) * (cka * cka);
+    const long long ncol = kList ? (long long)*count : (long long)d.N;
+    const size_t N = d.N;
+    GRID_LOOP(ii, ncol) {
+        const int node = kList ? list[ii] : (int)ii;
+        const int NS = d.NS, L = d.L;
+        const real *bt = d.bt + (size_t)node * NS;
+        const real *Un = d.Unode + (size_t)node * L;
+        const real *Vn = d.Vnode + (size_t)node * L;
+        real *tke = d.tke_dissip + (size_t)node * NS;
+        // constants of interface nz (2..NS-1) and snu(nz) (1..NS), level-major
+        auto PB = [&](int nz) { return d.d3_pb[(size_t)(nz - 2) * N + node]; };
+        auto QB = [&](int nz) { return d.d3_qb[(size_t)(nz - 2) * N + node]; };
+        auto C2 = [&](int nz) { return d.d3_c2[(size_t)(nz - 2) * N + node]; };
+        auto SN = [&](int nz) { return d.d3_sn[(size_t)(nz - 1) * N + node]; };
+        real xx1[ARR], yy1[ARR], bA[ARR], bB[ARR];
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const real dmean2 = dmean * dmean;
+        const real ajac = jac_a(d, d.eta_jac, node);
+        for (int nz = 1; nz <= NS; ++nz) bA[nz] = bt[nz - 1];
+        real y2;
+        {
+            const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const real wx = d.windx[node], wy = d.windy[node];
+            const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+            const real snu_m = real(0.5) * (SN(NS) + SN(NS - 1));
+            y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
+        }
+        xx1[2] = real(1.0);
+        yy1[2] = y2;
+        const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const real lg = fesomc_log(delta_b / d.z0b_min);
+        const real bott_R = B1cka2 / (lg * lg);
+        const real ubt = Un[L - 1], vbt = Vn[L - 1];
+        const real bot = bott_R * (ubt * ubt + vbt * vbt);
+        real *btr = bA, *btr1 = bB;
+        bool converged = false;
+        int iters = 200;
+        for (int it = 1; it <= 200; ++it) {
+            real x = real(1.0), y = y2;
+            real s_lo = SN(1), s_mid = SN(2);
+            real b_n = btr[2], pb_n = PB(2), qb_n = QB(2), c2_n = C2(2), sh_n = SN(3);
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const real s_hi = sh_n;
+                const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n;
+                if (nz + 1 <= NS - 1) {
+                    b_n = btr[nz + 1]; pb_n = PB(nz + 1); qb_n = QB(nz + 1); c2_n = C2(nz + 1); sh_n = SN(nz + 2);
+                }
+                const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const real dd1 = s_m - s_0;
+                const real dd2 = s_0 - s_p;
+                const real dd = real(0.5) * (dd1 + dd2);
+                const real c1 = real(0.046) * (b * b) / s_mid;
+                if (it == 200) tke[nz - 1] = c1;
+                const real fr = pbv - c1 - qbv - c2v;
+                const real snu_p = real(0.5) * (s_lo + s_mid);
+                const real snu_mm = real(0.5) * (s_mid + s_hi);
+                const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+                const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
+                const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
+                const real a = bm - am * x;
+                const real xn = cm / a;
+                const real yn = (am * y - fr) / a;
+                xx1[nz + 1] = xn;
+                yy1[nz + 1] = yn;
+                x = xn;
+                y = yn;
+                s_lo = s_mid;
+                s_mid = s_hi;
+            }
+            real b1v = bot;  // btr1(NS)
+            btr1[NS] = b1v;
+            bool above = d3_above_tol(btr[NS] - b1v, dmax(b1v, btr[NS]) + real(1.0e-8));
+            real x_n = xx1[NS], y_n = yy1[NS], o_n = btr[NS - 1];
+            for (int nz = NS; nz >= 2; --nz) {
+                const real xv = x_n, yv = y_n, ov = o_n;
+                if (nz - 1 >= 2) { x_n = xx1[nz - 1]; y_n = yy1[nz - 1]; o_n = btr[nz - 2]; }
+                b1v = b1v * xv + yv;  // btr1(nz-1)
+                btr1[nz - 1] = b1v;
+                above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
+            }
+            if (!above) { converged = true; iters = it; break; }
+            real *t = btr;
+            btr = btr1;
+            btr1 = t;
+        }
+        if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
+        if (converged) {
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (btr[nz] * btr[nz]) / SN(nz);
+        } else {
+            atomicAdd(d.notconv, 1);
+        }
+        real *btw = d.bt + (size_t)node * NS;
+        real *snw = d.snu + (size_t)node * NS;
+        real *Kvw = d.Kv + (size_t)node * NS;
+        for (int nz = 1; nz <= NS; ++nz) {
+            const real btn = dmax(btr[nz], real(1.0e-8));
+            btw[nz - 1] = btn;
+            const real zt = __ldg(d.sig + nz - 1) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = cka * Zh * Zd * Z0 / dmean;
+            real s = scale_t * sqrt(btn) + d.snul;
+            if (s >= real(0.2)) s = real(0.2);
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+}
+
 // Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
 __global__ void k_av(Dev d) {
     const long long total = (long long)d.E * d.NS;
@@ -385,13 +595,26 @@ __global__ void k_av(Dev d) {
 }
 
 static size_t d3end_smem(const Dev &d) { return (size_t)d3end_values(d.NS) * kD3Block * sizeof(real); }
+static size_t d3end_setup_smem(const Dev &d) { return ((size_t)8 * kD3Tile * d.NS + 2 * kD3Tile) * sizeof(real); }
+// the two-kernel form: up to 40 levels (its sweep's local arrays are sized
+// like k_d3end's)
+static bool d3end_split(const Dev &d) { return d.tune[TK_D3END] == 3 && d.NS <= 40; }
 int config_d3end(const Dev &d) {
     if (d.NS > 127) return 1;
+    if (d.NS <= 40 && raise_smem_limit(k_d3end_setup, d3end_setup_smem(d)) != cudaSuccess) return 1;
     return (raise_smem_limit(k_d3end_sm<false>, d3end_smem(d)) == cudaSuccess &&
             raise_smem_limit(k_d3end_sm<true>, d3end_smem(d)) == cudaSuccess) ? 0 : 1;
 }
+static void launch_d3end_split(const Dev &d, cudaStream_t s) {
+    const int tiles = (d.N + kD3Tile - 1) / kD3Tile;
+    k_d3end_setup<<<tiles < 148 * 16 ? tiles : 148 * 16, kD3SetupThreads, d3end_setup_smem(d), s>>>(d);
+    if (d.NS <= 11) k_d3end_sweep<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else if (d.NS <= 21) k_d3end_sweep<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    else k_d3end_sweep<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+}
 void launch_d3end(const Dev &d, cudaStream_t s) {
-    if (d.tune[TK_D3END] == 2) k_d3end_sm<false><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, nullptr, nullptr);
+    if (d3end_split(d)) launch_d3end_split(d, s);
+    else if (d.tune[TK_D3END] == 2) k_d3end_sm<false><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, nullptr, nullptr);
     else if (d.NS <= 11) k_d3end<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 21) k_d3end<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 40) k_d3end<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
@@ -399,6 +622,8 @@ void launch_d3end(const Dev &d, cudaStream_t s) {
 }
 // the plain closure on the listed columns (count read on the device, so the
 // launch covers every node and the grid-stride loop stops at the count)
+// (the two-kernel form sets up every column, so the listed columns take the
+// one-kernel forms, which leave the others' Ri alone)
 void launch_d3end_list(const Dev &d, const int *list, const unsigned long long *count, cudaStream_t s) {
     if (d.tune[TK_D3END] == 2) k_d3end_sm<true><<<grid_for(d.N, kD3Block), kD3Block, d3end_smem(d), s>>>(d, list, count);
     else if (d.NS <= 11) k_d3end<12, true><<<grid_for(d.N, 64), 64, 0, s>>>(d, list, count);

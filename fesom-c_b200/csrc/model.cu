@@ -734,6 +734,10 @@ int alloc_3d(fesomc_model *m, D &d) {
     }
     decltype(&d.U_n) nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
     for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
+    if (m->p.ver_mix == 3) {
+        decltype(&d.U_n) d3s[] = {&d.d3_pb, &d.d3_qb, &d.d3_c2, &d.d3_sn};
+        for (auto p : d3s) if ((rc = dalloc(m, p, NS * N))) return rc;
+    }
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
     const size_t nm = (size_t)m->n_members;
     if ((rc = dalloc(m, &d.mm_part, (size_t)4 * nm * fesomc::f64::minmax_parts((int)nm)))) return rc;
@@ -1855,7 +1859,7 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     fesomc::f32::tune_limits_baroclinic(lim); fesomc::f32::tune_limits_barotropic(lim);
     fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
-    lim[fesomc::TK_D3END] = 2;
+    lim[fesomc::TK_D3END] = 3;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         if (values) {
             const int v = m->d.tune[k];
