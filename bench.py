@@ -270,6 +270,13 @@ def run_ours(args, ws, rank, local):
             shapes, tune_rep = autotune.shapes_for(case, refresh=args.launch_shapes == "search")
         except Exception as ex:        # timing stays valid with the default shapes
             shapes, tune_rep = None, {"error": repr(ex)}
+    if args.shape:
+        # explicit knob values on top of the chosen shapes
+        from fesomc import autotune
+        shapes = dict(shapes or {})
+        for kv in args.shape:
+            k, v = kv.split("=")
+            shapes[k] = int(v)
     g = model.GpuModel(case)
     if shapes:
         autotune.apply(g, shapes)
@@ -750,6 +757,8 @@ def main():
                     help="kernel launch shapes: built-in defaults, the autotuner's (cached, searched when "
                          "absent), or a fresh search")
     ap.add_argument("--shuffle", type=int, default=None, help="number the mesh's nodes and elements at random (seed)")
+    ap.add_argument("--shape", action="append", default=[],
+                    help="a launch-shape knob set explicitly, NAME=VALUE (repeatable), e.g. d3end_arrays=3")
     args = ap.parse_args()
     if not args.mesh_order:
         BUILD_OPTS["sfc_order"] = 1
