@@ -580,6 +580,136 @@ __global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *
     }
 }
 
+// The sweeps with xx1, yy1 and the btr pair in shared memory, [array][level]
+// [thread] (launch-shape knob "d3end_arrays" = 4): no local memory at all,
+// 4*NS - 2 values per column, blocks of kD3Block columns.
+__global__ void __launch_bounds__(kD3Block) k_d3end_sweep_sm(Dev d) {
+    extern __shared__ unsigned char d3w_smem[];
+    constexpr int B = kD3Block;
+    const real t_inv = real(1.0) / d.dt;
+    const real cka = d.cka;
+    const real B1cka2 = real(16.6) * (cka * cka);
+    const size_t N = d.N;
+    const int NS = d.NS, L = d.L;
+    real *const base = reinterpret_cast<real *>(d3w_smem) + threadIdx.x;
+    // element nz of an array at [(nz - first) * B]
+    real *const s_x = base - 2 * B;                      // xx1, nz = 2..NS
+    real *const s_y = base + (NS - 1 - 2) * B;           // yy1, nz = 2..NS
+    real *const s_bA = base + (2 * NS - 2 - 1) * B;      // nz = 1..NS
+    real *const s_bB = base + (3 * NS - 2 - 1) * B;      // nz = 1..NS
+#define W3(a, nz) a[(size_t)(nz) * B]
+    GRID_LOOP(ii, (long long)d.N) {
+        const int node = (int)ii;
+        const real *bt = d.bt + (size_t)node * NS;
+        const real *Un = d.Unode + (size_t)node * L;
+        const real *Vn = d.Vnode + (size_t)node * L;
+        real *tke = d.tke_dissip + (size_t)node * NS;
+        // constants of interface nz (2..NS-1) and snu(nz) (1..NS), level-major
+        auto PB = [&](int nz) { return d.d3_pb[(size_t)(nz - 2) * N + node]; };
+        auto QB = [&](int nz) { return d.d3_qb[(size_t)(nz - 2) * N + node]; };
+        auto C2 = [&](int nz) { return d.d3_c2[(size_t)(nz - 2) * N + node]; };
+        auto SN = [&](int nz) { return d.d3_sn[(size_t)(nz - 1) * N + node]; };
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const real dmean2 = dmean * dmean;
+        const real ajac = jac_a(d, d.eta_jac, node);
+        for (int nz = 1; nz <= NS; ++nz) W3(s_bA, nz) = bt[nz - 1];
+        real y2;
+        {
+            const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const real wx = d.windx[node], wy = d.windy[node];
+            const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+            const real snu_m = real(0.5) * (SN(NS) + SN(NS - 1));
+            y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
+        }
+        W3(s_x, 2) = real(1.0);
+        W3(s_y, 2) = y2;
+        const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const real lg = fesomc_log(delta_b / d.z0b_min);
+        const real bott_R = B1cka2 / (lg * lg);
+        const real ubt = Un[L - 1], vbt = Vn[L - 1];
+        const real bot = bott_R * (ubt * ubt + vbt * vbt);
+        real *btr = s_bA, *btr1 = s_bB;
+        bool converged = false;
+        int iters = 200;
+        for (int it = 1; it <= 200; ++it) {
+            real x = real(1.0), y = y2;
+            real s_lo = SN(1), s_mid = SN(2);
+            real b_n = W3(btr, 2), pb_n = PB(2), qb_n = QB(2), c2_n = C2(2), sh_n = SN(3);
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const real s_hi = sh_n;
+                const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n;
+                if (nz + 1 <= NS - 1) {
+                    b_n = W3(btr, nz + 1); pb_n = PB(nz + 1); qb_n = QB(nz + 1); c2_n = C2(nz + 1); sh_n = SN(nz + 2);
+                }
+                const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const real dd1 = s_m - s_0;
+                const real dd2 = s_0 - s_p;
+                const real dd = real(0.5) * (dd1 + dd2);
+                const real c1 = real(0.046) * (b * b) / s_mid;
+                if (it == 200) tke[nz - 1] = c1;
+                const real fr = pbv - c1 - qbv - c2v;
+                const real snu_p = real(0.5) * (s_lo + s_mid);
+                const real snu_mm = real(0.5) * (s_mid + s_hi);
+                const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+                const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
+                const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
+                const real a = bm - am * x;
+                const real xn = cm / a;
+                const real yn = (am * y - fr) / a;
+                W3(s_x, nz + 1) = xn;
+                W3(s_y, nz + 1) = yn;
+                x = xn;
+                y = yn;
+                s_lo = s_mid;
+                s_mid = s_hi;
+            }
+            real b1v = bot;  // btr1(NS)
+            const real top = W3(btr, NS);
+            W3(btr1, NS) = b1v;
+            bool above = d3_above_tol(top - b1v, dmax(b1v, top) + real(1.0e-8));
+            real x_n = W3(s_x, NS), y_n = W3(s_y, NS), o_n = W3(btr, NS - 1);
+            for (int nz = NS; nz >= 2; --nz) {
+                const real xv = x_n, yv = y_n, ov = o_n;
+                if (nz - 1 >= 2) { x_n = W3(s_x, nz - 1); y_n = W3(s_y, nz - 1); o_n = W3(btr, nz - 2); }
+                b1v = b1v * xv + yv;  // btr1(nz-1)
+                W3(btr1, nz - 1) = b1v;
+                above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
+            }
+            if (!above) { converged = true; iters = it; break; }
+            real *t = btr;
+            btr = btr1;
+            btr1 = t;
+        }
+        if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
+        if (converged) {
+            for (int nz = 2; nz <= NS - 1; ++nz) {
+                const real b = W3(btr, nz);
+                tke[nz - 1] = real(0.046) * (b * b) / SN(nz);
+            }
+        } else {
+            atomicAdd(d.notconv, 1);
+        }
+        real *btw = d.bt + (size_t)node * NS;
+        real *snw = d.snu + (size_t)node * NS;
+        real *Kvw = d.Kv + (size_t)node * NS;
+        for (int nz = 1; nz <= NS; ++nz) {
+            const real btn = dmax(W3(btr, nz), real(1.0e-8));
+            btw[nz - 1] = btn;
+            const real zt = __ldg(d.sig + nz - 1) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = cka * Zh * Zd * Z0 / dmean;
+            real s = scale_t * sqrt(btn) + d.snul;
+            if (s >= real(0.2)) s = real(0.2);
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+#undef W3
+}
+
+
 // Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
 __global__ void k_av(Dev d) {
     const long long total = (long long)d.E * d.NS;
@@ -598,17 +728,21 @@ static size_t d3end_smem(const Dev &d) { return (size_t)d3end_values(d.NS) * kD3
 static size_t d3end_setup_smem(const Dev &d) { return ((size_t)8 * kD3Tile * d.NS + 2 * kD3Tile) * sizeof(real); }
 // the two-kernel form: up to 40 levels (its sweep's local arrays are sized
 // like k_d3end's)
-static bool d3end_split(const Dev &d) { return d.tune[TK_D3END] == 3 && d.NS <= 40; }
+static bool d3end_split(const Dev &d) { return (d.tune[TK_D3END] == 3 || d.tune[TK_D3END] == 4) && d.NS <= 40; }
+static size_t d3end_sweep_smem(const Dev &d) { return (size_t)(4 * d.NS - 2) * kD3Block * sizeof(real); }
 int config_d3end(const Dev &d) {
     if (d.NS > 127) return 1;
-    if (d.NS <= 40 && raise_smem_limit(k_d3end_setup, d3end_setup_smem(d)) != cudaSuccess) return 1;
+    if (d.NS <= 40 && (raise_smem_limit(k_d3end_setup, d3end_setup_smem(d)) != cudaSuccess ||
+                       raise_smem_limit(k_d3end_sweep_sm, d3end_sweep_smem(d)) != cudaSuccess))
+        return 1;
     return (raise_smem_limit(k_d3end_sm<false>, d3end_smem(d)) == cudaSuccess &&
             raise_smem_limit(k_d3end_sm<true>, d3end_smem(d)) == cudaSuccess) ? 0 : 1;
 }
 static void launch_d3end_split(const Dev &d, cudaStream_t s) {
     const int tiles = (d.N + kD3Tile - 1) / kD3Tile;
     k_d3end_setup<<<tiles < 148 * 16 ? tiles : 148 * 16, kD3SetupThreads, d3end_setup_smem(d), s>>>(d);
-    if (d.NS <= 11) k_d3end_sweep<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
+    if (d.tune[TK_D3END] == 4) k_d3end_sweep_sm<<<grid_for(d.N, kD3Block), kD3Block, d3end_sweep_smem(d), s>>>(d);
+    else if (d.NS <= 11) k_d3end_sweep<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 21) k_d3end_sweep<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else k_d3end_sweep<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
 }

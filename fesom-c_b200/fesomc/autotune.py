@@ -28,7 +28,9 @@ from . import abi, cases, model
 
 THREADS = (64, 128, 256, 512, 1024)
 COLUMNS = (1, 2, 4, 8, 16, 32)
-D3END_ARRAYS = (1, 2, 3)   # d3_end: local-memory arrays, shared-memory arrays, set-up and sweep kernels
+# d3_end: local-memory arrays, shared-memory arrays, set-up and sweep kernels
+# (the sweep's arrays in local, or in shared memory)
+D3END_ARRAYS = (1, 2, 3, 4)
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "launch_shapes_b200.json")
 
 

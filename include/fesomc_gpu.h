@@ -402,9 +402,10 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * largest each knob accepts on this device), either may be NULL.
  * fesomc_gpu_tune_set takes one value per knob (0 = the default) and
  * returns FESOMC_EINVAL, changing nothing, when a thread count is not a
- * multiple of 32 or a value exceeds its limit ("d3end_arrays" takes 1 to 3:
+ * multiple of 32 or a value exceeds its limit ("d3end_arrays" takes 1 to 4:
  * d3_end's column arrays in local or in shared memory, or a set-up and a
- * sweep kernel); the next step captures its
+ * sweep kernel with the sweep's arrays in local or in shared memory); the
+ * next step captures its
  * graph again.  The search over the knobs and its cache per mesh size and
  * level count live with the host driver (fesomc/autotune.py).  No
  * counterpart in the reference. */
