@@ -428,10 +428,18 @@ def run_compare_forms(args):
     cfg = args.config
     chunk = args.chunk if args.chunk > 0 else args.steps
     models = []
+    shapes_used = {}
     for form in (0, 1):
         case = build_case(cfg)
         case.params.fp32_form = form
+        shapes = None
+        if args.launch_shapes != "default":
+            from fesomc import autotune
+            shapes, _ = autotune.shapes_for(case, refresh=args.launch_shapes == "search")
         g = model.GpuModel(case)
+        if shapes:
+            autotune.apply(g, shapes)
+        shapes_used["fp32" if form else "fp64"] = shapes
         t_next = cases.advance_time(g.time_jd, case.params.dt)
         g.set_forcing(case.forcing_fn(1, t_next))
         device_forcing(lib, abi, g, case)
@@ -490,6 +498,7 @@ def run_compare_forms(args):
         "plain_fp64": {"ms_per_step": ms0, "s_per_tidal_day": ms0 * steps_per_day / 1000.0},
         "chosen_fp32": {"ms_per_step": ms1, "s_per_tidal_day": ms1 * steps_per_day / 1000.0},
         "speedup": ms0 / ms1 if ms1 > 0 else None, "errors_vs_fp64": errors, "per_chunk": per_chunk,
+        "launch_shapes": shapes_used,
         "notes": "device-timed graph replay, both runs from the same initial state; stress and wind held, open-boundary "
                  "tide and ramped river runoff evaluated on the GPU each step",
     }
