@@ -78,12 +78,13 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // per block of the column kernels (pressure_col, bpg_elem, update3d, wvel),
 // and the form of d3_end (1 column arrays in local memory, 2 in shared
 // memory, 3 a level-parallel set-up kernel and a sweep kernel, 4 the same
-// with the sweep's arrays in shared memory).  A value of 0 selects the
-// built-in default.
+// with the sweep's arrays in shared memory), and the form of the tracers'
+// implicit vertical diffusion (1 one kernel, 2 a level-parallel set-up
+// kernel and a sweep kernel).  A value of 0 selects the built-in default.
 enum TuneKnob : int {
     TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_P1EDGE, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
     TK_SSHNODE, TK_ADV2D, TK_U2D, TK_ROT, TK_ZEROFILT, TK_AB2, TK_MEGRAD, TK_MNGRAD, TK_MEDGE, TK_MH,
-    TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, kTuneKnobs
+    TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, TK_VDIFF, kTuneKnobs
 };
 
 namespace f64 {

@@ -738,6 +738,8 @@ int alloc_3d(fesomc_model *m, D &d) {
         decltype(&d.U_n) d3s[] = {&d.d3_pb, &d.d3_qb, &d.d3_c2, &d.d3_sn};
         for (auto p : d3s) if ((rc = dalloc(m, p, NS * N))) return rc;
     }
+    decltype(&d.U_n) vds[] = {&d.vd_a, &d.vd_b, &d.vd_c, &d.vd_tr, &d.vd_sr, &d.vd_t, &d.vd_s};
+    for (auto p : vds) if ((rc = dalloc(m, p, L * N))) return rc;
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
     const size_t nm = (size_t)m->n_members;
     if ((rc = dalloc(m, &d.mm_part, (size_t)4 * nm * fesomc::f64::minmax_parts((int)nm)))) return rc;
@@ -1831,6 +1833,7 @@ const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"muscl_h", "muscl_h", 128}, {"upwind_h", "upwind_h", 128}, {"av", "av", 256},
     {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
     {"d3end_arrays", "d3end,d3end_list", 1},
+    {"vdiff_form", "vdiff_col", 1},
 };
 int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
 void drop_graph(fesomc_model *m);
@@ -1860,12 +1863,15 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
     lim[fesomc::TK_D3END] = 4;
+    lim[fesomc::TK_VDIFF] = 2;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         if (values) {
             const int v = m->d.tune[k];
             values[k] = v > 0 ? v : (kKnobs[k].def > 0 ? kKnobs[k].def : default_columns(m->d.L));
         }
-        if (limits) limits[k] = (k == fesomc::TK_COLUMNS || k == fesomc::TK_D3END) ? lim[k] : (lim[k] / 32) * 32;
+        if (limits)
+            limits[k] = (k == fesomc::TK_COLUMNS || k == fesomc::TK_D3END || k == fesomc::TK_VDIFF) ? lim[k]
+                                                                                                : (lim[k] / 32) * 32;
     }
     return FESOMC_OK;
 }
@@ -1878,7 +1884,8 @@ int fesomc_gpu_tune_set(fesomc_model *m, const int32_t *values) {
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         const int v = values[k];
         if (v < 0 || v > lim[k]) return FESOMC_EINVAL;
-        if (k != fesomc::TK_COLUMNS && k != fesomc::TK_D3END && v != 0 && (v < 32 || v % 32 != 0)) return FESOMC_EINVAL;
+        if (k != fesomc::TK_COLUMNS && k != fesomc::TK_D3END && k != fesomc::TK_VDIFF && v != 0 && (v < 32 || v % 32 != 0))
+            return FESOMC_EINVAL;
     }
     drop_graph(m);   // the captured step holds the old launch shapes
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) m->d.tune[k] = m->d32.tune[k] = values[k];

@@ -31,6 +31,10 @@ COLUMNS = (1, 2, 4, 8, 16, 32)
 # d3_end: local-memory arrays, shared-memory arrays, set-up and sweep kernels
 # (the sweep's arrays in local, or in shared memory)
 D3END_ARRAYS = (1, 2, 3, 4)
+# tracer_impl_vert_diff: one kernel, or set-up and sweep kernels
+VDIFF_FORMS = (1, 2)
+# the knobs that pick a form rather than a block size
+FORMS = {"columns": COLUMNS, "d3end_arrays": D3END_ARRAYS, "vdiff_form": VDIFF_FORMS}
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "launch_shapes_b200.json")
 
 
@@ -132,7 +136,7 @@ def search(case, steps=3, warmup=2, margin=0.02, log=None):
         before = profile(g, steps)
         trials = 0
         for name, recs in ks:
-            cands = COLUMNS if name == "columns" else (D3END_ARRAYS if name == "d3end_arrays" else THREADS)
+            cands = FORMS.get(name, THREADS)
             cands = [c for c in cands if c <= lim[name]]
 
             def t_of(v):

@@ -404,8 +404,10 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * returns FESOMC_EINVAL, changing nothing, when a thread count is not a
  * multiple of 32 or a value exceeds its limit ("d3end_arrays" takes 1 to 4:
  * d3_end's column arrays in local or in shared memory, or a set-up and a
- * sweep kernel with the sweep's arrays in local or in shared memory); the
- * next step captures its
+ * sweep kernel with the sweep's arrays in local or in shared memory;
+ * "vdiff_form" 1 or 2: the tracers' implicit vertical diffusion as one
+ * kernel per column, or as a set-up kernel over (node, layer) and a sweep
+ * kernel per column, for up to 64 layers); the next step captures its
  * graph again.  The search over the knobs and its cache per mesh size and
  * level count live with the host driver (fesomc/autotune.py).  No
  * counterpart in the reference. */

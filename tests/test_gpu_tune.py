@@ -42,7 +42,7 @@ def test_every_shape_gives_the_same_bits(built, fp32, adv):
         _, lim = autotune.get(g)
     finally:
         g.close()
-    small = {k: (1 if k in ("columns", "d3end_arrays") else 64) for k in lim}
+    small = {k: (1 if k in autotune.FORMS else 64) for k in lim}
     large = dict(lim)
     for shapes in (small, large):
         got = _run(_case(fp32, adv), shapes)
