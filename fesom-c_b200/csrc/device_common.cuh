@@ -78,7 +78,8 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // per block of the column kernels (pressure_col, bpg_elem, update3d, wvel),
 // and the form of d3_end (1 column arrays in local memory, 2 in shared
 // memory, 3 a level-parallel set-up kernel and a sweep kernel, 4 the same
-// with the sweep's arrays in shared memory), and the form of the tracers'
+// with the sweep's arrays in shared memory, 5 and 6 in registers for 11 or
+// 21 levels), and the form of the tracers'
 // implicit vertical diffusion (1 one kernel, 2 a level-parallel set-up
 // kernel and a sweep kernel).  A value of 0 selects the built-in default.
 enum TuneKnob : int {

@@ -710,6 +710,143 @@ __global__ void __launch_bounds__(kD3Block) k_d3end_sweep_sm(Dev d) {
 }
 
 
+// ---- the sweeps in registers (launch-shape knob "d3end_arrays" = 5, 6) -----
+// For a level count fixed at compile time (NSC) every loop over the levels
+// unrolls, so the column arrays live in registers and the sweep touches no
+// local memory.  Three arrays instead of four: the back substitution writes
+// btr1(m) into the slot of xx1(m + 1) it has just read (xx1(2) = 1 is a
+// constant), so with btr(m) = P[m] the sweep leaves btr1(m) in Q[m + 1],
+// copied back into P when the column has not converged.  yy1 keeps its own
+// array (yy1(2) = y2 a constant).  The arithmetic is k_d3end_sweep's, in
+// the same order; the constants are read level-major through the
+// read-only path.
+template <int NSC>
+__device__ __forceinline__ bool d3_sweep_reg(const Dev &d, size_t N, int node, const real (&P)[NSC + 2],
+                                             real (&Q)[NSC + 2], real (&Y)[NSC + 2], real y2, real bot, real dmean2,
+                                             real t_inv, bool last, real *tke) {
+    constexpr int PO = 0, QO = 0;
+    const real *pb = d.d3_pb + node, *qb = d.d3_qb + node, *c2 = d.d3_c2 + node, *sn = d.d3_sn + node;
+    real x = real(1.0), y = y2;
+    real s_lo = __ldg(sn), s_mid = __ldg(sn + N);
+#pragma unroll
+    for (int nz = 2; nz <= NSC - 1; ++nz) {
+        const real s_hi = __ldg(sn + (size_t)nz * N);
+        const real b = P[nz + PO];
+        const real pbv = __ldg(pb + (size_t)(nz - 2) * N), qbv = __ldg(qb + (size_t)(nz - 2) * N);
+        const real c2v = __ldg(c2 + (size_t)(nz - 2) * N);
+        const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+        const real dd1 = s_m - s_0;
+        const real dd2 = s_0 - s_p;
+        const real dd = real(0.5) * (dd1 + dd2);
+        const real c1 = real(0.046) * (b * b) / s_mid;
+        if (last) tke[nz - 1] = c1;
+        const real fr = pbv - c1 - qbv - c2v;
+        const real snu_p = real(0.5) * (s_lo + s_mid);
+        const real snu_mm = real(0.5) * (s_mid + s_hi);
+        const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+        const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
+        const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
+        const real a = bm - am * x;
+        const real xn = cm / a;
+        const real yn = (am * y - fr) / a;
+        Q[nz + 1 + QO] = xn;
+        Y[nz + 1] = yn;
+        x = xn;
+        y = yn;
+        s_lo = s_mid;
+        s_mid = s_hi;
+    }
+    real b1v = bot;  // btr1(NS)
+    bool above = d3_above_tol(P[NSC + PO] - b1v, dmax(b1v, P[NSC + PO]) + real(1.0e-8));
+    Q[NSC + 1 + QO] = b1v;
+#pragma unroll
+    for (int nz = NSC; nz >= 2; --nz) {
+        const real xv = nz == 2 ? real(1.0) : Q[nz + QO];
+        const real yv = nz == 2 ? y2 : Y[nz];
+        const real ov = P[nz - 1 + PO];
+        b1v = b1v * xv + yv;  // btr1(nz-1)
+        Q[nz + QO] = b1v;
+        above |= d3_above_tol(ov - b1v, dmax(b1v, ov) + real(1.0e-8));
+    }
+    return above;
+}
+
+// MINB resident blocks of 64 columns per SM: 6 (at most 168 registers) or
+// 8 (128 registers, a few spilled)
+template <int NSC, int MINB>
+__global__ void __launch_bounds__(64, MINB) k_d3end_sweep_reg(Dev d) {
+    const real t_inv = real(1.0) / d.dt;
+    const real cka = d.cka;
+    const real B1cka2 = real(16.6) * (cka * cka);
+    const size_t N = d.N;
+    constexpr int NS = NSC;
+    const int L = d.L;
+    GRID_LOOP(ii, (long long)d.N) {
+        const int node = (int)ii;
+        const real *bt = d.bt + (size_t)node * NS;
+        const real *Un = d.Unode + (size_t)node * L;
+        const real *Vn = d.Vnode + (size_t)node * L;
+        real *tke = d.tke_dissip + (size_t)node * NS;
+        auto SN = [&](int nz) { return __ldg(d.d3_sn + (size_t)(nz - 1) * N + node); };
+        real A[NSC + 2], B[NSC + 2], Y[NSC + 2];
+        const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
+        const real dmean2 = dmean * dmean;
+        const real ajac = jac_a(d, d.eta_jac, node);
+#pragma unroll
+        for (int nz = 1; nz <= NS; ++nz) A[nz] = bt[nz - 1];
+        real y2;
+        {
+            const real d1 = real(0.5) * (__ldg(d.sig + NS - 2) - __ldg(d.sig + NS - 1));
+            const real wx = d.windx[node], wy = d.windy[node];
+            const real u_din_sur = real(0.05) * (wx * wx + wy * wy);
+            const real snu_m = real(0.5) * (SN(NS) + SN(NS - 1));
+            y2 = (real(0.4e-3) * (u_din_sur * u_din_sur * u_din_sur) * dmean * d1) / (snu_m * real(0.76));
+        }
+        const real delta_b = jc_of(d, ajac, NS - 2) + d.z0b_min;
+        const real lg = fesomc_log(delta_b / d.z0b_min);
+        const real bott_R = B1cka2 / (lg * lg);
+        const real ubt = Un[L - 1], vbt = Vn[L - 1];
+        const real bot = bott_R * (ubt * ubt + vbt * vbt);
+        // A ends as the final btr: the previous iterate when a sweep
+        // converges, the last sweep's result after 200 without convergence
+        bool converged = false;
+        int iters = 200;
+        for (int it = 1; it <= 200; ++it) {
+            if (!d3_sweep_reg<NSC>(d, N, node, A, B, Y, y2, bot, dmean2, t_inv, it == 200, tke)) {
+                converged = true;
+                iters = it;
+                break;
+            }
+#pragma unroll
+            for (int m = 1; m <= NS; ++m) A[m] = B[m + 1];
+        }
+        if (d.d3_iters) d.d3_iters[node] = iters;   // measurement only (fesomc_gpu_d3end_iterations)
+        if (converged) {
+#pragma unroll
+            for (int nz = 2; nz <= NS - 1; ++nz) tke[nz - 1] = real(0.046) * (A[nz] * A[nz]) / SN(nz);
+        } else {
+            atomicAdd(d.notconv, 1);
+        }
+        real *btw = d.bt + (size_t)node * NS;
+        real *snw = d.snu + (size_t)node * NS;
+        real *Kvw = d.Kv + (size_t)node * NS;
+#pragma unroll
+        for (int nz = 1; nz <= NS; ++nz) {
+            const real btn = dmax(A[nz], real(1.0e-8));
+            btw[nz - 1] = btn;
+            const real zt = __ldg(d.sig + nz - 1) * dmean;
+            const real Zh = zt + d.z0b_min;
+            const real Zd = fabs(dmean - zt) + d.z0s_min;
+            const real Z0 = real(1.0) - d.beta_scale * Zh * Zd / (dmean * dmean);
+            const real scale_t = cka * Zh * Zd * Z0 / dmean;
+            real s = scale_t * sqrt(btn) + d.snul;
+            if (s >= real(0.2)) s = real(0.2);
+            snw[nz - 1] = s;
+            Kvw[nz - 1] = d.Pr_num * s;
+        }
+    }
+}
+
 // Av(nz,elem) = sum(w_cv*snu(nz,nodes)) (fv_mixing.F90:308-313)
 __global__ void k_av(Dev d) {
     const long long total = (long long)d.E * d.NS;
@@ -728,7 +865,10 @@ static size_t d3end_smem(const Dev &d) { return (size_t)d3end_values(d.NS) * kD3
 static size_t d3end_setup_smem(const Dev &d) { return ((size_t)8 * kD3Tile * d.NS + 2 * kD3Tile) * sizeof(real); }
 // the two-kernel form: up to 40 levels (its sweep's local arrays are sized
 // like k_d3end's)
-static bool d3end_split(const Dev &d) { return (d.tune[TK_D3END] == 3 || d.tune[TK_D3END] == 4) && d.NS <= 40; }
+static bool d3end_split(const Dev &d) { return d.tune[TK_D3END] >= 3 && d.NS <= 40; }
+// the register sweep is compiled for these level counts; others take the
+// local-memory sweep
+static bool d3end_reg(const Dev &d) { return d.tune[TK_D3END] >= 5 && (d.NS == 11 || d.NS == 21); }
 static size_t d3end_sweep_smem(const Dev &d) { return (size_t)(4 * d.NS - 2) * kD3Block * sizeof(real); }
 int config_d3end(const Dev &d) {
     if (d.NS > 127) return 1;
@@ -741,7 +881,14 @@ int config_d3end(const Dev &d) {
 static void launch_d3end_split(const Dev &d, cudaStream_t s) {
     const int tiles = (d.N + kD3Tile - 1) / kD3Tile;
     k_d3end_setup<<<tiles < 148 * 16 ? tiles : 148 * 16, kD3SetupThreads, d3end_setup_smem(d), s>>>(d);
-    if (d.tune[TK_D3END] == 4) k_d3end_sweep_sm<<<grid_for(d.N, kD3Block), kD3Block, d3end_sweep_smem(d), s>>>(d);
+    if (d3end_reg(d)) {
+        const bool b8 = d.tune[TK_D3END] == 6;
+        if (d.NS == 11 && b8) k_d3end_sweep_reg<11, 8><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+        else if (d.NS == 11) k_d3end_sweep_reg<11, 6><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+        else if (b8) k_d3end_sweep_reg<21, 8><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+        else k_d3end_sweep_reg<21, 6><<<grid_for(d.N, 64), 64, 0, s>>>(d);
+    }
+    else if (d.tune[TK_D3END] == 4) k_d3end_sweep_sm<<<grid_for(d.N, kD3Block), kD3Block, d3end_sweep_smem(d), s>>>(d);
     else if (d.NS <= 11) k_d3end_sweep<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 21) k_d3end_sweep<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else k_d3end_sweep<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);

@@ -29,8 +29,9 @@ from . import abi, cases, model
 THREADS = (64, 128, 256, 512, 1024)
 COLUMNS = (1, 2, 4, 8, 16, 32)
 # d3_end: local-memory arrays, shared-memory arrays, set-up and sweep kernels
-# (the sweep's arrays in local, or in shared memory)
-D3END_ARRAYS = (1, 2, 3, 4)
+# (the sweep's arrays in local memory, in shared memory, or in registers at
+# 6 or 8 resident blocks per SM)
+D3END_ARRAYS = (1, 2, 3, 4, 5, 6)
 # tracer_impl_vert_diff: one kernel, or set-up and sweep kernels
 VDIFF_FORMS = (1, 2)
 # the knobs that pick a form rather than a block size

@@ -50,10 +50,15 @@ def build_pair(mods, make):
     return make(None), make(pyoracle.MeshLib(abi))
 
 
-def run_pair(mods, make, steps):
+def run_pair(mods, make, steps, shapes=None):
+    """steps of the GPU path (launch shapes / kernel forms `shapes`, by knob
+    name) and of the oracle; returns (differing fields, the two energies)."""
     abi, cases, model, pyoracle = mods
     gcase, ocase = build_pair(mods, make)
     g = model.GpuModel(gcase)
+    if shapes:
+        from fesomc import autotune
+        autotune.apply(g, shapes)
     o = pyoracle.Oracle(ocase, abi, cases)
     g.step(steps)
     o.step(steps)
@@ -438,6 +443,37 @@ def test_key_atm_bit_exact(mods, variant):
         "jerlov_per_node": (_atm_per_node, {"jer_const": 0}),
     }[variant]
     bad, eg, eo = run_pair(mods, est(cases, "small", atm=atm, **kw), 20)
+    assert bad == []
+    assert abs(eg - eo) <= 1e-12 * abs(eo)
+
+
+def _estuary21(cases, **kw):
+    """the small estuary with 21 sigma levels (cfg1's level count)"""
+    return lambda lib: cases.estuary_case("small21", 40, 16, 300.0, 21, 2.0, 25.0, stress=(0.0, 0.05), lib=lib,
+                                          **kw)
+
+
+@pytest.mark.parametrize("variant", ["rivers_split_local", "atm_split_shared", "atm_per_node_split",
+                                     "reg6_11", "reg8_11_atm", "reg6_21", "reg8_21"])
+def test_two_kernel_forms_bit_exact(mods, variant):
+    """The set-up + sweep forms of d3_end (sweep arrays in local memory, in
+    shared memory, in registers for 11 and 21 levels) and of the tracers'
+    vertical diffusion against the oracle, with the river salinity source
+    and with atmospheric heat and freshwater sources in the column solve,
+    20 steps, exact."""
+    abi, cases, model, pyoracle = mods
+    make, shapes = {
+        "rivers_split_local": (est(cases, "small"), {"d3end_arrays": 3, "vdiff_form": 2}),
+        "atm_split_shared": (est(cases, "small", atm=_atm_varied, type_swr_body=2),
+                             {"d3end_arrays": 4, "vdiff_form": 2}),
+        "atm_per_node_split": (est(cases, "small", atm=_atm_per_node, jer_const=0),
+                               {"d3end_arrays": 3, "vdiff_form": 2}),
+        "reg6_11": (est(cases, "small"), {"d3end_arrays": 5}),
+        "reg8_11_atm": (est(cases, "small", atm=_atm_varied), {"d3end_arrays": 6, "vdiff_form": 2}),
+        "reg6_21": (_estuary21(cases), {"d3end_arrays": 5, "vdiff_form": 2}),
+        "reg8_21": (_estuary21(cases), {"d3end_arrays": 6}),
+    }[variant]
+    bad, eg, eo = run_pair(mods, make, 20, shapes)
     assert bad == []
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
