@@ -1083,165 +1083,146 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) {
     const int b = tuned(d, TK_MH, 128);
     k_muscl_h<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
 }
-// ---- tracer_impl_vert_diff in two kernels (knob vdiff_form = 2) ------------
-// The coefficients and right-hand sides of every layer (vd_coef's
-// divisions, the river salt term, the atmospheric sources) do not depend on
-// the elimination, and the layers are independent.  The set-up kernel takes
-// blocks of kVdTile consecutive nodes, stages their T, S and Kv columns in
-// shared memory with coalesced loads, forms a, b, c and the right-hand sides
-// with one thread per (node, layer) exactly as k_vdiff_col's forward loop
-// does, and writes them level-major with the tracers the update adds to;
-// it also copies Told_new / Sold_new to T_old / S_old.  The sweep kernel
-// (one thread per column) runs the elimination and the back substitution
-// on them.
-constexpr int kVdTile = 32;
-constexpr int kVdSetupThreads = 256;
-// odd row strides (in elements) keep the per-node rows of the set-up's tiles
-// free of shared-memory bank conflicts when a warp walks 32 nodes of one layer
+// ---- tracer_impl_vert_diff on tiles of columns (knob vdiff_form = 2) -------
+// k_vdiff_col reads each column with one thread, so a warp's loads of one
+// layer touch 32 rows L values apart.  Here a block takes kVtCols
+// consecutive nodes, whose columns are one contiguous range of every
+// [node][layer] field: it stages T - T_aver, the river-adjusted S - S_aver
+// and Kv in shared memory with coalesced loads (copying Told_new / Sold_new
+// to T_old / S_old on the way), solves each column with one thread from
+// shared memory (rows of odd stride: no bank conflicts) with the sweep's
+// recurrences in registers (the layer count LC is fixed at compile time),
+// writes the new tracers over the staged ones and stores them coalesced.
+// The arithmetic and its order are k_vdiff_col's.
+constexpr int kVtCols = 128;
 __host__ __device__ __forceinline__ int vd_odd(int x) { return x | 1; }
 
-template <bool kAtm>
-__global__ void __launch_bounds__(kVdSetupThreads) k_vdiff_setup(Dev d) {
-    extern __shared__ __align__(16) unsigned char vds_smem[];
-    const int L = d.L, NS = d.NS, N = d.N;
-    const int LP = vd_odd(L), KP = vd_odd(NS);
-    real *sm = reinterpret_cast<real *>(vds_smem);
-    real *sT = sm, *sS = sm + kVdTile * LP;  // TF_adv - T_aver and vd_salt, row j = node n0 + j
-    real *sK = sm + 2 * kVdTile * LP;        // Kv
-    real *sA = sK + kVdTile * KP;            // aj
-    for (long long n0 = (long long)blockIdx.x * kVdTile; n0 < N; n0 += (long long)gridDim.x * kVdTile) {
-        const int nt = (int)(N - n0 < kVdTile ? N - n0 : kVdTile);
-        if ((int)threadIdx.x < nt) sA[threadIdx.x] = jac_a(d, d.eta_jac, (int)n0 + threadIdx.x);
-        for (int i = threadIdx.x; i < nt * NS; i += blockDim.x) {
+template <bool kAtm, int LC>
+__global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
+    extern __shared__ __align__(16) unsigned char vt_smem[];
+    constexpr int L = LC, LP = LC | 1;
+    const int NS = d.NS, KP = vd_odd(d.NS), N = d.N;
+    real *sT = reinterpret_cast<real *>(vt_smem);  // row j: node n0 + j
+    real *sS = sT + kVtCols * LP;
+    real *sK = sS + kVtCols * LP;
+    for (long long n0 = (long long)blockIdx.x * kVtCols; n0 < N; n0 += (long long)gridDim.x * kVtCols) {
+        const int nt = (int)(N - n0 < kVtCols ? N - n0 : kVtCols);
+        for (int i = threadIdx.x; i < nt * NS; i += kVtCols) {
             const int j = i / NS;
             sK[j * KP + (i - j * NS)] = d.Kv[(size_t)n0 * NS + i];
         }
-        __syncthreads();
-        // the tile's columns are contiguous node-major: coalesced reads
-        for (int i = threadIdx.x; i < nt * L; i += blockDim.x) {
+        for (int i = threadIdx.x; i < nt * L; i += kVtCols) {
             const int j = i / L, z = i - j * L;
             const int n = (int)n0 + j;
             const size_t g = (size_t)n0 * L + i;
             sT[j * LP + z] = d.TF_adv[g] - t_aver_of(d, n);
-            sS[j * LP + z] = vd_salt(d, n, (size_t)n * L, z, sA[j], s_aver_of(d, n));
+            sS[j * LP + z] = vd_salt(d, n, (size_t)n * L, z, jac_a(d, d.eta_jac, n), s_aver_of(d, n));
             d.T_old[g] = d.Told_new[g];
             d.S_old[g] = d.Sold_new[g];
         }
         __syncthreads();
-        // one thread per (node, layer), node fastest: level-major writes
-        for (int i = threadIdx.x; i < kVdTile * L; i += blockDim.x) {
-            const int j = i % kVdTile, k = i / kVdTile;
-            if (j >= nt) continue;
-            const int n = (int)n0 + j;
-            const real aj = sA[j];
-            const real *T = sT + j * LP, *S = sS + j * LP;
-            real a, b, c, tr, sr;
-            vd_coef(d, sK + j * KP, aj, k, a, b, c);
-            const real T0 = T[k], S0 = S[k];
-            if (k == 0) {
-                tr = c * (-T[1] + T0);
-                sr = c * (-S[1] + S0);
-            } else if (k == L - 1) {
-                tr = a * (T0 - T[k - 1]);
-                sr = a * (S0 - S[k - 1]);
-            } else {
-                tr = -a * T[k - 1] - c * T[k + 1] + (a + c) * T0;
-                sr = -a * S[k - 1] - c * S[k + 1] + (a + c) * S0;
+        if ((int)threadIdx.x < nt) {
+            const int j = threadIdx.x, n = (int)n0 + j;
+            const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
+            const size_t base = (size_t)n * L;
+            const real aj = jac_a(d, d.eta_jac, n);
+            const real *Kv = sK + j * KP;
+            real *T = sT + j * LP, *S = sS + j * LP;
+            real CP[LC], TP[LC], SP[LC];
+            real cpv = real(0.0), tpv = real(0.0), spv = real(0.0);
+            const bool atm = kAtm && d.mask_wd_node[n] != real(0.0);
+            const real frw = atm ? evap_precip(d, n, aj, T[0], S[0], T_aver, S_aver) : real(0.0);
+#pragma unroll
+            for (int k = 0; k < L; ++k) {
+                real a, b, c, tr, sr;
+                vd_coef(d, Kv, aj, k, a, b, c);
+                const real T0 = T[k], S0 = S[k];
+                if (k == 0) {
+                    tr = c * (-T[1] + T0);
+                    sr = c * (-S[1] + S0);
+                } else if (k == L - 1) {
+                    tr = a * (T0 - T[k - 1]);
+                    sr = a * (S0 - S[k - 1]);
+                } else {
+                    tr = -a * T[k - 1] - c * T[k + 1] + (a + c) * T0;
+                    sr = -a * S[k - 1] - c * S[k + 1] + (a + c) * S0;
+                }
+                if (atm) {
+                    tr = tr + d.dt * heat_source(d, n, base, k, aj, T_aver, S_aver);
+                    if (k == 0) sr = sr + d.dt * frw;
+                }
+                if (k == 0) {
+                    cpv = c / b;
+                    tpv = tr / b;
+                    spv = sr / b;
+                } else {
+                    const real m = real(1.0) / (b - cpv * a);
+                    cpv = c * m;
+                    tpv = (tr - tpv * a) * m;
+                    spv = (sr - spv * a) * m;
+                }
+                CP[k] = cpv;
+                TP[k] = tpv;
+                SP[k] = spv;
             }
-            if (kAtm && d.mask_wd_node[n] != real(0.0)) {
-                const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
-                tr = tr + d.dt * heat_source(d, n, (size_t)n * L, k, aj, T_aver, S_aver);
-                if (k == 0) sr = sr + d.dt * evap_precip(d, n, aj, T[0], S[0], T_aver, S_aver);
+            unsigned int st = 0;
+            real tr = real(0.0), sr = real(0.0);
+#pragma unroll
+            for (int z = L - 1; z >= 0; --z) {
+                if (z == L - 1) { tr = TP[z]; sr = SP[z]; }
+                else { tr = TP[z] - CP[z] * tr; sr = SP[z] - CP[z] * sr; }
+                real t = T[z] + tr + T_aver;
+                real s = S[z] + sr + S_aver;
+                if (fabs(s) < real(1.0e-12)) s = fabs(s);
+                if (s < real(0.0)) st |= 0x1u;
+                if (t < -real(3.0)) st |= 0x2u;
+                if (!isfinite(t) || !isfinite(s)) st |= 0x4u;
+                T[z] = t;
+                S[z] = s;
             }
-            const size_t o = (size_t)k * N + n;
-            d.vd_a[o] = a;
-            d.vd_b[o] = b;
-            d.vd_c[o] = c;
-            d.vd_tr[o] = tr;
-            d.vd_sr[o] = sr;
-            d.vd_t[o] = T0;
-            d.vd_s[o] = S0;
+            if (!isfinite(d.eta_n[n])) st |= 0x4u;
+            if (st) atomicOr(d.status, st);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt * L; i += kVtCols) {
+            const int j = i / L, z = i - j * L;
+            const size_t g = (size_t)n0 * L + i;
+            d.TF[g] = sT[j * LP + z];
+            d.SF[g] = sS[j * LP + z];
         }
         __syncthreads();
     }
 }
 
-// Elimination and back substitution of each column (ARR >= L) from the
-// set-up's level-major arrays; the recurrences of k_vdiff_col in the same
-// order, and the same update and status bits.
-template <int ARR>
-__global__ void __launch_bounds__(128) k_vdiff_sweep(Dev d) {
-    const int L = d.L;
-    const size_t N = d.N;
-    GRID_LOOP(ii, d.N) {
-        const int n = (int)ii;
-        const real T_aver = t_aver_of(d, n), S_aver = s_aver_of(d, n);
-        real CP[ARR], TP[ARR], SP[ARR];
-        real cpv = real(0.0), tpv = real(0.0), spv = real(0.0);
-#pragma unroll 4
-        for (int k = 0; k < L; ++k) {
-            const size_t o = (size_t)k * N + n;
-            const real a = d.vd_a[o], b = d.vd_b[o], c = d.vd_c[o], tr = d.vd_tr[o], sr = d.vd_sr[o];
-            if (k == 0) {
-                cpv = c / b;
-                tpv = tr / b;
-                spv = sr / b;
-            } else {
-                const real m = real(1.0) / (b - cpv * a);
-                cpv = c * m;
-                tpv = (tr - tpv * a) * m;
-                spv = (sr - spv * a) * m;
-            }
-            CP[k] = cpv;
-            TP[k] = tpv;
-            SP[k] = spv;
-        }
-        unsigned int st = 0;
-        real tr = real(0.0), sr = real(0.0);
-        const size_t base = (size_t)n * L;
-#pragma unroll 4
-        for (int z = L - 1; z >= 0; --z) {
-            if (z == L - 1) { tr = TP[z]; sr = SP[z]; }
-            else { tr = TP[z] - CP[z] * tr; sr = SP[z] - CP[z] * sr; }
-            const size_t o = (size_t)z * N + n;
-            real t = d.vd_t[o] + tr + T_aver;
-            real s = d.vd_s[o] + sr + S_aver;
-            if (fabs(s) < real(1.0e-12)) s = fabs(s);
-            if (s < real(0.0)) st |= 0x1u;
-            if (t < -real(3.0)) st |= 0x2u;
-            if (!isfinite(t) || !isfinite(s)) st |= 0x4u;
-            d.TF[base + z] = t;
-            d.SF[base + z] = s;
-        }
-        if (!isfinite(d.eta_n[n])) st |= 0x4u;
-        if (st) atomicOr(d.status, st);
-    }
+static size_t vdiff_tile_smem(const Dev &d) {
+    return (size_t)kVtCols * (2 * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
 }
-
-static size_t vdiff_setup_smem(const Dev &d) {
-    return ((size_t)kVdTile * (2 * vd_odd(d.L) + vd_odd(d.NS)) + kVdTile) * sizeof(real);
-}
-// the two-kernel form, for columns of up to 64 layers (the sweep's arrays)
-static bool vdiff_split(const Dev &d) { return d.tune[TK_VDIFF] == 2 && d.L <= 64; }
+// the tiled form is compiled for 10 and 20 layers (11 and 21 sigma levels)
+static bool vdiff_tiled(const Dev &d) { return d.tune[TK_VDIFF] == 2 && (d.L == 10 || d.L == 20); }
 
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 int config_vdiff(const Dev &d) {
-    return (raise_smem_limit(k_vdiff_col<false>, vdiff_smem(d)) == cudaSuccess &&
-            raise_smem_limit(k_vdiff_col<true>, vdiff_smem(d)) == cudaSuccess &&
-            (d.L > 64 || (raise_smem_limit(k_vdiff_setup<false>, vdiff_setup_smem(d)) == cudaSuccess &&
-                          raise_smem_limit(k_vdiff_setup<true>, vdiff_setup_smem(d)) == cudaSuccess))) ? 0 : 1;
+    if (raise_smem_limit(k_vdiff_col<false>, vdiff_smem(d)) != cudaSuccess ||
+        raise_smem_limit(k_vdiff_col<true>, vdiff_smem(d)) != cudaSuccess)
+        return 1;
+    if (d.L != 10 && d.L != 20) return 0;
+    const size_t sm = vdiff_tile_smem(d);
+    const bool ok = d.L == 10 ? (raise_smem_limit(k_vdiff_tile<false, 10>, sm) == cudaSuccess &&
+                                 raise_smem_limit(k_vdiff_tile<true, 10>, sm) == cudaSuccess)
+                              : (raise_smem_limit(k_vdiff_tile<false, 20>, sm) == cudaSuccess &&
+                                 raise_smem_limit(k_vdiff_tile<true, 20>, sm) == cudaSuccess);
+    return ok ? 0 : 1;
 }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
-    if (vdiff_split(d)) {
-        const int tiles = (d.N + kVdTile - 1) / kVdTile;
-        const int g = tiles < 148 * 16 ? tiles : 148 * 16;
-        if (d.key_atm) k_vdiff_setup<true><<<g, kVdSetupThreads, vdiff_setup_smem(d), s>>>(d);
-        else k_vdiff_setup<false><<<g, kVdSetupThreads, vdiff_setup_smem(d), s>>>(d);
-        if (d.L <= 11) k_vdiff_sweep<11><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-        else if (d.L <= 21) k_vdiff_sweep<21><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-        else if (d.L <= 40) k_vdiff_sweep<40><<<grid_for(d.N, 128), 128, 0, s>>>(d);
-        else k_vdiff_sweep<64><<<grid_for(d.N, 128), 128, 0, s>>>(d);
+    if (vdiff_tiled(d)) {
+        const long long tiles = ((long long)d.N + kVtCols - 1) / kVtCols;
+        const int g = (int)(tiles < (1LL << 30) ? tiles : (1LL << 30));
+        const size_t sm = vdiff_tile_smem(d);
+        if (d.L == 10 && d.key_atm) k_vdiff_tile<true, 10><<<g, kVtCols, sm, s>>>(d);
+        else if (d.L == 10) k_vdiff_tile<false, 10><<<g, kVtCols, sm, s>>>(d);
+        else if (d.key_atm) k_vdiff_tile<true, 20><<<g, kVtCols, sm, s>>>(d);
+        else k_vdiff_tile<false, 20><<<g, kVtCols, sm, s>>>(d);
         return;
     }
     if (d.key_atm) k_vdiff_col<true><<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);

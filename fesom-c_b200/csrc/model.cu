@@ -738,8 +738,6 @@ int alloc_3d(fesomc_model *m, D &d) {
         decltype(&d.U_n) d3s[] = {&d.d3_pb, &d.d3_qb, &d.d3_c2, &d.d3_sn};
         for (auto p : d3s) if ((rc = dalloc(m, p, NS * N))) return rc;
     }
-    decltype(&d.U_n) vds[] = {&d.vd_a, &d.vd_b, &d.vd_c, &d.vd_tr, &d.vd_sr, &d.vd_t, &d.vd_s};
-    for (auto p : vds) if ((rc = dalloc(m, p, L * N))) return rc;
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
     const size_t nm = (size_t)m->n_members;
     if ((rc = dalloc(m, &d.mm_part, (size_t)4 * nm * fesomc::f64::minmax_parts((int)nm)))) return rc;

@@ -457,10 +457,10 @@ def _estuary21(cases, **kw):
                                      "reg6_11", "reg8_11_atm", "reg6_21", "reg8_21"])
 def test_two_kernel_forms_bit_exact(mods, variant):
     """The set-up + sweep forms of d3_end (sweep arrays in local memory, in
-    shared memory, in registers for 11 and 21 levels) and of the tracers'
-    vertical diffusion against the oracle, with the river salinity source
-    and with atmospheric heat and freshwater sources in the column solve,
-    20 steps, exact."""
+    shared memory, in registers for 11 and 21 levels) and the tiled form of
+    the tracers' vertical diffusion (10 and 20 layers) against the oracle,
+    with the river salinity source and with atmospheric heat and freshwater
+    sources in the column solve, 20 steps, exact."""
     abi, cases, model, pyoracle = mods
     make, shapes = {
         "rivers_split_local": (est(cases, "small"), {"d3end_arrays": 3, "vdiff_form": 2}),
