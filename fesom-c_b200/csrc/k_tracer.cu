@@ -772,17 +772,21 @@ __global__ void __launch_bounds__(128, 8) k_miura_h(Dev d) {
 // Tracer after advection and the river source, minus its mean: T(k) / S(k)
 // of tracer_impl_vert_diff.  The river source (fv_main.F90:1804-1823) adds
 // its terms to S in river-list order.
-__device__ __forceinline__ real vd_salt(const Dev &d, int n, size_t base, int z, real aj, real S_aver) {
-    real S = d.SF_adv[base + z];
+// S: SF_adv of (n, z); Sn: Sold_new of (n, z), read only at river nodes
+__device__ __forceinline__ real vd_salt_of(const Dev &d, int n, int z, real aj, real S, real Sn, real S_aver) {
     if (d.key_rivers) {
         for (int p = d.node_rptr[n]; p < d.node_rptr[n + 1]; ++p) {
             const real r = d.runoff[d.node_ridx[p]];
             const real coeff = r * __ldg(d.dsig + z) * d.dt / (d.area[n] * jc_of(d, aj, z));
-            const real delta = (d.river_salinity - d.Sold_new[base + z]);
+            const real delta = (d.river_salinity - Sn);
             S = S + delta * coeff;
         }
     }
     return S - S_aver;
+}
+__device__ __forceinline__ real vd_salt(const Dev &d, int n, size_t base, int z, real aj, real S_aver) {
+    const bool river = d.key_rivers && d.node_rptr[n] < d.node_rptr[n + 1];
+    return vd_salt_of(d, n, z, aj, d.SF_adv[base + z], river ? d.Sold_new[base + z] : real(0.0), S_aver);
 }
 
 // Tridiagonal coefficients a(k), b(k), c(k) of layer k (0-based) of node
@@ -1089,12 +1093,14 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) {
 // consecutive nodes, whose columns are one contiguous range of every
 // [node][layer] field: it stages T - T_aver, the river-adjusted S - S_aver
 // and Kv in shared memory with coalesced loads (copying Told_new / Sold_new
-// to T_old / S_old on the way), solves each column with one thread from
+// to T_old / S_old on the way; each thread loads a batch of items before
+// storing any), solves each column with one thread from
 // shared memory (rows of odd stride: no bank conflicts) with the sweep's
 // recurrences in registers (the layer count LC is fixed at compile time),
 // writes the new tracers over the staged ones and stores them coalesced.
 // The arithmetic and its order are k_vdiff_col's.
 constexpr int kVtCols = 128;
+constexpr int kVtBatch = 4;
 __host__ __device__ __forceinline__ int vd_odd(int x) { return x | 1; }
 
 template <bool kAtm, int LC>
@@ -1107,18 +1113,44 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
     real *sK = sS + kVtCols * LP;
     for (long long n0 = (long long)blockIdx.x * kVtCols; n0 < N; n0 += (long long)gridDim.x * kVtCols) {
         const int nt = (int)(N - n0 < kVtCols ? N - n0 : kVtCols);
-        for (int i = threadIdx.x; i < nt * NS; i += kVtCols) {
-            const int j = i / NS;
-            sK[j * KP + (i - j * NS)] = d.Kv[(size_t)n0 * NS + i];
+        // staging: kVtBatch items per thread loaded before any is used, so
+        // that each thread keeps several loads in flight
+        for (int i0 = threadIdx.x; i0 < nt * NS; i0 += kVtBatch * kVtCols) {
+            real kv[kVtBatch];
+#pragma unroll
+            for (int u = 0; u < kVtBatch; ++u) {
+                const int i = i0 + u * kVtCols;
+                kv[u] = i < nt * NS ? d.Kv[(size_t)n0 * NS + i] : real(0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kVtBatch; ++u) {
+                const int i = i0 + u * kVtCols, j = i / NS;
+                if (i < nt * NS) sK[j * KP + (i - j * NS)] = kv[u];
+            }
         }
-        for (int i = threadIdx.x; i < nt * L; i += kVtCols) {
-            const int j = i / L, z = i - j * L;
-            const int n = (int)n0 + j;
-            const size_t g = (size_t)n0 * L + i;
-            sT[j * LP + z] = d.TF_adv[g] - t_aver_of(d, n);
-            sS[j * LP + z] = vd_salt(d, n, (size_t)n * L, z, jac_a(d, d.eta_jac, n), s_aver_of(d, n));
-            d.T_old[g] = d.Told_new[g];
-            d.S_old[g] = d.Sold_new[g];
+        for (int i0 = threadIdx.x; i0 < nt * L; i0 += kVtBatch * kVtCols) {
+            real ta[kVtBatch], sa[kVtBatch], tn[kVtBatch], sn[kVtBatch];
+#pragma unroll
+            for (int u = 0; u < kVtBatch; ++u) {
+                const int i = i0 + u * kVtCols;
+                const size_t g = (size_t)n0 * L + (i < nt * L ? i : 0);
+                ta[u] = d.TF_adv[g];
+                sa[u] = d.SF_adv[g];
+                tn[u] = d.Told_new[g];
+                sn[u] = d.Sold_new[g];
+            }
+#pragma unroll
+            for (int u = 0; u < kVtBatch; ++u) {
+                const int i = i0 + u * kVtCols;
+                if (i >= nt * L) continue;
+                const int j = i / L, z = i - j * L;
+                const int n = (int)n0 + j;
+                const size_t g = (size_t)n0 * L + i;
+                sT[j * LP + z] = ta[u] - t_aver_of(d, n);
+                sS[j * LP + z] = vd_salt_of(d, n, z, jac_a(d, d.eta_jac, n), sa[u], sn[u], s_aver_of(d, n));
+                d.T_old[g] = tn[u];
+                d.S_old[g] = sn[u];
+            }
         }
         __syncthreads();
         if ((int)threadIdx.x < nt) {
