@@ -1089,7 +1089,8 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) {
 }
 // ---- tracer_impl_vert_diff on tiles of columns (knob vdiff_form = 2) -------
 // k_vdiff_col reads each column with one thread, so a warp's loads of one
-// layer touch 32 rows L values apart.  Here a block takes kVtCols
+// layer touch 32 rows L values apart.  Here a block takes kVtCols (128 or
+// 64)
 // consecutive nodes, whose columns are one contiguous range of every
 // [node][layer] field: it stages T - T_aver, the river-adjusted S - S_aver
 // and Kv in shared memory with coalesced loads (copying Told_new / Sold_new
@@ -1099,11 +1100,10 @@ void launch_muscl_h(const Dev &d, cudaStream_t s) {
 // recurrences in registers (the layer count LC is fixed at compile time),
 // writes the new tracers over the staged ones and stores them coalesced.
 // The arithmetic and its order are k_vdiff_col's.
-constexpr int kVtCols = 128;
 constexpr int kVtBatch = 4;
 __host__ __device__ __forceinline__ int vd_odd(int x) { return x | 1; }
 
-template <bool kAtm, int LC>
+template <bool kAtm, int LC, int kVtCols>
 __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
     extern __shared__ __align__(16) unsigned char vt_smem[];
     constexpr int L = LC, LP = LC | 1;
@@ -1226,35 +1226,45 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
     }
 }
 
-static size_t vdiff_tile_smem(const Dev &d) {
-    return (size_t)kVtCols * (2 * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
+// columns per tile: 128 (vdiff_form 2, the default) or 64 (3)
+static int vdiff_cols(const Dev &d) { return d.tune[TK_VDIFF] == 3 ? 64 : 128; }
+static size_t vdiff_tile_smem(const Dev &d, int cols) {
+    return (size_t)cols * (2 * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
 }
 // the tiled form is compiled for 10 and 20 layers (11 and 21 sigma levels)
-static bool vdiff_tiled(const Dev &d) { return d.tune[TK_VDIFF] == 2 && (d.L == 10 || d.L == 20); }
+static bool vdiff_tiled(const Dev &d) { return d.tune[TK_VDIFF] != 1 && (d.L == 10 || d.L == 20); }
 
 static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
+template <int LC, int C>
+static bool config_vdiff_tile(const Dev &d) {
+    const size_t sm = vdiff_tile_smem(d, C);
+    return raise_smem_limit(k_vdiff_tile<false, LC, C>, sm) == cudaSuccess &&
+           raise_smem_limit(k_vdiff_tile<true, LC, C>, sm) == cudaSuccess;
+}
 int config_vdiff(const Dev &d) {
     if (raise_smem_limit(k_vdiff_col<false>, vdiff_smem(d)) != cudaSuccess ||
         raise_smem_limit(k_vdiff_col<true>, vdiff_smem(d)) != cudaSuccess)
         return 1;
-    if (d.L != 10 && d.L != 20) return 0;
-    const size_t sm = vdiff_tile_smem(d);
-    const bool ok = d.L == 10 ? (raise_smem_limit(k_vdiff_tile<false, 10>, sm) == cudaSuccess &&
-                                 raise_smem_limit(k_vdiff_tile<true, 10>, sm) == cudaSuccess)
-                              : (raise_smem_limit(k_vdiff_tile<false, 20>, sm) == cudaSuccess &&
-                                 raise_smem_limit(k_vdiff_tile<true, 20>, sm) == cudaSuccess);
-    return ok ? 0 : 1;
+    if (d.L == 10) return config_vdiff_tile<10, 128>(d) && config_vdiff_tile<10, 64>(d) ? 0 : 1;
+    if (d.L == 20) return config_vdiff_tile<20, 128>(d) && config_vdiff_tile<20, 64>(d) ? 0 : 1;
+    return 0;
+}
+template <int LC, int C>
+static void launch_vdiff_tile(const Dev &d, cudaStream_t s) {
+    const long long tiles = ((long long)d.N + C - 1) / C;
+    const int g = (int)(tiles < (1LL << 30) ? tiles : (1LL << 30));
+    const size_t sm = vdiff_tile_smem(d, C);
+    if (d.key_atm) k_vdiff_tile<true, LC, C><<<g, C, sm, s>>>(d);
+    else k_vdiff_tile<false, LC, C><<<g, C, sm, s>>>(d);
 }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     if (vdiff_tiled(d)) {
-        const long long tiles = ((long long)d.N + kVtCols - 1) / kVtCols;
-        const int g = (int)(tiles < (1LL << 30) ? tiles : (1LL << 30));
-        const size_t sm = vdiff_tile_smem(d);
-        if (d.L == 10 && d.key_atm) k_vdiff_tile<true, 10><<<g, kVtCols, sm, s>>>(d);
-        else if (d.L == 10) k_vdiff_tile<false, 10><<<g, kVtCols, sm, s>>>(d);
-        else if (d.key_atm) k_vdiff_tile<true, 20><<<g, kVtCols, sm, s>>>(d);
-        else k_vdiff_tile<false, 20><<<g, kVtCols, sm, s>>>(d);
+        const bool c64 = vdiff_cols(d) == 64;
+        if (d.L == 10 && c64) launch_vdiff_tile<10, 64>(d, s);
+        else if (d.L == 10) launch_vdiff_tile<10, 128>(d, s);
+        else if (c64) launch_vdiff_tile<20, 64>(d, s);
+        else launch_vdiff_tile<20, 128>(d, s);
         return;
     }
     if (d.key_atm) k_vdiff_col<true><<<grid_for(d.N, vdiff_block(d)), vdiff_block(d), vdiff_smem(d), s>>>(d);

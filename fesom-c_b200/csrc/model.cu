@@ -1831,7 +1831,7 @@ const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"muscl_h", "muscl_h", 128}, {"upwind_h", "upwind_h", 128}, {"av", "av", 256},
     {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
     {"d3end_arrays", "d3end,d3end_list", 1},
-    {"vdiff_form", "vdiff_col", 1},
+    {"vdiff_form", "vdiff_col", 2},
 };
 int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
 void drop_graph(fesomc_model *m);
@@ -1861,7 +1861,7 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
     lim[fesomc::TK_D3END] = 6;
-    lim[fesomc::TK_VDIFF] = 2;
+    lim[fesomc::TK_VDIFF] = 3;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         if (values) {
             const int v = m->d.tune[k];

@@ -32,8 +32,9 @@ COLUMNS = (1, 2, 4, 8, 16, 32)
 # (the sweep's arrays in local memory, in shared memory, or in registers at
 # 6 or 8 resident blocks per SM)
 D3END_ARRAYS = (1, 2, 3, 4, 5, 6)
-# tracer_impl_vert_diff: columns read directly, or tiles staged in shared memory
-VDIFF_FORMS = (1, 2)
+# tracer_impl_vert_diff: columns read directly, or tiles of 128 or 64 columns
+# staged in shared memory
+VDIFF_FORMS = (1, 2, 3)
 # the knobs that pick a form rather than a block size
 FORMS = {"columns": COLUMNS, "d3end_arrays": D3END_ARRAYS, "vdiff_form": VDIFF_FORMS}
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "launch_shapes_b200.json")

@@ -406,9 +406,10 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * d3_end's column arrays in local or in shared memory, or a set-up and a
  * sweep kernel with the sweep's arrays in local memory, in shared memory, or
  * (11 or 21 levels) in registers at 6 or 8 blocks of 64 columns per SM;
- * "vdiff_form" 1 or 2: the tracers' implicit vertical diffusion with each
- * column read directly by its thread, or on tiles of 128 columns staged in
- * shared memory, for 10 or 20 layers); the next step captures its
+ * "vdiff_form" 1 to 3: the tracers' implicit vertical diffusion with each
+ * column read directly by its thread, or on tiles of 128 (the default) or
+ * 64 columns staged in shared memory, for 10 or 20 layers); the next step
+ * captures its
  * graph again.  The search over the knobs and its cache per mesh size and
  * level count live with the host driver (fesomc/autotune.py).  No
  * counterpart in the reference. */
