@@ -1056,6 +1056,18 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
     k_minmax_part<<<dim3(parts, d.n_members), kRedBlock, 0, s>>>(d);
     k_minmax_final<<<d.n_members, 32, 0, s>>>(d, parts);
 }
+// T_aver / S_aver from a range the host gives (fesomc_gpu_set_tracer_range:
+// the min / max over the whole domain of a decomposed mesh), with
+// k_minmax_final's expression
+__global__ void k_aver_from_range(Dev d, const double *r) {
+    if (threadIdx.x == 0) {
+        d.aver[0] = real(0.5) * ((real)r[0] + (real)r[1]);
+        d.aver[1] = real(0.5) * ((real)r[2] + (real)r[3]);
+    }
+}
+void launch_aver_from_range(const Dev &d, const double *range, cudaStream_t s) {
+    k_aver_from_range<<<1, 32, 0, s>>>(d, range);
+}
 void launch_ab2(const Dev &d, cudaStream_t s) {
     const int b = tuned(d, TK_AB2, 256);
     k_ab2_node<<<grid_for((long long)d.N * d.L, b), b, 0, s>>>(d);
@@ -1226,8 +1238,8 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
     }
 }
 
-// columns per tile: 128 (vdiff_form 2, the default) or 64 (3)
-static int vdiff_cols(const Dev &d) { return d.tune[TK_VDIFF] == 3 ? 64 : 128; }
+// columns per tile: 128 (vdiff_form 2) or 64 (3, the default)
+static int vdiff_cols(const Dev &d) { return d.tune[TK_VDIFF] == 2 ? 128 : 64; }
 static size_t vdiff_tile_smem(const Dev &d, int cols) {
     return (size_t)cols * (2 * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
 }

@@ -52,6 +52,7 @@ namespace fesomc {
     void launch_d3end(const Dev &, cudaStream_t); \
     void launch_av(const Dev &, cudaStream_t); \
     void launch_minmax(const Dev &, cudaStream_t); \
+    void launch_aver_from_range(const Dev &, const double *, cudaStream_t); \
     void launch_upwind(const Dev &, cudaStream_t); \
     void launch_muscl_egrad(const Dev &, cudaStream_t); \
     void launch_muscl_ngrad(const Dev &, cudaStream_t); \
@@ -172,6 +173,10 @@ struct fesomc_model {
     const int *d_nd_ref = nullptr, *d_el_ref = nullptr;
     void *d_perm_buf = nullptr;       // staging of one field in reference order
     size_t perm_buf_bytes = 0;
+    // tracer range given by the host (fesomc_gpu_set_tracer_range): tmin,
+    // tmax, smin, smax on the device, replacing the step's own min / max
+    bool ext_range = false;
+    double *d_ext_range = nullptr;
     // graph
     cudaGraphExec_t graph = nullptr;
     bool use_graph = true;
@@ -1064,8 +1069,9 @@ int enqueue_step(fesomc_model *m, double ff) {
     rec(m, "jac_swap", [&] { launch_jac_swap(d, s); });
     rec(m, "update3d", [&] { K3(launch_update3d, 1.0 / (double)d.Mt, s); });
     rec(m, "wvel", [&] { K3(launch_wvel, s); });
-    rec(m, "minmax", [&] { K3(launch_minmax, s); });
-    n += 5;
+    if (m->ext_range) rec(m, "minmax", [&] { K3(launch_aver_from_range, m->d_ext_range, s); });
+    else rec(m, "minmax", [&] { K3(launch_minmax, s); });
+    n += m->ext_range ? 4 : 5;
     if (d.tracer_adv != FESOMC_TRACER_MIURA) { rec(m, "ab2_node", [&] { K3(launch_ab2, s); }); n += 1; }
     if (d.tracer_adv == FESOMC_TRACER_MIURA) { rec(m, "miura", [&] { K3(launch_miura, s); }); n += 5; }
     else if (d.tracer_adv == FESOMC_TRACER_MUSCL) {
@@ -1831,7 +1837,7 @@ const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"muscl_h", "muscl_h", 128}, {"upwind_h", "upwind_h", 128}, {"av", "av", 256},
     {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
     {"d3end_arrays", "d3end,d3end_list", 1},
-    {"vdiff_form", "vdiff_col", 2},
+    {"vdiff_form", "vdiff_col", 3},
 };
 int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
 void drop_graph(fesomc_model *m);
@@ -1842,6 +1848,30 @@ int copy_str(const char *src, char *dst, int32_t len) {
     return FESOMC_OK;
 }
 }  // namespace
+
+int fesomc_gpu_set_tracer_range(fesomc_model *m, const double *range) {
+    if (!m) return FESOMC_EINVAL;
+    if (!range) {
+        if (m->ext_range) {
+            drop_graph(m);
+            m->ext_range = false;
+        }
+        return FESOMC_OK;
+    }
+    if (m->n_members > 1 || !(range[0] <= range[1]) || !(range[2] <= range[3])) return FESOMC_EINVAL;
+    if (!m->d_ext_range) {
+        const int rc = dalloc(m, &m->d_ext_range, 4);
+        if (rc) return rc;
+    }
+    // ordered after the steps already enqueued, which read the previous range
+    CK(cudaMemcpyAsync(m->d_ext_range, range, 4 * sizeof(double), cudaMemcpyHostToDevice, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    if (!m->ext_range) {
+        drop_graph(m);   // the captured step computes its own range
+        m->ext_range = true;
+    }
+    return FESOMC_OK;
+}
 
 int fesomc_gpu_tune_knobs(void) { return fesomc::kTuneKnobs; }
 

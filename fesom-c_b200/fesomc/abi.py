@@ -100,6 +100,7 @@ SIGNATURES = {
     "fesomc_gpu_run": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "fesomc_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
     "fesomc_gpu_sync_from_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
+    "fesomc_gpu_set_tracer_range": (C.c_int, [C.c_void_p, f64p]),
     "fesomc_gpu_snapshot_begin": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
     "fesomc_gpu_snapshot_end": (C.c_int, [C.c_void_p]),
     "fesomc_gpu_energy": (C.c_int, [C.c_void_p, f64p]),

@@ -308,6 +308,15 @@ int  fesomc_gpu_snapshot_begin(fesomc_model *m, uint32_t field_mask, fesomc_stat
 int  fesomc_gpu_snapshot_end(fesomc_model *m);
 int  fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t field_mask, const fesomc_state *state);
 int  fesomc_gpu_energy(fesomc_model *m, double *eout);
+/* Tracer range of a decomposed mesh: range = {Tmin, Tmax, Smin, Smax} over
+ * the whole domain (the min / max of solve_tracers, src/fv_tracer.F90:18-27,
+ * which the reference takes over all ranks), used by the following steps
+ * in place of the min / max over this model's own nodes: T_aver and S_aver
+ * are formed from it as from the model's own.  Give it before every step
+ * (the ranks' tracers change); NULL goes back to the model's own min / max.
+ * FESOMC_EINVAL for packed members or a range with min > max or NaN.  No
+ * counterpart in the reference (one MPI reduction there). */
+int  fesomc_gpu_set_tracer_range(fesomc_model *m, const double *range);
 int  fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv_columns);
 int  fesomc_gpu_finalize(fesomc_model *m);
 const char *fesomc_gpu_error_string(int code);
@@ -407,8 +416,8 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * sweep kernel with the sweep's arrays in local memory, in shared memory, or
  * (11 or 21 levels) in registers at 6 or 8 blocks of 64 columns per SM;
  * "vdiff_form" 1 to 3: the tracers' implicit vertical diffusion with each
- * column read directly by its thread, or on tiles of 128 (the default) or
- * 64 columns staged in shared memory, for 10 or 20 layers); the next step
+ * column read directly by its thread, or on tiles of 128 or 64 (the
+ * default) columns staged in shared memory, for 10 or 20 layers); the next step
  * captures its
  * graph again.  The search over the knobs and its cache per mesh size and
  * level count live with the host driver (fesomc/autotune.py).  No
