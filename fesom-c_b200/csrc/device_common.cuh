@@ -82,11 +82,14 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // 21 levels), and the form of the tracers'
 // implicit vertical diffusion (1 one thread per column reading the fields
 // directly, 2 and 3 tiles of 128 or 64 columns staged in shared memory, for
-// 10 or 20 layers; other layer counts take form 1).  A value of 0 selects the built-in default.
+// 10 or 20 layers; other layer counts take form 1), and the form of the
+// implicit vertical viscosity (1 one thread per element column reading the
+// fields directly, 2 tiles of 64 columns staged in shared memory: the fic
+// variant, 10 or 20 layers).  A value of 0 selects the built-in default.
 enum TuneKnob : int {
     TK_VELRHS, TK_VELGRAD3D, TK_ADV3, TK_PULS, TK_EL2NODES, TK_P1EDGE, TK_AB3, TK_VELGRAD2D, TK_SSHEDGE,
     TK_SSHNODE, TK_ADV2D, TK_U2D, TK_ROT, TK_ZEROFILT, TK_AB2, TK_MEGRAD, TK_MNGRAD, TK_MEDGE, TK_MH,
-    TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, TK_VDIFF, kTuneKnobs
+    TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, TK_VDIFF, TK_IMPLVISC, kTuneKnobs
 };
 
 namespace f64 {

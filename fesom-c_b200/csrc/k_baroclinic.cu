@@ -874,6 +874,138 @@ __global__ void k_wvel(Dev d) {
     }
 }
 
+// ---- momentum_vert_impl_visc_tmp on tiles of element columns --------------
+// (launch-shape knob "implvisc_form" 2, the default for 10 and 20 layers):
+// a block takes kIvCols consecutive elements, whose columns are one
+// contiguous range of U_rhs, V_rhs, Je and Av, stages them in shared memory
+// with coalesced loads (kIvBatch per thread in flight), solves each column
+// with one thread from shared memory (odd row strides: no bank conflicts),
+// the recurrences in registers (LC layers fixed at compile time), writes the
+// result over the staged U_rhs / V_rhs and stores it coalesced.  The
+// arithmetic and its order are k_implvisc's im_vert_visc_fic branch.
+constexpr int kIvCols = 64;
+constexpr int kIvBatch = 4;
+__host__ __device__ __forceinline__ int iv_odd(int x) { return x | 1; }
+
+template <int LC>
+__global__ void __launch_bounds__(kIvCols) k_implvisc_fic_tile(Dev d) {
+    extern __shared__ __align__(16) unsigned char iv_smem[];
+    constexpr int L = LC, LP = LC | 1;
+    const int NS = d.NS, KP = iv_odd(d.NS), E = d.E;
+    real *sU = reinterpret_cast<real *>(iv_smem);   // row j: element e0 + j
+    real *sV = sU + kIvCols * LP;
+    real *sJ = sV + kIvCols * LP;
+    real *sA = sJ + kIvCols * LP;                   // Av, stride KP
+    const real dt = d.dt;
+    for (long long e0 = (long long)blockIdx.x * kIvCols; e0 < E; e0 += (long long)gridDim.x * kIvCols) {
+        const int nt = (int)(E - e0 < kIvCols ? E - e0 : kIvCols);
+        for (int i0 = threadIdx.x; i0 < nt * NS; i0 += kIvBatch * kIvCols) {
+            real av[kIvBatch];
+#pragma unroll
+            for (int u = 0; u < kIvBatch; ++u) {
+                const int i = i0 + u * kIvCols;
+                av[u] = i < nt * NS ? d.Av[(size_t)e0 * NS + i] : real(0.0);
+            }
+#pragma unroll
+            for (int u = 0; u < kIvBatch; ++u) {
+                const int i = i0 + u * kIvCols, j = i / NS;
+                if (i < nt * NS) sA[j * KP + (i - j * NS)] = av[u];
+            }
+        }
+        for (int i0 = threadIdx.x; i0 < nt * L; i0 += kIvBatch * kIvCols) {
+            real ur[kIvBatch], vr[kIvBatch], jv[kIvBatch];
+#pragma unroll
+            for (int u = 0; u < kIvBatch; ++u) {
+                const int i = i0 + u * kIvCols;
+                const size_t g = (size_t)e0 * L + (i < nt * L ? i : 0);
+                ur[u] = d.U_rhs[g];
+                vr[u] = d.V_rhs[g];
+                jv[u] = d.Je[g];
+            }
+#pragma unroll
+            for (int u = 0; u < kIvBatch; ++u) {
+                const int i = i0 + u * kIvCols;
+                if (i >= nt * L) continue;
+                const int j = i / L, z = i - j * L;
+                sU[j * LP + z] = ur[u];
+                sV[j * LP + z] = vr[u];
+                sJ[j * LP + z] = jv[u];
+            }
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < nt) {
+            const int j = threadIdx.x, e = (int)e0 + j;
+            real *U = sU + j * LP, *V = sV + j * LP;
+            const real *J = sJ + j * LP, *A = sA + j * KP;
+            const real mwd = d.mask_wd[e];
+            if (mwd != real(0.0)) {
+                const real ub = d.U_n[(size_t)e * L + L - 1], vb = d.V_n[(size_t)e * L + L - 1];
+                const real a_Cd = d.C_d * ((real(1.0) - d.elem_acc[e]) * d.Cd_bz + real(1.0));
+                real xx1[LC + 1], yu[LC + 1], yv[LC + 1];
+                real de = J[0] / (A[0] + A[1]);
+                const real rw = de / d.density_0;
+                real xv = real(1.0), yuv = d.taux[e] * rw, yvv = d.tauy[e] * rw;
+                xx1[0] = xv;
+                yu[0] = yuv;
+                yv[0] = yvv;
+#pragma unroll
+                for (int z = 0; z < L; ++z) {
+                    const real jz = J[z];
+                    const real d1 = (z == 0) ? real(0.5) * jz : real(0.5) * (jz + J[z > 0 ? z - 1 : 0]);
+                    const real d2 = (z == L - 1) ? real(0.5) * jz : real(0.5) * (jz + J[z + 1 < L ? z + 1 : z]);
+                    const real zt = dt / jz;
+                    const real a = zt * A[z] / d1;
+                    const real c = zt * A[z + 1] / d2;
+                    const real b = a + c + real(1.0);
+                    const real dd = b - a * xv;
+                    xv = c / dd;
+                    yuv = (a * yuv + U[z]) / dd;
+                    yvv = (a * yvv + V[z]) / dd;
+                    xx1[z + 1] = xv;
+                    yu[z + 1] = yuv;
+                    yv[z + 1] = yvv;
+                }
+                de = J[L - 1] / (A[NS - 1] + A[L - 1]);
+                const real friction = de * a_Cd * sqrt(ub * ub + vb * vb);
+                real Ut, Vt;
+                if (d.fic_point == 0) { Ut = real(0.0); Vt = real(0.0); }
+                else if (d.fic_point == 1) {
+                    const real a = friction + real(1.0) - xx1[L];
+                    Ut = yu[L] / a; Vt = yv[L] / a;
+                } else {
+                    const real a = real(1.0) / (real(1.0) - friction) - xx1[L];
+                    Ut = yu[L] / a; Vt = yv[L] / a;
+                }
+#pragma unroll
+                for (int z = L - 1; z >= 0; --z) {
+                    Ut = Ut * xx1[z + 1] + yu[z + 1];
+                    Vt = Vt * xx1[z + 1] + yv[z + 1];
+                    U[z] = Ut * mwd;
+                    V[z] = Vt * mwd;
+                }
+            } else {
+#pragma unroll
+                for (int z = 0; z < L; ++z) { U[z] = real(0.0); V[z] = real(0.0); }
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt * L; i += kIvCols) {
+            const int j = i / L, z = i - j * L;
+            const size_t g = (size_t)e0 * L + i;
+            d.U_rhs[g] = sU[j * LP + z];
+            d.V_rhs[g] = sV[j * LP + z];
+        }
+        __syncthreads();
+    }
+}
+static size_t implvisc_tile_smem(const Dev &d) {
+    return (size_t)kIvCols * (3 * iv_odd(d.L) + iv_odd(d.NS)) * sizeof(real);
+}
+// the tiled form: the fic variant alone, 10 or 20 layers
+static bool implvisc_tiled(const Dev &d) {
+    return d.tune[TK_IMPLVISC] != 1 && !d.im_vert_visc && d.im_vert_visc_fic && (d.L == 10 || d.L == 20);
+}
+
 // ---- launch wrappers --------------------------------------------------------
 // column blocks: B = min(16, 1024 / L) entities, B * L threads
 static int col_b(const Dev &d) {
@@ -891,7 +1023,10 @@ static size_t col_smem(const Dev &d, int rows, int scalars) {
 }
 int config_columns(const Dev &d) {
     const size_t big = col_smem(d, 2, kU3Sc);
-    cudaError_t e = raise_smem_limit(k_bpg_elem, big);
+    cudaError_t e = cudaSuccess;
+    if (d.L == 10) e = raise_smem_limit(k_implvisc_fic_tile<10>, implvisc_tile_smem(d));
+    if (d.L == 20) e = raise_smem_limit(k_implvisc_fic_tile<20>, implvisc_tile_smem(d));
+    if (e == cudaSuccess) e = raise_smem_limit(k_bpg_elem, big);
     if (e == cudaSuccess) e = raise_smem_limit(k_update3d, big);
     if (e == cudaSuccess) e = raise_smem_limit(k_pressure_col, big);
     if (e == cudaSuccess) e = raise_smem_limit(k_wvel, big);
@@ -939,7 +1074,16 @@ void launch_velrhs(const Dev &d, real ff, cudaStream_t s) {
         else if (d.L <= 48) KERNEL<48><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);           \
         else KERNEL<128><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);                         \
     } while (0)
-void launch_implvisc(const Dev &d, cudaStream_t s) { MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d); }
+void launch_implvisc(const Dev &d, cudaStream_t s) {
+    if (implvisc_tiled(d)) {
+        const long long tiles = ((long long)d.E + kIvCols - 1) / kIvCols;
+        const int g = (int)(tiles < (1LL << 30) ? tiles : (1LL << 30));
+        if (d.L == 10) k_implvisc_fic_tile<10><<<g, kIvCols, implvisc_tile_smem(d), s>>>(d);
+        else k_implvisc_fic_tile<20><<<g, kIvCols, implvisc_tile_smem(d), s>>>(d);
+        return;
+    }
+    MAXL_DISPATCH(k_implvisc, grid_for(d.E, 128), 128, s, d);
+}
 void launch_jac_swap(const Dev &d, cudaStream_t s) { k_jac_swap<<<grid_for(d.N, 256), 256, 0, s>>>(d); }
 void launch_je(const Dev &d, cudaStream_t s) { k_je_elem<<<grid_for((long long)d.E * d.L, 256), 256, 0, s>>>(d); }
 void launch_update3d(const Dev &d, real Mt_inv, cudaStream_t s) {

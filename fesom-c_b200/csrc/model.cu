@@ -1838,8 +1838,13 @@ const KnobInfo kKnobs[fesomc::kTuneKnobs] = {
     {"columns", "pressure_col,bpg_elem,update3d,wvel", 0},
     {"d3end_arrays", "d3end,d3end_list", 1},
     {"vdiff_form", "vdiff_col", 3},
+    {"implvisc_form", "implvisc", 2},
 };
 int default_columns(int L) { const int b = 1024 / L; return b > 16 ? 16 : b; }
+// knobs that pick a form or a count rather than threads per block
+bool form_knob(int k) {
+    return k == fesomc::TK_COLUMNS || k == fesomc::TK_D3END || k == fesomc::TK_VDIFF || k == fesomc::TK_IMPLVISC;
+}
 void drop_graph(fesomc_model *m);
 int copy_str(const char *src, char *dst, int32_t len) {
     if (!dst) return FESOMC_OK;
@@ -1892,14 +1897,14 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
     lim[fesomc::TK_D3END] = 6;
     lim[fesomc::TK_VDIFF] = 3;
+    lim[fesomc::TK_IMPLVISC] = 2;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         if (values) {
             const int v = m->d.tune[k];
             values[k] = v > 0 ? v : (kKnobs[k].def > 0 ? kKnobs[k].def : default_columns(m->d.L));
         }
         if (limits)
-            limits[k] = (k == fesomc::TK_COLUMNS || k == fesomc::TK_D3END || k == fesomc::TK_VDIFF) ? lim[k]
-                                                                                                : (lim[k] / 32) * 32;
+            limits[k] = form_knob(k) ? lim[k] : (lim[k] / 32) * 32;
     }
     return FESOMC_OK;
 }
@@ -1912,8 +1917,7 @@ int fesomc_gpu_tune_set(fesomc_model *m, const int32_t *values) {
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {
         const int v = values[k];
         if (v < 0 || v > lim[k]) return FESOMC_EINVAL;
-        if (k != fesomc::TK_COLUMNS && k != fesomc::TK_D3END && k != fesomc::TK_VDIFF && v != 0 && (v < 32 || v % 32 != 0))
-            return FESOMC_EINVAL;
+        if (!form_knob(k) && v != 0 && (v < 32 || v % 32 != 0)) return FESOMC_EINVAL;
     }
     drop_graph(m);   // the captured step holds the old launch shapes
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) m->d.tune[k] = m->d32.tune[k] = values[k];

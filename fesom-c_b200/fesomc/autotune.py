@@ -36,7 +36,10 @@ D3END_ARRAYS = (1, 2, 3, 4, 5, 6)
 # staged in shared memory
 VDIFF_FORMS = (1, 2, 3)
 # the knobs that pick a form rather than a block size
-FORMS = {"columns": COLUMNS, "d3end_arrays": D3END_ARRAYS, "vdiff_form": VDIFF_FORMS}
+# momentum_vert_impl_visc_tmp: columns read directly, or tiles of 64 columns
+IMPLVISC_FORMS = (1, 2)
+FORMS = {"columns": COLUMNS, "d3end_arrays": D3END_ARRAYS, "vdiff_form": VDIFF_FORMS,
+         "implvisc_form": IMPLVISC_FORMS}
 SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "launch_shapes_b200.json")
 
 

@@ -62,6 +62,11 @@ FORCING_KIND = {
     "fazt": ("obn", 12), "amp_factor": ("all", 1), "phy_factor": ("all", 1),
 }
 BOUNDARY = -999   # edge_tri / elem_neighbors marker of a missing element
+# halo rings: one internal step of the estuary configuration (10 sub-steps,
+# MUSCL tracers, filter viscosity, wetting / drying) needs 12 for the owned
+# entities to come out exact, 8 is not enough; the default keeps a margin
+# for the options with wider stencils (biharmonic, filter-2x viscosities)
+DEFAULT_HALO = 16
 
 
 def _width(w, L, NS):
@@ -271,7 +276,7 @@ class Decomposition:
     by q, and send[q][r] = the same entities as local indices of q (both in
     ascending global order)."""
 
-    def __init__(self, case, nranks, halo):
+    def __init__(self, case, nranks, halo=DEFAULT_HALO):
         self.case, self.nranks, self.halo = case, nranks, halo
         self.owner = partition(case.mesh, nranks)
         self.parts = [RankPart(case, self.owner, r, halo) for r in range(nranks)]

@@ -417,7 +417,10 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * (11 or 21 levels) in registers at 6 or 8 blocks of 64 columns per SM;
  * "vdiff_form" 1 to 3: the tracers' implicit vertical diffusion with each
  * column read directly by its thread, or on tiles of 128 or 64 (the
- * default) columns staged in shared memory, for 10 or 20 layers); the next step
+ * default) columns staged in shared memory, for 10 or 20 layers;
+ * "implvisc_form" 1 or 2: the implicit vertical viscosity with each element
+ * column read directly, or on tiles of 64 columns staged in shared memory,
+ * the default for the fic variant at 10 or 20 layers); the next step
  * captures its
  * graph again.  The search over the knobs and its cache per mesh size and
  * level count live with the host driver (fesomc/autotune.py).  No

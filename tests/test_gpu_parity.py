@@ -455,14 +455,16 @@ def _estuary21(cases, **kw):
 
 @pytest.mark.parametrize("variant", ["rivers_split_local", "atm_split_shared", "atm_per_node_split",
                                      "reg6_11", "reg8_11_atm", "reg6_21", "reg8_21", "one_kernel_forms_21",
-                                     "tile64_atm_21"])
+                                     "tile64_atm_21", "implvisc_direct_21"])
 def test_two_kernel_forms_bit_exact(mods, variant):
     """The kernel forms beside the defaults against the oracle: d3_end in
     one kernel and as set-up + sweep (sweep arrays in local memory, in
     shared memory, in registers for 11 and 21 levels), the tracers' vertical
     diffusion with directly read columns and on tiles of 128 or 64 columns
-    (10 and 20 layers), with the river salinity source and with atmospheric
-    heat and freshwater sources in the column solve, 20 steps, exact."""
+    (10 and 20 layers), the implicit vertical viscosity with directly read
+    columns (the tiles are the default), with the river salinity source and
+    with atmospheric heat and freshwater sources in the column solve, 20
+    steps, exact."""
     abi, cases, model, pyoracle = mods
     make, shapes = {
         "rivers_split_local": (est(cases, "small"), {"d3end_arrays": 3, "vdiff_form": 2}),
@@ -476,6 +478,7 @@ def test_two_kernel_forms_bit_exact(mods, variant):
         "reg8_21": (_estuary21(cases), {"d3end_arrays": 6}),
         "one_kernel_forms_21": (_estuary21(cases), {"d3end_arrays": 1, "vdiff_form": 1}),
         "tile64_atm_21": (_estuary21(cases, atm=_atm_varied), {"vdiff_form": 3}),
+        "implvisc_direct_21": (_estuary21(cases), {"implvisc_form": 1, "vdiff_form": 2}),
     }[variant]
     bad, eg, eo = run_pair(mods, make, 20, shapes)
     assert bad == []
