@@ -95,6 +95,14 @@ static const double kPi = 3.14159265358979;
 using namespace fesomc;
 using namespace fesomc::f64;
 
+// a halo plan (fesomc_gpu_halo_plan): nodes and elements of one model
+struct fesomc_halo {
+    int n_nodes = 0, n_elems = 0;
+    int *d_nodes = nullptr, *d_elems = nullptr;   // device order
+    long long count = 0;                          // doubles per buffer
+    double *d_range = nullptr;                    // min / max scratch
+};
+
 struct fesomc_model {
     Dev d{};                    // FP64 view: 2D sub-cycle (always) and, in the FP64 form, everything
     fesomc::f32::Dev d32{};     // FP32 form: level fields, geometry and 3D arithmetic in FP32
@@ -246,6 +254,48 @@ __global__ void k_perm_scatter(const T *dev, T *ref, const int *ref_of, long lon
         const long long e = i / lev, k = i % lev;
         ref[(size_t)ref_of[e] * lev + k] = dev[i];
     }
+}
+
+// halo exchange of a decomposed mesh (fesomc_gpu_halo_*)
+template <typename T>
+__global__ void k_halo_gather(const T *src, int width, const int *idx, int n, double *dst) {
+    const long long total = (long long)n * width;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / width, c = i - r * width;
+        dst[i] = (double)src[(size_t)idx[r] * width + c];
+    }
+}
+template <typename T>
+__global__ void k_halo_scatter(T *dst, int width, const int *idx, int n, const double *src) {
+    const long long total = (long long)n * width;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long r = i / width, c = i - r * width;
+        dst[(size_t)idx[r] * width + c] = (T)src[i];
+    }
+}
+// min / max of two fields of width w over the listed entities: one block
+template <typename T>
+__global__ void k_halo_range(const T *a, const T *b, int w, const int *idx, int n, double *out) {
+    __shared__ double s[4][256];
+    double amin = (double)a[(size_t)idx[0] * w], amax = amin, bmin = (double)b[(size_t)idx[0] * w], bmax = bmin;
+    for (long long i = threadIdx.x; i < (long long)n * w; i += blockDim.x) {
+        const size_t g = (size_t)idx[i / w] * w + (size_t)(i % w);
+        const double x = (double)a[g], y = (double)b[g];
+        amin = fmin(amin, x); amax = fmax(amax, x);
+        bmin = fmin(bmin, y); bmax = fmax(bmax, y);
+    }
+    s[0][threadIdx.x] = amin; s[1][threadIdx.x] = amax; s[2][threadIdx.x] = bmin; s[3][threadIdx.x] = bmax;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            s[0][threadIdx.x] = fmin(s[0][threadIdx.x], s[0][threadIdx.x + o]);
+            s[1][threadIdx.x] = fmax(s[1][threadIdx.x], s[1][threadIdx.x + o]);
+            s[2][threadIdx.x] = fmin(s[2][threadIdx.x], s[2][threadIdx.x + o]);
+            s[3][threadIdx.x] = fmax(s[3][threadIdx.x], s[3][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = s[0][0]; out[1] = s[1][0]; out[2] = s[2][0]; out[3] = s[3][0]; }
 }
 
 enum { ENT_NODE = 0, ENT_ELEM = 1 };
@@ -1552,6 +1602,131 @@ int fesomc_gpu_sync_from_host(fesomc_model *m, uint32_t mask, const fesomc_state
         CK(cudaStreamSynchronize(m->stream));
     }
     return FESOMC_OK;
+}
+
+// ---- halo exchange of a decomposed mesh on the device ----------------------
+// A plan holds a list of the model's nodes and elements (device indices);
+// pack gathers every field of the restart set (the field table's order,
+// each entity's values consecutive, FP32 fields widened) for those entities
+// into a device buffer of doubles, unpack scatters such a buffer back.
+int fesomc_gpu_halo_plan(fesomc_model *m, int32_t n_nodes, const int32_t *nodes, int32_t n_elems,
+                         const int32_t *elems, fesomc_halo **out) {
+    if (!m || !out || n_nodes < 0 || n_elems < 0 || (n_nodes && !nodes) || (n_elems && !elems)) return FESOMC_EINVAL;
+    *out = nullptr;
+    const int N = m->d.N, E = m->d.E;
+    // reference -> device index (the storage order's inverse)
+    std::vector<int> nd(N), el(E);
+    if (m->perm) {
+        std::vector<int> nref(N), eref(E);
+        CK(cudaMemcpy(nref.data(), m->d_nd_ref, sizeof(int) * N, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(eref.data(), m->d_el_ref, sizeof(int) * E, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < N; ++i) nd[nref[i]] = i;
+        for (int i = 0; i < E; ++i) el[eref[i]] = i;
+    } else {
+        for (int i = 0; i < N; ++i) nd[i] = i;
+        for (int i = 0; i < E; ++i) el[i] = i;
+    }
+    std::vector<int> hn(n_nodes), he(n_elems);
+    for (int i = 0; i < n_nodes; ++i) {
+        if (nodes[i] < 0 || nodes[i] >= N) return FESOMC_EINVAL;
+        hn[i] = nd[nodes[i]];
+    }
+    for (int i = 0; i < n_elems; ++i) {
+        if (elems[i] < 0 || elems[i] >= E) return FESOMC_EINVAL;
+        he[i] = el[elems[i]];
+    }
+    fesomc_halo *h = new fesomc_halo();
+    h->n_nodes = n_nodes;
+    h->n_elems = n_elems;
+    for (const FieldRef &f : field_table(m))
+        h->count += (long long)(f.ent == ENT_NODE ? n_nodes : n_elems) * (long long)(f.count / ents(m, f.ent));
+    cudaError_t e = cudaMalloc(&h->d_range, 4 * sizeof(double));
+    if (e == cudaSuccess && n_nodes) e = cudaMalloc(&h->d_nodes, sizeof(int) * n_nodes);
+    if (e == cudaSuccess && n_elems) e = cudaMalloc(&h->d_elems, sizeof(int) * n_elems);
+    if (e == cudaSuccess && n_nodes) e = cudaMemcpy(h->d_nodes, hn.data(), sizeof(int) * n_nodes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n_elems) e = cudaMemcpy(h->d_elems, he.data(), sizeof(int) * n_elems, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        fesomc_gpu_halo_free(h);
+        return e == cudaErrorMemoryAllocation ? FESOMC_ENOMEM : FESOMC_ECUDA;
+    }
+    *out = h;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_halo_size(const fesomc_halo *h, int64_t *count) {
+    if (!h || !count) return FESOMC_EINVAL;
+    *count = h->count;
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_halo_pack(fesomc_model *m, const fesomc_halo *h, double *buf) {
+    if (!m || !h || (h->count && !buf)) return FESOMC_EINVAL;
+    long long off = 0;
+    for (const FieldRef &f : field_table(m)) {
+        const int n = f.ent == ENT_NODE ? h->n_nodes : h->n_elems;
+        const int w = (int)(f.count / ents(m, f.ent));
+        const int *idx = f.ent == ENT_NODE ? h->d_nodes : h->d_elems;
+        if (n) {
+            const int g = grid_for((long long)n * w, 256);
+            if (f.f32) k_halo_gather<<<g, 256, 0, m->stream>>>((const float *)f.dev, w, idx, n, buf + off);
+            else k_halo_gather<<<g, 256, 0, m->stream>>>((const double *)f.dev, w, idx, n, buf + off);
+        }
+        off += (long long)n * w;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->stream));
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_halo_unpack(fesomc_model *m, const fesomc_halo *h, const double *buf) {
+    if (!m || !h || (h->count && !buf)) return FESOMC_EINVAL;
+    long long off = 0;
+    for (const FieldRef &f : field_table(m)) {
+        const int n = f.ent == ENT_NODE ? h->n_nodes : h->n_elems;
+        const int w = (int)(f.count / ents(m, f.ent));
+        const int *idx = f.ent == ENT_NODE ? h->d_nodes : h->d_elems;
+        if (n) {
+            const int g = grid_for((long long)n * w, 256);
+            if (f.f32) k_halo_scatter<<<g, 256, 0, m->stream>>>((float *)f.dev, w, idx, n, buf + off);
+            else k_halo_scatter<<<g, 256, 0, m->stream>>>((double *)f.dev, w, idx, n, buf + off);
+        }
+        off += (long long)n * w;
+    }
+    // the jacobian state follows the elevation, as after a full upload: a
+    // running model holds eta_jac = eta_n at every step boundary
+    const size_t N = (size_t)m->d.N;
+    CK(cudaMemcpyAsync(m->d.eta_jac, m->d.eta_n, sizeof(double) * N, cudaMemcpyDeviceToDevice, m->stream));
+    CK(cudaMemcpyAsync(m->d.eta_jac_old, m->d.eta_n, sizeof(double) * N, cudaMemcpyDeviceToDevice, m->stream));
+    if (m->fp32) fesomc::f32::launch_je(m->d32, m->stream);
+    else launch_je(m->d, m->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(m->stream));
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_halo_range(fesomc_model *m, const fesomc_halo *h, double *range) {
+    if (!m || !h || !range || h->n_nodes < 1) return FESOMC_EINVAL;
+    const FieldRef *tf = nullptr, *sf = nullptr;
+    const std::vector<FieldRef> table = field_table(m);
+    for (const FieldRef &f : table) {
+        if (f.host == &fesomc_state::TF) tf = &f;
+        if (f.host == &fesomc_state::SF) sf = &f;
+    }
+    const int w = (int)(tf->count / ents(m, ENT_NODE));
+    if (tf->f32) k_halo_range<<<1, 256, 0, m->stream>>>((const float *)tf->dev, (const float *)sf->dev, w, h->d_nodes, h->n_nodes, h->d_range);
+    else k_halo_range<<<1, 256, 0, m->stream>>>((const double *)tf->dev, (const double *)sf->dev, w, h->d_nodes, h->n_nodes, h->d_range);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(range, h->d_range, 4 * sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return FESOMC_OK;
+}
+
+void fesomc_gpu_halo_free(fesomc_halo *h) {
+    if (!h) return;
+    cudaFree(h->d_nodes);
+    cudaFree(h->d_elems);
+    cudaFree(h->d_range);
+    delete h;
 }
 
 int fesomc_gpu_snapshot_begin(fesomc_model *m, uint32_t mask, fesomc_state *st) {

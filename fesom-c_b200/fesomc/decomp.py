@@ -30,10 +30,14 @@ is taken over every rank's own nodes and given to each rank's model before
 its step (fesomc_gpu_set_tracer_range); the energy diagnostic is summed
 over the ranks' own nodes and elements on the host.
 
-Transports.  `LocalRanks` runs all ranks in one process (one model each,
-on one GPU or several) and exchanges through host arrays; `exchange_dist`
-does the same exchange between processes over torch.distributed (gloo on
-the CPU, or NCCL), one rank per process.
+Transports.  `LocalRanks` runs all ranks in one process (one model each)
+and exchanges the whole state through host arrays; `DeviceRanks` does the
+same with the halos packed and unpacked on the device
+(fesomc_gpu_halo_pack / _unpack); `DistRank` is one rank per process over
+torch.distributed (the tracer range all-reduced, the packed halos sent
+with isend / irecv: device buffers with NCCL, staged through host tensors
+with gloo); `exchange_dist` is the host-array exchange over
+torch.distributed.
 """
 import ctypes as C
 
@@ -410,6 +414,154 @@ class LocalRanks:
         for g in self.models:
             g.close()
         self.models = []
+
+
+def _plan(g, nodes, elems):
+    n = np.ascontiguousarray(nodes, dtype=np.int32)
+    e = np.ascontiguousarray(elems, dtype=np.int32)
+    h = C.c_void_p()
+    abi.check(g.lib.fesomc_gpu_halo_plan(g.h, len(n), abi.iptr(n), len(e), abi.iptr(e), C.byref(h)),
+              "fesomc_gpu_halo_plan")
+    c = C.c_int64()
+    abi.check(g.lib.fesomc_gpu_halo_size(h, C.byref(c)), "fesomc_gpu_halo_size")
+    return h, int(c.value)
+
+
+class RankPlans:
+    """Device halo plans of rank r's model g: for every peer q the entities
+    it sends (send[q]) and receives (recv[q]), as (plan, doubles), and its
+    own nodes (own), whose tracer range it contributes."""
+
+    def __init__(self, dec, r, g):
+        self.g, self.send, self.recv = g, {}, {}
+        for q in range(dec.nranks):
+            if q != r:
+                self.send[q] = _plan(g, *dec.send[r][q])
+                self.recv[q] = _plan(g, *dec.recv[r][q])
+        self.own = _plan(g, np.nonzero(dec.parts[r].own_nodes)[0], np.zeros(0, dtype=np.int32))
+
+    def range(self):
+        out = np.zeros(4)
+        abi.check(self.g.lib.fesomc_gpu_halo_range(self.g.h, self.own[0], abi.dptr(out)), "fesomc_gpu_halo_range")
+        return out
+
+    def pack(self, q, ptr):
+        abi.check(self.g.lib.fesomc_gpu_halo_pack(self.g.h, self.send[q][0], C.c_void_p(ptr)), "fesomc_gpu_halo_pack")
+
+    def unpack(self, q, ptr):
+        abi.check(self.g.lib.fesomc_gpu_halo_unpack(self.g.h, self.recv[q][0], C.c_void_p(ptr)),
+                  "fesomc_gpu_halo_unpack")
+
+    def close(self):
+        for h, _ in list(self.send.values()) + list(self.recv.values()) + [self.own]:
+            self.g.lib.fesomc_gpu_halo_free(h)
+        self.send, self.recv = {}, {}
+
+
+def _set_range(g, rng):
+    arr = np.ascontiguousarray(rng, dtype=np.float64)
+    abi.check(g.lib.fesomc_gpu_set_tracer_range(g.h, abi.dptr(arr)), "fesomc_gpu_set_tracer_range")
+
+
+class DeviceRanks:
+    """All ranks in this process on the current GPU, the halos packed and
+    unpacked on the device (fesomc_gpu_halo_*) through device buffers, the
+    tracer range combined from the ranks' own nodes."""
+
+    def __init__(self, decomp):
+        import torch
+        self.dec = decomp
+        self.models = [model.GpuModel(p.case) for p in decomp.parts]
+        self.plans = [RankPlans(decomp, r, g) for r, g in enumerate(self.models)]
+        n = max([c for pl in self.plans for _, c in pl.send.values()] + [1])
+        self.buf = torch.empty(n, dtype=torch.float64, device="cuda")
+
+    def step(self, nsteps=1):
+        dec = self.dec
+        for _ in range(nsteps):
+            rng = combine_ranges([pl.range() for pl in self.plans])
+            for g in self.models:
+                _set_range(g, rng)
+                g.step(1)
+            for r in range(dec.nranks):
+                for q in range(dec.nranks):
+                    if q != r:
+                        self.plans[r].pack(q, self.buf.data_ptr())
+                        self.plans[q].unpack(r, self.buf.data_ptr())
+
+    def assemble(self):
+        return self.dec.assemble([g.state() for g in self.models])
+
+    def close(self):
+        for pl in self.plans:
+            pl.close()
+        for g in self.models:
+            g.close()
+        self.models, self.plans = [], []
+
+
+class DistRank:
+    """This process's rank of a decomposition over torch.distributed (`dist`,
+    initialised; world size = ranks): its model on the current GPU, the
+    tracer range all-reduced, the packed halos exchanged with isend / irecv
+    after every step (device buffers with NCCL; staged through host tensors
+    with gloo).  Every rank builds the same decomposition."""
+
+    def __init__(self, case, dist, halo=DEFAULT_HALO):
+        import torch
+        self.dist = dist
+        self.rank, world = dist.get_rank(), dist.get_world_size()
+        self.dec = Decomposition(case, world, halo)
+        self.g = model.GpuModel(self.dec.parts[self.rank].case)
+        self.plans = RankPlans(self.dec, self.rank, self.g)
+        self.nccl = dist.get_backend() == "nccl"
+        dev = "cuda" if self.nccl else "cpu"
+        self.sbuf = {q: torch.empty(c, dtype=torch.float64, device="cuda") for q, (_, c) in self.plans.send.items()}
+        self.rbuf = {q: torch.empty(c, dtype=torch.float64, device="cuda") for q, (_, c) in self.plans.recv.items()}
+        self.shost = {q: torch.empty(c, dtype=torch.float64, device=dev) for q, (_, c) in self.plans.send.items()}
+        self.rhost = {q: torch.empty(c, dtype=torch.float64, device=dev) for q, (_, c) in self.plans.recv.items()}
+
+    def step(self, nsteps=1):
+        import torch
+        dist = self.dist
+        dev = "cuda" if self.nccl else "cpu"
+        for _ in range(nsteps):
+            r = self.plans.range()
+            lo = torch.tensor([r[0], r[2]], dtype=torch.float64, device=dev)
+            hi = torch.tensor([r[1], r[3]], dtype=torch.float64, device=dev)
+            dist.all_reduce(lo, op=dist.ReduceOp.MIN)
+            dist.all_reduce(hi, op=dist.ReduceOp.MAX)
+            _set_range(self.g, [lo[0].item(), hi[0].item(), lo[1].item(), hi[1].item()])
+            self.g.step(1)
+            for q in self.sbuf:
+                self.plans.pack(q, self.sbuf[q].data_ptr())
+                if not self.nccl:
+                    self.shost[q].copy_(self.sbuf[q])
+            src = self.sbuf if self.nccl else self.shost
+            dst = self.rbuf if self.nccl else self.rhost
+            if self.nccl:   # one group: the sends and receives of every peer together
+                ops = [dist.P2POp(dist.isend, src[q], q) for q in sorted(src)]
+                ops += [dist.P2POp(dist.irecv, dst[q], q) for q in sorted(dst)]
+                reqs = dist.batch_isend_irecv(ops) if ops else []
+            else:
+                reqs = [dist.isend(src[q], q) for q in sorted(src)] + [dist.irecv(dst[q], q) for q in sorted(dst)]
+            for rq in reqs:
+                rq.wait()
+            if self.nccl:
+                torch.cuda.synchronize()
+            for q in self.rbuf:
+                if not self.nccl:
+                    self.rbuf[q].copy_(self.rhost[q])
+                    torch.cuda.synchronize()
+                self.plans.unpack(q, self.rbuf[q].data_ptr())
+
+    def own_state(self):
+        """This rank's state (its sub-mesh) for assembling on one rank."""
+        return self.g.state()
+
+    def close(self):
+        self.plans.close()
+        self.g.close()
 
 
 def exchange_dist(decomp, rank, state, dist):

@@ -317,6 +317,26 @@ int  fesomc_gpu_energy(fesomc_model *m, double *eout);
  * FESOMC_EINVAL for packed members or a range with min > max or NaN.  No
  * counterpart in the reference (one MPI reduction there). */
 int  fesomc_gpu_set_tracer_range(fesomc_model *m, const double *range);
+/* Halo exchange of a decomposed mesh on the device (the packed form of
+ * exchange_nod / exchange_elem, src/gen_halo_exchange_c.F90:130-165,663-793,
+ * for every field of the restart set at once).  A plan lists nodes and
+ * elements of this model (0-based, reference numbering, host arrays);
+ * _size gives the doubles of its buffer; _pack gathers the state of the
+ * listed entities (the fesomc_state fields in declaration order, each
+ * entity's values consecutive, FP32 fields widened) into a device buffer,
+ * _unpack writes such a buffer back (and, as a full upload does, the
+ * jacobian state from the elevation); both return when the device is done.
+ * _range gives {Tmin, Tmax, Smin, Smax} over the plan's nodes (a rank's own
+ * nodes: its part of the range fesomc_gpu_set_tracer_range takes).  Plans
+ * belong to the model they were made for; free them before it. */
+typedef struct fesomc_halo fesomc_halo;
+int  fesomc_gpu_halo_plan(fesomc_model *m, int32_t n_nodes, const int32_t *nodes, int32_t n_elems,
+                          const int32_t *elems, fesomc_halo **plan);
+int  fesomc_gpu_halo_size(const fesomc_halo *plan, int64_t *count);
+int  fesomc_gpu_halo_pack(fesomc_model *m, const fesomc_halo *plan, double *dev_buf);
+int  fesomc_gpu_halo_unpack(fesomc_model *m, const fesomc_halo *plan, const double *dev_buf);
+int  fesomc_gpu_halo_range(fesomc_model *m, const fesomc_halo *plan, double *range);
+void fesomc_gpu_halo_free(fesomc_halo *plan);
 int  fesomc_gpu_last_status(fesomc_model *m, uint32_t *status, int32_t *notconv_columns);
 int  fesomc_gpu_finalize(fesomc_model *m);
 const char *fesomc_gpu_error_string(int code);

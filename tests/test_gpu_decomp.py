@@ -115,3 +115,63 @@ def test_tracer_range_is_checked(built):
             ref.close()
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_device_halo_exchange_gives_the_same_bits(built, fp32):
+    """The halos packed and unpacked on the device (fesomc_gpu_halo_*), the
+    tracer range from the device: the bits of the whole-mesh run."""
+    from fesomc import decomp
+    steps = 8
+    case = _case(fp32)
+    ref, _ = _whole(case, steps)
+    dr = decomp.DeviceRanks(decomp.Decomposition(case, 3, HALO))
+    try:
+        dr.step(steps)
+        got = dr.assemble()
+    finally:
+        dr.close()
+    for k, v in got.items():
+        assert np.array_equal(v, ref[k]), (k, int(np.sum(v != ref[k])))
+
+
+def _dist_rank(rank, world, port, path, steps):
+    import os
+    import torch.distributed as dist
+    from fesomc import decomp
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        r = decomp.DistRank(_case(0), dist, HALO)
+        try:
+            r.step(steps)
+            st = r.own_state()
+            np.savez(os.path.join(path, "r%d.npz" % rank), **{k: v for k, v in st.items() if not k.startswith("_")})
+        finally:
+            r.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_one_rank_per_process(built, tmp_path):
+    """Two processes (gloo between them; both on this one GPU, no kernel of
+    one waits on the other), each a rank with its own model: the assembled
+    owned state equals the whole-mesh run."""
+    import socket
+    import torch.multiprocessing as mp
+    from fesomc import decomp
+    steps = 6
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    mp.start_processes(_dist_rank, args=(2, port, str(tmp_path), steps), nprocs=2, join=True, start_method="spawn")
+    case = _case(0)
+    d = decomp.Decomposition(case, 2, HALO)
+    states = [dict(np.load(tmp_path / ("r%d.npz" % r))) for r in range(2)]
+    got = d.assemble(states)
+    ref, _ = _whole(case, steps)
+    for k, v in got.items():
+        assert np.array_equal(v, ref[k]), (k, int(np.sum(v != ref[k])))
+
