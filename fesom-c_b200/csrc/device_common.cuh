@@ -79,7 +79,7 @@ __host__ __device__ __forceinline__ float4 make_real4(float x, float y, float z,
 // and the form of d3_end (1 column arrays in local memory, 2 in shared
 // memory, 3 a level-parallel set-up kernel and a sweep kernel, 4 the same
 // with the sweep's arrays in shared memory, 5 and 6 in registers for 11 or
-// 21 levels, 7 as 3 at 16 blocks per SM), and the form of the tracers'
+// 21 levels), and the form of the tracers'
 // implicit vertical diffusion (1 one thread per column reading the fields
 // directly, 2 and 3 tiles of 128 or 64 columns staged in shared memory, for
 // 10 or 20 layers; other layer counts take form 1), and the form of the

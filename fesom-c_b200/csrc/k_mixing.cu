@@ -465,11 +465,8 @@ __global__ void __launch_bounds__(kD3SetupThreads) k_d3end_setup(Dev d) {
 
 // The sweeps of d3_end per node column, from the set-up's level-major
 // constants; the same arithmetic as k_d3end, in the same order.
-// k_d3end_sweep16 asks for 16 resident blocks of 64 columns per SM (64
-// registers, a few values spilled: "d3end_arrays" 7), k_d3end_sweep leaves
-// the count to the compiler (11 blocks of 90 registers).
 template <int ARR, bool kList>
-__device__ __forceinline__ void d3end_sweep_body(const Dev &d, const int *list, const unsigned long long *count) {
+__global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *count) {
     const real t_inv = real(1.0) / d.dt;
     const real cka = d.cka;
     const real B1cka2 = real(16.6) * (cka * cka);
@@ -581,15 +578,6 @@ __device__ __forceinline__ void d3end_sweep_body(const Dev &d, const int *list, 
             Kvw[nz - 1] = d.Pr_num * s;
         }
     }
-}
-
-template <int ARR, bool kList>
-__global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *count) {
-    d3end_sweep_body<ARR, kList>(d, list, count);
-}
-template <int ARR>
-__global__ void __launch_bounds__(64, 16) k_d3end_sweep16(Dev d) {
-    d3end_sweep_body<ARR, false>(d, nullptr, nullptr);
 }
 
 // The sweeps with xx1, yy1 and the btr pair in shared memory, [array][level]
@@ -880,9 +868,7 @@ static size_t d3end_setup_smem(const Dev &d) { return ((size_t)8 * kD3Tile * d.N
 static bool d3end_split(const Dev &d) { return d.tune[TK_D3END] >= 3 && d.NS <= 40; }
 // the register sweep is compiled for these level counts; others take the
 // local-memory sweep
-static bool d3end_reg(const Dev &d) {
-    return (d.tune[TK_D3END] == 5 || d.tune[TK_D3END] == 6) && (d.NS == 11 || d.NS == 21);
-}
+static bool d3end_reg(const Dev &d) { return d.tune[TK_D3END] >= 5 && (d.NS == 11 || d.NS == 21); }
 static size_t d3end_sweep_smem(const Dev &d) { return (size_t)(4 * d.NS - 2) * kD3Block * sizeof(real); }
 int config_d3end(const Dev &d) {
     if (d.NS > 127) return 1;
@@ -903,10 +889,6 @@ static void launch_d3end_split(const Dev &d, cudaStream_t s) {
         else k_d3end_sweep_reg<21, 6><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     }
     else if (d.tune[TK_D3END] == 4) k_d3end_sweep_sm<<<grid_for(d.N, kD3Block), kD3Block, d3end_sweep_smem(d), s>>>(d);
-    else if (d.tune[TK_D3END] == 7 && d.NS <= 11)
-        k_d3end_sweep16<12><<<grid_for(d.N, 64), 64, 0, s>>>(d);
-    else if (d.tune[TK_D3END] == 7 && d.NS <= 21)
-        k_d3end_sweep16<22><<<grid_for(d.N, 64), 64, 0, s>>>(d);
     else if (d.NS <= 11) k_d3end_sweep<12, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else if (d.NS <= 21) k_d3end_sweep<22, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);
     else k_d3end_sweep<41, false><<<grid_for(d.N, 64), 64, 0, s>>>(d, nullptr, nullptr);

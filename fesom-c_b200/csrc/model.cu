@@ -2070,7 +2070,7 @@ int fesomc_gpu_tune_get(fesomc_model *m, int32_t *values, int32_t *limits) {
     fesomc::f32::tune_limits_baroclinic(lim); fesomc::f32::tune_limits_barotropic(lim);
     fesomc::f32::tune_limits_tracer(lim); fesomc::f32::tune_limits_mixing(lim);
     lim[fesomc::TK_COLUMNS] = 1024 / m->d.L < 32 ? 1024 / m->d.L : 32;
-    lim[fesomc::TK_D3END] = 7;
+    lim[fesomc::TK_D3END] = 6;
     lim[fesomc::TK_VDIFF] = 3;
     lim[fesomc::TK_IMPLVISC] = 2;
     for (int k = 0; k < fesomc::kTuneKnobs; ++k) {

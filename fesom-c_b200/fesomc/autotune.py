@@ -30,8 +30,8 @@ THREADS = (64, 128, 256, 512, 1024)
 COLUMNS = (1, 2, 4, 8, 16, 32)
 # d3_end: local-memory arrays, shared-memory arrays, set-up and sweep kernels
 # (the sweep's arrays in local memory, in shared memory, or in registers at
-# 6 or 8 resident blocks per SM, or in local memory at 16 blocks per SM)
-D3END_ARRAYS = (1, 2, 3, 4, 5, 6, 7)
+# 6 or 8 resident blocks per SM)
+D3END_ARRAYS = (1, 2, 3, 4, 5, 6)
 # tracer_impl_vert_diff: columns read directly, or tiles of 128 or 64 columns
 # staged in shared memory
 VDIFF_FORMS = (1, 2, 3)

@@ -431,11 +431,10 @@ int  fesomc_ensemble_run(fesomc_model *const *members, int32_t n_members, int32_
  * largest each knob accepts on this device), either may be NULL.
  * fesomc_gpu_tune_set takes one value per knob (0 = the default) and
  * returns FESOMC_EINVAL, changing nothing, when a thread count is not a
- * multiple of 32 or a value exceeds its limit ("d3end_arrays" takes 1 to 7:
+ * multiple of 32 or a value exceeds its limit ("d3end_arrays" takes 1 to 6:
  * d3_end's column arrays in local or in shared memory, or a set-up and a
  * sweep kernel with the sweep's arrays in local memory, in shared memory, or
- * (11 or 21 levels) in registers at 6 or 8 blocks of 64 columns per SM,
- * or (7) in local memory at 16 blocks per SM;
+ * (11 or 21 levels) in registers at 6 or 8 blocks of 64 columns per SM;
  * "vdiff_form" 1 to 3: the tracers' implicit vertical diffusion with each
  * column read directly by its thread, or on tiles of 128 or 64 (the
  * default) columns staged in shared memory, for 10 or 20 layers;

@@ -455,7 +455,7 @@ def _estuary21(cases, **kw):
 
 @pytest.mark.parametrize("variant", ["rivers_split_local", "atm_split_shared", "atm_per_node_split",
                                      "reg6_11", "reg8_11_atm", "reg6_21", "reg8_21", "one_kernel_forms_21",
-                                     "tile64_atm_21", "implvisc_direct_21", "sweep16_21"])
+                                     "tile64_atm_21", "implvisc_direct_21"])
 def test_two_kernel_forms_bit_exact(mods, variant):
     """The kernel forms beside the defaults against the oracle: d3_end in
     one kernel and as set-up + sweep (sweep arrays in local memory, in
@@ -479,7 +479,6 @@ def test_two_kernel_forms_bit_exact(mods, variant):
         "one_kernel_forms_21": (_estuary21(cases), {"d3end_arrays": 1, "vdiff_form": 1}),
         "tile64_atm_21": (_estuary21(cases, atm=_atm_varied), {"vdiff_form": 3}),
         "implvisc_direct_21": (_estuary21(cases), {"implvisc_form": 1, "vdiff_form": 2}),
-        "sweep16_21": (_estuary21(cases), {"d3end_arrays": 7}),
     }[variant]
     bad, eg, eo = run_pair(mods, make, 20, shapes)
     assert bad == []
