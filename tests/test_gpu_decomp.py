@@ -117,13 +117,16 @@ def test_tracer_range_is_checked(built):
         g.close()
 
 
-@pytest.mark.parametrize("fp32", [0, 1])
-def test_device_halo_exchange_gives_the_same_bits(built, fp32):
+@pytest.mark.parametrize("fp32,sfc", [(0, 0), (1, 0), (0, 1)])
+def test_device_halo_exchange_gives_the_same_bits(built, fp32, sfc):
     """The halos packed and unpacked on the device (fesomc_gpu_halo_*), the
-    tracer range from the device: the bits of the whole-mesh run."""
+    tracer range from the device: the bits of the whole-mesh run, also with
+    every model storing its sub-mesh along the Hilbert curve (the plans'
+    indices mapped to the storage order)."""
     from fesomc import decomp
     steps = 8
     case = _case(fp32)
+    case.params.sfc_order = sfc
     ref, _ = _whole(case, steps)
     dr = decomp.DeviceRanks(decomp.Decomposition(case, 3, HALO))
     try:
