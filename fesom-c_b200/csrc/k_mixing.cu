@@ -377,13 +377,11 @@ __global__ void __launch_bounds__(kD3Block, 6) k_d3end_sm(Dev d, const int *list
 // set-up kernel takes blocks of kD3Tile consecutive nodes, stages their
 // columns in shared memory with coalesced loads, forms the constants with
 // one thread per (node, interface) exactly as k_d3end's first loop does, and
-// writes -b1-b2, t_inv*bt, c2, snu and the sweep's coefficients am, cm
-// (which do not change from one sweep to the next) level-major
-// ([interface][node]: a warp of 32 consecutive nodes reads 256 contiguous
-// bytes of one interface) and Ri in the column layout.  The sweep kernel
-// then keeps only xx1, yy1 and the btr pair in local memory (4 arrays
-// instead of 8) and reads the constants level-major, two divisions per
-// level and sweep fewer than k_d3end.
+// writes -b1-b2, t_inv*bt, c2 and snu level-major ([interface][node]: a warp
+// of 32 consecutive nodes reads 256 contiguous bytes of one interface) and
+// Ri in the column layout.  The sweep kernel then keeps only xx1, yy1 and
+// the btr pair in local memory (4 arrays instead of 8: the working set of
+// the resident columns fits in L2) and reads the constants level-major.
 constexpr int kD3Tile = 32;
 constexpr int kD3SetupThreads = 256;
 
@@ -458,9 +456,6 @@ __global__ void __launch_bounds__(kD3SetupThreads) k_d3end_setup(Dev d) {
             else sR[j * NS + nz - 1] = real(10000.0);
             d.d3_pb[o] = -b1 - b2;
             d.d3_qb[o] = t_inv * bt[nz - 1];
-            // the sweep's am and cm (the same for every sweep of the column)
-            d.d3_am[o] = real(0.5) * (snu_p * real(0.73)) / (dmean2 * d1 * dd);
-            d.d3_cm[o] = real(0.5) * (snu_m * real(0.73)) / (dmean2 * d2 * dd);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < nt * NS; i += blockDim.x) d.Ri[(size_t)n0 * NS + i] = sR[i];
@@ -489,8 +484,6 @@ __global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *
         auto QB = [&](int nz) { return d.d3_qb[(size_t)(nz - 2) * N + node]; };
         auto C2 = [&](int nz) { return d.d3_c2[(size_t)(nz - 2) * N + node]; };
         auto SN = [&](int nz) { return d.d3_sn[(size_t)(nz - 1) * N + node]; };
-        auto AM = [&](int nz) { return d.d3_am[(size_t)(nz - 2) * N + node]; };
-        auto CM = [&](int nz) { return d.d3_cm[(size_t)(nz - 2) * N + node]; };
         real xx1[ARR], yy1[ARR], bA[ARR], bB[ARR];
         const real dmean = dmax<real>(d.Dmin, d.depth[node] + d.eta_n[node]);
         const real dmean2 = dmean * dmean;
@@ -516,18 +509,25 @@ __global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *
         int iters = 200;
         for (int it = 1; it <= 200; ++it) {
             real x = real(1.0), y = y2;
-            real s_mid = SN(2);
-            real b_n = btr[2], pb_n = PB(2), qb_n = QB(2), c2_n = C2(2), am_n = AM(2), cm_n = CM(2);
+            real s_lo = SN(1), s_mid = SN(2);
+            real b_n = btr[2], pb_n = PB(2), qb_n = QB(2), c2_n = C2(2), sh_n = SN(3);
             for (int nz = 2; nz <= NS - 1; ++nz) {
-                const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n, am = am_n, cm = cm_n;
-                real s_next = real(0.0);
+                const real s_hi = sh_n;
+                const real b = b_n, pbv = pb_n, qbv = qb_n, c2v = c2_n;
                 if (nz + 1 <= NS - 1) {
-                    b_n = btr[nz + 1]; pb_n = PB(nz + 1); qb_n = QB(nz + 1); c2_n = C2(nz + 1);
-                    am_n = AM(nz + 1); cm_n = CM(nz + 1); s_next = SN(nz + 1);
+                    b_n = btr[nz + 1]; pb_n = PB(nz + 1); qb_n = QB(nz + 1); c2_n = C2(nz + 1); sh_n = SN(nz + 2);
                 }
+                const real s_m = __ldg(d.sig + nz - 2), s_0 = __ldg(d.sig + nz - 1), s_p = __ldg(d.sig + nz);
+                const real dd1 = s_m - s_0;
+                const real dd2 = s_0 - s_p;
+                const real dd = real(0.5) * (dd1 + dd2);
                 const real c1 = real(0.046) * (b * b) / s_mid;
                 if (it == 200) tke[nz - 1] = c1;
                 const real fr = pbv - c1 - qbv - c2v;
+                const real snu_p = real(0.5) * (s_lo + s_mid);
+                const real snu_mm = real(0.5) * (s_mid + s_hi);
+                const real am = real(0.5) * (snu_p * real(0.73)) / (dmean2 * dd1 * dd);
+                const real cm = real(0.5) * (snu_mm * real(0.73)) / (dmean2 * dd2 * dd);
                 const real bm = am + cm + (real(2.0) * real(0.046) * b) / s_mid + t_inv;
                 const real a = bm - am * x;
                 const real xn = cm / a;
@@ -536,7 +536,8 @@ __global__ void k_d3end_sweep(Dev d, const int *list, const unsigned long long *
                 yy1[nz + 1] = yn;
                 x = xn;
                 y = yn;
-                s_mid = s_next;
+                s_lo = s_mid;
+                s_mid = s_hi;
             }
             real b1v = bot;  // btr1(NS)
             btr1[NS] = b1v;

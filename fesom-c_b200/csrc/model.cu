@@ -790,7 +790,7 @@ int alloc_3d(fesomc_model *m, D &d) {
     decltype(&d.U_n) nsn[] = {&d.hpressure, &d.bt, &d.snu, &d.Kv, &d.Ri, &d.tke_dissip, &d.Wvel};
     for (auto p : nsn) if ((rc = dalloc(m, p, NS * N))) return rc;
     if (m->p.ver_mix == 3) {
-        decltype(&d.U_n) d3s[] = {&d.d3_pb, &d.d3_qb, &d.d3_c2, &d.d3_sn, &d.d3_am, &d.d3_cm};
+        decltype(&d.U_n) d3s[] = {&d.d3_pb, &d.d3_qb, &d.d3_c2, &d.d3_sn};
         for (auto p : d3s) if ((rc = dalloc(m, p, NS * N))) return rc;
     }
     if ((rc = dalloc(m, &d.Av, NS * E))) return rc;
