@@ -92,6 +92,18 @@ enum TuneKnob : int {
     TK_UPWIND, TK_AV, TK_COLUMNS, TK_D3END, TK_VDIFF, TK_IMPLVISC, kTuneKnobs
 };
 
+// sbc_do on the device (fesomc_gpu_set_atm_fields): the time-interpolation
+// coefficients of the 8 atmospheric fields per node (device order, 8
+// consecutive values per node), the device clock, a scratch for the stress
+// per node (2 values per node), and the namelist's nm_net_flux and
+// nm_prec_coef
+struct AtmDev {
+    const double *coef_a, *coef_b, *clock;
+    double *tau_node;
+    int net_flux;
+    double prec_coef;
+};
+
 namespace f64 {
 using real = double;
 using real2 = double2;

@@ -15,6 +15,7 @@
 //                 compensated deterministic two-pass reduction
 #include "device_common.cuh"
 #include "fesomc_exp.h"
+#include "fesomc_atan.h"
 
 FESOMC_PREC_BEGIN
 
@@ -1056,6 +1057,146 @@ void launch_minmax(const Dev &d, cudaStream_t s) {
     k_minmax_part<<<dim3(parts, d.n_members), kRedBlock, 0, s>>>(d);
     k_minmax_final<<<d.n_members, 32, 0, s>>>(d, parts);
 }
+// ---- sbc_do on the device: bulk surface fluxes ------------------------------
+// psi_h / psi_m of Large & Yeager (2004), eq. 8c-8e (fv_sbc.F90:620-662);
+// SIGN(0.5, x) is copysign.  FP64 throughout.
+__device__ __forceinline__ double sbc_psi_h(double zta) {
+    double X2 = sqrt(fabs(1.0 - 16.0 * zta));
+    X2 = fmax(X2, 1.0);
+    const double stabit = 0.5 + copysign(0.5, zta);
+    return -5.0 * zta * stabit + (1.0 - stabit) * (2.0 * fesomc_log((1.0 + X2) / 2.0));
+}
+__device__ __forceinline__ double sbc_psi_m(double zta) {
+    double X2 = sqrt(fabs(1.0 - 16.0 * zta));
+    X2 = fmax(X2, 1.0);
+    const double X = sqrt(X2);
+    const double stabit = 0.5 + copysign(0.5, zta);
+    const double pi = 3.141592653589793;
+    return -5.0 * zta * stabit + (1.0 - stabit) * (2.0 * fesomc_log((1.0 + X) / 2.0) + fesomc_log((1.0 + X2) / 2.0) -
+                                                    2.0 * fesomc_atan(X) + pi / 2.0);
+}
+
+// core_coeff_2z (fv_sbc.F90:484-641): transfer coefficients for momentum,
+// sensible and latent heat, and the air temperature and humidity shifted
+// from zt to zu, in 5 iterations on the Monin-Obukhov length
+__device__ void sbc_core_coeff_2z(double zt, double zu, double sst, double T_zt, double q_sat, double q_zt, double dU,
+                                  double &Cd, double &Ch, double &Ce, double &T_zu, double &q_zu) {
+    const double grav = 9.8, kappa = 0.4;
+    const double dU10 = fmax(0.5, dU);
+    double dT = T_zt - sst;
+    double dq = q_zt - q_sat;
+    double stab = 0.5 + copysign(0.5, dT);
+    double Cd_n10 = 1E-3 * (2.7 / dU10 + 0.142 + dU10 / 13.09);
+    double sqrt_Cd_n10 = sqrt(Cd_n10);
+    double Ce_n10 = 1E-3 * (34.6 * sqrt_Cd_n10);
+    double Ch_n10 = 1E-3 * sqrt_Cd_n10 * (18.0 * stab + 32.7 * (1.0 - stab));
+    Cd = Cd_n10;
+    Ce = Ce_n10;
+    Ch = Ch_n10;
+    double sqrt_Cd = sqrt(Cd);
+    T_zu = T_zt;
+    q_zu = q_zt;
+    const double log_zt_zu = fesomc_log(zt / zu), log_zu_10 = fesomc_log(zu / 10.0);
+    for (int j_itt = 1; j_itt <= 5; ++j_itt) {
+        dT = T_zu - sst;
+        dq = q_zu - q_sat;
+        const double T_vpot = T_zu * (1.0 + 0.608 * q_zu);
+        const double U_star = sqrt_Cd * dU10;
+        const double T_star = Ch / sqrt_Cd * dT;
+        const double q_star = Ce / sqrt_Cd * dq;
+        const double L = (U_star * U_star) / (kappa * grav / T_vpot * (T_star * (1.0 + 0.608 * q_zu) + 0.608 * T_zu * q_star));
+        double zeta_u = zu / L;
+        zeta_u = copysign(fmin(fabs(zeta_u), 10.0), zeta_u);
+        double zeta_t = zt / L;
+        zeta_t = copysign(fmin(fabs(zeta_t), 10.0), zeta_t);
+        const double zpsi_hu = sbc_psi_h(zeta_u);
+        const double zpsi_ht = sbc_psi_h(zeta_t);
+        const double zpsi_m = sbc_psi_m(zeta_u);
+        const double U_n10 = fmax(0.25, dU10 / (1.0 + sqrt_Cd_n10 / kappa * (log_zu_10 - zpsi_m)));
+        T_zu = T_zt - T_star / kappa * (log_zt_zu + zpsi_hu - zpsi_ht);
+        q_zu = q_zt - q_star / kappa * (log_zt_zu + zpsi_hu - zpsi_ht);
+        stab = 0.5 + copysign(0.5, q_zu);
+        q_zu = stab * q_zu;
+        Cd_n10 = 1E-3 * (2.7 / U_n10 + 0.142 + U_n10 / 13.09);
+        sqrt_Cd_n10 = sqrt(Cd_n10);
+        Ce_n10 = 1E-3 * (34.6 * sqrt_Cd_n10);
+        stab = 0.5 + copysign(0.5, zeta_u);
+        Ch_n10 = 1E-3 * sqrt_Cd_n10 * (18.0 * stab + 32.7 * (1.0 - stab));
+        double xct = 1.0 + sqrt_Cd_n10 / kappa * (log_zu_10 - zpsi_m);
+        Cd = Cd_n10 / (xct * xct);
+        sqrt_Cd = sqrt(Cd);
+        const double xlogt = log_zu_10 - zpsi_hu;
+        xct = 1.0 + Ch_n10 * xlogt / kappa / sqrt_Cd_n10;
+        Ch = Ch_n10 * sqrt_Cd / sqrt_Cd_n10 / xct;
+        xct = 1.0 + Ce_n10 * xlogt / kappa / sqrt_Cd_n10;
+        Ce = Ce_n10 * sqrt_Cd / sqrt_Cd_n10 / xct;
+    }
+}
+
+// data_timeinterp + apply_atm_fluxes (fv_sbc.F90:838-868, 368-482) per node,
+// type_task 3 without sea ice: the fields at the step's time, the winds,
+// the heat and freshwater fluxes, the stress per node.  The relative wind
+// subtracts the surface Unode / Vnode of the previous step, the surface
+// temperature is TF's top layer.  rhoa, albo, emiss_wat are REAL(4).
+__global__ void k_atm_nodes(Dev d, AtmDev a) {
+    const double now_date = a.clock[0];
+    const double rhoa = (double)1.3f, cpa = 1005.0, Lv = 2.5e6, Stef = 5.67e-8, albo = (double)0.1f,
+                 emiss_wat = (double)0.97f;
+    const int L = d.L;
+    GRID_LOOP(ii, d.N) {
+        const int i = (int)ii;
+        const double *ca = a.coef_a + (size_t)i * 8, *cb = a.coef_b + (size_t)i * 8;
+        double atm[8];
+#pragma unroll
+        for (int f = 0; f < 8; ++f) atm[f] = now_date * ca[f] + cb[f];
+        d.windx[i] = (real)atm[0];
+        d.windy[i] = (real)atm[1];
+        const double wdx = atm[0] - (double)d.Unode[(size_t)i * L];
+        const double wdy = atm[1] - (double)d.Vnode[(size_t)i * L];
+        const double wndm = sqrt(wdx * wdx + wdy * wdy);
+        const double tf0 = (double)d.TF[(size_t)i * L];
+        const double zst = tf0 + 273.15;
+        const double q_sat = 0.98 * 640380.0 / rhoa * fesomc_exp(-5107.4 / zst);
+        double Cd, Ch, Ce, t_zu, q_zu;
+        sbc_core_coeff_2z(2.0, 10.0, zst, atm[5], q_sat, atm[2], wndm, Cd, Ch, Ce, t_zu, q_zu);
+        const double rtmp = rhoa * wndm * Cd;
+        a.tau_node[2 * (size_t)i] = rtmp * wdx;
+        a.tau_node[2 * (size_t)i + 1] = rtmp * wdy;
+        const double zevap = fmax(0.0, rhoa * Ce * (q_sat - q_zu) * wndm);
+        const double zqsb = rhoa * cpa * Ch * (zst - t_zu) * wndm;
+        const double zqlw = a.net_flux == 0 ? atm[4] - emiss_wat * Stef * zst * zst * zst * zst : atm[4];
+        const double zqla = Lv * zevap;
+        double qns = zqlw - zqsb - zqla;
+        if (tf0 < -2.0 && qns < 0.0) qns = 0.0;
+        d.qns[i] = qns;
+        d.emp[i] = zevap - atm[6] / a.prec_coef;
+        d.qsr[i] = (1.0 - albo) * atm[3];
+        d.mslp[i] = atm[7];
+    }
+}
+// the stress per element: sum(w_cv * taux_node(elem2D_nodes)) in node order
+__global__ void k_atm_stress(Dev d, AtmDev a) {
+    GRID_LOOP(ee, d.E) {
+        const int e = (int)ee;
+        const int4 en = d.elem_nodes[e];
+        const real4 w = d.w_cv[e];
+        const int nd[4] = {en.x, en.y, en.z, en.w};
+        const double wv[4] = {(double)w.x, (double)w.y, (double)w.z, (double)w.w};
+        double sx = 0.0, sy = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            sx = sx + wv[k] * a.tau_node[2 * (size_t)nd[k]];
+            sy = sy + wv[k] * a.tau_node[2 * (size_t)nd[k] + 1];
+        }
+        d.taux[e] = (real)sx;
+        d.tauy[e] = (real)sy;
+    }
+}
+void launch_atm(const Dev &d, const AtmDev &a, cudaStream_t s) {
+    k_atm_nodes<<<grid_for(d.N, 128), 128, 0, s>>>(d, a);
+    k_atm_stress<<<grid_for(d.E, 256), 256, 0, s>>>(d, a);
+}
+
 // T_aver / S_aver from a range the host gives (fesomc_gpu_set_tracer_range:
 // the min / max over the whole domain of a decomposed mesh), with
 // k_minmax_final's expression

@@ -53,6 +53,7 @@ namespace fesomc {
     void launch_av(const Dev &, cudaStream_t); \
     void launch_minmax(const Dev &, cudaStream_t); \
     void launch_aver_from_range(const Dev &, const double *, cudaStream_t); \
+    void launch_atm(const Dev &, const AtmDev &, cudaStream_t); \
     void launch_upwind(const Dev &, cudaStream_t); \
     void launch_muscl_egrad(const Dev &, cudaStream_t); \
     void launch_muscl_ngrad(const Dev &, cudaStream_t); \
@@ -181,6 +182,13 @@ struct fesomc_model {
     const int *d_nd_ref = nullptr, *d_el_ref = nullptr;
     void *d_perm_buf = nullptr;       // staging of one field in reference order
     size_t perm_buf_bytes = 0;
+    // sbc_do on the device (fesomc_gpu_set_atm_fields): the atmospheric
+    // fields' time-interpolation coefficients (device order) and the stress
+    // per node
+    bool dev_atm = false;
+    double *d_atm_a = nullptr, *d_atm_b = nullptr, *d_tau_node = nullptr;
+    int atm_net_flux = 0;
+    double atm_prec_coef = 1.0;
     // tracer range given by the host (fesomc_gpu_set_tracer_range): tmin,
     // tmax, smin, smax on the device, replacing the step's own min / max
     bool ext_range = false;
@@ -1043,6 +1051,13 @@ int enqueue_step(fesomc_model *m, double ff) {
         rec(m, "forcing", [&] { launch_forcing(forcing_view(m), s); });
         n += 2;
     }
+    if (m->dev_atm) {
+        // sbc_do (fv_main.F90:419), before the step, from the previous
+        // step's surface velocity and temperature
+        const AtmDev a{m->d_atm_a, m->d_atm_b, m->d_clock, m->d_tau_node, m->atm_net_flux, m->atm_prec_coef};
+        rec(m, "atm_fluxes", [&] { fesomc::f64::launch_atm(d, a, s); });
+        n += 2;
+    }
     if (m->p.T_potential) {
         // potential at the head of oce_timestep (fv_main.F90:1899)
         PotentialDev pd{};
@@ -1171,7 +1186,7 @@ int upload_step_inputs(fesomc_model *m, double time, double time_jd) {
     const int nobn = m->d.nobn, nr = m->d.n_rivers;
     const bool need_ob = m->p.TF_presence && nobn > 0;
     const bool need_r = m->p.key_rivers && nr > 0 && m->runoff_dirty;
-    const bool need_clock = m->p.T_potential != 0;
+    const bool need_clock = (m->p.T_potential != 0 || m->dev_atm) && !m->dev_forcing;
     if (!need_ob && !need_r && !need_clock) return FESOMC_OK;
     const int i = m->stage_i;
     m->stage_i ^= 1;
@@ -1457,8 +1472,13 @@ int fesomc_gpu_init_packed(const fesomc_mesh *mesh, const fesomc_params *par, co
     return FESOMC_OK;
 }
 
-int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *f) {
-    if (!m || !f) return FESOMC_EINVAL;
+int fesomc_gpu_set_forcing(fesomc_model *m, const fesomc_forcing *fin) {
+    if (!m || !fin) return FESOMC_EINVAL;
+    // with sbc_do on the device the step forms the winds, the stress and the
+    // surface fluxes itself
+    fesomc_forcing fa = *fin;
+    if (m->dev_atm) fa.taux = fa.tauy = fa.windx = fa.windy = fa.mslp = fa.emp = fa.qsr = fa.qns = nullptr;
+    const fesomc_forcing *f = &fa;
     Dev &d = m->d;
     const size_t N = d.N, E = d.E, L = d.L;
     cudaStream_t s = m->stream;
@@ -2049,6 +2069,34 @@ int fesomc_gpu_set_tracer_range(fesomc_model *m, const double *range) {
     if (!m->ext_range) {
         drop_graph(m);   // the captured step computes its own range
         m->ext_range = true;
+    }
+    return FESOMC_OK;
+}
+
+int fesomc_gpu_set_atm_fields(fesomc_model *m, const double *coef_a, const double *coef_b, int32_t net_flux,
+                              double prec_coef) {
+    if (!m || !coef_a || !coef_b || !m->p.key_atm || m->fp32 || !(prec_coef != 0.0)) return FESOMC_EINVAL;
+    const size_t N = (size_t)m->d.N;
+    int rc;
+    CK(cudaStreamSynchronize(m->stream));
+    if (!m->d_atm_a) {
+        if ((rc = dalloc(m, &m->d_atm_a, 8 * N)) || (rc = dalloc(m, &m->d_atm_b, 8 * N)) ||
+            (rc = dalloc(m, &m->d_tau_node, 2 * N)))
+            return rc;
+    }
+    if (!m->d_clock) {
+        if ((rc = dalloc(m, &m->d_clock, 1))) return rc;
+        CK(cudaMemcpy(m->d_clock, &m->time_jd, sizeof(double), cudaMemcpyHostToDevice));
+    }
+    // reference order [node][8] -> the storage order
+    if ((rc = field_from_host(m, m->d_atm_a, false, 8 * N, coef_a, ENT_NODE)) ||
+        (rc = field_from_host(m, m->d_atm_b, false, 8 * N, coef_b, ENT_NODE)))
+        return rc;
+    m->atm_net_flux = net_flux;
+    m->atm_prec_coef = prec_coef;
+    if (!m->dev_atm) {
+        drop_graph(m);   // the captured step has no surface-flux kernels
+        m->dev_atm = true;
     }
     return FESOMC_OK;
 }

@@ -101,6 +101,7 @@ SIGNATURES = {
     "fesomc_gpu_sync_to_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
     "fesomc_gpu_sync_from_host": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(State)]),
     "fesomc_gpu_set_tracer_range": (C.c_int, [C.c_void_p, f64p]),
+    "fesomc_gpu_set_atm_fields": (C.c_int, [C.c_void_p, f64p, f64p, C.c_int32, C.c_double]),
     "fesomc_gpu_halo_plan": (C.c_int, [C.c_void_p, C.c_int32, i32p, C.c_int32, i32p, C.POINTER(C.c_void_p)]),
     "fesomc_gpu_halo_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "fesomc_gpu_halo_pack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

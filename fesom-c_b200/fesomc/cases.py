@@ -433,6 +433,28 @@ def ensemble_member(index, seed=20261203, nodes_range=ENSEMBLE_NODES, **override
                         seed=d["seed"], **overrides)
 
 
+ATM_FIELDS = ("xwind", "ywind", "humidity", "shortwave", "longwave", "tair", "precipitation", "mslp")
+
+
+def atm_coefficients(mesh, time_jd0, seed=3):
+    """Synthetic atmospheric forcing for sbc_do (fesomc_gpu_set_atm_fields):
+    the time-interpolation coefficients of the 8 fields per node (ATM_FIELDS
+    order; m/s, kg/kg, W/m2, W/m2, K, kg/m2/s, Pa) for fields that vary over
+    the mesh and drift over a day from time_jd0: value(t) = t * a + b, as
+    getcoeffld (src/fv_sbc.F90:664-836) prepares them.  Returns (a, b), each
+    8 values per node in the reference layout coef(i_totfl, nod2D)."""
+    rng = np.random.default_rng(seed)
+    N = mesh.N
+    x = mesh.coord_nod2D[:, 0] / max(mesh.coord_nod2D[:, 0].max(), 1.0)
+    v0 = np.stack([6.0 + 4.0 * x, -3.0 + 2.0 * rng.random(N), 0.004 + 0.002 * rng.random(N),
+                   150.0 + 100.0 * x, 300.0 + 20.0 * rng.random(N), 281.0 + 4.0 * x,
+                   2.0e-5 * rng.random(N), 101000.0 + 600.0 * x], axis=1)
+    rate = np.stack([2.0 + 0 * x, -1.0 + 0 * x, 0.001 + 0 * x, 50.0 * x, 5.0 + 0 * x, 1.5 + 0 * x,
+                     1.0e-6 + 0 * x, 100.0 + 0 * x], axis=1)
+    return (np.ascontiguousarray(rate).reshape(-1),
+            np.ascontiguousarray(v0 - time_jd0 * rate).reshape(-1))
+
+
 def forcing_struct(fdict):
     """fesomc_forcing pointing at the arrays of fdict (kept alive by caller)."""
     f = abi.Forcing()

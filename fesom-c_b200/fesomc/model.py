@@ -32,6 +32,14 @@ class GpuModel:
         self.time_jd = case.params.time_jd0
         self.nstep = 0
 
+    def set_atm_fields(self, coef_a, coef_b, net_flux=0, prec_coef=1.0):
+        """sbc_do on the device from the atmospheric fields' time-interpolation
+        coefficients (fesomc_gpu_set_atm_fields)."""
+        a = np.ascontiguousarray(coef_a, dtype=np.float64)
+        b = np.ascontiguousarray(coef_b, dtype=np.float64)
+        abi.check(self.lib.fesomc_gpu_set_atm_fields(self.h, abi.dptr(a), abi.dptr(b), int(net_flux),
+                                                      float(prec_coef)), "fesomc_gpu_set_atm_fields")
+
     def set_forcing(self, fdict):
         f = cases.forcing_struct(fdict)
         abi.check(self.lib.fesomc_gpu_set_forcing(self.h, C.byref(f)), "fesomc_gpu_set_forcing")

@@ -317,6 +317,24 @@ int  fesomc_gpu_energy(fesomc_model *m, double *eout);
  * FESOMC_EINVAL for packed members or a range with min > max or NaN.  No
  * counterpart in the reference (one MPI reduction there). */
 int  fesomc_gpu_set_tracer_range(fesomc_model *m, const double *range);
+/* sbc_do on the device (src/fv_sbc.F90:1012-1046 with data_timeinterp,
+ * :838-868, and apply_atm_fluxes, :368-482, with the Large & Yeager (2004)
+ * transfer coefficients of core_coeff_2z, :484-662): from the coefficients
+ * that getcoeffld computes from the forcing files (coef_a, coef_b: 8 per
+ * node in the reference layout coef(i_totfl, nod2D): x / y wind at 10 m,
+ * specific humidity, shortwave, longwave, 2 m air temperature,
+ * precipitation, sea-level pressure), every following step forms the fields
+ * at its time_jd (now_date * coef_a + coef_b), the winds, the wind stress
+ * against the surface current (per node, then per element with w_cv), the
+ * non-solar heat flux (longwave less emission when net_flux == 0, as
+ * nm_net_flux), E - P (precipitation divided by prec_coef, nm_prec_coef),
+ * the shortwave and the sea-level pressure, before the step, as the
+ * reference's main loop calls sbc_do before oce_timestep; fesomc_gpu_
+ * set_forcing then leaves those fields alone.  Call again whenever
+ * getcoeffld gives new coefficients.  type_task 3 without sea ice.
+ * FESOMC_EINVAL without key_atm, in the FP32 form or for prec_coef 0. */
+int  fesomc_gpu_set_atm_fields(fesomc_model *m, const double *coef_a, const double *coef_b, int32_t net_flux,
+                               double prec_coef);
 /* Halo exchange of a decomposed mesh on the device (the packed form of
  * exchange_nod / exchange_elem, src/gen_halo_exchange_c.F90:130-165,663-793,
  * for every field of the restart set at once).  A plan lists nodes and

@@ -38,6 +38,7 @@
 #include "../fesom-c_b200/csrc/fesomc_log.h"
 #include "../fesom-c_b200/csrc/fesomc_exp.h"
 #include "../fesom-c_b200/csrc/fesomc_trig.h"
+#include "../fesom-c_b200/csrc/fesomc_atan.h"
 
 /* ---------------------------------------------------------------- consts */
 static const double WP_PI = 3.14159265358979;   /* fv_var.F90:8 */
@@ -2279,6 +2280,134 @@ double oracle_energy(oracle_model *m) {
 }
 
 /* ====================================================================== */
+/* sbc_do: bulk surface fluxes from atmospheric data                       */
+/* ====================================================================== */
+/* psi_h / psi_m, Large & Yeager (2004) eq. 8c-8e (src/fv_sbc.F90:620-662).
+ * SIGN(0.5, x) is copysign (gfortran). */
+static double sbc_psi_h(double zta) {
+    double X2 = sqrt(fabs(1.0 - 16.0 * zta));
+    X2 = MAXD(X2, 1.0);
+    const double stabit = 0.5 + copysign(0.5, zta);
+    return -5.0 * zta * stabit + (1.0 - stabit) * (2.0 * fesomc_log((1.0 + X2) / 2.0));
+}
+static double sbc_psi_m(double zta) {
+    double X2 = sqrt(fabs(1.0 - 16.0 * zta));
+    X2 = MAXD(X2, 1.0);
+    const double X = sqrt(X2);
+    const double stabit = 0.5 + copysign(0.5, zta);
+    const double pi = 3.141592653589793;
+    return -5.0 * zta * stabit + (1.0 - stabit) * (2.0 * fesomc_log((1.0 + X) / 2.0) + fesomc_log((1.0 + X2) / 2.0) -
+                                                    2.0 * fesomc_atan(X) + pi / 2.0);
+}
+
+/* core_coeff_2z (src/fv_sbc.F90:484-641): transfer coefficients Cd, Ch, Ce
+ * and the air temperature / humidity shifted to zu, 5 iterations. */
+static void sbc_core_coeff_2z(double zt, double zu, double sst, double T_zt, double q_sat, double q_zt, double dU,
+                              double *Cd_o, double *Ch_o, double *Ce_o, double *T_zu_o, double *q_zu_o) {
+    const double grav = 9.8, kappa = 0.4;
+    const double dU10 = MAXD(0.5, dU);
+    double dT = T_zt - sst;
+    double dq = q_zt - q_sat;
+    double stab = 0.5 + copysign(0.5, dT);
+    double Cd_n10 = 1E-3 * (2.7 / dU10 + 0.142 + dU10 / 13.09);
+    double sqrt_Cd_n10 = sqrt(Cd_n10);
+    double Ce_n10 = 1E-3 * (34.6 * sqrt_Cd_n10);
+    double Ch_n10 = 1E-3 * sqrt_Cd_n10 * (18.0 * stab + 32.7 * (1.0 - stab));
+    double Cd = Cd_n10, Ce = Ce_n10, Ch = Ch_n10, sqrt_Cd = sqrt(Cd);
+    double T_zu = T_zt, q_zu = q_zt;
+    for (int j_itt = 1; j_itt <= 5; ++j_itt) {
+        dT = T_zu - sst;
+        dq = q_zu - q_sat;
+        const double T_vpot = T_zu * (1.0 + 0.608 * q_zu);
+        const double U_star = sqrt_Cd * dU10;
+        const double T_star = Ch / sqrt_Cd * dT;
+        const double q_star = Ce / sqrt_Cd * dq;
+        const double L = (U_star * U_star) / (kappa * grav / T_vpot * (T_star * (1.0 + 0.608 * q_zu) + 0.608 * T_zu * q_star));
+        double zeta_u = zu / L;
+        zeta_u = copysign(MIND(fabs(zeta_u), 10.0), zeta_u);
+        double zeta_t = zt / L;
+        zeta_t = copysign(MIND(fabs(zeta_t), 10.0), zeta_t);
+        const double zpsi_hu = sbc_psi_h(zeta_u);
+        const double zpsi_ht = sbc_psi_h(zeta_t);
+        const double zpsi_m = sbc_psi_m(zeta_u);
+        const double U_n10 = MAXD(0.25, dU10 / (1.0 + sqrt_Cd_n10 / kappa * (fesomc_log(zu / 10.0) - zpsi_m)));
+        T_zu = T_zt - T_star / kappa * (fesomc_log(zt / zu) + zpsi_hu - zpsi_ht);
+        q_zu = q_zt - q_star / kappa * (fesomc_log(zt / zu) + zpsi_hu - zpsi_ht);
+        stab = 0.5 + copysign(0.5, q_zu);
+        q_zu = stab * q_zu;
+        Cd_n10 = 1E-3 * (2.7 / U_n10 + 0.142 + U_n10 / 13.09);
+        sqrt_Cd_n10 = sqrt(Cd_n10);
+        Ce_n10 = 1E-3 * (34.6 * sqrt_Cd_n10);
+        stab = 0.5 + copysign(0.5, zeta_u);
+        Ch_n10 = 1E-3 * sqrt_Cd_n10 * (18.0 * stab + 32.7 * (1.0 - stab));
+        double xct = 1.0 + sqrt_Cd_n10 / kappa * (fesomc_log(zu / 10.0) - zpsi_m);
+        Cd = Cd_n10 / (xct * xct);
+        sqrt_Cd = sqrt(Cd);
+        const double xlogt = fesomc_log(zu / 10.0) - zpsi_hu;
+        xct = 1.0 + Ch_n10 * xlogt / kappa / sqrt_Cd_n10;
+        Ch = Ch_n10 * sqrt_Cd / sqrt_Cd_n10 / xct;
+        xct = 1.0 + Ce_n10 * xlogt / kappa / sqrt_Cd_n10;
+        Ce = Ce_n10 * sqrt_Cd / sqrt_Cd_n10 / xct;
+    }
+    *Cd_o = Cd; *Ch_o = Ch; *Ce_o = Ce; *T_zu_o = T_zu; *q_zu_o = q_zu;
+}
+
+/* sbc_do's data_timeinterp and apply_atm_fluxes (src/fv_sbc.F90:838-868,
+ * 368-482) for type_task 3 without sea ice: atmdata(f, i) = now_date *
+ * coef_a(f, i) + coef_b(f, i) for the 8 fields (x / y wind, humidity,
+ * shortwave, longwave, air temperature, precipitation, sea-level pressure),
+ * then windx, windy, qns, emp, qsr, mslp per node and the stress per node,
+ * averaged onto the elements with w_cv.  The relative wind subtracts the
+ * surface Unode / Vnode the model holds (those of the previous step), the
+ * surface temperature is TF's top layer.  rhoa, albo and emiss_wat are
+ * REAL(4) literals in the Fortran. */
+int oracle_atm_fluxes(oracle_model *m, const double *coef_a, const double *coef_b, int net_flux, double prec_coef,
+                      double now_date) {
+    const double rhoa = R4(1.3f), cpa = 1005.0, Lv = 2.5e6, Stef = 5.67e-8, albo = R4(0.1f), emiss_wat = R4(0.97f);
+    double *tn = (double *)malloc(sizeof(double) * 2 * (size_t)m->N);
+    if (!tn) return 1;
+    for (int i = 1; i <= m->N; ++i) {
+        double atm[8];
+        for (int f = 0; f < 8; ++f) atm[f] = now_date * coef_a[8 * (size_t)(i - 1) + f] + coef_b[8 * (size_t)(i - 1) + f];
+        N1(m->windx, i) = atm[0];
+        N1(m->windy, i) = atm[1];
+        const double wdx = atm[0] - F3(m->Unode, 1, i);
+        const double wdy = atm[1] - F3(m->Vnode, 1, i);
+        const double wndm = sqrt(wdx * wdx + wdy * wdy);
+        const double zst = F3(m->TF, 1, i) + 273.15;
+        const double q_sat = 0.98 * 640380.0 / rhoa * fesomc_exp(-5107.4 / zst);
+        double Cd, Ch, Ce, t_zu, q_zu;
+        sbc_core_coeff_2z(2.0, 10.0, zst, atm[5], q_sat, atm[2], wndm, &Cd, &Ch, &Ce, &t_zu, &q_zu);
+        const double rtmp = rhoa * wndm * Cd;
+        tn[2 * (size_t)(i - 1)] = rtmp * wdx;
+        tn[2 * (size_t)(i - 1) + 1] = rtmp * wdy;
+        const double zevap = MAXD(0.0, rhoa * Ce * (q_sat - q_zu) * wndm);
+        const double zqsb = rhoa * cpa * Ch * (zst - t_zu) * wndm;
+        const double zqlw = net_flux == 0 ? atm[4] - emiss_wat * Stef * zst * zst * zst * zst : atm[4];
+        const double zqla = Lv * zevap;
+        double qns = zqlw - zqsb - zqla;
+        if (F3(m->TF, 1, i) < -2.0 && qns < 0.0) qns = 0.0;
+        N1(m->qns, i) = qns;
+        N1(m->emp, i) = zevap - atm[6] / prec_coef;
+        N1(m->qsr, i) = (1.0 - albo) * atm[3];
+        N1(m->mslp, i) = atm[7];
+    }
+    for (int el = 1; el <= m->E; ++el) {
+        double sx = 0.0, sy = 0.0;
+        for (int k = 1; k <= 4; ++k) {
+            sx = sx + WCV(k, el) * tn[2 * (size_t)(ELN(k, el) - 1)];
+            sy = sy + WCV(k, el) * tn[2 * (size_t)(ELN(k, el) - 1) + 1];
+        }
+        N1(m->taux, el) = sx;
+        N1(m->tauy, el) = sy;
+    }
+    free(tn);
+    return 0;
+}
+
+double oracle_atan(double x) { return fesomc_atan(x); }
+
+/* ====================================================================== */
 /* public API                                                              */
 /* ====================================================================== */
 oracle_model *oracle_create(const fesomc_mesh *msh, const fesomc_params *par, const fesomc_state *st) {
@@ -2413,6 +2542,8 @@ const double *oracle_array(oracle_model *m, const char *name, int64_t *count) {
         {"Bar_prv_3D", m->Bar_prv_3D, L * E}, {"vel_grad", m->vel_grad, 4 * E}, {"UAB", m->UAB, 2 * E},
         {"ssh_rhs", m->ssh_rhs, N}, {"U_rhs_2D_3D", m->U_rhs_2D_3D, 2 * E}, {"mask_ad", m->mask_ad, N},
         {"vgux", m->vgux, L * E}, {"vguy", m->vguy, L * E}, {"vgvx", m->vgvx, L * E}, {"vgvy", m->vgvy, L * E},
+        {"taux", m->taux, E}, {"tauy", m->tauy, E}, {"windx", m->windx, N}, {"windy", m->windy, N},
+        {"qns", m->qns, N}, {"qsr", m->qsr, N}, {"emp", m->emp, N}, {"mslp", m->mslp, N},
     };
     for (size_t i = 0; i < sizeof(t) / sizeof(t[0]); ++i)
         if (strcmp(t[i].n, name) == 0) { if (count) *count = t[i].c; return t[i].p; }

@@ -51,6 +51,10 @@ def load(abi):
         lib.oracle_densityJM.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
         lib.oracle_log.restype = C.c_double
         lib.oracle_log.argtypes = [C.c_double]
+        lib.oracle_atm_fluxes.restype = C.c_int
+        lib.oracle_atm_fluxes.argtypes = [C.c_void_p, abi.f64p, abi.f64p, C.c_int, C.c_double, C.c_double]
+        lib.oracle_atan.restype = C.c_double
+        lib.oracle_atan.argtypes = [C.c_double]
         lib.oracle_cos.restype = C.c_double
         lib.oracle_cos.argtypes = [C.c_double]
         lib.oracle_sin.restype = C.c_double
@@ -118,6 +122,13 @@ class Oracle:
             raise RuntimeError("oracle_create failed")
         self.time_jd = case.params.time_jd0
         self.nstep = 0
+        self.atm = None
+
+    def set_atm_fields(self, coef_a, coef_b, net_flux=0, prec_coef=1.0):
+        """sbc_do before every step from the time-interpolation coefficients
+        (8 per node, reference layout), as fesomc_gpu_set_atm_fields."""
+        self.atm = (np.ascontiguousarray(coef_a, dtype=np.float64), np.ascontiguousarray(coef_b, dtype=np.float64),
+                    int(net_flux), float(prec_coef))
 
     def step(self, nsteps=1):
         rc = 0
@@ -127,6 +138,10 @@ class Oracle:
             f = self.case.forcing_fn(self.nstep, t_next)
             fs = self.cm.forcing_struct(f)
             self.lib.oracle_set_forcing(self.h, C.byref(fs))
+            if self.atm is not None:
+                a, b, nf, pc = self.atm
+                self.lib.oracle_atm_fluxes(self.h, a.ctypes.data_as(C.POINTER(C.c_double)),
+                                           b.ctypes.data_as(C.POINTER(C.c_double)), nf, pc, t_next)
             rc |= self.lib.oracle_step(self.h)
             self.time_jd = t_next
         return rc

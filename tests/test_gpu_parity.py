@@ -485,6 +485,43 @@ def test_two_kernel_forms_bit_exact(mods, variant):
     assert abs(eg - eo) <= 1e-12 * abs(eo)
 
 
+@pytest.mark.parametrize("net_flux,sfc", [(0, 0), (1, 1)])
+def test_device_surface_fluxes_bit_exact(mods, net_flux, sfc):
+    """sbc_do on the device (fesomc_gpu_set_atm_fields: the atmospheric
+    fields at every step's time, the Large & Yeager bulk formulae of
+    apply_atm_fluxes / core_coeff_2z, the stress onto the elements) against
+    the oracle's restatement, 20 steps on the small estuary, exact; with the
+    longwave as a net flux and the mesh stored along the Hilbert curve in
+    the second case."""
+    abi, cases, model, pyoracle = mods
+    gcase, ocase = build_pair(mods, est(cases, "small", atm={"qns": 0.0}))
+    gcase.params.sfc_order = sfc
+    a, b = cases.atm_coefficients(gcase.mesh, gcase.params.time_jd0)
+    g = model.GpuModel(gcase)
+    o = pyoracle.Oracle(ocase, abi, cases)
+    try:
+        g.set_atm_fields(a, b, net_flux, 1.0)
+        o.set_atm_fields(a, b, net_flux, 1.0)
+        g.step(20)
+        o.step(20)
+        assert compare(g.state(), o.state()) == []
+        eg, eo = g.energy(), o.energy()
+        assert abs(eg - eo) <= 1e-12 * abs(eo)
+    finally:
+        g.close()
+        o.close()
+
+
+def test_device_surface_fluxes_refused_without_key_atm(mods):
+    abi, cases, model, pyoracle = mods
+    g = model.GpuModel(cases.estuary("small"))
+    try:
+        a, b = cases.atm_coefficients(g.case.mesh, g.case.params.time_jd0)
+        assert g.lib.fesomc_gpu_set_atm_fields(g.h, abi.dptr(a), abi.dptr(b), 0, 1.0) == 1
+    finally:
+        g.close()
+
+
 def test_key_atm_changes_the_run_and_fp32_form_runs(mods):
     """The surface heat loss cools the estuary against the run without it,
     and the FP32 form runs the same forcing (finite, within 0.01 C of FP64)."""

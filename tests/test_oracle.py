@@ -191,6 +191,56 @@ def test_shared_cos_within_one_ulp_of_libm(mods):
     assert math.isnan(lib.oracle_cos(2e6)) and math.isnan(lib.oracle_cos(math.inf))
 
 
+def test_shared_atan_within_four_ulp_of_libm(mods):
+    """fesomc_atan (psi_m of the bulk transfer coefficients, shared by the
+    oracle and the device surface-flux kernel) against the C library's
+    atan: at most 4 ulp apart over 12 decades of argument, exact at the
+    reduction points."""
+    abi, cases, pyoracle = mods
+    lib = pyoracle.load(abi)
+    rng = np.random.default_rng(11)
+    xs = np.concatenate([rng.uniform(-4.0, 4.0, 20000), np.exp(rng.uniform(-14.0, 14.0, 20000)),
+                         -np.exp(rng.uniform(-14.0, 14.0, 5000)), [0.0, 1.0, -1.0, 1e-300, 1e300]])
+    ours = np.array([lib.oracle_atan(float(x)) for x in xs])
+    ref = np.array([math.atan(float(x)) for x in xs])
+    ulps = np.abs(ours.view(np.int64) - ref.view(np.int64))
+    assert ulps.max() <= 4
+    assert lib.oracle_atan(1.0) == math.atan(1.0) and lib.oracle_atan(0.0) == 0.0
+    assert lib.oracle_atan(math.inf) == math.pi / 2 and math.isnan(lib.oracle_atan(math.nan))
+
+
+def test_bulk_surface_fluxes_in_range(mods):
+    """The oracle's sbc_do (bulk formulae of apply_atm_fluxes and
+    core_coeff_2z, src/fv_sbc.F90:368-662): with 6-10 m/s winds over a
+    12 C sea, the stress is of order rho_a Cd U^2 (Cd about 1.2e-3), it
+    points along the wind, the sea loses heat to the colder, drier air
+    through evaporation and sensible heat, and E - P is evaporation less
+    precipitation."""
+    abi, cases, pyoracle = mods
+    c = cases.estuary("small", atm={"qns": 0.0})
+    o = pyoracle.Oracle(c, abi, cases)
+    try:
+        a, b = cases.atm_coefficients(c.mesh, c.params.time_jd0)
+        o.set_atm_fields(a, b, net_flux=0, prec_coef=1.0)
+        o.step(1)
+        t = o.time_jd
+        atm = (t * a + b).reshape(-1, 8)
+        wx = o.array("windx")
+        assert np.array_equal(wx, atm[:, 0])
+        tx, ty = o.array("taux"), o.array("tauy")
+        speed2 = (atm[:, 0] ** 2 + atm[:, 1] ** 2).mean()
+        assert 0.5e-3 < np.abs(tx).mean() / (1.3 * speed2 ** 0.5 * np.abs(atm[:, 0]).mean()) < 3e-3
+        assert (tx > 0).all() and (ty < 0).mean() > 0.5
+        qns = o.array("qns")
+        assert np.isfinite(qns).all() and (qns < 0).all()
+        emp = o.array("emp")
+        assert (emp > -atm[:, 6]).all()          # evaporation over the drier air
+        assert np.allclose(o.array("qsr"), (1.0 - float(np.float32(0.1))) * atm[:, 3])
+        assert np.array_equal(o.array("mslp"), atm[:, 7])
+    finally:
+        o.close()
+
+
 def test_shared_sin_within_one_ulp_of_libm(mods):
     """fesomc_sin (the equilibrium tide of the tidal potential) against the C
     library's sin, as the cosine above."""
