@@ -1264,6 +1264,10 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
     real *sT = reinterpret_cast<real *>(vt_smem);  // row j: node n0 + j
     real *sS = sT + kVtCols * LP;
     real *sK = sS + kVtCols * LP;
+    // with the atmospheric sources: the heat source of every (node, layer),
+    // formed in the staging phase by all threads instead of in the serial
+    // column solve
+    real *sH = sK + kVtCols * KP;
     for (long long n0 = (long long)blockIdx.x * kVtCols; n0 < N; n0 += (long long)gridDim.x * kVtCols) {
         const int nt = (int)(N - n0 < kVtCols ? N - n0 : kVtCols);
         // staging: kVtBatch items per thread loaded before any is used, so
@@ -1299,8 +1303,13 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
                 const int j = i / L, z = i - j * L;
                 const int n = (int)n0 + j;
                 const size_t g = (size_t)n0 * L + i;
+                const real ajn = jac_a(d, d.eta_jac, n);
                 sT[j * LP + z] = ta[u] - t_aver_of(d, n);
-                sS[j * LP + z] = vd_salt_of(d, n, z, jac_a(d, d.eta_jac, n), sa[u], sn[u], s_aver_of(d, n));
+                sS[j * LP + z] = vd_salt_of(d, n, z, ajn, sa[u], sn[u], s_aver_of(d, n));
+                if (kAtm)
+                    sH[j * LP + z] = d.mask_wd_node[n] != real(0.0)
+                                         ? heat_source(d, n, (size_t)n * L, z, ajn, t_aver_of(d, n), s_aver_of(d, n))
+                                         : real(0.0);
                 d.T_old[g] = tn[u];
                 d.S_old[g] = sn[u];
             }
@@ -1333,7 +1342,7 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
                     sr = -a * S[k - 1] - c * S[k + 1] + (a + c) * S0;
                 }
                 if (atm) {
-                    tr = tr + d.dt * heat_source(d, n, base, k, aj, T_aver, S_aver);
+                    tr = tr + d.dt * sH[j * LP + k];
                     if (k == 0) sr = sr + d.dt * frw;
                 }
                 if (k == 0) {
@@ -1381,8 +1390,8 @@ __global__ void __launch_bounds__(kVtCols) k_vdiff_tile(Dev d) {
 
 // columns per tile: 128 (vdiff_form 2) or 64 (3, the default)
 static int vdiff_cols(const Dev &d) { return d.tune[TK_VDIFF] == 2 ? 128 : 64; }
-static size_t vdiff_tile_smem(const Dev &d, int cols) {
-    return (size_t)cols * (2 * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
+static size_t vdiff_tile_smem(const Dev &d, int cols, bool atm) {
+    return (size_t)cols * ((atm ? 3 : 2) * vd_odd(d.L) + vd_odd(d.NS)) * sizeof(real);
 }
 // the tiled form is compiled for 10 and 20 layers (11 and 21 sigma levels)
 static bool vdiff_tiled(const Dev &d) { return d.tune[TK_VDIFF] != 1 && (d.L == 10 || d.L == 20); }
@@ -1391,9 +1400,8 @@ static int vdiff_block(const Dev &d) { return d.L <= 48 ? kVdBlock : 32; }
 static size_t vdiff_smem(const Dev &d) { return (size_t)3 * d.L * vdiff_block(d) * sizeof(real); }
 template <int LC, int C>
 static bool config_vdiff_tile(const Dev &d) {
-    const size_t sm = vdiff_tile_smem(d, C);
-    return raise_smem_limit(k_vdiff_tile<false, LC, C>, sm) == cudaSuccess &&
-           raise_smem_limit(k_vdiff_tile<true, LC, C>, sm) == cudaSuccess;
+    return raise_smem_limit(k_vdiff_tile<false, LC, C>, vdiff_tile_smem(d, C, false)) == cudaSuccess &&
+           raise_smem_limit(k_vdiff_tile<true, LC, C>, vdiff_tile_smem(d, C, true)) == cudaSuccess;
 }
 int config_vdiff(const Dev &d) {
     if (raise_smem_limit(k_vdiff_col<false>, vdiff_smem(d)) != cudaSuccess ||
@@ -1407,9 +1415,8 @@ template <int LC, int C>
 static void launch_vdiff_tile(const Dev &d, cudaStream_t s) {
     const long long tiles = ((long long)d.N + C - 1) / C;
     const int g = (int)(tiles < (1LL << 30) ? tiles : (1LL << 30));
-    const size_t sm = vdiff_tile_smem(d, C);
-    if (d.key_atm) k_vdiff_tile<true, LC, C><<<g, C, sm, s>>>(d);
-    else k_vdiff_tile<false, LC, C><<<g, C, sm, s>>>(d);
+    if (d.key_atm) k_vdiff_tile<true, LC, C><<<g, C, vdiff_tile_smem(d, C, true), s>>>(d);
+    else k_vdiff_tile<false, LC, C><<<g, C, vdiff_tile_smem(d, C, false), s>>>(d);
 }
 void launch_vdiff(const Dev &d, cudaStream_t s) {
     if (vdiff_tiled(d)) {
