@@ -218,7 +218,13 @@ template <typename T>
 static int lc_alloc(LcNet *n, T **p, size_t count) {
     void *q = nullptr;
     if (cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) return FESOMC_ENOMEM_LC;
+    // zero fill on the legacy default stream, finished before the closure's
+    // non-blocking stream may touch the buffer
     cudaMemset(q, 0, std::max<size_t>(count, 1) * sizeof(T));
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        cudaFree(q);
+        return FESOMC_ECUDA_LC;
+    }
     n->allocs.push_back(q);
     *p = static_cast<T *>(q);
     return 0;

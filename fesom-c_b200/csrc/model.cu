@@ -227,7 +227,15 @@ int dalloc(fesomc_model *m, T **p, size_t n) {
     void *q = nullptr;
     cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
     if (e != cudaSuccess) return FESOMC_ENOMEM;
+    // the zero fill runs on the legacy default stream, which the model's
+    // non-blocking streams do not wait for: let it land before anything
+    // is enqueued on them (an upload into a buffer allocated just before
+    // could otherwise be overwritten by the fill)
     cudaMemset(q, 0, (n ? n : 1) * sizeof(T));
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+        cudaFree(q);
+        return FESOMC_ECUDA;
+    }
     m->allocs.push_back(q);
     *p = static_cast<T *>(q);
     return FESOMC_OK;
@@ -2386,6 +2394,7 @@ int fesomc_closure_attach(fesomc_model *m, fesomc_closure *c, int32_t judge_ever
     m->lcv.rules = c->net->rules;
     CK(cudaMemset(m->lcv.acc, 0, 4 * sizeof(unsigned long long)));
     CK(cudaMemset(m->lcv.judge, 0, 3 * sizeof(double)));
+    CK(cudaDeviceSynchronize());   // the fills (legacy stream) before the model stream's next step
     m->lc = c->net;
     m->lc_on = true;
     m->lc_judge_every = judge_every;
