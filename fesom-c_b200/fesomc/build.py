@@ -4,6 +4,17 @@ Host C++ (mesh builder, orchestration helpers) is compiled with g++, CUDA
 sources with nvcc for compute_100a/sm_100a.  FMA contraction is off in both so
 the FP64 path follows the reference's operation order (bit-for-bit parity
 with the CPU oracle, which is built the same way).
+
+The FP32-form objects (the second compilation of the kernel sources, which
+holds only fesomc::f32 kernels) are held to an error budget against the FP64
+path instead of to bit parity, so they are compiled for speed: FMA
+contraction, FP32 division and square root to within 2 ulp instead of
+correctly rounded, FP32 subnormals flushed to zero.  These flags act on
+every operation of those objects, the FP64 elevation family of the form
+included (contraction only: FP64 division and square root stay correctly
+rounded whatever the flags).  The results are still deterministic, and two
+runs of the form that differ only in launch shapes, storage order, packing
+or decomposition give the same bits.
 """
 import concurrent.futures as cf
 import glob
@@ -19,6 +30,8 @@ INC = os.path.join(REPO_DIR, "include")
 OBJ_DIR = os.path.join(ROOT_DIR, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 DUAL_PRECISION = ("k_baroclinic.cu", "k_barotropic.cu", "k_tracer.cu", "k_mixing.cu", "k_closure.cu")
+FP64_FLAGS = ["--fmad=false"]
+FP32_FORM_FLAGS = ["--fmad=true", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
 
 
 def _nvcc():
@@ -55,7 +68,8 @@ def _compile(cmd):
 
 def build_library(verbose=False, ptxas_v=False):
     os.makedirs(OBJ_DIR, exist_ok=True)
-    hdrs = _headers()
+    # this file holds the compile flags: a change to them rebuilds every object
+    hdrs = _headers() + [os.path.abspath(__file__)]
     jobs, objs = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "**", "*.cpp"), recursive=True)):
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
@@ -74,9 +88,9 @@ def build_library(verbose=False, ptxas_v=False):
             obj = os.path.join(OBJ_DIR, os.path.basename(src) + suffix + ".o")
             objs.append(obj)
             if _stale(obj, [src] + hdrs) or ptxas_v:
-                cmd = [nvcc] + ARCH + ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-                                       "-ccbin", _cxx(), "-DFESOMC_FP32=" + fp32, "-I", INC, "-I", CSRC, "-c", src,
-                                       "-o", obj]
+                cmd = [nvcc] + ARCH + ["-lineinfo", "-O3"] + (FP32_FORM_FLAGS if fp32 == "1" else FP64_FLAGS) + [
+                    "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", _cxx(), "-DFESOMC_FP32=" + fp32, "-I", INC,
+                    "-I", CSRC, "-c", src, "-o", obj]
                 if ptxas_v:
                     cmd += ["-Xptxas", "-v"]
                 jobs.append(cmd)
