@@ -1,8 +1,9 @@
 """The FP32 form (fesomc_params.fp32_form = 1): level fields, mesh geometry
 and the 3D arithmetic in FP32, the barotropic sub-cycle and the energy
 integral in FP64.  It is compared with the plain FP64 path on the same case
-through the C-ABI.  Tolerances follow the north-star error budget (SSH RMS
-1 mm, T/S 0.01) scaled to these short runs, and the domain volume, whose
+through the C-ABI.  Tolerances follow the form's error budget against the
+FP64 path (SSH RMS 1 mm, T/S 0.01) scaled to these short runs, and the
+domain volume, whose
 accumulation stays FP64, is held to round-off in a closed basin."""
 import numpy as np
 import pytest
