@@ -151,7 +151,9 @@ typedef struct fesomc_params {
      * 1 = FP32 form: level fields, the 2D momentum, mesh geometry and the
      *     flux / advection / viscosity / tracer / mixing arithmetic in FP32;
      *     the elevation, SSH and total-depth accumulation, wet/dry tests
-     *     and the energy integral stay FP64.                                */
+     *     and the energy integral stay FP64.  Its kernels are compiled
+     *     with FMA contraction and FP32 division / square root to 2 ulp;
+     *     its results are deterministic but not those of form 0.          */
     int32_t fp32_form;
     /* biharmonic viscosity of the 3D momentum (bih_3D, Abh0 of fv_run.dat,
      * src/fv_read_run.F90:320-326,396-401; biharmonic_viscosity,
